@@ -1,0 +1,75 @@
+/*
+ * broccoli_oracle.h -- CPU restatement of BROCCOLI's registration and
+ * filtering path.  TEST INFRASTRUCTURE ONLY: the product (libbroccoli_b200)
+ * never links or calls this code.  It is the checker that the CUDA path is
+ * compared against, and the timed CPU baseline of bench.py.
+ *
+ * Every function exists twice, with suffix _f32 (float arithmetic, the
+ * parity target: same operation order as the reference's OpenCL kernels) and
+ * _f64 (double arithmetic, the accuracy oracle).  `real` below is float or
+ * double accordingly.
+ *
+ * Layouts follow the reference (code/Kernels/kernelRegistration.cpp:32-40):
+ *   volume index  = x + y*W + z*W*H (+ t*W*H*D)
+ *   7x7x7 filters = 343 reals, x fastest; one filter is re[343] then im[343]
+ *   complex response = interleaved (re, im) pairs, one volume per filter
+ *   parameters    = [tx ty tz a11-1 a12 a13 a21 a22-1 a23 a31 a32 a33-1]
+ */
+#ifndef BROCCOLI_ORACLE_H
+#define BROCCOLI_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ORC_TRANSLATION = 0, ORC_RIGID = 1, ORC_AFFINE = 2 };
+
+#define ORC_DECLARE(real, SFX)                                                  \
+  void orc_filter3d##SFX(const real* vol, int W, int H, int D,                  \
+                         const real* filters, int nfilt, real* out);            \
+  void orc_phase_diff_cert##SFX(const real* q1, const real* q2, long V,         \
+                                real* pd, real* cert);                          \
+  void orc_phase_grad##SFX(const real* q1, const real* q2, int axis, int W,     \
+                           int H, int D, real* grad);                           \
+  void orc_ah_axis##SFX(const real* pd, const real* grad, const real* cert,     \
+                        int axis, int W, int H, int D, int filter_size,         \
+                        real* A144, real* h12);                                 \
+  void orc_normal_equations##SFX(const real* q1, const real* q2, int W, int H,  \
+                                 int D, real* A144, real* h12);                 \
+  void orc_solve##SFX(const real* A, const real* h, int n, real* p);            \
+  void orc_remove_scaling##SFX(real* p12);                                      \
+  void orc_add_affine##SFX(real* old12, const real* new12);                     \
+  void orc_add_affine_next_scale##SFX(real* old12, const real* new12);          \
+  void orc_rotation_angles##SFX(const real* p12, real* rot3);                   \
+  void orc_warp_affine##SFX(const real* src, int W, int H, int D,               \
+                            const real* p12, real* out);                        \
+  void orc_warp_field##SFX(const real* src, int W, int H, int D,                \
+                           const real* dx, const real* dy, const real* dz,      \
+                           real* out);                                          \
+  void orc_align_linear##SFX(const real* ref, real* aligned,                    \
+                             const real* original, int W, int H, int D,         \
+                             const real* filters, int niter, int type,          \
+                             real* p12, real* rot3);                            \
+  void orc_motion_correct##SFX(real* vols, int W, int H, int D, int T,          \
+                               const real* voxel_size, const real* filters,     \
+                               int niter, real* motion6T);                      \
+  void orc_smoothing_filter_sigma##SFX(int size, double sigma, real* f);        \
+  void orc_smoothing_filter_fwhm##SFX(int size, double fwhm, double vx,         \
+                                      double vy, double vz, real* fx,           \
+                                      real* fy, real* fz);                      \
+  void orc_smooth3d##SFX(const real* vol, const real* cert,                     \
+                         const real* smoothed_cert, int W, int H, int D,        \
+                         const real* fx, const real* fy, const real* fz,        \
+                         real* out);                                            \
+  void orc_rescale_linear##SFX(const real* src, int W, int H, int D, int W2,    \
+                               int H2, int D2, real* out);
+
+ORC_DECLARE(float, _f32)
+ORC_DECLARE(double, _f64)
+
+int orc_num_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,353 @@
+"""ctypes bindings of the CPU oracle.
+
+TEST INFRASTRUCTURE ONLY.  Only tests/, ``__graft_entry__.smoke()`` and the
+CPU-baseline legs of ``bench.py`` import this module, as the checker.  The
+product package ``broccoli_b200`` never imports it.
+
+Two libraries are bound:
+
+* ``liborc.so`` -- the C restatement (``orc_impl.h``), float (``*_f32``, the
+  FP32 parity target) and double (``*_f64``, the accuracy oracle).
+* ``_ref/libbroccoli_ref.so`` -- the reference's own OpenCL C kernels compiled
+  for the CPU through ``clshim.hpp`` with the host loops restated
+  (``ref_shim.cpp``).  Present only where it was built.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORC_PATH = os.path.join(HERE, "liborc.so")
+REF_PATH = os.path.join(HERE, "_ref", "libbroccoli_ref.so")
+
+TRANSLATION, RIGID, AFFINE = 0, 1, 2
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_L = ctypes.c_long
+_D = ctypes.c_double
+
+
+def build(ref: bool = False) -> None:
+    """Compile liborc.so (and _ref/ when the reference tree is present)."""
+    subprocess.check_call(["make", "-s", "-C", HERE, "all"])
+    if ref:
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
+
+
+_orc = None
+_ref = None
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_P)
+
+
+def orc_lib():
+    global _orc
+    if _orc is None:
+        if not os.path.exists(ORC_PATH):
+            build()
+        _orc = ctypes.CDLL(ORC_PATH)
+    return _orc
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_PATH)
+
+
+def ref_lib():
+    global _ref
+    if _ref is None:
+        _ref = ctypes.CDLL(REF_PATH)
+    return _ref
+
+
+def _dt(prec: str):
+    return (np.float32, "_f32") if prec == "f32" else (np.float64, "_f64")
+
+
+def _arr(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def num_threads() -> int:
+    return orc_lib().orc_num_threads()
+
+
+# --------------------------------------------------------------------------
+# restatement (liborc.so)
+# --------------------------------------------------------------------------
+
+def filter3d(vol: np.ndarray, filters: np.ndarray, prec: str = "f32") -> np.ndarray:
+    """Complex responses of `vol` (D,H,W) to nfilt 7^3 filters.
+
+    `filters` has shape (nfilt, 2, 7, 7, 7) (re/im, z, y, x).  Returns
+    complex array (nfilt, D, H, W)."""
+    dt, s = _dt(prec)
+    D, H, W = vol.shape
+    f = _arr(filters, dt)
+    nf = f.shape[0]
+    v = _arr(vol, dt)
+    out = np.empty((nf, D, H, W, 2), dt)
+    getattr(orc_lib(), "orc_filter3d" + s)(_ptr(v), W, H, D, _ptr(f), nf, _ptr(out))
+    return out[..., 0] + 1j * out[..., 1]
+
+
+def _interleave(q: np.ndarray, dt) -> np.ndarray:
+    out = np.empty(q.shape + (2,), dt)
+    out[..., 0] = q.real
+    out[..., 1] = q.imag
+    return out
+
+
+def normal_equations(q1: np.ndarray, q2: np.ndarray, prec: str = "f32"):
+    """A (12x12) and h (12) of one affine iteration from (3,D,H,W) complex
+    responses of the reference (q1) and aligned (q2) volumes."""
+    dt, s = _dt(prec)
+    _, D, H, W = q1.shape
+    a = _interleave(q1, dt)
+    c = _interleave(q2, dt)
+    A = np.zeros(144, dt)
+    h = np.zeros(12, dt)
+    getattr(orc_lib(), "orc_normal_equations" + s)(_ptr(a), _ptr(c), W, H, D, _ptr(A), _ptr(h))
+    return A.reshape(12, 12).T.copy(), h
+
+
+def solve(A: np.ndarray, h: np.ndarray, prec: str = "f32") -> np.ndarray:
+    dt, s = _dt(prec)
+    n = h.shape[0]
+    Acm = _arr(np.asarray(A).T, dt)  # column-major
+    hv = _arr(h, dt)
+    p = np.zeros(n, dt)
+    getattr(orc_lib(), "orc_solve" + s)(_ptr(Acm), _ptr(hv), n, _ptr(p))
+    return p
+
+
+def remove_scaling(p: np.ndarray, prec: str = "f32") -> np.ndarray:
+    dt, s = _dt(prec)
+    q = _arr(p, dt).copy()
+    getattr(orc_lib(), "orc_remove_scaling" + s)(_ptr(q))
+    return q
+
+
+def add_affine(old: np.ndarray, new: np.ndarray, prec: str = "f32") -> np.ndarray:
+    dt, s = _dt(prec)
+    o = _arr(old, dt).copy()
+    n = _arr(new, dt)
+    getattr(orc_lib(), "orc_add_affine" + s)(_ptr(o), _ptr(n))
+    return o
+
+
+def rotation_angles(p: np.ndarray, prec: str = "f32") -> np.ndarray:
+    dt, s = _dt(prec)
+    q = _arr(p, dt)
+    r = np.zeros(3, dt)
+    getattr(orc_lib(), "orc_rotation_angles" + s)(_ptr(q), _ptr(r))
+    return r
+
+
+def warp_affine(src: np.ndarray, p12: np.ndarray, prec: str = "f32") -> np.ndarray:
+    dt, s = _dt(prec)
+    D, H, W = src.shape
+    v = _arr(src, dt)
+    p = _arr(p12, dt)
+    out = np.empty_like(v)
+    getattr(orc_lib(), "orc_warp_affine" + s)(_ptr(v), W, H, D, _ptr(p), _ptr(out))
+    return out
+
+
+def warp_field(src: np.ndarray, dx, dy, dz, prec: str = "f32") -> np.ndarray:
+    dt, s = _dt(prec)
+    D, H, W = src.shape
+    v = _arr(src, dt)
+    fx, fy, fz = (_arr(a, dt) for a in (dx, dy, dz))
+    out = np.empty_like(v)
+    getattr(orc_lib(), "orc_warp_field" + s)(_ptr(v), W, H, D, _ptr(fx), _ptr(fy), _ptr(fz), _ptr(out))
+    return out
+
+
+def align_linear(ref: np.ndarray, moving: np.ndarray, filters: np.ndarray, niter: int,
+                 type_: int = AFFINE, prec: str = "f32"):
+    """Single-scale linear registration of `moving` to `ref`.
+
+    Returns (params12, aligned volume, rotations in degrees or None)."""
+    dt, s = _dt(prec)
+    D, H, W = ref.shape
+    r = _arr(ref, dt)
+    orig = _arr(moving, dt).copy()
+    aligned = orig.copy()
+    f = _arr(filters, dt)
+    p = np.zeros(12, dt)
+    rot = np.zeros(3, dt)
+    getattr(orc_lib(), "orc_align_linear" + s)(_ptr(r), _ptr(aligned), _ptr(orig), W, H, D, _ptr(f),
+                                               niter, type_, _ptr(p), _ptr(rot))
+    return p, aligned, (rot if type_ == RIGID else None)
+
+
+def motion_correct(vols: np.ndarray, voxel_size, filters: np.ndarray, niter: int, prec: str = "f32"):
+    """Rigid motion correction of a (T,D,H,W) series to volume 0.
+
+    Returns (corrected series, motion parameters (6,T): mm then degrees)."""
+    dt, s = _dt(prec)
+    T, D, H, W = vols.shape
+    v = _arr(vols, dt).copy()
+    vs = _arr(voxel_size, dt)
+    f = _arr(filters, dt)
+    m = np.zeros(6 * T, dt)
+    getattr(orc_lib(), "orc_motion_correct" + s)(_ptr(v), W, H, D, T, _ptr(vs), _ptr(f), niter, _ptr(m))
+    return v, m.reshape(6, T)
+
+
+def smoothing_filter_sigma(sigma: float, size: int = 9, prec: str = "f32") -> np.ndarray:
+    dt, s = _dt(prec)
+    f = np.zeros(size, dt)
+    fn = getattr(orc_lib(), "orc_smoothing_filter_sigma" + s)
+    fn.argtypes = [_I, _D, _P]
+    fn(size, float(sigma), _ptr(f))
+    return f
+
+
+def smooth3d(vol: np.ndarray, fx, fy, fz, cert=None, smoothed_cert=None, prec: str = "f32"):
+    dt, s = _dt(prec)
+    D, H, W = vol.shape
+    v = _arr(vol, dt)
+    c = _arr(cert, dt) if cert is not None else None
+    sc = _arr(smoothed_cert, dt) if smoothed_cert is not None else None
+    fxa, fya, fza = (_arr(a, dt) for a in (fx, fy, fz))
+    out = np.empty_like(v)
+    getattr(orc_lib(), "orc_smooth3d" + s)(_ptr(v), _ptr(c) if c is not None else None,
+                                           _ptr(sc) if sc is not None else None, W, H, D,
+                                           _ptr(fxa), _ptr(fya), _ptr(fza), _ptr(out))
+    return out
+
+
+def rescale_linear(src: np.ndarray, shape, prec: str = "f32") -> np.ndarray:
+    dt, s = _dt(prec)
+    D, H, W = src.shape
+    D2, H2, W2 = shape
+    v = _arr(src, dt)
+    out = np.empty((D2, H2, W2), dt)
+    getattr(orc_lib(), "orc_rescale_linear" + s)(_ptr(v), W, H, D, W2, H2, D2, _ptr(out))
+    return out
+
+
+# --------------------------------------------------------------------------
+# the reference's own kernels (oracle/_ref/libbroccoli_ref.so), float only
+# --------------------------------------------------------------------------
+
+def ref_filter3d(vol: np.ndarray, filters: np.ndarray) -> np.ndarray:
+    D, H, W = vol.shape
+    v = _arr(vol, np.float32)
+    f = _arr(filters, np.float32)
+    assert f.shape[0] == 3
+    out = np.empty((3, D, H, W, 2), np.float32)
+    ref_lib().ref_filter3d(_ptr(v), W, H, D, _ptr(f), _ptr(out))
+    return out[..., 0] + 1j * out[..., 1]
+
+
+def ref_normal_equations(q1: np.ndarray, q2: np.ndarray):
+    _, D, H, W = q1.shape
+    a = _interleave(q1, np.float32)
+    c = _interleave(q2, np.float32)
+    A = np.zeros(144, np.float32)
+    h = np.zeros(12, np.float32)
+    ref_lib().ref_normal_equations(_ptr(a), _ptr(c), W, H, D, _ptr(A), _ptr(h))
+    return A.reshape(12, 12).T.copy(), h
+
+
+def ref_solve(A: np.ndarray, h: np.ndarray) -> np.ndarray:
+    n = h.shape[0]
+    Acm = _arr(np.asarray(A).T, np.float32)
+    hv = _arr(h, np.float32)
+    p = np.zeros(n, np.float32)
+    ref_lib().ref_solve(_ptr(Acm), _ptr(hv), n, _ptr(p))
+    return p
+
+
+def ref_remove_scaling(p: np.ndarray) -> np.ndarray:
+    q = _arr(p, np.float32).copy()
+    ref_lib().ref_remove_scaling(_ptr(q))
+    return q
+
+
+def ref_add_affine(old: np.ndarray, new: np.ndarray) -> np.ndarray:
+    o = _arr(old, np.float32).copy()
+    n = _arr(new, np.float32)
+    ref_lib().ref_add_affine(_ptr(o), _ptr(n))
+    return o
+
+
+def ref_rotation_angles(p: np.ndarray) -> np.ndarray:
+    q = _arr(p, np.float32)
+    r = np.zeros(3, np.float32)
+    ref_lib().ref_rotation_angles(_ptr(q), _ptr(r))
+    return r
+
+
+def ref_warp_affine(src: np.ndarray, p12: np.ndarray) -> np.ndarray:
+    D, H, W = src.shape
+    v = _arr(src, np.float32)
+    p = _arr(p12, np.float32)
+    out = np.empty_like(v)
+    ref_lib().ref_warp_affine(_ptr(v), W, H, D, _ptr(p), _ptr(out))
+    return out
+
+
+def ref_warp_field(src: np.ndarray, dx, dy, dz) -> np.ndarray:
+    D, H, W = src.shape
+    v = _arr(src, np.float32)
+    fx, fy, fz = (_arr(a, np.float32) for a in (dx, dy, dz))
+    out = np.empty_like(v)
+    ref_lib().ref_warp_field(_ptr(v), W, H, D, _ptr(fx), _ptr(fy), _ptr(fz), _ptr(out))
+    return out
+
+
+def ref_rescale_linear(src: np.ndarray, shape) -> np.ndarray:
+    D, H, W = src.shape
+    D2, H2, W2 = shape
+    v = _arr(src, np.float32)
+    out = np.empty((D2, H2, W2), np.float32)
+    ref_lib().ref_rescale_linear(_ptr(v), W, H, D, W2, H2, D2, _ptr(out))
+    return out
+
+
+def ref_align_linear(ref: np.ndarray, moving: np.ndarray, filters: np.ndarray, niter: int,
+                     type_: int = AFFINE):
+    D, H, W = ref.shape
+    r = _arr(ref, np.float32)
+    orig = _arr(moving, np.float32).copy()
+    aligned = orig.copy()
+    f = _arr(filters, np.float32)
+    p = np.zeros(12, np.float32)
+    rot = np.zeros(3, np.float32)
+    ref_lib().ref_align_linear(_ptr(r), _ptr(aligned), _ptr(orig), W, H, D, _ptr(f), niter, type_,
+                               _ptr(p), _ptr(rot))
+    return p, aligned, (rot if type_ == RIGID else None)
+
+
+def ref_motion_correct(vols: np.ndarray, voxel_size, filters: np.ndarray, niter: int):
+    T, D, H, W = vols.shape
+    v = _arr(vols, np.float32).copy()
+    vs = _arr(voxel_size, np.float32)
+    f = _arr(filters, np.float32)
+    m = np.zeros(6 * T, np.float32)
+    ref_lib().ref_motion_correct(_ptr(v), W, H, D, T, _ptr(vs), _ptr(f), niter, _ptr(m))
+    return v, m.reshape(6, T)
+
+
+def ref_smooth3d(vol: np.ndarray, fx, fy, fz, cert=None, smoothed_cert=None):
+    D, H, W = vol.shape
+    v = _arr(vol, np.float32)
+    c = _arr(cert, np.float32) if cert is not None else None
+    sc = _arr(smoothed_cert, np.float32) if smoothed_cert is not None else None
+    fxa, fya, fza = (_arr(a, np.float32) for a in (fx, fy, fz))
+    out = np.empty_like(v)
+    ref_lib().ref_smooth3d(_ptr(v), _ptr(c) if c is not None else None,
+                           _ptr(sc) if sc is not None else None, W, H, D,
+                           _ptr(fxa), _ptr(fya), _ptr(fza), _ptr(out))
+    return out

@@ -1,0 +1,686 @@
+/*
+ * orc_impl.h -- body of the CPU oracle, included twice by broccoli_oracle.c
+ * with REAL = float / SFX = _f32 and REAL = double / SFX = _f64.
+ *
+ * TEST INFRASTRUCTURE ONLY (see broccoli_oracle.h).  Each function restates
+ * one piece of the reference and cites the file:line it follows; paths are
+ * relative to the BROCCOLI source tree.  The float build keeps the
+ * reference's operation order (per-slice partial sums, per-row / per-column /
+ * per-slice reduction order) so that it is the FP32 parity target; the double
+ * build is the same algorithm in double precision.
+ */
+
+#define CAT_(a, b) a##b
+#define CAT(a, b) CAT_(a, b)
+#define FN(name) CAT(name, SFX)
+
+#if REAL_IS_FLOAT
+#define RSQRT(x) sqrtf(x)
+#define RATAN2(y, x) atan2f(y, x)
+#define RCOS(x) cosf(x)
+#define RFLOOR(x) floorf(x)
+#define RHALF 0.5f
+#define RONE 1.0f
+#define RZERO 0.0f
+#else
+#define RSQRT(x) sqrt(x)
+#define RATAN2(y, x) atan2(y, x)
+#define RCOS(x) cos(x)
+#define RFLOOR(x) floor(x)
+#define RHALF 0.5
+#define RONE 1.0
+#define RZERO 0.0
+#endif
+
+/* Non-separable 3D filtering with nfilt complex 7x7x7 filters.
+ * Follows BROCCOLI_LIB::NonseparableConvolution3D (code/BROCCOLI_LIB/
+ * broccoli_lib.cpp:4974-5027): responses are zeroed, then for z-offsets
+ * -3..+3 (filter slice zz = 6..0) a 2D 7x7 pass over the slice z+zoff is
+ * accumulated.  The 2D pass is kernelConvolution.cpp:2802-2867: the filter
+ * index runs 6..0 while the offset runs -3..+3 (a true convolution), with
+ * zero padding outside the volume.  `filters` holds nfilt x {re[343],
+ * im[343]}; `out` holds nfilt interleaved complex volumes. */
+void FN(orc_filter3d)(const REAL* vol, int W, int H, int D, const REAL* filters,
+                      int nfilt, REAL* out) {
+  const long V = (long)W * H * D;
+  for (int f = 0; f < nfilt; f++)
+    for (long i = 0; i < 2 * V; i++) out[(long)f * 2 * V + i] = RZERO;
+#pragma omp parallel for schedule(static)
+  for (int z = 0; z < D; z++) {
+    REAL s[2 * 6];
+    for (int y = 0; y < H; y++)
+      for (int x = 0; x < W; x++) {
+        const long idx = x + (long)y * W + (long)z * W * H;
+        for (int zz = 6; zz >= 0; zz--) {
+          const int zoff = 3 - zz;
+          const int zi = z + zoff;
+          for (int k = 0; k < 2 * nfilt; k++) s[k] = RZERO;
+          if (zi >= 0 && zi < D) {
+            for (int fy = 6; fy >= 0; fy--) {
+              const int yi = y + 3 - fy;
+              if (yi < 0 || yi >= H) continue;
+              for (int fx = 6; fx >= 0; fx--) {
+                const int xi = x + 3 - fx;
+                if (xi < 0 || xi >= W) continue;
+                const REAL pixel = vol[xi + (long)yi * W + (long)zi * W * H];
+                const int tap = fx + fy * 7 + zz * 49;
+                for (int f = 0; f < nfilt; f++) {
+                  s[2 * f] += filters[f * 686 + tap] * pixel;
+                  s[2 * f + 1] += filters[f * 686 + 343 + tap] * pixel;
+                }
+              }
+            }
+          }
+          for (int f = 0; f < nfilt; f++) {
+            out[(long)f * 2 * V + 2 * idx] += s[2 * f];
+            out[(long)f * 2 * V + 2 * idx + 1] += s[2 * f + 1];
+          }
+        }
+      }
+  }
+}
+
+/* Phase difference arg(q1 conj q2) and certainty |q1 q2| cos^2(dphi/2).
+ * kernelRegistration.cpp:173-211. */
+void FN(orc_phase_diff_cert)(const REAL* q1, const REAL* q2, long V, REAL* pd,
+                             REAL* cert) {
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < V; i++) {
+    const REAL ax = q1[2 * i], ay = q1[2 * i + 1];
+    const REAL cx = q2[2 * i], cy = q2[2 * i + 1];
+    REAL re = ax * cx + ay * cy;
+    REAL im = ay * cx - ax * cy;
+    const REAL d = RATAN2(im, re);
+    re = ax * cx - ay * cy;
+    im = ay * cx + ax * cy;
+    const REAL c = RCOS(d * RHALF);
+    pd[i] = d;
+    cert[i] = RSQRT(re * re + im * im) * c * c;
+  }
+}
+
+/* Phase gradient along `axis` (0=x,1=y,2=z): arg of the sum of the four
+ * neighbour products q[+1] conj q[0] + q[0] conj q[-1] of both responses.
+ * kernelRegistration.cpp:213-382.  The first and last sample along the axis
+ * are left unwritten, as in the reference. */
+void FN(orc_phase_grad)(const REAL* q1, const REAL* q2, int axis, int W, int H,
+                        int D, REAL* grad) {
+  const long step = axis == 0 ? 1 : (axis == 1 ? (long)W : (long)W * H);
+  const int n = axis == 0 ? W : (axis == 1 ? H : D);
+#pragma omp parallel for schedule(static)
+  for (int z = 0; z < D; z++)
+    for (int y = 0; y < H; y++)
+      for (int x = 0; x < W; x++) {
+        const int c = axis == 0 ? x : (axis == 1 ? y : z);
+        if (c - 1 < 0 || c + 1 >= n) continue;
+        const long i = x + (long)y * W + (long)z * W * H;
+        const long ip = i + step, im = i - step;
+        REAL tr = RZERO, ti = RZERO;
+        const REAL* qs[2] = {q1, q2};
+        for (int k = 0; k < 2; k++) {
+          const REAL* q = qs[k];
+          REAL ax = q[2 * ip], ay = q[2 * ip + 1];
+          REAL cx = q[2 * i], cy = q[2 * i + 1];
+          tr += ax * cx + ay * cy;
+          ti += ay * cx - ax * cy;
+          ax = cx;
+          ay = cy;
+          cx = q[2 * im];
+          cy = q[2 * im + 1];
+          tr += ax * cx + ay * cy;
+          ti += ay * cx - ax * cy;
+        }
+        grad[i] = RATAN2(ti, tr);
+      }
+}
+
+/* (row, column) of the 10 A-matrix entries filled by one axis, in the order
+ * of the monomials [1, x, y, z, xx, xy, xz, yy, yz, zz].  This is the table
+ * of GetParameterIndices (kernelRegistration.cpp:43-171): axis k owns the
+ * parameters {k, 3+3k, 4+3k, 5+3k}. */
+static void FN(orc_axis_entry)(int axis, int e, int* i, int* j) {
+  static const int mono_a[10] = {0, 1, 2, 3, 1, 2, 3, 2, 3, 3};
+  static const int mono_b[10] = {0, 0, 0, 0, 1, 1, 1, 2, 2, 3};
+  const int param[4] = {axis, 3 + 3 * axis, 4 + 3 * axis, 5 + 3 * axis};
+  *i = param[mono_a[e]];
+  *j = param[mono_b[e]];
+}
+
+/* Sums of c g^2 [1,x,y,z,xx,xy,xz,yy,yz,zz] and c g dphi [1,x,y,z] over the
+ * interior (border (filter_size-1)/2 in every axis), coordinates relative to
+ * the volume centre.  Order of summation as in the reference: along x per
+ * (y,z) row (kernelRegistration.cpp:387-485), then over y per z
+ * (:695-720, :750-776), then over z (:723-747, :780-800).  Writes the 10
+ * lower-triangle entries of A (column-major 12x12, A[i + 12 j]) and the 4
+ * entries of h that belong to this axis. */
+void FN(orc_ah_axis)(const REAL* pd, const REAL* grad, const REAL* cert,
+                     int axis, int W, int H, int D, int filter_size, REAL* A144,
+                     REAL* h12) {
+  const int b = (filter_size - 1) / 2;
+  REAL A[10], h[4];
+  for (int e = 0; e < 10; e++) A[e] = RZERO;
+  for (int e = 0; e < 4; e++) h[e] = RZERO;
+  for (int z = b; z < D - b; z++) {
+    REAL A1[10], h1[4];
+    for (int e = 0; e < 10; e++) A1[e] = RZERO;
+    for (int e = 0; e < 4; e++) h1[e] = RZERO;
+    for (int y = b; y < H - b; y++) {
+      const REAL yf = (REAL)y - ((REAL)H - RONE) * RHALF;
+      const REAL zf = (REAL)z - ((REAL)D - RONE) * RHALF;
+      REAL a[10], hv[4];
+      for (int e = 0; e < 10; e++) a[e] = RZERO;
+      for (int e = 0; e < 4; e++) hv[e] = RZERO;
+      for (int x = b; x < W - b; x++) {
+        const REAL xf = (REAL)x - ((REAL)W - RONE) * RHALF;
+        const long i = x + (long)y * W + (long)z * W * H;
+        const REAL d = pd[i], g = grad[i], c = cert[i];
+        const REAL cgg = c * g * g;
+        const REAL cgd = c * g * d;
+        a[0] += cgg;
+        a[1] += xf * cgg;
+        a[2] += yf * cgg;
+        a[3] += zf * cgg;
+        a[4] += xf * xf * cgg;
+        a[5] += xf * yf * cgg;
+        a[6] += xf * zf * cgg;
+        a[7] += yf * yf * cgg;
+        a[8] += yf * zf * cgg;
+        a[9] += zf * zf * cgg;
+        hv[0] += cgd;
+        hv[1] += xf * cgd;
+        hv[2] += yf * cgd;
+        hv[3] += zf * cgd;
+      }
+      for (int e = 0; e < 10; e++) A1[e] += a[e];
+      for (int e = 0; e < 4; e++) h1[e] += hv[e];
+    }
+    for (int e = 0; e < 10; e++) A[e] += A1[e];
+    for (int e = 0; e < 4; e++) h[e] += h1[e];
+  }
+  for (int e = 0; e < 10; e++) {
+    int i, j;
+    FN(orc_axis_entry)(axis, e, &i, &j);
+    A144[i + 12 * j] = A[e];
+  }
+  h12[axis] = h[0];
+  h12[3 + 3 * axis] = h[1];
+  h12[4 + 3 * axis] = h[2];
+  h12[5 + 3 * axis] = h[3];
+}
+
+/* The 12x12 normal equations of one affine iteration from the three pairs of
+ * responses (q1: reference, q2: aligned volume; each 3 interleaved complex
+ * volumes).  Follows the kernel sequence of AlignTwoVolumesLinear
+ * (broccoli_lib.cpp:5315-5381) and the mirroring of :5384-5392.  A is
+ * returned full and symmetric, column-major. */
+void FN(orc_normal_equations)(const REAL* q1, const REAL* q2, int W, int H,
+                              int D, REAL* A144, REAL* h12) {
+  const long V = (long)W * H * D;
+  REAL* pd = (REAL*)calloc(V, sizeof(REAL));
+  REAL* cert = (REAL*)calloc(V, sizeof(REAL));
+  REAL* grad = (REAL*)calloc(V, sizeof(REAL));
+  for (int e = 0; e < 144; e++) A144[e] = RZERO;
+  for (int e = 0; e < 12; e++) h12[e] = RZERO;
+  for (int axis = 0; axis < 3; axis++) {
+    const REAL* a = q1 + (long)axis * 2 * V;
+    const REAL* c = q2 + (long)axis * 2 * V;
+    FN(orc_phase_diff_cert)(a, c, V, pd, cert);
+    FN(orc_phase_grad)(a, c, axis, W, H, D, grad);
+    FN(orc_ah_axis)(pd, grad, cert, axis, W, H, D, 7, A144, h12);
+  }
+  for (int j = 0; j < 12; j++)
+    for (int i = 0; i < 12; i++) A144[j + i * 12] = A144[i + j * 12];
+  free(pd);
+  free(cert);
+  free(grad);
+}
+
+/* p = A^-1 h in double precision, A column-major n x n, result rounded to
+ * `real`.  The reference uses Eigen's full-pivoting Householder QR
+ * (SolveEquationSystem, broccoli_lib.cpp:17157-17186); this is Gaussian
+ * elimination with complete pivoting, which gives the same solution to
+ * double rounding.  Rank handling follows the same rule: pivots below
+ * eps * n * |largest pivot| are treated as zero and the matching unknowns are
+ * set to 0 (a zero matrix gives p = 0). */
+void FN(orc_solve)(const REAL* Ain, const REAL* hin, int n, REAL* p) {
+  double A[144], h[12], x[12];
+  int colperm[12];
+  for (int i = 0; i < n; i++) {
+    h[i] = (double)hin[i];
+    colperm[i] = i;
+    for (int j = 0; j < n; j++) A[i * n + j] = (double)Ain[i + j * n];
+  }
+  double maxpiv = 0.0;
+  int rank = 0;
+  for (int k = 0; k < n; k++) {
+    int pr = k, pc = k;
+    double best = -1.0;
+    for (int i = k; i < n; i++)
+      for (int j = k; j < n; j++)
+        if (fabs(A[i * n + j]) > best) {
+          best = fabs(A[i * n + j]);
+          pr = i;
+          pc = j;
+        }
+    if (k == 0) maxpiv = best;
+    if (best <= maxpiv * 2.220446049250313e-16 * n || best == 0.0) break;
+    rank++;
+    if (pr != k) {
+      for (int j = 0; j < n; j++) {
+        double t = A[k * n + j];
+        A[k * n + j] = A[pr * n + j];
+        A[pr * n + j] = t;
+      }
+      double t = h[k];
+      h[k] = h[pr];
+      h[pr] = t;
+    }
+    if (pc != k) {
+      for (int i = 0; i < n; i++) {
+        double t = A[i * n + k];
+        A[i * n + k] = A[i * n + pc];
+        A[i * n + pc] = t;
+      }
+      int t = colperm[k];
+      colperm[k] = colperm[pc];
+      colperm[pc] = t;
+    }
+    for (int i = k + 1; i < n; i++) {
+      const double m = A[i * n + k] / A[k * n + k];
+      if (m == 0.0) continue;
+      for (int j = k; j < n; j++) A[i * n + j] -= m * A[k * n + j];
+      h[i] -= m * h[k];
+    }
+  }
+  double y[12];
+  for (int i = 0; i < n; i++) y[i] = 0.0;
+  for (int i = rank - 1; i >= 0; i--) {
+    double s = h[i];
+    for (int j = i + 1; j < rank; j++) s -= A[i * n + j] * y[j];
+    y[i] = s / A[i * n + i];
+  }
+  for (int i = 0; i < n; i++) x[colperm[i]] = y[i];
+  for (int i = 0; i < n; i++) p[i] = (REAL)x[i];
+}
+
+/* Polar factor U V^T of a 3x3 matrix from its SVD, by one-sided (Hestenes)
+ * Jacobi sweeps in double.  M is row-major. */
+static void FN(orc_polar3)(const double* M, double* R) {
+  double A[9], Vm[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  for (int i = 0; i < 9; i++) A[i] = M[i];
+  for (int sweep = 0; sweep < 60; sweep++) {
+    int rotated = 0;
+    for (int p = 0; p < 2; p++)
+      for (int q = p + 1; q < 3; q++) {
+        double al = 0, be = 0, ga = 0;
+        for (int i = 0; i < 3; i++) {
+          al += A[i * 3 + p] * A[i * 3 + p];
+          be += A[i * 3 + q] * A[i * 3 + q];
+          ga += A[i * 3 + p] * A[i * 3 + q];
+        }
+        if (fabs(ga) <= 1e-300 || fabs(ga) <= 2.220446049250313e-16 * sqrt(al * be))
+          continue;
+        rotated = 1;
+        const double zeta = (be - al) / (2.0 * ga);
+        const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
+        for (int i = 0; i < 3; i++) {
+          const double ap = A[i * 3 + p], aq = A[i * 3 + q];
+          A[i * 3 + p] = c * ap - s * aq;
+          A[i * 3 + q] = s * ap + c * aq;
+          const double vp = Vm[i * 3 + p], vq = Vm[i * 3 + q];
+          Vm[i * 3 + p] = c * vp - s * vq;
+          Vm[i * 3 + q] = s * vp + c * vq;
+        }
+      }
+    if (!rotated) break;
+  }
+  /* U = A Sigma^-1 column by column; a zero singular value gets the
+   * orthonormal completion. */
+  double U[9];
+  double sig[3];
+  for (int j = 0; j < 3; j++) {
+    sig[j] = sqrt(A[j] * A[j] + A[3 + j] * A[3 + j] + A[6 + j] * A[6 + j]);
+    for (int i = 0; i < 3; i++) U[i * 3 + j] = sig[j] > 0 ? A[i * 3 + j] / sig[j] : 0.0;
+  }
+  for (int j = 0; j < 3; j++)
+    if (!(sig[j] > 0)) {
+      const int a = (j + 1) % 3, b = (j + 2) % 3;
+      U[0 * 3 + j] = U[1 * 3 + a] * U[2 * 3 + b] - U[2 * 3 + a] * U[1 * 3 + b];
+      U[1 * 3 + j] = U[2 * 3 + a] * U[0 * 3 + b] - U[0 * 3 + a] * U[2 * 3 + b];
+      U[2 * 3 + j] = U[0 * 3 + a] * U[1 * 3 + b] - U[1 * 3 + a] * U[0 * 3 + b];
+    }
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      double s = 0;
+      for (int k = 0; k < 3; k++) s += U[i * 3 + k] * Vm[j * 3 + k];
+      R[i * 3 + j] = s;
+    }
+}
+
+/* RIGID projection: replace I+P by the orthogonal factor U V^T of its SVD.
+ * RemoveTransformationScaling, broccoli_lib.cpp:6153-6194. */
+void FN(orc_remove_scaling)(REAL* p) {
+  double M[9], R[9];
+  for (int i = 0; i < 9; i++) M[i] = (double)p[3 + i];
+  M[0] += 1.0;
+  M[4] += 1.0;
+  M[8] += 1.0;
+  FN(orc_polar3)(M, R);
+  R[0] -= 1.0;
+  R[4] -= 1.0;
+  R[8] -= 1.0;
+  for (int i = 0; i < 9; i++) p[3 + i] = (REAL)R[i];
+}
+
+/* 4x4 homogeneous matrix of a parameter vector; the diagonal one is added
+ * in `real` before widening, as the reference does ((double)(p + 1.0f)). */
+static void FN(orc_to_mat4)(const REAL* p, double tscale, double* Mt) {
+  Mt[0] = (double)(p[3] + RONE); Mt[1] = (double)p[4]; Mt[2] = (double)p[5];
+  Mt[3] = (double)(tscale == 1.0 ? p[0] : p[0] * (REAL)tscale);
+  Mt[4] = (double)p[6]; Mt[5] = (double)(p[7] + RONE); Mt[6] = (double)p[8];
+  Mt[7] = (double)(tscale == 1.0 ? p[1] : p[1] * (REAL)tscale);
+  Mt[8] = (double)p[9]; Mt[9] = (double)p[10]; Mt[10] = (double)(p[11] + RONE);
+  Mt[11] = (double)(tscale == 1.0 ? p[2] : p[2] * (REAL)tscale);
+  Mt[12] = 0; Mt[13] = 0; Mt[14] = 0; Mt[15] = 1;
+}
+
+static void FN(orc_compose)(REAL* old12, const REAL* new12, double tscale) {
+  double O[16], N[16], T[16];
+  FN(orc_to_mat4)(old12, tscale, O);
+  FN(orc_to_mat4)(new12, tscale, N);
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) {
+      double s = 0;
+      for (int k = 0; k < 4; k++) s += N[i * 4 + k] * O[k * 4 + j];
+      T[i * 4 + j] = s;
+    }
+  old12[0] = (REAL)T[3];
+  old12[1] = (REAL)T[7];
+  old12[2] = (REAL)T[11];
+  old12[3] = (REAL)(T[0] - 1.0); old12[4] = (REAL)T[1]; old12[5] = (REAL)T[2];
+  old12[6] = (REAL)T[4]; old12[7] = (REAL)(T[5] - 1.0); old12[8] = (REAL)T[6];
+  old12[9] = (REAL)T[8]; old12[10] = (REAL)T[9]; old12[11] = (REAL)(T[10] - 1.0);
+}
+
+/* Total = New * Old.  AddAffineRegistrationParameters,
+ * broccoli_lib.cpp:7252-7340. */
+void FN(orc_add_affine)(REAL* old12, const REAL* new12) {
+  FN(orc_compose)(old12, new12, 1.0);
+}
+
+/* Same with both translations doubled (next pyramid scale).
+ * AddAffineRegistrationParametersNextScale, broccoli_lib.cpp:7344-7431. */
+void FN(orc_add_affine_next_scale)(REAL* old12, const REAL* new12) {
+  FN(orc_compose)(old12, new12, 2.0);
+}
+
+/* Euler angles in degrees.  CalculateRotationAnglesFromRotationMatrix,
+ * broccoli_lib.cpp:6199-6244. */
+void FN(orc_rotation_angles)(const REAL* p, REAL* rot) {
+  const double PI_ = 3.14159265358979323846;
+  double m[9];
+  for (int i = 0; i < 9; i++) m[i] = (double)p[3 + i];
+  m[0] += 1.0;
+  m[4] += 1.0;
+  m[8] += 1.0;
+  const double a1 = -atan2(m[5], m[8]) * 180.0 / PI_;
+  const double c2 = sqrt(m[0] * m[0] + m[1] * m[1]);
+  const double a2 = -atan2(-m[2], c2) * 180.0 / PI_;
+  const double s1 = sin(a1 * PI_ / 180.0), c1 = cos(a1 * PI_ / 180.0);
+  const double a3 = -atan2(s1 * m[6] - c1 * m[3], c1 * m[4] - s1 * m[7]) * 180.0 / PI_;
+  rot[0] = (REAL)a1;
+  rot[1] = (REAL)a2;
+  rot[2] = (REAL)a3;
+}
+
+/* OpenCL 1.2 (section 8.2) linear filtering of a float image with
+ * CLK_ADDRESS_CLAMP_TO_EDGE and unnormalised coordinates, exact weights:
+ * i0 = floor(u - 0.5), a = frac(u - 0.5), indices clamped to the edge. */
+static REAL FN(orc_sample_linear)(const REAL* T, int W, int H, int D, REAL u,
+                                  REAL v, REAL w) {
+  const REAL uu = u - RHALF, vv = v - RHALF, ww = w - RHALF;
+  const REAL fu = RFLOOR(uu), fv = RFLOOR(vv), fw = RFLOOR(ww);
+  const REAL a = uu - fu, b = vv - fv, c = ww - fw;
+  int i0 = (int)fu, j0 = (int)fv, k0 = (int)fw;
+  int i1 = i0 + 1, j1 = j0 + 1, k1 = k0 + 1;
+#define CLAMPI(q, n) q = q < 0 ? 0 : (q > n - 1 ? n - 1 : q)
+  CLAMPI(i0, W); CLAMPI(i1, W); CLAMPI(j0, H); CLAMPI(j1, H); CLAMPI(k0, D); CLAMPI(k1, D);
+#undef CLAMPI
+#define TV(i, j, k) T[(i) + (long)(j) * W + (long)(k) * W * H]
+  return (RONE - a) * (RONE - b) * (RONE - c) * TV(i0, j0, k0) +
+         a * (RONE - b) * (RONE - c) * TV(i1, j0, k0) +
+         (RONE - a) * b * (RONE - c) * TV(i0, j1, k0) +
+         a * b * (RONE - c) * TV(i1, j1, k0) +
+         (RONE - a) * (RONE - b) * c * TV(i0, j0, k1) +
+         a * (RONE - b) * c * TV(i1, j0, k1) +
+         (RONE - a) * b * c * TV(i0, j1, k1) + a * b * c * TV(i1, j1, k1);
+#undef TV
+}
+
+/* Affine warp: out(x) = linear sample of src at
+ * x + t + (A - I)(x - c), c the volume centre.
+ * InterpolateVolumeLinearLinear, kernelRegistration.cpp:1066-1101. */
+void FN(orc_warp_affine)(const REAL* src, int W, int H, int D, const REAL* p,
+                         REAL* out) {
+#pragma omp parallel for schedule(static)
+  for (int z = 0; z < D; z++)
+    for (int y = 0; y < H; y++)
+      for (int x = 0; x < W; x++) {
+        const REAL xf = (REAL)x - ((REAL)W - RONE) * RHALF;
+        const REAL yf = (REAL)y - ((REAL)H - RONE) * RHALF;
+        const REAL zf = (REAL)z - ((REAL)D - RONE) * RHALF;
+        const REAL u = (REAL)x + p[0] + p[3] * xf + p[4] * yf + p[5] * zf + RHALF;
+        const REAL v = (REAL)y + p[1] + p[6] * xf + p[7] * yf + p[8] * zf + RHALF;
+        const REAL w = (REAL)z + p[2] + p[9] * xf + p[10] * yf + p[11] * zf + RHALF;
+        out[x + (long)y * W + (long)z * W * H] = FN(orc_sample_linear)(src, W, H, D, u, v, w);
+      }
+}
+
+/* Displacement-field warp.  InterpolateVolumeLinearNonLinear,
+ * kernelRegistration.cpp:1111-1140. */
+void FN(orc_warp_field)(const REAL* src, int W, int H, int D, const REAL* dx,
+                        const REAL* dy, const REAL* dz, REAL* out) {
+#pragma omp parallel for schedule(static)
+  for (int z = 0; z < D; z++)
+    for (int y = 0; y < H; y++)
+      for (int x = 0; x < W; x++) {
+        const long i = x + (long)y * W + (long)z * W * H;
+        const REAL u = (REAL)x + dx[i] + RHALF;
+        const REAL v = (REAL)y + dy[i] + RHALF;
+        const REAL w = (REAL)z + dz[i] + RHALF;
+        out[i] = FN(orc_sample_linear)(src, W, H, D, u, v, w);
+      }
+}
+
+/* Linear registration of `aligned` (warped from `original`) to `ref` over a
+ * fixed number of iterations.  AlignTwoVolumesLinear,
+ * broccoli_lib.cpp:5273-5437: the reference is filtered once per call, each
+ * iteration filters the current aligned volume, builds and solves the
+ * normal equations, applies the TRANSLATION / RIGID / AFFINE update
+ * (:5398-5421) and re-warps the original with the total parameters.  On
+ * return `aligned` holds the last warp, p12 the total parameters and rot3
+ * (RIGID only) the Euler angles in degrees. */
+void FN(orc_align_linear)(const REAL* ref, REAL* aligned, const REAL* original,
+                          int W, int H, int D, const REAL* filters, int niter,
+                          int type, REAL* p12, REAL* rot3) {
+  const long V = (long)W * H * D;
+  REAL* q1 = (REAL*)malloc(sizeof(REAL) * 6 * V);
+  REAL* q2 = (REAL*)malloc(sizeof(REAL) * 6 * V);
+  REAL A[144], h[12], p[12];
+  FN(orc_filter3d)(ref, W, H, D, filters, 3, q1);
+  for (int i = 0; i < 12; i++) p12[i] = RZERO;
+  for (int it = 0; it < niter; it++) {
+    FN(orc_filter3d)(aligned, W, H, D, filters, 3, q2);
+    FN(orc_normal_equations)(q1, q2, W, H, D, A, h);
+    FN(orc_solve)(A, h, 12, p);
+    if (type == ORC_TRANSLATION) {
+      p12[0] += p[0];
+      p12[1] += p[1];
+      p12[2] += p[2];
+      for (int i = 3; i < 12; i++) p12[i] = RZERO;
+    } else if (type == ORC_RIGID) {
+      FN(orc_remove_scaling)(p);
+      FN(orc_add_affine)(p12, p);
+    } else {
+      FN(orc_add_affine)(p12, p);
+    }
+    FN(orc_warp_affine)(original, W, H, D, p12, aligned);
+  }
+  if (type == ORC_RIGID && rot3) FN(orc_rotation_angles)(p12, rot3);
+  free(q1);
+  free(q2);
+}
+
+/* Rigid motion correction of a series to its first volume.
+ * PerformMotionCorrectionWrapper, broccoli_lib.cpp:10658-10720: volume 0 is
+ * the reference and keeps zero motion; every later volume is registered
+ * (RIGID, niter iterations), replaced in place by its corrected copy, and
+ * its motion is written as motion6T[t + k*T] for k = translations x,y,z in
+ * mm (voxels times voxel size) then rotations in degrees. */
+void FN(orc_motion_correct)(REAL* vols, int W, int H, int D, int T,
+                            const REAL* voxel_size, const REAL* filters,
+                            int niter, REAL* motion6T) {
+  const long V = (long)W * H * D;
+  REAL* ref = (REAL*)malloc(sizeof(REAL) * V);
+  REAL* orig = (REAL*)malloc(sizeof(REAL) * V);
+  for (long i = 0; i < V; i++) ref[i] = vols[i];
+  for (int k = 0; k < 6; k++) motion6T[k * T] = RZERO;
+  for (int t = 1; t < T; t++) {
+    REAL p[12], rot[3];
+    REAL* vt = vols + (long)t * V;
+    for (long i = 0; i < V; i++) orig[i] = vt[i];
+    FN(orc_align_linear)(ref, vt, orig, W, H, D, filters, niter, ORC_RIGID, p, rot);
+    motion6T[t + 0 * T] = p[0] * voxel_size[0];
+    motion6T[t + 1 * T] = p[1] * voxel_size[1];
+    motion6T[t + 2 * T] = p[2] * voxel_size[2];
+    motion6T[t + 3 * T] = rot[0];
+    motion6T[t + 4 * T] = rot[1];
+    motion6T[t + 5 * T] = rot[2];
+  }
+  free(ref);
+  free(orig);
+}
+
+/* Gaussian smoothing filter of `size` taps for a given sigma (voxels),
+ * normalised by its float sum.  CreateSmoothingFilters(..., double sigma),
+ * broccoli_lib.cpp:11093-11121. */
+void FN(orc_smoothing_filter_sigma)(int size, double sigma, REAL* f) {
+  const int half = (size - 1) / 2;
+  const double s2 = 2.0 * sigma * sigma;
+  REAL sum = RZERO;
+  for (int i = 0; i < size; i++) {
+    const double u = (double)(i - half);
+    f[i] = (REAL)exp(-pow(u, 2.0) / s2);
+    sum += f[i];
+  }
+  for (int i = 0; i < size; i++) f[i] /= sum;
+}
+
+/* Per-axis Gaussian filters from a FWHM in mm and the voxel sizes.
+ * CreateSmoothingFilters(..., FWHM, voxel sizes), broccoli_lib.cpp:11055-11091. */
+void FN(orc_smoothing_filter_fwhm)(int size, double fwhm, double vx, double vy,
+                                   double vz, REAL* fx, REAL* fy, REAL* fz) {
+  const int half = (size - 1) / 2;
+  const double sx = fwhm / 2.354 / vx, sy = fwhm / 2.354 / vy, sz = fwhm / 2.354 / vz;
+  const double sx2 = 2.0 * sx * sx, sy2 = 2.0 * sy * sy, sz2 = 2.0 * sz * sz;
+  REAL ax = RZERO, ay = RZERO, az = RZERO;
+  for (int i = 0; i < size; i++) {
+    const double u = (double)(i - half);
+    fx[i] = (REAL)exp(-pow(u, 2.0) / sx2);
+    fy[i] = (REAL)exp(-pow(u, 2.0) / sy2);
+    fz[i] = (REAL)exp(-pow(u, 2.0) / sz2);
+    ax += fx[i];
+    ay += fy[i];
+    az += fz[i];
+  }
+  for (int i = 0; i < size; i++) {
+    fx[i] /= ax;
+    fy[i] /= ay;
+    fz[i] /= az;
+  }
+}
+
+/* Separable 9-tap normalised convolution: along y of vol*cert (Rows,
+ * kernelConvolution.cpp:52-91), along x (Columns, :531-569), along z divided
+ * by the smoothed certainty (Rods, :1201-1240).  Zero padding; the filter
+ * index runs 8..0 as the offset runs -4..+4.  cert / smoothed_cert may be
+ * NULL for all-ones (the in-place smoothing of PerformSmoothing,
+ * broccoli_lib.cpp:11274-11357 and :11461-11545). */
+void FN(orc_smooth3d)(const REAL* vol, const REAL* cert, const REAL* scert,
+                      int W, int H, int D, const REAL* fx, const REAL* fy,
+                      const REAL* fz, REAL* out) {
+  const long V = (long)W * H * D;
+  REAL* rows = (REAL*)malloc(sizeof(REAL) * V);
+  REAL* cols = (REAL*)malloc(sizeof(REAL) * V);
+#pragma omp parallel for schedule(static)
+  for (int z = 0; z < D; z++)
+    for (int y = 0; y < H; y++)
+      for (int x = 0; x < W; x++) {
+        REAL s = RZERO;
+        int off = -4;
+        for (int f = 8; f >= 0; f--, off++) {
+          REAL px = RZERO;
+          if (y + off >= 0 && y + off < H) {
+            const long j = x + (long)(y + off) * W + (long)z * W * H;
+            px = cert ? vol[j] * cert[j] : vol[j] * RONE;
+          }
+          s += px * fy[f];
+        }
+        rows[x + (long)y * W + (long)z * W * H] = s;
+      }
+#pragma omp parallel for schedule(static)
+  for (int z = 0; z < D; z++)
+    for (int y = 0; y < H; y++)
+      for (int x = 0; x < W; x++) {
+        REAL s = RZERO;
+        int off = -4;
+        for (int f = 8; f >= 0; f--, off++) {
+          REAL px = RZERO;
+          if (x + off >= 0 && x + off < W) px = rows[x + off + (long)y * W + (long)z * W * H];
+          s += px * fx[f];
+        }
+        cols[x + (long)y * W + (long)z * W * H] = s;
+      }
+#pragma omp parallel for schedule(static)
+  for (int z = 0; z < D; z++)
+    for (int y = 0; y < H; y++)
+      for (int x = 0; x < W; x++) {
+        REAL s = RZERO;
+        int off = -4;
+        for (int f = 8; f >= 0; f--, off++) {
+          REAL px = RZERO;
+          if (z + off >= 0 && z + off < D) px = cols[x + (long)y * W + (long)(z + off) * W * H];
+          s += px * fz[f];
+        }
+        const long i = x + (long)y * W + (long)z * W * H;
+        out[i] = s / (scert ? scert[i] : RONE);
+      }
+  free(rows);
+  free(cols);
+}
+
+/* Resample to a new grid size by linear interpolation with sample spacing
+ * (N-1)/(N'-1) per axis.  RescaleVolumeLinear, kernelRegistration.cpp:
+ * 1340-1366, driven by ChangeVolumeSize, broccoli_lib.cpp:6247-6388. */
+void FN(orc_rescale_linear)(const REAL* src, int W, int H, int D, int W2,
+                            int H2, int D2, REAL* out) {
+  const REAL dx = (REAL)(W - 1) / (REAL)(W2 - 1);
+  const REAL dy = (REAL)(H - 1) / (REAL)(H2 - 1);
+  const REAL dz = (REAL)(D - 1) / (REAL)(D2 - 1);
+#pragma omp parallel for schedule(static)
+  for (int z = 0; z < D2; z++)
+    for (int y = 0; y < H2; y++)
+      for (int x = 0; x < W2; x++)
+        out[x + (long)y * W2 + (long)z * W2 * H2] = FN(orc_sample_linear)(
+            src, W, H, D, (REAL)x * dx + RHALF, (REAL)y * dy + RHALF, (REAL)z * dz + RHALF);
+}
+
+#undef RSQRT
+#undef RATAN2
+#undef RCOS
+#undef RFLOOR
+#undef RHALF
+#undef RONE
+#undef RZERO
+#undef FN

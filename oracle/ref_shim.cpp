@@ -1,0 +1,287 @@
+// ref_shim.cpp -- runs the reference's own OpenCL C kernels on the CPU.
+// TEST INFRASTRUCTURE ONLY.  Built by `make ref` into oracle/_ref/ from the
+// kernel sources where they lie in the BROCCOLI tree (the Makefile turns the
+// OpenCL vector literals `(float2)(a,b)` into make_float2(a,b) in _ref/; the
+// sources are never copied into this repository).  The host loops below
+// restate BROCCOLI_LIB's drivers (code/BROCCOLI_LIB/broccoli_lib.cpp, cited
+// per function) and call the vendored Eigen exactly where the reference does.
+// Its outputs cross-check the C restatement in orc_impl.h and seed the golden
+// fixtures under tests/golden/.
+#include <Eigen/Dense>
+#include <cstring>
+#include <vector>
+
+#include "clshim.hpp"
+
+namespace clk {
+#include "kernelConvolution_cl.cpp"
+}
+namespace clr {
+#include "kernelRegistration_cl.cpp"
+}
+
+namespace {
+
+// Runs `body` once per work-item of an NDRange (global g, local l); groups
+// along the slowest non-trivial dimension are spread over OpenMP threads.
+template <class F>
+void ndrange(int g0, int g1, int g2, int l0, int l1, int l2, F body, bool parallel = true) {
+  const int n2 = g2 / l2;
+#pragma omp parallel for schedule(static) if (parallel)
+  for (int b2 = 0; b2 < n2; b2++)
+    for (int b1 = 0; b1 < g1 / l1; b1++)
+      for (int b0 = 0; b0 < g0 / l0; b0++)
+        for (int i2 = 0; i2 < l2; i2++)
+          for (int i1 = 0; i1 < l1; i1++)
+            for (int i0 = 0; i0 < l0; i0++) {
+              g_ndr.lid[0] = i0; g_ndr.lid[1] = i1; g_ndr.lid[2] = i2;
+              g_ndr.grp[0] = b0; g_ndr.grp[1] = b1; g_ndr.grp[2] = b2;
+              g_ndr.gid[0] = b0 * l0 + i0; g_ndr.gid[1] = b1 * l1 + i1; g_ndr.gid[2] = b2 * l2 + i2;
+              g_ndr.lsz[0] = l0; g_ndr.lsz[1] = l1; g_ndr.lsz[2] = l2;
+              body();
+            }
+}
+
+int roundup(int n, int m) { return (n + m - 1) / m * m; }
+
+const int NPARAM = 12;
+const int NNZ = 30;
+
+}  // namespace
+
+extern "C" {
+
+// NonseparableConvolution3D, broccoli_lib.cpp:4974-5027, with the
+// GlobalMemory kernel (kernelConvolution.cpp:2802-2867).  filters: 3 x
+// {re[343], im[343]}; out: 3 interleaved complex volumes.
+void ref_filter3d(const float* vol, int W, int H, int D, const float* filters, float* out) {
+  const long V = (long)W * H * D;
+  std::memset(out, 0, sizeof(float) * 6 * V);
+  float2* q1 = reinterpret_cast<float2*>(out);
+  float2* q2 = q1 + V;
+  float2* q3 = q2 + V;
+  int z_offset = -3;
+  for (int zz = 6; zz >= 0; zz--) {
+    const float* f1r = filters + 0 * 686 + zz * 49;
+    const float* f1i = filters + 0 * 686 + 343 + zz * 49;
+    const float* f2r = filters + 1 * 686 + zz * 49;
+    const float* f2i = filters + 1 * 686 + 343 + zz * 49;
+    const float* f3r = filters + 2 * 686 + zz * 49;
+    const float* f3i = filters + 2 * 686 + 343 + zz * 49;
+    ndrange(roundup(W, 16), roundup(H, 16), D, 16, 16, 1, [&] {
+      clk::Nonseparable3DConvolutionComplexThreeQuadratureFiltersGlobalMemory(
+          q1, q2, q3, vol, f1r, f1i, f2r, f2i, f3r, f3i, z_offset, W, H, D);
+    });
+    z_offset++;
+  }
+}
+
+// The normal-equation part of one AlignTwoVolumesLinear iteration,
+// broccoli_lib.cpp:5315-5392: phase differences / certainties / gradients
+// and the 2D -> 1D -> final reductions per axis, then the mirroring.
+void ref_normal_equations(const float* q1, const float* q2, int W, int H, int D, float* A144,
+                          float* h12) {
+  const long V = (long)W * H * D;
+  std::vector<float> pd(V, 0.f), cert(V, 0.f), grad(V, 0.f);
+  std::vector<float> A2((long)H * D * NNZ, 0.f), h2((long)H * D * NPARAM, 0.f);
+  std::vector<float> A1((long)D * NNZ, 0.f), h1((long)D * NPARAM, 0.f);
+  const float2* Q1 = reinterpret_cast<const float2*>(q1);
+  const float2* Q2 = reinterpret_cast<const float2*>(q2);
+  const int gx = roundup(W, 16), gy = roundup(H, 16);
+  for (int axis = 0; axis < 3; axis++) {
+    const float2* a = Q1 + axis * V;
+    const float2* c = Q2 + axis * V;
+    ndrange(gx, gy, D, 16, 16, 1, [&] {
+      clr::CalculatePhaseDifferencesAndCertainties(pd.data(), cert.data(), a, c, W, H, D);
+    });
+    ndrange(gx, gy, D, 16, 16, 1, [&] {
+      if (axis == 0) clr::CalculatePhaseGradientsX(grad.data(), a, c, W, H, D);
+      if (axis == 1) clr::CalculatePhaseGradientsY(grad.data(), a, c, W, H, D);
+      if (axis == 2) clr::CalculatePhaseGradientsZ(grad.data(), a, c, W, H, D);
+    });
+    ndrange(H, D, 1, H, 1, 1, [&] {
+      if (axis == 0)
+        clr::CalculateAMatrixAndHVector2DValuesX(A2.data(), h2.data(), pd.data(), grad.data(), cert.data(), W, H, D, 7);
+      if (axis == 1)
+        clr::CalculateAMatrixAndHVector2DValuesY(A2.data(), h2.data(), pd.data(), grad.data(), cert.data(), W, H, D, 7);
+      if (axis == 2)
+        clr::CalculateAMatrixAndHVector2DValuesZ(A2.data(), h2.data(), pd.data(), grad.data(), cert.data(), W, H, D, 7);
+    }, false);
+  }
+  ndrange(D, NNZ, 1, D, 1, 1, [&] { clr::CalculateAMatrix1DValues(A1.data(), A2.data(), W, H, D, 7); }, false);
+  ndrange(D, NPARAM, 1, D, 1, 1, [&] { clr::CalculateHVector1DValues(h1.data(), h2.data(), W, H, D, 7); }, false);
+  std::memset(A144, 0, sizeof(float) * 144);
+  ndrange(NNZ, 1, 1, NNZ, 1, 1, [&] { clr::CalculateAMatrix(A144, A1.data(), W, H, D, 7); }, false);
+  ndrange(NPARAM, 1, 1, NPARAM, 1, 1, [&] { clr::CalculateHVector(h12, h1.data(), W, H, D, 7); }, false);
+  for (int j = 0; j < NPARAM; j++)
+    for (int i = 0; i < NPARAM; i++) A144[j + i * NPARAM] = A144[i + j * NPARAM];
+}
+
+// SolveEquationSystem, broccoli_lib.cpp:17157-17186.
+void ref_solve(const float* A, const float* h, int N, float* p) {
+  Eigen::MatrixXd Am(N, N);
+  Eigen::VectorXd hv(N);
+  for (int i = 0; i < N; i++) {
+    hv(i) = (double)h[i];
+    for (int j = 0; j < N; j++) Am(i, j) = (double)A[i + j * N];
+  }
+  Eigen::VectorXd x = Am.fullPivHouseholderQr().solve(hv);
+  for (int i = 0; i < N; i++) p[i] = (float)x(i);
+}
+
+// RemoveTransformationScaling, broccoli_lib.cpp:6153-6194.
+void ref_remove_scaling(float* p) {
+  Eigen::MatrixXd T(3, 3);
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++) T(r, c) = (double)p[3 + r * 3 + c];
+  for (int d = 0; d < 3; d++) T(d, d) += 1.0;
+  Eigen::JacobiSVD<Eigen::MatrixXd> svd(T, Eigen::ComputeThinU | Eigen::ComputeThinV);
+  Eigen::MatrixXd R = svd.matrixU() * svd.matrixV().transpose();
+  for (int d = 0; d < 3; d++) R(d, d) -= 1.0;
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++) p[3 + r * 3 + c] = (float)R(r, c);
+}
+
+static Eigen::MatrixXd to_affine(const float* p, float tscale) {
+  Eigen::MatrixXd M(4, 4);
+  M(0, 0) = (double)(p[3] + 1.0f); M(0, 1) = (double)p[4]; M(0, 2) = (double)p[5];
+  M(1, 0) = (double)p[6]; M(1, 1) = (double)(p[7] + 1.0f); M(1, 2) = (double)p[8];
+  M(2, 0) = (double)p[9]; M(2, 1) = (double)p[10]; M(2, 2) = (double)(p[11] + 1.0f);
+  if (tscale == 1.0f) {
+    M(0, 3) = (double)p[0]; M(1, 3) = (double)p[1]; M(2, 3) = (double)p[2];
+  } else {
+    M(0, 3) = (double)(p[0] * tscale); M(1, 3) = (double)(p[1] * tscale); M(2, 3) = (double)(p[2] * tscale);
+  }
+  M(3, 0) = 0.0; M(3, 1) = 0.0; M(3, 2) = 0.0; M(3, 3) = 1.0;
+  return M;
+}
+
+static void from_affine(const Eigen::MatrixXd& T, float* p) {
+  p[0] = (float)T(0, 3); p[1] = (float)T(1, 3); p[2] = (float)T(2, 3);
+  p[3] = (float)(T(0, 0) - 1.0); p[4] = (float)T(0, 1); p[5] = (float)T(0, 2);
+  p[6] = (float)T(1, 0); p[7] = (float)(T(1, 1) - 1.0); p[8] = (float)T(1, 2);
+  p[9] = (float)T(2, 0); p[10] = (float)T(2, 1); p[11] = (float)(T(2, 2) - 1.0);
+}
+
+// AddAffineRegistrationParameters, broccoli_lib.cpp:7252-7340.
+void ref_add_affine(float* old12, const float* new12) {
+  Eigen::MatrixXd T = to_affine(new12, 1.0f) * to_affine(old12, 1.0f);
+  from_affine(T, old12);
+}
+
+// AddAffineRegistrationParametersNextScale, broccoli_lib.cpp:7344-7431.
+void ref_add_affine_next_scale(float* old12, const float* new12) {
+  Eigen::MatrixXd T = to_affine(new12, 2.0f) * to_affine(old12, 2.0f);
+  from_affine(T, old12);
+}
+
+// CalculateRotationAnglesFromRotationMatrix, broccoli_lib.cpp:6199-6244.
+void ref_rotation_angles(const float* p, float* rot) {
+  const double PI_ = 3.14159265358979323846;
+  double m[9];
+  for (int i = 3; i < 12; i++) m[i - 3] = (double)p[i];
+  m[0] += 1.0; m[4] += 1.0; m[8] += 1.0;
+  const double a1 = -atan2(m[5], m[8]) * 180.0 / PI_;
+  const double c2 = sqrt(m[0] * m[0] + m[1] * m[1]);
+  const double a2 = -atan2(-m[2], c2) * 180.0 / PI_;
+  const double s1 = sin(a1 * PI_ / 180.0), c1 = cos(a1 * PI_ / 180.0);
+  const double a3 = -atan2(s1 * m[6] - c1 * m[3], c1 * m[4] - s1 * m[7]) * 180.0 / PI_;
+  rot[0] = (float)a1; rot[1] = (float)a2; rot[2] = (float)a3;
+}
+
+// InterpolateVolumeLinearLinear (kernelRegistration.cpp:1066-1101) as driven
+// at broccoli_lib.cpp:5424-5427.
+void ref_warp_affine(const float* src, int W, int H, int D, const float* p12, float* out) {
+  const image3d_t im{src, W, H, D};
+  ndrange(roundup(W, 16), roundup(H, 16), D, 16, 16, 1,
+          [&] { clr::InterpolateVolumeLinearLinear(out, im, p12, W, H, D, 0); });
+}
+
+// InterpolateVolumeLinearNonLinear, kernelRegistration.cpp:1111-1140.
+void ref_warp_field(const float* src, int W, int H, int D, const float* dx, const float* dy,
+                    const float* dz, float* out) {
+  const image3d_t im{src, W, H, D};
+  ndrange(roundup(W, 16), roundup(H, 16), D, 16, 16, 1,
+          [&] { clr::InterpolateVolumeLinearNonLinear(out, im, dx, dy, dz, W, H, D, 0); });
+}
+
+// ChangeVolumeSize with LINEAR interpolation, broccoli_lib.cpp:6247-6388.
+void ref_rescale_linear(const float* src, int W, int H, int D, int W2, int H2, int D2, float* out) {
+  const image3d_t im{src, W, H, D};
+  const float vx = (float)(W - 1) / (float)(W2 - 1);
+  const float vy = (float)(H - 1) / (float)(H2 - 1);
+  const float vz = (float)(D - 1) / (float)(D2 - 1);
+  ndrange(roundup(W2, 16), roundup(H2, 16), D2, 16, 16, 1,
+          [&] { clr::RescaleVolumeLinear(out, im, vx, vy, vz, W2, H2, D2); });
+}
+
+// AlignTwoVolumesLinear, broccoli_lib.cpp:5273-5437 (type 0 TRANSLATION,
+// 1 RIGID, 2 AFFINE).  `aligned` is updated in place; `original` is the
+// image that is re-sampled each iteration.
+void ref_align_linear(const float* ref, float* aligned, const float* original, int W, int H, int D,
+                      const float* filters, int niter, int type, float* p12, float* rot3) {
+  const long V = (long)W * H * D;
+  std::vector<float> q1(6 * V), q2(6 * V);
+  float A[144], h[12], p[12];
+  ref_filter3d(ref, W, H, D, filters, q1.data());
+  for (int i = 0; i < 12; i++) p12[i] = 0.f;
+  for (int it = 0; it < niter; it++) {
+    ref_filter3d(aligned, W, H, D, filters, q2.data());
+    ref_normal_equations(q1.data(), q2.data(), W, H, D, A, h);
+    ref_solve(A, h, 12, p);
+    if (type == 0) {
+      p12[0] += p[0]; p12[1] += p[1]; p12[2] += p[2];
+      for (int i = 3; i < 12; i++) p12[i] = 0.f;
+    } else if (type == 1) {
+      ref_remove_scaling(p);
+      ref_add_affine(p12, p);
+    } else {
+      ref_add_affine(p12, p);
+    }
+    ref_warp_affine(original, W, H, D, p12, aligned);
+  }
+  if (type == 1 && rot3) ref_rotation_angles(p12, rot3);
+}
+
+// PerformMotionCorrectionWrapper, broccoli_lib.cpp:10658-10720 (reference =
+// volume 0; the reference volume is refiltered for every volume, as there).
+void ref_motion_correct(float* vols, int W, int H, int D, int T, const float* voxel_size,
+                        const float* filters, int niter, float* motion6T) {
+  const long V = (long)W * H * D;
+  std::vector<float> ref(vols, vols + V), orig(V);
+  for (int k = 0; k < 6; k++) motion6T[k * T] = 0.f;
+  for (int t = 1; t < T; t++) {
+    float p[12], rot[3];
+    float* vt = vols + (long)t * V;
+    std::memcpy(orig.data(), vt, sizeof(float) * V);
+    ref_align_linear(ref.data(), vt, orig.data(), W, H, D, filters, niter, 1, p, rot);
+    motion6T[t + 0 * T] = p[0] * voxel_size[0];
+    motion6T[t + 1 * T] = p[1] * voxel_size[1];
+    motion6T[t + 2 * T] = p[2] * voxel_size[2];
+    motion6T[t + 3 * T] = rot[0];
+    motion6T[t + 4 * T] = rot[1];
+    motion6T[t + 5 * T] = rot[2];
+  }
+}
+
+// PerformSmoothing (broccoli_lib.cpp:11274-11357): Rows (x certainty),
+// Columns, Rods (/ smoothed certainty) with the GlobalMemory kernels
+// (kernelConvolution.cpp:52-91, :531-569, :1201-1240).  cert and
+// smoothed_cert may be NULL for all-ones.
+void ref_smooth3d(const float* vol, const float* cert, const float* scert, int W, int H, int D,
+                  const float* fx, const float* fy, const float* fz, float* out) {
+  const long V = (long)W * H * D;
+  std::vector<float> ones, rows(V), cols(V);
+  if (!cert || !scert) ones.assign(V, 1.f);
+  const float* c = cert ? cert : ones.data();
+  const float* sc = scert ? scert : ones.data();
+  const int gx = roundup(W, 16), gy = roundup(H, 16);
+  ndrange(gx, gy, D, 16, 16, 1,
+          [&] { clk::SeparableConvolutionRowsGlobalMemory(rows.data(), vol, c, fy, 0, W, H, D, 1); });
+  ndrange(gx, gy, D, 16, 16, 1,
+          [&] { clk::SeparableConvolutionColumnsGlobalMemory(cols.data(), rows.data(), fx, 0, W, H, D, 1); });
+  ndrange(gx, gy, D, 16, 16, 1,
+          [&] { clk::SeparableConvolutionRodsGlobalMemory(out, cols.data(), sc, fz, 0, W, H, D, 1); });
+}
+
+}  // extern "C"
