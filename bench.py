@@ -1,0 +1,373 @@
+"""Benchmark: batched rigid motion correction of a 64x64x33x200 series.
+
+One step = registering volumes 1..199 of a synthetic fMRI-like series to
+volume 0 (199 rigid registrations, up to 20 iterations each, per-volume
+early exit at a 1e-3-voxel update), all instances in one batched launch
+sequence replayed from a CUDA graph.  Metric: registrations per second.
+
+  value   inputs resident in HBM (device-pointer entry point)
+  e2e     the host-buffer entry point brc_motion_correct: pinned host
+          series in, corrected series and motion parameters out, copies
+          inside the timed region
+  --impl reference   the reference's CPU implementation of the path
+          (oracle/_ref: its OpenCL C kernels compiled for the CPU with the
+          host loops restated; else the C restatement) on a bounded sample
+          of the same workload, all host threads
+
+Multi-GPU (torchrun, --gpus N): replicas -- every rank corrects its own
+series (weak scaling); no data-path collective; time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SHAPE = (33, 64, 64)  # D, H, W
+T = 200  # series length (--series overrides, e.g. for small profiling runs)
+ITERS = 20
+TOL = 1e-3
+VOXEL = (3.0, 3.0, 3.0)
+METRIC = "registrations/sec at <=0.05-voxel RMS err (batched rigid motion correction)"
+UNIT = "registrations/s"
+FLOP_PER_VOXEL_FILTER = 1372  # per complex 7^3 filter (343 taps x 2 real MACs x 2)
+
+
+def workload_config(n_gpus: int, extra: dict | None = None) -> dict:
+    c = {
+        "workload": "batched rigid motion correction, 64x64x33x200 series to volume 0",
+        "volume": [64, 64, 33],
+        "series_length": T,
+        "registrations_per_step_per_gpu": T - 1,
+        "max_iterations": ITERS,
+        "early_exit_voxels": TOL,
+        "filters": "3 complex 7x7x7 quadrature filters (lognormal, u0=pi/3, 2 octaves)",
+        "noise": "Rician, SNR 50",
+        "certainty_smoothing": "off",
+        "parallelism": f"replicas x{n_gpus}",
+        "l2": "flushed between timed steps (256 MiB write)",
+    }
+    if extra:
+        c.update(extra)
+    return c
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_series(rank: int = 0):
+    from broccoli_b200 import synthetic as S
+    vols, truth = S.motion_series(T=T, shape=SHAPE, base_seed=rank, snr=50.0)
+    return vols, truth
+
+
+def filters():
+    from broccoli_b200 import filters as F
+    return F.linear_registration_filters()
+
+
+def accuracy(vols, truth, params, flt, n_oracle: int = 2) -> dict:
+    """RMS displacement error of the GPU results against the FP64 oracle on
+    a sample of volumes, and against the known motion on all volumes."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from broccoli_b200 import synthetic as S
+    vs_truth = []
+    for i in range(params.shape[0]):
+        rel = S.relative_params(truth[0], truth[i + 1])
+        vs_truth.append(S.rms_displacement_error(params[i], rel, SHAPE))
+    vs_oracle = []
+    for i in range(n_oracle):
+        p64, _, _ = oracle.align_linear(vols[0], vols[i + 1], flt, ITERS, oracle.RIGID, prec="f64")
+        vs_oracle.append(S.rms_displacement_error(params[i], p64, SHAPE))
+    return {"rms_vs_fp64_oracle_max": float(max(vs_oracle)) if vs_oracle else None,
+            "oracle_sample": n_oracle,
+            "rms_vs_truth_mean": float(np.mean(vs_truth)),
+            "rms_vs_truth_max": float(np.max(vs_truth))}
+
+
+def cpu_reference_rate(vols, flt, n_regs: int, iters: int = ITERS):
+    """Registrations/s of the reference's CPU path on n_regs volumes of the
+    series.  Returns (rate, kind, threads, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    kind = "reference" if oracle.ref_available() else "port"
+    fn = oracle.ref_align_linear if kind == "reference" else oracle.align_linear
+    t0 = time.perf_counter()
+    for i in range(n_regs):
+        fn(vols[0], vols[1 + i], flt, iters, oracle.RIGID)
+    dt = time.perf_counter() - t0
+    return n_regs / dt, kind, oracle.num_threads(), dt
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    vols, _ = make_series(0)
+    flt = filters()
+    n_regs = 2
+    rates = []
+    for _ in range(args.warmup):
+        cpu_reference_rate(vols, flt, 1)
+    secs = 0.0
+    for _ in range(args.steps):
+        r, kind, thr, dt = cpu_reference_rate(vols, flt, n_regs)
+        rates.append(r)
+        secs += dt
+    value = float(np.median(rates))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * secs / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": workload_config(args.gpus),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": thr, "kind": kind,
+                         "sample": f"{n_regs} of the {T - 1} registrations per step, {ITERS} iterations "
+                                   "each (the reference runs every iteration; no early exit)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_gpu(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from broccoli_b200 import _lib as L
+    from broccoli_b200.api import Context
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    ctx = Context(local_rank)
+    flt = filters()
+    vols, truth = make_series(rank)
+    D, H, W = SHAPE
+    V = D * H * W
+    d_series = torch.from_numpy(vols).to(dev)
+    ref = d_series[0]
+    moving = d_series[1:]
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+
+    def step():
+        return ctx.register_linear(ref, moving, flt, ITERS, L.RIGID, tolerance=TOL)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        out = step()
+    torch.cuda.synchronize()
+
+    # ---- device-resident timed region ----
+    sampler = ClockSampler(local_rank) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    launches0 = ctx.kernel_launches
+    st = torch.cuda.current_stream()
+    times = []
+    barrier()
+    torch.cuda.synchronize()
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        out = step()
+        e1.record(st)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    torch.cuda.synchronize()
+    barrier()
+    launches = ctx.kernel_launches - launches0
+    clocks = sampler.stop() if sampler else None
+    ms = float(np.sum(times))
+    iters_used = out["iterations"].cpu().numpy()
+
+    # ---- end-to-end through the host-buffer entry point ----
+    host = torch.from_numpy(vols).pin_memory()
+    motion = np.zeros(6 * T, np.float32)
+    e2e_times = []
+    import ctypes
+    opts = L.LinearOpts()
+    L.lib().brc_linear_opts_default(ctypes.byref(opts), ITERS)
+    opts.type = L.RIGID
+    opts.tolerance = TOL
+    vs = np.asarray(VOXEL, np.float32)
+    fl = np.ascontiguousarray(flt, np.float32)
+    work = torch.empty_like(host).pin_memory()
+    ctx._bind_stream()
+    for k in range(args.warmup + args.steps):
+        work.copy_(host)
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        s = L.lib().brc_motion_correct(ctx.handle, ctypes.c_void_p(work.data_ptr()), W, H, D, T,
+                                       vs.ctypes.data_as(ctypes.c_void_p), fl.ctypes.data_as(ctypes.c_void_p),
+                                       ctypes.byref(opts), None, motion.ctypes.data_as(ctypes.c_void_p))
+        dt = time.perf_counter() - t0
+        if s != 0:
+            raise RuntimeError(f"brc_motion_correct failed: {s}")
+        if k >= args.warmup:
+            e2e_times.append(dt * 1000.0)
+    e2e_ms = float(np.sum(e2e_times))
+
+    # ---- dominant kernel alone: 7^3 filtering of the 199 moving volumes ----
+    q = torch.empty((T - 1, 3, D, H, W, 2), dtype=torch.float32, device=dev)
+    for _ in range(3):
+        L.lib().brc_filter3d(ctx.handle, ctypes.c_void_p(moving.data_ptr()), W, H, D, T - 1, V,
+                             fl.ctypes.data_as(ctypes.c_void_p), 3, 0, ctypes.c_void_p(q.data_ptr()))
+    torch.cuda.synchronize()
+    nrep = 20
+    fe0 = torch.cuda.Event(enable_timing=True)
+    fe1 = torch.cuda.Event(enable_timing=True)
+    fe0.record(st)
+    for _ in range(nrep):
+        L.lib().brc_filter3d(ctx.handle, ctypes.c_void_p(moving.data_ptr()), W, H, D, T - 1, V,
+                             fl.ctypes.data_as(ctypes.c_void_p), 3, 0, ctypes.c_void_p(q.data_ptr()))
+    fe1.record(st)
+    fe1.synchronize()
+    f_ms = fe0.elapsed_time(fe1) / nrep
+    f_flop = FLOP_PER_VOXEL_FILTER * 3 * V * (T - 1)
+
+    # ---- reduce over ranks ----
+    t_max = ms
+    e_max = e2e_ms
+    if world > 1:
+        tt = torch.tensor([ms, e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max, e_max = float(tt[0]), float(tt[1])
+    if rank != 0:
+        return
+    regs = (T - 1) * world * args.steps
+    value = regs / (t_max / 1000.0)
+    e2e_value = regs / (e_max / 1000.0)
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    sm_max = clocks.get("sm_max_mhz") if clocks else None
+    fp32_peak = 148 * 128 * 2 * (sm_max or 1965.0) * 1e6 / 1e12
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "filter3d_fp32_traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get("dram_bytes_per_launch")
+    achieved = f_flop / (f_ms / 1000.0) / 1e12
+    acc = accuracy(vols, truth, out["params"].cpu().numpy(), flt) if not args.skip_accuracy else None
+    cpu = None
+    if not args.skip_cpu:
+        r, kind, thr, dt = cpu_reference_rate(vols, flt, 8)
+        cpu = {"value": r, "unit": UNIT, "cores": thr, "kind": kind,
+               "sample": f"8 of the {T - 1} registrations of one series, {ITERS} iterations each, "
+                         f"{dt:.1f} s"}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(world, {"mean_iterations": float(iters_used.mean()),
+                                          "precision": "fp32"}),
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(4 * V * T),
+                "d2h_bytes_per_step": int(4 * V * (T - 1) + 4 * 15 * (T - 1))},
+        "gpu_launches": int(launches),
+        "roofline": {"kernel": "filter3d_fp32_kernel<3,8,3>", "bound": "fp32",
+                     "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                     "frac": achieved / fp32_peak,
+                     "peak_source": "nominal FP32 FMA rate 148 SMs x 128 lanes x 2 at the sampled max SM clock "
+                                    "(MEASURED_PEAKS.json has no FP32 figure)",
+                     "flop_per_launch": f_flop, "launch_ms": f_ms, "traffic": traffic},
+        "accuracy": acc,
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-accuracy", action="store_true")
+    ap.add_argument("--series", type=int, default=T, help="series length (volumes)")
+    args = ap.parse_args()
+    globals()["T"] = args.series
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_gpu(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

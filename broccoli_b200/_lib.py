@@ -1,0 +1,103 @@
+"""ctypes binding of libbroccoli_b200.so (the C-ABI in include/broccoli_b200.h).
+
+The shared library is built in-tree (``make -C broccoli_b200``) and loaded
+from this directory.  There is no fallback: if the library is missing or no
+sm_100 device is present the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbroccoli_b200.so")
+HEADER_PATH = os.path.join(os.path.dirname(HERE), "include", "broccoli_b200.h")
+
+BRC_OK = 0
+BRC_ERR_INVALID = -1
+BRC_ERR_NOMEM = -2
+BRC_ERR_CUDA = -3
+BRC_ERR_TIMEOUT = -4
+BRC_ERR_NODEVICE = -5
+BRC_ERR_UNSUPPORTED = -6
+BRC_ERR_NONFINITE = -7
+
+TRANSLATION, RIGID, AFFINE = 0, 1, 2
+PREC_FP32, PREC_BF16X3 = 0, 1
+
+
+class BrcError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+
+
+class LinearOpts(ctypes.Structure):
+    _fields_ = [
+        ("iterations", ctypes.c_int),
+        ("type", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("tolerance", ctypes.c_float),
+        ("use_graph", ctypes.c_int),
+        ("certainty_sigma_x100", ctypes.c_int),
+    ]
+
+
+_lib = None
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_LL = ctypes.c_longlong
+
+_SIGS = {
+    "brc_version": ([], ctypes.c_char_p),
+    "brc_status_string": ([_I], ctypes.c_char_p),
+    "brc_last_error": ([_P], ctypes.c_char_p),
+    "brc_ctx_create": ([_I, ctypes.POINTER(_P)], _I),
+    "brc_ctx_destroy": ([_P], _I),
+    "brc_ctx_set_stream": ([_P, _P], _I),
+    "brc_ctx_stream": ([_P], _P),
+    "brc_ctx_synchronize": ([_P], _I),
+    "brc_ctx_workspace_bytes": ([_P], ctypes.c_size_t),
+    "brc_ctx_kernel_launches": ([_P], ctypes.c_ulonglong),
+    "brc_filter3d": ([_P, _P, _I, _I, _I, _I, _LL, _P, _I, _I, _P], _I),
+    "brc_normal_equations": ([_P, _P, _LL, _P, _I, _I, _I, _I, _P, _P], _I),
+    "brc_solve_affine_fp64": ([_P, _P, _P, _I, _P], _I),
+    "brc_warp_affine": ([_P, _P, _I, _I, _I, _I, _P, _P], _I),
+    "brc_warp_field": ([_P, _P, _I, _I, _I, _P, _P, _P, _P], _I),
+    "brc_smooth3d": ([_P, _P, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P], _I),
+    "brc_rescale_linear": ([_P, _P, _I, _I, _I, _P, _I, _I, _I], _I),
+    "brc_linear_opts_default": ([ctypes.POINTER(LinearOpts), _I], None),
+    "brc_register_linear_batched": (
+        [_P, _P, _LL, _P, _I, _I, _I, _I, _P, ctypes.POINTER(LinearOpts), _P, _P, _P, _P], _I),
+    "brc_motion_correct": (
+        [_P, _P, _I, _I, _I, _I, _P, _P, ctypes.POINTER(LinearOpts), _P, _P], _I),
+}
+
+
+def header_symbols(path: str = HEADER_PATH) -> list:
+    """Function names declared in the C-ABI header."""
+    text = open(path).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(brc_[a-z0-9_]+)\s*\(", text)))
+
+
+def lib():
+    """The loaded library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C {HERE}` "
+                               "or __graft_entry__.build()")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (args, res) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def status_string(s: int) -> str:
+    return lib().brc_status_string(s).decode()

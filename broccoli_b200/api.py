@@ -1,0 +1,225 @@
+"""Torch-facing wrappers over the C-ABI.
+
+Device memory and streams come from torch (plumbing only); every operation
+runs in libbroccoli_b200's sm_100a kernels.  Volumes are float32 tensors
+shaped (D, H, W) or batches (B, D, H, W), x fastest in memory as in the
+reference.  Filter banks are numpy/torch arrays shaped (nfilt, 2, 7, 7, 7)
+(filter, re/im, z, y, x).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+
+def _check(ctx: "Context", status: int) -> None:
+    if status != L.BRC_OK:
+        msg = L.lib().brc_last_error(ctx.handle).decode() if ctx is not None else ""
+        raise L.BrcError(status, f"{L.status_string(status)}: {msg}")
+
+
+def _host_filters(filters) -> np.ndarray:
+    f = filters.detach().cpu().numpy() if isinstance(filters, torch.Tensor) else np.asarray(filters)
+    f = np.ascontiguousarray(f, dtype=np.float32)
+    if f.ndim != 5 or f.shape[1:] != (2, 7, 7, 7):
+        raise ValueError("filter bank must have shape (nfilt, 2, 7, 7, 7)")
+    return f
+
+
+def _vol_batch(t: torch.Tensor):
+    if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != torch.float32:
+        raise TypeError("volumes must be float32 CUDA tensors")
+    if t.dim() == 3:
+        t = t.unsqueeze(0)
+    if t.dim() != 4:
+        raise ValueError("volumes must be (D,H,W) or (B,D,H,W)")
+    return t.contiguous()
+
+
+def _p(t: torch.Tensor):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class Context:
+    """A library context bound to one CUDA device.  Work is queued on torch's
+    current stream of that device at call time."""
+
+    def __init__(self, device: int = 0):
+        h = ctypes.c_void_p()
+        s = L.lib().brc_ctx_create(device, ctypes.byref(h))
+        if s != L.BRC_OK:
+            raise L.BrcError(s, f"brc_ctx_create({device}): {L.status_string(s)}")
+        self.handle = h
+        self.device = device
+
+    def close(self) -> None:
+        if self.handle:
+            L.lib().brc_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _bind_stream(self) -> None:
+        # torch's default stream is the legacy NULL stream (handle 0), which
+        # the C-ABI takes as NULL; other torch streams pass their handle.
+        st = torch.cuda.current_stream(self.device).cuda_stream
+        _check(self, L.lib().brc_ctx_set_stream(self.handle, ctypes.c_void_p(st) if st else None))
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(L.lib().brc_ctx_kernel_launches(self.handle))
+
+    @property
+    def workspace_bytes(self) -> int:
+        return int(L.lib().brc_ctx_workspace_bytes(self.handle))
+
+    # ---- kernels ---------------------------------------------------------
+
+    def filter3d(self, vol: torch.Tensor, filters, precision: int = L.PREC_FP32) -> torch.Tensor:
+        """Complex responses (B, nfilt, D, H, W) of the 7^3 filter bank."""
+        v = _vol_batch(vol)
+        f = _host_filters(filters)
+        B, D, H, W = v.shape
+        out = torch.empty((B, f.shape[0], D, H, W, 2), dtype=torch.float32, device=v.device)
+        self._bind_stream()
+        _check(self, L.lib().brc_filter3d(self.handle, _p(v), W, H, D, B, D * H * W,
+                                          f.ctypes.data_as(ctypes.c_void_p), f.shape[0], precision,
+                                          _p(out)))
+        return torch.view_as_complex(out)
+
+    def normal_equations(self, q1: torch.Tensor, q2: torch.Tensor):
+        """A (B,12,12) and h (B,12) in float64 from reference responses q1
+        ((3,D,H,W) shared, or (B,3,D,H,W)) and aligned responses q2
+        (B,3,D,H,W) (complex64)."""
+        if q2.dim() == 4:
+            q2 = q2.unsqueeze(0)
+        B, nf, D, H, W = q2.shape
+        shared = q1.dim() == 4
+        a = torch.view_as_real(q1.contiguous()).contiguous()
+        c = torch.view_as_real(q2.contiguous()).contiguous()
+        A = torch.empty((B, 12, 12), dtype=torch.float64, device=q2.device)
+        h = torch.empty((B, 12), dtype=torch.float64, device=q2.device)
+        self._bind_stream()
+        _check(self, L.lib().brc_normal_equations(self.handle, _p(a), 0 if shared else 6 * D * H * W,
+                                                  _p(c), W, H, D, B, _p(A), _p(h)))
+        return A.transpose(1, 2), h
+
+    def solve(self, A: torch.Tensor, h: torch.Tensor) -> torch.Tensor:
+        if A.dim() == 2:
+            A, h = A.unsqueeze(0), h.unsqueeze(0)
+        Acm = A.transpose(1, 2).contiguous().to(torch.float64)
+        hv = h.contiguous().to(torch.float64)
+        p = torch.empty((A.shape[0], 12), dtype=torch.float32, device=A.device)
+        self._bind_stream()
+        _check(self, L.lib().brc_solve_affine_fp64(self.handle, _p(Acm), _p(hv), A.shape[0], _p(p)))
+        return p
+
+    def warp_affine(self, src: torch.Tensor, params: torch.Tensor) -> torch.Tensor:
+        v = _vol_batch(src)
+        B, D, H, W = v.shape
+        p = params.reshape(B, 12).contiguous().to(torch.float32)
+        out = torch.empty_like(v)
+        self._bind_stream()
+        _check(self, L.lib().brc_warp_affine(self.handle, _p(v), W, H, D, B, _p(p), _p(out)))
+        return out
+
+    def warp_field(self, src: torch.Tensor, dx, dy, dz) -> torch.Tensor:
+        v = src.contiguous()
+        D, H, W = v.shape
+        fx, fy, fz = (t.contiguous().to(torch.float32) for t in (dx, dy, dz))
+        out = torch.empty_like(v)
+        self._bind_stream()
+        _check(self, L.lib().brc_warp_field(self.handle, _p(v), W, H, D, _p(fx), _p(fy), _p(fz), _p(out)))
+        return out
+
+    def smooth3d(self, vol: torch.Tensor, fx, fy, fz, cert=None, smoothed_cert=None) -> torch.Tensor:
+        v = _vol_batch(vol)
+        B, D, H, W = v.shape
+        taps = [np.ascontiguousarray(np.asarray(f, np.float32).reshape(9)) for f in (fx, fy, fz)]
+        out = torch.empty_like(v)
+        c = cert.contiguous() if cert is not None else None
+        sc = smoothed_cert.contiguous() if smoothed_cert is not None else None
+        self._bind_stream()
+        _check(self, L.lib().brc_smooth3d(self.handle, _p(v), W, H, D, B,
+                                          *[t.ctypes.data_as(ctypes.c_void_p) for t in taps],
+                                          _p(c) if c is not None else None,
+                                          _p(sc) if sc is not None else None, _p(out)))
+        return out if vol.dim() == 4 else out[0]
+
+    def rescale_linear(self, src: torch.Tensor, shape) -> torch.Tensor:
+        v = src.contiguous()
+        D, H, W = v.shape
+        D2, H2, W2 = shape
+        out = torch.empty((D2, H2, W2), dtype=torch.float32, device=v.device)
+        self._bind_stream()
+        _check(self, L.lib().brc_rescale_linear(self.handle, _p(v), W, H, D, _p(out), W2, H2, D2))
+        return out
+
+    # ---- whole path ------------------------------------------------------
+
+    def register_linear(self, ref: torch.Tensor, moving: torch.Tensor, filters, iterations: int,
+                        type_: int = L.AFFINE, tolerance: float = 0.0, use_graph: bool = True,
+                        precision: int = L.PREC_FP32, certainty_sigma: float = 0.0):
+        """Batched single-scale registration of moving (B,D,H,W) onto ref
+        ((D,H,W) shared or (B,D,H,W)).  Returns dict with params (B,12),
+        aligned (B,D,H,W), rotations (B,3) and iterations (B,)."""
+        m = _vol_batch(moving)
+        B, D, H, W = m.shape
+        r = ref.contiguous()
+        ref_stride = 0 if r.dim() == 3 else D * H * W
+        f = _host_filters(filters)
+        if f.shape[0] != 3:
+            raise ValueError("linear registration uses 3 filters")
+        opts = L.LinearOpts()
+        L.lib().brc_linear_opts_default(ctypes.byref(opts), iterations)
+        opts.type = type_
+        opts.tolerance = tolerance
+        opts.use_graph = 1 if use_graph else 0
+        opts.precision = precision
+        opts.certainty_sigma_x100 = int(round(certainty_sigma * 100))
+        params = torch.empty((B, 12), dtype=torch.float32, device=m.device)
+        aligned = torch.empty_like(m)
+        rot = torch.empty((B, 3), dtype=torch.float32, device=m.device)
+        iters = torch.empty((B,), dtype=torch.int32, device=m.device)
+        self._bind_stream()
+        _check(self, L.lib().brc_register_linear_batched(
+            self.handle, _p(r), ref_stride, _p(m), W, H, D, B, f.ctypes.data_as(ctypes.c_void_p),
+            ctypes.byref(opts), _p(params), _p(aligned), _p(rot), _p(iters)))
+        return {"params": params, "aligned": aligned, "rotations": rot, "iterations": iters}
+
+    def motion_correct(self, volumes: np.ndarray, voxel_size, filters, iterations: int,
+                       tolerance: float = 0.0, reference: np.ndarray = None, use_graph: bool = True,
+                       precision: int = L.PREC_FP32, certainty_sigma: float = 0.0):
+        """Host-buffer motion correction of a (T,D,H,W) float32 series.
+        Returns (corrected series, motion (6,T): mm then degrees).  The
+        input array is not modified (a copy is corrected)."""
+        v = np.ascontiguousarray(volumes, dtype=np.float32).copy()
+        T, D, H, W = v.shape
+        vs = np.ascontiguousarray(voxel_size, dtype=np.float32)
+        f = _host_filters(filters)
+        motion = np.zeros(6 * T, np.float32)
+        opts = L.LinearOpts()
+        L.lib().brc_linear_opts_default(ctypes.byref(opts), iterations)
+        opts.type = L.RIGID
+        opts.tolerance = tolerance
+        opts.use_graph = 1 if use_graph else 0
+        opts.precision = precision
+        opts.certainty_sigma_x100 = int(round(certainty_sigma * 100))
+        refp = None
+        if reference is not None:
+            ref_arr = np.ascontiguousarray(reference, dtype=np.float32)
+            refp = ref_arr.ctypes.data_as(ctypes.c_void_p)
+        self._bind_stream()
+        _check(self, L.lib().brc_motion_correct(
+            self.handle, v.ctypes.data_as(ctypes.c_void_p), W, H, D, T, vs.ctypes.data_as(ctypes.c_void_p),
+            f.ctypes.data_as(ctypes.c_void_p), ctypes.byref(opts), refp,
+            motion.ctypes.data_as(ctypes.c_void_p)))
+        return v, motion.reshape(6, T)

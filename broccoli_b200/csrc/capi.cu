@@ -1,0 +1,472 @@
+// capi.cu -- the C-ABI of libbroccoli_b200 (include/broccoli_b200.h):
+// context and workspace management, argument checking, the batched
+// registration driver (optionally captured once into a CUDA graph and
+// replayed) and the host-buffer motion-correction entry point.
+#include <cuda_runtime.h>
+#include <limits.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <map>
+#include <memory>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/broccoli_b200.h"
+#include "common.cuh"
+
+#include "capi_ctx.h"
+#include "internal.h"
+
+namespace {
+
+uint64_t fnv1a(const void* data, size_t n, uint64_t h = 1469598103934665603ull) {
+  const unsigned char* p = static_cast<const unsigned char*>(data);
+  for (size_t i = 0; i < n; i++) {
+    h ^= p[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+// Interior slices per CTA of the normal-equation reduction: about 4k
+// interior voxels per CTA.
+int pick_zpb(int W, int H) {
+  const long long plane = (long long)(W > 6 ? W - 6 : 1) * (H > 6 ? H - 6 : 1);
+  long long z = 4096 / (plane > 0 ? plane : 1);
+  if (z < 1) z = 1;
+  if (z > 64) z = 64;
+  return (int)z;
+}
+
+}  // namespace
+
+static bool bad_dims(int W, int H, int D) {
+  return W <= 0 || H <= 0 || D <= 0 || (long long)W * H * D > (1ll << 31);
+}
+
+extern "C" {
+
+const char* brc_version(void) { return "broccoli_b200 0.1 (sm_100a)"; }
+
+const char* brc_status_string(int s) {
+  switch (s) {
+    case BRC_OK: return "ok";
+    case BRC_ERR_INVALID: return "invalid argument";
+    case BRC_ERR_NOMEM: return "out of memory";
+    case BRC_ERR_CUDA: return "CUDA error";
+    case BRC_ERR_TIMEOUT: return "device-side wait timed out";
+    case BRC_ERR_NODEVICE: return "no usable CUDA device";
+    case BRC_ERR_UNSUPPORTED: return "unsupported option";
+    case BRC_ERR_NONFINITE: return "non-finite solution";
+    default: return "unknown status";
+  }
+}
+
+const char* brc_last_error(const brc_ctx* ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+int brc_ctx_create(int device, brc_ctx** out) {
+  if (!out) return BRC_ERR_INVALID;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return BRC_ERR_NODEVICE;
+  if (device < 0 || device >= n) return BRC_ERR_INVALID;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return BRC_ERR_NODEVICE;
+  if (prop.major != 10) return BRC_ERR_NODEVICE;  // built for sm_100a only
+  std::unique_ptr<brc_ctx> ctx(new brc_ctx());
+  ctx->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) return BRC_ERR_NODEVICE;
+  if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess)
+    return BRC_ERR_CUDA;
+  if (cudaEventCreateWithFlags(&ctx->ev_in, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_out, cudaEventDisableTiming) != cudaSuccess)
+    return BRC_ERR_CUDA;
+  if (brc::filter3d_init() != cudaSuccess) return BRC_ERR_CUDA;
+  *out = ctx.release();
+  return BRC_OK;
+}
+
+int brc_ctx_destroy(brc_ctx* ctx) {
+  BRC_CHECK_CTX(ctx);
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->own_stream);
+  if (ctx->use_user_stream) cudaStreamSynchronize(ctx->user_stream);
+  ctx->graphs.clear();
+  if (ctx->ev_in) cudaEventDestroy(ctx->ev_in);
+  if (ctx->ev_out) cudaEventDestroy(ctx->ev_out);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+  return BRC_OK;
+}
+
+int brc_ctx_set_stream(brc_ctx* ctx, void* s) {
+  BRC_CHECK_CTX(ctx);
+  if (s == BRC_OWN_STREAM) {
+    ctx->use_user_stream = false;
+    ctx->user_stream = nullptr;
+  } else {
+    ctx->use_user_stream = true;
+    ctx->user_stream = static_cast<cudaStream_t>(s);
+  }
+  return BRC_OK;
+}
+
+void* brc_ctx_stream(brc_ctx* ctx) { return ctx ? (void*)ctx->stream() : nullptr; }
+
+int brc_ctx_synchronize(brc_ctx* ctx) {
+  BRC_CHECK_CTX(ctx);
+  return ctx->cuda(cudaStreamSynchronize(ctx->stream()), "synchronize");
+}
+
+size_t brc_ctx_workspace_bytes(const brc_ctx* ctx) { return ctx ? ctx->workspace() : 0; }
+
+unsigned long long brc_ctx_kernel_launches(const brc_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int brc_filter3d(brc_ctx* ctx, const float* d_vol, int W, int H, int D, int batch,
+                 long long vol_stride, const float* h_filters, int nfilt, int precision,
+                 float* d_out) {
+  BRC_CHECK_CTX(ctx);
+  if (!d_vol || !d_out || !h_filters || bad_dims(W, H, D) || batch <= 0 || batch > 65535)
+    return ctx->fail(BRC_ERR_INVALID, "brc_filter3d: bad pointer or size");
+  if (nfilt != 3 && nfilt != 6) return ctx->fail(BRC_ERR_INVALID, "brc_filter3d: nfilt must be 3 or 6");
+  if (batch > 1 && vol_stride < (long long)W * H * D)
+    return ctx->fail(BRC_ERR_INVALID, "brc_filter3d: vol_stride smaller than a volume");
+  if (precision != BRC_PREC_FP32)
+    return ctx->fail(BRC_ERR_UNSUPPORTED, "brc_filter3d: precision not available");
+  cudaSetDevice(ctx->device);
+  BRC_TRY(ctx, brc::filter3d_fp32(d_vol, W, H, D, batch, vol_stride, h_filters, nfilt, d_out, nullptr,
+                                  0, ctx->stream()),
+          "filter3d");
+  ctx->launches += 1;
+  return BRC_OK;
+}
+
+int brc_normal_equations(brc_ctx* ctx, const float* d_q1, long long q1_stride, const float* d_q2,
+                         int W, int H, int D, int batch, double* d_A, double* d_h) {
+  BRC_CHECK_CTX(ctx);
+  if (!d_q1 || !d_q2 || !d_A || !d_h || bad_dims(W, H, D) || batch <= 0 || batch > 65535)
+    return ctx->fail(BRC_ERR_INVALID, "brc_normal_equations: bad pointer or size");
+  cudaSetDevice(ctx->device);
+  const int zpb = pick_zpb(W, H);
+  const int nint = D - 6 > 0 ? D - 6 : 1;
+  const int nblk = (nint + zpb - 1) / zpb;
+  BRC_TRY(ctx, ctx->partials.ensure(sizeof(double) * brc::kNSums * nblk * (size_t)batch), "alloc");
+  BRC_TRY(ctx, brc::normal_eq_partials(d_q1, q1_stride, d_q2, W, H, D, batch,
+                                       ctx->partials.as<double>(), nblk, zpb, nullptr, 0, ctx->stream()),
+          "normal_eq_partials");
+  BRC_TRY(ctx, brc::assemble_normal_eq(ctx->partials.as<double>(), nblk, batch, d_A, d_h, ctx->stream()),
+          "assemble");
+  ctx->launches += 2;
+  return BRC_OK;
+}
+
+int brc_solve_affine_fp64(brc_ctx* ctx, const double* d_A, const double* d_h, int batch, float* d_p) {
+  BRC_CHECK_CTX(ctx);
+  if (!d_A || !d_h || !d_p || batch <= 0) return ctx->fail(BRC_ERR_INVALID, "brc_solve_affine_fp64: bad argument");
+  cudaSetDevice(ctx->device);
+  BRC_TRY(ctx, brc::solve_given(d_A, d_h, batch, d_p, ctx->stream()), "solve");
+  ctx->launches += 1;
+  return BRC_OK;
+}
+
+int brc_warp_affine(brc_ctx* ctx, const float* d_src, int W, int H, int D, int batch,
+                    const float* d_params, float* d_out) {
+  BRC_CHECK_CTX(ctx);
+  if (!d_src || !d_params || !d_out || bad_dims(W, H, D) || batch <= 0 || batch > 65535)
+    return ctx->fail(BRC_ERR_INVALID, "brc_warp_affine: bad pointer or size");
+  if (d_src == d_out) return ctx->fail(BRC_ERR_INVALID, "brc_warp_affine: in-place warp not supported");
+  cudaSetDevice(ctx->device);
+  const long long V = (long long)W * H * D;
+  BRC_TRY(ctx, brc::warp_affine(d_src, V, W, H, D, batch, d_params, d_out, V, nullptr, 0, ctx->stream()),
+          "warp_affine");
+  ctx->launches += 1;
+  return BRC_OK;
+}
+
+int brc_warp_field(brc_ctx* ctx, const float* d_src, int W, int H, int D, const float* d_dx,
+                   const float* d_dy, const float* d_dz, float* d_out) {
+  BRC_CHECK_CTX(ctx);
+  if (!d_src || !d_dx || !d_dy || !d_dz || !d_out || bad_dims(W, H, D) || d_src == d_out)
+    return ctx->fail(BRC_ERR_INVALID, "brc_warp_field: bad pointer or size");
+  cudaSetDevice(ctx->device);
+  BRC_TRY(ctx, brc::warp_field(d_src, W, H, D, d_dx, d_dy, d_dz, d_out, ctx->stream()), "warp_field");
+  ctx->launches += 1;
+  return BRC_OK;
+}
+
+int brc_rescale_linear(brc_ctx* ctx, const float* d_src, int W, int H, int D, float* d_out, int W2,
+                       int H2, int D2) {
+  BRC_CHECK_CTX(ctx);
+  if (!d_src || !d_out || bad_dims(W, H, D) || bad_dims(W2, H2, D2) || W2 < 2 || H2 < 2 || D2 < 2)
+    return ctx->fail(BRC_ERR_INVALID, "brc_rescale_linear: bad pointer or size");
+  cudaSetDevice(ctx->device);
+  BRC_TRY(ctx, brc::rescale_linear(d_src, W, H, D, d_out, W2, H2, D2, ctx->stream()), "rescale");
+  ctx->launches += 1;
+  return BRC_OK;
+}
+
+int brc_smooth3d(brc_ctx* ctx, const float* d_vol, int W, int H, int D, int batch, const float* h_fx,
+                 const float* h_fy, const float* h_fz, const float* d_cert, const float* d_scert,
+                 float* d_out) {
+  BRC_CHECK_CTX(ctx);
+  if (!d_vol || !d_out || !h_fx || !h_fy || !h_fz || bad_dims(W, H, D) || batch <= 0 || batch > 65535)
+    return ctx->fail(BRC_ERR_INVALID, "brc_smooth3d: bad pointer or size");
+  cudaSetDevice(ctx->device);
+  const size_t bytes = sizeof(float) * (size_t)W * H * D * batch;
+  BRC_TRY(ctx, ctx->tmp1.ensure(bytes), "alloc");
+  BRC_TRY(ctx, ctx->tmp2.ensure(bytes), "alloc");
+  BRC_TRY(ctx, brc::smooth3d(d_vol, W, H, D, batch, h_fx, h_fy, h_fz, d_cert, d_scert,
+                             ctx->tmp1.as<float>(), ctx->tmp2.as<float>(), d_out, ctx->stream()),
+          "smooth3d");
+  ctx->launches += 3;
+  return BRC_OK;
+}
+
+void brc_linear_opts_default(brc_linear_opts* o, int iterations) {
+  if (!o) return;
+  o->iterations = iterations;
+  o->type = BRC_AFFINE;
+  o->precision = BRC_PREC_FP32;
+  o->tolerance = 0.f;
+  o->use_graph = 1;
+  o->certainty_sigma_x100 = 0;
+}
+
+}  // extern "C"
+
+namespace {
+
+struct RegPlan {
+  const float* ref;
+  long long ref_stride;
+  const float* moving;
+  int W, H, D, batch;
+  const float* filters;
+  brc_linear_opts opts;
+  float* params;
+  float* aligned;
+  float* rotations;
+  int* iterations;
+  // workspace
+  float* q1;
+  float* q2;
+  double* partials;
+  int* conv_iter;
+  int* iters_ws;
+  int* status;
+  int nblk, zpb;
+};
+
+// Queues the whole registration on stream st; returns the number of
+// kernels launched or a negative brc_status.
+long long enqueue_registration(brc_ctx* ctx, const RegPlan& p, cudaStream_t st) {
+  const long long V = (long long)p.W * p.H * p.D;
+  const int ref_batch = p.ref_stride ? p.batch : 1;
+  long long kernels = 0;
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(p.params, 0, sizeof(float) * 12 * p.batch, st)) != cudaSuccess)
+    return ctx->cuda(e, "memset params");
+  if ((e = cudaMemsetAsync(p.conv_iter, 0x7f, sizeof(int) * p.batch, st)) != cudaSuccess)
+    return ctx->cuda(e, "memset ctl");
+  if ((e = cudaMemsetAsync(p.iters_ws, 0, sizeof(int) * p.batch, st)) != cudaSuccess)
+    return ctx->cuda(e, "memset ctl");
+  if ((e = cudaMemsetAsync(p.status, 0, sizeof(int), st)) != cudaSuccess) return ctx->cuda(e, "memset");
+  if (p.rotations && (e = cudaMemsetAsync(p.rotations, 0, sizeof(float) * 3 * p.batch, st)) != cudaSuccess)
+    return ctx->cuda(e, "memset rot");
+  if ((e = brc::filter3d_fp32(p.ref, p.W, p.H, p.D, ref_batch, p.ref_stride ? p.ref_stride : V,
+                              p.filters, 3, p.q1, nullptr, 0, st)) != cudaSuccess)
+    return ctx->cuda(e, "filter3d(ref)");
+  kernels++;
+  if (p.opts.iterations == 0 &&
+      (e = cudaMemcpyAsync(p.aligned, p.moving, sizeof(float) * V * p.batch, cudaMemcpyDeviceToDevice,
+                           st)) != cudaSuccess)
+    return ctx->cuda(e, "copy");
+  for (int it = 0; it < p.opts.iterations; it++) {
+    const float* cur = it == 0 ? p.moving : p.aligned;
+    if ((e = brc::filter3d_fp32(cur, p.W, p.H, p.D, p.batch, V, p.filters, 3, p.q2, p.conv_iter, it,
+                                st)) != cudaSuccess)
+      return ctx->cuda(e, "filter3d");
+    if ((e = brc::normal_eq_partials(p.q1, p.ref_stride ? 6 * V : 0, p.q2, p.W, p.H, p.D, p.batch,
+                                     p.partials, p.nblk, p.zpb, p.conv_iter, it, st)) != cudaSuccess)
+      return ctx->cuda(e, "normal_eq");
+    if ((e = brc::solve_update(p.partials, p.nblk, p.batch, p.opts.type, p.opts.tolerance, p.W, p.H,
+                               p.D, p.params, p.rotations, p.conv_iter, p.iters_ws, p.status, it,
+                               st)) != cudaSuccess)
+      return ctx->cuda(e, "solve");
+    if ((e = brc::warp_affine(p.moving, V, p.W, p.H, p.D, p.batch, p.params, p.aligned, V,
+                              p.conv_iter, it, st)) != cudaSuccess)
+      return ctx->cuda(e, "warp");
+    kernels += 4;
+  }
+  if (p.iterations &&
+      (e = cudaMemcpyAsync(p.iterations, p.iters_ws, sizeof(int) * p.batch, cudaMemcpyDeviceToDevice,
+                           st)) != cudaSuccess)
+    return ctx->cuda(e, "copy iterations");
+  return kernels;
+}
+
+}  // namespace
+
+extern "C" int brc_register_linear_batched(brc_ctx* ctx, const float* d_ref, long long ref_stride,
+                                           const float* d_moving, int W, int H, int D, int batch,
+                                           const float* h_filters, const brc_linear_opts* opts,
+                                           float* d_params, float* d_aligned, float* d_rotations,
+                                           int* d_iterations) {
+  BRC_CHECK_CTX(ctx);
+  if (!d_ref || !d_moving || !h_filters || !opts || !d_params || bad_dims(W, H, D) || batch <= 0 ||
+      batch > 65535)
+    return ctx->fail(BRC_ERR_INVALID, "brc_register_linear_batched: bad pointer or size");
+  if (opts->iterations < 0 || opts->iterations > 10000 || opts->type < 0 || opts->type > 2 ||
+      !(opts->tolerance >= 0.f))
+    return ctx->fail(BRC_ERR_INVALID, "brc_register_linear_batched: bad options");
+  if (opts->precision != BRC_PREC_FP32)
+    return ctx->fail(BRC_ERR_UNSUPPORTED, "brc_register_linear_batched: precision not available");
+  if (opts->certainty_sigma_x100 != 0)
+    return ctx->fail(BRC_ERR_UNSUPPORTED, "brc_register_linear_batched: certainty smoothing not available");
+  const long long V = (long long)W * H * D;
+  if (ref_stride != 0 && ref_stride < V)
+    return ctx->fail(BRC_ERR_INVALID, "brc_register_linear_batched: ref_stride smaller than a volume");
+  cudaSetDevice(ctx->device);
+
+  RegPlan p;
+  p.ref = d_ref;
+  p.ref_stride = ref_stride;
+  p.moving = d_moving;
+  p.W = W;
+  p.H = H;
+  p.D = D;
+  p.batch = batch;
+  p.filters = h_filters;
+  p.opts = *opts;
+  p.params = d_params;
+  p.rotations = d_rotations;
+  p.iterations = d_iterations;
+  p.zpb = pick_zpb(W, H);
+  const int nint = D - 6 > 0 ? D - 6 : 1;
+  p.nblk = (nint + p.zpb - 1) / p.zpb;
+
+  const size_t q1n = sizeof(float) * 6 * V * (ref_stride ? batch : 1);
+  const size_t q2n = sizeof(float) * 6 * V * batch;
+  BRC_TRY(ctx, ctx->q1.ensure(q1n), "alloc q1");
+  BRC_TRY(ctx, ctx->q2.ensure(q2n), "alloc q2");
+  BRC_TRY(ctx, ctx->partials.ensure(sizeof(double) * brc::kNSums * p.nblk * (size_t)batch), "alloc");
+  BRC_TRY(ctx, ctx->ctl.ensure(sizeof(int) * (2 * (size_t)batch + 4)), "alloc ctl");
+  if (!d_aligned) BRC_TRY(ctx, ctx->aligned.ensure(sizeof(float) * V * batch), "alloc aligned");
+  p.aligned = d_aligned ? d_aligned : ctx->aligned.as<float>();
+  p.q1 = ctx->q1.as<float>();
+  p.q2 = ctx->q2.as<float>();
+  p.partials = ctx->partials.as<double>();
+  p.conv_iter = ctx->ctl.as<int>();
+  p.iters_ws = p.conv_iter + batch;
+  p.status = p.iters_ws + batch;
+
+  const cudaStream_t user = ctx->stream();
+  if (!opts->use_graph) {
+    long long k = enqueue_registration(ctx, p, user);
+    if (k < 0) return (int)k;
+    ctx->launches += k;
+  } else {
+    GraphKey key;
+    const uint64_t fh = fnv1a(h_filters, sizeof(float) * 3 * brc::kFilterFloats);
+    key.v = {(uint64_t)d_ref, (uint64_t)ref_stride, (uint64_t)d_moving, (uint64_t)W, (uint64_t)H,
+             (uint64_t)D, (uint64_t)batch, fh, (uint64_t)opts->iterations, (uint64_t)opts->type,
+             (uint64_t)fnv1a(&opts->tolerance, sizeof(float)), (uint64_t)d_params,
+             (uint64_t)p.aligned, (uint64_t)d_rotations, (uint64_t)d_iterations,
+             (uint64_t)ctx->q1.ptr, (uint64_t)ctx->q2.ptr, (uint64_t)ctx->partials.ptr,
+             (uint64_t)ctx->ctl.ptr};
+    auto itg = ctx->graphs.find(key);
+    GraphEntry* ge = nullptr;
+    if (itg == ctx->graphs.end()) {
+      if (ctx->graphs.size() >= 16) ctx->graphs.clear();
+      std::unique_ptr<GraphEntry> ne(new GraphEntry());
+      cudaStream_t cs = ctx->own_stream;
+      BRC_TRY(ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "begin capture");
+      long long k = enqueue_registration(ctx, p, cs);
+      cudaGraph_t g = nullptr;
+      cudaError_t ee = cudaStreamEndCapture(cs, &g);
+      if (k < 0) {
+        if (g) cudaGraphDestroy(g);
+        return (int)k;
+      }
+      BRC_TRY(ctx, ee, "end capture");
+      ne->graph = g;
+      BRC_TRY(ctx, cudaGraphInstantiate(&ne->exec, g, 0), "instantiate");
+      ne->kernels = (unsigned long long)k;
+      ge = ne.get();
+      ctx->graphs[key] = std::move(ne);
+    } else {
+      ge = itg->second.get();
+    }
+    // Order the replay on the caller's stream: own stream waits for the
+    // caller, the caller waits for the replay.
+    if (user != ctx->own_stream) {
+      BRC_TRY(ctx, cudaEventRecord(ctx->ev_in, user), "event");
+      BRC_TRY(ctx, cudaStreamWaitEvent(ctx->own_stream, ctx->ev_in, 0), "wait");
+    }
+    BRC_TRY(ctx, cudaGraphLaunch(ge->exec, ctx->own_stream), "graph launch");
+    if (user != ctx->own_stream) {
+      BRC_TRY(ctx, cudaEventRecord(ctx->ev_out, ctx->own_stream), "event");
+      BRC_TRY(ctx, cudaStreamWaitEvent(user, ctx->ev_out, 0), "wait");
+    }
+    ctx->launches += ge->kernels;
+  }
+  return BRC_OK;
+}
+
+extern "C" int brc_motion_correct(brc_ctx* ctx, float* h_volumes, int W, int H, int D, int T,
+                                  const float* voxel_size3, const float* h_filters,
+                                  const brc_linear_opts* opts, const float* h_reference,
+                                  float* h_motion) {
+  BRC_CHECK_CTX(ctx);
+  if (!h_volumes || !h_filters || !opts || bad_dims(W, H, D) || T <= 0)
+    return ctx->fail(BRC_ERR_INVALID, "brc_motion_correct: bad pointer or size");
+  const long long V = (long long)W * H * D;
+  const int first = h_reference ? 0 : 1;
+  const int batch = T - first;
+  float vs[3] = {1.f, 1.f, 1.f};
+  if (voxel_size3) memcpy(vs, voxel_size3, sizeof(vs));
+  if (h_motion)
+    for (int k = 0; k < 6; k++) h_motion[k * T] = 0.f;
+  if (batch <= 0) return BRC_OK;
+  cudaSetDevice(ctx->device);
+  const cudaStream_t st = ctx->stream();
+  BRC_TRY(ctx, ctx->series.ensure(sizeof(float) * V * (T + 1)), "alloc series");
+  BRC_TRY(ctx, ctx->corrected.ensure(sizeof(float) * V * batch), "alloc corrected");
+  BRC_TRY(ctx, ctx->params.ensure(sizeof(float) * 12 * batch), "alloc params");
+  BRC_TRY(ctx, ctx->rot.ensure(sizeof(float) * 3 * batch), "alloc rot");
+  float* d_series = ctx->series.as<float>();
+  BRC_TRY(ctx, cudaMemcpyAsync(d_series, h_volumes, sizeof(float) * V * T, cudaMemcpyHostToDevice, st), "H2D");
+  const float* d_ref = d_series;
+  if (h_reference) {
+    BRC_TRY(ctx, cudaMemcpyAsync(d_series + V * T, h_reference, sizeof(float) * V, cudaMemcpyHostToDevice, st), "H2D");
+    d_ref = d_series + V * T;
+  }
+  brc_linear_opts o = *opts;
+  o.type = BRC_RIGID;
+  int s = brc_register_linear_batched(ctx, d_ref, 0, d_series + V * first, W, H, D, batch, h_filters, &o,
+                                      ctx->params.as<float>(), ctx->corrected.as<float>(),
+                                      ctx->rot.as<float>(), nullptr);
+  if (s != BRC_OK) return s;
+  BRC_TRY(ctx, cudaMemcpyAsync(h_volumes + V * first, ctx->corrected.as<float>(), sizeof(float) * V * batch,
+                               cudaMemcpyDeviceToHost, st), "D2H");
+  std::vector<float> prm(12 * (size_t)batch), rot(3 * (size_t)batch);
+  BRC_TRY(ctx, cudaMemcpyAsync(prm.data(), ctx->params.as<float>(), sizeof(float) * 12 * batch,
+                               cudaMemcpyDeviceToHost, st), "D2H");
+  BRC_TRY(ctx, cudaMemcpyAsync(rot.data(), ctx->rot.as<float>(), sizeof(float) * 3 * batch,
+                               cudaMemcpyDeviceToHost, st), "D2H");
+  BRC_TRY(ctx, cudaStreamSynchronize(st), "synchronize");
+  if (h_motion) {
+    for (int i = 0; i < batch; i++) {
+      const int t = first + i;
+      h_motion[t + 0 * T] = prm[12 * i + 0] * vs[0];
+      h_motion[t + 1 * T] = prm[12 * i + 1] * vs[1];
+      h_motion[t + 2 * T] = prm[12 * i + 2] * vs[2];
+      h_motion[t + 3 * T] = rot[3 * i + 0];
+      h_motion[t + 4 * T] = rot[3 * i + 1];
+      h_motion[t + 5 * T] = rot[3 * i + 2];
+    }
+  }
+  return BRC_OK;
+}

@@ -1,0 +1,88 @@
+// capi_ctx.h -- the library context (struct brc_ctx) and the workspace and
+// error helpers shared by the C-ABI translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/broccoli_b200.h"
+
+// Grow-only device buffer.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  ~DevBuf() {
+    if (ptr) cudaFree(ptr);
+  }
+  cudaError_t ensure(size_t n) {
+    if (n <= bytes) return cudaSuccess;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMalloc(&ptr, n);
+    if (e == cudaSuccess) bytes = n;
+    return e;
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(ptr);
+  }
+};
+
+struct GraphKey {
+  std::vector<unsigned long long> v;
+  bool operator<(const GraphKey& o) const { return v < o.v; }
+};
+
+struct GraphEntry {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  unsigned long long kernels = 0;
+  ~GraphEntry() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+  }
+};
+
+struct brc_ctx {
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t user_stream = nullptr;
+  bool use_user_stream = false;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  std::string last_error;
+  unsigned long long launches = 0;
+  DevBuf q1, q2, aligned, partials, ctl, tmp1, tmp2, series, corrected, params, rot, nl, pyr;
+  std::map<GraphKey, std::unique_ptr<GraphEntry>> graphs;
+
+  cudaStream_t stream() const { return use_user_stream ? user_stream : own_stream; }
+
+  int fail(int status, const std::string& msg) {
+    last_error = msg;
+    return status;
+  }
+  int cuda(cudaError_t e, const char* where) {
+    if (e == cudaSuccess) return BRC_OK;
+    last_error = std::string(where) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? BRC_ERR_NOMEM : BRC_ERR_CUDA;
+  }
+  size_t workspace() const {
+    return q1.bytes + q2.bytes + aligned.bytes + partials.bytes + ctl.bytes + tmp1.bytes +
+           tmp2.bytes + series.bytes + corrected.bytes + params.bytes + rot.bytes + nl.bytes + pyr.bytes;
+  }
+};
+
+#define BRC_CHECK_CTX(ctx) \
+  do {                     \
+    if (!(ctx)) return BRC_ERR_INVALID; \
+  } while (0)
+
+#define BRC_TRY(ctx, expr, where)                  \
+  do {                                             \
+    int _s = (ctx)->cuda((expr), (where));         \
+    if (_s != BRC_OK) return _s;                   \
+  } while (0)
+

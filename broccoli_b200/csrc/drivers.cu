@@ -1,0 +1,263 @@
+// drivers.cu -- multi-step entry points of the C-ABI: one nonlinear update
+// step, single- and multi-scale nonlinear registration, and multi-scale
+// (pyramid) linear registration.  Host code: it sequences the kernels of
+// filter3d.cu / registration.cu / nonlinear.cu on the context's stream;
+// nothing here synchronises with the host except where stated.
+#include <math.h>
+#include <string.h>
+
+#include <string>
+
+#include "../../include/broccoli_b200.h"
+#include "capi_ctx.h"
+#include "common.cuh"
+#include "internal.h"
+
+namespace {
+
+// Gaussian smoothing filter of 9 taps for a sigma in voxels, normalised by
+// its float sum (CreateSmoothingFilters(..., double sigma),
+// broccoli_lib.cpp:11093-11121).
+void smoothing_taps(double sigma, float* f) {
+  const double s2 = 2.0 * sigma * sigma;
+  float sum = 0.0f;
+  for (int i = 0; i < 9; i++) {
+    const double u = (double)(i - 4);
+    f[i] = (float)exp(-pow(u, 2.0) / s2);
+    sum += f[i];
+  }
+  for (int i = 0; i < 9; i++) f[i] /= sum;
+}
+
+int myround(float a) { return (int)floorf(a + 0.5f); }
+
+}  // namespace
+
+// One nonlinear update from given responses: T, its smoothing, norm and
+// max, A and h, their smoothing, the per-voxel solve, the smoothing of the
+// update and its addition into the field (AlignTwoVolumesNonLinear loop
+// body, broccoli_lib.cpp:5784-6025).
+static int nonlinear_step(brc_ctx* ctx, const float* q1, const float* q2, int W, int H, int D,
+                          const float* m36, const float* dirs18, const float* ft, const float* fe,
+                          const float* fd, int fp64, float* field) {
+  const long long V = (long long)W * H * D;
+  cudaStream_t st = ctx->stream();
+  float* t6 = ctx->nl.as<float>();
+  float* ah = t6 + 6 * V;  // a6 then h3, contiguous (9 volumes)
+  float* d3 = ah + 9 * V;
+  unsigned int* maxbits = reinterpret_cast<unsigned int*>(d3 + 3 * V);
+  BRC_TRY(ctx, brc::tensor_components(q2, V, m36, t6, st), "tensor_components");
+  BRC_TRY(ctx, brc::smooth3d(t6, W, H, D, 6, ft, ft, ft, nullptr, nullptr, ctx->tmp1.as<float>(),
+                             ctx->tmp2.as<float>(), t6, st),
+          "smooth T");
+  BRC_TRY(ctx, brc::tensor_norm_max(t6, V, ah, maxbits, st), "tensor_norm_max");
+  BRC_TRY(ctx, brc::nonlinear_ah(q1, q2, t6, V, maxbits, m36, dirs18, ah, ah + 6 * V, st), "nonlinear_ah");
+  BRC_TRY(ctx, brc::smooth3d(ah, W, H, D, 9, fe, fe, fe, nullptr, nullptr, ctx->tmp1.as<float>(),
+                             ctx->tmp2.as<float>(), ah, st),
+          "smooth A,h");
+  BRC_TRY(ctx, brc::displacement_update(ah, ah + 6 * V, V, fp64, d3, st), "displacement_update");
+  BRC_TRY(ctx, brc::smooth3d(d3, W, H, D, 3, fd, fd, fd, nullptr, nullptr, ctx->tmp1.as<float>(),
+                             ctx->tmp2.as<float>(), field, st, 1),
+          "smooth update");
+  ctx->launches += 1 + 3 + 1 + 1 + 3 + 1 + 3;
+  return BRC_OK;
+}
+
+static int ensure_nonlinear_ws(brc_ctx* ctx, long long V) {
+  BRC_TRY(ctx, ctx->nl.ensure(sizeof(float) * (18 * V + 64)), "alloc nonlinear");
+  BRC_TRY(ctx, ctx->tmp1.ensure(sizeof(float) * 9 * V), "alloc tmp");
+  BRC_TRY(ctx, ctx->tmp2.ensure(sizeof(float) * 9 * V), "alloc tmp");
+  return BRC_OK;
+}
+
+extern "C" void brc_nonlinear_opts_default(brc_nonlinear_opts* o, int iterations) {
+  if (!o) return;
+  o->iterations = iterations;
+  o->coarsest_scale = 1;
+  o->tsigma = 5.0f;
+  o->esigma = 5.0f;
+  o->dsigma = 5.0f;
+  o->precision = BRC_PREC_FP32;
+  o->solve_fp64 = 0;
+}
+
+extern "C" int brc_nonlinear_step(brc_ctx* ctx, const float* d_q1, const float* d_q2, int W, int H,
+                                  int D, const float* h_tensors, const float* h_dirs, float tsigma,
+                                  float esigma, float dsigma, int solve_fp64, float* d_field) {
+  if (!ctx) return BRC_ERR_INVALID;
+  if (!d_q1 || !d_q2 || !h_tensors || !h_dirs || !d_field || W <= 0 || H <= 0 || D <= 0 ||
+      !(tsigma > 0) || !(esigma > 0) || !(dsigma > 0))
+    return ctx->fail(BRC_ERR_INVALID, "brc_nonlinear_step: bad argument");
+  cudaSetDevice(ctx->device);
+  const long long V = (long long)W * H * D;
+  int s = ensure_nonlinear_ws(ctx, V);
+  if (s != BRC_OK) return s;
+  float ft[9], fe[9], fd[9];
+  smoothing_taps(tsigma, ft);
+  smoothing_taps(esigma, fe);
+  smoothing_taps(dsigma, fd);
+  return nonlinear_step(ctx, d_q1, d_q2, W, H, D, h_tensors, h_dirs, ft, fe, fd, solve_fp64, d_field);
+}
+
+// One scale of nonlinear registration: `aligned` (in: start volume, out:
+// last warp) and `original` (the volume the field warps) at size W,H,D;
+// `field` receives this scale's total update (zeroed first).
+static int nonlinear_scale(brc_ctx* ctx, const float* ref, float* aligned, const float* original, int W,
+                           int H, int D, const float* filters6, const float* m36, const float* dirs18,
+                           int iterations, const brc_nonlinear_opts* o, float* field) {
+  const long long V = (long long)W * H * D;
+  cudaStream_t st = ctx->stream();
+  int s = ensure_nonlinear_ws(ctx, V);
+  if (s != BRC_OK) return s;
+  BRC_TRY(ctx, ctx->q1.ensure(sizeof(float) * 12 * V), "alloc q1");
+  BRC_TRY(ctx, ctx->q2.ensure(sizeof(float) * 12 * V), "alloc q2");
+  float* q1 = ctx->q1.as<float>();
+  float* q2 = ctx->q2.as<float>();
+  float ft[9], fe[9], fd[9];
+  smoothing_taps(o->tsigma, ft);
+  smoothing_taps(o->esigma, fe);
+  smoothing_taps(o->dsigma, fd);
+  BRC_TRY(ctx, brc::filter3d_fp32(ref, W, H, D, 1, V, filters6, 6, q1, nullptr, 0, st), "filter ref");
+  ctx->launches += 1;
+  BRC_TRY(ctx, cudaMemsetAsync(field, 0, sizeof(float) * 3 * V, st), "memset field");
+  for (int it = 0; it < iterations; it++) {
+    BRC_TRY(ctx, brc::filter3d_fp32(aligned, W, H, D, 1, V, filters6, 6, q2, nullptr, 0, st), "filter");
+    ctx->launches += 1;
+    s = nonlinear_step(ctx, q1, q2, W, H, D, m36, dirs18, ft, fe, fd, o->solve_fp64, field);
+    if (s != BRC_OK) return s;
+    BRC_TRY(ctx, brc::warp_field(original, W, H, D, field, field + V, field + 2 * V, aligned, st), "warp");
+    ctx->launches += 1;
+  }
+  return BRC_OK;
+}
+
+extern "C" int brc_register_nonlinear(brc_ctx* ctx, const float* d_ref, const float* d_moving, int W,
+                                      int H, int D, const float* h_filters6, const float* h_tensors,
+                                      const float* h_dirs, const brc_nonlinear_opts* o, float* d_field,
+                                      float* d_aligned) {
+  if (!ctx) return BRC_ERR_INVALID;
+  if (!d_ref || !d_moving || !h_filters6 || !h_tensors || !h_dirs || !o || !d_field || !d_aligned ||
+      W <= 0 || H <= 0 || D <= 0 || o->iterations < 0 || o->coarsest_scale < 1 ||
+      !(o->tsigma > 0) || !(o->esigma > 0) || !(o->dsigma > 0))
+    return ctx->fail(BRC_ERR_INVALID, "brc_register_nonlinear: bad argument");
+  if (o->precision != BRC_PREC_FP32)
+    return ctx->fail(BRC_ERR_UNSUPPORTED, "brc_register_nonlinear: precision not available");
+  if (d_aligned == d_moving)
+    return ctx->fail(BRC_ERR_INVALID, "brc_register_nonlinear: d_aligned must not alias d_moving");
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream();
+  const long long V = (long long)W * H * D;
+  // scale buffers: ref, original, aligned at the scale, two field sets
+  BRC_TRY(ctx, ctx->pyr.ensure(sizeof(float) * 10 * V), "alloc pyramid");
+  float* r_s = ctx->pyr.as<float>();
+  float* o_s = r_s + V;
+  float* a_s = o_s + V;
+  float* tot = a_s + V;       // 3V
+  float* upd = tot + 3 * V;   // 3V
+  int cw = myround((float)W / (float)o->coarsest_scale);
+  int ch = myround((float)H / (float)o->coarsest_scale);
+  int cd = myround((float)D / (float)o->coarsest_scale);
+  if (cw < 2 || ch < 2 || cd < 2)
+    return ctx->fail(BRC_ERR_INVALID, "brc_register_nonlinear: coarsest scale leaves fewer than 2 voxels");
+  if (o->coarsest_scale == 1) {
+    BRC_TRY(ctx, cudaMemcpyAsync(o_s, d_moving, sizeof(float) * V, cudaMemcpyDeviceToDevice, st), "copy");
+    BRC_TRY(ctx, cudaMemcpyAsync(r_s, d_ref, sizeof(float) * V, cudaMemcpyDeviceToDevice, st), "copy");
+  } else {
+    BRC_TRY(ctx, brc::rescale_batch(d_moving, W, H, D, 1, o_s, cw, ch, cd, 1.0f, st), "rescale");
+    BRC_TRY(ctx, brc::rescale_batch(d_ref, W, H, D, 1, r_s, cw, ch, cd, 1.0f, st), "rescale");
+    ctx->launches += 2;
+  }
+  BRC_TRY(ctx, cudaMemsetAsync(tot, 0, sizeof(float) * 3 * (long long)cw * ch * cd, st), "memset");
+  for (int scale = o->coarsest_scale; scale >= 1; scale /= 2) {
+    const long long vs = (long long)cw * ch * cd;
+    BRC_TRY(ctx, cudaMemcpyAsync(a_s, o_s, sizeof(float) * vs, cudaMemcpyDeviceToDevice, st), "copy");
+    const int iters = scale == 1 ? (int)ceilf((float)o->iterations / 2.0f) : o->iterations;
+    int s = nonlinear_scale(ctx, r_s, a_s, o_s, cw, ch, cd, h_filters6, h_tensors, h_dirs, iters, o, upd);
+    if (s != BRC_OK) return s;
+    BRC_TRY(ctx, brc::add_volumes(tot, tot, upd, 3 * vs, st), "add");
+    ctx->launches += 1;
+    if (scale != 1) {
+      const int pw = cw, ph = ch, pd = cd;
+      cw = myround((float)W / ((float)scale / 2.0f));
+      ch = myround((float)H / ((float)scale / 2.0f));
+      cd = myround((float)D / ((float)scale / 2.0f));
+      const long long nv = (long long)cw * ch * cd;
+      // field to the finer grid, doubled (voxel units), via the upd buffer
+      BRC_TRY(ctx, brc::rescale_batch(tot, pw, ph, pd, 3, upd, cw, ch, cd, 2.0f, st), "rescale field");
+      BRC_TRY(ctx, cudaMemcpyAsync(tot, upd, sizeof(float) * 3 * nv, cudaMemcpyDeviceToDevice, st), "copy");
+      BRC_TRY(ctx, brc::rescale_batch(d_ref, W, H, D, 1, r_s, cw, ch, cd, 1.0f, st), "rescale");
+      BRC_TRY(ctx, brc::rescale_batch(d_moving, W, H, D, 1, a_s, cw, ch, cd, 1.0f, st), "rescale");
+      BRC_TRY(ctx, brc::warp_field(a_s, cw, ch, cd, tot, tot + nv, tot + 2 * nv, o_s, st), "warp");
+      ctx->launches += 4;
+    } else {
+      BRC_TRY(ctx, cudaMemcpyAsync(d_field, tot, sizeof(float) * 3 * V, cudaMemcpyDeviceToDevice, st), "copy");
+      BRC_TRY(ctx, brc::warp_field(d_moving, W, H, D, d_field, d_field + V, d_field + 2 * V, d_aligned, st),
+              "warp");
+      ctx->launches += 1;
+    }
+  }
+  return BRC_OK;
+}
+
+extern "C" int brc_register_linear_scales(brc_ctx* ctx, const float* d_ref, const float* d_moving, int W,
+                                          int H, int D, int batch, const float* h_filters,
+                                          const brc_linear_opts* opts, int coarsest_scale,
+                                          float* d_params, float* d_aligned, float* d_rotations) {
+  if (!ctx) return BRC_ERR_INVALID;
+  if (!d_ref || !d_moving || !h_filters || !opts || !d_params || !d_aligned || W <= 0 || H <= 0 ||
+      D <= 0 || batch <= 0 || batch > 65535 || coarsest_scale < 1)
+    return ctx->fail(BRC_ERR_INVALID, "brc_register_linear_scales: bad argument");
+  if (d_aligned == d_moving)
+    return ctx->fail(BRC_ERR_INVALID, "brc_register_linear_scales: d_aligned must not alias d_moving");
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream();
+  const long long V = (long long)W * H * D;
+  int cw = myround((float)W / (float)coarsest_scale);
+  int ch = myround((float)H / (float)coarsest_scale);
+  int cd = myround((float)D / (float)coarsest_scale);
+  if (cw < 2 || ch < 2 || cd < 2)
+    return ctx->fail(BRC_ERR_INVALID, "brc_register_linear_scales: coarsest scale leaves fewer than 2 voxels");
+  // per scale: ref (1), resampled moving (B), pre-warped moving (B), scale
+  // result (B), scale params (12B) and rotations (3B)
+  BRC_TRY(ctx, ctx->pyr.ensure(sizeof(float) * ((1 + 3 * (size_t)batch) * V + 15 * (size_t)batch)), "alloc");
+  float* r_s = ctx->pyr.as<float>();
+  float* m_s = r_s + V;
+  float* o_s = m_s + V * batch;
+  float* a_s = o_s + V * batch;
+  float* tmp = a_s + V * batch;
+  float* rt = tmp + 12 * batch;
+  BRC_TRY(ctx, cudaMemsetAsync(d_params, 0, sizeof(float) * 12 * batch, st), "memset");
+  if (d_rotations) BRC_TRY(ctx, cudaMemsetAsync(d_rotations, 0, sizeof(float) * 3 * batch, st), "memset");
+  brc_linear_opts so = *opts;
+  so.use_graph = 0;
+  for (int scale = coarsest_scale; scale >= 1; scale /= 2) {
+    const long long vs = (long long)cw * ch * cd;
+    BRC_TRY(ctx, brc::rescale_batch(d_ref, W, H, D, 1, r_s, cw, ch, cd, 1.0f, st), "rescale");
+    if (scale == coarsest_scale) {
+      BRC_TRY(ctx, brc::rescale_batch(d_moving, W, H, D, batch, o_s, cw, ch, cd, 1.0f, st), "rescale");
+    } else {
+      BRC_TRY(ctx, brc::rescale_batch(d_moving, W, H, D, batch, m_s, cw, ch, cd, 1.0f, st), "rescale");
+      BRC_TRY(ctx, brc::warp_affine(m_s, vs, cw, ch, cd, batch, d_params, o_s, vs, nullptr, 0, st), "prewarp");
+      ctx->launches += 1;
+    }
+    ctx->launches += 2;
+    so.iterations = scale == 1 ? (int)ceilf((float)opts->iterations / 5.0f) : opts->iterations;
+    int s = brc_register_linear_batched(ctx, r_s, 0, o_s, cw, ch, cd, batch, h_filters, &so, tmp, a_s,
+                                        rt, nullptr);
+    if (s != BRC_OK) return s;
+    BRC_TRY(ctx, brc::compose(d_params, tmp, batch, scale == 1 ? 1.0f : 2.0f, st), "compose");
+    ctx->launches += 1;
+    if (d_rotations && so.type == BRC_RIGID) {
+      BRC_TRY(ctx, brc::add_volumes(d_rotations, d_rotations, rt, 3 * batch, st), "rotations");
+      ctx->launches += 1;
+    }
+    if (scale != 1) {
+      cw = myround((float)W / ((float)scale / 2.0f));
+      ch = myround((float)H / ((float)scale / 2.0f));
+      cd = myround((float)D / ((float)scale / 2.0f));
+    }
+  }
+  BRC_TRY(ctx, brc::warp_affine(d_moving, V, W, H, D, batch, d_params, d_aligned, V, nullptr, 0, st), "warp");
+  ctx->launches += 1;
+  return BRC_OK;
+}

@@ -1,0 +1,214 @@
+// filter3d.cu -- 7x7x7 complex quadrature filtering, FP32 on the CUDA cores.
+//
+// One CTA computes a 32 (x) x 8 (y) x TZ (z) block of outputs for all NF
+// complex filters of one volume of the batch.  The input block with its
+// +-3 halo is staged in shared memory once (zero padding outside the
+// volume, rows padded to 44 floats so that the 16-byte row loads of a
+// quarter-warp hit distinct banks); the tap-major filter bank is staged in
+// shared memory from the kernel parameters.  Each thread owns a run of R
+// consecutive x outputs and keeps 2*NF*R accumulators in registers: per
+// (dz,dy) it loads one row segment of R+6 samples with 16-byte loads, then
+// for each of the 7 dx taps it loads the 2*NF coefficients (a broadcast)
+// and issues 2*NF*R FMAs.  FMAs per shared-memory load is ~40, so the
+// kernel is bound by the FP32 pipe.
+//
+// Algorithm (what is computed, not how): NonseparableConvolution3D,
+// broccoli_lib.cpp:4974-5027, with the 2D passes of
+// kernelConvolution.cpp:2802-3693.
+#include "common.cuh"
+
+namespace brc {
+
+constexpr int kTX = 32;   // outputs per CTA along x
+constexpr int kTY = 8;    // outputs per CTA along y
+constexpr int kRowPad = 44;  // shared row length (38 used)
+
+template <int NF, int R, int TZ>
+struct Filter3dCfg {
+  static constexpr int kThreadsX = kTX / R;
+  static constexpr int kThreads = kThreadsX * kTY * TZ;
+  static constexpr int kCP = (2 * NF + 3) / 4 * 4;  // coefficient stride per tap
+  static constexpr int kSlices = TZ + 6;
+  static constexpr int kRows = kTY + 6;
+  static constexpr int kVolFloats = kSlices * kRows * kRowPad;
+  static constexpr int kCoefFloats = kTaps * kCP;
+  static constexpr size_t kSmemBytes = sizeof(float) * (kVolFloats + kCoefFloats);
+};
+
+template <int NF, int R, int TZ>
+__global__ void __launch_bounds__(Filter3dCfg<NF, R, TZ>::kThreads)
+filter3d_fp32_kernel(const float* __restrict__ vol, int W, int H, int D, long long vol_stride,
+                     const __grid_constant__ FilterBank<NF> bank, float* __restrict__ out,
+                     const int* __restrict__ conv_iter, int it) {
+  using Cfg = Filter3dCfg<NF, R, TZ>;
+  extern __shared__ __align__(16) float smem[];
+  float* s_vol = smem;
+  float* s_coef = smem + Cfg::kVolFloats;
+
+  const int b = blockIdx.z;
+  if (instance_done(conv_iter, b, it)) return;
+  const int z_tiles = (D + TZ - 1) / TZ;
+  const int tile_x0 = blockIdx.x * kTX;
+  const int tile_y0 = (blockIdx.y / z_tiles) * kTY;
+  const int tile_z0 = (blockIdx.y % z_tiles) * TZ;
+  const float* src = vol + (long long)b * vol_stride;
+  const long long V = (long long)W * H * D;
+
+  // Stage the coefficients: tap-major, 2*NF values per tap, padded to kCP.
+  for (int i = threadIdx.x; i < kTaps * Cfg::kCP; i += Cfg::kThreads) {
+    const int t = i / Cfg::kCP, c = i % Cfg::kCP;
+    s_coef[i] = c < 2 * NF ? bank.coef[t * 2 * NF + c] : 0.f;
+  }
+  // Stage the input block: x from tile_x0-4 (16-byte aligned in shared
+  // memory), y from tile_y0-3, z from tile_z0-3; zero outside the volume.
+  for (int i = threadIdx.x; i < Cfg::kVolFloats; i += Cfg::kThreads) {
+    const int xs = i % kRowPad;
+    const int ys = (i / kRowPad) % Cfg::kRows;
+    const int zs = i / (kRowPad * Cfg::kRows);
+    const int x = tile_x0 - 4 + xs, y = tile_y0 - 3 + ys, z = tile_z0 - 3 + zs;
+    float v = 0.f;
+    if (x >= 0 && x < W && y >= 0 && y < H && z >= 0 && z < D)
+      v = __ldg(src + x + (long long)y * W + (long long)z * W * H);
+    s_vol[i] = v;
+  }
+  __syncthreads();
+
+  const int tx = threadIdx.x % Cfg::kThreadsX;
+  const int ty = (threadIdx.x / Cfg::kThreadsX) % kTY;
+  const int tz = threadIdx.x / (Cfg::kThreadsX * kTY);
+
+  float acc[2 * NF][R];
+#pragma unroll
+  for (int f = 0; f < 2 * NF; f++)
+#pragma unroll
+    for (int r = 0; r < R; r++) acc[f][r] = 0.f;
+
+  constexpr int kSeg = (R + 8) / 4;  // float4 loads per row segment
+#pragma unroll 1
+  for (int dz = 0; dz < 7; dz++) {
+#pragma unroll
+    for (int dy = 0; dy < 7; dy++) {
+      const float4* row = reinterpret_cast<const float4*>(
+          s_vol + ((tz + dz) * Cfg::kRows + (ty + dy)) * kRowPad + R * tx);
+      float d[4 * kSeg];
+#pragma unroll
+      for (int s = 0; s < kSeg; s++) {
+        const float4 q = row[s];
+        d[4 * s] = q.x;
+        d[4 * s + 1] = q.y;
+        d[4 * s + 2] = q.z;
+        d[4 * s + 3] = q.w;
+      }
+      const float* ct = s_coef + (dz * 49 + dy * 7) * Cfg::kCP;
+#pragma unroll
+      for (int dx = 0; dx < 7; dx++) {
+        float c[Cfg::kCP];
+#pragma unroll
+        for (int s = 0; s < Cfg::kCP / 4; s++) {
+          const float4 q = reinterpret_cast<const float4*>(ct + dx * Cfg::kCP)[s];
+          c[4 * s] = q.x;
+          c[4 * s + 1] = q.y;
+          c[4 * s + 2] = q.z;
+          c[4 * s + 3] = q.w;
+        }
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+          const float px = d[1 + r + dx];
+#pragma unroll
+          for (int f = 0; f < 2 * NF; f++) acc[f][r] = fmaf(px, c[f], acc[f][r]);
+        }
+      }
+    }
+  }
+
+  const int x0 = tile_x0 + R * tx;
+  const int y = tile_y0 + ty;
+  const int z = tile_z0 + tz;
+  if (y >= H || z >= D || x0 >= W) return;
+  const long long idx0 = x0 + (long long)y * W + (long long)z * W * H;
+  float* o = out + (long long)b * NF * 2 * V;
+  const bool full = x0 + R <= W;
+#pragma unroll
+  for (int k = 0; k < NF; k++) {
+    float* ok = o + (long long)k * 2 * V + 2 * idx0;
+    if (full && (reinterpret_cast<uintptr_t>(ok) & 15) == 0) {
+#pragma unroll
+      for (int r = 0; r < R; r += 2)
+        reinterpret_cast<float4*>(ok)[r / 2] =
+            make_float4(acc[2 * k][r], acc[2 * k + 1][r], acc[2 * k][r + 1], acc[2 * k + 1][r + 1]);
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; r++)
+        if (x0 + r < W) {
+          ok[2 * r] = acc[2 * k][r];
+          ok[2 * r + 1] = acc[2 * k + 1][r];
+        }
+    }
+  }
+}
+
+template <int NF>
+static void pack_bank(const float* h_filters, FilterBank<NF>& bank) {
+  for (int t = 0; t < kTaps; t++) {
+    const int dx = t % 7, dy = (t / 7) % 7, dz = t / 49;
+    const int src = (6 - dx) + 7 * (6 - dy) + 49 * (6 - dz);
+    for (int k = 0; k < NF; k++) {
+      bank.coef[t * 2 * NF + 2 * k] = h_filters[k * kFilterFloats + src];
+      bank.coef[t * 2 * NF + 2 * k + 1] = h_filters[k * kFilterFloats + kTaps + src];
+    }
+  }
+}
+
+template <int NF, int R, int TZ>
+static cudaError_t launch_fp32(const float* vol, int W, int H, int D, int batch, long long stride,
+                               const FilterBank<NF>& bank, float* out, const int* conv_iter, int it,
+                               cudaStream_t st) {
+  using Cfg = Filter3dCfg<NF, R, TZ>;
+  const int z_tiles = (D + TZ - 1) / TZ;
+  dim3 grid((W + kTX - 1) / kTX, ((H + kTY - 1) / kTY) * z_tiles, batch);
+  filter3d_fp32_kernel<NF, R, TZ><<<grid, Cfg::kThreads, Cfg::kSmemBytes, st>>>(
+      vol, W, H, D, stride, bank, out, conv_iter, it);
+  return cudaGetLastError();
+}
+
+template <int NF, int R, int TZ>
+static cudaError_t set_smem_attr() {
+  return cudaFuncSetAttribute(filter3d_fp32_kernel<NF, R, TZ>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)Filter3dCfg<NF, R, TZ>::kSmemBytes);
+}
+
+// Raises the dynamic shared-memory limit of every instantiation; called
+// once per device when a context is created.
+cudaError_t filter3d_init() {
+  cudaError_t e;
+  if ((e = set_smem_attr<3, 8, 3>()) != cudaSuccess) return e;
+  if ((e = set_smem_attr<3, 8, 4>()) != cudaSuccess) return e;
+  if ((e = set_smem_attr<6, 4, 3>()) != cudaSuccess) return e;
+  return set_smem_attr<6, 4, 4>();
+}
+
+// Chooses the z depth of the tile: 3 when it divides D exactly and 4 does
+// not (e.g. D = 33), else 4.
+static int pick_tz(int D) { return (D % 4 != 0 && D % 3 == 0) ? 3 : 4; }
+
+cudaError_t filter3d_fp32(const float* vol, int W, int H, int D, int batch, long long stride,
+                          const float* h_filters, int nfilt, float* out, const int* conv_iter,
+                          int it, cudaStream_t st) {
+  const int tz = pick_tz(D);
+  if (nfilt == 3) {
+    FilterBank<3> bank;
+    pack_bank<3>(h_filters, bank);
+    return tz == 3 ? launch_fp32<3, 8, 3>(vol, W, H, D, batch, stride, bank, out, conv_iter, it, st)
+                   : launch_fp32<3, 8, 4>(vol, W, H, D, batch, stride, bank, out, conv_iter, it, st);
+  }
+  if (nfilt == 6) {
+    FilterBank<6> bank;
+    pack_bank<6>(h_filters, bank);
+    return tz == 3 ? launch_fp32<6, 4, 3>(vol, W, H, D, batch, stride, bank, out, conv_iter, it, st)
+                   : launch_fp32<6, 4, 4>(vol, W, H, D, batch, stride, bank, out, conv_iter, it, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace brc

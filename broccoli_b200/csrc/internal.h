@@ -1,0 +1,45 @@
+// internal.h -- host-side launchers of the kernels (namespace brc), shared by
+// the C-ABI (capi.cu) and the multi-step drivers (drivers.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace brc {
+// filter3d.cu
+cudaError_t filter3d_init();
+cudaError_t filter3d_fp32(const float* vol, int W, int H, int D, int batch, long long stride,
+                          const float* h_filters, int nfilt, float* out, const int* conv_iter,
+                          int it, cudaStream_t st);
+// registration.cu
+cudaError_t normal_eq_partials(const float* q1, long long q1_stride_floats, const float* q2, int W,
+                               int H, int D, int batch, double* partials, int nblk, int zpb,
+                               const int* conv_iter, int it, cudaStream_t st);
+cudaError_t assemble_normal_eq(const double* partials, int nblk, int batch, double* A, double* h,
+                               cudaStream_t st);
+cudaError_t solve_update(const double* partials, int nblk, int batch, int type, float tol, int W,
+                         int H, int D, float* params, float* rotations, int* conv_iter,
+                         int* iterations, int* status, int it, cudaStream_t st);
+cudaError_t solve_given(const double* A, const double* h, int batch, float* p, cudaStream_t st);
+cudaError_t warp_affine(const float* src, long long src_stride, int W, int H, int D, int batch,
+                        const float* params, float* out, long long out_stride, const int* conv_iter,
+                        int it, cudaStream_t st);
+cudaError_t warp_field(const float* src, int W, int H, int D, const float* dx, const float* dy,
+                       const float* dz, float* out, cudaStream_t st);
+cudaError_t rescale_linear(const float* src, int W, int H, int D, float* out, int W2, int H2, int D2,
+                           cudaStream_t st);
+cudaError_t smooth3d(const float* vol, int W, int H, int D, int batch, const float* fx,
+                     const float* fy, const float* fz, const float* cert, const float* scert,
+                     float* tmp1, float* tmp2, float* out, cudaStream_t st, int accumulate = 0);
+// nonlinear.cu
+cudaError_t tensor_norm_max(const float* t6, long long V, float* a11, unsigned int* maxbits,
+                            cudaStream_t st);
+cudaError_t nonlinear_ah(const float* q1, const float* q2, float* t6, long long V,
+                         const unsigned int* maxbits, const float* m36, const float* dirs18, float* a6,
+                         float* h3, cudaStream_t st);
+cudaError_t tensor_components(const float* q2, long long V, const float* m36, float* t6, cudaStream_t st);
+cudaError_t displacement_update(const float* a6, const float* h3, long long V, int fp64, float* d3,
+                                cudaStream_t st);
+cudaError_t rescale_batch(const float* src, int W, int H, int D, int batch, float* out, int W2, int H2,
+                          int D2, float factor, cudaStream_t st);
+cudaError_t compose(float* total, const float* add, int batch, float tscale, cudaStream_t st);
+cudaError_t add_volumes(float* out, const float* a, const float* b, long long n, cudaStream_t st);
+}  // namespace brc

@@ -1,0 +1,316 @@
+// nonlinear.cu -- per-voxel kernels of the nonlinear (displacement field)
+// registration step, and the small helpers of the multi-scale drivers.
+//
+// One nonlinear iteration on the device (AlignTwoVolumesNonLinear,
+// broccoli_lib.cpp:5748-6058), every arrow one launch:
+//   filter3d<6> (+ fused structure tensor T = sum_k |q2_k| M_k)
+//   -> smooth T (6 volumes, one batched launch per pass)
+//   -> tensor_norm_max: |T| into a11 (the reference leaves it there) and the
+//      global max into a device scalar (no host round trip)
+//   -> nonlinear_ah: T scaled by 1/max, a += c TT, h += c dphi TT n for the
+//      six filter pairs in registers (one pass instead of six)
+//   -> smooth a, h (9 volumes)
+//   -> displacement_update (3x3 per voxel, FP32 cofactors as the reference or
+//      FP64 elimination)
+//   -> smooth update, accumulated into the field by the last pass
+//   -> warp_field
+#include <math.h>
+
+#include "common.cuh"
+
+namespace brc {
+
+struct NonlinearConsts {
+  float m[6][6];    // projection tensor of filter k: m11 m12 m13 m22 m23 m33
+  float dir[3][6];  // filter directions: x[6], y[6], z[6]
+};
+
+// |T| (Frobenius, symmetric) into a11 and the volume maximum into *maxbits
+// (float bits of a non-negative value, so unsigned ordering is float
+// ordering).  CalculateTensorNorms (kernelRegistration.cpp:847-875) and
+// CalculateMax (broccoli_lib.cpp:10889-10928).
+__global__ void __launch_bounds__(256)
+tensor_norm_max_kernel(const float* __restrict__ t6, long long V, float* __restrict__ a11,
+                       unsigned int* __restrict__ maxbits) {
+  float mx = 0.f;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < V;
+       i += (long long)gridDim.x * blockDim.x) {
+    const float a = t6[i], b = t6[V + i], c = t6[2 * V + i], d = t6[3 * V + i], e = t6[4 * V + i],
+                f = t6[5 * V + i];
+    const float n = sqrtf(a * a + 2.0f * b * b + 2.0f * c * c + d * d + 2.0f * e * e + f * f);
+    a11[i] = n;
+    mx = fmaxf(mx, n);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  __shared__ float s[8];
+  if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) mx = fmaxf(mx, s[w]);
+    atomicMax(maxbits, __float_as_uint(mx));
+  }
+}
+
+// a (6) and h (3) from the six filter pairs, T scaled by 1/max first; a11
+// starts from the tensor norm already stored there.
+// CalculateAMatricesAndHVectors, kernelRegistration.cpp:880-943.
+__global__ void __launch_bounds__(256)
+nonlinear_ah_kernel(const float2* __restrict__ q1, const float2* __restrict__ q2,
+                    float* __restrict__ t6, long long V, const unsigned int* __restrict__ maxbits,
+                    NonlinearConsts cst, float* __restrict__ a6, float* __restrict__ h3) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V) return;
+  const float mx = fmaxf(__uint_as_float(*maxbits), 1.17549435e-38f);
+  const float f = 1.0f / mx;
+  const float t11 = t6[i] * f, t12 = t6[V + i] * f, t13 = t6[2 * V + i] * f;
+  const float t22 = t6[3 * V + i] * f, t23 = t6[4 * V + i] * f, t33 = t6[5 * V + i] * f;
+  const float tt11 = t11 * t11 + t12 * t12 + t13 * t13;
+  const float tt12 = t11 * t12 + t12 * t22 + t13 * t23;
+  const float tt13 = t11 * t13 + t12 * t23 + t13 * t33;
+  const float tt22 = t12 * t12 + t22 * t22 + t23 * t23;
+  const float tt23 = t12 * t13 + t22 * t23 + t23 * t33;
+  const float tt33 = t13 * t13 + t23 * t23 + t33 * t33;
+  float a11 = a6[i], a12 = 0.f, a13 = 0.f, a22 = 0.f, a23 = 0.f, a33 = 0.f;
+  float h1 = 0.f, h2 = 0.f, h3v = 0.f;
+#pragma unroll
+  for (int k = 0; k < 6; k++) {
+    const float2 a = __ldg(q1 + k * V + i), c = __ldg(q2 + k * V + i);
+    const float qr = __fadd_rn(__fmul_rn(a.x, c.x), __fmul_rn(a.y, c.y));
+    const float qi = __fadd_rn(-__fmul_rn(a.x, c.y), __fmul_rn(a.y, c.x));
+    const float pd = atan2f(qi, qr);
+    const float aqq = sqrtf(qr * qr + qi * qi);
+    const float cs = cosf(pd / 2.0f);
+    const float cert = sqrtf(aqq) * cs * cs;
+    a11 += cert * tt11;
+    a12 += cert * tt12;
+    a13 += cert * tt13;
+    a22 += cert * tt22;
+    a23 += cert * tt23;
+    a33 += cert * tt33;
+    const float cp = cert * pd;
+    const float nx = cst.dir[0][k], ny = cst.dir[1][k], nz = cst.dir[2][k];
+    h1 += cp * (nx * tt11 + ny * tt12 + nz * tt13);
+    h2 += cp * (nx * tt12 + ny * tt22 + nz * tt23);
+    h3v += cp * (nx * tt13 + ny * tt23 + nz * tt33);
+  }
+  a6[i] = a11;
+  a6[V + i] = a12;
+  a6[2 * V + i] = a13;
+  a6[3 * V + i] = a22;
+  a6[4 * V + i] = a23;
+  a6[5 * V + i] = a33;
+  h3[i] = h1;
+  h3[V + i] = h2;
+  h3[2 * V + i] = h3v;
+  // the scaled tensor is what the reference keeps (MultiplyVolume in place)
+  t6[i] = t11;
+  t6[V + i] = t12;
+  t6[2 * V + i] = t13;
+  t6[3 * V + i] = t22;
+  t6[4 * V + i] = t23;
+  t6[5 * V + i] = t33;
+}
+
+// d = A^-1 h per voxel.  fp64 = 0: cofactors in FP32 with det + 1e-16f
+// (CalculateDisplacementUpdate, kernelRegistration.cpp:948-988); fp64 = 1:
+// the same cofactor solve in FP64 (no regularising 1e-16, a singular system
+// gives d = 0).
+__global__ void __launch_bounds__(256)
+displacement_update_kernel(const float* __restrict__ a6, const float* __restrict__ h3, long long V,
+                           int fp64, float* __restrict__ d3) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V) return;
+  if (!fp64) {
+    const float a11 = a6[i], a12 = a6[V + i], a13 = a6[2 * V + i], a22 = a6[3 * V + i],
+                a23 = a6[4 * V + i], a33 = a6[5 * V + i];
+    const float h1 = h3[i], h2 = h3[V + i], hh3 = h3[2 * V + i];
+    const float norm = 1.0f / (a11 * a22 * a33 - a11 * a23 * a23 - a12 * a12 * a33 + a12 * a23 * a13 +
+                               a13 * a12 * a23 - a13 * a22 * a13 + 1e-16f);
+    d3[i] = norm * ((hh3 * (a12 * a23 - a13 * a22)) - (h2 * (a12 * a33 - a13 * a23)) +
+                    (h1 * (a22 * a33 - a23 * a23)));
+    d3[V + i] = norm * ((h2 * (a11 * a33 - a13 * a13)) - (hh3 * (a11 * a23 - a13 * a12)) -
+                        (h1 * (a12 * a33 - a23 * a13)));
+    d3[2 * V + i] = norm * ((hh3 * (a11 * a22 - a12 * a12)) - (h2 * (a11 * a23 - a12 * a13)) +
+                            (h1 * (a12 * a23 - a22 * a13)));
+  } else {
+    const double a11 = a6[i], a12 = a6[V + i], a13 = a6[2 * V + i], a22 = a6[3 * V + i],
+                 a23 = a6[4 * V + i], a33 = a6[5 * V + i];
+    const double h1 = h3[i], h2 = h3[V + i], hh3 = h3[2 * V + i];
+    const double c11 = a22 * a33 - a23 * a23, c12 = a13 * a23 - a12 * a33, c13 = a12 * a23 - a13 * a22;
+    const double c22 = a11 * a33 - a13 * a13, c23 = a12 * a13 - a11 * a23, c33 = a11 * a22 - a12 * a12;
+    const double det = a11 * c11 + a12 * c12 + a13 * c13;
+    if (det == 0.0 || !isfinite(det)) {
+      d3[i] = 0.f;
+      d3[V + i] = 0.f;
+      d3[2 * V + i] = 0.f;
+      return;
+    }
+    const double r = 1.0 / det;
+    d3[i] = (float)(r * (c11 * h1 + c12 * h2 + c13 * hh3));
+    d3[V + i] = (float)(r * (c12 * h1 + c22 * h2 + c23 * hh3));
+    d3[2 * V + i] = (float)(r * (c13 * h1 + c23 * h2 + c33 * hh3));
+  }
+}
+
+// Structure tensor from six complex responses (used when the filter kernel
+// did not fuse it): T = sum_k |q2_k| M_k (CalculateTensorComponents,
+// kernelRegistration.cpp:806-845, accumulated over k = 0..5).
+__global__ void __launch_bounds__(256)
+tensor_components_kernel(const float2* __restrict__ q2, long long V, NonlinearConsts cst,
+                         float* __restrict__ t6) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V) return;
+  float t[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+  for (int k = 0; k < 6; k++) {
+    const float2 q = __ldg(q2 + k * V + i);
+    const float mag = sqrtf(q.x * q.x + q.y * q.y);
+#pragma unroll
+    for (int c = 0; c < 6; c++) t[c] += mag * cst.m[k][c];
+  }
+#pragma unroll
+  for (int c = 0; c < 6; c++) t6[c * V + i] = t[c];
+}
+
+// Linear resample of `batch` volumes to a new size, scaled by `factor`
+// (ChangeVolumeSize, broccoli_lib.cpp:6247-6388, followed by MultiplyVolume
+// for displacement fields, :6604-6611).
+__device__ __forceinline__ float sample_lin(const float* __restrict__ T, int W, int H, int D,
+                                            float u, float v, float w) {
+  const float uu = u - 0.5f, vv = v - 0.5f, ww = w - 0.5f;
+  const float fu = floorf(uu), fv = floorf(vv), fw = floorf(ww);
+  const float a = uu - fu, bb = vv - fv, c = ww - fw;
+  const int i0 = (int)fu, j0 = (int)fv, k0 = (int)fw;
+  const int xi0 = min(max(i0, 0), W - 1), xi1 = min(max(i0 + 1, 0), W - 1);
+  const int yj0 = min(max(j0, 0), H - 1), yj1 = min(max(j0 + 1, 0), H - 1);
+  const int zk0 = min(max(k0, 0), D - 1), zk1 = min(max(k0 + 1, 0), D - 1);
+  const long long r00 = (long long)yj0 * W + (long long)zk0 * W * H;
+  const long long r10 = (long long)yj1 * W + (long long)zk0 * W * H;
+  const long long r01 = (long long)yj0 * W + (long long)zk1 * W * H;
+  const long long r11 = (long long)yj1 * W + (long long)zk1 * W * H;
+  return (1.f - a) * (1.f - bb) * (1.f - c) * __ldg(T + xi0 + r00) +
+         a * (1.f - bb) * (1.f - c) * __ldg(T + xi1 + r00) +
+         (1.f - a) * bb * (1.f - c) * __ldg(T + xi0 + r10) + a * bb * (1.f - c) * __ldg(T + xi1 + r10) +
+         (1.f - a) * (1.f - bb) * c * __ldg(T + xi0 + r01) + a * (1.f - bb) * c * __ldg(T + xi1 + r01) +
+         (1.f - a) * bb * c * __ldg(T + xi0 + r11) + a * bb * c * __ldg(T + xi1 + r11);
+}
+
+__global__ void __launch_bounds__(256)
+rescale_batch_kernel(const float* __restrict__ src, int W, int H, int D, float* __restrict__ out, int W2,
+                     int H2, int D2, float vx, float vy, float vz, float factor) {
+  const int b = blockIdx.y;
+  const long long V2 = (long long)W2 * H2 * D2;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V2) return;
+  const int x = (int)(i % W2), y = (int)((i / W2) % H2), z = (int)(i / ((long long)W2 * H2));
+  const float v = sample_lin(src + (long long)b * W * H * D, W, H, D, x * vx + 0.5f, y * vy + 0.5f,
+                             z * vz + 0.5f);
+  out[(long long)b * V2 + i] = factor == 1.0f ? v : v * factor;
+}
+
+// Total = New * Old per instance with translations scaled by tscale (2 for
+// the next pyramid scale) (AddAffineRegistrationParameters[NextScale],
+// broccoli_lib.cpp:7252-7431), rounded to float as the reference does.
+__global__ void compose_kernel(float* __restrict__ total, const float* __restrict__ add, int batch,
+                               float tscale) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= batch) return;
+  float* o = total + 12 * b;
+  const float* n = add + 12 * b;
+  double O[16], N[16];
+  const float* src[2] = {o, n};
+  double* dst[2] = {O, N};
+  for (int m = 0; m < 2; m++) {
+    const float* p = src[m];
+    double* M = dst[m];
+    M[0] = (double)(p[3] + 1.0f); M[1] = (double)p[4]; M[2] = (double)p[5];
+    M[3] = tscale == 1.0f ? (double)p[0] : (double)(p[0] * tscale);
+    M[4] = (double)p[6]; M[5] = (double)(p[7] + 1.0f); M[6] = (double)p[8];
+    M[7] = tscale == 1.0f ? (double)p[1] : (double)(p[1] * tscale);
+    M[8] = (double)p[9]; M[9] = (double)p[10]; M[10] = (double)(p[11] + 1.0f);
+    M[11] = tscale == 1.0f ? (double)p[2] : (double)(p[2] * tscale);
+    M[12] = 0; M[13] = 0; M[14] = 0; M[15] = 1;
+  }
+  double T[16];
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) {
+      double s = 0;
+      for (int k = 0; k < 4; k++) s += N[i * 4 + k] * O[k * 4 + j];
+      T[i * 4 + j] = s;
+    }
+  o[0] = (float)T[3]; o[1] = (float)T[7]; o[2] = (float)T[11];
+  o[3] = (float)(T[0] - 1.0); o[4] = (float)T[1]; o[5] = (float)T[2];
+  o[6] = (float)T[4]; o[7] = (float)(T[5] - 1.0); o[8] = (float)T[6];
+  o[9] = (float)T[8]; o[10] = (float)T[9]; o[11] = (float)(T[10] - 1.0);
+}
+
+// out = a + b elementwise (AddVolumes, kernelMisc.cpp:383-400).
+__global__ void __launch_bounds__(256)
+add_kernel(float* __restrict__ out, const float* __restrict__ a, const float* __restrict__ b, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = a[i] + b[i];
+}
+
+// ---------------------------------------------------------------------------
+
+static unsigned grid1(long long n) { return (unsigned)((n + 255) / 256); }
+
+cudaError_t tensor_norm_max(const float* t6, long long V, float* a11, unsigned int* maxbits,
+                            cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(maxbits, 0, sizeof(unsigned int), st);
+  if (e != cudaSuccess) return e;
+  long long blocks = (V + 255) / 256;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  tensor_norm_max_kernel<<<(unsigned)blocks, 256, 0, st>>>(t6, V, a11, maxbits);
+  return cudaGetLastError();
+}
+
+cudaError_t nonlinear_ah(const float* q1, const float* q2, float* t6, long long V, const unsigned int* maxbits,
+                         const float* m36, const float* dirs18, float* a6, float* h3, cudaStream_t st) {
+  NonlinearConsts c;
+  for (int k = 0; k < 6; k++)
+    for (int j = 0; j < 6; j++) c.m[k][j] = m36[6 * k + j];
+  for (int a = 0; a < 3; a++)
+    for (int k = 0; k < 6; k++) c.dir[a][k] = dirs18[6 * a + k];
+  nonlinear_ah_kernel<<<grid1(V), 256, 0, st>>>(reinterpret_cast<const float2*>(q1),
+                                                 reinterpret_cast<const float2*>(q2), t6, V, maxbits, c,
+                                                 a6, h3);
+  return cudaGetLastError();
+}
+
+cudaError_t tensor_components(const float* q2, long long V, const float* m36, float* t6, cudaStream_t st) {
+  NonlinearConsts c;
+  for (int k = 0; k < 6; k++)
+    for (int j = 0; j < 6; j++) c.m[k][j] = m36[6 * k + j];
+  tensor_components_kernel<<<grid1(V), 256, 0, st>>>(reinterpret_cast<const float2*>(q2), V, c, t6);
+  return cudaGetLastError();
+}
+
+cudaError_t displacement_update(const float* a6, const float* h3, long long V, int fp64, float* d3,
+                                cudaStream_t st) {
+  displacement_update_kernel<<<grid1(V), 256, 0, st>>>(a6, h3, V, fp64, d3);
+  return cudaGetLastError();
+}
+
+cudaError_t rescale_batch(const float* src, int W, int H, int D, int batch, float* out, int W2, int H2,
+                          int D2, float factor, cudaStream_t st) {
+  const float vx = (float)(W - 1) / (float)(W2 - 1);
+  const float vy = (float)(H - 1) / (float)(H2 - 1);
+  const float vz = (float)(D - 1) / (float)(D2 - 1);
+  dim3 grid(grid1((long long)W2 * H2 * D2), batch);
+  rescale_batch_kernel<<<grid, 256, 0, st>>>(src, W, H, D, out, W2, H2, D2, vx, vy, vz, factor);
+  return cudaGetLastError();
+}
+
+cudaError_t compose(float* total, const float* add, int batch, float tscale, cudaStream_t st) {
+  compose_kernel<<<(batch + 63) / 64, 64, 0, st>>>(total, add, batch, tscale);
+  return cudaGetLastError();
+}
+
+cudaError_t add_volumes(float* out, const float* a, const float* b, long long n, cudaStream_t st) {
+  add_kernel<<<grid1(n), 256, 0, st>>>(out, a, b, n);
+  return cudaGetLastError();
+}
+
+}  // namespace brc

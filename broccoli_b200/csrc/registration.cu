@@ -1,0 +1,689 @@
+// registration.cu -- the per-iteration kernels of batched linear registration
+// and the volume helpers around it (warps, separable smoothing, rescale).
+//
+// Per affine iteration and instance:
+//   normal_eq_partial_kernel  phase difference, certainty and phase gradient
+//                             of the three filter pairs, reduced to the 42
+//                             distinct sums of the 12x12 system (FP64).
+//   solve_update_kernel       reduces the partial sums in a fixed order,
+//                             solves the three decoupled 4x4 systems in FP64,
+//                             applies the TRANSLATION / RIGID / AFFINE update
+//                             and the convergence test.
+//   warp_affine_kernel        exact-weight trilinear resampling of the
+//                             original volume with the total parameters.
+#include <math.h>
+
+#include "common.cuh"
+
+namespace brc {
+
+// ---------------------------------------------------------------------------
+// Normal equations
+// ---------------------------------------------------------------------------
+
+constexpr int kNEThreads = 256;
+
+// Phase difference and certainty of one response pair, in the reference's
+// operation order (CalculatePhaseDifferencesAndCertainties,
+// kernelRegistration.cpp:173-211).
+__device__ __forceinline__ void phase_diff_cert(float2 a, float2 c, float& pd, float& cert) {
+  // products rounded separately (no FMA contraction), as in the reference's
+  // arithmetic: identical responses then give exactly zero phase difference
+  float re = __fadd_rn(__fmul_rn(a.x, c.x), __fmul_rn(a.y, c.y));
+  float im = __fsub_rn(__fmul_rn(a.y, c.x), __fmul_rn(a.x, c.y));
+  pd = atan2f(im, re);
+  re = a.x * c.x - a.y * c.y;
+  im = a.y * c.x + a.x * c.y;
+  const float cs = cosf(pd * 0.5f);
+  cert = sqrtf(re * re + im * im) * cs * cs;
+}
+
+// Phase gradient from the neighbours along one axis
+// (CalculatePhaseGradientsX/Y/Z, kernelRegistration.cpp:213-382).
+__device__ __forceinline__ float phase_grad(float2 a_p, float2 a_c, float2 a_m, float2 c_p,
+                                            float2 c_c, float2 c_m) {
+  float tr = 0.f, ti = 0.f;
+  tr += a_p.x * a_c.x + a_p.y * a_c.y;
+  ti += a_p.y * a_c.x - a_p.x * a_c.y;
+  tr += a_c.x * a_m.x + a_c.y * a_m.y;
+  ti += a_c.y * a_m.x - a_c.x * a_m.y;
+  tr += c_p.x * c_c.x + c_p.y * c_c.y;
+  ti += c_p.y * c_c.x - c_p.x * c_c.y;
+  tr += c_c.x * c_m.x + c_c.y * c_m.y;
+  ti += c_c.y * c_m.x - c_c.x * c_m.y;
+  return atan2f(ti, tr);
+}
+
+// Sums over the interior (3 voxels from every face) of
+//   c g^2 [1, x, y, z, xx, xy, xz, yy, yz, zz]  and  c g dphi [1, x, y, z]
+// for each axis k (sum index 14k + e), coordinates relative to the volume
+// centre: the 30 + 12 values that CalculateAMatrixAndHVector2DValuesX/Y/Z,
+// CalculateAMatrix1DValues / HVector1DValues and CalculateAMatrix /
+// HVector accumulate (kernelRegistration.cpp:387-800).  One CTA handles
+// `zpb` interior slices of one instance and writes 42 FP64 partial sums.
+__global__ void __launch_bounds__(kNEThreads)
+normal_eq_partial_kernel(const float2* __restrict__ q1, long long q1_stride,
+                         const float2* __restrict__ q2, int W, int H, int D, int zpb,
+                         double* __restrict__ partials, const int* __restrict__ conv_iter, int it) {
+  const int b = blockIdx.y;
+  if (instance_done(conv_iter, b, it)) return;
+  const long long V = (long long)W * H * D;
+  const float2* Q1 = q1 + (long long)b * q1_stride;
+  const float2* Q2 = q2 + (long long)b * 3 * V;
+  double acc[kNSums];
+#pragma unroll
+  for (int j = 0; j < kNSums; j++) acc[j] = 0.0;
+
+  const int nx = W - 6, ny = H - 6;
+  const int z0 = 3 + blockIdx.x * zpb;
+  const int z1 = min(D - 3, z0 + zpb);
+  const long long n = (nx > 0 && ny > 0 && z1 > z0) ? (long long)nx * ny * (z1 - z0) : 0;
+  const double cx = 0.5 * (W - 1), cy = 0.5 * (H - 1), cz = 0.5 * (D - 1);
+  const long long stride[3] = {1, W, (long long)W * H};
+
+  for (long long e = threadIdx.x; e < n; e += kNEThreads) {
+    const int x = 3 + (int)(e % nx);
+    const int y = 3 + (int)((e / nx) % ny);
+    const int z = z0 + (int)(e / ((long long)nx * ny));
+    const long long i = x + (long long)y * W + (long long)z * W * H;
+    const double xf = x - cx, yf = y - cy, zf = z - cz;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const float2* A = Q1 + k * V;
+      const float2* C = Q2 + k * V;
+      const long long s = stride[k];
+      const float2 a = __ldg(A + i), c = __ldg(C + i);
+      float pd, cert;
+      phase_diff_cert(a, c, pd, cert);
+      const float g = phase_grad(__ldg(A + i + s), a, __ldg(A + i - s), __ldg(C + i + s), c,
+                                 __ldg(C + i - s));
+      const float cg = cert * g;
+      const double w = (double)(cg * g);
+      const double v = (double)(cg * pd);
+      double* ak = acc + 14 * k;
+      ak[0] += w;
+      ak[1] += w * xf;
+      ak[2] += w * yf;
+      ak[3] += w * zf;
+      ak[4] += w * xf * xf;
+      ak[5] += w * xf * yf;
+      ak[6] += w * xf * zf;
+      ak[7] += w * yf * yf;
+      ak[8] += w * yf * zf;
+      ak[9] += w * zf * zf;
+      ak[10] += v;
+      ak[11] += v * xf;
+      ak[12] += v * yf;
+      ak[13] += v * zf;
+    }
+  }
+
+  // Deterministic block reduction: warp shuffles, then warps in order.
+  __shared__ double s_part[kNEThreads / 32][kNSums];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < kNSums; j++) {
+    double v = acc[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) s_part[warp][j] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < kNSums) {
+    double v = 0.0;
+#pragma unroll
+    for (int w = 0; w < kNEThreads / 32; w++) v += s_part[w][threadIdx.x];
+    partials[((long long)b * gridDim.x + blockIdx.x) * kNSums + threadIdx.x] = v;
+  }
+}
+
+// (row, column) of the 10 A entries of one axis, monomial order
+// [1, x, y, z, xx, xy, xz, yy, yz, zz]; axis k owns parameters
+// {k, 3+3k, 4+3k, 5+3k} (the GetParameterIndices table,
+// kernelRegistration.cpp:43-171).
+__constant__ int c_mono_a[10] = {0, 1, 2, 3, 1, 2, 3, 2, 3, 3};
+__constant__ int c_mono_b[10] = {0, 0, 0, 0, 1, 1, 1, 2, 2, 3};
+
+__device__ __forceinline__ int axis_param(int k, int m) { return m == 0 ? k : 2 + 3 * k + m; }
+
+// Threads [0, 42) of the CTA sum the nblk partial rows of instance b.
+__device__ void reduce_partials(const double* __restrict__ partials, int nblk, int b, double* s) {
+  if (threadIdx.x < kNSums) {
+    double v = 0.0;
+    for (int r = 0; r < nblk; r++) v += partials[((long long)b * nblk + r) * kNSums + threadIdx.x];
+    s[threadIdx.x] = v;
+  }
+  __syncthreads();
+}
+
+// Full symmetric 12x12 A (column-major) and h of one instance.
+__global__ void assemble_kernel(const double* __restrict__ partials, int nblk, double* __restrict__ A,
+                                double* __restrict__ h) {
+  __shared__ double s[kNSums];
+  const int b = blockIdx.x;
+  reduce_partials(partials, nblk, b, s);
+  double* Ab = A + (long long)b * 144;
+  for (int j = threadIdx.x; j < 144; j += blockDim.x) Ab[j] = 0.0;
+  __syncthreads();
+  if (threadIdx.x < 30) {
+    const int k = threadIdx.x / 10, e = threadIdx.x % 10;
+    const int i = axis_param(k, c_mono_a[e]), j = axis_param(k, c_mono_b[e]);
+    Ab[i + 12 * j] = s[14 * k + e];
+    Ab[j + 12 * i] = s[14 * k + e];
+  } else if (threadIdx.x >= 32 && threadIdx.x < 44) {
+    const int t = threadIdx.x - 32, k = t / 4, m = t % 4;
+    h[(long long)b * 12 + axis_param(k, m)] = s[14 * k + 10 + m];
+  }
+}
+
+// Solves the 4x4 block of axis k by Gaussian elimination with complete
+// pivoting.  Pivots at or below `thresh` end the elimination and the
+// remaining unknowns are 0, the rank rule of the reference's full-pivoting
+// QR solve (SolveEquationSystem, broccoli_lib.cpp:17157-17186).
+__device__ void solve4(double M[4][4], double r[4], double thresh, double x[4]) {
+  int perm[4] = {0, 1, 2, 3};
+  int rank = 0;
+  for (int k = 0; k < 4; k++) {
+    int pr = k, pc = k;
+    double best = -1.0;
+    for (int i = k; i < 4; i++)
+      for (int j = k; j < 4; j++)
+        if (fabs(M[i][j]) > best) {
+          best = fabs(M[i][j]);
+          pr = i;
+          pc = j;
+        }
+    if (best <= thresh || best == 0.0) break;
+    rank++;
+    if (pr != k) {
+      for (int j = 0; j < 4; j++) {
+        const double t = M[k][j];
+        M[k][j] = M[pr][j];
+        M[pr][j] = t;
+      }
+      const double t = r[k];
+      r[k] = r[pr];
+      r[pr] = t;
+    }
+    if (pc != k) {
+      for (int i = 0; i < 4; i++) {
+        const double t = M[i][k];
+        M[i][k] = M[i][pc];
+        M[i][pc] = t;
+      }
+      const int t = perm[k];
+      perm[k] = perm[pc];
+      perm[pc] = t;
+    }
+    for (int i = k + 1; i < 4; i++) {
+      const double m = M[i][k] / M[k][k];
+      if (m == 0.0) continue;
+      for (int j = k; j < 4; j++) M[i][j] -= m * M[k][j];
+      r[i] -= m * r[k];
+    }
+  }
+  double y[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int i = rank - 1; i >= 0; i--) {
+    double s = r[i];
+    for (int j = i + 1; j < rank; j++) s -= M[i][j] * y[j];
+    y[i] = s / M[i][i];
+  }
+  for (int i = 0; i < 4; i++) x[perm[i]] = y[i];
+}
+
+// p = A^-1 h for the 12-parameter system given by the 42 sums, FP64,
+// rounded to float (the reference casts its Eigen solution to float).
+__device__ void solve12_from_sums(const double* s, float p[12]) {
+  double maxabs = 0.0;
+  for (int j = 0; j < kNSums; j++)
+    if ((j % 14) < 10) maxabs = fmax(maxabs, fabs(s[j]));
+  const double thresh = maxabs * 2.220446049250313e-16 * 12.0;
+  for (int k = 0; k < 3; k++) {
+    double M[4][4], r[4], x[4];
+    for (int e = 0; e < 10; e++) {
+      const int a = c_mono_a[e], bb = c_mono_b[e];
+      M[a][bb] = s[14 * k + e];
+      M[bb][a] = s[14 * k + e];
+    }
+    for (int m = 0; m < 4; m++) r[m] = s[14 * k + 10 + m];
+    solve4(M, r, thresh, x);
+    for (int m = 0; m < 4; m++) p[axis_param(k, m)] = (float)x[m];
+  }
+}
+
+// Orthogonal polar factor U V^T of a 3x3 matrix (row-major) from one-sided
+// Jacobi sweeps, FP64 (the reference takes U V^T of Eigen's JacobiSVD in
+// RemoveTransformationScaling, broccoli_lib.cpp:6153-6194).
+__device__ void polar3(const double* M, double* R) {
+  double A[9], Vm[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  for (int i = 0; i < 9; i++) A[i] = M[i];
+  for (int sweep = 0; sweep < 60; sweep++) {
+    bool rotated = false;
+    for (int p = 0; p < 2; p++)
+      for (int q = p + 1; q < 3; q++) {
+        double al = 0, be = 0, ga = 0;
+        for (int i = 0; i < 3; i++) {
+          al += A[i * 3 + p] * A[i * 3 + p];
+          be += A[i * 3 + q] * A[i * 3 + q];
+          ga += A[i * 3 + p] * A[i * 3 + q];
+        }
+        if (fabs(ga) <= 1e-300 || fabs(ga) <= 2.220446049250313e-16 * sqrt(al * be)) continue;
+        rotated = true;
+        const double zeta = (be - al) / (2.0 * ga);
+        const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        const double c = 1.0 / sqrt(1.0 + t * t), sn = c * t;
+        for (int i = 0; i < 3; i++) {
+          const double ap = A[i * 3 + p], aq = A[i * 3 + q];
+          A[i * 3 + p] = c * ap - sn * aq;
+          A[i * 3 + q] = sn * ap + c * aq;
+          const double vp = Vm[i * 3 + p], vq = Vm[i * 3 + q];
+          Vm[i * 3 + p] = c * vp - sn * vq;
+          Vm[i * 3 + q] = sn * vp + c * vq;
+        }
+      }
+    if (!rotated) break;
+  }
+  double U[9], sig[3];
+  for (int j = 0; j < 3; j++) {
+    sig[j] = sqrt(A[j] * A[j] + A[3 + j] * A[3 + j] + A[6 + j] * A[6 + j]);
+    for (int i = 0; i < 3; i++) U[i * 3 + j] = sig[j] > 0 ? A[i * 3 + j] / sig[j] : 0.0;
+  }
+  for (int j = 0; j < 3; j++)
+    if (!(sig[j] > 0)) {
+      const int a = (j + 1) % 3, bb = (j + 2) % 3;
+      U[0 * 3 + j] = U[1 * 3 + a] * U[2 * 3 + bb] - U[2 * 3 + a] * U[1 * 3 + bb];
+      U[1 * 3 + j] = U[2 * 3 + a] * U[0 * 3 + bb] - U[0 * 3 + a] * U[2 * 3 + bb];
+      U[2 * 3 + j] = U[0 * 3 + a] * U[1 * 3 + bb] - U[1 * 3 + a] * U[0 * 3 + bb];
+    }
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      double s = 0;
+      for (int k = 0; k < 3; k++) s += U[i * 3 + k] * Vm[j * 3 + k];
+      R[i * 3 + j] = s;
+    }
+}
+
+__device__ void remove_scaling(float* p) {
+  double M[9], R[9];
+  for (int i = 0; i < 9; i++) M[i] = (double)p[3 + i];
+  M[0] += 1.0;
+  M[4] += 1.0;
+  M[8] += 1.0;
+  polar3(M, R);
+  R[0] -= 1.0;
+  R[4] -= 1.0;
+  R[8] -= 1.0;
+  for (int i = 0; i < 9; i++) p[3 + i] = (float)R[i];
+}
+
+// Total = New * Old on 4x4 homogeneous matrices in FP64, the diagonal ones
+// added in float first (AddAffineRegistrationParameters,
+// broccoli_lib.cpp:7252-7340).
+__device__ void compose(float* old12, const float* n12) {
+  double O[16], N[16], T[16];
+  const float* src[2] = {old12, n12};
+  double* dst[2] = {O, N};
+  for (int m = 0; m < 2; m++) {
+    const float* p = src[m];
+    double* Mt = dst[m];
+    Mt[0] = (double)(p[3] + 1.0f); Mt[1] = (double)p[4]; Mt[2] = (double)p[5]; Mt[3] = (double)p[0];
+    Mt[4] = (double)p[6]; Mt[5] = (double)(p[7] + 1.0f); Mt[6] = (double)p[8]; Mt[7] = (double)p[1];
+    Mt[8] = (double)p[9]; Mt[9] = (double)p[10]; Mt[10] = (double)(p[11] + 1.0f); Mt[11] = (double)p[2];
+    Mt[12] = 0; Mt[13] = 0; Mt[14] = 0; Mt[15] = 1;
+  }
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) {
+      double s = 0;
+      for (int k = 0; k < 4; k++) s += N[i * 4 + k] * O[k * 4 + j];
+      T[i * 4 + j] = s;
+    }
+  old12[0] = (float)T[3];
+  old12[1] = (float)T[7];
+  old12[2] = (float)T[11];
+  old12[3] = (float)(T[0] - 1.0); old12[4] = (float)T[1]; old12[5] = (float)T[2];
+  old12[6] = (float)T[4]; old12[7] = (float)(T[5] - 1.0); old12[8] = (float)T[6];
+  old12[9] = (float)T[8]; old12[10] = (float)T[9]; old12[11] = (float)(T[10] - 1.0);
+}
+
+// Euler angles in degrees (CalculateRotationAnglesFromRotationMatrix,
+// broccoli_lib.cpp:6199-6244).
+__device__ void rotation_angles(const float* p, float* rot) {
+  const double PI_ = 3.14159265358979323846;
+  double m[9];
+  for (int i = 0; i < 9; i++) m[i] = (double)p[3 + i];
+  m[0] += 1.0;
+  m[4] += 1.0;
+  m[8] += 1.0;
+  const double a1 = -atan2(m[5], m[8]) * 180.0 / PI_;
+  const double c2 = sqrt(m[0] * m[0] + m[1] * m[1]);
+  const double a2 = -atan2(-m[2], c2) * 180.0 / PI_;
+  const double s1 = sin(a1 * PI_ / 180.0), c1 = cos(a1 * PI_ / 180.0);
+  const double a3 = -atan2(s1 * m[6] - c1 * m[3], c1 * m[4] - s1 * m[7]) * 180.0 / PI_;
+  rot[0] = (float)a1;
+  rot[1] = (float)a2;
+  rot[2] = (float)a3;
+}
+
+// Largest displacement (voxels) of the update p over the 8 volume corners.
+__device__ double update_magnitude(const float* p, int W, int H, int D) {
+  const double hx = 0.5 * (W - 1), hy = 0.5 * (H - 1), hz = 0.5 * (D - 1);
+  double best = 0.0;
+  for (int c = 0; c < 8; c++) {
+    const double x = (c & 1) ? hx : -hx, y = (c & 2) ? hy : -hy, z = (c & 4) ? hz : -hz;
+    const double dx = p[0] + p[3] * x + p[4] * y + p[5] * z;
+    const double dy = p[1] + p[6] * x + p[7] * y + p[8] * z;
+    const double dz = p[2] + p[9] * x + p[10] * y + p[11] * z;
+    best = fmax(best, sqrt(dx * dx + dy * dy + dz * dz));
+  }
+  return best;
+}
+
+// One iteration's solve and parameter update for every active instance
+// (AlignTwoVolumesLinear, broccoli_lib.cpp:5380-5421).
+__global__ void solve_update_kernel(const double* __restrict__ partials, int nblk, int type,
+                                    float tol, int W, int H, int D, float* __restrict__ params,
+                                    float* __restrict__ rotations, int* __restrict__ conv_iter,
+                                    int* __restrict__ iterations, int* __restrict__ status, int it) {
+  __shared__ double s[kNSums];
+  const int b = blockIdx.x;
+  if (conv_iter != nullptr && conv_iter[b] < it) return;
+  reduce_partials(partials, nblk, b, s);
+  if (threadIdx.x != 0) return;
+  float p[12];
+  solve12_from_sums(s, p);
+  bool finite = true;
+  for (int i = 0; i < 12; i++) finite = finite && isfinite(p[i]);
+  if (!finite) {
+    for (int i = 0; i < 12; i++) p[i] = 0.f;
+    if (status) atomicOr(status, 1);
+  }
+  float* tot = params + (long long)b * 12;
+  float t[12];
+  for (int i = 0; i < 12; i++) t[i] = tot[i];
+  if (type == 0) {
+    t[0] += p[0];
+    t[1] += p[1];
+    t[2] += p[2];
+    for (int i = 3; i < 12; i++) t[i] = 0.f;
+    for (int i = 3; i < 12; i++) p[i] = 0.f;
+  } else if (type == 1) {
+    remove_scaling(p);
+    compose(t, p);
+  } else {
+    compose(t, p);
+  }
+  for (int i = 0; i < 12; i++) tot[i] = t[i];
+  if (iterations) iterations[b] = it + 1;
+  if (rotations && type == 1) rotation_angles(t, rotations + (long long)b * 3);
+  if (conv_iter != nullptr && tol > 0.f && update_magnitude(p, W, H, D) < (double)tol)
+    conv_iter[b] = it;
+}
+
+// Plain solve of given A/h (brc_solve_affine_fp64): A column-major 12x12.
+__global__ void solve_given_kernel(const double* __restrict__ A, const double* __restrict__ h,
+                                   float* __restrict__ p) {
+  const int b = blockIdx.x;
+  if (threadIdx.x != 0) return;
+  const double* Ab = A + (long long)b * 144;
+  const double* hb = h + (long long)b * 12;
+  // The 12x12 of this path is block diagonal; solve it as a general 12x12
+  // with complete pivoting so that any symmetric system is handled.
+  double M[144], r[12], x[12];
+  int perm[12];
+  for (int i = 0; i < 12; i++) {
+    r[i] = hb[i];
+    perm[i] = i;
+    for (int j = 0; j < 12; j++) M[i * 12 + j] = Ab[i + 12 * j];
+  }
+  double maxpiv = 0.0;
+  int rank = 0;
+  for (int k = 0; k < 12; k++) {
+    int pr = k, pc = k;
+    double best = -1.0;
+    for (int i = k; i < 12; i++)
+      for (int j = k; j < 12; j++)
+        if (fabs(M[i * 12 + j]) > best) {
+          best = fabs(M[i * 12 + j]);
+          pr = i;
+          pc = j;
+        }
+    if (k == 0) maxpiv = best;
+    if (best <= maxpiv * 2.220446049250313e-16 * 12.0 || best == 0.0) break;
+    rank++;
+    if (pr != k) {
+      for (int j = 0; j < 12; j++) {
+        const double t = M[k * 12 + j];
+        M[k * 12 + j] = M[pr * 12 + j];
+        M[pr * 12 + j] = t;
+      }
+      const double t = r[k];
+      r[k] = r[pr];
+      r[pr] = t;
+    }
+    if (pc != k) {
+      for (int i = 0; i < 12; i++) {
+        const double t = M[i * 12 + k];
+        M[i * 12 + k] = M[i * 12 + pc];
+        M[i * 12 + pc] = t;
+      }
+      const int t = perm[k];
+      perm[k] = perm[pc];
+      perm[pc] = t;
+    }
+    for (int i = k + 1; i < 12; i++) {
+      const double m = M[i * 12 + k] / M[k * 12 + k];
+      if (m == 0.0) continue;
+      for (int j = k; j < 12; j++) M[i * 12 + j] -= m * M[k * 12 + j];
+      r[i] -= m * r[k];
+    }
+  }
+  double y[12];
+  for (int i = 0; i < 12; i++) y[i] = 0.0;
+  for (int i = rank - 1; i >= 0; i--) {
+    double s = r[i];
+    for (int j = i + 1; j < rank; j++) s -= M[i * 12 + j] * y[j];
+    y[i] = s / M[i * 12 + i];
+  }
+  for (int i = 0; i < 12; i++) x[perm[i]] = y[i];
+  for (int i = 0; i < 12; i++) p[(long long)b * 12 + i] = (float)x[i];
+}
+
+// ---------------------------------------------------------------------------
+// Trilinear sampling
+// ---------------------------------------------------------------------------
+
+// OpenCL 1.2 section 8.2 linear filtering with unnormalised coordinates and
+// clamp-to-edge addressing, exact float weights (the sampler of
+// kernelRegistration.cpp:1064).  u, v, w include the +0.5 texel offset.
+__device__ __forceinline__ float sample_linear(const float* __restrict__ T, int W, int H, int D,
+                                              float u, float v, float w) {
+  const float uu = u - 0.5f, vv = v - 0.5f, ww = w - 0.5f;
+  const float fu = floorf(uu), fv = floorf(vv), fw = floorf(ww);
+  const float a = uu - fu, bb = vv - fv, c = ww - fw;
+  const int i0 = (int)fu, j0 = (int)fv, k0 = (int)fw;
+  const int xi0 = min(max(i0, 0), W - 1), xi1 = min(max(i0 + 1, 0), W - 1);
+  const int yj0 = min(max(j0, 0), H - 1), yj1 = min(max(j0 + 1, 0), H - 1);
+  const int zk0 = min(max(k0, 0), D - 1), zk1 = min(max(k0 + 1, 0), D - 1);
+  const long long r00 = (long long)yj0 * W + (long long)zk0 * W * H;
+  const long long r10 = (long long)yj1 * W + (long long)zk0 * W * H;
+  const long long r01 = (long long)yj0 * W + (long long)zk1 * W * H;
+  const long long r11 = (long long)yj1 * W + (long long)zk1 * W * H;
+  return (1.f - a) * (1.f - bb) * (1.f - c) * __ldg(T + xi0 + r00) +
+         a * (1.f - bb) * (1.f - c) * __ldg(T + xi1 + r00) +
+         (1.f - a) * bb * (1.f - c) * __ldg(T + xi0 + r10) +
+         a * bb * (1.f - c) * __ldg(T + xi1 + r10) +
+         (1.f - a) * (1.f - bb) * c * __ldg(T + xi0 + r01) +
+         a * (1.f - bb) * c * __ldg(T + xi1 + r01) +
+         (1.f - a) * bb * c * __ldg(T + xi0 + r11) + a * bb * c * __ldg(T + xi1 + r11);
+}
+
+// out_b(x) = src_b(x + t + (A - I)(x - centre)), params_b of instance b
+// (InterpolateVolumeLinearLinear, kernelRegistration.cpp:1066-1101).
+__global__ void __launch_bounds__(256)
+warp_affine_kernel(const float* __restrict__ src, long long src_stride, int W, int H, int D,
+                   const float* __restrict__ params, float* __restrict__ out, long long out_stride,
+                   const int* __restrict__ conv_iter, int it) {
+  const int b = blockIdx.y;
+  if (instance_done(conv_iter, b, it)) return;
+  const long long V = (long long)W * H * D;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V) return;
+  const int x = (int)(i % W), y = (int)((i / W) % H), z = (int)(i / ((long long)W * H));
+  const float* p = params + (long long)b * 12;
+  const float xf = (float)x - ((float)W - 1.0f) * 0.5f;
+  const float yf = (float)y - ((float)H - 1.0f) * 0.5f;
+  const float zf = (float)z - ((float)D - 1.0f) * 0.5f;
+  const float u = (float)x + p[0] + p[3] * xf + p[4] * yf + p[5] * zf + 0.5f;
+  const float v = (float)y + p[1] + p[6] * xf + p[7] * yf + p[8] * zf + 0.5f;
+  const float w = (float)z + p[2] + p[9] * xf + p[10] * yf + p[11] * zf + 0.5f;
+  out[(long long)b * out_stride + i] = sample_linear(src + (long long)b * src_stride, W, H, D, u, v, w);
+}
+
+// Displacement-field warp (InterpolateVolumeLinearNonLinear,
+// kernelRegistration.cpp:1111-1140).
+__global__ void __launch_bounds__(256)
+warp_field_kernel(const float* __restrict__ src, int W, int H, int D, const float* __restrict__ dx,
+                  const float* __restrict__ dy, const float* __restrict__ dz, float* __restrict__ out) {
+  const long long V = (long long)W * H * D;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V) return;
+  const int x = (int)(i % W), y = (int)((i / W) % H), z = (int)(i / ((long long)W * H));
+  out[i] = sample_linear(src, W, H, D, (float)x + dx[i] + 0.5f, (float)y + dy[i] + 0.5f,
+                         (float)z + dz[i] + 0.5f);
+}
+
+// Linear resample with spacing (N-1)/(N'-1) (RescaleVolumeLinear,
+// kernelRegistration.cpp:1340-1366).
+__global__ void __launch_bounds__(256)
+rescale_linear_kernel(const float* __restrict__ src, int W, int H, int D, float* __restrict__ out,
+                      int W2, int H2, int D2, float vx, float vy, float vz) {
+  const long long V2 = (long long)W2 * H2 * D2;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V2) return;
+  const int x = (int)(i % W2), y = (int)((i / W2) % H2), z = (int)(i / ((long long)W2 * H2));
+  out[i] = sample_linear(src, W, H, D, x * vx + 0.5f, y * vy + 0.5f, z * vz + 0.5f);
+}
+
+// ---------------------------------------------------------------------------
+// Separable 9-tap smoothing (three passes)
+// ---------------------------------------------------------------------------
+
+struct Taps9 {
+  float f[9];
+};
+
+// axis 1 (y): out = sum (vol * cert)[y+o] f[4-o]; axis 0 (x): along x;
+// axis 2 (z): along z, then divided by the smoothed certainty.
+// SeparableConvolutionRows / Columns / Rods, kernelConvolution.cpp:52-91,
+// :531-569, :1201-1240.
+template <int AXIS>
+__global__ void __launch_bounds__(256)
+smooth_pass_kernel(const float* __restrict__ in, long long in_stride, const float* __restrict__ cert,
+                   const float* __restrict__ scert, int W, int H, int D, Taps9 taps,
+                   float* __restrict__ out, long long out_stride, int accumulate) {
+  const int b = blockIdx.y;
+  const long long V = (long long)W * H * D;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V) return;
+  const int x = (int)(i % W), y = (int)((i / W) % H), z = (int)(i / ((long long)W * H));
+  const float* src = in + (long long)b * in_stride;
+  const int c = AXIS == 0 ? x : (AXIS == 1 ? y : z);
+  const int n = AXIS == 0 ? W : (AXIS == 1 ? H : D);
+  const long long s = AXIS == 0 ? 1 : (AXIS == 1 ? (long long)W : (long long)W * H);
+  float sum = 0.f;
+#pragma unroll
+  for (int o = -4; o <= 4; o++) {
+    float px = 0.f;
+    if (c + o >= 0 && c + o < n) {
+      const long long j = i + o * s;
+      px = __ldg(src + j);
+      if (AXIS == 1 && cert != nullptr) px *= __ldg(cert + j);
+    }
+    sum += px * taps.f[4 - o];
+  }
+  if (AXIS == 2 && scert != nullptr) sum = sum / __ldg(scert + i);
+  float* o = out + (long long)b * out_stride + i;
+  // accumulate: the field update of the nonlinear step (AddVolumes after
+  // the smoothing, broccoli_lib.cpp:6021-6025) folded into the last pass
+  *o = accumulate ? *o + sum : sum;
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers
+// ---------------------------------------------------------------------------
+
+cudaError_t normal_eq_partials(const float* q1, long long q1_stride_floats, const float* q2, int W,
+                               int H, int D, int batch, double* partials, int nblk, int zpb,
+                               const int* conv_iter, int it, cudaStream_t st) {
+  dim3 grid(nblk, batch);
+  normal_eq_partial_kernel<<<grid, kNEThreads, 0, st>>>(
+      reinterpret_cast<const float2*>(q1), q1_stride_floats / 2, reinterpret_cast<const float2*>(q2),
+      W, H, D, zpb, partials, conv_iter, it);
+  return cudaGetLastError();
+}
+
+cudaError_t assemble_normal_eq(const double* partials, int nblk, int batch, double* A, double* h,
+                               cudaStream_t st) {
+  assemble_kernel<<<batch, 64, 0, st>>>(partials, nblk, A, h);
+  return cudaGetLastError();
+}
+
+cudaError_t solve_update(const double* partials, int nblk, int batch, int type, float tol, int W,
+                         int H, int D, float* params, float* rotations, int* conv_iter,
+                         int* iterations, int* status, int it, cudaStream_t st) {
+  solve_update_kernel<<<batch, 64, 0, st>>>(partials, nblk, type, tol, W, H, D, params, rotations,
+                                            conv_iter, iterations, status, it);
+  return cudaGetLastError();
+}
+
+cudaError_t solve_given(const double* A, const double* h, int batch, float* p, cudaStream_t st) {
+  solve_given_kernel<<<batch, 32, 0, st>>>(A, h, p);
+  return cudaGetLastError();
+}
+
+cudaError_t warp_affine(const float* src, long long src_stride, int W, int H, int D, int batch,
+                        const float* params, float* out, long long out_stride, const int* conv_iter,
+                        int it, cudaStream_t st) {
+  const long long V = (long long)W * H * D;
+  dim3 grid((unsigned)((V + 255) / 256), batch);
+  warp_affine_kernel<<<grid, 256, 0, st>>>(src, src_stride, W, H, D, params, out, out_stride,
+                                           conv_iter, it);
+  return cudaGetLastError();
+}
+
+cudaError_t warp_field(const float* src, int W, int H, int D, const float* dx, const float* dy,
+                       const float* dz, float* out, cudaStream_t st) {
+  const long long V = (long long)W * H * D;
+  warp_field_kernel<<<(unsigned)((V + 255) / 256), 256, 0, st>>>(src, W, H, D, dx, dy, dz, out);
+  return cudaGetLastError();
+}
+
+cudaError_t rescale_linear(const float* src, int W, int H, int D, float* out, int W2, int H2, int D2,
+                           cudaStream_t st) {
+  const long long V2 = (long long)W2 * H2 * D2;
+  const float vx = (float)(W - 1) / (float)(W2 - 1);
+  const float vy = (float)(H - 1) / (float)(H2 - 1);
+  const float vz = (float)(D - 1) / (float)(D2 - 1);
+  rescale_linear_kernel<<<(unsigned)((V2 + 255) / 256), 256, 0, st>>>(src, W, H, D, out, W2, H2, D2,
+                                                                     vx, vy, vz);
+  return cudaGetLastError();
+}
+
+cudaError_t smooth3d(const float* vol, int W, int H, int D, int batch, const float* fx,
+                     const float* fy, const float* fz, const float* cert, const float* scert,
+                     float* tmp1, float* tmp2, float* out, cudaStream_t st, int accumulate) {
+  const long long V = (long long)W * H * D;
+  dim3 grid((unsigned)((V + 255) / 256), batch);
+  Taps9 tx, ty, tz;
+  for (int i = 0; i < 9; i++) {
+    tx.f[i] = fx[i];
+    ty.f[i] = fy[i];
+    tz.f[i] = fz[i];
+  }
+  smooth_pass_kernel<1><<<grid, 256, 0, st>>>(vol, V, cert, nullptr, W, H, D, ty, tmp1, V, 0);
+  smooth_pass_kernel<0><<<grid, 256, 0, st>>>(tmp1, V, nullptr, nullptr, W, H, D, tx, tmp2, V, 0);
+  smooth_pass_kernel<2><<<grid, 256, 0, st>>>(tmp2, V, nullptr, scert, W, H, D, tz, out, V, accumulate);
+  return cudaGetLastError();
+}
+
+}  // namespace brc

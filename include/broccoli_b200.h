@@ -1,0 +1,249 @@
+/*
+ * broccoli_b200.h -- C-ABI of the B200-native registration and filtering
+ * path of BROCCOLI (libbroccoli_b200.so).
+ *
+ * Plain C: opaque context, raw pointers, explicit sizes, int status codes.
+ * Every entry point below names the reference interface it replaces
+ * (file:line in the BROCCOLI source tree).  The reference exposes this path
+ * through the C++ class BROCCOLI_LIB (code/BROCCOLI_LIB/broccoli_lib.h:
+ * 108-467) running OpenCL kernels; the same class interface is provided on
+ * top of this ABI by include/broccoli_lib.h, and the Python package binds
+ * this ABI with ctypes.
+ *
+ * Conventions
+ *   - Volumes are float32, x fastest: index = x + y*W + z*W*H (+ t*W*H*D),
+ *     as in code/Kernels/kernelRegistration.cpp:32-40.
+ *   - A 7x7x7 complex filter is 686 floats: re[343] then im[343], x fastest.
+ *     A bank of n filters is n*686 floats.  Filters are always HOST pointers
+ *     (they are passed to the kernels by value).
+ *   - Complex responses are interleaved (re, im) float pairs; a bank of n
+ *     filters gives n consecutive complex volumes per instance.
+ *   - Registration parameters: 12 floats
+ *     [tx ty tz a11-1 a12 a13 a21 a22-1 a23 a31 a32 a33-1] in voxels,
+ *     origin at the volume centre ((W-1)/2, (H-1)/2, (D-1)/2).
+ *   - "d_" arguments are device pointers, "h_" host pointers.  All device
+ *     work is queued on the context's stream; functions that take host
+ *     buffers return after the results are back on the host.
+ *   - No exceptions; every function returns a brc_status.  Device-side
+ *     waits are bounded and report BRC_ERR_TIMEOUT instead of spinning.
+ */
+#ifndef BROCCOLI_B200_H
+#define BROCCOLI_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  BRC_OK = 0,
+  BRC_ERR_INVALID = -1,     /* bad size, null pointer, unknown option     */
+  BRC_ERR_NOMEM = -2,       /* device or pinned-host allocation failed    */
+  BRC_ERR_CUDA = -3,        /* CUDA runtime error; see brc_last_error()   */
+  BRC_ERR_TIMEOUT = -4,     /* a bounded device-side wait gave up         */
+  BRC_ERR_NODEVICE = -5,    /* no usable sm_100 device                    */
+  BRC_ERR_UNSUPPORTED = -6, /* option combination not implemented         */
+  BRC_ERR_NONFINITE = -7    /* a solve produced NaN/Inf (update dropped)  */
+} brc_status;
+
+/* Alignment types, same values as broccoli_constants.h:93-95. */
+enum { BRC_TRANSLATION = 0, BRC_RIGID = 1, BRC_AFFINE = 2 };
+
+/* Arithmetic of the 7^3 filtering.  FP32: plain fp32 FMA on the CUDA cores.
+ * BF16X3: split-bf16 (hi*hi + hi*lo + lo*hi) products on the tensor cores
+ * with fp32 accumulation. */
+enum { BRC_PREC_FP32 = 0, BRC_PREC_BF16X3 = 1 };
+
+typedef struct brc_ctx brc_ctx;
+
+/* ---- context ---------------------------------------------------------- */
+
+/* Replaces BROCCOLI_LIB::OpenCLInitiate (broccoli_lib.cpp:1181-1878):
+ * binds the context to CUDA device `device` and creates its stream. */
+int brc_ctx_create(int device, brc_ctx** out);
+int brc_ctx_destroy(brc_ctx* ctx);
+/* Queue the context's work on an existing cudaStream_t (e.g. torch's
+ * current stream).  NULL is the legacy default stream (stream 0), as in the
+ * CUDA runtime; BRC_OWN_STREAM returns to the context's own stream. */
+#define BRC_OWN_STREAM ((void*)-1)
+int brc_ctx_set_stream(brc_ctx* ctx, void* cuda_stream);
+void* brc_ctx_stream(brc_ctx* ctx);
+int brc_ctx_synchronize(brc_ctx* ctx);
+/* Bytes of device workspace the context currently holds. */
+size_t brc_ctx_workspace_bytes(const brc_ctx* ctx);
+/* Number of kernels this context has launched so far (graph replays count
+ * every kernel node).  Used by benchmarks to report launch counts. */
+unsigned long long brc_ctx_kernel_launches(const brc_ctx* ctx);
+/* Replaces GetOpenCLErrorMessage / the INITIALIZATION_ERROR getters
+ * (broccoli_lib.h:399-413). */
+const char* brc_status_string(int status);
+const char* brc_last_error(const brc_ctx* ctx);
+/* Library version string. */
+const char* brc_version(void);
+
+/* ---- kernel-level entry points (device pointers, asynchronous) --------- */
+
+/* Complex 7x7x7 filtering with zero padding (a true convolution:
+ * q(x) = sum_d vol(x+d) F[3-d]) of `batch` volumes, each `vol_stride`
+ * floats apart.  out: batch x nfilt complex volumes (2*W*H*D floats each).
+ * nfilt is 3 (linear) or 6 (nonlinear).
+ * Replaces NonseparableConvolution3D (broccoli_lib.cpp:4974-5027) and
+ * Nonseparable3DConvolutionComplexThreeQuadratureFilters*
+ * (kernelConvolution.cpp:2802-3693). */
+int brc_filter3d(brc_ctx* ctx, const float* d_vol, int W, int H, int D, int batch,
+                 long long vol_stride, const float* h_filters, int nfilt, int precision,
+                 float* d_out);
+
+/* Normal equations of the affine registration step from reference
+ * responses d_q1 and aligned-volume responses d_q2 (3 complex volumes
+ * each per instance; q1_stride = 0 shares one reference across the batch).
+ * Outputs the full symmetric 12x12 A (column-major) and h per instance in
+ * double precision.
+ * Replaces CalculatePhaseDifferencesAndCertainties, CalculatePhaseGradients
+ * X/Y/Z, CalculateAMatrixAndHVector2DValuesX/Y/Z, CalculateAMatrix1DValues,
+ * CalculateHVector1DValues, CalculateAMatrix, CalculateHVector
+ * (kernelRegistration.cpp:173-800) as driven at broccoli_lib.cpp:5315-5392. */
+int brc_normal_equations(brc_ctx* ctx, const float* d_q1, long long q1_stride,
+                         const float* d_q2, int W, int H, int D, int batch,
+                         double* d_A, double* d_h);
+
+/* p = A^-1 h per instance in double, rounded to float.
+ * Replaces SolveEquationSystem (broccoli_lib.cpp:17157-17186). */
+int brc_solve_affine_fp64(brc_ctx* ctx, const double* d_A, const double* d_h, int batch,
+                          float* d_p);
+
+/* Trilinear (exact-weight, clamp-to-edge) warp of `batch` volumes by their
+ * own 12-parameter affine transforms (d_params: batch x 12).
+ * Replaces InterpolateVolumeLinearLinear (kernelRegistration.cpp:1066-1101). */
+int brc_warp_affine(brc_ctx* ctx, const float* d_src, int W, int H, int D, int batch,
+                    const float* d_params, float* d_out);
+
+/* Warp by a displacement field (three volumes, voxels).
+ * Replaces InterpolateVolumeLinearNonLinear (kernelRegistration.cpp:
+ * 1111-1140). */
+int brc_warp_field(brc_ctx* ctx, const float* d_src, int W, int H, int D,
+                   const float* d_dx, const float* d_dy, const float* d_dz, float* d_out);
+
+/* Separable 9-tap smoothing of `batch` volumes: along y of vol*cert, along
+ * x, along z divided by the smoothed certainty (d_cert / d_smoothed_cert
+ * may be NULL for all-ones).  Filters are host arrays of 9 taps.
+ * Replaces PerformSmoothing (broccoli_lib.cpp:11274-11357, :11461-11545)
+ * and SeparableConvolutionRows/Columns/Rods (kernelConvolution.cpp:
+ * 52-1665). */
+int brc_smooth3d(brc_ctx* ctx, const float* d_vol, int W, int H, int D, int batch,
+                 const float* h_fx, const float* h_fy, const float* h_fz,
+                 const float* d_cert, const float* d_smoothed_cert, float* d_out);
+
+/* Linear resample to a new grid size, sample spacing (N-1)/(N'-1).
+ * Replaces ChangeVolumeSize (broccoli_lib.cpp:6247-6388) with
+ * RescaleVolumeLinear (kernelRegistration.cpp:1340-1366). */
+int brc_rescale_linear(brc_ctx* ctx, const float* d_src, int W, int H, int D,
+                       float* d_out, int W2, int H2, int D2);
+
+/* ---- whole-path entry points ------------------------------------------ */
+
+typedef struct {
+  int iterations;        /* maximum iterations per instance               */
+  int type;              /* BRC_TRANSLATION / BRC_RIGID / BRC_AFFINE       */
+  int precision;         /* BRC_PREC_FP32 / BRC_PREC_BF16X3                */
+  float tolerance;       /* early exit when the largest displacement of an
+                            update over the volume corners is below this
+                            (voxels); 0 = always run all iterations        */
+  int use_graph;         /* capture the iteration loop in a CUDA graph     */
+  int certainty_sigma_x100; /* >0: Gaussian smoothing (3x3x3 taps, sigma
+                            = value/100 voxels) of the phase certainties
+                            before the reductions; 0 = reference behaviour */
+} brc_linear_opts;
+
+/* Fill `opts` with the reference defaults (AFFINE, FP32, no early exit,
+ * graph on, no certainty smoothing, `iterations` iterations). */
+void brc_linear_opts_default(brc_linear_opts* opts, int iterations);
+
+/* Batched single-scale linear registration of `batch` moving volumes to
+ * reference volume(s) (ref_stride = 0: one shared reference).  All
+ * instances run together; an instance whose update falls below the
+ * tolerance stops updating (its convergence mask bit is set).
+ * d_params (batch x 12) receives the total parameters, d_aligned (batch
+ * volumes, may be NULL) the final warped volumes, d_rotations (batch x 3,
+ * may be NULL; RIGID) the Euler angles in degrees, d_iterations (batch,
+ * may be NULL) the iterations each instance ran.
+ * Replaces AlignTwoVolumesLinear (broccoli_lib.cpp:5273-5437) called once
+ * per volume, with its Setup/Cleanup (:5072-5266, :6670-6726). */
+int brc_register_linear_batched(brc_ctx* ctx, const float* d_ref, long long ref_stride,
+                                const float* d_moving, int W, int H, int D, int batch,
+                                const float* h_filters, const brc_linear_opts* opts,
+                                float* d_params, float* d_aligned, float* d_rotations,
+                                int* d_iterations);
+
+/* Rigid motion correction of a T-volume series (host buffers) to volume 0,
+ * or to h_reference when it is not NULL.  h_volumes is replaced in place by
+ * the corrected series (volume 0 unchanged when it is the reference);
+ * h_motion (6*T, may be NULL) receives translations in mm (voxels times
+ * voxel size) then rotations in degrees, laid out [t + k*T].
+ * Replaces PerformMotionCorrectionWrapper (broccoli_lib.cpp:10658-10720). */
+int brc_motion_correct(brc_ctx* ctx, float* h_volumes, int W, int H, int D, int T,
+                       const float* voxel_size3, const float* h_filters,
+                       const brc_linear_opts* opts, const float* h_reference,
+                       float* h_motion);
+
+/* Multi-scale (pyramid) linear registration of a batch to one shared
+ * reference: volumes resampled to round(N/scale) for scale = coarsest,
+ * coarsest/2, ..., 1; each scale registers the resampled moving volume
+ * pre-warped by the total so far; totals carried with doubled translations;
+ * the finest scale runs ceil(iterations/5) iterations; rotations (RIGID)
+ * summed over scales.  d_aligned (batch volumes, full size) receives the
+ * moving volumes warped by the total parameters.
+ * Replaces AlignTwoVolumesLinearSeveralScales (broccoli_lib.cpp:6391-6513)
+ * with ChangeVolumeSize (:6247-6388) and
+ * AddAffineRegistrationParametersNextScale (:7344-7431). */
+int brc_register_linear_scales(brc_ctx* ctx, const float* d_ref, const float* d_moving, int W, int H,
+                               int D, int batch, const float* h_filters, const brc_linear_opts* opts,
+                               int coarsest_scale, float* d_params, float* d_aligned,
+                               float* d_rotations);
+
+/* ---- nonlinear (displacement field) registration ----------------------- */
+
+typedef struct {
+  int iterations;      /* iterations per scale (finest: ceil(iterations/2)) */
+  int coarsest_scale;  /* 1, 2, 4, 8 or 16                                  */
+  float tsigma;        /* smoothing of the structure tensor (voxels)        */
+  float esigma;        /* smoothing of A and h (voxels)                     */
+  float dsigma;        /* smoothing of the field update (voxels)            */
+  int precision;       /* BRC_PREC_FP32 / BRC_PREC_BF16X3 (filtering)        */
+  int solve_fp64;      /* 0: FP32 cofactors + 1e-16 (reference); 1: FP64    */
+} brc_nonlinear_opts;
+
+/* Defaults of SetStartValues (broccoli_lib.cpp:325-355): sigmas 5,
+ * coarsest scale 1, FP32, reference solve. */
+void brc_nonlinear_opts_default(brc_nonlinear_opts* opts, int iterations);
+
+/* One nonlinear update from given responses (d_q1: reference, d_q2:
+ * aligned; 6 complex volumes each): structure tensor of q2 with projection
+ * tensors h_tensors (6 x {m11 m12 m13 m22 m23 m33}), tensor smoothing,
+ * norm (kept in a11) and max normalisation, per-voxel A and h over the six
+ * filters with directions h_dirs (x[6] y[6] z[6]), their smoothing, the 3x3
+ * solve, and the smoothed update ADDED to d_field (3 volumes x, y, z).
+ * Replaces the loop body of AlignTwoVolumesNonLinear (broccoli_lib.cpp:
+ * 5784-6025): CalculateTensorComponents, CalculateTensorNorms,
+ * CalculateAMatricesAndHVectors, CalculateDisplacementUpdate
+ * (kernelRegistration.cpp:806-988), CalculateMax (:10889), MultiplyVolume,
+ * AddVolumes and PerformSmoothing. */
+int brc_nonlinear_step(brc_ctx* ctx, const float* d_q1, const float* d_q2, int W, int H, int D,
+                       const float* h_tensors, const float* h_dirs, float tsigma, float esigma,
+                       float dsigma, int solve_fp64, float* d_field);
+
+/* Multi-scale nonlinear registration of d_moving to d_ref with six filters
+ * (h_filters6: 6 x 686 floats).  d_field (3 volumes) receives the total
+ * displacement field, d_aligned the moving volume warped by it.
+ * Replaces AlignTwoVolumesNonLinearSeveralScales (broccoli_lib.cpp:
+ * 6516-6665) and AlignTwoVolumesNonLinear (:5748-6058). */
+int brc_register_nonlinear(brc_ctx* ctx, const float* d_ref, const float* d_moving, int W, int H,
+                           int D, const float* h_filters6, const float* h_tensors,
+                           const float* h_dirs, const brc_nonlinear_opts* opts, float* d_field,
+                           float* d_aligned);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

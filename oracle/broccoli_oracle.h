@@ -62,7 +62,28 @@ enum { ORC_TRANSLATION = 0, ORC_RIGID = 1, ORC_AFFINE = 2 };
                          const real* fx, const real* fy, const real* fz,        \
                          real* out);                                            \
   void orc_rescale_linear##SFX(const real* src, int W, int H, int D, int W2,    \
-                               int H2, int D2, real* out);
+                               int H2, int D2, real* out);                      \
+  void orc_align_linear_scales##SFX(const real* ref, real* aligned, int W,      \
+                                    int H, int D, int coarsest,                 \
+                                    const real* filters, int niter, int type,   \
+                                    real* p12, real* rot3);                     \
+  void orc_tensor_components##SFX(const real* q2, long V, const real* m6,       \
+                                  real* t6);                                    \
+  void orc_tensor_norms##SFX(const real* t6, long V, real* norm);               \
+  void orc_nonlinear_ah##SFX(const real* q1, const real* q2, const real* t6,    \
+                             long V, real nx, real ny, real nz, real* a6,       \
+                             real* h3);                                         \
+  void orc_displacement_update##SFX(const real* a6, const real* h3, long V,     \
+                                    real* d3);                                  \
+  void orc_align_nonlinear##SFX(const real* ref, real* aligned,                 \
+                                const real* original, int W, int H, int D,      \
+                                const real* filters6, const real* tensors,      \
+                                const real* dirs, int niter, double tsigma,     \
+                                double esigma, double dsigma, real* field);     \
+  void orc_align_nonlinear_scales##SFX(                                         \
+      const real* ref, real* aligned, int W, int H, int D, int coarsest,        \
+      const real* filters6, const real* tensors, const real* dirs, int niter,   \
+      double tsigma, double esigma, double dsigma, real* field);
 
 ORC_DECLARE(float, _f32)
 ORC_DECLARE(double, _f64)

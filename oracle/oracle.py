@@ -236,9 +236,79 @@ def rescale_linear(src: np.ndarray, shape, prec: str = "f32") -> np.ndarray:
     return out
 
 
+def align_linear_scales(ref: np.ndarray, moving: np.ndarray, filters: np.ndarray, niter: int,
+                        coarsest: int, type_: int = AFFINE, prec: str = "f32"):
+    """Multi-scale linear registration.  Returns (params12, aligned, rot3)."""
+    dt, s = _dt(prec)
+    D, H, W = ref.shape
+    r = _arr(ref, dt)
+    aligned = _arr(moving, dt).copy()
+    f = _arr(filters, dt)
+    p = np.zeros(12, dt)
+    rot = np.zeros(3, dt)
+    getattr(orc_lib(), "orc_align_linear_scales" + s)(_ptr(r), _ptr(aligned), W, H, D, coarsest, _ptr(f),
+                                                      niter, type_, _ptr(p), _ptr(rot))
+    return p, aligned, rot
+
+
+def _nl_args(bank: dict, dt):
+    f6 = _arr(bank["nonlinear"], dt)
+    m = _arr(bank["projection_tensors"], dt)
+    d = _arr(bank["directions"], dt)
+    return f6, m, d
+
+
+def align_nonlinear(ref: np.ndarray, moving: np.ndarray, bank: dict, niter: int, tsigma=5.0,
+                    esigma=5.0, dsigma=5.0, prec: str = "f32"):
+    """Single-scale nonlinear registration.  `bank` is the dict of
+    broccoli_b200.filters.load_filter_dir.  Returns (field (3,D,H,W),
+    aligned)."""
+    dt, s = _dt(prec)
+    D, H, W = ref.shape
+    r = _arr(ref, dt)
+    orig = _arr(moving, dt).copy()
+    aligned = orig.copy()
+    f6, m, d = _nl_args(bank, dt)
+    field = np.zeros((3, D, H, W), dt)
+    fn = getattr(orc_lib(), "orc_align_nonlinear" + s)
+    fn.argtypes = [_P, _P, _P, _I, _I, _I, _P, _P, _P, _I, _D, _D, _D, _P]
+    fn(_ptr(r), _ptr(aligned), _ptr(orig), W, H, D, _ptr(f6), _ptr(m), _ptr(d), niter, tsigma, esigma,
+       dsigma, _ptr(field))
+    return field, aligned
+
+
+def align_nonlinear_scales(ref: np.ndarray, moving: np.ndarray, bank: dict, niter: int, coarsest: int,
+                           tsigma=5.0, esigma=5.0, dsigma=5.0, prec: str = "f32"):
+    dt, s = _dt(prec)
+    D, H, W = ref.shape
+    r = _arr(ref, dt)
+    aligned = _arr(moving, dt).copy()
+    f6, m, d = _nl_args(bank, dt)
+    field = np.zeros((3, D, H, W), dt)
+    fn = getattr(orc_lib(), "orc_align_nonlinear_scales" + s)
+    fn.argtypes = [_P, _P, _I, _I, _I, _I, _P, _P, _P, _I, _D, _D, _D, _P]
+    fn(_ptr(r), _ptr(aligned), W, H, D, coarsest, _ptr(f6), _ptr(m), _ptr(d), niter, tsigma, esigma,
+       dsigma, _ptr(field))
+    return field, aligned
+
+
 # --------------------------------------------------------------------------
 # the reference's own kernels (oracle/_ref/libbroccoli_ref.so), float only
 # --------------------------------------------------------------------------
+
+def ref_align_nonlinear(ref: np.ndarray, moving: np.ndarray, bank: dict, niter: int, tsigma=5.0,
+                        esigma=5.0, dsigma=5.0):
+    D, H, W = ref.shape
+    r = _arr(ref, np.float32)
+    orig = _arr(moving, np.float32).copy()
+    aligned = orig.copy()
+    f6, m, d = _nl_args(bank, np.float32)
+    field = np.zeros((3, D, H, W), np.float32)
+    fn = ref_lib().ref_align_nonlinear
+    fn.argtypes = [_P, _P, _P, _I, _I, _I, _P, _P, _P, _I, _D, _D, _D, _P]
+    fn(_ptr(r), _ptr(aligned), _ptr(orig), W, H, D, _ptr(f6), _ptr(m), _ptr(d), niter, tsigma, esigma,
+       dsigma, _ptr(field))
+    return field, aligned
 
 def ref_filter3d(vol: np.ndarray, filters: np.ndarray) -> np.ndarray:
     D, H, W = vol.shape

@@ -676,6 +676,276 @@ void FN(orc_rescale_linear)(const REAL* src, int W, int H, int D, int W2,
             src, W, H, D, (REAL)x * dx + RHALF, (REAL)y * dy + RHALF, (REAL)z * dz + RHALF);
 }
 
+/* myround, broccoli_lib.cpp:94-97. */
+static int FN(orc_myround)(float a) { return (int)floorf(a + 0.5f); }
+
+/* Multi-scale linear registration.  AlignTwoVolumesLinearSeveralScales,
+ * broccoli_lib.cpp:6391-6513: both volumes are resampled to
+ * round(N/scale) per axis; at every scale after the coarsest the resampled
+ * moving volume is first warped with the total parameters found so far and
+ * that warped copy is what the scale registers; the coarse-scale totals are
+ * carried to the next scale with doubled translations
+ * (AddAffineRegistrationParametersNextScale); the finest scale runs
+ * ceil(niter/5) iterations; the rotations of all scales are summed.  On
+ * return `aligned` (full size) is the moving volume warped by the total
+ * parameters (the DO_OVERWRITE behaviour). */
+void FN(orc_align_linear_scales)(const REAL* ref, REAL* aligned, int W, int H, int D,
+                                 int coarsest, const REAL* filters, int niter, int type,
+                                 REAL* p12, REAL* rot3) {
+  const long V = (long)W * H * D;
+  REAL* orig_full = (REAL*)malloc(sizeof(REAL) * V);
+  for (long i = 0; i < V; i++) orig_full[i] = aligned[i];
+  REAL tmp[12], rt[3] = {RZERO, RZERO, RZERO};
+  for (int i = 0; i < 12; i++) p12[i] = RZERO;
+  if (rot3) rot3[0] = rot3[1] = rot3[2] = RZERO;
+  int cw = FN(orc_myround)((float)W / (float)coarsest);
+  int ch = FN(orc_myround)((float)H / (float)coarsest);
+  int cd = FN(orc_myround)((float)D / (float)coarsest);
+  REAL* r_s = (REAL*)malloc(sizeof(REAL) * V);
+  REAL* o_s = (REAL*)malloc(sizeof(REAL) * V);
+  REAL* a_s = (REAL*)malloc(sizeof(REAL) * V);
+  FN(orc_rescale_linear)(orig_full, W, H, D, cw, ch, cd, o_s);
+  FN(orc_rescale_linear)(ref, W, H, D, cw, ch, cd, r_s);
+  for (int scale = coarsest; scale >= 1; scale /= 2) {
+    const long vs = (long)cw * ch * cd;
+    for (long i = 0; i < vs; i++) a_s[i] = o_s[i];
+    const int it = scale == 1 ? (int)ceilf((float)niter / 5.0f) : niter;
+    FN(orc_align_linear)(r_s, a_s, o_s, cw, ch, cd, filters, it, type, tmp, rt);
+    if (type != ORC_RIGID) rt[0] = rt[1] = rt[2] = RZERO;
+    if (scale != 1) {
+      if (rot3) {
+        rot3[0] += rt[0];
+        rot3[1] += rt[1];
+        rot3[2] += rt[2];
+      }
+      FN(orc_add_affine_next_scale)(p12, tmp);
+      cw = FN(orc_myround)((float)W / ((float)scale / 2.0f));
+      ch = FN(orc_myround)((float)H / ((float)scale / 2.0f));
+      cd = FN(orc_myround)((float)D / ((float)scale / 2.0f));
+      REAL* resc = (REAL*)malloc(sizeof(REAL) * (long)cw * ch * cd);
+      FN(orc_rescale_linear)(orig_full, W, H, D, cw, ch, cd, resc);
+      FN(orc_rescale_linear)(ref, W, H, D, cw, ch, cd, r_s);
+      FN(orc_warp_affine)(resc, cw, ch, cd, p12, o_s);
+      free(resc);
+    } else {
+      FN(orc_add_affine)(p12, tmp);
+      if (rot3) {
+        rot3[0] += rt[0];
+        rot3[1] += rt[1];
+        rot3[2] += rt[2];
+      }
+      FN(orc_warp_affine)(orig_full, W, H, D, p12, aligned);
+    }
+  }
+  free(orig_full);
+  free(r_s);
+  free(o_s);
+  free(a_s);
+}
+
+/* Structure tensor of the aligned volume: T = sum_k |q2_k| M_k, with M_k
+ * the projection tensor (m11 m12 m13 m22 m23 m33) of filter k.
+ * CalculateTensorComponents, kernelRegistration.cpp:806-845 (called once
+ * per filter, accumulating). */
+void FN(orc_tensor_components)(const REAL* q2, long V, const REAL* m6, REAL* t6) {
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < V; i++) {
+    const REAL mag = RSQRT(q2[2 * i] * q2[2 * i] + q2[2 * i + 1] * q2[2 * i + 1]);
+    for (int c = 0; c < 6; c++) t6[(long)c * V + i] += mag * m6[c];
+  }
+}
+
+/* Frobenius norm of the symmetric tensor.  CalculateTensorNorms,
+ * kernelRegistration.cpp:847-875. */
+void FN(orc_tensor_norms)(const REAL* t6, long V, REAL* norm) {
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < V; i++) {
+    const REAL a = t6[i], b = t6[V + i], c = t6[2 * V + i], d = t6[3 * V + i],
+               e = t6[4 * V + i], f = t6[5 * V + i];
+    norm[i] = RSQRT(a * a + (REAL)2.0 * b * b + (REAL)2.0 * c * c + d * d + (REAL)2.0 * e * e + f * f);
+  }
+}
+
+/* a += c TT and h += c dphi TT n for one filter, with TT = T T (symmetric)
+ * and c = sqrt|q1 q2*| cos^2(dphi/2).  CalculateAMatricesAndHVectors,
+ * kernelRegistration.cpp:880-943.  a6: a11 a12 a13 a22 a23 a33; h3. */
+void FN(orc_nonlinear_ah)(const REAL* q1, const REAL* q2, const REAL* t6, long V, REAL nx, REAL ny,
+                          REAL nz, REAL* a6, REAL* h3) {
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < V; i++) {
+    const REAL q1x = q1[2 * i], q1y = q1[2 * i + 1], q2x = q2[2 * i], q2y = q2[2 * i + 1];
+    const REAL qr = q1x * q2x + q1y * q2y;
+    const REAL qi = -q1x * q2y + q1y * q2x;
+    const REAL pd = RATAN2(qi, qr);
+    const REAL aqq = RSQRT(qr * qr + qi * qi);
+    const REAL cert = RSQRT(aqq) * RCOS(pd / (REAL)2.0) * RCOS(pd / (REAL)2.0);
+    const REAL t11 = t6[i], t12 = t6[V + i], t13 = t6[2 * V + i], t22 = t6[3 * V + i],
+               t23 = t6[4 * V + i], t33 = t6[5 * V + i];
+    const REAL tt11 = t11 * t11 + t12 * t12 + t13 * t13;
+    const REAL tt12 = t11 * t12 + t12 * t22 + t13 * t23;
+    const REAL tt13 = t11 * t13 + t12 * t23 + t13 * t33;
+    const REAL tt22 = t12 * t12 + t22 * t22 + t23 * t23;
+    const REAL tt23 = t12 * t13 + t22 * t23 + t23 * t33;
+    const REAL tt33 = t13 * t13 + t23 * t23 + t33 * t33;
+    a6[i] += cert * tt11;
+    a6[V + i] += cert * tt12;
+    a6[2 * V + i] += cert * tt13;
+    a6[3 * V + i] += cert * tt22;
+    a6[4 * V + i] += cert * tt23;
+    a6[5 * V + i] += cert * tt33;
+    h3[i] += cert * pd * (nx * tt11 + ny * tt12 + nz * tt13);
+    h3[V + i] += cert * pd * (nx * tt12 + ny * tt22 + nz * tt23);
+    h3[2 * V + i] += cert * pd * (nx * tt13 + ny * tt23 + nz * tt33);
+  }
+}
+
+/* Per-voxel 3x3 solve by cofactors with det + 1e-16.
+ * CalculateDisplacementUpdate, kernelRegistration.cpp:948-988. */
+void FN(orc_displacement_update)(const REAL* a6, const REAL* h3, long V, REAL* d3) {
+#pragma omp parallel for schedule(static)
+  for (long i = 0; i < V; i++) {
+    const REAL a11 = a6[i], a12 = a6[V + i], a13 = a6[2 * V + i], a22 = a6[3 * V + i],
+               a23 = a6[4 * V + i], a33 = a6[5 * V + i];
+    const REAL h1 = h3[i], h2 = h3[V + i], hh3 = h3[2 * V + i];
+    const REAL norm = RONE / (a11 * a22 * a33 - a11 * a23 * a23 - a12 * a12 * a33 + a12 * a23 * a13 +
+                              a13 * a12 * a23 - a13 * a22 * a13 + (REAL)1e-16);
+    d3[i] = norm * ((hh3 * (a12 * a23 - a13 * a22)) - (h2 * (a12 * a33 - a13 * a23)) +
+                    (h1 * (a22 * a33 - a23 * a23)));
+    d3[V + i] = norm * ((h2 * (a11 * a33 - a13 * a13)) - (hh3 * (a11 * a23 - a13 * a12)) -
+                        (h1 * (a12 * a33 - a23 * a13)));
+    d3[2 * V + i] = norm * ((hh3 * (a11 * a22 - a12 * a12)) - (h2 * (a11 * a23 - a12 * a13)) +
+                            (h1 * (a12 * a23 - a22 * a13)));
+  }
+}
+
+/* Nonlinear (displacement field) registration at one scale.
+ * AlignTwoVolumesNonLinear, broccoli_lib.cpp:5748-6058.  Per iteration:
+ * six responses of the aligned volume; structure tensor from their
+ * magnitudes; tensor smoothed (tsigma); tensor norm written into a11 (it
+ * stays there: a11 = norm + sum c tt11, the reference's accumulation); the
+ * tensor is divided by its largest norm (max from FLT_MIN); A and h from
+ * the six filter pairs; A, h smoothed (esigma); 3x3 solve per voxel;
+ * update smoothed (dsigma) and added to the field; the original re-warped
+ * by the field.  tensors: 6 x {m11 m12 m13 m22 m23 m33}; dirs: x[6] y[6]
+ * z[6]; field: 3 volumes (x, y, z), zeroed here. */
+void FN(orc_align_nonlinear)(const REAL* ref, REAL* aligned, const REAL* original, int W, int H,
+                             int D, const REAL* filters6, const REAL* tensors, const REAL* dirs,
+                             int niter, double tsigma, double esigma, double dsigma, REAL* field) {
+  const long V = (long)W * H * D;
+  REAL* q1 = (REAL*)malloc(sizeof(REAL) * 12 * V);
+  REAL* q2 = (REAL*)malloc(sizeof(REAL) * 12 * V);
+  REAL* t6 = (REAL*)malloc(sizeof(REAL) * 6 * V);
+  REAL* a6 = (REAL*)malloc(sizeof(REAL) * 6 * V);
+  REAL* h3 = (REAL*)malloc(sizeof(REAL) * 3 * V);
+  REAL* d3 = (REAL*)malloc(sizeof(REAL) * 3 * V);
+  REAL* tmp = (REAL*)malloc(sizeof(REAL) * V);
+  REAL ft[9], fe[9], fd[9];
+  FN(orc_smoothing_filter_sigma)(9, tsigma, ft);
+  FN(orc_smoothing_filter_sigma)(9, esigma, fe);
+  FN(orc_smoothing_filter_sigma)(9, dsigma, fd);
+  FN(orc_filter3d)(ref, W, H, D, filters6, 6, q1);
+  for (long i = 0; i < 3 * V; i++) field[i] = RZERO;
+  for (int it = 0; it < niter; it++) {
+    FN(orc_filter3d)(aligned, W, H, D, filters6, 6, q2);
+    for (long i = 0; i < 6 * V; i++) t6[i] = RZERO;
+    for (long i = 0; i < 6 * V; i++) a6[i] = RZERO;
+    for (long i = 0; i < 3 * V; i++) h3[i] = RZERO;
+    for (int k = 0; k < 6; k++) FN(orc_tensor_components)(q2 + (long)k * 2 * V, V, tensors + 6 * k, t6);
+    for (int c = 0; c < 6; c++) {
+      FN(orc_smooth3d)(t6 + (long)c * V, NULL, NULL, W, H, D, ft, ft, ft, tmp);
+      for (long i = 0; i < V; i++) t6[(long)c * V + i] = tmp[i];
+    }
+    FN(orc_tensor_norms)(t6, V, a6);
+    float mx = 1.17549435e-38f;
+    for (long i = 0; i < V; i++) mx = (float)a6[i] > mx ? (float)a6[i] : mx;
+    const REAL f = (REAL)(1.0f / mx);
+    for (long i = 0; i < 6 * V; i++) t6[i] = t6[i] * f;
+    for (int k = 0; k < 6; k++)
+      FN(orc_nonlinear_ah)(q1 + (long)k * 2 * V, q2 + (long)k * 2 * V, t6, V, dirs[k], dirs[6 + k],
+                           dirs[12 + k], a6, h3);
+    for (int c = 0; c < 6; c++) {
+      FN(orc_smooth3d)(a6 + (long)c * V, NULL, NULL, W, H, D, fe, fe, fe, tmp);
+      for (long i = 0; i < V; i++) a6[(long)c * V + i] = tmp[i];
+    }
+    for (int c = 0; c < 3; c++) {
+      FN(orc_smooth3d)(h3 + (long)c * V, NULL, NULL, W, H, D, fe, fe, fe, tmp);
+      for (long i = 0; i < V; i++) h3[(long)c * V + i] = tmp[i];
+    }
+    FN(orc_displacement_update)(a6, h3, V, d3);
+    for (int c = 0; c < 3; c++) {
+      FN(orc_smooth3d)(d3 + (long)c * V, NULL, NULL, W, H, D, fd, fd, fd, tmp);
+      for (long i = 0; i < V; i++) field[(long)c * V + i] = field[(long)c * V + i] + tmp[i];
+    }
+    FN(orc_warp_field)(original, W, H, D, field, field + V, field + 2 * V, aligned);
+  }
+  free(q1);
+  free(q2);
+  free(t6);
+  free(a6);
+  free(h3);
+  free(d3);
+  free(tmp);
+}
+
+/* Multi-scale nonlinear registration.  AlignTwoVolumesNonLinearSeveralScales,
+ * broccoli_lib.cpp:6516-6665: scales coarsest..1 (halving); each scale
+ * registers the resampled moving volume pre-warped by the total field so far
+ * (resampled to the scale and doubled, :6604-6611); the finest scale runs
+ * ceil(niter/2) iterations.  On return `field` (3 full-size volumes) is the
+ * total field and `aligned` the moving volume warped by it. */
+void FN(orc_align_nonlinear_scales)(const REAL* ref, REAL* aligned, int W, int H, int D,
+                                    int coarsest, const REAL* filters6, const REAL* tensors,
+                                    const REAL* dirs, int niter, double tsigma, double esigma,
+                                    double dsigma, REAL* field) {
+  const long V = (long)W * H * D;
+  REAL* orig_full = (REAL*)malloc(sizeof(REAL) * V);
+  for (long i = 0; i < V; i++) orig_full[i] = aligned[i];
+  int cw = FN(orc_myround)((float)W / (float)coarsest);
+  int ch = FN(orc_myround)((float)H / (float)coarsest);
+  int cd = FN(orc_myround)((float)D / (float)coarsest);
+  REAL* r_s = (REAL*)malloc(sizeof(REAL) * V);
+  REAL* o_s = (REAL*)malloc(sizeof(REAL) * V);
+  REAL* a_s = (REAL*)malloc(sizeof(REAL) * V);
+  REAL* tot = (REAL*)calloc(3 * V, sizeof(REAL));
+  REAL* upd = (REAL*)malloc(sizeof(REAL) * 3 * V);
+  REAL* tmp = (REAL*)malloc(sizeof(REAL) * 3 * V);
+  FN(orc_rescale_linear)(orig_full, W, H, D, cw, ch, cd, o_s);
+  FN(orc_rescale_linear)(ref, W, H, D, cw, ch, cd, r_s);
+  for (int scale = coarsest; scale >= 1; scale /= 2) {
+    const long vs = (long)cw * ch * cd;
+    for (long i = 0; i < vs; i++) a_s[i] = o_s[i];
+    const int it = scale == 1 ? (int)ceilf((float)niter / 2.0f) : niter;
+    FN(orc_align_nonlinear)(r_s, a_s, o_s, cw, ch, cd, filters6, tensors, dirs, it, tsigma, esigma,
+                            dsigma, upd);
+    for (int c = 0; c < 3; c++)
+      for (long i = 0; i < vs; i++) tot[c * vs + i] = tot[c * vs + i] + upd[c * vs + i];
+    if (scale != 1) {
+      const int pw = cw, ph = ch, pdp = cd;
+      cw = FN(orc_myround)((float)W / ((float)scale / 2.0f));
+      ch = FN(orc_myround)((float)H / ((float)scale / 2.0f));
+      cd = FN(orc_myround)((float)D / ((float)scale / 2.0f));
+      const long nv = (long)cw * ch * cd;
+      for (int c = 0; c < 3; c++) FN(orc_rescale_linear)(tot + c * (long)pw * ph * pdp, pw, ph, pdp, cw, ch, cd, tmp + c * nv);
+      for (long i = 0; i < 3 * nv; i++) tot[i] = tmp[i] * (REAL)2.0;
+      REAL* resc = (REAL*)malloc(sizeof(REAL) * nv);
+      FN(orc_rescale_linear)(orig_full, W, H, D, cw, ch, cd, resc);
+      FN(orc_rescale_linear)(ref, W, H, D, cw, ch, cd, r_s);
+      FN(orc_warp_field)(resc, cw, ch, cd, tot, tot + nv, tot + 2 * nv, o_s);
+      free(resc);
+    } else {
+      for (long i = 0; i < 3 * V; i++) field[i] = tot[i];
+      FN(orc_warp_field)(orig_full, W, H, D, field, field + V, field + 2 * V, aligned);
+    }
+  }
+  free(orig_full);
+  free(r_s);
+  free(o_s);
+  free(a_s);
+  free(tot);
+  free(upd);
+  free(tmp);
+}
+
 #undef RSQRT
 #undef RATAN2
 #undef RCOS

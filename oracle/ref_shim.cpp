@@ -8,7 +8,9 @@
 // Its outputs cross-check the C restatement in orc_impl.h and seed the golden
 // fixtures under tests/golden/.
 #include <Eigen/Dense>
+#include <cmath>
 #include <cstring>
+#include <limits>
 #include <vector>
 
 #include "clshim.hpp"
@@ -18,6 +20,12 @@ namespace clk {
 }
 namespace clr {
 #include "kernelRegistration_cl.cpp"
+}
+namespace clm {
+static inline void atomic_max(volatile int* p, int v) {
+  if (v > *p) *p = v;
+}
+#include "kernelMisc_cl.cpp"
 }
 
 namespace {
@@ -282,6 +290,99 @@ void ref_smooth3d(const float* vol, const float* cert, const float* scert, int W
           [&] { clk::SeparableConvolutionColumnsGlobalMemory(cols.data(), rows.data(), fx, 0, W, H, D, 1); });
   ndrange(gx, gy, D, 16, 16, 1,
           [&] { clk::SeparableConvolutionRodsGlobalMemory(out, cols.data(), sc, fz, 0, W, H, D, 1); });
+}
+
+static void smooth_inplace(float* vol, int W, int H, int D, const float* f) {
+  const long V = (long)W * H * D;
+  std::vector<float> out(V);
+  ref_smooth3d(vol, nullptr, nullptr, W, H, D, f, f, f, out.data());
+  std::memcpy(vol, out.data(), sizeof(float) * V);
+}
+
+static void smoothing_filter(double sigma, float* f) {
+  // CreateSmoothingFilters(..., double sigma), broccoli_lib.cpp:11093-11121
+  const double s2 = 2.0 * sigma * sigma;
+  float sum = 0.0f;
+  for (int i = 0; i < 9; i++) {
+    const double u = (double)(i - 4);
+    f[i] = (float)exp(-pow(u, 2.0) / s2);
+    sum += f[i];
+  }
+  for (int i = 0; i < 9; i++) f[i] /= sum;
+}
+
+// AlignTwoVolumesNonLinear, broccoli_lib.cpp:5748-6058, with the
+// reference's kernels (kernelRegistration.cpp:806-988, kernelMisc.cpp
+// CalculateColumnMaxs/RowMaxs, AddVolumes, MultiplyVolume) and the host max
+// of CalculateMax (broccoli_lib.cpp:10889-10928).  field: 3 volumes.
+void ref_align_nonlinear(const float* ref, float* aligned, const float* original, int W, int H,
+                         int D, const float* filters6, const float* tensors, const float* dirs,
+                         int niter, double tsigma, double esigma, double dsigma, float* field) {
+  const long V = (long)W * H * D;
+  std::vector<float> q1(12 * V), q2(12 * V), t(6 * V), a(6 * V), h(3 * V), d(3 * V), tmp(V);
+  std::vector<float> colmax((long)H * D), maxs(D);
+  ref_filter3d(ref, W, H, D, filters6, q1.data());
+  ref_filter3d(ref, W, H, D, filters6 + 3 * 686, q1.data() + 6 * V);
+  std::memset(field, 0, sizeof(float) * 3 * V);
+  float ft[9], fe[9], fd[9];
+  smoothing_filter(tsigma, ft);
+  smoothing_filter(esigma, fe);
+  smoothing_filter(dsigma, fd);
+  const int gx = roundup(W, 16), gy = roundup(H, 16);
+  const float2* Q1 = reinterpret_cast<const float2*>(q1.data());
+  const float2* Q2 = reinterpret_cast<const float2*>(q2.data());
+  float *t11 = t.data(), *t12 = t11 + V, *t13 = t12 + V, *t22 = t13 + V, *t23 = t22 + V, *t33 = t23 + V;
+  float *a11 = a.data(), *a12 = a11 + V, *a13 = a12 + V, *a22 = a13 + V, *a23 = a22 + V, *a33 = a23 + V;
+  float *h1 = h.data(), *h2 = h1 + V, *h3 = h2 + V;
+  float *dx = d.data(), *dy = dx + V, *dz = dy + V;
+  const image3d_t im{original, W, H, D};
+  for (int it = 0; it < niter; it++) {
+    ref_filter3d(aligned, W, H, D, filters6, q2.data());
+    ref_filter3d(aligned, W, H, D, filters6 + 3 * 686, q2.data() + 6 * V);
+    std::fill(t.begin(), t.end(), 0.f);
+    std::fill(a.begin(), a.end(), 0.f);
+    std::fill(h.begin(), h.end(), 0.f);
+    for (int k = 0; k < 6; k++) {
+      const float* m = tensors + 6 * k;
+      ndrange(gx, gy, D, 16, 16, 1, [&] {
+        clr::CalculateTensorComponents(t11, t12, t13, t22, t23, t33, Q1 + k * V, Q2 + k * V, m[0], m[1],
+                                       m[2], m[3], m[4], m[5], W, H, D);
+      });
+    }
+    ndrange(gx, gy, D, 16, 16, 1, [&] { clr::CalculateTensorNorms(a11, t11, t12, t13, t22, t23, t33, W, H, D); });
+    for (int c = 0; c < 6; c++) smooth_inplace(t.data() + c * V, W, H, D, ft);
+    ndrange(gx, gy, D, 16, 16, 1, [&] { clr::CalculateTensorNorms(a11, t11, t12, t13, t22, t23, t33, W, H, D); });
+    ndrange(roundup(H, 16), roundup(D, 16), 1, 16, 16, 1,
+            [&] { clm::CalculateColumnMaxs(colmax.data(), a11, W, H, D); }, false);
+    ndrange(roundup(D, 16), 1, 1, 16, 1, 1, [&] { clm::CalculateRowMaxs(maxs.data(), colmax.data(), H, D); }, false);
+    float mx = std::numeric_limits<float>::min();
+    for (int z = 0; z < D; z++) mx = clm::mymax(mx, maxs[z]);
+    const float f = 1.0f / mx;
+    for (int c = 0; c < 6; c++) {
+      float* tc = t.data() + c * V;
+      ndrange(gx, gy, D, 16, 16, 1, [&] { clm::MultiplyVolume(tc, f, W, H, D); });
+    }
+    for (int k = 0; k < 6; k++) {
+      ndrange(gx, gy, D, 16, 16, 1, [&] {
+        clr::CalculateAMatricesAndHVectors(a11, a12, a13, a22, a23, a33, h1, h2, h3, Q1 + k * V, Q2 + k * V,
+                                           t11, t12, t13, t22, t23, t33, dirs, dirs + 6, dirs + 12, W, H, D, k);
+      });
+    }
+    for (int c = 0; c < 6; c++) smooth_inplace(a.data() + c * V, W, H, D, fe);
+    for (int c = 0; c < 3; c++) smooth_inplace(h.data() + c * V, W, H, D, fe);
+    ndrange(gx, gy, D, 16, 16, 1, [&] {
+      clr::CalculateDisplacementUpdate(dx, dy, dz, a11, a12, a13, a22, a23, a33, h1, h2, h3, W, H, D);
+    });
+    for (int c = 0; c < 3; c++) {
+      smooth_inplace(d.data() + c * V, W, H, D, fd);
+      float* fc = field + c * V;
+      const float* dc = d.data() + c * V;
+      ndrange(gx, gy, D, 16, 16, 1, [&] { clm::AddVolumesOverwrite(fc, dc, W, H, D); });
+    }
+    ndrange(gx, gy, D, 16, 16, 1, [&] {
+      clr::InterpolateVolumeLinearNonLinear(aligned, im, field, field + V, field + 2 * V, W, H, D, 0);
+    });
+  }
 }
 
 }  // extern "C"

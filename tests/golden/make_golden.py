@@ -1,0 +1,100 @@
+"""Generates the golden fixtures of this directory from the reference itself.
+
+Run in a tree where the BROCCOLI sources are present (default
+/root/reference, override with BROCCOLI_REF):
+
+    python tests/golden/make_golden.py
+
+1. Copies the reference's shipped filter coefficients (``filters/*.bin``:
+   quadrature filters, projection tensors, filter directions) into
+   ``tests/golden/filters/`` -- they are input data of the path.
+2. Builds ``oracle/_ref`` (the reference's own OpenCL C kernels compiled for
+   the CPU, see oracle/ref_shim.cpp) and records its outputs on small seeded
+   inputs into ``golden_small.npz``: filter responses, normal equations,
+   solve, rigid projection, composition, angles, warps, smoothing, rescale,
+   full single-scale registrations of every type and a short motion
+   correction.
+
+The reference ships no output vectors for this path; these fixtures are the
+reference's kernels run here on fixed inputs, and the inputs are stored with
+them so the tests never regenerate data.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.abspath(os.path.join(HERE, "..", ".."))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import oracle as O  # noqa: E402
+from broccoli_b200 import filters as F  # noqa: E402
+from broccoli_b200 import synthetic as S  # noqa: E402
+
+REF = os.environ.get("BROCCOLI_REF", "/root/reference")
+
+
+def main() -> None:
+    src = os.path.join(REF, "filters")
+    dst = os.path.join(HERE, "filters")
+    os.makedirs(dst, exist_ok=True)
+    for name in sorted(os.listdir(src)):
+        if name.endswith(".bin"):
+            shutil.copyfile(os.path.join(src, name), os.path.join(dst, name))
+
+    os.environ.setdefault("REF", REF)
+    O.build(ref=True)
+    bank = F.load_filter_dir(dst)
+    flt = bank["linear"]
+
+    g = {}
+    shape = (20, 24, 22)  # D, H, W -- odd/even mix, not tile multiples
+    base, moved, truth = S.affine_pair(shape, base_seed=0, motion_seed=1)
+    g["base"], g["moved"], g["truth"] = base, moved, truth
+    q1 = O.ref_filter3d(base, flt)
+    q2 = O.ref_filter3d(moved, flt)
+    g["q1"], g["q2"] = q1.astype(np.complex64), q2.astype(np.complex64)
+    A, h = O.ref_normal_equations(q1, q2)
+    g["A"], g["h"] = A, h
+    p = O.ref_solve(A, h)
+    g["p_solve"] = p
+    g["p_rigid"] = O.ref_remove_scaling(p)
+    g["p_compose"] = O.ref_add_affine(p, 0.5 * p)
+    g["rot"] = O.ref_rotation_angles(g["p_rigid"])
+    g["warp_affine"] = O.ref_warp_affine(moved, p)
+    rng = np.random.Generator(np.random.PCG64(7))
+    fld = [(rng.standard_normal(shape) * 2.0).astype(np.float32) for _ in range(3)]
+    g["field_x"], g["field_y"], g["field_z"] = fld
+    g["warp_field"] = O.ref_warp_field(moved, *fld)
+    fs = O.smoothing_filter_sigma(2.0)
+    g["smooth_filter"] = fs
+    g["smooth"] = O.ref_smooth3d(moved, fs, fs, fs)
+    cert = (rng.uniform(0.2, 1.0, shape)).astype(np.float32)
+    scert = O.ref_smooth3d(cert, fs, fs, fs)
+    g["cert"], g["smooth_cert"] = cert, scert
+    g["smooth_normalized"] = O.ref_smooth3d(moved, fs, fs, fs, cert=cert, smoothed_cert=scert)
+    g["rescale"] = O.ref_rescale_linear(moved, (11, 13, 17))
+    for typ, name in ((0, "translation"), (1, "rigid"), (2, "affine")):
+        pp, al, rr = O.ref_align_linear(base, moved, flt, 10, typ)
+        g[f"align_{name}_p"] = pp
+        g[f"align_{name}_vol"] = al
+        if rr is not None:
+            g[f"align_{name}_rot"] = rr
+
+    series, _ = S.motion_series(T=4, shape=(14, 18, 16), snr=50.0)
+    g["mc_series"] = series
+    g["mc_voxel"] = np.array([3.0, 3.0, 3.5], np.float32)
+    corr, motion = O.ref_motion_correct(series, g["mc_voxel"], flt, 5)
+    g["mc_corrected"], g["mc_motion"] = corr, motion
+
+    np.savez_compressed(os.path.join(HERE, "golden_small.npz"), **g)
+    print("wrote", os.path.join(HERE, "golden_small.npz"), "with", len(g), "arrays")
+
+
+if __name__ == "__main__":
+    main()

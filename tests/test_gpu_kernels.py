@@ -1,0 +1,115 @@
+"""Kernel-level parity of the CUDA path (through the C-ABI) with the oracle
+and with the golden fixtures made by the reference's own kernels.
+
+Tolerance (FP32 parity, the reference's 1e-4 relative): for every volume
+output, max |gpu - ref| <= 1e-4 * max |ref| (norm-wise relative error)."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_err
+from broccoli_b200 import filters as F
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-4
+
+
+def cuda(a):
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).cuda()
+
+
+def test_filter_matches_golden(ctx, golden, lin_filters):
+    q = ctx.filter3d(cuda(np.stack([golden["base"], golden["moved"]])), lin_filters).cpu().numpy()
+    assert rel_err(q[0], golden["q1"]) < TOL
+    assert rel_err(q[1], golden["q2"]) < TOL
+
+
+@pytest.mark.parametrize("shape", [(5, 17, 33), (11, 9, 7), (9, 40, 65), (33, 64, 64), (4, 3, 2)])
+@pytest.mark.parametrize("nf", [3, 6])
+def test_filter_odd_shapes_vs_oracle(ctx, orc, bank, shape, nf):
+    rng = np.random.default_rng(sum(shape) + nf)
+    vol = (rng.standard_normal(shape) * 50 + 100).astype(np.float32)
+    flt = bank["linear"] if nf == 3 else bank["nonlinear"]
+    ref = orc.filter3d(vol, flt)
+    got = ctx.filter3d(cuda(vol), flt).cpu().numpy()[0]
+    assert got.shape == ref.shape
+    assert rel_err(got, ref) < TOL
+
+
+def test_filter_batch_matches_single(ctx, lin_filters):
+    rng = np.random.default_rng(5)
+    vols = rng.standard_normal((4, 9, 12, 20)).astype(np.float32)
+    qb = ctx.filter3d(cuda(vols), lin_filters).cpu().numpy()
+    for b in range(4):
+        qs = ctx.filter3d(cuda(vols[b]), lin_filters).cpu().numpy()[0]
+        assert np.array_equal(qb[b], qs)
+
+
+def test_lognormal_filters_are_quadrature(ctx):
+    flt = F.linear_registration_filters()
+    # a plane wave along x: filter 0 responds with a constant-magnitude
+    # analytic signal, the other two barely respond.
+    x = np.arange(40)
+    vol = np.broadcast_to(np.cos(np.pi / 3 * x), (20, 24, 40)).astype(np.float32)
+    q = ctx.filter3d(cuda(vol), flt).cpu().numpy()[0]
+    inner = q[:, 8:-8, 8:-8, 8:-8]
+    mag = np.abs(inner[0])
+    assert mag.std() / mag.mean() < 0.05
+    assert np.abs(inner[1]).mean() < 0.05 * mag.mean()
+
+
+def test_normal_equations_match_golden(ctx, golden):
+    q1 = torch.from_numpy(golden["q1"]).cuda()
+    q2 = torch.from_numpy(golden["q2"]).cuda()
+    A, h = ctx.normal_equations(q1, q2[None])
+    A = A.cpu().numpy()[0]
+    h = h.cpu().numpy()[0]
+    assert rel_err(A, golden["A"]) < TOL
+    assert rel_err(h, golden["h"]) < TOL
+    # zero structure identical
+    assert np.array_equal(A != 0, golden["A"] != 0)
+
+
+def test_solve_matches_golden(ctx, golden):
+    A = torch.from_numpy(golden["A"].astype(np.float64)).cuda()
+    h = torch.from_numpy(golden["h"].astype(np.float64)).cuda()
+    p = ctx.solve(A, h).cpu().numpy()[0]
+    np.testing.assert_allclose(p, golden["p_solve"], rtol=1e-6, atol=1e-7)
+
+
+def test_solve_zero_system(ctx):
+    A = torch.zeros((2, 12, 12), dtype=torch.float64, device="cuda")
+    h = torch.zeros((2, 12), dtype=torch.float64, device="cuda")
+    p = ctx.solve(A, h).cpu().numpy()
+    assert np.all(p == 0)
+
+
+def test_warp_affine_matches_golden(ctx, golden):
+    out = ctx.warp_affine(cuda(golden["moved"]), torch.from_numpy(golden["p_solve"]).cuda())
+    assert rel_err(out.cpu().numpy()[0], golden["warp_affine"]) < TOL
+
+
+def test_warp_field_matches_golden(ctx, golden):
+    out = ctx.warp_field(cuda(golden["moved"]), cuda(golden["field_x"]), cuda(golden["field_y"]),
+                         cuda(golden["field_z"]))
+    assert rel_err(out.cpu().numpy(), golden["warp_field"]) < TOL
+
+
+def test_warp_identity_is_exact(ctx, golden):
+    v = cuda(golden["moved"])
+    out = ctx.warp_affine(v, torch.zeros(12, device="cuda"))
+    assert torch.equal(out[0], v)
+
+
+def test_smoothing_matches_golden(ctx, golden):
+    fs = golden["smooth_filter"]
+    out = ctx.smooth3d(cuda(golden["moved"]), fs, fs, fs).cpu().numpy()
+    assert rel_err(out, golden["smooth"]) < TOL
+    out = ctx.smooth3d(cuda(golden["moved"]), fs, fs, fs, cert=cuda(golden["cert"]),
+                       smoothed_cert=cuda(golden["smooth_cert"])).cpu().numpy()
+    assert rel_err(out, golden["smooth_normalized"]) < TOL
+
+
+def test_rescale_matches_golden(ctx, golden):
+    out = ctx.rescale_linear(cuda(golden["moved"]), (11, 13, 17)).cpu().numpy()
+    assert rel_err(out, golden["rescale"]) < TOL
