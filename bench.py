@@ -213,14 +213,17 @@ def run_gpu(args, rank, world, local_rank):
         if world > 1:
             dist.barrier()
 
+    # clocks are sampled from the warm-up through the end of the timed
+    # region (nvidia-smi needs ~0.2 s per sample; the timed region is short)
+    sampler = ClockSampler(local_rank) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
     for _ in range(args.warmup):
         out = step()
     torch.cuda.synchronize()
 
     # ---- device-resident timed region ----
-    sampler = ClockSampler(local_rank) if rank == 0 else None
-    if sampler:
-        sampler.start()
     launches0 = ctx.kernel_launches
     st = torch.cuda.current_stream()
     times = []
@@ -238,6 +241,8 @@ def run_gpu(args, rank, world, local_rank):
     torch.cuda.synchronize()
     barrier()
     launches = ctx.kernel_launches - launches0
+    if sampler:
+        time.sleep(0.25)
     clocks = sampler.stop() if sampler else None
     ms = float(np.sum(times))
     iters_used = out["iterations"].cpu().numpy()
@@ -341,7 +346,7 @@ def run_gpu(args, rank, world, local_rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--skip-cpu", action="store_true")

@@ -24,7 +24,7 @@ BRC_ERR_UNSUPPORTED = -6
 BRC_ERR_NONFINITE = -7
 
 TRANSLATION, RIGID, AFFINE = 0, 1, 2
-PREC_FP32, PREC_BF16X3 = 0, 1
+PREC_FP32, PREC_BF16X3, PREC_FP32_GENERAL = 0, 1, 2
 
 
 class BrcError(RuntimeError):
@@ -41,6 +41,32 @@ class LinearOpts(ctypes.Structure):
         ("tolerance", ctypes.c_float),
         ("use_graph", ctypes.c_int),
         ("certainty_sigma_x100", ctypes.c_int),
+    ]
+
+
+class NonlinearOpts(ctypes.Structure):
+    _fields_ = [
+        ("iterations", ctypes.c_int),
+        ("coarsest_scale", ctypes.c_int),
+        ("tsigma", ctypes.c_float),
+        ("esigma", ctypes.c_float),
+        ("dsigma", ctypes.c_float),
+        ("precision", ctypes.c_int),
+        ("solve_fp64", ctypes.c_int),
+    ]
+
+
+class TwoVolumeOpts(ctypes.Structure):
+    _fields_ = [
+        ("linear_iterations", ctypes.c_int),
+        ("nonlinear_iterations", ctypes.c_int),
+        ("coarsest_scale", ctypes.c_int),
+        ("mm_z_cut", ctypes.c_int),
+        ("tsigma", ctypes.c_float),
+        ("esigma", ctypes.c_float),
+        ("dsigma", ctypes.c_float),
+        ("precision", ctypes.c_int),
+        ("solve_fp64", ctypes.c_int),
     ]
 
 
@@ -73,6 +99,19 @@ _SIGS = {
         [_P, _P, _LL, _P, _I, _I, _I, _I, _P, ctypes.POINTER(LinearOpts), _P, _P, _P, _P], _I),
     "brc_motion_correct": (
         [_P, _P, _I, _I, _I, _I, _P, _P, ctypes.POINTER(LinearOpts), _P, _P], _I),
+    "brc_register_linear_scales": (
+        [_P, _P, _P, _I, _I, _I, _I, _P, ctypes.POINTER(LinearOpts), _I, _P, _P, _P], _I),
+    "brc_nonlinear_opts_default": ([ctypes.POINTER(NonlinearOpts), _I], None),
+    "brc_nonlinear_step": (
+        [_P, _P, _P, _I, _I, _I, _P, _P, ctypes.c_float, ctypes.c_float, ctypes.c_float, _I, _P], _I),
+    "brc_register_nonlinear": (
+        [_P, _P, _P, _I, _I, _I, _P, _P, _P, ctypes.POINTER(NonlinearOpts), _P, _P], _I),
+    "brc_change_resolution_and_size": ([_P, _P, _I, _I, _I, _P, _P, _I, _I, _I, _P, _I], _I),
+    "brc_center_of_mass": ([_P, _P, _I, _I, _I, _P], _I),
+    "brc_two_volume_opts_default": ([ctypes.POINTER(TwoVolumeOpts)], None),
+    "brc_register_two_volumes": (
+        [_P, _P, _I, _I, _I, _P, _P, _I, _I, _I, _P, _P, _P, _P, _P, ctypes.POINTER(TwoVolumeOpts), _P, _P,
+         _P, _P, _P], _I),
 }
 
 

@@ -195,6 +195,133 @@ class Context:
             ctypes.byref(opts), _p(params), _p(aligned), _p(rot), _p(iters)))
         return {"params": params, "aligned": aligned, "rotations": rot, "iterations": iters}
 
+    def register_linear_scales(self, ref: torch.Tensor, moving: torch.Tensor, filters, iterations: int,
+                               coarsest_scale: int, type_: int = L.AFFINE):
+        """Multi-scale linear registration of moving (B,D,H,W) onto a shared
+        ref (D,H,W).  Returns dict with params (B,12), aligned (B,D,H,W) and
+        rotations (B,3)."""
+        m = _vol_batch(moving)
+        B, D, H, W = m.shape
+        r = ref.contiguous()
+        f = _host_filters(filters)
+        opts = L.LinearOpts()
+        L.lib().brc_linear_opts_default(ctypes.byref(opts), iterations)
+        opts.type = type_
+        params = torch.empty((B, 12), dtype=torch.float32, device=m.device)
+        aligned = torch.empty_like(m)
+        rot = torch.empty((B, 3), dtype=torch.float32, device=m.device)
+        self._bind_stream()
+        _check(self, L.lib().brc_register_linear_scales(
+            self.handle, _p(r), _p(m), W, H, D, B, f.ctypes.data_as(ctypes.c_void_p), ctypes.byref(opts),
+            coarsest_scale, _p(params), _p(aligned), _p(rot)))
+        return {"params": params, "aligned": aligned, "rotations": rot}
+
+    @staticmethod
+    def _nl_consts(bank: dict):
+        f6 = np.ascontiguousarray(bank["nonlinear"], np.float32)
+        m = np.ascontiguousarray(bank["projection_tensors"], np.float32)
+        d = np.ascontiguousarray(bank["directions"], np.float32)
+        return f6, m, d
+
+    def nonlinear_step(self, q1: torch.Tensor, q2: torch.Tensor, bank: dict, field: torch.Tensor,
+                       tsigma=5.0, esigma=5.0, dsigma=5.0, solve_fp64: bool = False) -> torch.Tensor:
+        """Adds one nonlinear update computed from responses q1, q2 (6,D,H,W
+        complex64) to `field` (3,D,H,W float32, in place)."""
+        _, D, H, W = q2.shape
+        a = torch.view_as_real(q1.contiguous()).contiguous()
+        c = torch.view_as_real(q2.contiguous()).contiguous()
+        _, m, d = self._nl_consts(bank)
+        self._bind_stream()
+        _check(self, L.lib().brc_nonlinear_step(self.handle, _p(a), _p(c), W, H, D,
+                                                m.ctypes.data_as(ctypes.c_void_p),
+                                                d.ctypes.data_as(ctypes.c_void_p), tsigma, esigma, dsigma,
+                                                1 if solve_fp64 else 0, _p(field)))
+        return field
+
+    def register_nonlinear(self, ref: torch.Tensor, moving: torch.Tensor, bank: dict, iterations: int,
+                           coarsest_scale: int = 1, tsigma=5.0, esigma=5.0, dsigma=5.0,
+                           solve_fp64: bool = False, precision: int = L.PREC_FP32):
+        """Multi-scale nonlinear registration.  Returns (field (3,D,H,W),
+        aligned (D,H,W))."""
+        r = ref.contiguous()
+        m = moving.contiguous()
+        D, H, W = m.shape
+        f6, mt, d = self._nl_consts(bank)
+        o = L.NonlinearOpts()
+        L.lib().brc_nonlinear_opts_default(ctypes.byref(o), iterations)
+        o.coarsest_scale = coarsest_scale
+        o.tsigma, o.esigma, o.dsigma = tsigma, esigma, dsigma
+        o.solve_fp64 = 1 if solve_fp64 else 0
+        o.precision = precision
+        field = torch.empty((3, D, H, W), dtype=torch.float32, device=m.device)
+        aligned = torch.empty_like(m)
+        self._bind_stream()
+        _check(self, L.lib().brc_register_nonlinear(self.handle, _p(r), _p(m), W, H, D,
+                                                    f6.ctypes.data_as(ctypes.c_void_p),
+                                                    mt.ctypes.data_as(ctypes.c_void_p),
+                                                    d.ctypes.data_as(ctypes.c_void_p), ctypes.byref(o),
+                                                    _p(field), _p(aligned)))
+        return field, aligned
+
+    def change_resolution_and_size(self, src: torch.Tensor, voxel_size, shape, new_voxel_size,
+                                   mm_z_cut: int = 0) -> torch.Tensor:
+        v = src.contiguous()
+        D, H, W = v.shape
+        D2, H2, W2 = shape
+        out = torch.empty((D2, H2, W2), dtype=torch.float32, device=v.device)
+        vs = np.ascontiguousarray(voxel_size, np.float32)
+        nvs = np.ascontiguousarray(new_voxel_size, np.float32)
+        self._bind_stream()
+        _check(self, L.lib().brc_change_resolution_and_size(
+            self.handle, _p(v), W, H, D, vs.ctypes.data_as(ctypes.c_void_p), _p(out), W2, H2, D2,
+            nvs.ctypes.data_as(ctypes.c_void_p), mm_z_cut))
+        return out
+
+    def center_of_mass(self, vol: torch.Tensor) -> np.ndarray:
+        v = vol.contiguous()
+        D, H, W = v.shape
+        c = np.zeros(3, np.float32)
+        self._bind_stream()
+        _check(self, L.lib().brc_center_of_mass(self.handle, _p(v), W, H, D, c.ctypes.data_as(ctypes.c_void_p)))
+        return c
+
+    def register_two_volumes(self, subject: torch.Tensor, voxel_size, template: torch.Tensor,
+                             template_voxel_size, bank: dict, linear_iterations: int,
+                             nonlinear_iterations: int, coarsest_scale: int, mm_z_cut: int = 0,
+                             tsigma=5.0, esigma=5.0, dsigma=5.0, solve_fp64: bool = False,
+                             precision: int = L.PREC_FP32):
+        """T1-to-template normalisation.  Returns dict: params (12,),
+        interpolated, aligned_linear, aligned_nonlinear (template size) and
+        field (3, D, H, W)."""
+        s = subject.contiguous()
+        t = template.contiguous()
+        D, H, W = s.shape
+        D2, H2, W2 = t.shape
+        f3 = np.ascontiguousarray(bank["linear"], np.float32)
+        f6, m, d = self._nl_consts(bank)
+        o = L.TwoVolumeOpts()
+        L.lib().brc_two_volume_opts_default(ctypes.byref(o))
+        o.linear_iterations, o.nonlinear_iterations = linear_iterations, nonlinear_iterations
+        o.coarsest_scale, o.mm_z_cut = coarsest_scale, mm_z_cut
+        o.tsigma, o.esigma, o.dsigma = tsigma, esigma, dsigma
+        o.solve_fp64 = 1 if solve_fp64 else 0
+        o.precision = precision
+        vs = np.ascontiguousarray(voxel_size, np.float32)
+        tvs = np.ascontiguousarray(template_voxel_size, np.float32)
+        params = np.zeros(12, np.float32)
+        out = {k: torch.empty((D2, H2, W2), dtype=torch.float32, device=t.device)
+               for k in ("interpolated", "aligned_linear", "aligned_nonlinear")}
+        field = torch.zeros((3, D2, H2, W2), dtype=torch.float32, device=t.device)
+        cp = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+        self._bind_stream()
+        _check(self, L.lib().brc_register_two_volumes(
+            self.handle, _p(s), W, H, D, cp(vs), _p(t), W2, H2, D2, cp(tvs), cp(f3), cp(f6), cp(m), cp(d),
+            ctypes.byref(o), cp(params), _p(out["interpolated"]), _p(out["aligned_linear"]),
+            _p(out["aligned_nonlinear"]), _p(field)))
+        out["params"] = params
+        out["field"] = field
+        return out
+
     def motion_correct(self, volumes: np.ndarray, voxel_size, filters, iterations: int,
                        tolerance: float = 0.0, reference: np.ndarray = None, use_graph: bool = True,
                        precision: int = L.PREC_FP32, certainty_sigma: float = 0.0):

@@ -1,0 +1,311 @@
+"""Python mirror of BROCCOLI's Python wrapper for the registration path.
+
+The reference's wrapper (code/Python_Wrapper/broccoli/broccoli_common.py:
+55-200) subclasses the SWIG-bound C++ class; its helpers pack numpy volumes
+(flipud, then transpose (2, 0, 1) so x is fastest) and its module functions
+(motion_correction.py:4-73, registration.py) drive the class.  This module
+keeps those names and conventions and runs the path through the C-ABI of
+libbroccoli_b200 with host arrays (no torch needed).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+
+_pack_permutation = (2, 0, 1)
+_pack_permutation_4d = (3, 2, 0, 1)
+
+TRANSLATION, RIGID, AFFINE = 0, 1, 2
+NEAREST, LINEAR, CUBIC = 0, 1, 2
+
+
+def _permute(permutation, array):
+    return [array[permutation[i]] for i in range(len(array))]
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class BROCCOLI_LIB:
+    """Setter/wrapper interface of BROCCOLI_LIB for this path, on the C-ABI."""
+
+    def __init__(self, *args):
+        self._ctx = None
+        self._initiated = False
+        self._init_error = ""
+        self._input_arrays = []
+        self.epi = [0, 0, 0, 1]
+        self.t1 = [0, 0, 0]
+        self.mni = [0, 0, 0]
+        self.epi_vox = [1.0, 1.0, 1.0]
+        self.t1_vox = [1.0, 1.0, 1.0]
+        self.mni_vox = [1.0, 1.0, 1.0]
+        self.fmri = None
+        self.t1_volume = None
+        self.mni_volume = None
+        self.linear_filters = None
+        self.nonlinear_filters = None
+        self.projection_tensors = np.zeros((6, 6), np.float32)
+        self.directions = None
+        self.it_linear, self.it_nonlinear, self.it_mc = 10, 10, 5
+        self.coarsest = 4
+        self.mm_z_cut = 0
+        self.sigmas = [5.0, 5.0, 5.0]
+        self.mc_tolerance = 0.0
+        self.precision = L.PREC_FP32
+        self.out = {}
+        if len(args) == 2:
+            self.OpenCLInitiate(*args)
+
+    # ---- runtime ----------------------------------------------------------
+
+    def OpenCLInitiate(self, platform, device):
+        """Binds a CUDA device (platform must be 0)."""
+        if platform != 0:
+            self._init_error = "platform must be 0"
+            return False
+        h = ctypes.c_void_p()
+        s = L.lib().brc_ctx_create(int(device), ctypes.byref(h))
+        if s != L.BRC_OK:
+            self._init_error = L.status_string(s)
+            return False
+        self._ctx = h
+        self._initiated = True
+        return True
+
+    def GetOpenCLInitiated(self):
+        return 1 if self._initiated else 0
+
+    def GetOpenCLInitializationError(self):
+        return self._init_error
+
+    def __del__(self):
+        if getattr(self, "_ctx", None):
+            L.lib().brc_ctx_destroy(self._ctx)
+            self._ctx = None
+
+    def _check(self, s):
+        if s != L.BRC_OK:
+            msg = L.lib().brc_last_error(self._ctx).decode() if self._ctx else ""
+            raise L.BrcError(s, f"{L.status_string(s)}: {msg}")
+
+    # ---- packing (broccoli_common.py:144-200) -----------------------------
+
+    def packArray(self, array):
+        return np.ascontiguousarray(array, dtype=np.float32)
+
+    def packVolume(self, array):
+        if len(array.shape) == 3:
+            t = np.flipud(array).transpose(_pack_permutation)
+        elif len(array.shape) == 4:
+            t = np.flipud(array).transpose(_pack_permutation_4d)
+        else:
+            t = array
+        t = self.packArray(t.flatten())
+        self._input_arrays.append(t)
+        return t
+
+    def createOutputArray(self, shape, dtype=np.float32):
+        return np.empty(shape=shape, dtype=dtype).flatten()
+
+    def unpackOutputArray(self, array, shape):
+        return array.reshape(shape)
+
+    def unpackOutputVolume(self, array, shape=None):
+        unpack = None
+        if shape:
+            if len(shape) == 3:
+                t_shape = _permute(_pack_permutation, shape)
+                unpack = np.argsort(_pack_permutation)
+            elif len(shape) == 4:
+                t_shape = _permute(_pack_permutation_4d, shape)
+                unpack = np.argsort(_pack_permutation_4d)
+            else:
+                t_shape = shape
+            array = self.unpackOutputArray(array, t_shape)
+            array = np.fliplr(array)
+        return array.transpose(unpack) if unpack is not None else array
+
+    # ---- data setters (broccoli_common.py:75-127) --------------------------
+
+    def SetEPIData(self, array, voxel_sizes):
+        self.SetEPIHeight(array.shape[0])
+        self.SetEPIWidth(array.shape[1])
+        self.SetEPIDepth(array.shape[2])
+        self.SetInputEPIVolume(self.packVolume(array))
+        self.SetEPIVoxelSizeX(voxel_sizes[0])
+        self.SetEPIVoxelSizeY(voxel_sizes[1])
+        self.SetEPIVoxelSizeZ(voxel_sizes[2])
+
+    def SetT1Data(self, array, voxel_sizes):
+        self.SetT1Height(array.shape[0])
+        self.SetT1Width(array.shape[1])
+        self.SetT1Depth(array.shape[2])
+        self.SetInputT1Volume(self.packVolume(array))
+        self.SetT1VoxelSizeX(voxel_sizes[0])
+        self.SetT1VoxelSizeY(voxel_sizes[1])
+        self.SetT1VoxelSizeZ(voxel_sizes[2])
+
+    def SetMNIData(self, array, voxel_sizes):
+        self.SetMNIHeight(array.shape[0])
+        self.SetMNIWidth(array.shape[1])
+        self.SetMNIDepth(array.shape[2])
+        self.SetInputMNIVolume(self.packVolume(array))
+        self.SetMNIVoxelSizeX(voxel_sizes[0])
+        self.SetMNIVoxelSizeY(voxel_sizes[1])
+        self.SetMNIVoxelSizeZ(voxel_sizes[2])
+
+    def SetfMRIData(self, array, voxel_sizes):
+        self.SetEPIHeight(array.shape[0])
+        self.SetEPIWidth(array.shape[1])
+        self.SetEPIDepth(array.shape[2])
+        self.SetEPITimepoints(array.shape[3])
+        self.SetInputfMRIVolumes(self.packVolume(array))
+        self.SetEPIVoxelSizeX(voxel_sizes[0])
+        self.SetEPIVoxelSizeY(voxel_sizes[1])
+        self.SetEPIVoxelSizeZ(voxel_sizes[2])
+
+    def SetParametricImageRegistrationFilters(self, filters):
+        """Three complex 7x7x7 arrays (linear registration)."""
+        bank = np.zeros((3, 2, 7, 7, 7), np.float32)
+        for i in range(3):
+            bank[i, 0] = self.packVolume(np.real(filters[i])).reshape(7, 7, 7)
+            bank[i, 1] = self.packVolume(np.imag(filters[i])).reshape(7, 7, 7)
+        self.linear_filters = bank
+
+    def SetNonParametricImageRegistrationFilters(self, filters):
+        bank = np.zeros((6, 2, 7, 7, 7), np.float32)
+        for i in range(6):
+            bank[i, 0] = self.packVolume(np.real(filters[i])).reshape(7, 7, 7)
+            bank[i, 1] = self.packVolume(np.imag(filters[i])).reshape(7, 7, 7)
+        self.nonlinear_filters = bank
+
+    def SetProjectionTensorMatrixFilters(self, filters):
+        for k in range(6):
+            self.projection_tensors[k] = np.asarray(filters[k], np.float32)
+
+    def SetFilterDirections(self, x, y, z):
+        self.directions = np.stack([np.asarray(a, np.float32).reshape(6) for a in (x, y, z)])
+
+    # ---- raw setters with the C++ class's names ----------------------------
+
+    def SetEPIWidth(self, w): self.epi[0] = int(w)
+    def SetEPIHeight(self, h): self.epi[1] = int(h)
+    def SetEPIDepth(self, d): self.epi[2] = int(d)
+    def SetEPITimepoints(self, t): self.epi[3] = int(t)
+    def SetEPIVoxelSizeX(self, v): self.epi_vox[0] = float(v)
+    def SetEPIVoxelSizeY(self, v): self.epi_vox[1] = float(v)
+    def SetEPIVoxelSizeZ(self, v): self.epi_vox[2] = float(v)
+    def SetT1Width(self, w): self.t1[0] = int(w)
+    def SetT1Height(self, h): self.t1[1] = int(h)
+    def SetT1Depth(self, d): self.t1[2] = int(d)
+    def SetT1VoxelSizeX(self, v): self.t1_vox[0] = float(v)
+    def SetT1VoxelSizeY(self, v): self.t1_vox[1] = float(v)
+    def SetT1VoxelSizeZ(self, v): self.t1_vox[2] = float(v)
+    def SetMNIWidth(self, w): self.mni[0] = int(w)
+    def SetMNIHeight(self, h): self.mni[1] = int(h)
+    def SetMNIDepth(self, d): self.mni[2] = int(d)
+    def SetMNIVoxelSizeX(self, v): self.mni_vox[0] = float(v)
+    def SetMNIVoxelSizeY(self, v): self.mni_vox[1] = float(v)
+    def SetMNIVoxelSizeZ(self, v): self.mni_vox[2] = float(v)
+    def SetInputfMRIVolumes(self, a): self.fmri = a
+    def SetInputEPIVolume(self, a): self.fmri = a
+    def SetInputT1Volume(self, a): self.t1_volume = a
+    def SetInputMNIVolume(self, a): self.mni_volume = a
+    def SetInputMNIBrainVolume(self, a): self.mni_volume = a
+    def SetImageRegistrationFilterSize(self, n):
+        if int(n) != 7:
+            raise ValueError("filter size must be 7")
+    def SetNumberOfIterationsForLinearImageRegistration(self, n): self.it_linear = int(n)
+    def SetNumberOfIterationsForParametricImageRegistration(self, n): self.it_linear = int(n)
+    def SetNumberOfIterationsForNonLinearImageRegistration(self, n): self.it_nonlinear = int(n)
+    def SetNumberOfIterationsForNonParametricImageRegistration(self, n): self.it_nonlinear = int(n)
+    def SetNumberOfIterationsForMotionCorrection(self, n): self.it_mc = int(n)
+    def SetCoarsestScaleT1MNI(self, n): self.coarsest = int(n)
+    def SetMMT1ZCUT(self, mm): self.mm_z_cut = int(mm)
+    def SetInterpolationMode(self, mode):
+        if mode != LINEAR:
+            raise ValueError("only LINEAR interpolation is implemented")
+    def SetTsigma(self, s): self.sigmas[0] = float(s)
+    def SetEsigma(self, s): self.sigmas[1] = float(s)
+    def SetDsigma(self, s): self.sigmas[2] = float(s)
+    def SetMotionCorrectionTolerance(self, v): self.mc_tolerance = float(v)
+    def SetPrecision(self, p): self.precision = int(p)
+    def SetOutputMotionParameters(self, a): self.out["motion"] = a
+    def SetOutputMotionCorrectedfMRIVolumes(self, a): self.out["mc"] = a
+    def SetOutputT1MNIRegistrationParameters(self, a): self.out["params"] = a
+    def SetOutputAlignedT1VolumeLinear(self, a): self.out["aligned_linear"] = a
+    def SetOutputAlignedT1VolumeNonLinear(self, a): self.out["aligned_nonlinear"] = a
+    def SetOutputInterpolatedT1Volume(self, a): self.out["interpolated"] = a
+    def SetOutputDisplacementField(self, x, y, z): self.out["field"] = (x, y, z)
+
+    # ---- entry points -------------------------------------------------------
+
+    def PerformMotionCorrectionWrapper(self):
+        W, H, D, T = self.epi
+        vols = np.ascontiguousarray(self.fmri, np.float32)
+        opts = L.LinearOpts()
+        L.lib().brc_linear_opts_default(ctypes.byref(opts), self.it_mc)
+        opts.type = RIGID
+        opts.tolerance = self.mc_tolerance
+        opts.precision = self.precision
+        motion = np.zeros(6 * T, np.float32)
+        vs = np.asarray(self.epi_vox, np.float32)
+        bank = np.ascontiguousarray(self.linear_filters, np.float32)
+        self._check(L.lib().brc_motion_correct(self._ctx, _ptr(vols), W, H, D, T, _ptr(vs), _ptr(bank),
+                                               ctypes.byref(opts), None, _ptr(motion)))
+        if self.fmri is not vols:
+            self.fmri[...] = vols.reshape(self.fmri.shape)
+        if "motion" in self.out:
+            self.out["motion"][...] = motion.reshape(self.out["motion"].shape)
+        if "mc" in self.out:
+            self.out["mc"][...] = vols.reshape(self.out["mc"].shape)
+
+    def PerformRegistrationTwoVolumesWrapper(self):
+        import torch
+        from .api import Context
+        ctx = Context(0)
+        W, H, D = self.t1
+        W2, H2, D2 = self.mni
+        sub = torch.from_numpy(np.ascontiguousarray(self.t1_volume, np.float32).reshape(D, H, W)).cuda()
+        tpl = torch.from_numpy(np.ascontiguousarray(self.mni_volume, np.float32).reshape(D2, H2, W2)).cuda()
+        bank = {"linear": self.linear_filters, "nonlinear": self.nonlinear_filters,
+                "projection_tensors": self.projection_tensors, "directions": self.directions}
+        r = ctx.register_two_volumes(sub, self.t1_vox, tpl, self.mni_vox, bank, self.it_linear,
+                                     self.it_nonlinear if self.nonlinear_filters is not None else 0,
+                                     self.coarsest, self.mm_z_cut, *self.sigmas)
+        if "params" in self.out:
+            self.out["params"][: 12] = r["params"]
+        for k in ("aligned_linear", "aligned_nonlinear", "interpolated"):
+            if k in self.out:
+                self.out[k][...] = r[k].cpu().numpy().reshape(self.out[k].shape)
+        if "field" in self.out:
+            f = r["field"].cpu().numpy()
+            for a in range(3):
+                self.out["field"][a][...] = f[a].reshape(self.out["field"][a].shape)
+        ctx.close()
+
+
+def performMotionCorrection(h_fMRI_Volumes, h_fMRI_Voxel_Sizes, h_Quadrature_Filters, iterations,
+                            OPENCL_PLATFORM=0, OPENCL_DEVICE=0):
+    """motion_correction.py:performMotionCorrection on the C-ABI.  Returns
+    (corrected volumes, motion parameters (6, T))."""
+    B = BROCCOLI_LIB(OPENCL_PLATFORM, OPENCL_DEVICE)
+    if not B.GetOpenCLInitiated():
+        raise RuntimeError("initialisation failed: " + B.GetOpenCLInitializationError())
+    shape = h_fMRI_Volumes.shape
+    T = shape[3]
+    B.SetfMRIData(h_fMRI_Volumes, h_fMRI_Voxel_Sizes)
+    B.SetImageRegistrationFilterSize(len(h_Quadrature_Filters[0]))
+    B.SetParametricImageRegistrationFilters(h_Quadrature_Filters)
+    B.SetNumberOfIterationsForMotionCorrection(iterations)
+    corrected = B.createOutputArray(shape)
+    B.SetOutputMotionCorrectedfMRIVolumes(corrected)
+    motion = B.createOutputArray((6, T))
+    B.SetOutputMotionParameters(motion)
+    B.PerformMotionCorrectionWrapper()
+    return B.unpackOutputVolume(corrected, shape), B.unpackOutputArray(motion, (6, T))

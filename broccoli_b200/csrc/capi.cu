@@ -133,11 +133,11 @@ int brc_filter3d(brc_ctx* ctx, const float* d_vol, int W, int H, int D, int batc
   if (nfilt != 3 && nfilt != 6) return ctx->fail(BRC_ERR_INVALID, "brc_filter3d: nfilt must be 3 or 6");
   if (batch > 1 && vol_stride < (long long)W * H * D)
     return ctx->fail(BRC_ERR_INVALID, "brc_filter3d: vol_stride smaller than a volume");
-  if (precision != BRC_PREC_FP32)
+  if (precision != BRC_PREC_FP32 && precision != BRC_PREC_FP32_GENERAL)
     return ctx->fail(BRC_ERR_UNSUPPORTED, "brc_filter3d: precision not available");
   cudaSetDevice(ctx->device);
   BRC_TRY(ctx, brc::filter3d_fp32(d_vol, W, H, D, batch, vol_stride, h_filters, nfilt, d_out, nullptr,
-                                  0, ctx->stream()),
+                                  0, ctx->stream(), precision == BRC_PREC_FP32),
           "filter3d");
   ctx->launches += 1;
   return BRC_OK;
@@ -224,6 +224,42 @@ int brc_smooth3d(brc_ctx* ctx, const float* d_vol, int W, int H, int D, int batc
   return BRC_OK;
 }
 
+int brc_device_alloc(brc_ctx* ctx, size_t bytes, void** d_out) {
+  BRC_CHECK_CTX(ctx);
+  if (!d_out) return ctx->fail(BRC_ERR_INVALID, "brc_device_alloc: null output");
+  *d_out = nullptr;
+  cudaSetDevice(ctx->device);
+  BRC_TRY(ctx, cudaMalloc(d_out, bytes ? bytes : 1), "brc_device_alloc");
+  return BRC_OK;
+}
+
+int brc_device_free(brc_ctx* ctx, void* d_ptr) {
+  BRC_CHECK_CTX(ctx);
+  if (!d_ptr) return BRC_OK;
+  cudaSetDevice(ctx->device);
+  BRC_TRY(ctx, cudaStreamSynchronize(ctx->stream()), "sync");
+  BRC_TRY(ctx, cudaFree(d_ptr), "brc_device_free");
+  return BRC_OK;
+}
+
+int brc_copy_to_device(brc_ctx* ctx, void* d_dst, const void* h_src, size_t bytes) {
+  BRC_CHECK_CTX(ctx);
+  if ((!d_dst || !h_src) && bytes) return ctx->fail(BRC_ERR_INVALID, "brc_copy_to_device: null pointer");
+  cudaSetDevice(ctx->device);
+  BRC_TRY(ctx, cudaMemcpyAsync(d_dst, h_src, bytes, cudaMemcpyHostToDevice, ctx->stream()), "H2D");
+  BRC_TRY(ctx, cudaStreamSynchronize(ctx->stream()), "sync");
+  return BRC_OK;
+}
+
+int brc_copy_to_host(brc_ctx* ctx, void* h_dst, const void* d_src, size_t bytes) {
+  BRC_CHECK_CTX(ctx);
+  if ((!d_src || !h_dst) && bytes) return ctx->fail(BRC_ERR_INVALID, "brc_copy_to_host: null pointer");
+  cudaSetDevice(ctx->device);
+  BRC_TRY(ctx, cudaMemcpyAsync(h_dst, d_src, bytes, cudaMemcpyDeviceToHost, ctx->stream()), "D2H");
+  BRC_TRY(ctx, cudaStreamSynchronize(ctx->stream()), "sync");
+  return BRC_OK;
+}
+
 void brc_linear_opts_default(brc_linear_opts* o, int iterations) {
   if (!o) return;
   o->iterations = iterations;
@@ -257,6 +293,7 @@ struct RegPlan {
   int* iters_ws;
   int* status;
   int nblk, zpb;
+  float* cert;  // [batch][3][V] certainty volumes when smoothing them, else null
 };
 
 // Queues the whole registration on stream st; returns the number of
@@ -289,8 +326,10 @@ long long enqueue_registration(brc_ctx* ctx, const RegPlan& p, cudaStream_t st) 
                                 st)) != cudaSuccess)
       return ctx->cuda(e, "filter3d");
     if ((e = brc::normal_eq_partials(p.q1, p.ref_stride ? 6 * V : 0, p.q2, p.W, p.H, p.D, p.batch,
-                                     p.partials, p.nblk, p.zpb, p.conv_iter, it, st)) != cudaSuccess)
+                                     p.partials, p.nblk, p.zpb, p.conv_iter, it, st, p.cert,
+                                     p.opts.certainty_sigma_x100 / 100.0f)) != cudaSuccess)
       return ctx->cuda(e, "normal_eq");
+    if (p.cert) kernels++;
     if ((e = brc::solve_update(p.partials, p.nblk, p.batch, p.opts.type, p.opts.tolerance, p.W, p.H,
                                p.D, p.params, p.rotations, p.conv_iter, p.iters_ws, p.status, it,
                                st)) != cudaSuccess)
@@ -323,8 +362,8 @@ extern "C" int brc_register_linear_batched(brc_ctx* ctx, const float* d_ref, lon
     return ctx->fail(BRC_ERR_INVALID, "brc_register_linear_batched: bad options");
   if (opts->precision != BRC_PREC_FP32)
     return ctx->fail(BRC_ERR_UNSUPPORTED, "brc_register_linear_batched: precision not available");
-  if (opts->certainty_sigma_x100 != 0)
-    return ctx->fail(BRC_ERR_UNSUPPORTED, "brc_register_linear_batched: certainty smoothing not available");
+  if (opts->certainty_sigma_x100 < 0)
+    return ctx->fail(BRC_ERR_INVALID, "brc_register_linear_batched: negative certainty sigma");
   const long long V = (long long)W * H * D;
   if (ref_stride != 0 && ref_stride < V)
     return ctx->fail(BRC_ERR_INVALID, "brc_register_linear_batched: ref_stride smaller than a volume");
@@ -361,6 +400,11 @@ extern "C" int brc_register_linear_batched(brc_ctx* ctx, const float* d_ref, lon
   p.conv_iter = ctx->ctl.as<int>();
   p.iters_ws = p.conv_iter + batch;
   p.status = p.iters_ws + batch;
+  p.cert = nullptr;
+  if (opts->certainty_sigma_x100 > 0) {
+    BRC_TRY(ctx, ctx->cert.ensure(sizeof(float) * 3 * V * batch), "alloc certainty");
+    p.cert = ctx->cert.as<float>();
+  }
 
   const cudaStream_t user = ctx->stream();
   if (!opts->use_graph) {
@@ -375,7 +419,7 @@ extern "C" int brc_register_linear_batched(brc_ctx* ctx, const float* d_ref, lon
              (uint64_t)fnv1a(&opts->tolerance, sizeof(float)), (uint64_t)d_params,
              (uint64_t)p.aligned, (uint64_t)d_rotations, (uint64_t)d_iterations,
              (uint64_t)ctx->q1.ptr, (uint64_t)ctx->q2.ptr, (uint64_t)ctx->partials.ptr,
-             (uint64_t)ctx->ctl.ptr};
+             (uint64_t)ctx->ctl.ptr, (uint64_t)p.cert, (uint64_t)opts->certainty_sigma_x100};
     auto itg = ctx->graphs.find(key);
     GraphEntry* ge = nullptr;
     if (itg == ctx->graphs.end()) {

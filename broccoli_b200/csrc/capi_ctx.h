@@ -55,7 +55,7 @@ struct brc_ctx {
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   std::string last_error;
   unsigned long long launches = 0;
-  DevBuf q1, q2, aligned, partials, ctl, tmp1, tmp2, series, corrected, params, rot, nl, pyr;
+  DevBuf q1, q2, aligned, partials, ctl, tmp1, tmp2, series, corrected, params, rot, nl, pyr, cert;
   std::map<GraphKey, std::unique_ptr<GraphEntry>> graphs;
 
   cudaStream_t stream() const { return use_user_stream ? user_stream : own_stream; }

@@ -199,6 +199,168 @@ extern "C" int brc_register_nonlinear(brc_ctx* ctx, const float* d_ref, const fl
   return BRC_OK;
 }
 
+extern "C" int brc_change_resolution_and_size(brc_ctx* ctx, const float* d_src, int W, int H, int D,
+                                              const float* voxel_size3, float* d_out, int W2, int H2,
+                                              int D2, const float* new_voxel_size3, int mm_z_cut) {
+  if (!ctx) return BRC_ERR_INVALID;
+  if (!d_src || !d_out || !voxel_size3 || !new_voxel_size3 || W <= 0 || H <= 0 || D <= 0 || W2 <= 0 ||
+      H2 <= 0 || D2 <= 0 || d_src == d_out)
+    return ctx->fail(BRC_ERR_INVALID, "brc_change_resolution_and_size: bad argument");
+  for (int a = 0; a < 3; a++)
+    if (!(voxel_size3[a] > 0) || !(new_voxel_size3[a] > 0))
+      return ctx->fail(BRC_ERR_INVALID, "brc_change_resolution_and_size: voxel sizes must be positive");
+  cudaSetDevice(ctx->device);
+  BRC_TRY(ctx, brc::resize_to_grid(d_src, W, H, D, voxel_size3[0], voxel_size3[1], voxel_size3[2], d_out, W2,
+                                   H2, D2, new_voxel_size3[0], new_voxel_size3[1], new_voxel_size3[2],
+                                   mm_z_cut, ctx->stream()),
+          "resize");
+  ctx->launches += 1;
+  return BRC_OK;
+}
+
+extern "C" int brc_center_of_mass(brc_ctx* ctx, const float* d_vol, int W, int H, int D, float* h_com3) {
+  if (!ctx) return BRC_ERR_INVALID;
+  if (!d_vol || !h_com3 || W <= 0 || H <= 0 || D <= 0)
+    return ctx->fail(BRC_ERR_INVALID, "brc_center_of_mass: bad argument");
+  cudaSetDevice(ctx->device);
+  BRC_TRY(ctx, ctx->ctl.ensure(sizeof(double) * 8), "alloc");
+  double* sums = ctx->ctl.as<double>();
+  BRC_TRY(ctx, brc::mass_moments(d_vol, W, H, D, sums, ctx->stream()), "mass_moments");
+  ctx->launches += 1;
+  double h[4];
+  BRC_TRY(ctx, cudaMemcpyAsync(h, sums, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream()), "D2H");
+  BRC_TRY(ctx, cudaStreamSynchronize(ctx->stream()), "sync");
+  for (int a = 0; a < 3; a++) h_com3[a] = (float)(h[a + 1] / h[0]);
+  return BRC_OK;
+}
+
+extern "C" void brc_two_volume_opts_default(brc_two_volume_opts* o) {
+  if (!o) return;
+  o->linear_iterations = 10;
+  o->nonlinear_iterations = 10;
+  o->coarsest_scale = 4;
+  o->mm_z_cut = 0;
+  o->tsigma = 5.0f;
+  o->esigma = 5.0f;
+  o->dsigma = 5.0f;
+  o->precision = BRC_PREC_FP32;
+  o->solve_fp64 = 0;
+}
+
+// PerformRegistrationTwoVolumesWrapper, broccoli_lib.cpp:7973-8112 (single
+// volume, no pre-centring, no skull strip): resample to the template grid,
+// match centres of mass, multi-scale affine, compose with the mass match,
+// multi-scale nonlinear, add the affine motion to the field, resample the
+// input again and warp it once by the combined field.
+extern "C" int brc_register_two_volumes(brc_ctx* ctx, const float* d_in, int W, int H, int D,
+                                        const float* voxel_size3, const float* d_tpl, int W2, int H2,
+                                        int D2, const float* tpl_voxel_size3, const float* h_filters3,
+                                        const float* h_filters6, const float* h_tensors,
+                                        const float* h_dirs, const brc_two_volume_opts* o,
+                                        float* h_params12, float* d_interpolated,
+                                        float* d_aligned_linear, float* d_aligned_nonlinear,
+                                        float* d_field) {
+  if (!ctx) return BRC_ERR_INVALID;
+  if (!d_in || !d_tpl || !voxel_size3 || !tpl_voxel_size3 || !h_filters3 || !o || !h_params12 ||
+      W <= 0 || H <= 0 || D <= 0 || W2 <= 0 || H2 <= 0 || D2 <= 0 || o->linear_iterations < 0 ||
+      o->nonlinear_iterations < 0 || o->coarsest_scale < 1)
+    return ctx->fail(BRC_ERR_INVALID, "brc_register_two_volumes: bad argument");
+  if (o->nonlinear_iterations > 0 && (!h_filters6 || !h_tensors || !h_dirs || !d_field))
+    return ctx->fail(BRC_ERR_INVALID, "brc_register_two_volumes: nonlinear stage needs filters and a field");
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream();
+  const long long V2 = (long long)W2 * H2 * D2;
+  // own buffers for the template-size working volumes
+  DevBuf work, lin;
+  BRC_TRY(ctx, work.ensure(sizeof(float) * V2), "alloc");
+  BRC_TRY(ctx, lin.ensure(sizeof(float) * (V2 + 12)), "alloc");
+  float* w = work.as<float>();
+  float* a = lin.as<float>();
+  float* dparams = a + V2;
+  int s = brc_change_resolution_and_size(ctx, d_in, W, H, D, voxel_size3, w, W2, H2, D2, tpl_voxel_size3,
+                                         o->mm_z_cut);
+  if (s != BRC_OK) return s;
+  float c1[3], c2[3];
+  if ((s = brc_center_of_mass(ctx, w, W2, H2, D2, c1)) != BRC_OK) return s;
+  if ((s = brc_center_of_mass(ctx, d_tpl, W2, H2, D2, c2)) != BRC_OK) return s;
+  float match[12] = {0};
+  for (int k = 0; k < 3; k++) match[k] = -(float)myround(c2[k] - c1[k]);
+  BRC_TRY(ctx, cudaMemcpyAsync(dparams, match, sizeof(match), cudaMemcpyHostToDevice, st), "H2D");
+  BRC_TRY(ctx, brc::warp_affine(w, V2, W2, H2, D2, 1, dparams, a, V2, nullptr, 0, st), "match");
+  ctx->launches += 1;
+  if (d_interpolated)
+    BRC_TRY(ctx, cudaMemcpyAsync(d_interpolated, a, sizeof(float) * V2, cudaMemcpyDeviceToDevice, st), "copy");
+  float total[12] = {0};
+  if (o->linear_iterations > 0) {
+    brc_linear_opts lo;
+    brc_linear_opts_default(&lo, o->linear_iterations);
+    lo.type = BRC_AFFINE;
+    lo.precision = o->precision;
+    DevBuf prm;
+    BRC_TRY(ctx, prm.ensure(sizeof(float) * 12), "alloc");
+    s = brc_register_linear_scales(ctx, d_tpl, a, W2, H2, D2, 1, h_filters3, &lo, o->coarsest_scale,
+                                   prm.as<float>(), w, nullptr);
+    if (s != BRC_OK) return s;
+    BRC_TRY(ctx, cudaMemcpyAsync(total, prm.as<float>(), sizeof(total), cudaMemcpyDeviceToHost, st), "D2H");
+    BRC_TRY(ctx, cudaStreamSynchronize(st), "sync");
+  } else {
+    BRC_TRY(ctx, cudaMemcpyAsync(w, a, sizeof(float) * V2, cudaMemcpyDeviceToDevice, st), "copy");
+  }
+  if (d_aligned_linear)
+    BRC_TRY(ctx, cudaMemcpyAsync(d_aligned_linear, w, sizeof(float) * V2, cudaMemcpyDeviceToDevice, st), "copy");
+  // total = match * linear (AddAffineRegistrationParameters(total, match))
+  {
+    double O[16] = {0}, N[16] = {0}, T[16];
+    const float* src[2] = {total, match};
+    double* dst[2] = {O, N};
+    for (int m = 0; m < 2; m++) {
+      const float* p = src[m];
+      double* M = dst[m];
+      M[0] = (double)(p[3] + 1.0f); M[1] = p[4]; M[2] = p[5]; M[3] = p[0];
+      M[4] = p[6]; M[5] = (double)(p[7] + 1.0f); M[6] = p[8]; M[7] = p[1];
+      M[8] = p[9]; M[9] = p[10]; M[10] = (double)(p[11] + 1.0f); M[11] = p[2];
+      M[15] = 1.0;
+    }
+    for (int i = 0; i < 4; i++)
+      for (int j = 0; j < 4; j++) {
+        double acc = 0;
+        for (int k = 0; k < 4; k++) acc += N[i * 4 + k] * O[k * 4 + j];
+        T[i * 4 + j] = acc;
+      }
+    total[0] = (float)T[3]; total[1] = (float)T[7]; total[2] = (float)T[11];
+    total[3] = (float)(T[0] - 1.0); total[4] = (float)T[1]; total[5] = (float)T[2];
+    total[6] = (float)T[4]; total[7] = (float)(T[5] - 1.0); total[8] = (float)T[6];
+    total[9] = (float)T[8]; total[10] = (float)T[9]; total[11] = (float)(T[10] - 1.0);
+  }
+  for (int i = 0; i < 12; i++) h_params12[i] = total[i];
+  if (o->nonlinear_iterations > 0) {
+    brc_nonlinear_opts no;
+    brc_nonlinear_opts_default(&no, o->nonlinear_iterations);
+    no.coarsest_scale = o->coarsest_scale;
+    no.tsigma = o->tsigma;
+    no.esigma = o->esigma;
+    no.dsigma = o->dsigma;
+    no.precision = o->precision;
+    no.solve_fp64 = o->solve_fp64;
+    s = brc_register_nonlinear(ctx, d_tpl, w, W2, H2, D2, h_filters6, h_tensors, h_dirs, &no, d_field, a);
+    if (s != BRC_OK) return s;
+    if (o->linear_iterations > 0) {
+      BRC_TRY(ctx, brc::add_affine_to_field(d_field, W2, H2, D2, total, st), "field");
+      ctx->launches += 1;
+      s = brc_change_resolution_and_size(ctx, d_in, W, H, D, voxel_size3, w, W2, H2, D2, tpl_voxel_size3,
+                                         o->mm_z_cut);
+      if (s != BRC_OK) return s;
+      BRC_TRY(ctx, brc::warp_field(w, W2, H2, D2, d_field, d_field + V2, d_field + 2 * V2, a, st), "warp");
+      ctx->launches += 1;
+    }
+    if (d_aligned_nonlinear)
+      BRC_TRY(ctx, cudaMemcpyAsync(d_aligned_nonlinear, a, sizeof(float) * V2, cudaMemcpyDeviceToDevice, st),
+              "copy");
+  }
+  BRC_TRY(ctx, cudaStreamSynchronize(st), "sync");
+  return BRC_OK;
+}
+
 extern "C" int brc_register_linear_scales(brc_ctx* ctx, const float* d_ref, const float* d_moving, int W,
                                           int H, int D, int batch, const float* h_filters,
                                           const brc_linear_opts* opts, int coarsest_scale,

@@ -8,11 +8,14 @@ namespace brc {
 cudaError_t filter3d_init();
 cudaError_t filter3d_fp32(const float* vol, int W, int H, int D, int batch, long long stride,
                           const float* h_filters, int nfilt, float* out, const int* conv_iter,
-                          int it, cudaStream_t st);
+                          int it, cudaStream_t st, bool allow_symmetric = true);
 // registration.cu
+// cert != nullptr: certainty volumes [batch][3][V] are computed into `cert`
+// and the sums use their 3x3x3 Gaussian smoothing (sigma cert_sigma).
 cudaError_t normal_eq_partials(const float* q1, long long q1_stride_floats, const float* q2, int W,
                                int H, int D, int batch, double* partials, int nblk, int zpb,
-                               const int* conv_iter, int it, cudaStream_t st);
+                               const int* conv_iter, int it, cudaStream_t st, const float* cert = nullptr,
+                               float cert_sigma = 0.f);
 cudaError_t assemble_normal_eq(const double* partials, int nblk, int batch, double* A, double* h,
                                cudaStream_t st);
 cudaError_t solve_update(const double* partials, int nblk, int batch, int type, float tol, int W,
@@ -42,4 +45,12 @@ cudaError_t rescale_batch(const float* src, int W, int H, int D, int batch, floa
                           int D2, float factor, cudaStream_t st);
 cudaError_t compose(float* total, const float* add, int batch, float tscale, cudaStream_t st);
 cudaError_t add_volumes(float* out, const float* a, const float* b, long long n, cudaStream_t st);
+}  // namespace brc
+
+namespace brc {
+cudaError_t resize_to_grid(const float* src, int W, int H, int D, float vx, float vy, float vz, float* out,
+                           int W2, int H2, int D2, float nvx, float nvy, float nvz, int mm_z_cut,
+                           cudaStream_t st);
+cudaError_t mass_moments(const float* vol, int W, int H, int D, double* sums, cudaStream_t st);
+cudaError_t add_affine_to_field(float* field, int W, int H, int D, const float* p12, cudaStream_t st);
 }  // namespace brc

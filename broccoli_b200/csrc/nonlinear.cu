@@ -252,9 +252,136 @@ add_kernel(float* __restrict__ out, const float* __restrict__ a, const float* __
   if (i < n) out[i] = a[i] + b[i];
 }
 
+// Resample to new voxel sizes and centre in / crop to a new grid in one pass:
+// new(xn) = interp(xi) where xi is xn shifted by the centring offsets (and
+// mm_z_cut along z) and interp is the linear resample with spacing
+// (N-1)/(Ni-1); uncovered voxels are 0.  ChangeVolumesResolutionAndSize,
+// broccoli_lib.cpp:6950-7100, fusing RescaleVolumeLinear and
+// CopyVolumeToNew (kernelRegistration.cpp:1340-1366, :1593-1678).
+struct ResizeGeom {
+  int Wi, Hi, Di;     // interpolated size
+  int offn[3];        // added to the loop index to get the new-grid index
+  int offi[3];        // added to the loop index to get the interpolated index
+  float vd[3];        // (N-1)/(Ni-1)
+};
+
+__global__ void __launch_bounds__(256)
+resize_to_grid_kernel(const float* __restrict__ src, int W, int H, int D, float* __restrict__ out, int W2,
+                      int H2, int D2, ResizeGeom g) {
+  const long long V2 = (long long)W2 * H2 * D2;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V2) return;
+  const int xn = (int)(i % W2), yn = (int)((i / W2) % H2), zn = (int)(i / ((long long)W2 * H2));
+  const int x = xn - g.offn[0], y = yn - g.offn[1], z = zn - g.offn[2];
+  const int xi = x + g.offi[0], yi = y + g.offi[1], zi = z + g.offi[2];
+  float v = 0.f;
+  if (x >= 0 && y >= 0 && z >= 0 && xi >= 0 && yi >= 0 && zi >= 0 && xi < g.Wi && yi < g.Hi && zi < g.Di)
+    v = sample_lin(src, W, H, D, xi * g.vd[0] + 0.5f, yi * g.vd[1] + 0.5f, zi * g.vd[2] + 0.5f);
+  out[i] = v;
+}
+
+// Sums of m, m x, m y, m z over the volume in FP64 (centre of mass;
+// CalculateCenterOfMass, broccoli_lib.cpp:6763-6800, accumulates in float
+// on the host after a full device-to-host copy).
+__global__ void __launch_bounds__(256)
+mass_moments_kernel(const float* __restrict__ vol, int W, int H, int D, double* __restrict__ sums) {
+  const long long V = (long long)W * H * D;
+  double m = 0, mx = 0, my = 0, mz = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < V;
+       i += (long long)gridDim.x * blockDim.x) {
+    const double v = vol[i];
+    const int x = (int)(i % W), y = (int)((i / W) % H), z = (int)(i / ((long long)W * H));
+    m += v;
+    mx += v * x;
+    my += v * y;
+    mz += v * z;
+  }
+  double s[4] = {m, mx, my, mz};
+  __shared__ double red[8][4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s[k] += __shfl_down_sync(0xffffffffu, s[k], o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][k] = s[k];
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w][threadIdx.x];
+    atomicAdd(sums + threadIdx.x, t);
+  }
+}
+
+// field += t + (A - I)(x - c) (AddLinearAndNonLinearDisplacement,
+// kernelRegistration.cpp:1142-1178).
+struct Params12 {
+  float p[12];
+};
+
+__global__ void __launch_bounds__(256)
+add_affine_to_field_kernel(float* __restrict__ field, int W, int H, int D, Params12 prm) {
+  const long long V = (long long)W * H * D;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V) return;
+  const int x = (int)(i % W), y = (int)((i / W) % H), z = (int)(i / ((long long)W * H));
+  const float* p = prm.p;
+  const float xf = (float)x - ((float)W - 1.0f) * 0.5f;
+  const float yf = (float)y - ((float)H - 1.0f) * 0.5f;
+  const float zf = (float)z - ((float)D - 1.0f) * 0.5f;
+  field[i] += p[0] + p[3] * xf + p[4] * yf + p[5] * zf;
+  field[V + i] += p[1] + p[6] * xf + p[7] * yf + p[8] * zf;
+  field[2 * V + i] += p[2] + p[9] * xf + p[10] * yf + p[11] * zf;
+}
+
 // ---------------------------------------------------------------------------
 
 static unsigned grid1(long long n) { return (unsigned)((n + 255) / 256); }
+
+static int round_half_away(float v) { return (int)roundf(v); }
+
+cudaError_t resize_to_grid(const float* src, int W, int H, int D, float vx, float vy, float vz, float* out,
+                           int W2, int H2, int D2, float nvx, float nvy, float nvz, int mm_z_cut,
+                           cudaStream_t st) {
+  ResizeGeom g;
+  g.Wi = (int)floorf((float)W * vx / nvx + 0.5f);
+  g.Hi = (int)floorf((float)H * vy / nvy + 0.5f);
+  g.Di = (int)floorf((float)D * vz / nvz + 0.5f);
+  if (g.Wi < 2 || g.Hi < 2 || g.Di < 2) return cudaErrorInvalidValue;
+  const int diff[3] = {g.Wi - W2, g.Hi - H2, g.Di - D2};
+  const int zcut = (int)round((float)mm_z_cut / nvz);
+  for (int a = 0; a < 3; a++) {
+    const int half = round_half_away((float)(diff[a] > 0 ? diff[a] : -diff[a]) / 2.0f);
+    if (diff[a] > 0) {
+      g.offn[a] = 0;
+      g.offi[a] = half;
+    } else {
+      g.offn[a] = half;
+      g.offi[a] = 0;
+    }
+  }
+  g.offi[2] += zcut;
+  g.vd[0] = (float)(W - 1) / (float)(g.Wi - 1);
+  g.vd[1] = (float)(H - 1) / (float)(g.Hi - 1);
+  g.vd[2] = (float)(D - 1) / (float)(g.Di - 1);
+  resize_to_grid_kernel<<<grid1((long long)W2 * H2 * D2), 256, 0, st>>>(src, W, H, D, out, W2, H2, D2, g);
+  return cudaGetLastError();
+}
+
+cudaError_t mass_moments(const float* vol, int W, int H, int D, double* sums, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(sums, 0, 4 * sizeof(double), st);
+  if (e != cudaSuccess) return e;
+  long long blocks = ((long long)W * H * D + 255) / 256;
+  if (blocks > 148 * 4) blocks = 148 * 4;
+  mass_moments_kernel<<<(unsigned)blocks, 256, 0, st>>>(vol, W, H, D, sums);
+  return cudaGetLastError();
+}
+
+cudaError_t add_affine_to_field(float* field, int W, int H, int D, const float* p12, cudaStream_t st) {
+  Params12 prm;
+  for (int i = 0; i < 12; i++) prm.p[i] = p12[i];
+  add_affine_to_field_kernel<<<grid1((long long)W * H * D), 256, 0, st>>>(field, W, H, D, prm);
+  return cudaGetLastError();
+}
 
 cudaError_t tensor_norm_max(const float* t6, long long V, float* a11, unsigned int* maxbits,
                             cudaStream_t st) {

@@ -61,10 +61,51 @@ __device__ __forceinline__ float phase_grad(float2 a_p, float2 a_c, float2 a_m, 
 // CalculateAMatrix1DValues / HVector1DValues and CalculateAMatrix /
 // HVector accumulate (kernelRegistration.cpp:387-800).  One CTA handles
 // `zpb` interior slices of one instance and writes 42 FP64 partial sums.
+// Certainty volumes |q1 q2| cos^2(dphi/2) of the three filter pairs of every
+// active instance, [b][k][voxel]; input of the optional certainty smoothing.
+__global__ void __launch_bounds__(256)
+certainty_kernel(const float2* __restrict__ q1, long long q1_stride, const float2* __restrict__ q2, int W,
+                 int H, int D, float* __restrict__ cert, const int* __restrict__ conv_iter, int it) {
+  const int b = blockIdx.y;
+  if (instance_done(conv_iter, b, it)) return;
+  const long long V = (long long)W * H * D;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V) return;
+  const float2* Q1 = q1 + (long long)b * q1_stride;
+  const float2* Q2 = q2 + (long long)b * 3 * V;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    float pd, c;
+    phase_diff_cert(__ldg(Q1 + k * V + i), __ldg(Q2 + k * V + i), pd, c);
+    cert[((long long)b * 3 + k) * V + i] = c;
+  }
+}
+
+// Separable 3x3x3 Gaussian (weights w1, w0, w1 per axis, normalised) of a
+// certainty volume at an interior voxel (all 27 neighbours inside).
+__device__ __forceinline__ float smoothed_certainty(const float* __restrict__ c, long long i, int W,
+                                                   long long WH, float w0, float w1) {
+  const float w[3] = {w1, w0, w1};
+  float s = 0.f;
+#pragma unroll
+  for (int dz = -1; dz <= 1; dz++) {
+    float sy = 0.f;
+#pragma unroll
+    for (int dy = -1; dy <= 1; dy++) {
+      const float* r = c + i + dz * WH + (long long)dy * W;
+      const float sx = w1 * __ldg(r - 1) + w0 * __ldg(r) + w1 * __ldg(r + 1);
+      sy += w[dy + 1] * sx;
+    }
+    s += w[dz + 1] * sy;
+  }
+  return s;
+}
+
 __global__ void __launch_bounds__(kNEThreads)
 normal_eq_partial_kernel(const float2* __restrict__ q1, long long q1_stride,
                          const float2* __restrict__ q2, int W, int H, int D, int zpb,
-                         double* __restrict__ partials, const int* __restrict__ conv_iter, int it) {
+                         double* __restrict__ partials, const int* __restrict__ conv_iter, int it,
+                         const float* __restrict__ cert_in, float cw0, float cw1) {
   const int b = blockIdx.y;
   if (instance_done(conv_iter, b, it)) return;
   const long long V = (long long)W * H * D;
@@ -95,6 +136,8 @@ normal_eq_partial_kernel(const float2* __restrict__ q1, long long q1_stride,
       const float2 a = __ldg(A + i), c = __ldg(C + i);
       float pd, cert;
       phase_diff_cert(a, c, pd, cert);
+      if (cert_in != nullptr)
+        cert = smoothed_certainty(cert_in + ((long long)b * 3 + k) * V, i, W, (long long)W * H, cw0, cw1);
       const float g = phase_grad(__ldg(A + i + s), a, __ldg(A + i - s), __ldg(C + i + s), c,
                                  __ldg(C + i - s));
       const float cg = cert * g;
@@ -614,11 +657,23 @@ smooth_pass_kernel(const float* __restrict__ in, long long in_stride, const floa
 
 cudaError_t normal_eq_partials(const float* q1, long long q1_stride_floats, const float* q2, int W,
                                int H, int D, int batch, double* partials, int nblk, int zpb,
-                               const int* conv_iter, int it, cudaStream_t st) {
+                               const int* conv_iter, int it, cudaStream_t st, const float* cert,
+                               float cert_sigma) {
+  float w0 = 1.f, w1 = 0.f;
+  if (cert != nullptr) {
+    // 3-tap Gaussian, weights normalised to sum 1
+    const float e = (float)exp(-1.0 / (2.0 * (double)cert_sigma * (double)cert_sigma));
+    w0 = 1.0f / (1.0f + 2.0f * e);
+    w1 = e * w0;
+    dim3 cgrid((unsigned)(((long long)W * H * D + 255) / 256), batch);
+    certainty_kernel<<<cgrid, 256, 0, st>>>(reinterpret_cast<const float2*>(q1), q1_stride_floats / 2,
+                                            reinterpret_cast<const float2*>(q2), W, H, D,
+                                            const_cast<float*>(cert), conv_iter, it);
+  }
   dim3 grid(nblk, batch);
   normal_eq_partial_kernel<<<grid, kNEThreads, 0, st>>>(
       reinterpret_cast<const float2*>(q1), q1_stride_floats / 2, reinterpret_cast<const float2*>(q2),
-      W, H, D, zpb, partials, conv_iter, it);
+      W, H, D, zpb, partials, conv_iter, it, cert, w0, w1);
   return cudaGetLastError();
 }
 

@@ -128,6 +128,67 @@ def motion_series(T: int = 200, shape=(33, 64, 64), base_seed: int = 0, snr: flo
     return vols, truth
 
 
+def head_phantom(shape, seed: int = 0, scale=None) -> np.ndarray:
+    """T1-like head: three nested ellipsoidal tissue classes at intensities
+    300 / 600 / 900 (outer, middle, inner), a few inner ellipsoidal
+    structures, a smooth multiplicative bias field (second-order polynomial,
+    within +-20 %) and Gaussian noise of sigma 15.  `scale` (3 floats, voxels
+    per unit) sets the head size; by default it fills ~80 % of the grid."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    D, H, W = shape
+    z, y, x = np.meshgrid(np.arange(D), np.arange(H), np.arange(W), indexing="ij")
+    c = np.array([(W - 1) / 2.0, (H - 1) / 2.0, (D - 1) / 2.0])
+    r = np.array([0.40 * W, 0.42 * H, 0.40 * D]) if scale is None else np.asarray(scale, np.float64)
+    px, py, pz = (x - c[0]) / r[0], (y - c[1]) / r[1], (z - c[2]) / r[2]
+    rho = np.sqrt(px * px + py * py + pz * pz)
+    vol = np.zeros(shape)
+    vol[rho <= 1.0] = 300.0
+    vol[rho <= 0.85] = 600.0
+    vol[rho <= 0.6] = 900.0
+    for _ in range(6):
+        cc = rng.uniform(-0.4, 0.4, 3)
+        ax = rng.uniform(0.08, 0.2, 3)
+        inside = ((px - cc[0]) / ax[0]) ** 2 + ((py - cc[1]) / ax[1]) ** 2 + ((pz - cc[2]) / ax[2]) ** 2 <= 1
+        vol[inside & (rho <= 0.85)] = rng.choice([300.0, 600.0])
+    coef = rng.uniform(-1, 1, 9)
+    bias = (coef[0] * px + coef[1] * py + coef[2] * pz + coef[3] * px * py + coef[4] * py * pz +
+            coef[5] * px * pz + coef[6] * px * px + coef[7] * py * py + coef[8] * pz * pz)
+    bias = 1.0 + 0.2 * bias / max(np.abs(bias).max(), 1e-12)
+    vol = vol * bias + rng.standard_normal(shape) * 15.0
+    return vol.astype(np.float32)
+
+
+def smooth_field(shape, seed: int = 200, max_mm: float = 6.0, sigma: float = 8.0) -> np.ndarray:
+    """Smooth displacement field (3, D, H, W) in voxels (1 mm voxels):
+    Gaussian-smoothed white noise scaled so the largest displacement
+    magnitude is max_mm."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    f = np.stack([ndimage.gaussian_filter(rng.standard_normal(shape), sigma, mode="nearest")
+                  for _ in range(3)])
+    mag = np.sqrt((f * f).sum(0)).max()
+    return (f * (max_mm / max(mag, 1e-12))).astype(np.float32)
+
+
+def warp_with_field(vol: np.ndarray, field: np.ndarray) -> np.ndarray:
+    """vol sampled at x + field(x) (trilinear, clamped)."""
+    D, H, W = vol.shape
+    z, y, x = np.meshgrid(np.arange(D), np.arange(H), np.arange(W), indexing="ij")
+    coords = np.stack([z + field[2], y + field[1], x + field[0]])
+    return ndimage.map_coordinates(vol.astype(np.float64), coords, order=1, mode="nearest").astype(np.float32)
+
+
+def t1_template_pair(subject_shape=(170, 256, 256), template_shape=(182, 218, 182), seed: int = 0):
+    """A subject T1-like head warped by a smooth field (seed 200, max 6 mm)
+    and a template built the same way (different seed, no warp), both 1 mm.
+    Shapes are (D, H, W).  Returns (subject, template, field)."""
+    tpl = head_phantom(template_shape, seed=seed + 1)
+    sub = head_phantom(subject_shape, seed=seed,
+                       scale=np.array([0.40 * template_shape[2], 0.42 * template_shape[1],
+                                       0.40 * template_shape[0]]))
+    fld = smooth_field(subject_shape, seed=200 + seed, max_mm=6.0, sigma=max(2.0, min(subject_shape) / 20))
+    return warp_with_field(sub, fld), tpl, fld
+
+
 def relative_params(p_ref, p_t) -> np.ndarray:
     """Parameters that map volume t onto the reference volume when both are
     moved copies of one base: compose T_ref^-1 ... expressed as the

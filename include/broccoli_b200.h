@@ -50,10 +50,13 @@ typedef enum {
 /* Alignment types, same values as broccoli_constants.h:93-95. */
 enum { BRC_TRANSLATION = 0, BRC_RIGID = 1, BRC_AFFINE = 2 };
 
-/* Arithmetic of the 7^3 filtering.  FP32: plain fp32 FMA on the CUDA cores.
- * BF16X3: split-bf16 (hi*hi + hi*lo + lo*hi) products on the tensor cores
- * with fp32 accumulation. */
-enum { BRC_PREC_FP32 = 0, BRC_PREC_BF16X3 = 1 };
+/* Arithmetic of the 7^3 filtering.  FP32: fp32 FMA on the CUDA cores; a
+ * bank whose filters have even real and odd imaginary parts (to 1e-6 of
+ * the largest tap, true of quadrature filters) uses the half-tap even/odd
+ * form.  FP32_GENERAL: fp32, always all 343 taps.  BF16X3: split-bf16
+ * (hi*hi + hi*lo + lo*hi) products on the tensor cores with fp32
+ * accumulation. */
+enum { BRC_PREC_FP32 = 0, BRC_PREC_BF16X3 = 1, BRC_PREC_FP32_GENERAL = 2 };
 
 typedef struct brc_ctx brc_ctx;
 
@@ -242,6 +245,66 @@ int brc_register_nonlinear(brc_ctx* ctx, const float* d_ref, const float* d_movi
                            int D, const float* h_filters6, const float* h_tensors,
                            const float* h_dirs, const brc_nonlinear_opts* opts, float* d_field,
                            float* d_aligned);
+
+/* ---- device memory and host copies (for hosts without a CUDA runtime) --- */
+
+/* cudaMalloc / cudaFree on the context's device.  Replaces the clCreateBuffer
+ * / clReleaseMemObject pairs of the reference's Setup/Cleanup functions
+ * (e.g. broccoli_lib.cpp:5072-5266). */
+int brc_device_alloc(brc_ctx* ctx, size_t bytes, void** d_out);
+int brc_device_free(brc_ctx* ctx, void* d_ptr);
+/* Copies on the context's stream; both return after the copy completed.
+ * Replace clEnqueueWriteBuffer / clEnqueueReadBuffer with CL_TRUE. */
+int brc_copy_to_device(brc_ctx* ctx, void* d_dst, const void* h_src, size_t bytes);
+int brc_copy_to_host(brc_ctx* ctx, void* h_dst, const void* d_src, size_t bytes);
+
+/* ---- the steps either side of the registration loops -------------------- */
+
+/* Resample d_src (voxel sizes voxel_size3, mm) to new_voxel_size3 and
+ * centre it in / crop it to a W2 x H2 x D2 grid, shifted by mm_z_cut mm
+ * along z; uncovered voxels are 0.
+ * Replaces ChangeVolumesResolutionAndSize (broccoli_lib.cpp:6950-7100)
+ * with RescaleVolumeLinear and CopyVolumeToNew (kernelRegistration.cpp:
+ * 1340-1366, :1593-1678). */
+int brc_change_resolution_and_size(brc_ctx* ctx, const float* d_src, int W, int H, int D,
+                                   const float* voxel_size3, float* d_out, int W2, int H2, int D2,
+                                   const float* new_voxel_size3, int mm_z_cut);
+
+/* Centre of mass (voxel coordinates) of a volume, FP64 reduction on the
+ * device; synchronises.  Replaces CalculateCenterOfMass
+ * (broccoli_lib.cpp:6763-6800, a host loop after a full device-to-host
+ * copy). */
+int brc_center_of_mass(brc_ctx* ctx, const float* d_vol, int W, int H, int D, float* h_com3);
+
+typedef struct {
+  int linear_iterations;     /* NUMBER_OF_ITERATIONS_FOR_LINEAR_IMAGE_REGISTRATION */
+  int nonlinear_iterations;  /* ... _NONLINEAR_ ...; 0 skips the nonlinear stage   */
+  int coarsest_scale;        /* COARSEST_SCALE_T1_MNI                              */
+  int mm_z_cut;              /* MM_T1_Z_CUT                                        */
+  float tsigma, esigma, dsigma;
+  int precision;
+  int solve_fp64;
+} brc_two_volume_opts;
+
+void brc_two_volume_opts_default(brc_two_volume_opts* opts);
+
+/* T1-to-template normalisation of one volume: resample onto the template
+ * grid, match centres of mass, multi-scale affine registration, parameters
+ * composed with the mass match (h_params12, host), multi-scale nonlinear
+ * registration, affine motion added to the field, and one final warp of a
+ * fresh resample by the combined field.  Output volumes are template size
+ * and optional (NULL to skip); d_field (3 volumes) is required when the
+ * nonlinear stage runs.  Synchronises before returning.
+ * Replaces PerformRegistrationTwoVolumesWrapper (broccoli_lib.cpp:
+ * 7973-8112) with MatchVolumeMasses (:6876-6948) and
+ * CreateCombinedDisplacementField (:8115-8150). */
+int brc_register_two_volumes(brc_ctx* ctx, const float* d_in, int W, int H, int D,
+                             const float* voxel_size3, const float* d_tpl, int W2, int H2, int D2,
+                             const float* tpl_voxel_size3, const float* h_filters3,
+                             const float* h_filters6, const float* h_tensors, const float* h_dirs,
+                             const brc_two_volume_opts* opts, float* h_params12,
+                             float* d_interpolated, float* d_aligned_linear,
+                             float* d_aligned_nonlinear, float* d_field);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,215 @@
+/*
+ * broccoli_lib.h -- drop-in BROCCOLI_LIB class for the registration and
+ * filtering path, implemented on the C-ABI of libbroccoli_b200
+ * (broccoli_b200.h) instead of OpenCL.
+ *
+ * It keeps the reference's class interface (code/BROCCOLI_LIB/
+ * broccoli_lib.h:108-467) for the members this path uses: the same
+ * constructors, OpenCLInitiate / GetOpenCLInitiated, the raw-pointer
+ * setters (the caller owns every host array; setters store the pointer),
+ * the Perform*Wrapper() entry points and the error getters.  No OpenCL
+ * header is needed: cl_uint and cl_float2 are layout-compatible stand-ins.
+ * Members of the reference outside this path (statistics, ICA, ...) are not
+ * declared.
+ *
+ * Behaviour notes (same as the reference unless stated):
+ *   - OpenCLInitiate(platform, device): platform must be 0; device is the
+ *     CUDA device index.
+ *   - PerformMotionCorrectionWrapper corrects h_fMRI_Volumes in place and
+ *     writes 6 x T motion parameters (mm, degrees); when an output series is
+ *     set with SetOutputMotionCorrectedfMRIVolumes it is filled as well.
+ *   - PerformRegistrationTwoVolumesWrapper: T1 -> MNI, single volume.
+ *   - PerformSmoothingWrapper: LOWPASS (from SetEPISmoothingAmount, FWHM in
+ *     mm) or RANDOM (filters from SetSmoothingFilters).
+ *   - Extensions (new setters): SetPrecision, SetMotionCorrectionTolerance,
+ *     SetSolveFP64.
+ */
+#ifndef BROCCOLI_LIB_B200_H
+#define BROCCOLI_LIB_B200_H
+
+#include <stddef.h>
+
+#include <string>
+
+#include "broccoli_b200.h"
+
+typedef unsigned int cl_uint;
+typedef union {
+  float s[2];
+  struct {
+    float x, y;
+  };
+} cl_float2;
+
+/* values of code/BROCCOLI_LIB/broccoli_constants.h used on this path */
+#ifndef BROCCOLI_CONSTANTS_H
+#define MATLAB 0
+#define PYTHON 1
+#define BASH 2
+#define TRANSLATION 0
+#define RIGID 1
+#define AFFINE 2
+#define NEAREST 0
+#define LINEAR 1
+#define CUBIC 2
+#define DO_OVERWRITE 0
+#define NO_OVERWRITE 1
+#define SUCCESS 0
+#define FAIL 1
+#define LOWPASS 0
+#define RANDOM 1
+#endif
+
+class BROCCOLI_LIB {
+ public:
+  BROCCOLI_LIB();
+  BROCCOLI_LIB(cl_uint platform, cl_uint device);
+  BROCCOLI_LIB(cl_uint platform, cl_uint device, const char* location);
+  BROCCOLI_LIB(cl_uint platform, cl_uint device, int wrapper, bool verbos);
+  ~BROCCOLI_LIB();
+
+  bool OpenCLInitiate(cl_uint platform, cl_uint device);
+  bool GetOpenCLInitiated();
+  std::string GetOpenCLInitializationError();
+  const char* GetOpenCLError();
+  const char* GetOpenCLErrorMessage(int error);
+  int* GetOpenCLRunKernelErrors();
+
+  void SetWrapper(int wrapper);
+  void SetVerbose(bool verbos);
+  void SetDebug(bool debug);
+
+  // sizes and voxel sizes
+  void SetEPIWidth(size_t w);
+  void SetEPIHeight(size_t h);
+  void SetEPIDepth(size_t d);
+  void SetEPITimepoints(size_t t);
+  void SetEPIVoxelSizeX(float v);
+  void SetEPIVoxelSizeY(float v);
+  void SetEPIVoxelSizeZ(float v);
+  void SetT1Width(size_t w);
+  void SetT1Height(size_t h);
+  void SetT1Depth(size_t d);
+  void SetT1Timepoints(size_t t);
+  void SetT1VoxelSizeX(float v);
+  void SetT1VoxelSizeY(float v);
+  void SetT1VoxelSizeZ(float v);
+  void SetMNIWidth(size_t w);
+  void SetMNIHeight(size_t h);
+  void SetMNIDepth(size_t d);
+  void SetMNIVoxelSizeX(float v);
+  void SetMNIVoxelSizeY(float v);
+  void SetMNIVoxelSizeZ(float v);
+
+  // inputs
+  void SetInputfMRIVolumes(float* input);
+  void SetInputEPIVolume(float* input);
+  void SetInputT1Volume(float* input);
+  void SetInputMNIVolume(float* input);
+  void SetInputMNIBrainVolume(float* input);
+
+  // filters and algorithm settings
+  void SetImageRegistrationFilterSize(int N);
+  void SetLinearImageRegistrationFilters(float* qf1r, float* qf1i, float* qf2r, float* qf2i, float* qf3r,
+                                         float* qf3i);
+  void SetNonLinearImageRegistrationFilters(float* qf1r, float* qf1i, float* qf2r, float* qf2i, float* qf3r,
+                                            float* qf3i, float* qf4r, float* qf4i, float* qf5r, float* qf5i,
+                                            float* qf6r, float* qf6i);
+  void SetProjectionTensorMatrixFirstFilter(float m11, float m12, float m13, float m22, float m23, float m33);
+  void SetProjectionTensorMatrixSecondFilter(float m11, float m12, float m13, float m22, float m23, float m33);
+  void SetProjectionTensorMatrixThirdFilter(float m11, float m12, float m13, float m22, float m23, float m33);
+  void SetProjectionTensorMatrixFourthFilter(float m11, float m12, float m13, float m22, float m23, float m33);
+  void SetProjectionTensorMatrixFifthFilter(float m11, float m12, float m13, float m22, float m23, float m33);
+  void SetProjectionTensorMatrixSixthFilter(float m11, float m12, float m13, float m22, float m23, float m33);
+  void SetFilterDirections(float* x, float* y, float* z);
+  void SetNumberOfIterationsForLinearImageRegistration(int N);
+  void SetNumberOfIterationsForNonLinearImageRegistration(int N);
+  void SetNumberOfIterationsForMotionCorrection(int N);
+  void SetChangeMotionCorrectionReferenceVolume(bool change);
+  void SetMotionCorrectionReferenceVolume(float* reference);
+  void SetCoarsestScaleT1MNI(int N);
+  void SetMMT1ZCUT(int mm);
+  void SetInterpolationMode(int mode);
+  void SetTsigma(float s);
+  void SetEsigma(float s);
+  void SetDsigma(float s);
+  void SetSmoothingFilters(float* fx, float* fy, float* fz);
+  void SetSmoothingType(int type);
+  void SetEPISmoothingAmount(float fwhm_mm);
+
+  // extensions of this implementation
+  void SetPrecision(int precision);             // BRC_PREC_FP32 / BRC_PREC_BF16X3
+  void SetMotionCorrectionTolerance(float voxels);  // per-volume early exit (0: off)
+  void SetSolveFP64(bool fp64);                 // per-voxel 3x3 solves in FP64
+
+  // outputs (caller-allocated host arrays)
+  void SetOutputMotionParameters(float* output);
+  void SetOutputMotionCorrectedfMRIVolumes(float* output);
+  void SetOutputT1MNIRegistrationParameters(float* output);
+  void SetOutputAlignedT1VolumeLinear(float* output);
+  void SetOutputAlignedT1VolumeNonLinear(float* output);
+  void SetOutputInterpolatedT1Volume(float* output);
+  void SetOutputDisplacementField(float* x, float* y, float* z);
+  void SetOutputSmoothedfMRIVolumes(float* output);
+  void SetOutputQuadratureFilterResponses(cl_float2* q1, cl_float2* q2, cl_float2* q3);
+
+  // entry points
+  void PerformMotionCorrectionWrapper();
+  void PerformRegistrationTwoVolumesWrapper();
+  void PerformSmoothingWrapper();
+
+  int GetLastStatus() const { return last_status_; }
+
+ private:
+  brc_ctx* ctx_ = nullptr;
+  bool initiated_ = false;
+  std::string init_error_;
+  int last_status_ = BRC_OK;
+  int run_errors_[200] = {0};
+  int wrapper_ = BASH;
+  bool verbose_ = false;
+
+  size_t epi_w_ = 0, epi_h_ = 0, epi_d_ = 0, epi_t_ = 0;
+  size_t t1_w_ = 0, t1_h_ = 0, t1_d_ = 0, t1_t_ = 1;
+  size_t mni_w_ = 0, mni_h_ = 0, mni_d_ = 0;
+  float epi_vox_[3] = {1, 1, 1}, t1_vox_[3] = {1, 1, 1}, mni_vox_[3] = {1, 1, 1};
+
+  float* h_fmri_ = nullptr;
+  float* h_epi_ = nullptr;
+  float* h_t1_ = nullptr;
+  float* h_mni_ = nullptr;
+  float* h_mni_brain_ = nullptr;
+  float* h_mc_reference_ = nullptr;
+
+  int filter_size_ = 7;
+  const float* lin_[6] = {nullptr};
+  const float* nonlin_[12] = {nullptr};
+  float tensors_[36] = {0};
+  const float* dirs_[3] = {nullptr};
+  int it_linear_ = 10, it_nonlinear_ = 10, it_mc_ = 5;
+  bool change_mc_reference_ = false;
+  int coarsest_ = 4, mm_z_cut_ = 0, interpolation_ = LINEAR;
+  float tsigma_ = 5.0f, esigma_ = 5.0f, dsigma_ = 5.0f;
+  const float* smooth_f_[3] = {nullptr};
+  int smoothing_type_ = LOWPASS;
+  float epi_fwhm_ = 8.0f;
+  int precision_ = BRC_PREC_FP32;
+  float mc_tolerance_ = 0.0f;
+  bool solve_fp64_ = false;
+
+  float* out_motion_ = nullptr;
+  float* out_mc_ = nullptr;
+  float* out_params_ = nullptr;
+  float* out_aligned_lin_ = nullptr;
+  float* out_aligned_nonlin_ = nullptr;
+  float* out_interpolated_ = nullptr;
+  float* out_field_[3] = {nullptr};
+  float* out_smoothed_ = nullptr;
+  cl_float2* out_q_[3] = {nullptr};
+
+  bool check(int status, const char* where);
+  bool pack_linear(float* bank3);
+  bool pack_nonlinear(float* bank6, float* dirs18);
+};
+
+#endif

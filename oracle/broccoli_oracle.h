@@ -36,6 +36,9 @@ enum { ORC_TRANSLATION = 0, ORC_RIGID = 1, ORC_AFFINE = 2 };
                         real* A144, real* h12);                                 \
   void orc_normal_equations##SFX(const real* q1, const real* q2, int W, int H,  \
                                  int D, real* A144, real* h12);                 \
+  void orc_normal_equations_smoothcert##SFX(const real* q1, const real* q2,     \
+                                            int W, int H, int D, double sigma,  \
+                                            real* A144, real* h12);             \
   void orc_solve##SFX(const real* A, const real* h, int n, real* p);            \
   void orc_remove_scaling##SFX(real* p12);                                      \
   void orc_add_affine##SFX(real* old12, const real* new12);                     \
@@ -83,7 +86,23 @@ enum { ORC_TRANSLATION = 0, ORC_RIGID = 1, ORC_AFFINE = 2 };
   void orc_align_nonlinear_scales##SFX(                                         \
       const real* ref, real* aligned, int W, int H, int D, int coarsest,        \
       const real* filters6, const real* tensors, const real* dirs, int niter,   \
-      double tsigma, double esigma, double dsigma, real* field);
+      double tsigma, double esigma, double dsigma, real* field);                \
+  void orc_change_resolution_and_size##SFX(                                     \
+      const real* src, int W, int H, int D, float vx, float vy, float vz,       \
+      real* out, int W2, int H2, int D2, float nvx, float nvy, float nvz,       \
+      int mm_z_cut);                                                            \
+  void orc_center_of_mass##SFX(const real* vol, int W, int H, int D, real* c3); \
+  void orc_match_volume_masses##SFX(real* v1, const real* v2, int W, int H,     \
+                                    int D, real* p12);                          \
+  void orc_add_linear_nonlinear##SFX(real* field, int W, int H, int D,          \
+                                     const real* p);                            \
+  void orc_register_two_volumes##SFX(                                           \
+      const real* in, int W, int H, int D, const float* vin, const real* tpl,   \
+      int W2, int H2, int D2, const float* vtpl, int mm_z_cut, int coarsest,    \
+      int lin_iter, int nl_iter, const real* filters3, const real* filters6,    \
+      const real* tensors, const real* dirs, double tsigma, double esigma,      \
+      double dsigma, real* p12, real* interpolated, real* aligned_linear,       \
+      real* aligned_nonlinear, real* field);
 
 ORC_DECLARE(float, _f32)
 ORC_DECLARE(double, _f64)

@@ -421,3 +421,113 @@ def ref_smooth3d(vol: np.ndarray, fx, fy, fz, cert=None, smoothed_cert=None):
                            _ptr(sc) if sc is not None else None, W, H, D,
                            _ptr(fxa), _ptr(fya), _ptr(fza), _ptr(out))
     return out
+
+
+def ref_align_linear_scales(ref: np.ndarray, moving: np.ndarray, filters: np.ndarray, niter: int,
+                            coarsest: int, type_: int = AFFINE):
+    D, H, W = ref.shape
+    r = _arr(ref, np.float32)
+    aligned = _arr(moving, np.float32).copy()
+    f = _arr(filters, np.float32)
+    p = np.zeros(12, np.float32)
+    rot = np.zeros(3, np.float32)
+    ref_lib().ref_align_linear_scales(_ptr(r), _ptr(aligned), W, H, D, coarsest, _ptr(f), niter, type_,
+                                      _ptr(p), _ptr(rot))
+    return p, aligned, rot
+
+
+def ref_align_nonlinear_scales(ref: np.ndarray, moving: np.ndarray, bank: dict, niter: int, coarsest: int,
+                               tsigma=5.0, esigma=5.0, dsigma=5.0):
+    D, H, W = ref.shape
+    r = _arr(ref, np.float32)
+    aligned = _arr(moving, np.float32).copy()
+    f6, m, d = _nl_args(bank, np.float32)
+    field = np.zeros((3, D, H, W), np.float32)
+    fn = ref_lib().ref_align_nonlinear_scales
+    fn.argtypes = [_P, _P, _I, _I, _I, _I, _P, _P, _P, _I, _D, _D, _D, _P]
+    fn(_ptr(r), _ptr(aligned), W, H, D, coarsest, _ptr(f6), _ptr(m), _ptr(d), niter, tsigma, esigma,
+       dsigma, _ptr(field))
+    return field, aligned
+
+
+def _r2v_args(bank):
+    return (_arr(bank["linear"], np.float32), _arr(bank["nonlinear"], np.float32),
+            _arr(bank["projection_tensors"], np.float32), _arr(bank["directions"], np.float32))
+
+
+def _register_two_volumes(lib_fn, dt, subject, vin, template, vtpl, bank, lin_iter, nl_iter, coarsest,
+                          mm_z_cut=0, tsigma=5.0, esigma=5.0, dsigma=5.0):
+    D, H, W = subject.shape
+    D2, H2, W2 = template.shape
+    s = _arr(subject, dt)
+    t = _arr(template, dt)
+    f3, f6, m, d = (_arr(a, dt) for a in _r2v_args(bank))
+    v1 = np.asarray(vin, np.float32)
+    v2 = np.asarray(vtpl, np.float32)
+    p = np.zeros(12, dt)
+    interp = np.zeros((D2, H2, W2), dt)
+    al = np.zeros_like(interp)
+    anl = np.zeros_like(interp)
+    field = np.zeros((3, D2, H2, W2), dt)
+    lib_fn.argtypes = [_P, _I, _I, _I, _P, _P, _I, _I, _I, _P, _I, _I, _I, _I, _P, _P, _P, _P, _D, _D, _D,
+                       _P, _P, _P, _P, _P]
+    lib_fn(_ptr(s), W, H, D, _ptr(v1), _ptr(t), W2, H2, D2, _ptr(v2), mm_z_cut, coarsest, lin_iter, nl_iter,
+           _ptr(f3), _ptr(f6), _ptr(m), _ptr(d), tsigma, esigma, dsigma, _ptr(p), _ptr(interp), _ptr(al),
+           _ptr(anl), _ptr(field))
+    return {"params": p, "interpolated": interp, "aligned_linear": al, "aligned_nonlinear": anl,
+            "field": field}
+
+
+def register_two_volumes(subject, vin, template, vtpl, bank, lin_iter, nl_iter, coarsest, mm_z_cut=0,
+                         prec="f32", **kw):
+    """T1-to-template normalisation (restatement)."""
+    dt, s = _dt(prec)
+    return _register_two_volumes(getattr(orc_lib(), "orc_register_two_volumes" + s), dt, subject, vin,
+                                 template, vtpl, bank, lin_iter, nl_iter, coarsest, mm_z_cut, **kw)
+
+
+def ref_register_two_volumes(subject, vin, template, vtpl, bank, lin_iter, nl_iter, coarsest, mm_z_cut=0,
+                             **kw):
+    """T1-to-template normalisation with the reference's kernels."""
+    return _register_two_volumes(ref_lib().ref_register_two_volumes, np.float32, subject, vin, template,
+                                 vtpl, bank, lin_iter, nl_iter, coarsest, mm_z_cut, **kw)
+
+
+def change_resolution_and_size(src, vin, shape, vnew, mm_z_cut=0, prec="f32"):
+    dt, s = _dt(prec)
+    D, H, W = src.shape
+    D2, H2, W2 = shape
+    v = _arr(src, dt)
+    out = np.zeros((D2, H2, W2), dt)
+    fn = getattr(orc_lib(), "orc_change_resolution_and_size" + s)
+    fn.argtypes = [_P, _I, _I, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float, _P, _I, _I, _I,
+                   ctypes.c_float, ctypes.c_float, ctypes.c_float, _I]
+    fn(_ptr(v), W, H, D, *[float(a) for a in vin], _ptr(out), W2, H2, D2, *[float(a) for a in vnew], mm_z_cut)
+    return out
+
+
+def ref_change_resolution_and_size(src, vin, shape, vnew, mm_z_cut=0):
+    D, H, W = src.shape
+    D2, H2, W2 = shape
+    v = _arr(src, np.float32)
+    out = np.zeros((D2, H2, W2), np.float32)
+    fn = ref_lib().ref_change_resolution_and_size
+    fn.argtypes = [_P, _I, _I, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float, _P, _I, _I, _I,
+                   ctypes.c_float, ctypes.c_float, ctypes.c_float, _I]
+    fn(_ptr(v), W, H, D, *[float(a) for a in vin], _ptr(out), W2, H2, D2, *[float(a) for a in vnew], mm_z_cut)
+    return out
+
+
+def normal_equations_smoothcert(q1: np.ndarray, q2: np.ndarray, sigma: float, prec: str = "f32"):
+    """Normal equations with 3x3x3-smoothed certainties (the certainty
+    smoothing switch of the motion-correction workload)."""
+    dt, s = _dt(prec)
+    _, D, H, W = q1.shape
+    a = _interleave(q1, dt)
+    c = _interleave(q2, dt)
+    A = np.zeros(144, dt)
+    h = np.zeros(12, dt)
+    fn = getattr(orc_lib(), "orc_normal_equations_smoothcert" + s)
+    fn.argtypes = [_P, _P, _I, _I, _I, _D, _P, _P]
+    fn(_ptr(a), _ptr(c), W, H, D, float(sigma), _ptr(A), _ptr(h))
+    return A.reshape(12, 12).T.copy(), h

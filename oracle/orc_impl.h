@@ -235,6 +235,55 @@ void FN(orc_normal_equations)(const REAL* q1, const REAL* q2, int W, int H,
   free(grad);
 }
 
+/* Normal equations with the certainties smoothed first by a separable
+ * 3x3x3 Gaussian (sigma in voxels, weights exp(-1/2sigma^2), 1, exp(...)
+ * normalised).  Not in the reference (its linear path uses the raw
+ * certainties); this is the certainty-smoothing switch of the batched
+ * motion-correction workload, specified here.  Interior voxels only, so
+ * every neighbour is inside the volume. */
+void FN(orc_normal_equations_smoothcert)(const REAL* q1, const REAL* q2, int W, int H, int D,
+                                         double sigma, REAL* A144, REAL* h12) {
+  const long V = (long)W * H * D;
+  REAL* pd = (REAL*)calloc(V, sizeof(REAL));
+  REAL* cert = (REAL*)calloc(V, sizeof(REAL));
+  REAL* cs = (REAL*)calloc(V, sizeof(REAL));
+  REAL* grad = (REAL*)calloc(V, sizeof(REAL));
+  const float e = (float)exp(-1.0 / (2.0 * sigma * sigma));
+  const REAL w0 = (REAL)(1.0f / (1.0f + 2.0f * e));
+  const REAL w1 = (REAL)(e * (1.0f / (1.0f + 2.0f * e)));
+  const REAL w[3] = {w1, w0, w1};
+  for (int e2 = 0; e2 < 144; e2++) A144[e2] = RZERO;
+  for (int e2 = 0; e2 < 12; e2++) h12[e2] = RZERO;
+  for (int axis = 0; axis < 3; axis++) {
+    const REAL* a = q1 + (long)axis * 2 * V;
+    const REAL* c = q2 + (long)axis * 2 * V;
+    FN(orc_phase_diff_cert)(a, c, V, pd, cert);
+    FN(orc_phase_grad)(a, c, axis, W, H, D, grad);
+    for (int z = 1; z < D - 1; z++)
+      for (int y = 1; y < H - 1; y++)
+        for (int x = 1; x < W - 1; x++) {
+          REAL s = RZERO;
+          for (int dz = -1; dz <= 1; dz++) {
+            REAL sy = RZERO;
+            for (int dy = -1; dy <= 1; dy++) {
+              const long r = x + (long)(y + dy) * W + (long)(z + dz) * W * H;
+              const REAL sx = w1 * cert[r - 1] + w0 * cert[r] + w1 * cert[r + 1];
+              sy += w[dy + 1] * sx;
+            }
+            s += w[dz + 1] * sy;
+          }
+          cs[x + (long)y * W + (long)z * W * H] = s;
+        }
+    FN(orc_ah_axis)(pd, grad, cs, axis, W, H, D, 7, A144, h12);
+  }
+  for (int j = 0; j < 12; j++)
+    for (int i = 0; i < 12; i++) A144[j + i * 12] = A144[i + j * 12];
+  free(pd);
+  free(cert);
+  free(cs);
+  free(grad);
+}
+
 /* p = A^-1 h in double precision, A column-major n x n, result rounded to
  * `real`.  The reference uses Eigen's full-pivoting Householder QR
  * (SolveEquationSystem, broccoli_lib.cpp:17157-17186); this is Gaussian
@@ -944,6 +993,128 @@ void FN(orc_align_nonlinear_scales)(const REAL* ref, REAL* aligned, int W, int H
   free(tot);
   free(upd);
   free(tmp);
+}
+
+/* Resample a volume to new voxel sizes, then centre it in (or crop it to)
+ * the new grid, with an extra shift of mm_z_cut mm along z.
+ * ChangeVolumesResolutionAndSize, broccoli_lib.cpp:6950-7100, with
+ * RescaleVolumeLinear and CopyVolumeToNew (kernelRegistration.cpp:
+ * 1340-1366, :1593-1678).  Voxels of the new grid not covered stay 0. */
+void FN(orc_change_resolution_and_size)(const REAL* src, int W, int H, int D, float vx, float vy,
+                                        float vz, REAL* out, int W2, int H2, int D2, float nvx,
+                                        float nvy, float nvz, int mm_z_cut) {
+  const int Wi = FN(orc_myround)((float)W * vx / nvx);
+  const int Hi = FN(orc_myround)((float)H * vy / nvy);
+  const int Di = FN(orc_myround)((float)D * vz / nvz);
+  REAL* interp = (REAL*)malloc(sizeof(REAL) * (long)Wi * Hi * Di);
+  FN(orc_rescale_linear)(src, W, H, D, Wi, Hi, Di, interp);
+  for (long i = 0; i < (long)W2 * H2 * D2; i++) out[i] = RZERO;
+  const int xd = Wi - W2, yd = Hi - H2, zd = Di - D2;
+  const int zcut = (int)round((float)mm_z_cut / nvz);
+  const int gx = W2 > Wi ? W2 : Wi, gy = H2 > Hi ? H2 : Hi, gz = D2 > Di ? D2 : Di;
+  for (int z = 0; z < gz; z++)
+    for (int y = 0; y < gy; y++)
+      for (int x = 0; x < gx; x++) {
+        int xn, xi, yn, yi, zn, zi;
+        if (xd > 0) { xn = x; xi = x + (int)round((float)xd / 2.0); }
+        else { xn = x + (int)round((float)abs(xd) / 2.0); xi = x; }
+        if (yd > 0) { yn = y; yi = y + (int)round((float)yd / 2.0); }
+        else { yn = y + (int)round((float)abs(yd) / 2.0); yi = y; }
+        if (zd > 0) { zn = z; zi = z + (int)round((float)zd / 2.0) + zcut; }
+        else { zn = z + (int)round((float)abs(zd) / 2.0); zi = z + zcut; }
+        if (xi >= Wi || yi >= Hi || zi >= Di || xn >= W2 || yn >= H2 || zn >= D2) continue;
+        if (xi < 0 || yi < 0 || zi < 0 || xn < 0 || yn < 0 || zn < 0) continue;
+        out[xn + (long)yn * W2 + (long)zn * W2 * H2] = interp[xi + (long)yi * Wi + (long)zi * Wi * Hi];
+      }
+  free(interp);
+}
+
+/* Centre of mass (voxels), float accumulation in x-fastest order.
+ * CalculateCenterOfMass, broccoli_lib.cpp:6763-6800. */
+void FN(orc_center_of_mass)(const REAL* vol, int W, int H, int D, REAL* c3) {
+  REAL tm = RZERO, rx = RZERO, ry = RZERO, rz = RZERO;
+  for (int z = 0; z < D; z++)
+    for (int y = 0; y < H; y++)
+      for (int x = 0; x < W; x++) {
+        const REAL m = vol[x + (long)y * W + (long)z * W * H];
+        rx += m * (REAL)x;
+        ry += m * (REAL)y;
+        rz += m * (REAL)z;
+        tm += m;
+      }
+  c3[0] = rx / tm;
+  c3[1] = ry / tm;
+  c3[2] = rz / tm;
+}
+
+/* Translate v1 by the rounded difference of the centres of mass so that it
+ * overlaps v2; returns the translation as parameters.
+ * MatchVolumeMasses, broccoli_lib.cpp:6876-6948. */
+void FN(orc_match_volume_masses)(REAL* v1, const REAL* v2, int W, int H, int D, REAL* p12) {
+  REAL c1[3], c2[3];
+  FN(orc_center_of_mass)(v1, W, H, D, c1);
+  FN(orc_center_of_mass)(v2, W, H, D, c2);
+  for (int i = 0; i < 12; i++) p12[i] = RZERO;
+  p12[0] = -(REAL)FN(orc_myround)((float)(c2[0] - c1[0]));
+  p12[1] = -(REAL)FN(orc_myround)((float)(c2[1] - c1[1]));
+  p12[2] = -(REAL)FN(orc_myround)((float)(c2[2] - c1[2]));
+  const long V = (long)W * H * D;
+  REAL* tmp = (REAL*)malloc(sizeof(REAL) * V);
+  for (long i = 0; i < V; i++) tmp[i] = v1[i];
+  FN(orc_warp_affine)(tmp, W, H, D, p12, v1);
+  free(tmp);
+}
+
+/* field += affine displacement t + (A - I)(x - c).
+ * AddLinearAndNonLinearDisplacement, kernelRegistration.cpp:1142-1178. */
+void FN(orc_add_linear_nonlinear)(REAL* field, int W, int H, int D, const REAL* p) {
+  const long V = (long)W * H * D;
+  for (int z = 0; z < D; z++)
+    for (int y = 0; y < H; y++)
+      for (int x = 0; x < W; x++) {
+        const REAL xf = (REAL)x - ((REAL)W - RONE) * RHALF;
+        const REAL yf = (REAL)y - ((REAL)H - RONE) * RHALF;
+        const REAL zf = (REAL)z - ((REAL)D - RONE) * RHALF;
+        const long i = x + (long)y * W + (long)z * W * H;
+        field[i] += p[0] + p[3] * xf + p[4] * yf + p[5] * zf;
+        field[V + i] += p[1] + p[6] * xf + p[7] * yf + p[8] * zf;
+        field[2 * V + i] += p[2] + p[9] * xf + p[10] * yf + p[11] * zf;
+      }
+}
+
+/* T1-to-template normalisation.  PerformRegistrationTwoVolumesWrapper,
+ * broccoli_lib.cpp:7973-8112 (single volume, no pre-centring, no skull
+ * strip): resample the input onto the template grid; match centres of
+ * mass; multi-scale AFFINE registration; parameters composed with the mass
+ * match; multi-scale nonlinear registration; the affine motion added to the
+ * field; the input resampled again and warped once by the combined field.
+ * Outputs (template size): params12, interpolated (after the resample and
+ * mass match), aligned_linear, aligned_nonlinear and field (3 volumes). */
+void FN(orc_register_two_volumes)(const REAL* in, int W, int H, int D, const float* vin,
+                                  const REAL* tpl, int W2, int H2, int D2, const float* vtpl,
+                                  int mm_z_cut, int coarsest, int lin_iter, int nl_iter,
+                                  const REAL* filters3, const REAL* filters6, const REAL* tensors,
+                                  const REAL* dirs, double tsigma, double esigma, double dsigma,
+                                  REAL* p12, REAL* interpolated, REAL* aligned_linear,
+                                  REAL* aligned_nonlinear, REAL* field) {
+  const long V2 = (long)W2 * H2 * D2;
+  REAL* work = (REAL*)malloc(sizeof(REAL) * V2);
+  REAL match[12], rot[3];
+  for (int i = 0; i < 12; i++) p12[i] = RZERO;
+  FN(orc_change_resolution_and_size)(in, W, H, D, vin[0], vin[1], vin[2], work, W2, H2, D2, vtpl[0],
+                                     vtpl[1], vtpl[2], mm_z_cut);
+  FN(orc_match_volume_masses)(work, tpl, W2, H2, D2, match);
+  for (long i = 0; i < V2; i++) interpolated[i] = work[i];
+  FN(orc_align_linear_scales)(tpl, work, W2, H2, D2, coarsest, filters3, lin_iter, ORC_AFFINE, p12, rot);
+  for (long i = 0; i < V2; i++) aligned_linear[i] = work[i];
+  FN(orc_add_affine)(p12, match);
+  FN(orc_align_nonlinear_scales)(tpl, work, W2, H2, D2, coarsest, filters6, tensors, dirs, nl_iter,
+                                 tsigma, esigma, dsigma, field);
+  FN(orc_add_linear_nonlinear)(field, W2, H2, D2, p12);
+  FN(orc_change_resolution_and_size)(in, W, H, D, vin[0], vin[1], vin[2], work, W2, H2, D2, vtpl[0],
+                                     vtpl[1], vtpl[2], mm_z_cut);
+  FN(orc_warp_field)(work, W2, H2, D2, field, field + V2, field + 2 * V2, aligned_nonlinear);
+  free(work);
 }
 
 #undef RSQRT

@@ -385,4 +385,171 @@ void ref_align_nonlinear(const float* ref, float* aligned, const float* original
   }
 }
 
+static int myround_(float a) { return (int)floorf(a + 0.5f); }
+
+// ChangeVolumesResolutionAndSize, broccoli_lib.cpp:6950-7100: the
+// reference's RescaleVolumeLinear then CopyVolumeToNew kernels.
+void ref_change_resolution_and_size(const float* src, int W, int H, int D, float vx, float vy, float vz,
+                                    float* out, int W2, int H2, int D2, float nvx, float nvy, float nvz,
+                                    int mm_z_cut) {
+  const int Wi = myround_((float)W * vx / nvx), Hi = myround_((float)H * vy / nvy),
+            Di = myround_((float)D * vz / nvz);
+  std::vector<float> interp((long)Wi * Hi * Di, 0.f);
+  ref_rescale_linear(src, W, H, D, Wi, Hi, Di, interp.data());
+  std::memset(out, 0, sizeof(float) * (long)W2 * H2 * D2);
+  const int gx = W2 > Wi ? W2 : Wi, gy = H2 > Hi ? H2 : Hi, gz = D2 > Di ? D2 : Di;
+  ndrange(roundup(gx, 16), roundup(gy, 16), gz, 16, 16, 1, [&] {
+    clr::CopyVolumeToNew(out, interp.data(), W2, H2, D2, Wi, Hi, Di, Wi - W2, Hi - H2, Di - D2, mm_z_cut,
+                         nvz, 0);
+  });
+}
+
+// CalculateCenterOfMass, broccoli_lib.cpp:6763-6800 (host loop).
+static void com_(const float* v, int W, int H, int D, float* c) {
+  float tm = 0.f, rx = 0.f, ry = 0.f, rz = 0.f;
+  for (int z = 0; z < D; z++)
+    for (int y = 0; y < H; y++)
+      for (int x = 0; x < W; x++) {
+        const float m = v[x + (long)y * W + (long)z * W * H];
+        rx += m * (float)x;
+        ry += m * (float)y;
+        rz += m * (float)z;
+        tm += m;
+      }
+  c[0] = rx / tm;
+  c[1] = ry / tm;
+  c[2] = rz / tm;
+}
+
+// MatchVolumeMasses, broccoli_lib.cpp:6876-6948, with
+// TransformVolumesLinear (InterpolateVolumeLinearLinear).
+void ref_match_volume_masses(float* v1, const float* v2, int W, int H, int D, float* p12) {
+  float c1[3], c2[3];
+  com_(v1, W, H, D, c1);
+  com_(v2, W, H, D, c2);
+  for (int i = 0; i < 12; i++) p12[i] = 0.f;
+  p12[0] = -(float)myround_(c2[0] - c1[0]);
+  p12[1] = -(float)myround_(c2[1] - c1[1]);
+  p12[2] = -(float)myround_(c2[2] - c1[2]);
+  std::vector<float> tmp(v1, v1 + (long)W * H * D);
+  ref_warp_affine(tmp.data(), W, H, D, p12, v1);
+}
+
+// CreateCombinedDisplacementField, broccoli_lib.cpp:8115-8150, with
+// AddLinearAndNonLinearDisplacement (kernelRegistration.cpp:1142-1178).
+void ref_add_linear_nonlinear(float* field, int W, int H, int D, const float* p12) {
+  const long V = (long)W * H * D;
+  ndrange(roundup(W, 16), roundup(H, 16), D, 16, 16, 1, [&] {
+    clr::AddLinearAndNonLinearDisplacement(field, field + V, field + 2 * V, p12, W, H, D);
+  });
+}
+
+// AlignTwoVolumesLinearSeveralScales, broccoli_lib.cpp:6391-6513, around
+// the reference kernels (ChangeVolumeSize = RescaleVolumeLinear,
+// InterpolateVolumeLinearLinear).  `aligned` in: moving volume, out: the
+// moving volume warped by the total parameters (DO_OVERWRITE).
+void ref_align_linear_scales(const float* ref, float* aligned, int W, int H, int D, int coarsest,
+                             const float* filters, int niter, int type, float* p12, float* rot3) {
+  const long V = (long)W * H * D;
+  std::vector<float> orig(aligned, aligned + V), r_s(V), o_s(V), a_s(V), resc(V);
+  float tmp[12], rt[3] = {0.f, 0.f, 0.f};
+  for (int i = 0; i < 12; i++) p12[i] = 0.f;
+  rot3[0] = rot3[1] = rot3[2] = 0.f;
+  int cw = myround_((float)W / (float)coarsest), ch = myround_((float)H / (float)coarsest),
+      cd = myround_((float)D / (float)coarsest);
+  ref_rescale_linear(orig.data(), W, H, D, cw, ch, cd, o_s.data());
+  ref_rescale_linear(ref, W, H, D, cw, ch, cd, r_s.data());
+  for (int scale = coarsest; scale >= 1; scale /= 2) {
+    const long vs = (long)cw * ch * cd;
+    std::memcpy(a_s.data(), o_s.data(), sizeof(float) * vs);
+    const int it = scale == 1 ? (int)ceilf((float)niter / 5.0f) : niter;
+    ref_align_linear(r_s.data(), a_s.data(), o_s.data(), cw, ch, cd, filters, it, type, tmp, rt);
+    if (type != 1) rt[0] = rt[1] = rt[2] = 0.f;
+    if (scale != 1) {
+      rot3[0] += rt[0]; rot3[1] += rt[1]; rot3[2] += rt[2];
+      ref_add_affine_next_scale(p12, tmp);
+      cw = myround_((float)W / ((float)scale / 2.0f));
+      ch = myround_((float)H / ((float)scale / 2.0f));
+      cd = myround_((float)D / ((float)scale / 2.0f));
+      ref_rescale_linear(orig.data(), W, H, D, cw, ch, cd, resc.data());
+      ref_rescale_linear(ref, W, H, D, cw, ch, cd, r_s.data());
+      ref_warp_affine(resc.data(), cw, ch, cd, p12, o_s.data());
+    } else {
+      ref_add_affine(p12, tmp);
+      rot3[0] += rt[0]; rot3[1] += rt[1]; rot3[2] += rt[2];
+      ref_warp_affine(orig.data(), W, H, D, p12, aligned);
+    }
+  }
+}
+
+// AlignTwoVolumesNonLinearSeveralScales, broccoli_lib.cpp:6516-6665.
+void ref_align_nonlinear_scales(const float* ref, float* aligned, int W, int H, int D, int coarsest,
+                                const float* filters6, const float* tensors, const float* dirs,
+                                int niter, double tsigma, double esigma, double dsigma, float* field) {
+  const long V = (long)W * H * D;
+  std::vector<float> orig(aligned, aligned + V), r_s(V), o_s(V), a_s(V), resc(V);
+  std::vector<float> tot(3 * V, 0.f), upd(3 * V), tmp(3 * V);
+  int cw = myround_((float)W / (float)coarsest), ch = myround_((float)H / (float)coarsest),
+      cd = myround_((float)D / (float)coarsest);
+  ref_rescale_linear(orig.data(), W, H, D, cw, ch, cd, o_s.data());
+  ref_rescale_linear(ref, W, H, D, cw, ch, cd, r_s.data());
+  for (int scale = coarsest; scale >= 1; scale /= 2) {
+    const long vs = (long)cw * ch * cd;
+    std::memcpy(a_s.data(), o_s.data(), sizeof(float) * vs);
+    const int it = scale == 1 ? (int)ceilf((float)niter / 2.0f) : niter;
+    ref_align_nonlinear(r_s.data(), a_s.data(), o_s.data(), cw, ch, cd, filters6, tensors, dirs, it,
+                        tsigma, esigma, dsigma, upd.data());
+    for (int c = 0; c < 3; c++) {
+      float* t = tot.data() + c * vs;
+      const float* u = upd.data() + c * vs;
+      ndrange(roundup(cw, 16), roundup(ch, 16), cd, 16, 16, 1, [&] { clm::AddVolumesOverwrite(t, u, cw, ch, cd); });
+    }
+    if (scale != 1) {
+      const int pw = cw, ph = ch, pdp = cd;
+      cw = myround_((float)W / ((float)scale / 2.0f));
+      ch = myround_((float)H / ((float)scale / 2.0f));
+      cd = myround_((float)D / ((float)scale / 2.0f));
+      const long nv = (long)cw * ch * cd;
+      for (int c = 0; c < 3; c++) {
+        ref_rescale_linear(tot.data() + c * (long)pw * ph * pdp, pw, ph, pdp, cw, ch, cd, tmp.data() + c * nv);
+        float* t = tmp.data() + c * nv;
+        ndrange(roundup(cw, 16), roundup(ch, 16), cd, 16, 16, 1, [&] { clm::MultiplyVolume(t, 2.0f, cw, ch, cd); });
+      }
+      std::memcpy(tot.data(), tmp.data(), sizeof(float) * 3 * nv);
+      ref_rescale_linear(orig.data(), W, H, D, cw, ch, cd, resc.data());
+      ref_rescale_linear(ref, W, H, D, cw, ch, cd, r_s.data());
+      ref_warp_field(resc.data(), cw, ch, cd, tot.data(), tot.data() + nv, tot.data() + 2 * nv, o_s.data());
+    } else {
+      std::memcpy(field, tot.data(), sizeof(float) * 3 * V);
+      ref_warp_field(orig.data(), W, H, D, field, field + V, field + 2 * V, aligned);
+    }
+  }
+}
+
+// PerformRegistrationTwoVolumesWrapper, broccoli_lib.cpp:7973-8112 (one
+// volume, no pre-centring, no skull strip).
+void ref_register_two_volumes(const float* in, int W, int H, int D, const float* vin, const float* tpl,
+                              int W2, int H2, int D2, const float* vtpl, int mm_z_cut, int coarsest,
+                              int lin_iter, int nl_iter, const float* filters3, const float* filters6,
+                              const float* tensors, const float* dirs, double tsigma, double esigma,
+                              double dsigma, float* p12, float* interpolated, float* aligned_linear,
+                              float* aligned_nonlinear, float* field) {
+  const long V2 = (long)W2 * H2 * D2;
+  std::vector<float> work(V2);
+  float match[12], rot[3];
+  ref_change_resolution_and_size(in, W, H, D, vin[0], vin[1], vin[2], work.data(), W2, H2, D2, vtpl[0],
+                                 vtpl[1], vtpl[2], mm_z_cut);
+  ref_match_volume_masses(work.data(), tpl, W2, H2, D2, match);
+  std::memcpy(interpolated, work.data(), sizeof(float) * V2);
+  ref_align_linear_scales(tpl, work.data(), W2, H2, D2, coarsest, filters3, lin_iter, 2, p12, rot);
+  std::memcpy(aligned_linear, work.data(), sizeof(float) * V2);
+  ref_add_affine(p12, match);
+  ref_align_nonlinear_scales(tpl, work.data(), W2, H2, D2, coarsest, filters6, tensors, dirs, nl_iter,
+                             tsigma, esigma, dsigma, field);
+  ref_add_linear_nonlinear(field, W2, H2, D2, p12);
+  ref_change_resolution_and_size(in, W, H, D, vin[0], vin[1], vin[2], work.data(), W2, H2, D2, vtpl[0],
+                                 vtpl[1], vtpl[2], mm_z_cut);
+  ref_warp_field(work.data(), W2, H2, D2, field, field + V2, field + 2 * V2, aligned_nonlinear);
+}
+
 }  // extern "C"

@@ -86,6 +86,38 @@ def main() -> None:
         if rr is not None:
             g[f"align_{name}_rot"] = rr
 
+    # nonlinear: six filters, projection tensors and directions
+    nshape = (18, 22, 20)
+    nbase, nmoved, _ = S.affine_pair(nshape, base_seed=4, motion_seed=5)
+    g["nl_base"], g["nl_moved"] = nbase, nmoved
+    f6 = bank["nonlinear"]
+    g["nl_q1"] = np.concatenate([O.ref_filter3d(nbase, f6[:3]), O.ref_filter3d(nbase, f6[3:])]).astype(np.complex64)
+    g["nl_q2"] = np.concatenate([O.ref_filter3d(nmoved, f6[:3]), O.ref_filter3d(nmoved, f6[3:])]).astype(np.complex64)
+    fld1, _ = O.ref_align_nonlinear(nbase, nmoved, bank, 1)
+    g["nl_field1"] = fld1
+    fld3, al3 = O.ref_align_nonlinear(nbase, nmoved, bank, 3)
+    g["nl_field3"], g["nl_aligned3"] = fld3, al3
+    fs, als = O.ref_align_nonlinear_scales(nbase, nmoved, bank, 3, 2)
+    g["nl_scales_field"], g["nl_scales_aligned"] = fs, als
+
+    # pyramid linear registration
+    sshape = (26, 30, 28)
+    sbase, smoved, _ = S.affine_pair(sshape, base_seed=6, motion_seed=7)
+    g["sc_base"], g["sc_moved"] = sbase, smoved
+    for typ, name in ((1, "rigid"), (2, "affine")):
+        pp, al, rr = O.ref_align_linear_scales(sbase, smoved, flt, 8, 2, typ)
+        g[f"sc_{name}_p"], g[f"sc_{name}_vol"], g[f"sc_{name}_rot"] = pp, al, rr
+
+    # T1-to-template normalisation on a small synthetic head pair, with
+    # anisotropic input voxels and a z cut
+    sub, tpl, _ = S.t1_template_pair((30, 36, 34), (32, 38, 32), seed=0)
+    g["r2v_subject"], g["r2v_template"] = sub, tpl
+    g["r2v_voxel"] = np.array([1.1, 0.9, 1.2], np.float32)
+    g["r2v_crs"] = O.ref_change_resolution_and_size(sub, g["r2v_voxel"], tpl.shape, (1.0, 1.0, 1.0), 3)
+    r2v = O.ref_register_two_volumes(sub, g["r2v_voxel"], tpl, (1.0, 1.0, 1.0), bank, 6, 4, 2, mm_z_cut=3)
+    for k, v in r2v.items():
+        g["r2v_" + k] = v
+
     series, _ = S.motion_series(T=4, shape=(14, 18, 16), snr=50.0)
     g["mc_series"] = series
     g["mc_voxel"] = np.array([3.0, 3.0, 3.5], np.float32)

@@ -143,3 +143,19 @@ def test_kernel_launch_counter(ctx, lin_filters):
     ctx.register_linear(v, v[None], lin_filters, 4, L.AFFINE)
     torch.cuda.synchronize()
     assert ctx.kernel_launches - before == 1 + 4 * 4
+
+
+def test_certainty_smoothing_one_iteration_matches_oracle(ctx, orc, golden, lin_filters):
+    """The certainty-smoothing switch (3x3x3 Gaussian of the certainties
+    before the sums): one AFFINE iteration equals the oracle's solve of the
+    smoothed-certainty normal equations."""
+    q1 = orc.filter3d(golden["base"], lin_filters)
+    q2 = orc.filter3d(golden["moved"], lin_filters)
+    A, h = orc.normal_equations_smoothcert(q1, q2, 1.0, prec="f64")
+    p = orc.solve(A, h, prec="f64")
+    r = ctx.register_linear(cuda(golden["base"]), cuda(golden["moved"])[None], lin_filters, 1, L.AFFINE,
+                            certainty_sigma=1.0)
+    assert param_err(r["params"].cpu().numpy()[0], p) < TOL
+    # and it differs from the unsmoothed solve
+    r0 = ctx.register_linear(cuda(golden["base"]), cuda(golden["moved"])[None], lin_filters, 1, L.AFFINE)
+    assert param_err(r0["params"].cpu().numpy()[0], p) > 10 * TOL

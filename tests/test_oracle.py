@@ -111,3 +111,41 @@ def test_reference_build_agrees_on_fresh_case(orc, lin_filters):
     po, vo, _ = orc.align_linear(a, b, lin_filters, 3, 1)
     assert np.array_equal(pr, po)
     assert np.array_equal(vr, vo)
+
+
+def test_nonlinear_exact(orc, golden, bank):
+    f1, _ = orc.align_nonlinear(golden["nl_base"], golden["nl_moved"], bank, 1)
+    assert np.array_equal(f1, golden["nl_field1"])
+    f3, a3 = orc.align_nonlinear(golden["nl_base"], golden["nl_moved"], bank, 3)
+    assert np.array_equal(f3, golden["nl_field3"])
+    assert np.array_equal(a3, golden["nl_aligned3"])
+
+
+def test_nonlinear_scales_exact(orc, golden, bank):
+    f, a = orc.align_nonlinear_scales(golden["nl_base"], golden["nl_moved"], bank, 3, 2)
+    assert np.array_equal(f, golden["nl_scales_field"])
+    assert np.array_equal(a, golden["nl_scales_aligned"])
+
+
+@pytest.mark.parametrize("typ,name", [(1, "rigid"), (2, "affine")])
+def test_linear_scales_exact(orc, golden, lin_filters, typ, name):
+    p, v, r = orc.align_linear_scales(golden["sc_base"], golden["sc_moved"], lin_filters, 8, 2, typ)
+    assert np.array_equal(p, golden[f"sc_{name}_p"])
+    assert np.array_equal(v, golden[f"sc_{name}_vol"])
+    assert np.array_equal(r, golden[f"sc_{name}_rot"])
+
+
+def test_nonlinear_fp64_close(orc, golden, bank):
+    f32, _ = orc.align_nonlinear(golden["nl_base"], golden["nl_moved"], bank, 3)
+    f64, _ = orc.align_nonlinear(golden["nl_base"], golden["nl_moved"], bank, 3, prec="f64")
+    assert rel_err(f32, f64) < 1e-3
+
+
+def test_register_two_volumes_exact(orc, golden, bank):
+    r = orc.register_two_volumes(golden["r2v_subject"], golden["r2v_voxel"], golden["r2v_template"],
+                                 (1.0, 1.0, 1.0), bank, 6, 4, 2, mm_z_cut=3)
+    for k in ("params", "interpolated", "aligned_linear", "aligned_nonlinear", "field"):
+        assert np.array_equal(r[k], golden["r2v_" + k]), k
+    crs = orc.change_resolution_and_size(golden["r2v_subject"], golden["r2v_voxel"],
+                                         golden["r2v_template"].shape, (1.0, 1.0, 1.0), 3)
+    assert np.array_equal(crs, golden["r2v_crs"])
