@@ -60,6 +60,7 @@ const char* brc_status_string(int s) {
     case BRC_ERR_NODEVICE: return "no usable CUDA device";
     case BRC_ERR_UNSUPPORTED: return "unsupported option";
     case BRC_ERR_NONFINITE: return "non-finite solution";
+    case BRC_ERR_SCRATCH_LIMIT: return "request exceeds the fixed scratch of the no-allocation entry point";
     default: return "unknown status";
   }
 }

@@ -44,7 +44,9 @@ typedef enum {
   BRC_ERR_TIMEOUT = -4,     /* a bounded device-side wait gave up         */
   BRC_ERR_NODEVICE = -5,    /* no usable sm_100 device                    */
   BRC_ERR_UNSUPPORTED = -6, /* option combination not implemented         */
-  BRC_ERR_NONFINITE = -7    /* a solve produced NaN/Inf (update dropped)  */
+  BRC_ERR_NONFINITE = -7,   /* a solve produced NaN/Inf (update dropped)  */
+  BRC_ERR_SCRATCH_LIMIT = -8 /* request larger than the fixed scratch of
+                               brc_normal_equations_noalloc              */
 } brc_status;
 
 /* Alignment types, same values as broccoli_constants.h:93-95. */
@@ -110,6 +112,27 @@ int brc_filter3d(brc_ctx* ctx, const float* d_vol, int W, int H, int D, int batc
 int brc_normal_equations(brc_ctx* ctx, const float* d_q1, long long q1_stride,
                          const float* d_q2, int W, int H, int D, int batch,
                          double* d_A, double* d_h);
+
+/* brc_normal_equations without any device allocation.  No counterpart in
+ * the reference: it is for callers that cannot let a library allocate
+ * device memory -- processes whose HBM is reserved up front by a pooling
+ * allocator or serving runtime, and hosts that plan all memory before they
+ * start.  It takes a cudaStream_t instead of a context (NULL is the legacy
+ * default stream) and keeps its per-CTA partial sums in a fixed device
+ * array of BRC_NOALLOC_PARTIAL_ROWS rows x 42 doubles (about 1 MB) that
+ * every GPU loading the library holds until the process exits.
+ * A call needs ceil((D-6)/zpb) x batch rows, zpb = max(1, 4096 /
+ * ((W-6)(H-6))) interior slices per row (64x64x33: 27 rows per volume,
+ * batch <= 113); larger requests return BRC_ERR_SCRATCH_LIMIT and do
+ * nothing.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU race and must be ordered by the caller.  No cudaMalloc,
+ * cudaFree or allocating library routine is called. */
+#define BRC_NOALLOC_PARTIAL_ROWS 3072
+int brc_normal_equations_noalloc(void* cuda_stream, const float* d_q1, long long q1_stride,
+                                 const float* d_q2, int W, int H, int D, int batch,
+                                 double* d_A, double* d_h);
 
 /* p = A^-1 h per instance in double, rounded to float.
  * Replaces SolveEquationSystem (broccoli_lib.cpp:17157-17186). */
