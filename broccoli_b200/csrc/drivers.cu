@@ -423,3 +423,57 @@ extern "C" int brc_register_linear_scales(brc_ctx* ctx, const float* d_ref, cons
   ctx->launches += 1;
   return BRC_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Adjoints (differentiable registration)
+// ---------------------------------------------------------------------------
+
+extern "C" int brc_filter3d_adjoint(brc_ctx* ctx, const float* d_grad, int W, int H, int D, int batch,
+                                    const float* h_filters, int nfilt, float* d_out) {
+  if (!ctx) return BRC_ERR_INVALID;
+  if (!d_grad || !d_out || !h_filters || W <= 0 || H <= 0 || D <= 0 || batch <= 0 || batch > 65535 ||
+      (nfilt != 3 && nfilt != 6))
+    return ctx->fail(BRC_ERR_INVALID, "brc_filter3d_adjoint: bad argument");
+  cudaSetDevice(ctx->device);
+  BRC_TRY(ctx, brc::filter3d_adjoint(d_grad, W, H, D, batch, h_filters, nfilt, d_out, ctx->stream()),
+          "filter3d_adjoint");
+  ctx->launches += 1;
+  return BRC_OK;
+}
+
+extern "C" int brc_warp_affine_backward(brc_ctx* ctx, const float* d_src, int W, int H, int D, int batch,
+                                        const float* d_params, const float* d_grad_out, double* d_grad_params,
+                                        float* d_grad_src) {
+  if (!ctx) return BRC_ERR_INVALID;
+  if (!d_src || !d_params || !d_grad_out || !d_grad_params || W <= 0 || H <= 0 || D <= 0 || batch <= 0 ||
+      batch > 65535)
+    return ctx->fail(BRC_ERR_INVALID, "brc_warp_affine_backward: bad argument");
+  cudaSetDevice(ctx->device);
+  const long long V = (long long)W * H * D;
+  const int nblk = brc::warp_affine_backward_blocks(V);
+  BRC_TRY(ctx, ctx->partials.ensure(sizeof(double) * 12 * nblk * (size_t)batch), "alloc");
+  if (d_grad_src)
+    BRC_TRY(ctx, cudaMemsetAsync(d_grad_src, 0, sizeof(float) * V * batch, ctx->stream()), "memset");
+  BRC_TRY(ctx, brc::warp_affine_backward(d_src, W, H, D, batch, d_params, d_grad_out, ctx->partials.as<double>(),
+                                         nblk, d_grad_params, d_grad_src, ctx->stream()),
+          "warp_affine_backward");
+  ctx->launches += 2;
+  return BRC_OK;
+}
+
+extern "C" int brc_warp_field_backward(brc_ctx* ctx, const float* d_src, int W, int H, int D, const float* d_dx,
+                                       const float* d_dy, const float* d_dz, const float* d_grad_out,
+                                       float* d_grad_field, float* d_grad_src) {
+  if (!ctx) return BRC_ERR_INVALID;
+  if (!d_src || !d_dx || !d_dy || !d_dz || !d_grad_out || (!d_grad_field && !d_grad_src) || W <= 0 || H <= 0 ||
+      D <= 0)
+    return ctx->fail(BRC_ERR_INVALID, "brc_warp_field_backward: bad argument");
+  cudaSetDevice(ctx->device);
+  if (d_grad_src)
+    BRC_TRY(ctx, cudaMemsetAsync(d_grad_src, 0, sizeof(float) * W * (size_t)H * D, ctx->stream()), "memset");
+  BRC_TRY(ctx, brc::warp_field_backward(d_src, W, H, D, d_dx, d_dy, d_dz, d_grad_out, d_grad_field, d_grad_src,
+                                        ctx->stream()),
+          "warp_field_backward");
+  ctx->launches += 1;
+  return BRC_OK;
+}

@@ -54,3 +54,16 @@ cudaError_t resize_to_grid(const float* src, int W, int H, int D, float vx, floa
 cudaError_t mass_moments(const float* vol, int W, int H, int D, double* sums, cudaStream_t st);
 cudaError_t add_affine_to_field(float* field, int W, int H, int D, const float* p12, cudaStream_t st);
 }  // namespace brc
+
+namespace brc {
+// adjoint.cu
+cudaError_t filter3d_adjoint(const float* grad, int W, int H, int D, int batch, const float* h_filters, int nfilt,
+                             float* out, cudaStream_t st);
+int warp_affine_backward_blocks(long long V);
+cudaError_t warp_affine_backward(const float* src, int W, int H, int D, int batch, const float* params,
+                                 const float* gout, double* partials, int nblk, double* gparams, float* gsrc,
+                                 cudaStream_t st);
+cudaError_t warp_field_backward(const float* src, int W, int H, int D, const float* dx, const float* dy,
+                                const float* dz, const float* gout, float* gfield, float* gsrc,
+                                cudaStream_t st);
+}  // namespace brc

@@ -269,6 +269,33 @@ int brc_register_nonlinear(brc_ctx* ctx, const float* d_ref, const float* d_movi
                            const float* h_dirs, const brc_nonlinear_opts* opts, float* d_field,
                            float* d_aligned);
 
+/* ---- adjoints (differentiable registration) ---------------------------- */
+
+/* Adjoint of brc_filter3d: d_out (batch volumes) = sum over the nfilt
+ * filters of the correlation of the complex gradient d_grad (batch x nfilt
+ * interleaved complex volumes, dL/dRe and dL/dIm) with the filters.  No
+ * counterpart in the reference (its path is not differentiated); the
+ * forward it inverts is NonseparableConvolution3D (broccoli_lib.cpp:
+ * 4974-5027). */
+int brc_filter3d_adjoint(brc_ctx* ctx, const float* d_grad, int W, int H, int D, int batch,
+                         const float* h_filters, int nfilt, float* d_out);
+
+/* Adjoint of brc_warp_affine: dL/dparams (batch x 12, double) from the
+ * output gradient, with the exact derivative of the clamp-to-edge
+ * trilinear interpolant; d_grad_src (may be NULL) receives dL/dsrc by
+ * atomic scatter (zeroed first).  Forward: InterpolateVolumeLinearLinear
+ * (kernelRegistration.cpp:1066-1101). */
+int brc_warp_affine_backward(brc_ctx* ctx, const float* d_src, int W, int H, int D, int batch,
+                             const float* d_params, const float* d_grad_out, double* d_grad_params,
+                             float* d_grad_src);
+
+/* Adjoint of brc_warp_field: dL/dfield (3 volumes, may be NULL) and
+ * dL/dsrc (may be NULL, zeroed then scattered).  Forward:
+ * InterpolateVolumeLinearNonLinear (kernelRegistration.cpp:1111-1140). */
+int brc_warp_field_backward(brc_ctx* ctx, const float* d_src, int W, int H, int D, const float* d_dx,
+                            const float* d_dy, const float* d_dz, const float* d_grad_out,
+                            float* d_grad_field, float* d_grad_src);
+
 /* ---- device memory and host copies (for hosts without a CUDA runtime) --- */
 
 /* cudaMalloc / cudaFree on the context's device.  Replaces the clCreateBuffer

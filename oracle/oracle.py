@@ -531,3 +531,22 @@ def normal_equations_smoothcert(q1: np.ndarray, q2: np.ndarray, sigma: float, pr
     fn.argtypes = [_P, _P, _I, _I, _I, _D, _P, _P]
     fn(_ptr(a), _ptr(c), W, H, D, float(sigma), _ptr(A), _ptr(h))
     return A.reshape(12, 12).T.copy(), h
+
+
+def registration_objective(moving, ref, filters, sigma, params=None, field=None, prec="f64"):
+    """Filter-response SSD of the smoothed moving volume warped by `params`
+    (12,) or `field` (3,D,H,W) against the smoothed reference, evaluated with
+    the oracle's kernels in double (the finite-difference reference of the
+    differentiable registration)."""
+    taps = np.exp(-(np.arange(9) - 4.0) ** 2 / (2.0 * sigma * sigma))
+    taps = taps / taps.sum()
+    sm = smooth3d(moving, taps, taps, taps, prec=prec)
+    sr = smooth3d(ref, taps, taps, taps, prec=prec)
+    if params is not None:
+        w = warp_affine(sm, params, prec=prec)
+    else:
+        w = warp_field(sm, field[0], field[1], field[2], prec=prec)
+    qm = filter3d(w, filters, prec=prec)
+    qr = filter3d(sr, filters, prec=prec)
+    d = qm - qr
+    return float((d.real ** 2 + d.imag ** 2).sum())

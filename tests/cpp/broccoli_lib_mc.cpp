@@ -33,7 +33,7 @@ static void write_floats(const char* path, const float* p, size_t n) {
 }
 
 int main(int argc, char** argv) {
-  if (argc != 14) {
+  if (argc != 13) {
     fprintf(stderr, "usage: %s series W H D T vx vy vz filters iters out_series out_motion\n", argv[0]);
     return 2;
   }

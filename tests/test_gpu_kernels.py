@@ -8,6 +8,7 @@ import pytest
 import torch
 
 from conftest import rel_err
+from broccoli_b200 import _lib as L
 from broccoli_b200 import filters as F
 
 pytestmark = pytest.mark.gpu
@@ -26,13 +27,27 @@ def test_filter_matches_golden(ctx, golden, lin_filters):
 
 @pytest.mark.parametrize("shape", [(5, 17, 33), (11, 9, 7), (9, 40, 65), (33, 64, 64), (4, 3, 2)])
 @pytest.mark.parametrize("nf", [3, 6])
-def test_filter_odd_shapes_vs_oracle(ctx, orc, bank, shape, nf):
+@pytest.mark.parametrize("prec", [L.PREC_FP32, L.PREC_FP32_GENERAL])
+def test_filter_odd_shapes_vs_oracle(ctx, orc, bank, shape, nf, prec):
+    """FP32 (even/odd half-tap kernel for these quadrature banks) and
+    FP32_GENERAL (all 343 taps) against the oracle."""
     rng = np.random.default_rng(sum(shape) + nf)
     vol = (rng.standard_normal(shape) * 50 + 100).astype(np.float32)
     flt = bank["linear"] if nf == 3 else bank["nonlinear"]
     ref = orc.filter3d(vol, flt)
-    got = ctx.filter3d(cuda(vol), flt).cpu().numpy()[0]
+    got = ctx.filter3d(cuda(vol), flt, precision=prec).cpu().numpy()[0]
     assert got.shape == ref.shape
+    assert rel_err(got, ref) < TOL
+
+
+@pytest.mark.parametrize("nf", [3, 6])
+def test_filter_non_symmetric_bank(ctx, orc, nf):
+    """A bank without even/odd symmetry takes the general kernel."""
+    rng = np.random.default_rng(40 + nf)
+    flt = rng.standard_normal((nf, 2, 7, 7, 7)).astype(np.float32)
+    vol = rng.standard_normal((12, 20, 36)).astype(np.float32)
+    ref = orc.filter3d(vol, flt)
+    got = ctx.filter3d(cuda(vol), flt).cpu().numpy()[0]
     assert rel_err(got, ref) < TOL
 
 
