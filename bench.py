@@ -289,6 +289,21 @@ def run_gpu(args, rank, world, local_rank):
             e2e_times.append(dt * 1000.0)
     e2e_ms = float(np.sum(e2e_times))
 
+    # ---- the plain FP32 GPU path: the same registrations one volume at a
+    # time (batch 1, eager launches, no graph), on a sample of the series ----
+    n_serial = min(24, T - 1)
+    for i in range(2):
+        ctx.register_linear(ref, moving[i:i + 1], flt, ITERS, L.RIGID, tolerance=TOL, use_graph=False)
+    torch.cuda.synchronize()
+    se0 = torch.cuda.Event(enable_timing=True)
+    se1 = torch.cuda.Event(enable_timing=True)
+    se0.record(st)
+    for i in range(n_serial):
+        ctx.register_linear(ref, moving[i:i + 1], flt, ITERS, L.RIGID, tolerance=TOL, use_graph=False)
+    se1.record(st)
+    se1.synchronize()
+    serial_rate = n_serial / (se0.elapsed_time(se1) / 1000.0)
+
     # ---- dominant kernel alone: 7^3 filtering of the 199 moving volumes ----
     q = torch.empty((T - 1, 3, D, H, W, 2), dtype=torch.float32, device=dev)
     for _ in range(3):
@@ -352,6 +367,10 @@ def run_gpu(args, rank, world, local_rank):
                                     "(MEASURED_PEAKS.json has no FP32 figure)",
                      "flop_per_launch": f_flop, "launch_ms": f_ms, "traffic": traffic},
         "accuracy": acc,
+        "plain_fp32_serial": {"value": serial_rate, "unit": UNIT,
+                              "sample": f"{n_serial} volumes of the series registered one at a time "
+                                        "(batch 1, eager launches)",
+                              "batched_over_serial": value / serial_rate},
         "clocks": clocks,
         "cpu_baseline": cpu,
     }

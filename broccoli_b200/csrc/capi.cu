@@ -7,6 +7,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <map>
 #include <memory>
 #include <string>
@@ -97,6 +98,18 @@ int brc_ctx_destroy(brc_ctx* ctx) {
   ctx->graphs.clear();
   if (ctx->ev_in) cudaEventDestroy(ctx->ev_in);
   if (ctx->ev_out) cudaEventDestroy(ctx->ev_out);
+  for (int c = 0; c < brc_ctx::kMaxChunks; c++) {
+    if (ctx->ev_chunk_in[c]) cudaEventDestroy(ctx->ev_chunk_in[c]);
+    if (ctx->ev_chunk_done[c]) cudaEventDestroy(ctx->ev_chunk_done[c]);
+  }
+  if (ctx->copy_in) {
+    cudaStreamSynchronize(ctx->copy_in);
+    cudaStreamDestroy(ctx->copy_in);
+  }
+  if (ctx->copy_out) {
+    cudaStreamSynchronize(ctx->copy_out);
+    cudaStreamDestroy(ctx->copy_out);
+  }
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
   return BRC_OK;
@@ -482,26 +495,61 @@ extern "C" int brc_motion_correct(brc_ctx* ctx, float* h_volumes, int W, int H, 
   BRC_TRY(ctx, ctx->params.ensure(sizeof(float) * 12 * batch), "alloc params");
   BRC_TRY(ctx, ctx->rot.ensure(sizeof(float) * 3 * batch), "alloc rot");
   float* d_series = ctx->series.as<float>();
-  BRC_TRY(ctx, cudaMemcpyAsync(d_series, h_volumes, sizeof(float) * V * T, cudaMemcpyHostToDevice, st), "H2D");
+  BRC_TRY(ctx, ctx->ensure_copy_streams(), "copy streams");
+  // The series is registered in up to kMaxChunks chunks of >= 32 volumes so
+  // that the upload of chunk c+1 and the download of chunk c-1 run on the
+  // copy engines while chunk c registers.  Chunk 0's upload includes the
+  // reference (volume 0, or h_reference).
+  const int nchunk = std::max(1, std::min(brc_ctx::kMaxChunks, batch / 32));
+  const int per = (batch + nchunk - 1) / nchunk;
+  // the copy streams start after work the caller queued before this call
+  BRC_TRY(ctx, cudaEventRecord(ctx->ev_in, st), "event");
+  BRC_TRY(ctx, cudaStreamWaitEvent(ctx->copy_in, ctx->ev_in, 0), "wait");
+  BRC_TRY(ctx, cudaStreamWaitEvent(ctx->copy_out, ctx->ev_in, 0), "wait");
   const float* d_ref = d_series;
   if (h_reference) {
-    BRC_TRY(ctx, cudaMemcpyAsync(d_series + V * T, h_reference, sizeof(float) * V, cudaMemcpyHostToDevice, st), "H2D");
+    BRC_TRY(ctx, cudaMemcpyAsync(d_series + V * T, h_reference, sizeof(float) * V, cudaMemcpyHostToDevice,
+                                 ctx->copy_in), "H2D");
     d_ref = d_series + V * T;
+  }
+  for (int c = 0; c < nchunk; c++) {
+    const long long lo = c == 0 ? 0 : first + (long long)c * per;
+    const long long hi = std::min<long long>(T, first + (long long)(c + 1) * per);
+    if (hi > lo)
+      BRC_TRY(ctx, cudaMemcpyAsync(d_series + V * lo, h_volumes + V * lo, sizeof(float) * V * (hi - lo),
+                                   cudaMemcpyHostToDevice, ctx->copy_in), "H2D");
+    BRC_TRY(ctx, cudaEventRecord(ctx->ev_chunk_in[c], ctx->copy_in), "event");
   }
   brc_linear_opts o = *opts;
   o.type = BRC_RIGID;
-  int s = brc_register_linear_batched(ctx, d_ref, 0, d_series + V * first, W, H, D, batch, h_filters, &o,
-                                      ctx->params.as<float>(), ctx->corrected.as<float>(),
-                                      ctx->rot.as<float>(), nullptr);
-  if (s != BRC_OK) return s;
-  BRC_TRY(ctx, cudaMemcpyAsync(h_volumes + V * first, ctx->corrected.as<float>(), sizeof(float) * V * batch,
-                               cudaMemcpyDeviceToHost, st), "D2H");
+  for (int c = 0; c < nchunk; c++) {
+    const int i0 = c * per;
+    const int nb = std::min(batch, i0 + per) - i0;
+    BRC_TRY(ctx, cudaStreamWaitEvent(st, ctx->ev_chunk_in[c], 0), "wait");
+    if (nb > 0) {
+      int s = brc_register_linear_batched(ctx, d_ref, 0, d_series + V * (first + i0), W, H, D, nb, h_filters, &o,
+                                          ctx->params.as<float>() + 12 * (long long)i0,
+                                          ctx->corrected.as<float>() + V * i0,
+                                          ctx->rot.as<float>() + 3 * (long long)i0, nullptr);
+      if (s != BRC_OK) {
+        cudaStreamSynchronize(ctx->copy_in);
+        cudaStreamSynchronize(ctx->copy_out);
+        return s;
+      }
+    }
+    BRC_TRY(ctx, cudaEventRecord(ctx->ev_chunk_done[c], st), "event");
+    BRC_TRY(ctx, cudaStreamWaitEvent(ctx->copy_out, ctx->ev_chunk_done[c], 0), "wait");
+    if (nb > 0)
+      BRC_TRY(ctx, cudaMemcpyAsync(h_volumes + V * (first + i0), ctx->corrected.as<float>() + V * i0,
+                                   sizeof(float) * V * nb, cudaMemcpyDeviceToHost, ctx->copy_out), "D2H");
+  }
   std::vector<float> prm(12 * (size_t)batch), rot(3 * (size_t)batch);
   BRC_TRY(ctx, cudaMemcpyAsync(prm.data(), ctx->params.as<float>(), sizeof(float) * 12 * batch,
                                cudaMemcpyDeviceToHost, st), "D2H");
   BRC_TRY(ctx, cudaMemcpyAsync(rot.data(), ctx->rot.as<float>(), sizeof(float) * 3 * batch,
                                cudaMemcpyDeviceToHost, st), "D2H");
   BRC_TRY(ctx, cudaStreamSynchronize(st), "synchronize");
+  BRC_TRY(ctx, cudaStreamSynchronize(ctx->copy_out), "synchronize");
   if (h_motion) {
     for (int i = 0; i < batch; i++) {
       const int t = first + i;

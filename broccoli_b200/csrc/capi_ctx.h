@@ -53,12 +53,32 @@ struct brc_ctx {
   cudaStream_t user_stream = nullptr;
   bool use_user_stream = false;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  // host<->device copy streams of brc_motion_correct and their per-chunk
+  // events (created on first use)
+  static constexpr int kMaxChunks = 4;
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  cudaEvent_t ev_chunk_in[kMaxChunks] = {}, ev_chunk_done[kMaxChunks] = {};
   std::string last_error;
   unsigned long long launches = 0;
   DevBuf q1, q2, aligned, partials, ctl, tmp1, tmp2, series, corrected, params, rot, nl, pyr, cert;
   std::map<GraphKey, std::unique_ptr<GraphEntry>> graphs;
 
   cudaStream_t stream() const { return use_user_stream ? user_stream : own_stream; }
+
+  cudaError_t ensure_copy_streams() {
+    cudaError_t e = cudaSuccess;
+    if (!copy_in && (e = cudaStreamCreateWithFlags(&copy_in, cudaStreamNonBlocking)) != cudaSuccess) return e;
+    if (!copy_out && (e = cudaStreamCreateWithFlags(&copy_out, cudaStreamNonBlocking)) != cudaSuccess) return e;
+    for (int c = 0; c < kMaxChunks; c++) {
+      if (!ev_chunk_in[c] &&
+          (e = cudaEventCreateWithFlags(&ev_chunk_in[c], cudaEventDisableTiming)) != cudaSuccess)
+        return e;
+      if (!ev_chunk_done[c] &&
+          (e = cudaEventCreateWithFlags(&ev_chunk_done[c], cudaEventDisableTiming)) != cudaSuccess)
+        return e;
+    }
+    return e;
+  }
 
   int fail(int status, const std::string& msg) {
     last_error = msg;

@@ -22,6 +22,8 @@ namespace brc {
 // ---------------------------------------------------------------------------
 
 constexpr int kNEThreads = 256;
+// Largest volume the 32-bit voxel indexing of the resampling kernels takes.
+constexpr long long kMaxVoxels = 0x7fffff00LL;
 
 // Phase difference and certainty of one response pair, in the reference's
 // operation order (CalculatePhaseDifferencesAndCertainties,
@@ -54,13 +56,6 @@ __device__ __forceinline__ float phase_grad(float2 a_p, float2 a_c, float2 a_m, 
   return atan2f(ti, tr);
 }
 
-// Sums over the interior (3 voxels from every face) of
-//   c g^2 [1, x, y, z, xx, xy, xz, yy, yz, zz]  and  c g dphi [1, x, y, z]
-// for each axis k (sum index 14k + e), coordinates relative to the volume
-// centre: the 30 + 12 values that CalculateAMatrixAndHVector2DValuesX/Y/Z,
-// CalculateAMatrix1DValues / HVector1DValues and CalculateAMatrix /
-// HVector accumulate (kernelRegistration.cpp:387-800).  One CTA handles
-// `zpb` interior slices of one instance and writes 42 FP64 partial sums.
 // Certainty volumes |q1 q2| cos^2(dphi/2) of the three filter pairs of every
 // active instance, [b][k][voxel]; input of the optional certainty smoothing.
 __global__ void __launch_bounds__(256)
@@ -101,7 +96,45 @@ __device__ __forceinline__ float smoothed_certainty(const float* __restrict__ c,
   return s;
 }
 
-__global__ void __launch_bounds__(kNEThreads)
+// Sum e (0..13) of one axis as (row moment) x y^py x z^pz: moments
+// [sum w, sum w x, sum w x^2, sum v, sum v x] of the row, y and z relative
+// to the volume centre.
+__constant__ signed char c_sum_moment[14] = {0, 1, 0, 0, 2, 1, 1, 0, 0, 0, 3, 4, 3, 3};
+__constant__ signed char c_sum_ypow[14] = {0, 0, 1, 0, 0, 1, 0, 2, 1, 0, 0, 0, 1, 0};
+__constant__ signed char c_sum_zpow[14] = {0, 0, 0, 1, 0, 0, 1, 0, 1, 2, 0, 0, 0, 1};
+
+__device__ __forceinline__ double pick_moment(const float (&m)[3][5], int sel) {
+  float r = 0.f;
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+#pragma unroll
+    for (int q = 0; q < 5; q++) r = (sel == 5 * k + q) ? m[k][q] : r;
+  return (double)r;
+}
+__device__ __forceinline__ double ypow(double y, int e) {
+  const int p = c_sum_ypow[e];
+  return p == 0 ? 1.0 : (p == 1 ? y : y * y);
+}
+__device__ __forceinline__ double zpow(double z, int e) {
+  const int p = c_sum_zpow[e];
+  return p == 0 ? 1.0 : (p == 1 ? z : z * z);
+}
+
+// Sums over the interior (3 voxels from every face) of
+//   c g^2 [1, x, y, z, xx, xy, xz, yy, yz, zz]  and  c g dphi [1, x, y, z]
+// for each axis k (sum index 14k + e), coordinates relative to the volume
+// centre: the 30 + 12 values that CalculateAMatrixAndHVector2DValuesX/Y/Z,
+// CalculateAMatrix1DValues / HVector1DValues and CalculateAMatrix /
+// HVector accumulate (kernelRegistration.cpp:387-800).  One CTA handles
+// `zpb` interior slices of one instance and writes 42 FP64 partial sums.
+//
+// One warp walks one (y, z) row at a time, lanes along x (coalesced float2
+// loads).  Within a row y and z are constant, so the 42 sums factor into 15
+// row moments per lane, sum_x w [1, x, x^2] and sum_x v [1, x] for the three
+// axes, reduced over the warp in FP32 and expanded into the 42 sums in FP64
+// (lane j owns sums j and 32 + j).  The same order on every run: results
+// are deterministic.
+__global__ void __launch_bounds__(kNEThreads, 4)
 normal_eq_partial_kernel(const float2* __restrict__ q1, long long q1_stride,
                          const float2* __restrict__ q2, int W, int H, int D, int zpb,
                          double* __restrict__ partials, const int* __restrict__ conv_iter, int it,
@@ -109,68 +142,78 @@ normal_eq_partial_kernel(const float2* __restrict__ q1, long long q1_stride,
   const int b = blockIdx.y;
   if (instance_done(conv_iter, b, it)) return;
   const long long V = (long long)W * H * D;
+  const long long WH = (long long)W * H;
   const float2* Q1 = q1 + (long long)b * q1_stride;
   const float2* Q2 = q2 + (long long)b * 3 * V;
-  double acc[kNSums];
-#pragma unroll
-  for (int j = 0; j < kNSums; j++) acc[j] = 0.0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
   const int nx = W - 6, ny = H - 6;
   const int z0 = 3 + blockIdx.x * zpb;
   const int z1 = min(D - 3, z0 + zpb);
-  const long long n = (nx > 0 && ny > 0 && z1 > z0) ? (long long)nx * ny * (z1 - z0) : 0;
-  const double cx = 0.5 * (W - 1), cy = 0.5 * (H - 1), cz = 0.5 * (D - 1);
-  const long long stride[3] = {1, W, (long long)W * H};
+  const int nrows = (nx > 0 && ny > 0 && z1 > z0) ? ny * (z1 - z0) : 0;
+  const float cxf = 0.5f * (float)(W - 1);
+  const double cy = 0.5 * (H - 1), cz = 0.5 * (D - 1);
 
-  for (long long e = threadIdx.x; e < n; e += kNEThreads) {
-    const int x = 3 + (int)(e % nx);
-    const int y = 3 + (int)((e / nx) % ny);
-    const int z = z0 + (int)(e / ((long long)nx * ny));
-    const long long i = x + (long long)y * W + (long long)z * W * H;
-    const double xf = x - cx, yf = y - cy, zf = z - cz;
+  // lane j accumulates sums j and 32 + j (the latter for j < 10)
+  double acc_lo = 0.0, acc_hi = 0.0;
+  const int jlo = lane, jhi = 32 + lane;
+  const int elo = jlo % 14, ehi = jhi % 14;
+  const int slo = 5 * (jlo / 14) + c_sum_moment[elo];
+  const int shi = jhi < kNSums ? 5 * (jhi / 14) + c_sum_moment[ehi] : 0;
+
+  for (int r = warp; r < nrows; r += kNEThreads / 32) {
+    const int y = 3 + r % ny;
+    const int z = z0 + r / ny;
+    const long long row = (long long)y * W + (long long)z * WH;
+    // [k][0..4] = sum w, sum w x, sum w x^2, sum v, sum v x
+    float m[3][5];
 #pragma unroll
-    for (int k = 0; k < 3; k++) {
-      const float2* A = Q1 + k * V;
-      const float2* C = Q2 + k * V;
-      const long long s = stride[k];
-      const float2 a = __ldg(A + i), c = __ldg(C + i);
-      float pd, cert;
-      phase_diff_cert(a, c, pd, cert);
-      if (cert_in != nullptr)
-        cert = smoothed_certainty(cert_in + ((long long)b * 3 + k) * V, i, W, (long long)W * H, cw0, cw1);
-      const float g = phase_grad(__ldg(A + i + s), a, __ldg(A + i - s), __ldg(C + i + s), c,
-                                 __ldg(C + i - s));
-      const float cg = cert * g;
-      const double w = (double)(cg * g);
-      const double v = (double)(cg * pd);
-      double* ak = acc + 14 * k;
-      ak[0] += w;
-      ak[1] += w * xf;
-      ak[2] += w * yf;
-      ak[3] += w * zf;
-      ak[4] += w * xf * xf;
-      ak[5] += w * xf * yf;
-      ak[6] += w * xf * zf;
-      ak[7] += w * yf * yf;
-      ak[8] += w * yf * zf;
-      ak[9] += w * zf * zf;
-      ak[10] += v;
-      ak[11] += v * xf;
-      ak[12] += v * yf;
-      ak[13] += v * zf;
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+      for (int q = 0; q < 5; q++) m[k][q] = 0.f;
+    for (int x = 3 + lane; x < W - 3; x += 32) {
+      const long long i = row + x;
+      const float xf = (float)x - cxf;
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        const float2* A = Q1 + k * V;
+        const float2* C = Q2 + k * V;
+        const long long s = k == 0 ? 1 : (k == 1 ? (long long)W : WH);
+        const float2 a = __ldg(A + i), c = __ldg(C + i);
+        float pd, cert;
+        phase_diff_cert(a, c, pd, cert);
+        if (cert_in != nullptr)
+          cert = smoothed_certainty(cert_in + ((long long)b * 3 + k) * V, i, W, WH, cw0, cw1);
+        const float g = phase_grad(__ldg(A + i + s), a, __ldg(A + i - s), __ldg(C + i + s), c,
+                                   __ldg(C + i - s));
+        const float cg = cert * g;
+        const float w = cg * g;
+        const float v = cg * pd;
+        m[k][0] += w;
+        m[k][1] += w * xf;
+        m[k][2] += w * xf * xf;
+        m[k][3] += v;
+        m[k][4] += v * xf;
+      }
     }
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+      for (int q = 0; q < 5; q++) {
+        float t = m[k][q];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        m[k][q] = t;
+      }
+    const double yf = (double)y - cy, zf = (double)z - cz;
+    acc_lo += pick_moment(m, slo) * ypow(yf, elo) * zpow(zf, elo);
+    if (jhi < kNSums) acc_hi += pick_moment(m, shi) * ypow(yf, ehi) * zpow(zf, ehi);
   }
 
-  // Deterministic block reduction: warp shuffles, then warps in order.
+  // Deterministic block reduction: warps in order.
   __shared__ double s_part[kNEThreads / 32][kNSums];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int j = 0; j < kNSums; j++) {
-    double v = acc[j];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (lane == 0) s_part[warp][j] = v;
-  }
+  s_part[warp][jlo] = acc_lo;
+  if (jhi < kNSums) s_part[warp][jhi] = acc_hi;
   __syncthreads();
   if (threadIdx.x < kNSums) {
     double v = 0.0;
@@ -540,6 +583,7 @@ __global__ void solve_given_kernel(const double* __restrict__ A, const double* _
 // kernelRegistration.cpp:1064).  u, v, w include the +0.5 texel offset.
 __device__ __forceinline__ float sample_linear(const float* __restrict__ T, int W, int H, int D,
                                               float u, float v, float w) {
+  // volumes hold fewer than 2^31 voxels (checked by the launchers)
   const float uu = u - 0.5f, vv = v - 0.5f, ww = w - 0.5f;
   const float fu = floorf(uu), fv = floorf(vv), fw = floorf(ww);
   const float a = uu - fu, bb = vv - fv, c = ww - fw;
@@ -547,10 +591,11 @@ __device__ __forceinline__ float sample_linear(const float* __restrict__ T, int 
   const int xi0 = min(max(i0, 0), W - 1), xi1 = min(max(i0 + 1, 0), W - 1);
   const int yj0 = min(max(j0, 0), H - 1), yj1 = min(max(j0 + 1, 0), H - 1);
   const int zk0 = min(max(k0, 0), D - 1), zk1 = min(max(k0 + 1, 0), D - 1);
-  const long long r00 = (long long)yj0 * W + (long long)zk0 * W * H;
-  const long long r10 = (long long)yj1 * W + (long long)zk0 * W * H;
-  const long long r01 = (long long)yj0 * W + (long long)zk1 * W * H;
-  const long long r11 = (long long)yj1 * W + (long long)zk1 * W * H;
+  const int WH = W * H;
+  const int r00 = yj0 * W + zk0 * WH;
+  const int r10 = yj1 * W + zk0 * WH;
+  const int r01 = yj0 * W + zk1 * WH;
+  const int r11 = yj1 * W + zk1 * WH;
   return (1.f - a) * (1.f - bb) * (1.f - c) * __ldg(T + xi0 + r00) +
          a * (1.f - bb) * (1.f - c) * __ldg(T + xi1 + r00) +
          (1.f - a) * bb * (1.f - c) * __ldg(T + xi0 + r10) +
@@ -568,10 +613,11 @@ warp_affine_kernel(const float* __restrict__ src, long long src_stride, int W, i
                    const int* __restrict__ conv_iter, int it) {
   const int b = blockIdx.y;
   if (instance_done(conv_iter, b, it)) return;
-  const long long V = (long long)W * H * D;
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int V = W * H * D;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= V) return;
-  const int x = (int)(i % W), y = (int)((i / W) % H), z = (int)(i / ((long long)W * H));
+  const int r = i / W;
+  const int x = i - r * W, y = r % H, z = r / H;
   const float* p = params + (long long)b * 12;
   const float xf = (float)x - ((float)W - 1.0f) * 0.5f;
   const float yf = (float)y - ((float)H - 1.0f) * 0.5f;
@@ -587,10 +633,11 @@ warp_affine_kernel(const float* __restrict__ src, long long src_stride, int W, i
 __global__ void __launch_bounds__(256)
 warp_field_kernel(const float* __restrict__ src, int W, int H, int D, const float* __restrict__ dx,
                   const float* __restrict__ dy, const float* __restrict__ dz, float* __restrict__ out) {
-  const long long V = (long long)W * H * D;
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int V = W * H * D;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= V) return;
-  const int x = (int)(i % W), y = (int)((i / W) % H), z = (int)(i / ((long long)W * H));
+  const int r = i / W;
+  const int x = i - r * W, y = r % H, z = r / H;
   out[i] = sample_linear(src, W, H, D, (float)x + dx[i] + 0.5f, (float)y + dy[i] + 0.5f,
                          (float)z + dz[i] + 0.5f);
 }
@@ -600,10 +647,11 @@ warp_field_kernel(const float* __restrict__ src, int W, int H, int D, const floa
 __global__ void __launch_bounds__(256)
 rescale_linear_kernel(const float* __restrict__ src, int W, int H, int D, float* __restrict__ out,
                       int W2, int H2, int D2, float vx, float vy, float vz) {
-  const long long V2 = (long long)W2 * H2 * D2;
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int V2 = W2 * H2 * D2;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= V2) return;
-  const int x = (int)(i % W2), y = (int)((i / W2) % H2), z = (int)(i / ((long long)W2 * H2));
+  const int r = i / W2;
+  const int x = i - r * W2, y = r % H2, z = r / H2;
   out[i] = sample_linear(src, W, H, D, x * vx + 0.5f, y * vy + 0.5f, z * vz + 0.5f);
 }
 
@@ -700,6 +748,7 @@ cudaError_t warp_affine(const float* src, long long src_stride, int W, int H, in
                         const float* params, float* out, long long out_stride, const int* conv_iter,
                         int it, cudaStream_t st) {
   const long long V = (long long)W * H * D;
+  if (V > kMaxVoxels) return cudaErrorInvalidValue;
   dim3 grid((unsigned)((V + 255) / 256), batch);
   warp_affine_kernel<<<grid, 256, 0, st>>>(src, src_stride, W, H, D, params, out, out_stride,
                                            conv_iter, it);
@@ -709,6 +758,7 @@ cudaError_t warp_affine(const float* src, long long src_stride, int W, int H, in
 cudaError_t warp_field(const float* src, int W, int H, int D, const float* dx, const float* dy,
                        const float* dz, float* out, cudaStream_t st) {
   const long long V = (long long)W * H * D;
+  if (V > kMaxVoxels) return cudaErrorInvalidValue;
   warp_field_kernel<<<(unsigned)((V + 255) / 256), 256, 0, st>>>(src, W, H, D, dx, dy, dz, out);
   return cudaGetLastError();
 }
@@ -716,6 +766,7 @@ cudaError_t warp_field(const float* src, int W, int H, int D, const float* dx, c
 cudaError_t rescale_linear(const float* src, int W, int H, int D, float* out, int W2, int H2, int D2,
                            cudaStream_t st) {
   const long long V2 = (long long)W2 * H2 * D2;
+  if (V2 > kMaxVoxels || (long long)W * H * D > kMaxVoxels) return cudaErrorInvalidValue;
   const float vx = (float)(W - 1) / (float)(W2 - 1);
   const float vy = (float)(H - 1) / (float)(H2 - 1);
   const float vz = (float)(D - 1) / (float)(D2 - 1);
