@@ -211,6 +211,7 @@ def run_gpu(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     ctx = Context(local_rank)
     flt = filters()
+    prec = L.PREC_BF16X3 if args.precision == "bf16x3" else L.PREC_FP32
     vols, truth = make_series(rank)
     D, H, W = SHAPE
     V = D * H * W
@@ -219,8 +220,9 @@ def run_gpu(args, rank, world, local_rank):
     moving = d_series[1:]
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
 
-    def step():
-        return ctx.register_linear(ref, moving, flt, ITERS, L.RIGID, tolerance=TOL)
+    def step(precision=None):
+        return ctx.register_linear(ref, moving, flt, ITERS, L.RIGID, tolerance=TOL,
+                                   precision=prec if precision is None else precision)
 
     def barrier():
         if world > 1:
@@ -269,6 +271,7 @@ def run_gpu(args, rank, world, local_rank):
     L.lib().brc_linear_opts_default(ctypes.byref(opts), ITERS)
     opts.type = L.RIGID
     opts.tolerance = TOL
+    opts.precision = prec
     vs = np.asarray(VOXEL, np.float32)
     fl = np.ascontiguousarray(flt, np.float32)
     work = torch.empty_like(host).pin_memory()
@@ -304,22 +307,46 @@ def run_gpu(args, rank, world, local_rank):
     se1.synchronize()
     serial_rate = n_serial / (se0.elapsed_time(se1) / 1000.0)
 
-    # ---- dominant kernel alone: 7^3 filtering of the 199 moving volumes ----
+    # ---- the same batched step with FP32 filtering (when timing BF16X3) ----
+    fp32_batched = None
+    if prec != L.PREC_FP32:
+        for _ in range(2):
+            step(L.PREC_FP32)
+        torch.cuda.synchronize()
+        b_times = []
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            step(L.PREC_FP32)
+            e1.record(st)
+            e1.synchronize()
+            b_times.append(e0.elapsed_time(e1))
+        fp32_batched = (T - 1) * args.steps / (float(np.sum(b_times)) / 1000.0)
+
+    # ---- dominant kernel alone: 7^3 filtering of the 199 moving volumes
+    # (inputs 107 MB + responses 640 MB per launch, larger than L2) ----
     q = torch.empty((T - 1, 3, D, H, W, 2), dtype=torch.float32, device=dev)
-    for _ in range(3):
-        L.lib().brc_filter3d(ctx.handle, ctypes.c_void_p(moving.data_ptr()), W, H, D, T - 1, V,
-                             fl.ctypes.data_as(ctypes.c_void_p), 3, 0, ctypes.c_void_p(q.data_ptr()))
-    torch.cuda.synchronize()
-    nrep = 20
-    fe0 = torch.cuda.Event(enable_timing=True)
-    fe1 = torch.cuda.Event(enable_timing=True)
-    fe0.record(st)
-    for _ in range(nrep):
-        L.lib().brc_filter3d(ctx.handle, ctypes.c_void_p(moving.data_ptr()), W, H, D, T - 1, V,
-                             fl.ctypes.data_as(ctypes.c_void_p), 3, 0, ctypes.c_void_p(q.data_ptr()))
-    fe1.record(st)
-    fe1.synchronize()
-    f_ms = fe0.elapsed_time(fe1) / nrep
+
+    def time_filter(precision, nrep=20):
+        for _ in range(3):
+            L.lib().brc_filter3d(ctx.handle, ctypes.c_void_p(moving.data_ptr()), W, H, D, T - 1, V,
+                                 fl.ctypes.data_as(ctypes.c_void_p), 3, precision, ctypes.c_void_p(q.data_ptr()))
+        torch.cuda.synchronize()
+        fe0 = torch.cuda.Event(enable_timing=True)
+        fe1 = torch.cuda.Event(enable_timing=True)
+        fe0.record(st)
+        for _ in range(nrep):
+            L.lib().brc_filter3d(ctx.handle, ctypes.c_void_p(moving.data_ptr()), W, H, D, T - 1, V,
+                                 fl.ctypes.data_as(ctypes.c_void_p), 3, precision, ctypes.c_void_p(q.data_ptr()))
+        fe1.record(st)
+        fe1.synchronize()
+        return fe0.elapsed_time(fe1) / nrep
+
+    f_ms = time_filter(prec)
+    f32_ms = time_filter(L.PREC_FP32) if prec != L.PREC_FP32 else f_ms
+    ctx.synchronize()
     f_flop = FLOP_PER_VOXEL_FILTER * 3 * V * (T - 1)
 
     # ---- reduce over ranks ----
@@ -342,6 +369,30 @@ def run_gpu(args, rank, world, local_rank):
     if os.path.exists(tpath):
         traffic = json.load(open(tpath)).get("dram_bytes_per_launch")
     achieved = f_flop / (f_ms / 1000.0) / 1e12
+    if prec == L.PREC_BF16X3:
+        peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
+        tc_peak = peaks.get("bf16_tflops", 1590.0)
+        # the split form issues 3 BF16 products per tap: 3x the convolution FLOPs
+        tc_achieved = 3 * f_flop / (f_ms / 1000.0) / 1e12
+        roofline = {"kernel": "filter3d_tc_kernel (tcgen05.mma kind::f16, split BF16 x3, FP32 accumulate in TMEM)",
+                    "bound": "tensor", "achieved": tc_achieved, "peak": tc_peak, "unit": "TFLOP/s",
+                    "frac": tc_achieved / tc_peak,
+                    "peak_source": ("MEASURED_PEAKS.json bf16_tflops (burst, measured)" if "bf16_tflops" in peaks
+                                    else "fallback 1.59 PFLOP/s"),
+                    "flop_per_launch": 3 * f_flop,
+                    "flop_note": "3 split products x the 343-tap convolution of 3 complex filters; "
+                                 "the banded-Toeplitz zeros the GEMMs also issue are not counted",
+                    "launch_ms": f_ms, "fp32_equiv_tflops": achieved,
+                    "fp32_filter_launch_ms": f32_ms, "traffic": None}
+    else:
+        roofline = {"kernel": ("filter3d_sym_kernel<3,8,3> (even/odd half-tap form; FLOP counted "
+                               "as the full 343-tap convolution)") if symmetric_bank(fl) else
+                    "filter3d_fp32_kernel<3,8,3>", "bound": "fp32",
+                    "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                    "frac": achieved / fp32_peak,
+                    "peak_source": "nominal FP32 FMA rate 148 SMs x 128 lanes x 2 at the sampled max SM clock "
+                                   "(MEASURED_PEAKS.json has no FP32 figure)",
+                    "flop_per_launch": f_flop, "launch_ms": f_ms, "traffic": traffic}
     acc = accuracy(vols, truth, out["params"].cpu().numpy(), flt) if not args.skip_accuracy else None
     cpu = None
     if not args.skip_cpu:
@@ -352,25 +403,21 @@ def run_gpu(args, rank, world, local_rank):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3" if prec == L.PREC_BF16X3 else "f32",
+        "data": "synthetic",
         "config": workload_config(world, {"mean_iterations": float(iters_used.mean()),
-                                          "precision": "fp32"}),
+                                          "precision": args.precision}),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(4 * V * T),
                 "d2h_bytes_per_step": int(4 * V * (T - 1) + 4 * 15 * (T - 1))},
         "gpu_launches": int(launches),
-        "roofline": {"kernel": ("filter3d_sym_kernel<3,8,3> (even/odd half-tap form; FLOP counted "
-                                "as the full 343-tap convolution)") if symmetric_bank(fl) else
-                     "filter3d_fp32_kernel<3,8,3>", "bound": "fp32",
-                     "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                     "frac": achieved / fp32_peak,
-                     "peak_source": "nominal FP32 FMA rate 148 SMs x 128 lanes x 2 at the sampled max SM clock "
-                                    "(MEASURED_PEAKS.json has no FP32 figure)",
-                     "flop_per_launch": f_flop, "launch_ms": f_ms, "traffic": traffic},
+        "roofline": roofline,
         "accuracy": acc,
         "plain_fp32_serial": {"value": serial_rate, "unit": UNIT,
                               "sample": f"{n_serial} volumes of the series registered one at a time "
                                         "(batch 1, eager launches)",
                               "batched_over_serial": value / serial_rate},
+        "fp32_batched": ({"value": fp32_batched, "unit": UNIT,
+                          "sample": "the same batched step with FP32 filtering"} if fp32_batched else None),
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
@@ -386,6 +433,8 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-accuracy", action="store_true")
     ap.add_argument("--series", type=int, default=T, help="series length (volumes)")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16x3"],
+                    help="filtering precision of the timed path")
     args = ap.parse_args()
     globals()["T"] = args.series
     world = int(os.environ.get("WORLD_SIZE", "1"))

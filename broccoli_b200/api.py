@@ -81,6 +81,12 @@ class Context:
     def workspace_bytes(self) -> int:
         return int(L.lib().brc_ctx_workspace_bytes(self.handle))
 
+    def synchronize(self) -> None:
+        """Waits for the context's work; raises if a bounded device-side
+        wait of a tensor-core kernel gave up since the last check."""
+        self._bind_stream()
+        _check(self, L.lib().brc_ctx_synchronize(self.handle))
+
     # ---- kernels ---------------------------------------------------------
 
     def filter3d(self, vol: torch.Tensor, filters, precision: int = L.PREC_FP32) -> torch.Tensor:

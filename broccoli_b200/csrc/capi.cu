@@ -47,6 +47,58 @@ static bool bad_dims(int W, int H, int D) {
   return W <= 0 || H <= 0 || D <= 0 || (long long)W * H * D > (1ll << 31);
 }
 
+int brc_ctx::taps_for(const float* h_filters, int nfilt, const uint16_t** d_taps) {
+  const uint64_t key = fnv1a(h_filters, sizeof(float) * brc::kFilterFloats * (size_t)nfilt, 1469598103934665603ull ^ (uint64_t)nfilt);
+  auto it = tc_taps.find(key);
+  if (it == tc_taps.end()) {
+    if (tc_taps.size() >= 16) {
+      graphs.clear();  // graphs may hold the pointers released here
+      tc_taps.clear();
+    }
+    std::vector<uint16_t> packed(brc::tc::packed_tap_bytes(nfilt) / 2);
+    brc::tc::pack_taps(h_filters, nfilt, packed.data());
+    std::unique_ptr<DevBuf> buf(new DevBuf());
+    BRC_TRY(this, buf->ensure(packed.size() * 2), "alloc taps");
+    BRC_TRY(this, cudaMemcpy(buf->ptr, packed.data(), packed.size() * 2, cudaMemcpyHostToDevice), "upload taps");
+    it = tc_taps.emplace(key, std::move(buf)).first;
+  }
+  *d_taps = it->second->as<uint16_t>();
+  return BRC_OK;
+}
+
+int brc_ctx::check_tc_err() {
+  int flag = 0;
+  BRC_TRY(this, cudaMemcpy(&flag, tc_err.ptr, sizeof(int), cudaMemcpyDeviceToHost), "read wait flag");
+  if (flag == 0) return BRC_OK;
+  BRC_TRY(this, cudaMemset(tc_err.ptr, 0, sizeof(int)), "clear wait flag");
+  return fail(BRC_ERR_TIMEOUT, "a bounded wait of the tensor-core filtering kernel gave up");
+}
+
+int make_filter_path(brc_ctx* ctx, const float* h_filters, int nfilt, int precision, int H, int D,
+                     FilterPath* fp) {
+  if (nfilt != 3 && nfilt != 6) return ctx->fail(BRC_ERR_INVALID, "filtering needs 3 or 6 filters");
+  fp->precision = precision;
+  fp->h_filters = h_filters;
+  fp->nfilt = nfilt;
+  fp->d_taps = nullptr;
+  fp->d_err = ctx->tc_err.as<int>();
+  if (precision == BRC_PREC_FP32 || precision == BRC_PREC_FP32_GENERAL) return BRC_OK;
+  if (precision != BRC_PREC_BF16X3) return ctx->fail(BRC_ERR_UNSUPPORTED, "unknown precision");
+  const int ty = brc::tc::pick_ty(nfilt, H, D);
+  if (ty <= 0) return ctx->fail(BRC_ERR_UNSUPPORTED, "volume shape not supported by the BF16X3 filtering");
+  fp->g = brc::tc::make_geometry(nfilt, H, D, ty);
+  return ctx->taps_for(h_filters, nfilt, &fp->d_taps);
+}
+
+cudaError_t run_filter(const FilterPath& fp, const float* vol, int W, int H, int D, int batch, long long stride,
+                       float* out, const int* conv_iter, int it, cudaStream_t st) {
+  if (fp.precision == BRC_PREC_BF16X3)
+    return brc::tc::launch(vol, W, H, D, batch, stride, fp.d_taps, fp.nfilt, out, conv_iter, it, fp.d_err, fp.g,
+                           st);
+  return brc::filter3d_fp32(vol, W, H, D, batch, stride, fp.h_filters, fp.nfilt, out, conv_iter, it, st,
+                            fp.precision == BRC_PREC_FP32);
+}
+
 extern "C" {
 
 const char* brc_version(void) { return "broccoli_b200 0.1 (sm_100a)"; }
@@ -85,7 +137,9 @@ int brc_ctx_create(int device, brc_ctx** out) {
   if (cudaEventCreateWithFlags(&ctx->ev_in, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&ctx->ev_out, cudaEventDisableTiming) != cudaSuccess)
     return BRC_ERR_CUDA;
-  if (brc::filter3d_init() != cudaSuccess) return BRC_ERR_CUDA;
+  if (brc::filter3d_init() != cudaSuccess || brc::tc::init() != cudaSuccess) return BRC_ERR_CUDA;
+  if (ctx->tc_err.ensure(16) != cudaSuccess || cudaMemset(ctx->tc_err.ptr, 0, 16) != cudaSuccess)
+    return BRC_ERR_NOMEM;
   *out = ctx.release();
   return BRC_OK;
 }
@@ -131,7 +185,8 @@ void* brc_ctx_stream(brc_ctx* ctx) { return ctx ? (void*)ctx->stream() : nullptr
 
 int brc_ctx_synchronize(brc_ctx* ctx) {
   BRC_CHECK_CTX(ctx);
-  return ctx->cuda(cudaStreamSynchronize(ctx->stream()), "synchronize");
+  BRC_TRY(ctx, cudaStreamSynchronize(ctx->stream()), "synchronize");
+  return ctx->check_tc_err();
 }
 
 size_t brc_ctx_workspace_bytes(const brc_ctx* ctx) { return ctx ? ctx->workspace() : 0; }
@@ -147,12 +202,11 @@ int brc_filter3d(brc_ctx* ctx, const float* d_vol, int W, int H, int D, int batc
   if (nfilt != 3 && nfilt != 6) return ctx->fail(BRC_ERR_INVALID, "brc_filter3d: nfilt must be 3 or 6");
   if (batch > 1 && vol_stride < (long long)W * H * D)
     return ctx->fail(BRC_ERR_INVALID, "brc_filter3d: vol_stride smaller than a volume");
-  if (precision != BRC_PREC_FP32 && precision != BRC_PREC_FP32_GENERAL)
-    return ctx->fail(BRC_ERR_UNSUPPORTED, "brc_filter3d: precision not available");
   cudaSetDevice(ctx->device);
-  BRC_TRY(ctx, brc::filter3d_fp32(d_vol, W, H, D, batch, vol_stride, h_filters, nfilt, d_out, nullptr,
-                                  0, ctx->stream(), precision == BRC_PREC_FP32),
-          "filter3d");
+  FilterPath fp;
+  const int ps = make_filter_path(ctx, h_filters, nfilt, precision, H, D, &fp);
+  if (ps != BRC_OK) return ps;
+  BRC_TRY(ctx, run_filter(fp, d_vol, W, H, D, batch, vol_stride, d_out, nullptr, 0, ctx->stream()), "filter3d");
   ctx->launches += 1;
   return BRC_OK;
 }
@@ -308,6 +362,7 @@ struct RegPlan {
   int* status;
   int nblk, zpb;
   float* cert;  // [batch][3][V] certainty volumes when smoothing them, else null
+  FilterPath fpath;
 };
 
 // Queues the whole registration on stream st; returns the number of
@@ -326,8 +381,8 @@ long long enqueue_registration(brc_ctx* ctx, const RegPlan& p, cudaStream_t st) 
   if ((e = cudaMemsetAsync(p.status, 0, sizeof(int), st)) != cudaSuccess) return ctx->cuda(e, "memset");
   if (p.rotations && (e = cudaMemsetAsync(p.rotations, 0, sizeof(float) * 3 * p.batch, st)) != cudaSuccess)
     return ctx->cuda(e, "memset rot");
-  if ((e = brc::filter3d_fp32(p.ref, p.W, p.H, p.D, ref_batch, p.ref_stride ? p.ref_stride : V,
-                              p.filters, 3, p.q1, nullptr, 0, st)) != cudaSuccess)
+  if ((e = run_filter(p.fpath, p.ref, p.W, p.H, p.D, ref_batch, p.ref_stride ? p.ref_stride : V, p.q1, nullptr,
+                      0, st)) != cudaSuccess)
     return ctx->cuda(e, "filter3d(ref)");
   kernels++;
   if (p.opts.iterations == 0 &&
@@ -336,8 +391,7 @@ long long enqueue_registration(brc_ctx* ctx, const RegPlan& p, cudaStream_t st) 
     return ctx->cuda(e, "copy");
   for (int it = 0; it < p.opts.iterations; it++) {
     const float* cur = it == 0 ? p.moving : p.aligned;
-    if ((e = brc::filter3d_fp32(cur, p.W, p.H, p.D, p.batch, V, p.filters, 3, p.q2, p.conv_iter, it,
-                                st)) != cudaSuccess)
+    if ((e = run_filter(p.fpath, cur, p.W, p.H, p.D, p.batch, V, p.q2, p.conv_iter, it, st)) != cudaSuccess)
       return ctx->cuda(e, "filter3d");
     if ((e = brc::normal_eq_partials(p.q1, p.ref_stride ? 6 * V : 0, p.q2, p.W, p.H, p.D, p.batch,
                                      p.partials, p.nblk, p.zpb, p.conv_iter, it, st, p.cert,
@@ -374,8 +428,9 @@ extern "C" int brc_register_linear_batched(brc_ctx* ctx, const float* d_ref, lon
   if (opts->iterations < 0 || opts->iterations > 10000 || opts->type < 0 || opts->type > 2 ||
       !(opts->tolerance >= 0.f))
     return ctx->fail(BRC_ERR_INVALID, "brc_register_linear_batched: bad options");
-  if (opts->precision != BRC_PREC_FP32)
-    return ctx->fail(BRC_ERR_UNSUPPORTED, "brc_register_linear_batched: precision not available");
+  if (opts->precision != BRC_PREC_FP32 && opts->precision != BRC_PREC_FP32_GENERAL &&
+      opts->precision != BRC_PREC_BF16X3)
+    return ctx->fail(BRC_ERR_UNSUPPORTED, "brc_register_linear_batched: unknown precision");
   if (opts->certainty_sigma_x100 < 0)
     return ctx->fail(BRC_ERR_INVALID, "brc_register_linear_batched: negative certainty sigma");
   const long long V = (long long)W * H * D;
@@ -414,6 +469,10 @@ extern "C" int brc_register_linear_batched(brc_ctx* ctx, const float* d_ref, lon
   p.conv_iter = ctx->ctl.as<int>();
   p.iters_ws = p.conv_iter + batch;
   p.status = p.iters_ws + batch;
+  {
+    const int ps = make_filter_path(ctx, h_filters, 3, opts->precision, H, D, &p.fpath);
+    if (ps != BRC_OK) return ps;
+  }
   p.cert = nullptr;
   if (opts->certainty_sigma_x100 > 0) {
     BRC_TRY(ctx, ctx->cert.ensure(sizeof(float) * 3 * V * batch), "alloc certainty");
@@ -433,7 +492,8 @@ extern "C" int brc_register_linear_batched(brc_ctx* ctx, const float* d_ref, lon
              (uint64_t)fnv1a(&opts->tolerance, sizeof(float)), (uint64_t)d_params,
              (uint64_t)p.aligned, (uint64_t)d_rotations, (uint64_t)d_iterations,
              (uint64_t)ctx->q1.ptr, (uint64_t)ctx->q2.ptr, (uint64_t)ctx->partials.ptr,
-             (uint64_t)ctx->ctl.ptr, (uint64_t)p.cert, (uint64_t)opts->certainty_sigma_x100};
+             (uint64_t)ctx->ctl.ptr, (uint64_t)p.cert, (uint64_t)opts->certainty_sigma_x100,
+             (uint64_t)opts->precision, (uint64_t)p.fpath.d_taps};
     auto itg = ctx->graphs.find(key);
     GraphEntry* ge = nullptr;
     if (itg == ctx->graphs.end()) {

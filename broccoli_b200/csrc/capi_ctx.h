@@ -8,6 +8,8 @@
 #include <string>
 #include <vector>
 
+#include "filter3d_tc.h"
+
 #include "../../include/broccoli_b200.h"
 
 // Grow-only device buffer.
@@ -62,6 +64,11 @@ struct brc_ctx {
   unsigned long long launches = 0;
   DevBuf q1, q2, aligned, partials, ctl, tmp1, tmp2, series, corrected, params, rot, nl, pyr, cert;
   std::map<GraphKey, std::unique_ptr<GraphEntry>> graphs;
+  // packed split-BF16 taps of the tensor-core filtering, per filter bank
+  // (key: hash of the bank and its size); graphs may hold these pointers,
+  // so an entry lives as long as the graphs do
+  std::map<uint64_t, std::unique_ptr<DevBuf>> tc_taps;
+  DevBuf tc_err;  // device int: a bounded wait of a tensor-core kernel gave up
 
   cudaStream_t stream() const { return use_user_stream ? user_stream : own_stream; }
 
@@ -89,11 +96,33 @@ struct brc_ctx {
     last_error = std::string(where) + ": " + cudaGetErrorString(e);
     return e == cudaErrorMemoryAllocation ? BRC_ERR_NOMEM : BRC_ERR_CUDA;
   }
+  // Device copy of the packed taps of a bank (uploaded on first use; call
+  // outside stream capture).
+  int taps_for(const float* h_filters, int nfilt, const uint16_t** d_taps);
+  // Reads and clears the tensor-core wait flag (synchronises the device).
+  int check_tc_err();
+
   size_t workspace() const {
     return q1.bytes + q2.bytes + aligned.bytes + partials.bytes + ctl.bytes + tmp1.bytes +
            tmp2.bytes + series.bytes + corrected.bytes + params.bytes + rot.bytes + nl.bytes + pyr.bytes;
   }
 };
+
+// The filtering kernel of one precision with what it needs, fixed before
+// any stream capture (make_filter_path uploads the packed taps of the
+// tensor-core path).
+struct FilterPath {
+  int precision = 0;
+  const float* h_filters = nullptr;
+  int nfilt = 3;
+  const uint16_t* d_taps = nullptr;
+  brc::tc::Geometry g{};
+  int* d_err = nullptr;
+};
+int make_filter_path(brc_ctx* ctx, const float* h_filters, int nfilt, int precision, int H, int D,
+                     FilterPath* fp);
+cudaError_t run_filter(const FilterPath& fp, const float* vol, int W, int H, int D, int batch, long long stride,
+                       float* out, const int* conv_iter, int it, cudaStream_t st);
 
 #define BRC_CHECK_CTX(ctx) \
   do {                     \

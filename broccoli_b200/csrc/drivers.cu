@@ -117,11 +117,14 @@ static int nonlinear_scale(brc_ctx* ctx, const float* ref, float* aligned, const
   smoothing_taps(o->tsigma, ft);
   smoothing_taps(o->esigma, fe);
   smoothing_taps(o->dsigma, fd);
-  BRC_TRY(ctx, brc::filter3d_fp32(ref, W, H, D, 1, V, filters6, 6, q1, nullptr, 0, st), "filter ref");
+  FilterPath fp;
+  s = make_filter_path(ctx, filters6, 6, o->precision, H, D, &fp);
+  if (s != BRC_OK) return s;
+  BRC_TRY(ctx, run_filter(fp, ref, W, H, D, 1, V, q1, nullptr, 0, st), "filter ref");
   ctx->launches += 1;
   BRC_TRY(ctx, cudaMemsetAsync(field, 0, sizeof(float) * 3 * V, st), "memset field");
   for (int it = 0; it < iterations; it++) {
-    BRC_TRY(ctx, brc::filter3d_fp32(aligned, W, H, D, 1, V, filters6, 6, q2, nullptr, 0, st), "filter");
+    BRC_TRY(ctx, run_filter(fp, aligned, W, H, D, 1, V, q2, nullptr, 0, st), "filter");
     ctx->launches += 1;
     s = nonlinear_step(ctx, q1, q2, W, H, D, m36, dirs18, ft, fe, fd, o->solve_fp64, field);
     if (s != BRC_OK) return s;
@@ -140,8 +143,8 @@ extern "C" int brc_register_nonlinear(brc_ctx* ctx, const float* d_ref, const fl
       W <= 0 || H <= 0 || D <= 0 || o->iterations < 0 || o->coarsest_scale < 1 ||
       !(o->tsigma > 0) || !(o->esigma > 0) || !(o->dsigma > 0))
     return ctx->fail(BRC_ERR_INVALID, "brc_register_nonlinear: bad argument");
-  if (o->precision != BRC_PREC_FP32)
-    return ctx->fail(BRC_ERR_UNSUPPORTED, "brc_register_nonlinear: precision not available");
+  if (o->precision != BRC_PREC_FP32 && o->precision != BRC_PREC_FP32_GENERAL && o->precision != BRC_PREC_BF16X3)
+    return ctx->fail(BRC_ERR_UNSUPPORTED, "brc_register_nonlinear: unknown precision");
   if (d_aligned == d_moving)
     return ctx->fail(BRC_ERR_INVALID, "brc_register_nonlinear: d_aligned must not alias d_moving");
   cudaSetDevice(ctx->device);

@@ -1,0 +1,449 @@
+// filter3d_tc.cu -- 7x7x7 complex filtering on the tcgen05 tensor cores in
+// BF16 split precision with FP32 accumulation (BRC_PREC_BF16X3).
+//
+// The contraction q_f(z,y,x) = sum_{dz,dy,dx} F_f[3-dz][3-dy][3-dx] V(z+dz,
+// y+dy, x+dx) (NonseparableConvolution3D, broccoli_lib.cpp:4974-5027, true
+// convolution with zero padding) is recast as 49 (or 56) GEMMs per tile,
+// one per (input-plane offset, dy):
+//
+//   D[m][n] += A_{c,dy}[m][k] * B[k][n]
+//     m = (s, f, xo)  128 rows: real filter f (re/im of each complex filter),
+//                     output x offset xo in [0,10), stacked output plane s
+//     k = x_in        16 input samples along x (the window of the 10 outputs
+//                     plus the 6-sample halo): A is a banded Toeplitz matrix
+//                     with the 7 taps of row (dz, dy) of filter f
+//     n = (j, y)      output rows of the tile: plane group j, row y
+//
+// B is never materialised per GEMM: the input tile sits in shared memory as
+// K-major 8x16-byte core matrices (one 16-byte row per (plane, y) and half
+// window of x), so the dy / dz shift of a GEMM is a shift of its smem
+// descriptor's start address by whole rows.  With 3 complex filters (6 real
+// outputs = 60 rows) two output planes share M (s in {0,1}): the GEMM for
+// input-plane offset c feeds plane s with the taps of dz = c - s.  Input
+// planes are stored by parity then so that the rows of plane groups j are
+// evenly spaced for every c.
+//
+// Split precision: x = x_hi + x_lo with both parts BF16 (x_lo the BF16
+// rounding of x - x_hi), for the data and the taps; each GEMM is issued as
+// A_hi B_hi + A_hi B_lo + A_lo B_hi into the same FP32 TMEM accumulator
+// (relative error of a product ~2^-16; the dropped A_lo B_lo ~2^-18).
+//
+// Per CTA (128 threads, one tile = 10 x positions x Ty rows x SP*J planes of
+// one volume): thread 0 streams the packed taps of each GEMM (8 KB, hi+lo)
+// through a 4-slot ring with cp.async.bulk + mbarriers and issues the
+// tcgen05.mma's; tcgen05.commit releases a ring slot when its GEMMs are done.
+// All threads stage the input tile (FP32 -> BF16 hi/lo) before the GEMMs and
+// read the accumulator back with tcgen05.ld afterwards.  Two CTAs per SM
+// overlap one tile's staging/epilogue with the other's GEMMs.  Every wait is
+// bounded (about 2 s); a CTA that gives up sets *err, still waits (bounded)
+// for its GEMMs and copies, frees its TMEM and returns.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <vector>
+
+#include "common.cuh"
+#include "filter3d_tc.h"
+
+namespace brc {
+namespace tc {
+
+constexpr int kThreads = 128;
+constexpr int kRing = 4;
+constexpr int kStageHalves = kM * kK;              // BF16 elements of one A (hi or lo)
+constexpr int kStageBytes = 2 * kStageHalves * 2;  // hi + lo
+constexpr uint32_t kTmemCols = 256;
+constexpr unsigned long long kWaitNs = 2000000000ull;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Shared-memory matrix descriptor, K-major, no swizzle: start address, LBO
+// (byte distance between the two 8-element K halves), SBO (between groups
+// of 8 rows), descriptor version 1.
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+  const uint32_t z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
+      "}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred P1;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+      "selp.b32 %0, 1, 0, P1;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for the phase with the given parity; false after ~2 s.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  if (mbar_test(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  while (!mbar_test(bar, parity))
+    if (global_ns() - t0 > kWaitNs) return false;
+  return true;
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+// Plain (non-multicast) bulk copy global -> own shared memory.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+      "%14, %15}, [%16];\n"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+        "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(__nv_bfloat16 lo_elem, __nv_bfloat16 hi_elem) {
+  return (uint32_t)__bfloat16_as_ushort(lo_elem) | ((uint32_t)__bfloat16_as_ushort(hi_elem) << 16);
+}
+
+__global__ void __launch_bounds__(kThreads, 2)
+filter3d_tc_kernel(const float* __restrict__ vol, int W, int H, int D, long long vstride,
+                   const uint16_t* __restrict__ taps, float* __restrict__ out, int nfilt, Geometry g,
+                   int n_xchunks, const int* __restrict__ conv_iter, int it, int* __restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  const int b = blockIdx.z;
+  if (instance_done(conv_iter, b, it)) return;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int xc = blockIdx.x % n_xchunks, yt = blockIdx.x / n_xchunks;
+  const int x0 = xc * kXo, y0 = yt * g.Ty, z0 = blockIdx.y * g.SP * g.J;
+  const long long V = (long long)W * H * D;
+
+  uint8_t* ring = smem;
+  uint8_t* dhi = smem + kRing * kStageBytes;
+  const uint32_t hl_bytes = 32u * (uint32_t)g.NR;  // two K halves of NR 16-byte rows
+  uint8_t* dlo = dhi + hl_bytes;
+  uint64_t* full = reinterpret_cast<uint64_t*>(dlo + hl_bytes);
+  uint64_t* empty = full + kRing;
+  uint64_t* done = empty + kRing;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+
+  if (tid == 0) {
+    for (int s = 0; s < kRing; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  __syncthreads();
+
+  const int nst = g.nstage;
+  if (tid == 0)
+    for (int s = 0; s < kRing && s < nst; s++) {
+      mbar_expect_tx(&full[s], kStageBytes);
+      bulk_load(ring + s * kStageBytes, taps + (size_t)s * (kStageBytes / 2), kStageBytes, &full[s]);
+    }
+
+  // Stage the input tile: row (parity p, plane slot qq, y row yl) holds the
+  // 16 samples x0-3 .. x0+12 of input plane z0-3 + SP*qq + p, row y0-3+yl,
+  // as two 16-byte K halves (hi and lo arrays).  Rows past the tile are 0.
+  const float* src = vol + (long long)b * vstride;
+  const int NQ = g.SP * g.J + 6;
+  for (int item = tid; item < 2 * g.NR; item += kThreads) {
+    const int row = item >> 1, kh = item & 1;
+    const int par = row / g.RP, rr = row - par * g.RP;
+    const int qq = rr / g.Hp, yl = rr - qq * g.Hp;
+    const int q = qq * g.SP + par;
+    const int zg = z0 - 3 + q, yg = y0 - 3 + yl;
+    const bool rowok = q < NQ && zg >= 0 && zg < D && yg >= 0 && yg < H;
+    const float* rp = src + ((long long)zg * H + yg) * W;
+    float v[8];
+#pragma unroll
+    for (int e = 0; e < 8; e++) {
+      const int xg = x0 - 3 + 8 * kh + e;
+      v[e] = (rowok && xg >= 0 && xg < W) ? __ldg(rp + xg) : 0.f;
+    }
+    uint32_t ph[4], pl[4];
+#pragma unroll
+    for (int e = 0; e < 8; e += 2) {
+      const __nv_bfloat16 h0 = __float2bfloat16_rn(v[e]), h1 = __float2bfloat16_rn(v[e + 1]);
+      const __nv_bfloat16 l0 = __float2bfloat16_rn(v[e] - __bfloat162float(h0));
+      const __nv_bfloat16 l1 = __float2bfloat16_rn(v[e + 1] - __bfloat162float(h1));
+      ph[e / 2] = pack_bf16(h0, h1);
+      pl[e / 2] = pack_bf16(l0, l1);
+    }
+    const uint32_t off = (uint32_t)kh * (uint32_t)g.NR * 16u + (uint32_t)row * 16u;
+    *reinterpret_cast<uint4*>(dhi + off) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
+    *reinterpret_cast<uint4*>(dlo + off) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  // GEMMs (one thread).  Stage s = (c+3)*7 + (dy+3).
+  int ok = 1;
+  if (tid == 0) {
+    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(g.N >> 3) << 17) |
+                           ((uint32_t)(kM >> 4) << 24);
+    const uint32_t ring_a = smem_u32(ring), dhi_a = smem_u32(dhi), dlo_a = smem_u32(dlo);
+    const uint32_t lbo_b = (uint32_t)g.NR * 16u;
+    int s = 0;
+    for (; s < nst; s++) {
+      const int slot = s % kRing;
+      if (!mbar_wait(&full[slot], (uint32_t)(s / kRing) & 1u)) {
+        ok = 0;
+        break;
+      }
+      const int cq = s / 7, dyq = s % 7;  // c + 3, dy + 3
+      const int par = cq % g.SP, qoff = cq / g.SP;
+      const uint32_t brow = (uint32_t)(par * g.RP + qoff * g.Hp + dyq);
+      const uint32_t a_hi = ring_a + (uint32_t)slot * kStageBytes, a_lo = a_hi + kStageBytes / 2;
+      const uint64_t dah = sdesc(a_hi, kM * 16, 128), dal = sdesc(a_lo, kM * 16, 128);
+      const uint64_t dbh = sdesc(dhi_a + brow * 16u, lbo_b, 128), dbl = sdesc(dlo_a + brow * 16u, lbo_b, 128);
+      mma_bf16(tmem, dah, dbh, idesc, s > 0 ? 1u : 0u);
+      mma_bf16(tmem, dah, dbl, idesc, 1u);
+      mma_bf16(tmem, dal, dbh, idesc, 1u);
+      mma_commit(&empty[slot]);
+      // refill the slot of the previous stage once its GEMMs have completed
+      if (s >= 1 && s - 1 + kRing < nst) {
+        const int ps = s - 1, pslot = ps % kRing;
+        if (!mbar_wait(&empty[pslot], (uint32_t)(ps / kRing) & 1u)) {
+          ok = 0;
+          break;
+        }
+        mbar_expect_tx(&full[pslot], kStageBytes);
+        bulk_load(ring + pslot * kStageBytes, taps + (size_t)(ps + kRing) * (kStageBytes / 2), kStageBytes,
+                  &full[pslot]);
+      }
+    }
+    mma_commit(done);
+    if (!ok) {
+      // bounded drain of the copies still in flight before the CTA exits
+      const int issued = (s >= 1 ? s - 1 : 0) + kRing;
+      for (int t = s; t < issued && t < nst; t++) mbar_wait(&full[t % kRing], (uint32_t)(t / kRing) & 1u);
+    }
+  }
+  __syncwarp();
+  const int dok = mbar_wait(done, 0) ? 1 : 0;
+  tc_fence_after();
+
+  // Epilogue: TMEM lane r = M row (s, f, xo); columns n = (j, y).
+  const int r = warp * 32 + lane;
+  int sp, f, xo;
+  bool rvalid;
+  if (g.SP == 2) {
+    sp = r >> 6;
+    const int rr = r & 63;
+    f = rr / kXo;
+    xo = rr - f * kXo;
+    rvalid = rr < 2 * nfilt * kXo;
+  } else {
+    sp = 0;
+    f = r / kXo;
+    xo = r - f * kXo;
+    rvalid = r < 2 * nfilt * kXo;
+  }
+  const int x = x0 + xo;
+  rvalid = rvalid && x < W && ok && dok;
+  float* ob = out + ((long long)b * nfilt + (f >> 1)) * 2 * V + (f & 1);
+  for (int c0 = 0; c0 < g.N; c0 += 16) {
+    uint32_t v[16];
+    tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+#pragma unroll
+    for (int e = 0; e < 16; e++) {
+      const int n = c0 + e;
+      const int j = n / g.Hp, yl = n - j * g.Hp;
+      const int z = z0 + j * g.SP + sp, y = y0 + yl;
+      if (rvalid && j < g.J && yl < g.Ty && y < H && z < D)
+        ob[2 * (((long long)z * H + y) * W + x)] = __uint_as_float(v[e]);
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+  if (tid == 0 && (!ok || !dok)) atomicExch(err, 1);
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+
+static uint16_t bf16_rn(float f) {
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u) return (uint16_t)(u >> 16);  // inf / nan
+  u += 0x7fffu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+static float bf16_to_f(uint16_t h) {
+  const uint32_t u = (uint32_t)h << 16;
+  float f;
+  memcpy(&f, &u, 4);
+  return f;
+}
+
+int stacked_planes(int nfilt) { return nfilt == 3 ? 2 : 1; }
+int num_stages(int nfilt) { return (7 + stacked_planes(nfilt) - 1) * 7; }
+size_t packed_tap_bytes(int nfilt) { return (size_t)num_stages(nfilt) * kStageBytes; }
+
+void pack_taps(const float* h_filters, int nfilt, uint16_t* dst) {
+  const int SP = stacked_planes(nfilt);
+  const int nst = num_stages(nfilt);
+  memset(dst, 0, (size_t)nst * kStageBytes);
+  for (int st = 0; st < nst; st++) {
+    const int c = st / 7 - 3, dy = st % 7 - 3;
+    uint16_t* hi = dst + (size_t)st * 2 * kStageHalves;
+    uint16_t* lo = hi + kStageHalves;
+    for (int r = 0; r < kM; r++) {
+      int s, f, xo;
+      if (SP == 2) {
+        s = r >> 6;
+        const int rr = r & 63;
+        if (rr >= 2 * nfilt * kXo) continue;
+        f = rr / kXo;
+        xo = rr % kXo;
+      } else {
+        s = 0;
+        if (r >= 2 * nfilt * kXo) continue;
+        f = r / kXo;
+        xo = r % kXo;
+      }
+      const int dz = c - s;
+      if (dz < -3 || dz > 3) continue;
+      const float* F = h_filters + (size_t)(f >> 1) * kFilterFloats + (f & 1) * kTaps;
+      for (int kx = xo; kx <= xo + 6; kx++) {
+        const int dx = kx - 3 - xo;
+        const float w = F[(3 - dz) * 49 + (3 - dy) * 7 + (3 - dx)];
+        const uint16_t wh = bf16_rn(w);
+        const uint16_t wl = bf16_rn(w - bf16_to_f(wh));
+        const size_t e = (size_t)(kx / 8) * (kM * 8) + (size_t)r * 8 + (kx % 8);
+        hi[e] = wh;
+        lo[e] = wl;
+      }
+    }
+  }
+}
+
+Geometry make_geometry(int nfilt, int H, int D, int Ty) {
+  Geometry g;
+  g.SP = stacked_planes(nfilt);
+  g.Ty = Ty < H ? Ty : H;
+  g.Hp = g.Ty + 6;
+  g.J = kMaxN / g.Hp;
+  if (g.J < 1) g.J = 1;
+  // no more plane groups than the volume needs
+  const int jmax = (D + g.SP - 1) / g.SP;
+  if (g.J > jmax) g.J = jmax;
+  g.N = ((g.J * g.Hp + 15) / 16) * 16;
+  const int qmax = (5 + g.SP) / g.SP;  // largest plane-slot offset of a GEMM: (c+3)/SP, c <= 2+SP
+  g.RP = ((qmax * g.Hp + 6 + g.N) + 7) / 8 * 8;
+  g.NR = g.SP * g.RP;
+  g.nstage = num_stages(nfilt);
+  g.smem = kRing * kStageBytes + 2 * 32 * g.NR + (2 * kRing + 1) * 8 + 16;
+  return g;
+}
+
+bool geometry_ok(const Geometry& g) {
+  return g.Hp <= kMaxN && g.N >= 16 && g.N <= kMaxN && g.smem <= 227 * 1024;
+}
+
+// Tile rows along y: the candidate with the least GEMM work (tiles x N) that
+// fits, ties to the larger tile.
+int pick_ty(int nfilt, int H, int D) {
+  int best = -1;
+  long long best_cost = 0;
+  const int lo = H < 10 ? H : 10;
+  const int hi = H < kMaxN - 6 ? H : kMaxN - 6;
+  for (int ty = lo; ty <= hi; ty++) {
+    const Geometry g = make_geometry(nfilt, H, D, ty);
+    if (!geometry_ok(g)) continue;
+    const long long ny = (H + g.Ty - 1) / g.Ty;
+    const long long nz = (D + g.SP * g.J - 1) / (g.SP * g.J);
+    long long cost = ny * nz * (g.N + 32);
+    // one CTA per SM leaves no second tile to overlap staging and epilogue
+    if (g.smem > 113 * 1024) cost = cost * 13 / 10;
+    if (best < 0 || cost < best_cost || (cost == best_cost && ty > best)) {
+      best = g.Ty;
+      best_cost = cost;
+    }
+  }
+  return best;
+}
+
+cudaError_t init() {
+  return cudaFuncSetAttribute(filter3d_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+}
+
+cudaError_t launch(const float* vol, int W, int H, int D, int batch, long long stride, const uint16_t* d_taps,
+                   int nfilt, float* out, const int* conv_iter, int it, int* d_err, const Geometry& g,
+                   cudaStream_t st) {
+  if (!geometry_ok(g) || (nfilt != 3 && nfilt != 6) || g.SP != stacked_planes(nfilt)) return cudaErrorInvalidValue;
+  const int nxc = (W + kXo - 1) / kXo;
+  const int nyt = (H + g.Ty - 1) / g.Ty;
+  const int nzt = (D + g.SP * g.J - 1) / (g.SP * g.J);
+  if ((long long)nxc * nyt > 0x7fffffffLL || nzt > 65535 || batch > 65535) return cudaErrorInvalidValue;
+  // at least 77 KB per CTA: at most two CTAs (2 x 256 TMEM columns) per SM
+  const int smem = g.smem > 77 * 1024 ? g.smem : 77 * 1024;
+  dim3 grid((unsigned)(nxc * nyt), (unsigned)nzt, (unsigned)batch);
+  filter3d_tc_kernel<<<grid, kThreads, smem, st>>>(vol, W, H, D, stride, d_taps, out, nfilt, g, nxc, conv_iter,
+                                                   it, d_err);
+  return cudaGetLastError();
+}
+
+}  // namespace tc
+}  // namespace brc

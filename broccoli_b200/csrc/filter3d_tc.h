@@ -1,0 +1,45 @@
+// filter3d_tc.h -- host interface of the tcgen05 split-BF16 filtering kernel
+// (filter3d_tc.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace brc {
+namespace tc {
+
+constexpr int kM = 128;    // GEMM M: (stacked plane, real filter, x offset) rows
+constexpr int kK = 16;     // GEMM K: input samples along x per window
+constexpr int kXo = 10;    // outputs along x per window (kK - 6)
+constexpr int kMaxN = 256; // GEMM N limit (rows of one tile)
+
+// Tile geometry of one launch, chosen on the host.
+struct Geometry {
+  int SP;      // output planes stacked along M (2 for 3 filters, 1 for 6)
+  int Ty;      // output rows along y per tile
+  int Hp;      // Ty + 6: input rows per plane
+  int J;       // plane groups per tile (tile = SP*J output planes)
+  int N;       // GEMM N, multiple of 16, >= J*Hp
+  int RP;      // shared-memory rows per plane-parity array
+  int NR;      // SP * RP
+  int nstage;  // GEMMs per tile: (7 + SP - 1) * 7
+  int smem;    // dynamic shared memory bytes
+};
+
+int stacked_planes(int nfilt);
+int num_stages(int nfilt);
+// Bytes of the packed split-BF16 Toeplitz taps of a bank of nfilt (3 or 6)
+// complex filters, and the packing itself (dst holds packed_tap_bytes/2
+// 16-bit words).
+size_t packed_tap_bytes(int nfilt);
+void pack_taps(const float* h_filters, int nfilt, uint16_t* dst);
+Geometry make_geometry(int nfilt, int H, int D, int Ty);
+bool geometry_ok(const Geometry& g);
+int pick_ty(int nfilt, int H, int D);
+cudaError_t init();
+cudaError_t launch(const float* vol, int W, int H, int D, int batch, long long stride, const uint16_t* d_taps,
+                   int nfilt, float* out, const int* conv_iter, int it, int* d_err, const Geometry& g,
+                   cudaStream_t st);
+
+}  // namespace tc
+}  // namespace brc
