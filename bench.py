@@ -42,7 +42,7 @@ UNIT = "registrations/s"
 FLOP_PER_VOXEL_FILTER = 1372  # per complex 7^3 filter (343 taps x 2 real MACs x 2)
 
 
-def workload_config(n_gpus: int, extra: dict | None = None) -> dict:
+def workload_config(n_gpus: int, extra: dict | None = None, cert_sigma: float = 1.0) -> dict:
     c = {
         "workload": "batched rigid motion correction, 64x64x33x200 series to volume 0",
         "volume": [64, 64, 33],
@@ -52,7 +52,8 @@ def workload_config(n_gpus: int, extra: dict | None = None) -> dict:
         "early_exit_voxels": TOL,
         "filters": "3 complex 7x7x7 quadrature filters (lognormal, u0=pi/3, 2 octaves)",
         "noise": "Rician, SNR 50",
-        "certainty_smoothing": "off",
+        "certainty_smoothing": (f"separable 3x3x3 Gaussian, sigma {cert_sigma:g} voxel" if cert_sigma > 0
+                                else "off"),
         "parallelism": f"replicas x{n_gpus}",
         "l2": "flushed between timed steps (256 MiB write)",
     }
@@ -139,7 +140,7 @@ def symmetric_bank(flt) -> bool:
     return True
 
 
-def accuracy(vols, truth, params, flt, n_oracle: int = 2) -> dict:
+def accuracy(vols, truth, params, flt, n_oracle: int = 2, cert_sigma: float = 0.0) -> dict:
     """RMS displacement error of the GPU results against the FP64 oracle on
     a sample of volumes, and against the known motion on all volumes."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -151,7 +152,8 @@ def accuracy(vols, truth, params, flt, n_oracle: int = 2) -> dict:
         vs_truth.append(S.rms_displacement_error(params[i], rel, SHAPE))
     vs_oracle = []
     for i in range(n_oracle):
-        p64, _, _ = oracle.align_linear(vols[0], vols[i + 1], flt, ITERS, oracle.RIGID, prec="f64")
+        p64, _, _ = oracle.align_linear(vols[0], vols[i + 1], flt, ITERS, oracle.RIGID, prec="f64",
+                                        cert_sigma=cert_sigma)
         vs_oracle.append(S.rms_displacement_error(params[i], p64, SHAPE))
     return {"rms_vs_fp64_oracle_max": float(max(vs_oracle)) if vs_oracle else None,
             "oracle_sample": n_oracle,
@@ -192,7 +194,9 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * secs / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": workload_config(args.gpus),
+        "data": "synthetic",
+        "config": workload_config(args.gpus, {"certainty_smoothing": "none: the reference path has no certainty "
+                                                                     "smoothing (raw certainties)"}),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": thr, "kind": kind,
                          "sample": f"{n_regs} of the {T - 1} registrations per step, {ITERS} iterations "
                                    "each (the reference runs every iteration; no early exit)"},
@@ -220,9 +224,11 @@ def run_gpu(args, rank, world, local_rank):
     moving = d_series[1:]
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
 
+    cs = args.certainty_sigma
+
     def step(precision=None):
         return ctx.register_linear(ref, moving, flt, ITERS, L.RIGID, tolerance=TOL,
-                                   precision=prec if precision is None else precision)
+                                   precision=prec if precision is None else precision, certainty_sigma=cs)
 
     def barrier():
         if world > 1:
@@ -261,6 +267,13 @@ def run_gpu(args, rank, world, local_rank):
     clocks = sampler.stop() if sampler else None
     ms = float(np.sum(times))
     iters_used = out["iterations"].cpu().numpy()
+    if args.only_steps:
+        # the timed step alone (for launch lists and profiles of the step)
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": (T - 1) * args.steps / (ms / 1000.0), "unit": UNIT,
+                              "steps": args.steps, "warmup": args.warmup, "only_steps": True,
+                              "precision": args.precision, "gpu_launches": int(launches)}))
+        return
 
     # ---- end-to-end through the host-buffer entry point ----
     host = torch.from_numpy(vols).pin_memory()
@@ -272,6 +285,7 @@ def run_gpu(args, rank, world, local_rank):
     opts.type = L.RIGID
     opts.tolerance = TOL
     opts.precision = prec
+    opts.certainty_sigma_x100 = int(round(cs * 100))
     vs = np.asarray(VOXEL, np.float32)
     fl = np.ascontiguousarray(flt, np.float32)
     work = torch.empty_like(host).pin_memory()
@@ -296,13 +310,15 @@ def run_gpu(args, rank, world, local_rank):
     # time (batch 1, eager launches, no graph), on a sample of the series ----
     n_serial = min(24, T - 1)
     for i in range(2):
-        ctx.register_linear(ref, moving[i:i + 1], flt, ITERS, L.RIGID, tolerance=TOL, use_graph=False)
+        ctx.register_linear(ref, moving[i:i + 1], flt, ITERS, L.RIGID, tolerance=TOL, use_graph=False,
+                            certainty_sigma=cs)
     torch.cuda.synchronize()
     se0 = torch.cuda.Event(enable_timing=True)
     se1 = torch.cuda.Event(enable_timing=True)
     se0.record(st)
     for i in range(n_serial):
-        ctx.register_linear(ref, moving[i:i + 1], flt, ITERS, L.RIGID, tolerance=TOL, use_graph=False)
+        ctx.register_linear(ref, moving[i:i + 1], flt, ITERS, L.RIGID, tolerance=TOL, use_graph=False,
+                            certainty_sigma=cs)
     se1.record(st)
     se1.synchronize()
     serial_rate = n_serial / (se0.elapsed_time(se1) / 1000.0)
@@ -393,20 +409,21 @@ def run_gpu(args, rank, world, local_rank):
                     "peak_source": "nominal FP32 FMA rate 148 SMs x 128 lanes x 2 at the sampled max SM clock "
                                    "(MEASURED_PEAKS.json has no FP32 figure)",
                     "flop_per_launch": f_flop, "launch_ms": f_ms, "traffic": traffic}
-    acc = accuracy(vols, truth, out["params"].cpu().numpy(), flt) if not args.skip_accuracy else None
+    acc = (accuracy(vols, truth, out["params"].cpu().numpy(), flt, cert_sigma=cs)
+           if not args.skip_accuracy else None)
     cpu = None
     if not args.skip_cpu:
         r, kind, thr, dt = cpu_reference_rate(vols, flt, 8)
         cpu = {"value": r, "unit": UNIT, "cores": thr, "kind": kind,
                "sample": f"8 of the {T - 1} registrations of one series, {ITERS} iterations each, "
-                         f"{dt:.1f} s"}
+                         f"{dt:.1f} s (the reference path: raw certainties, no early exit)"}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3" if prec == L.PREC_BF16X3 else "f32",
         "data": "synthetic",
         "config": workload_config(world, {"mean_iterations": float(iters_used.mean()),
-                                          "precision": args.precision}),
+                                          "precision": args.precision}, cert_sigma=cs),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(4 * V * T),
                 "d2h_bytes_per_step": int(4 * V * (T - 1) + 4 * 15 * (T - 1))},
         "gpu_launches": int(launches),
@@ -433,8 +450,12 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-accuracy", action="store_true")
     ap.add_argument("--series", type=int, default=T, help="series length (volumes)")
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16x3"],
-                    help="filtering precision of the timed path")
+    ap.add_argument("--precision", default="bf16x3", choices=["fp32", "bf16x3"],
+                    help="filtering precision of the timed path (bf16x3: tensor-core split BF16)")
+    ap.add_argument("--certainty-sigma", type=float, default=1.0,
+                    help="sigma (voxels) of the 3x3x3 certainty smoothing; 0 = off")
+    ap.add_argument("--only-steps", action="store_true",
+                    help="time the device-resident steps only (no e2e, baselines or kernel timing)")
     args = ap.parse_args()
     globals()["T"] = args.series
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -56,44 +56,56 @@ __device__ __forceinline__ float phase_grad(float2 a_p, float2 a_c, float2 a_m, 
   return atan2f(ti, tr);
 }
 
-// Certainty volumes |q1 q2| cos^2(dphi/2) of the three filter pairs of every
-// active instance, [b][k][voxel]; input of the optional certainty smoothing.
+// Certainties |q1 q2| cos^2(dphi/2) of the three filter pairs smoothed along
+// x and then y by the 3-tap Gaussian (w1, w0, w1): the first two passes of
+// the separable 3x3x3 certainty smoothing, in the order x, y, z.  Computed
+// where the z pass of the interior voxels reads them: planes 2..D-3, rows
+// and columns 3..N-4 (their x/y neighbours 2..N-3 are inside the volume).
+// One CTA: a 32x8 patch of one plane of one instance; the certainties of
+// the patch and its 1-voxel halo are staged in shared memory.
+constexpr int kCxyTX = 32, kCxyTY = 8;
+
 __global__ void __launch_bounds__(256)
-certainty_kernel(const float2* __restrict__ q1, long long q1_stride, const float2* __restrict__ q2, int W,
-                 int H, int D, float* __restrict__ cert, const int* __restrict__ conv_iter, int it) {
-  const int b = blockIdx.y;
+cert_xy_kernel(const float2* __restrict__ q1, long long q1_stride, const float2* __restrict__ q2, int W, int H,
+               int D, int ntx, float* __restrict__ cxy, const int* __restrict__ conv_iter, int it, float w0,
+               float w1) {
+  const int b = blockIdx.z;
   if (instance_done(conv_iter, b, it)) return;
+  __shared__ float c[3][kCxyTY + 2][kCxyTX + 2];
+  __shared__ float sx[3][kCxyTY + 2][kCxyTX];
   const long long V = (long long)W * H * D;
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= V) return;
+  const int z = 2 + blockIdx.y;
+  const int tx0 = 3 + (blockIdx.x % ntx) * kCxyTX, ty0 = 3 + (blockIdx.x / ntx) * kCxyTY;
   const float2* Q1 = q1 + (long long)b * q1_stride;
   const float2* Q2 = q2 + (long long)b * 3 * V;
+  const long long zoff = (long long)z * W * H;
+  for (int idx = threadIdx.x; idx < (kCxyTY + 2) * (kCxyTX + 2); idx += blockDim.x) {
+    const int ly = idx / (kCxyTX + 2), lx = idx - ly * (kCxyTX + 2);
+    const int x = tx0 - 1 + lx, y = ty0 - 1 + ly;
+    const bool in = x <= W - 3 && y <= H - 3;
+    const long long i = zoff + (long long)y * W + x;
 #pragma unroll
-  for (int k = 0; k < 3; k++) {
-    float pd, c;
-    phase_diff_cert(__ldg(Q1 + k * V + i), __ldg(Q2 + k * V + i), pd, c);
-    cert[((long long)b * 3 + k) * V + i] = c;
-  }
-}
-
-// Separable 3x3x3 Gaussian (weights w1, w0, w1 per axis, normalised) of a
-// certainty volume at an interior voxel (all 27 neighbours inside).
-__device__ __forceinline__ float smoothed_certainty(const float* __restrict__ c, long long i, int W,
-                                                   long long WH, float w0, float w1) {
-  const float w[3] = {w1, w0, w1};
-  float s = 0.f;
-#pragma unroll
-  for (int dz = -1; dz <= 1; dz++) {
-    float sy = 0.f;
-#pragma unroll
-    for (int dy = -1; dy <= 1; dy++) {
-      const float* r = c + i + dz * WH + (long long)dy * W;
-      const float sx = w1 * __ldg(r - 1) + w0 * __ldg(r) + w1 * __ldg(r + 1);
-      sy += w[dy + 1] * sx;
+    for (int k = 0; k < 3; k++) {
+      float pd, cv = 0.f;
+      if (in) phase_diff_cert(__ldg(Q1 + k * V + i), __ldg(Q2 + k * V + i), pd, cv);
+      c[k][ly][lx] = cv;
     }
-    s += w[dz + 1] * sy;
   }
-  return s;
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < (kCxyTY + 2) * kCxyTX; idx += blockDim.x) {
+    const int ly = idx / kCxyTX, lx = idx - ly * kCxyTX;
+#pragma unroll
+    for (int k = 0; k < 3; k++) sx[k][ly][lx] = w1 * c[k][ly][lx] + w0 * c[k][ly][lx + 1] + w1 * c[k][ly][lx + 2];
+  }
+  __syncthreads();
+  const int ly = threadIdx.x / kCxyTX, lx = threadIdx.x - ly * kCxyTX;
+  const int x = tx0 + lx, y = ty0 + ly;
+  if (ly < kCxyTY && x < W - 3 && y < H - 3) {
+    const long long i = zoff + (long long)y * W + x;
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+      cxy[((long long)b * 3 + k) * V + i] = w1 * sx[k][ly][lx] + w0 * sx[k][ly + 1][lx] + w1 * sx[k][ly + 2][lx];
+  }
 }
 
 // Sum e (0..13) of one axis as (row moment) x y^py x z^pz: moments
@@ -182,8 +194,11 @@ normal_eq_partial_kernel(const float2* __restrict__ q1, long long q1_stride,
         const float2 a = __ldg(A + i), c = __ldg(C + i);
         float pd, cert;
         phase_diff_cert(a, c, pd, cert);
-        if (cert_in != nullptr)
-          cert = smoothed_certainty(cert_in + ((long long)b * 3 + k) * V, i, W, WH, cw0, cw1);
+        if (cert_in != nullptr) {
+          // z pass of the separable smoothing over the x/y-smoothed certainties
+          const float* cz = cert_in + ((long long)b * 3 + k) * V + i;
+          cert = cw1 * __ldg(cz - WH) + cw0 * __ldg(cz) + cw1 * __ldg(cz + WH);
+        }
         const float g = phase_grad(__ldg(A + i + s), a, __ldg(A + i - s), __ldg(C + i + s), c,
                                    __ldg(C + i - s));
         const float cg = cert * g;
@@ -713,10 +728,13 @@ cudaError_t normal_eq_partials(const float* q1, long long q1_stride_floats, cons
     const float e = (float)exp(-1.0 / (2.0 * (double)cert_sigma * (double)cert_sigma));
     w0 = 1.0f / (1.0f + 2.0f * e);
     w1 = e * w0;
-    dim3 cgrid((unsigned)(((long long)W * H * D + 255) / 256), batch);
-    certainty_kernel<<<cgrid, 256, 0, st>>>(reinterpret_cast<const float2*>(q1), q1_stride_floats / 2,
-                                            reinterpret_cast<const float2*>(q2), W, H, D,
-                                            const_cast<float*>(cert), conv_iter, it);
+    const int ntx = (W - 6 + kCxyTX - 1) / kCxyTX, nty = (H - 6 + kCxyTY - 1) / kCxyTY;
+    if (W > 6 && H > 6 && D > 6) {
+      dim3 cgrid((unsigned)(ntx * nty), (unsigned)(D - 4), batch);
+      cert_xy_kernel<<<cgrid, kCxyTX * kCxyTY, 0, st>>>(reinterpret_cast<const float2*>(q1), q1_stride_floats / 2,
+                                                          reinterpret_cast<const float2*>(q2), W, H, D, ntx,
+                                                          const_cast<float*>(cert), conv_iter, it, w0, w1);
+    }
   }
   dim3 grid(nblk, batch);
   normal_eq_partial_kernel<<<grid, kNEThreads, 0, st>>>(

@@ -53,6 +53,10 @@ enum { ORC_TRANSLATION = 0, ORC_RIGID = 1, ORC_AFFINE = 2 };
                              const real* original, int W, int H, int D,         \
                              const real* filters, int niter, int type,          \
                              real* p12, real* rot3);                            \
+  void orc_align_linear_cs##SFX(const real* ref, real* aligned,                 \
+                                const real* original, int W, int H, int D,      \
+                                const real* filters, int niter, int type,       \
+                                double cert_sigma, real* p12, real* rot3);      \
   void orc_motion_correct##SFX(real* vols, int W, int H, int D, int T,          \
                                const real* voxel_size, const real* filters,     \
                                int niter, real* motion6T);                      \

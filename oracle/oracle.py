@@ -172,8 +172,9 @@ def warp_field(src: np.ndarray, dx, dy, dz, prec: str = "f32") -> np.ndarray:
 
 
 def align_linear(ref: np.ndarray, moving: np.ndarray, filters: np.ndarray, niter: int,
-                 type_: int = AFFINE, prec: str = "f32"):
-    """Single-scale linear registration of `moving` to `ref`.
+                 type_: int = AFFINE, prec: str = "f32", cert_sigma: float = 0.0):
+    """Single-scale linear registration of `moving` to `ref`; cert_sigma > 0
+    smooths the certainties by the separable 3x3x3 Gaussian of that sigma.
 
     Returns (params12, aligned volume, rotations in degrees or None)."""
     dt, s = _dt(prec)
@@ -184,8 +185,9 @@ def align_linear(ref: np.ndarray, moving: np.ndarray, filters: np.ndarray, niter
     f = _arr(filters, dt)
     p = np.zeros(12, dt)
     rot = np.zeros(3, dt)
-    getattr(orc_lib(), "orc_align_linear" + s)(_ptr(r), _ptr(aligned), _ptr(orig), W, H, D, _ptr(f),
-                                               niter, type_, _ptr(p), _ptr(rot))
+    fn = getattr(orc_lib(), "orc_align_linear_cs" + s)
+    fn.argtypes = [_P, _P, _P, _I, _I, _I, _P, _I, _I, _D, _P, _P]
+    fn(_ptr(r), _ptr(aligned), _ptr(orig), W, H, D, _ptr(f), niter, type_, float(cert_sigma), _ptr(p), _ptr(rot))
     return p, aligned, (rot if type_ == RIGID else None)
 
 

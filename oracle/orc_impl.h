@@ -553,6 +553,16 @@ void FN(orc_warp_field)(const REAL* src, int W, int H, int D, const REAL* dx,
 void FN(orc_align_linear)(const REAL* ref, REAL* aligned, const REAL* original,
                           int W, int H, int D, const REAL* filters, int niter,
                           int type, REAL* p12, REAL* rot3) {
+  FN(orc_align_linear_cs)(ref, aligned, original, W, H, D, filters, niter, type, 0.0, p12, rot3);
+}
+
+/* orc_align_linear with the certainties smoothed by the separable 3x3x3
+ * Gaussian of orc_normal_equations_smoothcert when cert_sigma > 0 (the
+ * certainty-smoothing switch of the batched motion-correction workload;
+ * not in the reference). */
+void FN(orc_align_linear_cs)(const REAL* ref, REAL* aligned, const REAL* original,
+                             int W, int H, int D, const REAL* filters, int niter,
+                             int type, double cert_sigma, REAL* p12, REAL* rot3) {
   const long V = (long)W * H * D;
   REAL* q1 = (REAL*)malloc(sizeof(REAL) * 6 * V);
   REAL* q2 = (REAL*)malloc(sizeof(REAL) * 6 * V);
@@ -561,7 +571,10 @@ void FN(orc_align_linear)(const REAL* ref, REAL* aligned, const REAL* original,
   for (int i = 0; i < 12; i++) p12[i] = RZERO;
   for (int it = 0; it < niter; it++) {
     FN(orc_filter3d)(aligned, W, H, D, filters, 3, q2);
-    FN(orc_normal_equations)(q1, q2, W, H, D, A, h);
+    if (cert_sigma > 0.0)
+      FN(orc_normal_equations_smoothcert)(q1, q2, W, H, D, cert_sigma, A, h);
+    else
+      FN(orc_normal_equations)(q1, q2, W, H, D, A, h);
     FN(orc_solve)(A, h, 12, p);
     if (type == ORC_TRANSLATION) {
       p12[0] += p[0];
