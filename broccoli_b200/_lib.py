@@ -85,6 +85,7 @@ _SIGS = {
     "brc_ctx_set_stream": ([_P, _P], _I),
     "brc_ctx_stream": ([_P], _P),
     "brc_ctx_synchronize": ([_P], _I),
+    "brc_selftest_bounded_wait": ([_P, _I], _I),
     "brc_ctx_workspace_bytes": ([_P], ctypes.c_size_t),
     "brc_ctx_kernel_launches": ([_P], ctypes.c_ulonglong),
     "brc_filter3d": ([_P, _P, _I, _I, _I, _I, _LL, _P, _I, _I, _P], _I),
@@ -93,6 +94,7 @@ _SIGS = {
     "brc_warp_affine": ([_P, _P, _I, _I, _I, _I, _P, _P], _I),
     "brc_warp_field": ([_P, _P, _I, _I, _I, _P, _P, _P, _P], _I),
     "brc_smooth3d": ([_P, _P, _I, _I, _I, _I, _P, _P, _P, _P, _P, _P], _I),
+    "brc_smooth_normalized": ([_P, _P, _I, _I, _I, _I, _P, _P, _P, _P, _P], _I),
     "brc_rescale_linear": ([_P, _P, _I, _I, _I, _P, _I, _I, _I], _I),
     "brc_linear_opts_default": ([ctypes.POINTER(LinearOpts), _I], None),
     "brc_register_linear_batched": (

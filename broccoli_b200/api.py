@@ -87,6 +87,13 @@ class Context:
         self._bind_stream()
         _check(self, L.lib().brc_ctx_synchronize(self.handle))
 
+    def selftest_bounded_wait(self, wait_ms: int = 50) -> None:
+        """Queues the self-test of the device-side bounded wait: the next
+        synchronize() raises a timeout error, after which the context is
+        usable again."""
+        self._bind_stream()
+        _check(self, L.lib().brc_selftest_bounded_wait(self.handle, int(wait_ms)))
+
     # ---- kernels ---------------------------------------------------------
 
     def filter3d(self, vol: torch.Tensor, filters, precision: int = L.PREC_FP32) -> torch.Tensor:
@@ -159,6 +166,20 @@ class Context:
                                           _p(c) if c is not None else None,
                                           _p(sc) if sc is not None else None, _p(out)))
         return out if vol.dim() == 4 else out[0]
+
+    def smooth_normalized(self, vols: torch.Tensor, mask: torch.Tensor, fx, fy, fz) -> torch.Tensor:
+        """Normalised-convolution smoothing of vols (T,D,H,W) or (D,H,W) with
+        the certainty `mask` (D,H,W); NaN where the smoothed mask is 0, as in
+        the reference."""
+        v = _vol_batch(vols)
+        T, D, H, W = v.shape
+        m = mask.contiguous()
+        taps = [np.ascontiguousarray(np.asarray(f, np.float32).reshape(9)) for f in (fx, fy, fz)]
+        out = torch.empty_like(v)
+        self._bind_stream()
+        _check(self, L.lib().brc_smooth_normalized(self.handle, _p(v), W, H, D, T, _p(m),
+                                                   *[t.ctypes.data_as(ctypes.c_void_p) for t in taps], _p(out)))
+        return out if vols.dim() == 4 else out[0]
 
     def rescale_linear(self, src: torch.Tensor, shape) -> torch.Tensor:
         v = src.contiguous()

@@ -20,6 +20,7 @@ _pack_permutation_4d = (3, 2, 0, 1)
 
 TRANSLATION, RIGID, AFFINE = 0, 1, 2
 NEAREST, LINEAR, CUBIC = 0, 1, 2
+LOWPASS, RANDOM = 0, 1  # smoothing types (broccoli_constants.h)
 
 
 def _permute(permutation, array):
@@ -242,6 +243,12 @@ class BROCCOLI_LIB:
     def SetOutputAlignedT1VolumeNonLinear(self, a): self.out["aligned_nonlinear"] = a
     def SetOutputInterpolatedT1Volume(self, a): self.out["interpolated"] = a
     def SetOutputDisplacementField(self, x, y, z): self.out["field"] = (x, y, z)
+    def SetOutputSmoothedfMRIVolumes(self, a): self.out["smoothed"] = a
+    def SetEPISmoothingAmount(self, fwhm_mm): self.epi_fwhm = float(fwhm_mm)
+    def SetSmoothingType(self, t): self.smoothing_type = int(t)
+    def SetSmoothingFilters(self, fx, fy, fz):
+        self.smoothing_filters = [np.ascontiguousarray(f, np.float32).reshape(9) for f in (fx, fy, fz)]
+    def SetEPIMask(self, mask): self.epi_mask = mask  # packed like the volumes (packVolume)
 
     # ---- entry points -------------------------------------------------------
 
@@ -264,6 +271,36 @@ class BROCCOLI_LIB:
             self.out["motion"][...] = motion.reshape(self.out["motion"].shape)
         if "mc" in self.out:
             self.out["mc"][...] = vols.reshape(self.out["mc"].shape)
+
+    def _smoothing_taps(self):
+        if getattr(self, "smoothing_type", LOWPASS) == RANDOM:
+            return self.smoothing_filters
+        return fwhm_filters(getattr(self, "epi_fwhm", 0.0), self.epi_vox)
+
+    def _smooth(self, normalized: bool):
+        import torch
+        from .api import Context
+        W, H, D, T = self.epi
+        ctx = Context(0)
+        vols = torch.from_numpy(np.ascontiguousarray(self.fmri, np.float32).reshape(T, D, H, W)).cuda()
+        fx, fy, fz = self._smoothing_taps()
+        if normalized:
+            mask = torch.from_numpy(np.ascontiguousarray(self.epi_mask, np.float32).reshape(D, H, W)).cuda()
+            out = ctx.smooth_normalized(vols, mask, fx, fy, fz)
+        else:
+            out = ctx.smooth3d(vols, fx, fy, fz)
+        if "smoothed" in self.out:
+            self.out["smoothed"][...] = out.cpu().numpy().reshape(self.out["smoothed"].shape)
+        ctx.close()
+
+    def PerformSmoothingWrapper(self):
+        """PerformSmoothingWrapper (broccoli_lib.cpp:11122-11210)."""
+        self._smooth(False)
+
+    def PerformSmoothingNormalizedWrapper(self):
+        """PerformSmoothingNormalizedWrapper (broccoli_lib.cpp:11227-11272):
+        the EPI mask is the certainty."""
+        self._smooth(True)
 
     def PerformRegistrationTwoVolumesWrapper(self):
         import torch
@@ -288,6 +325,42 @@ class BROCCOLI_LIB:
             for a in range(3):
                 self.out["field"][a][...] = f[a].reshape(self.out["field"][a].shape)
         ctx.close()
+
+
+def fwhm_filters(fwhm_mm: float, voxel_sizes):
+    """9-tap Gaussians for a FWHM in mm along x, y, z: sigma = FWHM / 2.354 /
+    voxel size, weights exp(-u^2 / 2 sigma^2) in double, stored float and
+    normalised by their float sum (CreateSmoothingFilters,
+    broccoli_lib.cpp:11093-11121)."""
+    out = []
+    for a in range(3):
+        sigma = float(fwhm_mm) / 2.354 / float(voxel_sizes[a])
+        u = np.arange(9, dtype=np.float64) - 4
+        f = np.exp(-(u ** 2) / (2.0 * sigma * sigma)).astype(np.float32)
+        s = np.float32(0)
+        for v in f:
+            s = np.float32(s + v)
+        out.append((f / s).astype(np.float32))
+    return out
+
+
+def performSmoothingNormalized(h_fMRI_Volumes, h_EPI_Mask, h_fMRI_Voxel_Sizes, fwhm_mm,
+                               OPENCL_PLATFORM=0, OPENCL_DEVICE=0):
+    """Normalised-convolution smoothing of an fMRI series with a mask
+    (PerformSmoothingNormalizedWrapper) through the wrapper class.  Returns
+    the smoothed volumes in the wrapper's output layout."""
+    B = BROCCOLI_LIB(OPENCL_PLATFORM, OPENCL_DEVICE)
+    if not B.GetOpenCLInitiated():
+        raise RuntimeError("initialisation failed: " + B.GetOpenCLInitializationError())
+    shape = h_fMRI_Volumes.shape
+    B.SetfMRIData(h_fMRI_Volumes, h_fMRI_Voxel_Sizes)
+    B.SetEPIMask(B.packVolume(h_EPI_Mask))
+    B.SetEPISmoothingAmount(fwhm_mm)
+    B.SetSmoothingType(LOWPASS)
+    out = B.createOutputArray(shape)
+    B.SetOutputSmoothedfMRIVolumes(out)
+    B.PerformSmoothingNormalizedWrapper()
+    return B.unpackOutputVolume(out, shape)
 
 
 def performMotionCorrection(h_fMRI_Volumes, h_fMRI_Voxel_Sizes, h_Quadrature_Filters, iterations,

@@ -169,6 +169,9 @@ void BROCCOLI_LIB::SetSmoothingFilters(float* fx, float* fy, float* fz) {
 }
 void BROCCOLI_LIB::SetSmoothingType(int t) { smoothing_type_ = t; }
 void BROCCOLI_LIB::SetEPISmoothingAmount(float fwhm) { epi_fwhm_ = fwhm; }
+void BROCCOLI_LIB::SetEPIMask(float* m) { h_epi_mask_ = m; }
+void BROCCOLI_LIB::SetInputCertainty(float* c) { h_certainty_ = c; }
+void BROCCOLI_LIB::SetAutoMask(bool a) { auto_mask_ = a; }
 void BROCCOLI_LIB::SetPrecision(int p) { precision_ = p; }
 void BROCCOLI_LIB::SetMotionCorrectionTolerance(float v) { mc_tolerance_ = v; }
 void BROCCOLI_LIB::SetSolveFP64(bool b) { solve_fp64_ = b; }
@@ -275,6 +278,63 @@ void BROCCOLI_LIB::PerformSmoothingWrapper() {
              "brc_smooth3d"))
     return;
   check(brc_copy_to_host(ctx_, out_smoothed_, out.ptr, sizeof(float) * n), "D2H");
+}
+
+// PerformSmoothingNormalizedWrapper, broccoli_lib.cpp:11227-11272: the EPI
+// mask is the certainty; LOWPASS filters from the FWHM or RANDOM filters.
+void BROCCOLI_LIB::PerformSmoothingNormalizedWrapper() {
+  if (!initiated_ && !check(BRC_ERR_NODEVICE, "PerformSmoothingNormalizedWrapper")) return;
+  if (!h_fmri_ || !out_smoothed_ || !h_epi_mask_) {
+    check(BRC_ERR_INVALID, "PerformSmoothingNormalizedWrapper: input, mask or output not set");
+    return;
+  }
+  smooth_normalized(h_epi_mask_, out_smoothed_, "PerformSmoothingNormalizedWrapper");
+}
+
+// PerformSmoothingNormalizedHostWrapper, broccoli_lib.cpp:11729-11850 (the
+// Smoothing CLI, Bash_Wrapper/Smoothing.cpp:593-613): the certainty from
+// SetInputCertainty, LOWPASS filters from the FWHM, the fMRI volumes
+// smoothed in place.  The reference smooths one volume per upload; here all
+// volumes go through one batched call.
+void BROCCOLI_LIB::PerformSmoothingNormalizedHostWrapper() {
+  if (!initiated_ && !check(BRC_ERR_NODEVICE, "PerformSmoothingNormalizedHostWrapper")) return;
+  if (auto_mask_) {
+    check(BRC_ERR_UNSUPPORTED, "PerformSmoothingNormalizedHostWrapper: automatic EPI mask not available");
+    return;
+  }
+  if (!h_fmri_ || !h_certainty_) {
+    check(BRC_ERR_INVALID, "PerformSmoothingNormalizedHostWrapper: input or certainty not set");
+    return;
+  }
+  const int keep = smoothing_type_;
+  smoothing_type_ = LOWPASS;
+  smooth_normalized(h_certainty_, h_fmri_, "PerformSmoothingNormalizedHostWrapper");
+  smoothing_type_ = keep;
+}
+
+void BROCCOLI_LIB::smooth_normalized(const float* h_mask, float* h_out, const char* where) {
+  float fx[9], fy[9], fz[9];
+  if (smoothing_type_ == RANDOM) {
+    if (!smooth_f_[0] || !smooth_f_[1] || !smooth_f_[2]) {
+      check(BRC_ERR_INVALID, (std::string(where) + ": smoothing filters not set").c_str());
+      return;
+    }
+    memcpy(fx, smooth_f_[0], sizeof(fx));
+    memcpy(fy, smooth_f_[1], sizeof(fy));
+    memcpy(fz, smooth_f_[2], sizeof(fz));
+  } else {
+    fwhm_filters(epi_fwhm_, epi_vox_, fx, fy, fz);
+  }
+  const size_t V = epi_w_ * epi_h_ * epi_d_, n = V * epi_t_;
+  DeviceArray in(ctx_, sizeof(float) * n), out(ctx_, sizeof(float) * n), mask(ctx_, sizeof(float) * V);
+  if (!check(in.status, "alloc") || !check(out.status, "alloc") || !check(mask.status, "alloc")) return;
+  if (!check(brc_copy_to_device(ctx_, in.ptr, h_fmri_, sizeof(float) * n), "H2D")) return;
+  if (!check(brc_copy_to_device(ctx_, mask.ptr, h_mask, sizeof(float) * V), "H2D")) return;
+  if (!check(brc_smooth_normalized(ctx_, in.f(), (int)epi_w_, (int)epi_h_, (int)epi_d_, (int)epi_t_, mask.f(), fx,
+                                   fy, fz, out.f()),
+             "brc_smooth_normalized"))
+    return;
+  check(brc_copy_to_host(ctx_, h_out, out.ptr, sizeof(float) * n), "D2H");
 }
 
 // PerformRegistrationTwoVolumesWrapper, broccoli_lib.cpp:7973-8112.

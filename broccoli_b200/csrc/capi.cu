@@ -74,7 +74,66 @@ int brc_ctx::check_tc_err() {
   return fail(BRC_ERR_TIMEOUT, "a bounded wait of the tensor-core filtering kernel gave up");
 }
 
-int make_filter_path(brc_ctx* ctx, const float* h_filters, int nfilt, int precision, int H, int D,
+int brc_ctx::tune_tc(int nfilt, int W, int H, int D, const uint16_t* d_taps, int* ty) {
+  const auto key = std::make_tuple(nfilt, W, H, D);
+  auto it = tc_tuned.find(key);
+  if (it != tc_tuned.end()) {
+    *ty = it->second;
+    return BRC_OK;
+  }
+  int tys[3];
+  const int n = brc::tc::candidate_tys(nfilt, H, D, tys, 3);
+  if (n <= 0) return fail(BRC_ERR_UNSUPPORTED, "volume shape not supported by the BF16X3 filtering");
+  *ty = tys[0];
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  BRC_TRY(this, cudaStreamIsCapturing(stream(), &cap), "capture status");
+  if (cap != cudaStreamCaptureStatusNone) return BRC_OK;  // no timing inside a capture
+  if (n > 1) {
+    // time each candidate on zero-filled scratch volumes (the kernel's
+    // work does not depend on the data): one warm launch, best of three
+    const long long V = (long long)W * H * D;
+    long long nb = (1ll << 24) / (V > 0 ? V : 1);
+    nb = nb < 1 ? 1 : (nb > 32 ? 32 : nb);
+    BRC_TRY(this, cudaStreamSynchronize(stream()), "synchronize");
+    BRC_TRY(this, tmp1.ensure(sizeof(float) * (size_t)(V * nb)), "alloc");
+    BRC_TRY(this, tmp2.ensure(sizeof(float) * (size_t)(V * nb) * 2 * nfilt), "alloc");
+    BRC_TRY(this, cudaMemsetAsync(tmp1.ptr, 0, sizeof(float) * (size_t)(V * nb), own_stream), "memset");
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    BRC_TRY(this, cudaEventCreate(&e0), "event");
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+      cudaEventDestroy(e0);
+      return fail(BRC_ERR_CUDA, "event");
+    }
+    float best = -1.f;
+    cudaError_t err = cudaSuccess;
+    for (int c = 0; c < n && err == cudaSuccess; c++) {
+      const brc::tc::Geometry g = brc::tc::make_geometry(nfilt, H, D, tys[c]);
+      float ms_best = -1.f;
+      for (int rep = 0; rep < 4 && err == cudaSuccess; rep++) {
+        err = cudaEventRecord(e0, own_stream);
+        if (err == cudaSuccess)
+          err = brc::tc::launch(tmp1.as<float>(), W, H, D, (int)nb, V, d_taps, nfilt, tmp2.as<float>(), nullptr, 0,
+                                tc_err.as<int>(), g, own_stream);
+        if (err == cudaSuccess) err = cudaEventRecord(e1, own_stream);
+        if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+        if (err == cudaSuccess && rep > 0 && (ms_best < 0.f || ms < ms_best)) ms_best = ms;
+      }
+      if (err == cudaSuccess && (best < 0.f || ms_best < best)) {
+        best = ms_best;
+        *ty = tys[c];
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    BRC_TRY(this, err, "tile timing");
+  }
+  tc_tuned[key] = *ty;
+  return BRC_OK;
+}
+
+int make_filter_path(brc_ctx* ctx, const float* h_filters, int nfilt, int precision, int W, int H, int D,
                      FilterPath* fp) {
   if (nfilt != 3 && nfilt != 6) return ctx->fail(BRC_ERR_INVALID, "filtering needs 3 or 6 filters");
   fp->precision = precision;
@@ -84,10 +143,13 @@ int make_filter_path(brc_ctx* ctx, const float* h_filters, int nfilt, int precis
   fp->d_err = ctx->tc_err.as<int>();
   if (precision == BRC_PREC_FP32 || precision == BRC_PREC_FP32_GENERAL) return BRC_OK;
   if (precision != BRC_PREC_BF16X3) return ctx->fail(BRC_ERR_UNSUPPORTED, "unknown precision");
-  const int ty = brc::tc::pick_ty(nfilt, H, D);
-  if (ty <= 0) return ctx->fail(BRC_ERR_UNSUPPORTED, "volume shape not supported by the BF16X3 filtering");
+  int st = ctx->taps_for(h_filters, nfilt, &fp->d_taps);
+  if (st != BRC_OK) return st;
+  int ty = 0;
+  st = ctx->tune_tc(nfilt, W, H, D, fp->d_taps, &ty);
+  if (st != BRC_OK) return st;
   fp->g = brc::tc::make_geometry(nfilt, H, D, ty);
-  return ctx->taps_for(h_filters, nfilt, &fp->d_taps);
+  return BRC_OK;
 }
 
 cudaError_t run_filter(const FilterPath& fp, const float* vol, int W, int H, int D, int batch, long long stride,
@@ -189,6 +251,15 @@ int brc_ctx_synchronize(brc_ctx* ctx) {
   return ctx->check_tc_err();
 }
 
+int brc_selftest_bounded_wait(brc_ctx* ctx, int wait_ms) {
+  BRC_CHECK_CTX(ctx);
+  if (wait_ms < 1 || wait_ms > 1000) return ctx->fail(BRC_ERR_INVALID, "brc_selftest_bounded_wait: 1..1000 ms");
+  cudaSetDevice(ctx->device);
+  BRC_TRY(ctx, brc::tc::bounded_wait_probe(wait_ms, ctx->tc_err.as<int>(), ctx->stream()), "bounded wait probe");
+  ctx->launches += 1;
+  return BRC_OK;
+}
+
 size_t brc_ctx_workspace_bytes(const brc_ctx* ctx) { return ctx ? ctx->workspace() : 0; }
 
 unsigned long long brc_ctx_kernel_launches(const brc_ctx* ctx) { return ctx ? ctx->launches : 0; }
@@ -204,7 +275,7 @@ int brc_filter3d(brc_ctx* ctx, const float* d_vol, int W, int H, int D, int batc
     return ctx->fail(BRC_ERR_INVALID, "brc_filter3d: vol_stride smaller than a volume");
   cudaSetDevice(ctx->device);
   FilterPath fp;
-  const int ps = make_filter_path(ctx, h_filters, nfilt, precision, H, D, &fp);
+  const int ps = make_filter_path(ctx, h_filters, nfilt, precision, W, H, D, &fp);
   if (ps != BRC_OK) return ps;
   BRC_TRY(ctx, run_filter(fp, d_vol, W, H, D, batch, vol_stride, d_out, nullptr, 0, ctx->stream()), "filter3d");
   ctx->launches += 1;
@@ -289,6 +360,31 @@ int brc_smooth3d(brc_ctx* ctx, const float* d_vol, int W, int H, int D, int batc
                              ctx->tmp1.as<float>(), ctx->tmp2.as<float>(), d_out, ctx->stream()),
           "smooth3d");
   ctx->launches += 3;
+  return BRC_OK;
+}
+
+int brc_smooth_normalized(brc_ctx* ctx, const float* d_vols, int W, int H, int D, int T, const float* d_mask,
+                          const float* h_fx, const float* h_fy, const float* h_fz, float* d_out) {
+  BRC_CHECK_CTX(ctx);
+  if (!d_vols || !d_mask || !d_out || !h_fx || !h_fy || !h_fz || bad_dims(W, H, D) || T <= 0 || T > 65535)
+    return ctx->fail(BRC_ERR_INVALID, "brc_smooth_normalized: bad pointer or size");
+  cudaSetDevice(ctx->device);
+  const long long V = (long long)W * H * D;
+  const size_t bytes = sizeof(float) * (size_t)V * T;
+  BRC_TRY(ctx, ctx->tmp1.ensure(bytes), "alloc");
+  BRC_TRY(ctx, ctx->tmp2.ensure(bytes), "alloc");
+  BRC_TRY(ctx, ctx->smask.ensure(sizeof(float) * (size_t)V), "alloc");
+  const cudaStream_t st = ctx->stream();
+  // smoothed certainty (all-ones certainty), then the certainty-weighted
+  // smoothing of every volume divided by it, then the mask product
+  BRC_TRY(ctx, brc::smooth3d(d_mask, W, H, D, 1, h_fx, h_fy, h_fz, nullptr, nullptr, ctx->tmp1.as<float>(),
+                             ctx->tmp2.as<float>(), ctx->smask.as<float>(), st),
+          "smooth mask");
+  BRC_TRY(ctx, brc::smooth3d(d_vols, W, H, D, T, h_fx, h_fy, h_fz, d_mask, ctx->smask.as<float>(),
+                             ctx->tmp1.as<float>(), ctx->tmp2.as<float>(), d_out, st),
+          "smooth volumes");
+  BRC_TRY(ctx, brc::multiply_mask(d_out, d_mask, V, T, st), "multiply mask");
+  ctx->launches += 7;
   return BRC_OK;
 }
 
@@ -470,7 +566,7 @@ extern "C" int brc_register_linear_batched(brc_ctx* ctx, const float* d_ref, lon
   p.iters_ws = p.conv_iter + batch;
   p.status = p.iters_ws + batch;
   {
-    const int ps = make_filter_path(ctx, h_filters, 3, opts->precision, H, D, &p.fpath);
+    const int ps = make_filter_path(ctx, h_filters, 3, opts->precision, W, H, D, &p.fpath);
     if (ps != BRC_OK) return ps;
   }
   p.cert = nullptr;

@@ -6,6 +6,7 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "filter3d_tc.h"
@@ -69,6 +70,9 @@ struct brc_ctx {
   // so an entry lives as long as the graphs do
   std::map<uint64_t, std::unique_ptr<DevBuf>> tc_taps;
   DevBuf tc_err;  // device int: a bounded wait of a tensor-core kernel gave up
+  DevBuf smask;   // smoothed certainty of brc_smooth_normalized
+  // tensor-core tile height chosen by timing, per (nfilt, W, H, D)
+  std::map<std::tuple<int, int, int, int>, int> tc_tuned;
 
   cudaStream_t stream() const { return use_user_stream ? user_stream : own_stream; }
 
@@ -101,6 +105,10 @@ struct brc_ctx {
   int taps_for(const float* h_filters, int nfilt, const uint16_t** d_taps);
   // Reads and clears the tensor-core wait flag (synchronises the device).
   int check_tc_err();
+  // Tile height of the tensor-core filtering for a shape: the fastest of the
+  // cost model's candidates, timed once per shape (outside stream capture;
+  // under capture the cost model's first choice).
+  int tune_tc(int nfilt, int W, int H, int D, const uint16_t* d_taps, int* ty);
 
   size_t workspace() const {
     return q1.bytes + q2.bytes + aligned.bytes + partials.bytes + ctl.bytes + tmp1.bytes +
@@ -119,7 +127,7 @@ struct FilterPath {
   brc::tc::Geometry g{};
   int* d_err = nullptr;
 };
-int make_filter_path(brc_ctx* ctx, const float* h_filters, int nfilt, int precision, int H, int D,
+int make_filter_path(brc_ctx* ctx, const float* h_filters, int nfilt, int precision, int W, int H, int D,
                      FilterPath* fp);
 cudaError_t run_filter(const FilterPath& fp, const float* vol, int W, int H, int D, int batch, long long stride,
                        float* out, const int* conv_iter, int it, cudaStream_t st);

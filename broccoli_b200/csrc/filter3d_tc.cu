@@ -29,14 +29,14 @@
 // (relative error of a product ~2^-16; the dropped A_lo B_lo ~2^-18).
 //
 // Per CTA (128 threads, one tile = 10 x positions x Ty rows x SP*J planes of
-// one volume): thread 0 streams the packed taps of each GEMM (8 KB, hi+lo)
-// through a 4-slot ring with cp.async.bulk + mbarriers and issues the
-// tcgen05.mma's; tcgen05.commit releases a ring slot when its GEMMs are done.
-// All threads stage the input tile (FP32 -> BF16 hi/lo) before the GEMMs and
-// read the accumulator back with tcgen05.ld afterwards.  Two CTAs per SM
-// overlap one tile's staging/epilogue with the other's GEMMs.  Every wait is
-// bounded (about 2 s); a CTA that gives up sets *err, still waits (bounded)
-// for its GEMMs and copies, frees its TMEM and returns.
+// one volume): all threads stage the input tile (FP32 -> BF16 hi/lo); then
+// thread 32 streams the packed taps of each GEMM (8 KB, hi + lo) through a
+// 6-slot shared-memory ring with cp.async.bulk + mbarriers while thread 0
+// issues the tcgen05.mma's, each stage's tcgen05.commit freeing its slot;
+// at the end all threads read the accumulator back with tcgen05.ld.  Two
+// CTAs per SM overlap one tile's staging/epilogue with the other's GEMMs.
+// Every wait is bounded (about 2 s); a CTA that gives up sets *err, still
+// waits (bounded) for its GEMMs and copies, frees its TMEM and returns.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -51,7 +51,7 @@ namespace brc {
 namespace tc {
 
 constexpr int kThreads = 128;
-constexpr int kRing = 4;
+constexpr int kRing = 6;
 constexpr int kStageHalves = kM * kK;              // BF16 elements of one A (hi or lo)
 constexpr int kStageBytes = 2 * kStageHalves * 2;  // hi + lo
 constexpr uint32_t kTmemCols = 256;
@@ -111,12 +111,14 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity; false after ~2 s.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait for the phase with the given parity; false after limit_ns
+// (default ~2 s).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
+                                          unsigned long long limit_ns = kWaitNs) {
   if (mbar_test(bar, parity)) return true;
   const unsigned long long t0 = global_ns();
   while (!mbar_test(bar, parity))
-    if (global_ns() - t0 > kWaitNs) return false;
+    if (global_ns() - t0 > limit_ns) return false;
   return true;
 }
 
@@ -171,6 +173,7 @@ filter3d_tc_kernel(const float* __restrict__ vol, int W, int H, int D, long long
   uint64_t* empty = full + kRing;
   uint64_t* done = empty + kRing;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  int* flags = reinterpret_cast<int*>(tmem_slot + 1);  // [0] GEMM stages issued, [1] tap stages loaded
 
   if (tid == 0) {
     for (int s = 0; s < kRing; s++) {
@@ -200,19 +203,35 @@ filter3d_tc_kernel(const float* __restrict__ vol, int W, int H, int D, long long
   // as two 16-byte K halves (hi and lo arrays).  Rows past the tile are 0.
   const float* src = vol + (long long)b * vstride;
   const int NQ = g.SP * g.J + 6;
+  // consecutive threads take consecutive rows of one K half: each warp's
+  // 16-byte stores cover 512 contiguous bytes (no bank conflicts)
+  // rows are 16-byte aligned when W is a multiple of 4 (and the volume is):
+  // a window inside the row then takes three aligned float4 loads
+  const bool vec_rows = (W & 3) == 0 && (reinterpret_cast<uintptr_t>(src) & 15) == 0;
+#pragma unroll 2
   for (int item = tid; item < 2 * g.NR; item += kThreads) {
-    const int row = item >> 1, kh = item & 1;
+    const int kh = item >= g.NR ? 1 : 0, row = item - kh * g.NR;
     const int par = row / g.RP, rr = row - par * g.RP;
     const int qq = rr / g.Hp, yl = rr - qq * g.Hp;
     const int q = qq * g.SP + par;
     const int zg = z0 - 3 + q, yg = y0 - 3 + yl;
     const bool rowok = q < NQ && zg >= 0 && zg < D && yg >= 0 && yg < H;
-    const float* rp = src + ((long long)zg * H + yg) * W;
+    const int xs = x0 - 3 + 8 * kh;
     float v[8];
+    if (rowok && vec_rows && xs >= 0 && (xs & ~3) + 12 <= W) {
+      const int a = xs & 3;
+      const float4* p4 = reinterpret_cast<const float4*>(src + ((long long)zg * H + yg) * W + (xs - a));
+      const float4 f0 = __ldg(p4), f1 = __ldg(p4 + 1), f2 = __ldg(p4 + 2);
+      const float w[12] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, f1.z, f1.w, f2.x, f2.y, f2.z, f2.w};
 #pragma unroll
-    for (int e = 0; e < 8; e++) {
-      const int xg = x0 - 3 + 8 * kh + e;
-      v[e] = (rowok && xg >= 0 && xg < W) ? __ldg(rp + xg) : 0.f;
+      for (int e = 0; e < 8; e++) v[e] = a == 0 ? w[e] : (a == 1 ? w[e + 1] : (a == 2 ? w[e + 2] : w[e + 3]));
+    } else {
+      const float* rp = src + ((long long)zg * H + yg) * W;
+#pragma unroll
+      for (int e = 0; e < 8; e++) {
+        const int xg = xs + e;
+        v[e] = (rowok && xg >= 0 && xg < W) ? __ldg(rp + xg) : 0.f;
+      }
     }
     uint32_t ph[4], pl[4];
 #pragma unroll
@@ -233,8 +252,8 @@ filter3d_tc_kernel(const float* __restrict__ vol, int W, int H, int D, long long
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  // GEMMs (one thread).  Stage s = (c+3)*7 + (dy+3).
-  int ok = 1;
+  // Roles: thread 0 issues the GEMMs, thread 32 refills the tap ring.
+  // Stage s = (c+3)*7 + (dy+3) uses ring slot s % kRing.
   if (tid == 0) {
     const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(g.N >> 3) << 17) |
                            ((uint32_t)(kM >> 4) << 24);
@@ -243,10 +262,7 @@ filter3d_tc_kernel(const float* __restrict__ vol, int W, int H, int D, long long
     int s = 0;
     for (; s < nst; s++) {
       const int slot = s % kRing;
-      if (!mbar_wait(&full[slot], (uint32_t)(s / kRing) & 1u)) {
-        ok = 0;
-        break;
-      }
+      if (!mbar_wait(&full[slot], (uint32_t)(s / kRing) & 1u)) break;
       const int cq = s / 7, dyq = s % 7;  // c + 3, dy + 3
       const int par = cq % g.SP, qoff = cq / g.SP;
       const uint32_t brow = (uint32_t)(par * g.RP + qoff * g.Hp + dyq);
@@ -256,27 +272,26 @@ filter3d_tc_kernel(const float* __restrict__ vol, int W, int H, int D, long long
       mma_bf16(tmem, dah, dbh, idesc, s > 0 ? 1u : 0u);
       mma_bf16(tmem, dah, dbl, idesc, 1u);
       mma_bf16(tmem, dal, dbh, idesc, 1u);
-      mma_commit(&empty[slot]);
-      // refill the slot of the previous stage once its GEMMs have completed
-      if (s >= 1 && s - 1 + kRing < nst) {
-        const int ps = s - 1, pslot = ps % kRing;
-        if (!mbar_wait(&empty[pslot], (uint32_t)(ps / kRing) & 1u)) {
-          ok = 0;
-          break;
-        }
-        mbar_expect_tx(&full[pslot], kStageBytes);
-        bulk_load(ring + pslot * kStageBytes, taps + (size_t)(ps + kRing) * (kStageBytes / 2), kStageBytes,
-                  &full[pslot]);
-      }
+      mma_commit(&empty[slot]);  // the slot is free once these GEMMs retire
     }
+    flags[0] = s;  // stages issued
     mma_commit(done);
-    if (!ok) {
-      // bounded drain of the copies still in flight before the CTA exits
-      const int issued = (s >= 1 ? s - 1 : 0) + kRing;
-      for (int t = s; t < issued && t < nst; t++) mbar_wait(&full[t % kRing], (uint32_t)(t / kRing) & 1u);
+  } else if (tid == 32) {
+    int s = kRing;
+    for (; s < nst; s++) {
+      const int slot = s % kRing;
+      if (!mbar_wait(&empty[slot], (uint32_t)(s / kRing - 1) & 1u)) break;
+      mbar_expect_tx(&full[slot], kStageBytes);
+      bulk_load(ring + slot * kStageBytes, taps + (size_t)s * (kStageBytes / 2), kStageBytes, &full[slot]);
     }
+    flags[1] = s < nst ? s : nst;  // stages loaded
   }
-  __syncwarp();
+  __syncthreads();
+  const int issued = flags[0], loaded = flags[1];
+  int ok = issued == nst;
+  // a wait gave up: bounded drain of the tap copies no GEMM consumed
+  if (tid == 32)
+    for (int t = issued; t < loaded; t++) mbar_wait(&full[t % kRing], (uint32_t)(t / kRing) & 1u);
   const int dok = mbar_wait(done, 0) ? 1 : 0;
   tc_fence_after();
 
@@ -317,6 +332,19 @@ filter3d_tc_kernel(const float* __restrict__ vol, int W, int H, int D, long long
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
   if (tid == 0 && (!ok || !dok)) atomicExch(err, 1);
+}
+
+// Self-test of the bounded wait and the error flag: thread 0 waits on an
+// mbarrier that nothing arrives on, gives up after limit_ns and sets *err,
+// as a CTA of filter3d_tc_kernel does when a wait runs out.
+__global__ void bounded_wait_probe_kernel(unsigned long long limit_ns, int* __restrict__ err) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !mbar_wait(&bar, 0, limit_ns)) atomicExch(err, 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -394,7 +422,7 @@ Geometry make_geometry(int nfilt, int H, int D, int Ty) {
   g.RP = ((qmax * g.Hp + 6 + g.N) + 7) / 8 * 8;
   g.NR = g.SP * g.RP;
   g.nstage = num_stages(nfilt);
-  g.smem = kRing * kStageBytes + 2 * 32 * g.NR + (2 * kRing + 1) * 8 + 16;
+  g.smem = kRing * kStageBytes + 2 * 32 * g.NR + (2 * kRing + 1) * 8 + 32;
   return g;
 }
 
@@ -402,27 +430,55 @@ bool geometry_ok(const Geometry& g) {
   return g.Hp <= kMaxN && g.N >= 16 && g.N <= kMaxN && g.smem <= 227 * 1024;
 }
 
-// Tile rows along y: the candidate with the least GEMM work (tiles x N) that
-// fits, ties to the larger tile.
-int pick_ty(int nfilt, int H, int D) {
-  int best = -1;
-  long long best_cost = 0;
+// Cost model of a tile shape: GEMM columns issued over the volume (tiles x
+// (N + 32), the 32 standing for a tile's staging and epilogue), x1.3 when
+// the tile leaves no room for a second CTA on the SM.
+static long long tile_cost(const Geometry& g, int H, int D) {
+  const long long ny = (H + g.Ty - 1) / g.Ty;
+  const long long nz = (D + g.SP * g.J - 1) / (g.SP * g.J);
+  long long cost = ny * nz * (g.N + 32);
+  if (g.smem > 113 * 1024) cost = cost * 13 / 10;
+  return cost;
+}
+
+int candidate_tys(int nfilt, int H, int D, int* tys, int max_n) {
+  // the cheapest tile height for each plane-group count J (ties to the
+  // taller tile), then the max_n cheapest of those
+  long long best_cost[kMaxN + 1];
+  int best_ty[kMaxN + 1];
+  for (int j = 0; j <= kMaxN; j++) best_ty[j] = -1;
   const int lo = H < 10 ? H : 10;
   const int hi = H < kMaxN - 6 ? H : kMaxN - 6;
-  for (int ty = lo; ty <= hi; ty++) {
+  for (int ty = hi; ty >= lo; ty--) {
     const Geometry g = make_geometry(nfilt, H, D, ty);
     if (!geometry_ok(g)) continue;
-    const long long ny = (H + g.Ty - 1) / g.Ty;
-    const long long nz = (D + g.SP * g.J - 1) / (g.SP * g.J);
-    long long cost = ny * nz * (g.N + 32);
-    // one CTA per SM leaves no second tile to overlap staging and epilogue
-    if (g.smem > 113 * 1024) cost = cost * 13 / 10;
-    if (best < 0 || cost < best_cost || (cost == best_cost && ty > best)) {
-      best = g.Ty;
-      best_cost = cost;
+    const long long c = tile_cost(g, H, D);
+    if (best_ty[g.J] < 0 || c < best_cost[g.J]) {
+      best_ty[g.J] = g.Ty;
+      best_cost[g.J] = c;
     }
   }
-  return best;
+  int n = 0;
+  for (; n < max_n; n++) {
+    int pick = -1;
+    for (int j = 1; j <= kMaxN; j++)
+      if (best_ty[j] >= 0 && (pick < 0 || best_cost[j] < best_cost[pick])) pick = j;
+    if (pick < 0) break;
+    tys[n] = best_ty[pick];
+    best_ty[pick] = -1;
+  }
+  return n;
+}
+
+int pick_ty(int nfilt, int H, int D) {
+  int ty = -1;
+  return candidate_tys(nfilt, H, D, &ty, 1) == 1 ? ty : -1;
+}
+
+cudaError_t bounded_wait_probe(int wait_ms, int* d_err, cudaStream_t st) {
+  if (wait_ms < 1 || wait_ms > 1000) return cudaErrorInvalidValue;
+  bounded_wait_probe_kernel<<<1, 32, 0, st>>>((unsigned long long)wait_ms * 1000000ull, d_err);
+  return cudaGetLastError();
 }
 
 cudaError_t init() {

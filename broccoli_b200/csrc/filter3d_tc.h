@@ -35,8 +35,13 @@ size_t packed_tap_bytes(int nfilt);
 void pack_taps(const float* h_filters, int nfilt, uint16_t* dst);
 Geometry make_geometry(int nfilt, int H, int D, int Ty);
 bool geometry_ok(const Geometry& g);
+// The max_n cheapest tile heights by the cost model, cheapest first; returns
+// how many were found.  pick_ty is the cheapest.
+int candidate_tys(int nfilt, int H, int D, int* tys, int max_n);
 int pick_ty(int nfilt, int H, int D);
 cudaError_t init();
+// One CTA waits wait_ms (1..1000) on a barrier nothing completes, then sets *d_err.
+cudaError_t bounded_wait_probe(int wait_ms, int* d_err, cudaStream_t st);
 cudaError_t launch(const float* vol, int W, int H, int D, int batch, long long stride, const uint16_t* d_taps,
                    int nfilt, float* out, const int* conv_iter, int it, int* d_err, const Geometry& g,
                    cudaStream_t st);

@@ -32,6 +32,7 @@ cudaError_t rescale_linear(const float* src, int W, int H, int D, float* out, in
 cudaError_t smooth3d(const float* vol, int W, int H, int D, int batch, const float* fx,
                      const float* fy, const float* fz, const float* cert, const float* scert,
                      float* tmp1, float* tmp2, float* out, cudaStream_t st, int accumulate = 0);
+cudaError_t multiply_mask(float* vols, const float* mask, long long V, int batch, cudaStream_t st);
 // nonlinear.cu
 cudaError_t tensor_norm_max(const float* t6, long long V, float* a11, unsigned int* maxbits,
                             cudaStream_t st);

@@ -25,19 +25,18 @@ constexpr int kNEThreads = 256;
 // Largest volume the 32-bit voxel indexing of the resampling kernels takes.
 constexpr long long kMaxVoxels = 0x7fffff00LL;
 
-// Phase difference and certainty of one response pair, in the reference's
-// operation order (CalculatePhaseDifferencesAndCertainties,
-// kernelRegistration.cpp:173-211).
+// Phase difference and certainty of one response pair
+// (CalculatePhaseDifferencesAndCertainties, kernelRegistration.cpp:173-211):
+// dphi = arg(q1 q2*), c = |q1 q2| cos^2(dphi/2).  With cos^2(t/2) =
+// (1 + cos t)/2 and cos dphi = Re(q1 q2*)/|q1 q2*|, c = (|q1 q2*| + Re(q1 q2*))/2:
+// the same value without the cosine (|q1 q2| = |q1 q2*|).
 __device__ __forceinline__ void phase_diff_cert(float2 a, float2 c, float& pd, float& cert) {
   // products rounded separately (no FMA contraction), as in the reference's
   // arithmetic: identical responses then give exactly zero phase difference
-  float re = __fadd_rn(__fmul_rn(a.x, c.x), __fmul_rn(a.y, c.y));
-  float im = __fsub_rn(__fmul_rn(a.y, c.x), __fmul_rn(a.x, c.y));
+  const float re = __fadd_rn(__fmul_rn(a.x, c.x), __fmul_rn(a.y, c.y));
+  const float im = __fsub_rn(__fmul_rn(a.y, c.x), __fmul_rn(a.x, c.y));
   pd = atan2f(im, re);
-  re = a.x * c.x - a.y * c.y;
-  im = a.y * c.x + a.x * c.y;
-  const float cs = cosf(pd * 0.5f);
-  cert = sqrtf(re * re + im * im) * cs * cs;
+  cert = 0.5f * (sqrtf(re * re + im * im) + re);
 }
 
 // Phase gradient from the neighbours along one axis
@@ -183,25 +182,50 @@ normal_eq_partial_kernel(const float2* __restrict__ q1, long long q1_stride,
     for (int k = 0; k < 3; k++)
 #pragma unroll
       for (int q = 0; q < 5; q++) m[k][q] = 0.f;
-    for (int x = 3 + lane; x < W - 3; x += 32) {
-      const long long i = row + x;
+    // all lanes run every chunk (shuffles need the full warp); lanes past
+    // the interior load their clamped centre for their neighbours' use and
+    // add nothing
+    for (int xb = 3; xb < W - 3; xb += 32) {
+      const int x = xb + lane;
+      const bool act = x < W - 3;
+      const long long i = row + (x < W ? x : W - 1);
       const float xf = (float)x - cxf;
 #pragma unroll
       for (int k = 0; k < 3; k++) {
         const float2* A = Q1 + k * V;
         const float2* C = Q2 + k * V;
-        const long long s = k == 0 ? 1 : (k == 1 ? (long long)W : WH);
         const float2 a = __ldg(A + i), c = __ldg(C + i);
+        float2 ap, am, cp, cm;
+        if (k == 0) {
+          // x neighbours from the adjacent lanes; the warp's end lanes load
+          ap = make_float2(__shfl_down_sync(0xffffffffu, a.x, 1), __shfl_down_sync(0xffffffffu, a.y, 1));
+          cp = make_float2(__shfl_down_sync(0xffffffffu, c.x, 1), __shfl_down_sync(0xffffffffu, c.y, 1));
+          am = make_float2(__shfl_up_sync(0xffffffffu, a.x, 1), __shfl_up_sync(0xffffffffu, a.y, 1));
+          cm = make_float2(__shfl_up_sync(0xffffffffu, c.x, 1), __shfl_up_sync(0xffffffffu, c.y, 1));
+          if (lane == 31 && act) {
+            ap = __ldg(A + i + 1);
+            cp = __ldg(C + i + 1);
+          }
+          if (lane == 0) {
+            am = __ldg(A + i - 1);
+            cm = __ldg(C + i - 1);
+          }
+        } else {
+          const long long st = k == 1 ? (long long)W : WH;
+          ap = act ? __ldg(A + i + st) : a;
+          am = act ? __ldg(A + i - st) : a;
+          cp = act ? __ldg(C + i + st) : c;
+          cm = act ? __ldg(C + i - st) : c;
+        }
         float pd, cert;
         phase_diff_cert(a, c, pd, cert);
         if (cert_in != nullptr) {
           // z pass of the separable smoothing over the x/y-smoothed certainties
           const float* cz = cert_in + ((long long)b * 3 + k) * V + i;
-          cert = cw1 * __ldg(cz - WH) + cw0 * __ldg(cz) + cw1 * __ldg(cz + WH);
+          cert = act ? cw1 * __ldg(cz - WH) + cw0 * __ldg(cz) + cw1 * __ldg(cz + WH) : 0.f;
         }
-        const float g = phase_grad(__ldg(A + i + s), a, __ldg(A + i - s), __ldg(C + i + s), c,
-                                   __ldg(C + i - s));
-        const float cg = cert * g;
+        const float g = phase_grad(ap, a, am, cp, c, cm);
+        const float cg = act ? cert * g : 0.f;
         const float w = cg * g;
         const float v = cg * pd;
         m[k][0] += w;
@@ -790,6 +814,21 @@ cudaError_t rescale_linear(const float* src, int W, int H, int D, float* out, in
   const float vz = (float)(D - 1) / (float)(D2 - 1);
   rescale_linear_kernel<<<(unsigned)((V2 + 255) / 256), 256, 0, st>>>(src, W, H, D, out, W2, H2, D2,
                                                                      vx, vy, vz);
+  return cudaGetLastError();
+}
+
+// vols[b][i] *= mask[i] for every volume b (MultiplyVolumes,
+// kernelMisc.cpp, as PerformSmoothingNormalized ends, broccoli_lib.cpp:11359-11450).
+__global__ void __launch_bounds__(256)
+multiply_mask_kernel(float* __restrict__ vols, const float* __restrict__ mask, long long V) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V) return;
+  vols[(long long)blockIdx.y * V + i] *= __ldg(mask + i);
+}
+
+cudaError_t multiply_mask(float* vols, const float* mask, long long V, int batch, cudaStream_t st) {
+  dim3 grid((unsigned)((V + 255) / 256), batch);
+  multiply_mask_kernel<<<grid, 256, 0, st>>>(vols, mask, V);
   return cudaGetLastError();
 }
 

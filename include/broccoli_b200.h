@@ -161,6 +161,17 @@ int brc_smooth3d(brc_ctx* ctx, const float* d_vol, int W, int H, int D, int batc
                  const float* h_fx, const float* h_fy, const float* h_fz,
                  const float* d_cert, const float* d_smoothed_cert, float* d_out);
 
+/* Normalised-convolution smoothing of T volumes with one certainty
+ * (mask) volume: the mask is smoothed (all-ones certainty), every volume is
+ * smoothed with the mask as certainty and divided by the smoothed mask along
+ * the last pass, and the results are multiplied by the mask.  As in the
+ * reference the division is unguarded: voxels where the smoothed mask is
+ * exactly 0 come out NaN.  Filters are host arrays of 9 taps.  Replaces
+ * PerformSmoothingNormalizedWrapper (broccoli_lib.cpp:11227-11272) with
+ * PerformSmoothingNormalized (:11359-11450). */
+int brc_smooth_normalized(brc_ctx* ctx, const float* d_vols, int W, int H, int D, int T, const float* d_mask,
+                          const float* h_fx, const float* h_fy, const float* h_fz, float* d_out);
+
 /* Linear resample to a new grid size, sample spacing (N-1)/(N'-1).
  * Replaces ChangeVolumeSize (broccoli_lib.cpp:6247-6388) with
  * RescaleVolumeLinear (kernelRegistration.cpp:1340-1366). */
@@ -295,6 +306,14 @@ int brc_warp_affine_backward(brc_ctx* ctx, const float* d_src, int W, int H, int
 int brc_warp_field_backward(brc_ctx* ctx, const float* d_src, int W, int H, int D, const float* d_dx,
                             const float* d_dy, const float* d_dz, const float* d_grad_out,
                             float* d_grad_field, float* d_grad_src);
+
+/* Self-test of the failure path of the tensor-core kernels.  No counterpart
+ * in the reference.  Launches one CTA that waits wait_ms (1..1000) on a
+ * barrier nothing completes and then sets the context's device flag, the
+ * way a CTA of the BF16X3 filtering reports a wait that ran out; the next
+ * brc_ctx_synchronize returns BRC_ERR_TIMEOUT and clears the flag, and the
+ * context stays usable. */
+int brc_selftest_bounded_wait(brc_ctx* ctx, int wait_ms);
 
 /* ---- device memory and host copies (for hosts without a CUDA runtime) --- */
 

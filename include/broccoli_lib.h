@@ -136,6 +136,9 @@ class BROCCOLI_LIB {
   void SetSmoothingFilters(float* fx, float* fy, float* fz);
   void SetSmoothingType(int type);
   void SetEPISmoothingAmount(float fwhm_mm);
+  void SetEPIMask(float* mask);  // certainty of PerformSmoothingNormalizedWrapper
+  void SetInputCertainty(float* certainty);  // certainty of PerformSmoothingNormalizedHostWrapper
+  void SetAutoMask(bool automask);  // true is not supported (EPI segmentation is not built)
 
   // extensions of this implementation
   void SetPrecision(int precision);             // BRC_PREC_FP32 / BRC_PREC_BF16X3
@@ -157,6 +160,8 @@ class BROCCOLI_LIB {
   void PerformMotionCorrectionWrapper();
   void PerformRegistrationTwoVolumesWrapper();
   void PerformSmoothingWrapper();
+  void PerformSmoothingNormalizedWrapper();
+  void PerformSmoothingNormalizedHostWrapper();  // smooths the fMRI volumes in place
 
   int GetLastStatus() const { return last_status_; }
 
@@ -174,6 +179,7 @@ class BROCCOLI_LIB {
   size_t mni_w_ = 0, mni_h_ = 0, mni_d_ = 0;
   float epi_vox_[3] = {1, 1, 1}, t1_vox_[3] = {1, 1, 1}, mni_vox_[3] = {1, 1, 1};
 
+  void smooth_normalized(const float* h_mask, float* h_out, const char* where);
   float* h_fmri_ = nullptr;
   float* h_epi_ = nullptr;
   float* h_t1_ = nullptr;
@@ -205,6 +211,9 @@ class BROCCOLI_LIB {
   float* out_interpolated_ = nullptr;
   float* out_field_[3] = {nullptr};
   float* out_smoothed_ = nullptr;
+  float* h_epi_mask_ = nullptr;
+  float* h_certainty_ = nullptr;
+  bool auto_mask_ = false;
   cl_float2* out_q_[3] = {nullptr};
 
   bool check(int status, const char* where);

@@ -214,6 +214,20 @@ def smoothing_filter_sigma(sigma: float, size: int = 9, prec: str = "f32") -> np
     return f
 
 
+def smooth_normalized(vols: np.ndarray, mask: np.ndarray, fx, fy, fz, prec: str = "f32") -> np.ndarray:
+    """Normalised-convolution smoothing of a (T,D,H,W) series with one
+    certainty volume (PerformSmoothingNormalizedWrapper,
+    broccoli_lib.cpp:11227-11272; PerformSmoothingNormalized, :11359-11450):
+    smoothed mask = smoothing of the mask; each volume is smoothed with the
+    mask as certainty, divided by the smoothed mask in the last pass (no
+    guard: 0/0 gives NaN), then multiplied by the mask."""
+    sm = smooth3d(mask, fx, fy, fz, prec=prec)
+    dt, _ = _dt(prec)
+    m = _arr(mask, dt)
+    with np.errstate(invalid="ignore"):
+        return np.stack([smooth3d(v, fx, fy, fz, mask, sm, prec=prec) * m for v in vols])
+
+
 def smooth3d(vol: np.ndarray, fx, fy, fz, cert=None, smoothed_cert=None, prec: str = "f32"):
     dt, s = _dt(prec)
     D, H, W = vol.shape
@@ -410,6 +424,16 @@ def ref_motion_correct(vols: np.ndarray, voxel_size, filters: np.ndarray, niter:
     m = np.zeros(6 * T, np.float32)
     ref_lib().ref_motion_correct(_ptr(v), W, H, D, T, _ptr(vs), _ptr(f), niter, _ptr(m))
     return v, m.reshape(6, T)
+
+
+def ref_smooth_normalized(vols: np.ndarray, mask: np.ndarray, fx, fy, fz) -> np.ndarray:
+    """PerformSmoothingNormalizedWrapper (broccoli_lib.cpp:11227-11272) on
+    the reference's own kernels: the smoothed mask, then every volume
+    smoothed with the mask as certainty over the smoothed mask, times the
+    mask (PerformSmoothingNormalized, :11359-11450)."""
+    sm = ref_smooth3d(mask, fx, fy, fz)
+    with np.errstate(invalid="ignore"):
+        return np.stack([ref_smooth3d(v, fx, fy, fz, mask, sm) * np.asarray(mask, np.float32) for v in vols])
 
 
 def ref_smooth3d(vol: np.ndarray, fx, fy, fz, cert=None, smoothed_cert=None):

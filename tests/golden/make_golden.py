@@ -128,5 +128,24 @@ def main() -> None:
     print("wrote", os.path.join(HERE, "golden_small.npz"), "with", len(g), "arrays")
 
 
+def main_smooth_normalized() -> None:
+    """Normalised-convolution smoothing of a short series with a binary
+    ellipsoid mask (PerformSmoothingNormalizedWrapper) on the reference's
+    kernels; the corners lie more than 4 voxels from the mask, where the
+    reference's unguarded division leaves NaN."""
+    shape = (16, 18, 20)
+    rng = np.random.Generator(np.random.PCG64(11))
+    vols = (rng.standard_normal((3,) + shape) * 10 + 100).astype(np.float32)
+    z, y, x = np.meshgrid(*[np.arange(n) for n in shape], indexing="ij")
+    c = [(n - 1) / 2.0 for n in shape]
+    r = ((z - c[0]) / 5.0) ** 2 + ((y - c[1]) / 6.0) ** 2 + ((x - c[2]) / 6.5) ** 2
+    mask = (r <= 1.0).astype(np.float32)
+    fs = O.smoothing_filter_sigma(1.5)
+    out = O.ref_smooth_normalized(vols, mask, fs, fs, fs)
+    np.savez_compressed(os.path.join(HERE, "smooth_normalized.npz"), vols=vols, mask=mask, filter=fs, out=out)
+    print("wrote smooth_normalized.npz; NaN voxels per volume:", int(np.isnan(out[0]).sum()))
+
+
 if __name__ == "__main__":
     main()
+    main_smooth_normalized()

@@ -58,3 +58,40 @@ def test_class_motion_correction_matches_golden(tmp_path, golden, lin_filters):
     tr = np.abs(motion[:3] - gm[:3]).max() / max(1.0, np.abs(gm[:3]).max())
     assert tr < 1e-4 * max(vs)
     np.testing.assert_allclose(motion[3:], gm[3:], atol=2e-3)
+
+
+SMOOTH_SRC = os.path.join(ROOT, "tests", "cpp", "broccoli_lib_smooth.cpp")
+
+
+def build_smoothing_program(out_dir):
+    exe = os.path.join(out_dir, "broccoli_lib_smooth")
+    libdir = os.path.join(ROOT, "broccoli_b200")
+    subprocess.check_call(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), SMOOTH_SRC, "-L",
+                           libdir, "-lbroccoli_b200", f"-Wl,-rpath,{libdir}", "-o", exe])
+    return exe
+
+
+def test_smoothing_program_builds(tmp_path):
+    assert os.path.exists(build_smoothing_program(str(tmp_path)))
+
+
+@pytest.mark.gpu
+def test_class_normalized_smoothing_matches_golden(tmp_path):
+    """The Smoothing CLI's calls (PerformSmoothingNormalizedHostWrapper, FWHM
+    from the fixture's sigma at 3 mm voxels) against the reference kernels'
+    output: same NaN voxels, the rest within 1e-4 of the largest value."""
+    g = np.load(os.path.join(ROOT, "tests", "golden", "smooth_normalized.npz"))
+    vols, mask, ref = g["vols"], g["mask"], g["out"]
+    T, D, H, W = vols.shape
+    exe = build_smoothing_program(str(tmp_path))
+    p_in, p_c, p_out = tmp_path / "vols.f32", tmp_path / "cert.f32", tmp_path / "out.f32"
+    np.ascontiguousarray(vols, np.float32).tofile(p_in)
+    np.ascontiguousarray(mask, np.float32).tofile(p_c)
+    fwhm = 1.5 * 2.354 * 3.0  # sigma 1.5 voxels at 3 mm
+    r = subprocess.run([exe, str(p_in), str(p_c), str(W), str(H), str(D), str(T), "3", "3", "3", repr(fwhm),
+                        str(p_out)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = np.fromfile(p_out, np.float32).reshape(vols.shape)
+    assert np.array_equal(np.isnan(got), np.isnan(ref))
+    fin = np.isfinite(ref)
+    assert np.abs(got[fin] - ref[fin]).max() <= 1e-4 * np.abs(ref[fin]).max()

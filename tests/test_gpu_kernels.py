@@ -128,3 +128,16 @@ def test_smoothing_matches_golden(ctx, golden):
 def test_rescale_matches_golden(ctx, golden):
     out = ctx.rescale_linear(cuda(golden["moved"]), (11, 13, 17)).cpu().numpy()
     assert rel_err(out, golden["rescale"]) < TOL
+
+
+def test_smooth_normalized_matches_golden(ctx):
+    """brc_smooth_normalized against the reference kernels' output: the same
+    NaN voxels, the rest within 1e-4 of the largest value."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "smooth_normalized.npz"))
+    fs = g["filter"]
+    out = ctx.smooth_normalized(cuda(g["vols"]), cuda(g["mask"]), fs, fs, fs).cpu().numpy()
+    ref = g["out"]
+    assert np.array_equal(np.isnan(out), np.isnan(ref))
+    fin = np.isfinite(ref)
+    assert np.abs(out[fin] - ref[fin]).max() <= TOL * np.abs(ref[fin]).max()

@@ -93,3 +93,19 @@ def test_tc_nonlinear_close_to_fp32(ctx, bank):
     ctx.synchronize()
     d = np.abs(f.cpu().numpy() - f32.cpu().numpy()).max()
     assert d <= 0.02
+
+
+def test_bounded_wait_reports_timeout_and_context_survives(ctx, orc, lin_filters):
+    """A device-side wait that runs out (a barrier nothing completes) sets
+    the context's flag; synchronize() reports BRC_ERR_TIMEOUT once, then the
+    context keeps working."""
+    ctx.synchronize()
+    ctx.selftest_bounded_wait(50)
+    with pytest.raises(L.BrcError) as e:
+        ctx.synchronize()
+    assert e.value.status == L.BRC_ERR_TIMEOUT
+    ctx.synchronize()  # flag cleared
+    vol = np.random.default_rng(3).standard_normal((9, 12, 15)).astype(np.float32)
+    got = ctx.filter3d(cuda(vol), lin_filters, precision=L.PREC_BF16X3).cpu().numpy()[0]
+    ctx.synchronize()
+    assert rel_err(got, orc.filter3d(vol, lin_filters, prec="f64")) < FTOL

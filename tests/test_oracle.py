@@ -149,3 +149,16 @@ def test_register_two_volumes_exact(orc, golden, bank):
     crs = orc.change_resolution_and_size(golden["r2v_subject"], golden["r2v_voxel"],
                                          golden["r2v_template"].shape, (1.0, 1.0, 1.0), 3)
     assert np.array_equal(crs, golden["r2v_crs"])
+
+
+def test_smooth_normalized_matches_reference_kernels():
+    """Normalised-convolution smoothing (PerformSmoothingNormalizedWrapper):
+    the FP32 restatement equals the reference's kernels bit for bit,
+    including the NaN voxels of the unguarded division."""
+    import os
+    import oracle as O
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "smooth_normalized.npz"))
+    fs = g["filter"]
+    out = O.smooth_normalized(g["vols"], g["mask"], fs, fs, fs)
+    assert np.array_equal(out, g["out"], equal_nan=True)
+    assert np.isnan(out).any() and np.isfinite(out[:, 8, 9, 10]).all()

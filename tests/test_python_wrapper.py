@@ -52,3 +52,34 @@ def test_perform_motion_correction_matches_golden(golden, lin_filters):
     # undo unpackOutputVolume (transpose back, flip the second axis back)
     back = np.fliplr(corrected.transpose(3, 2, 0, 1))
     assert rel_err(back, golden["mc_corrected"]) < 1e-4
+
+
+def test_fwhm_filters_match_oracle():
+    """CreateSmoothingFilters from a FWHM: the wrapper's taps equal the
+    oracle's restatement bit for bit."""
+    import oracle as O
+    vox = (3.0, 3.0, 3.5)
+    fx, fy, fz = BL.fwhm_filters(6.0, vox)
+    for f, v in zip((fx, fy, fz), vox):
+        assert np.array_equal(f, O.smoothing_filter_sigma(6.0 / 2.354 / v))
+
+
+@pytest.mark.gpu
+def test_perform_smoothing_normalized_matches_golden():
+    """PerformSmoothingNormalizedWrapper through the wrapper class (RANDOM
+    filters = the fixture's taps) against the reference kernels' output."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "smooth_normalized.npz"))
+    vols, mask, fs, ref = g["vols"], g["mask"], g["filter"], g["out"]
+    B = BL.BROCCOLI_LIB(0, 0)
+    B.SetfMRIData(to_wrapper_layout(vols), (3.0, 3.0, 3.0))
+    B.SetEPIMask(B.packVolume(to_wrapper_layout(mask)))
+    B.SetSmoothingType(BL.RANDOM)
+    B.SetSmoothingFilters(fs, fs, fs)
+    out = B.createOutputArray(to_wrapper_layout(vols).shape)
+    B.SetOutputSmoothedfMRIVolumes(out)
+    B.PerformSmoothingNormalizedWrapper()
+    got = out.reshape(vols.shape)
+    assert np.array_equal(np.isnan(got), np.isnan(ref))
+    fin = np.isfinite(ref)
+    assert np.abs(got[fin] - ref[fin]).max() <= 1e-4 * np.abs(ref[fin]).max()
