@@ -311,20 +311,49 @@ filter3d_tc_kernel(const float* __restrict__ vol, int W, int H, int D, long long
     xo = r - f * kXo;
     rvalid = r < 2 * nfilt * kXo;
   }
-  const int x = x0 + xo;
-  rvalid = rvalid && x < W && ok && dok;
-  float* ob = out + ((long long)b * nfilt + (f >> 1)) * 2 * V + (f & 1);
-  for (int c0 = 0; c0 < g.N; c0 += 16) {
-    uint32_t v[16];
-    tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+  rvalid = rvalid && ok && dok;
+  // The accumulator is transposed through the shared memory the GEMMs no
+  // longer need (tap ring + input tile): element (column n, plane s, filter
+  // k, x offset xo, re/im) at E[((n - cbase) * SP + s) * 20 nfilt + 20 k +
+  // 2 xo + ri], so each output row (z, y) of a filter is 80 contiguous
+  // bytes (10 complex samples), written with 16-byte stores.
+  float* E = reinterpret_cast<float*>(smem);
+  const int rowf = 20 * nfilt;  // floats per (column, plane) row
+  const uint32_t avail = (uint32_t)(kRing * kStageBytes) + 2u * hl_bytes;
+  int C = (int)(avail / (uint32_t)(4 * rowf * g.SP)) / 16 * 16;
+  if (C > g.N) C = g.N;
+  const int ke = (f >> 1) * 20 + xo * 2 + (f & 1);
+  const bool vec16 = ((W & 1) == 0) && ((V & 1) == 0) && ((reinterpret_cast<uintptr_t>(out) & 15) == 0);
+  for (int cbase = 0; cbase < g.N; cbase += C) {
+    const int cend = cbase + C < g.N ? cbase + C : g.N;
+    for (int c0 = cbase; c0 < cend; c0 += 16) {
+      uint32_t v[16];
+      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+      if (rvalid) {
 #pragma unroll
-    for (int e = 0; e < 16; e++) {
-      const int n = c0 + e;
-      const int j = n / g.Hp, yl = n - j * g.Hp;
-      const int z = z0 + j * g.SP + sp, y = y0 + yl;
-      if (rvalid && j < g.J && yl < g.Ty && y < H && z < D)
-        ob[2 * (((long long)z * H + y) * W + x)] = __uint_as_float(v[e]);
+        for (int e = 0; e < 16; e++) E[((c0 + e - cbase) * g.SP + sp) * rowf + ke] = __uint_as_float(v[e]);
+      }
     }
+    __syncthreads();
+    const int segs = (cend - cbase) * g.SP * nfilt;
+    for (int item = tid; item < segs * 5; item += kThreads) {
+      const int seg = item / 5, part = item - seg * 5;
+      const int nl = seg / (g.SP * nfilt), rem = seg - nl * (g.SP * nfilt);
+      const int s2 = rem / nfilt, k = rem - s2 * nfilt;
+      const int n = cbase + nl;
+      const int j = n / g.Hp, yl = n - j * g.Hp;
+      const int z = z0 + j * g.SP + s2, y = y0 + yl, xs = x0 + 2 * part;
+      if (j >= g.J || yl >= g.Ty || y >= H || z >= D || xs >= W) continue;
+      const float4 q = *reinterpret_cast<const float4*>(E + (nl * g.SP + s2) * rowf + k * 20 + part * 4);
+      float* dst = out + (((long long)b * nfilt + k) * V + ((long long)z * H + y) * W + xs) * 2;
+      if (xs + 1 < W && vec16) {
+        *reinterpret_cast<float4*>(dst) = q;
+      } else {
+        *reinterpret_cast<float2*>(dst) = make_float2(q.x, q.y);
+        if (xs + 1 < W) *reinterpret_cast<float2*>(dst + 2) = make_float2(q.z, q.w);
+      }
+    }
+    __syncthreads();
   }
 
   tc_fence_before();
