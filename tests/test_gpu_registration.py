@@ -81,6 +81,25 @@ def test_motion_correction_matches_golden(ctx, golden, lin_filters):
     assert rel_err(corr, golden["mc_corrected"]) < TOL
 
 
+@pytest.mark.parametrize("prec", [L.PREC_FP32, L.PREC_BF16X3])
+def test_chunked_host_motion_correction_equals_device_batch(ctx, lin_filters, prec):
+    """A 70-volume series goes through brc_motion_correct in two chunks with
+    overlapped copies; every volume's parameters and corrected volume equal
+    those of the device-resident batch of all 69 registrations (the
+    instances are independent, so the split does not change any result)."""
+    vols, _ = S.motion_series(T=70, shape=(13, 18, 20), snr=50.0)
+    vs = np.array([3.0, 3.0, 3.5], np.float32)
+    corr, motion = ctx.motion_correct(vols, vs, lin_filters, 8, tolerance=1e-3, precision=prec,
+                                      certainty_sigma=1.0)
+    r = ctx.register_linear(cuda(vols[0]), cuda(vols[1:]), lin_filters, 8, L.RIGID, tolerance=1e-3,
+                            precision=prec, certainty_sigma=1.0)
+    p = r["params"].cpu().numpy()
+    assert np.array_equal(motion[:3, 1:].T, p[:, :3] * vs)
+    assert np.array_equal(motion[3:, 1:].T, r["rotations"].cpu().numpy())
+    assert np.array_equal(corr[1:], r["aligned"].cpu().numpy())
+    assert np.array_equal(corr[0], vols[0])
+
+
 def test_early_exit_stops_converged_instances(ctx, lin_filters):
     vols, _ = S.motion_series(T=6, shape=(17, 32, 32), snr=50.0)
     full = ctx.register_linear(cuda(vols[0]), cuda(vols[1:]), lin_filters, 30, L.RIGID)
