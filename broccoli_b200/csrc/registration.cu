@@ -60,50 +60,82 @@ __device__ __forceinline__ float phase_grad(float2 a_p, float2 a_c, float2 a_m, 
 // the separable 3x3x3 certainty smoothing, in the order x, y, z.  Computed
 // where the z pass of the interior voxels reads them: planes 2..D-3, rows
 // and columns 3..N-4 (their x/y neighbours 2..N-3 are inside the volume).
-// One CTA: a 32x8 patch of one plane of one instance; the certainties of
-// the patch and its 1-voxel halo are staged in shared memory.
-constexpr int kCxyTX = 32, kCxyTY = 8;
+// One CTA: a 32x8 patch of one instance through all those planes; the
+// certainties of the patch and its 1-voxel halo are staged in shared
+// memory, and each thread holds the responses of its (at most two) halo
+// cells for the next plane in registers while the current one is smoothed,
+// so every plane's loads overlap the previous plane's work.
+constexpr int kCxyTX = 32, kCxyTY = 8, kCxyCells = (kCxyTX + 2) * (kCxyTY + 2);
 
 __global__ void __launch_bounds__(256)
 cert_xy_kernel(const float2* __restrict__ q1, long long q1_stride, const float2* __restrict__ q2, int W, int H,
                int D, int ntx, float* __restrict__ cxy, const int* __restrict__ conv_iter, int it, float w0,
                float w1) {
-  const int b = blockIdx.z;
+  const int b = blockIdx.y;
   if (instance_done(conv_iter, b, it)) return;
   __shared__ float c[3][kCxyTY + 2][kCxyTX + 2];
   __shared__ float sx[3][kCxyTY + 2][kCxyTX];
   const long long V = (long long)W * H * D;
-  const int z = 2 + blockIdx.y;
+  const long long WH = (long long)W * H;
   const int tx0 = 3 + (blockIdx.x % ntx) * kCxyTX, ty0 = 3 + (blockIdx.x / ntx) * kCxyTY;
   const float2* Q1 = q1 + (long long)b * q1_stride;
   const float2* Q2 = q2 + (long long)b * 3 * V;
-  const long long zoff = (long long)z * W * H;
-  for (int idx = threadIdx.x; idx < (kCxyTY + 2) * (kCxyTX + 2); idx += blockDim.x) {
-    const int ly = idx / (kCxyTX + 2), lx = idx - ly * (kCxyTX + 2);
+  // the (at most two) halo cells of this thread
+  int cell[2];
+  bool in[2];
+  long long off[2];
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    cell[h] = threadIdx.x + h * 256;
+    const int ly = cell[h] / (kCxyTX + 2), lx = cell[h] - ly * (kCxyTX + 2);
     const int x = tx0 - 1 + lx, y = ty0 - 1 + ly;
-    const bool in = x <= W - 3 && y <= H - 3;
-    const long long i = zoff + (long long)y * W + x;
+    in[h] = cell[h] < kCxyCells && x <= W - 3 && y <= H - 3;
+    off[h] = (long long)y * W + x;
+  }
+  float2 qa[2][3], qc[2][3];
+  auto load_plane = [&](int z) {
 #pragma unroll
-    for (int k = 0; k < 3; k++) {
-      float pd, cv = 0.f;
-      if (in) phase_diff_cert(__ldg(Q1 + k * V + i), __ldg(Q2 + k * V + i), pd, cv);
-      c[k][ly][lx] = cv;
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+        if (in[h]) {
+          const long long i = (long long)z * WH + off[h];
+          qa[h][k] = __ldg(Q1 + k * V + i);
+          qc[h][k] = __ldg(Q2 + k * V + i);
+        }
+  };
+  load_plane(2);
+  for (int z = 2; z <= D - 3; z++) {
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      if (cell[h] >= kCxyCells) continue;
+      const int ly = cell[h] / (kCxyTX + 2), lx = cell[h] - ly * (kCxyTX + 2);
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        float pd, cv = 0.f;
+        if (in[h]) phase_diff_cert(qa[h][k], qc[h][k], pd, cv);
+        c[k][ly][lx] = cv;
+      }
     }
-  }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < (kCxyTY + 2) * kCxyTX; idx += blockDim.x) {
-    const int ly = idx / kCxyTX, lx = idx - ly * kCxyTX;
+    if (z < D - 3) load_plane(z + 1);  // in flight during the smoothing below
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < (kCxyTY + 2) * kCxyTX; idx += blockDim.x) {
+      const int ly = idx / kCxyTX, lx = idx - ly * kCxyTX;
 #pragma unroll
-    for (int k = 0; k < 3; k++) sx[k][ly][lx] = w1 * c[k][ly][lx] + w0 * c[k][ly][lx + 1] + w1 * c[k][ly][lx + 2];
-  }
-  __syncthreads();
-  const int ly = threadIdx.x / kCxyTX, lx = threadIdx.x - ly * kCxyTX;
-  const int x = tx0 + lx, y = ty0 + ly;
-  if (ly < kCxyTY && x < W - 3 && y < H - 3) {
-    const long long i = zoff + (long long)y * W + x;
+      for (int k = 0; k < 3; k++) sx[k][ly][lx] = w1 * c[k][ly][lx] + w0 * c[k][ly][lx + 1] + w1 * c[k][ly][lx + 2];
+    }
+    __syncthreads();
+    const int ly = threadIdx.x / kCxyTX, lx = threadIdx.x - ly * kCxyTX;
+    const int x = tx0 + lx, y = ty0 + ly;
+    if (ly < kCxyTY && x < W - 3 && y < H - 3) {
+      const long long i = (long long)z * WH + (long long)y * W + x;
 #pragma unroll
-    for (int k = 0; k < 3; k++)
-      cxy[((long long)b * 3 + k) * V + i] = w1 * sx[k][ly][lx] + w0 * sx[k][ly + 1][lx] + w1 * sx[k][ly + 2][lx];
+      for (int k = 0; k < 3; k++)
+        cxy[((long long)b * 3 + k) * V + i] = w1 * sx[k][ly][lx] + w0 * sx[k][ly + 1][lx] + w1 * sx[k][ly + 2][lx];
+    }
+    // next plane: c is rewritten at once (its last reader, the x pass, is
+    // behind the second barrier); sx only after the next plane's first
+    // barrier, which every thread reaches after this y pass
   }
 }
 
@@ -754,7 +786,7 @@ cudaError_t normal_eq_partials(const float* q1, long long q1_stride_floats, cons
     w1 = e * w0;
     const int ntx = (W - 6 + kCxyTX - 1) / kCxyTX, nty = (H - 6 + kCxyTY - 1) / kCxyTY;
     if (W > 6 && H > 6 && D > 6) {
-      dim3 cgrid((unsigned)(ntx * nty), (unsigned)(D - 4), batch);
+      dim3 cgrid((unsigned)(ntx * nty), batch);
       cert_xy_kernel<<<cgrid, kCxyTX * kCxyTY, 0, st>>>(reinterpret_cast<const float2*>(q1), q1_stride_floats / 2,
                                                           reinterpret_cast<const float2*>(q2), W, H, D, ntx,
                                                           const_cast<float*>(cert), conv_iter, it, w0, w1);
