@@ -114,6 +114,9 @@ _SIGS = {
     "brc_register_two_volumes": (
         [_P, _P, _I, _I, _I, _P, _P, _I, _I, _I, _P, _P, _P, _P, _P, ctypes.POINTER(TwoVolumeOpts), _P, _P,
          _P, _P, _P], _I),
+    "brc_register_cohort": (
+        [_P, _I, _P, _P, _P, _P, _I, _I, _I, _P, _P, _P, _P, _P, ctypes.POINTER(TwoVolumeOpts), _P, _P, _P, _P],
+        _I),
 }
 
 

@@ -349,6 +349,42 @@ class Context:
         out["field"] = field
         return out
 
+    def register_cohort(self, subjects, voxel_sizes, template: torch.Tensor, template_voxel_size, bank: dict,
+                        linear_iterations: int, nonlinear_iterations: int, coarsest_scale: int,
+                        mm_z_cut: int = 0, tsigma=5.0, esigma=5.0, dsigma=5.0, solve_fp64: bool = False,
+                        precision: int = L.PREC_FP32):
+        """T1-to-template normalisation of a cohort: `subjects` is a list of
+        (D,H,W) device volumes of any sizes, `voxel_sizes` a matching list of
+        (vx, vy, vz).  Returns dict: params (n,12), aligned_linear,
+        aligned_nonlinear (n, template size) and fields (n,3, template size)."""
+        subs = [v.contiguous() for v in subjects]
+        n = len(subs)
+        t = template.contiguous()
+        D2, H2, W2 = t.shape
+        f3 = np.ascontiguousarray(bank["linear"], np.float32)
+        f6, m, d = self._nl_consts(bank)
+        o = L.TwoVolumeOpts()
+        L.lib().brc_two_volume_opts_default(ctypes.byref(o))
+        o.linear_iterations, o.nonlinear_iterations = linear_iterations, nonlinear_iterations
+        o.coarsest_scale, o.mm_z_cut = coarsest_scale, mm_z_cut
+        o.tsigma, o.esigma, o.dsigma = tsigma, esigma, dsigma
+        o.solve_fp64 = 1 if solve_fp64 else 0
+        o.precision = precision
+        ptrs = (ctypes.c_void_p * n)(*[v.data_ptr() for v in subs])
+        sizes = np.ascontiguousarray([[v.shape[2], v.shape[1], v.shape[0]] for v in subs], np.int32)
+        vs = np.ascontiguousarray(voxel_sizes, np.float32).reshape(n, 3)
+        tvs = np.ascontiguousarray(template_voxel_size, np.float32)
+        params = np.zeros((n, 12), np.float32)
+        lin = torch.empty((n, D2, H2, W2), dtype=torch.float32, device=t.device)
+        nl = torch.empty((n, D2, H2, W2), dtype=torch.float32, device=t.device)
+        fields = torch.zeros((n, 3, D2, H2, W2), dtype=torch.float32, device=t.device)
+        cp = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+        self._bind_stream()
+        _check(self, L.lib().brc_register_cohort(
+            self.handle, n, ctypes.cast(ptrs, ctypes.c_void_p), cp(sizes), cp(vs), _p(t), W2, H2, D2, cp(tvs),
+            cp(f3), cp(f6), cp(m), cp(d), ctypes.byref(o), cp(params), _p(lin), _p(nl), _p(fields)))
+        return {"params": params, "aligned_linear": lin, "aligned_nonlinear": nl, "fields": fields}
+
     def motion_correct(self, volumes: np.ndarray, voxel_size, filters, iterations: int,
                        tolerance: float = 0.0, reference: np.ndarray = None, use_graph: bool = True,
                        precision: int = L.PREC_FP32, certainty_sigma: float = 0.0):

@@ -6,6 +6,8 @@
 #include <math.h>
 #include <string.h>
 
+#include <vector>
+
 #include <string>
 
 #include "../../include/broccoli_b200.h"
@@ -359,6 +361,137 @@ extern "C" int brc_register_two_volumes(brc_ctx* ctx, const float* d_in, int W, 
     if (d_aligned_nonlinear)
       BRC_TRY(ctx, cudaMemcpyAsync(d_aligned_nonlinear, a, sizeof(float) * V2, cudaMemcpyDeviceToDevice, st),
               "copy");
+  }
+  BRC_TRY(ctx, cudaStreamSynchronize(st), "sync");
+  return BRC_OK;
+}
+
+// Composition total = match * linear of two parameter vectors in double
+// (AddAffineRegistrationParameters(total, match), broccoli_lib.cpp:7252-7340).
+static void compose_params(const float* linear, const float* match, float* total) {
+  double O[16] = {0}, N[16] = {0}, T[16];
+  const float* src[2] = {linear, match};
+  double* dst[2] = {O, N};
+  for (int m = 0; m < 2; m++) {
+    const float* p = src[m];
+    double* M = dst[m];
+    M[0] = (double)(p[3] + 1.0f); M[1] = p[4]; M[2] = p[5]; M[3] = p[0];
+    M[4] = p[6]; M[5] = (double)(p[7] + 1.0f); M[6] = p[8]; M[7] = p[1];
+    M[8] = p[9]; M[9] = p[10]; M[10] = (double)(p[11] + 1.0f); M[11] = p[2];
+    M[15] = 1.0;
+  }
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) {
+      double acc = 0;
+      for (int k = 0; k < 4; k++) acc += N[i * 4 + k] * O[k * 4 + j];
+      T[i * 4 + j] = acc;
+    }
+  total[0] = (float)T[3]; total[1] = (float)T[7]; total[2] = (float)T[11];
+  total[3] = (float)(T[0] - 1.0); total[4] = (float)T[1]; total[5] = (float)T[2];
+  total[6] = (float)T[4]; total[7] = (float)(T[5] - 1.0); total[8] = (float)T[6];
+  total[9] = (float)T[8]; total[10] = (float)T[9]; total[11] = (float)(T[10] - 1.0);
+}
+
+extern "C" int brc_register_cohort(brc_ctx* ctx, int n, const float* const* d_subjects, const int* sizes3n,
+                                   const float* voxel_sizes3n, const float* d_tpl, int W2, int H2, int D2,
+                                   const float* tpl_voxel_size3, const float* h_filters3, const float* h_filters6,
+                                   const float* h_tensors, const float* h_dirs, const brc_two_volume_opts* o,
+                                   float* h_params12n, float* d_aligned_linear, float* d_aligned_nonlinear,
+                                   float* d_fields) {
+  if (!ctx) return BRC_ERR_INVALID;
+  if (n <= 0 || n > 65535 || !d_subjects || !sizes3n || !voxel_sizes3n || !d_tpl || !tpl_voxel_size3 ||
+      !h_filters3 || !o || !h_params12n || W2 <= 0 || H2 <= 0 || D2 <= 0 || o->linear_iterations < 0 ||
+      o->nonlinear_iterations < 0 || o->coarsest_scale < 1)
+    return ctx->fail(BRC_ERR_INVALID, "brc_register_cohort: bad argument");
+  if (o->nonlinear_iterations > 0 && (!h_filters6 || !h_tensors || !h_dirs || !d_fields))
+    return ctx->fail(BRC_ERR_INVALID, "brc_register_cohort: nonlinear stage needs filters and fields");
+  for (int b = 0; b < n; b++) {
+    if (!d_subjects[b] || sizes3n[3 * b] <= 0 || sizes3n[3 * b + 1] <= 0 || sizes3n[3 * b + 2] <= 0)
+      return ctx->fail(BRC_ERR_INVALID, "brc_register_cohort: bad subject pointer or size");
+    for (int a = 0; a < 3; a++)
+      if (!(voxel_sizes3n[3 * b + a] > 0) || !(tpl_voxel_size3[a] > 0))
+        return ctx->fail(BRC_ERR_INVALID, "brc_register_cohort: voxel sizes must be positive");
+  }
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream();
+  const long long V2 = (long long)W2 * H2 * D2;
+  // template-grid working volumes of all subjects: resampled originals,
+  // centred copies, linear results; parameters; resample descriptors
+  DevBuf res, mat, lin, prm, jobs;
+  BRC_TRY(ctx, res.ensure(sizeof(float) * V2 * n), "alloc");
+  BRC_TRY(ctx, mat.ensure(sizeof(float) * V2 * n), "alloc");
+  BRC_TRY(ctx, lin.ensure(sizeof(float) * V2 * n), "alloc");
+  BRC_TRY(ctx, prm.ensure(sizeof(float) * 12 * n), "alloc");
+  BRC_TRY(ctx, jobs.ensure(brc::resize_job_bytes() * n), "alloc");
+  std::vector<unsigned char> h_jobs(brc::resize_job_bytes() * n);
+  // 1. every subject onto the template grid in one ragged launch
+  BRC_TRY(ctx, brc::resize_to_grid_ragged(n, d_subjects, sizes3n, voxel_sizes3n, h_jobs.data(), jobs.ptr,
+                                          res.as<float>(), W2, H2, D2, tpl_voxel_size3, o->mm_z_cut, st),
+          "resize");
+  ctx->launches += 1;
+  // 2. centre of mass matching (MatchVolumeMasses), one batched warp
+  float ct[3];
+  int s = brc_center_of_mass(ctx, d_tpl, W2, H2, D2, ct);
+  if (s != BRC_OK) return s;
+  std::vector<float> match(12 * (size_t)n, 0.f);
+  for (int b = 0; b < n; b++) {
+    float cs[3];
+    if ((s = brc_center_of_mass(ctx, res.as<float>() + V2 * b, W2, H2, D2, cs)) != BRC_OK) return s;
+    for (int k = 0; k < 3; k++) match[12 * b + k] = -(float)myround(ct[k] - cs[k]);
+  }
+  BRC_TRY(ctx, cudaMemcpyAsync(prm.ptr, match.data(), sizeof(float) * 12 * n, cudaMemcpyHostToDevice, st), "H2D");
+  BRC_TRY(ctx, brc::warp_affine(res.as<float>(), V2, W2, H2, D2, n, prm.as<float>(), mat.as<float>(), V2, nullptr,
+                                0, st),
+          "match");
+  ctx->launches += 1;
+  // 3. affine stage of all subjects as one batched multi-scale registration
+  std::vector<float> total(12 * (size_t)n, 0.f), linp(12 * (size_t)n, 0.f);
+  if (o->linear_iterations > 0) {
+    brc_linear_opts lo;
+    brc_linear_opts_default(&lo, o->linear_iterations);
+    lo.type = BRC_AFFINE;
+    lo.precision = o->precision;
+    s = brc_register_linear_scales(ctx, d_tpl, mat.as<float>(), W2, H2, D2, n, h_filters3, &lo, o->coarsest_scale,
+                                   prm.as<float>(), lin.as<float>(), nullptr);
+    if (s != BRC_OK) return s;
+    BRC_TRY(ctx, cudaMemcpyAsync(linp.data(), prm.ptr, sizeof(float) * 12 * n, cudaMemcpyDeviceToHost, st), "D2H");
+    BRC_TRY(ctx, cudaStreamSynchronize(st), "sync");
+  } else {
+    BRC_TRY(ctx, cudaMemcpyAsync(lin.ptr, mat.ptr, sizeof(float) * V2 * n, cudaMemcpyDeviceToDevice, st), "copy");
+  }
+  for (int b = 0; b < n; b++) compose_params(&linp[12 * (size_t)b], &match[12 * (size_t)b], &total[12 * (size_t)b]);
+  memcpy(h_params12n, total.data(), sizeof(float) * 12 * n);
+  if (d_aligned_linear)
+    BRC_TRY(ctx, cudaMemcpyAsync(d_aligned_linear, lin.ptr, sizeof(float) * V2 * n, cudaMemcpyDeviceToDevice, st),
+            "copy");
+  // 4. nonlinear stage per subject (each runs at template size)
+  if (o->nonlinear_iterations > 0) {
+    brc_nonlinear_opts no;
+    brc_nonlinear_opts_default(&no, o->nonlinear_iterations);
+    no.coarsest_scale = o->coarsest_scale;
+    no.tsigma = o->tsigma;
+    no.esigma = o->esigma;
+    no.dsigma = o->dsigma;
+    no.precision = o->precision;
+    no.solve_fp64 = o->solve_fp64;
+    for (int b = 0; b < n; b++) {
+      float* field = d_fields + 3 * V2 * b;
+      float* out = mat.as<float>() + V2 * b;  // the centred copy is no longer needed
+      s = brc_register_nonlinear(ctx, d_tpl, lin.as<float>() + V2 * b, W2, H2, D2, h_filters6, h_tensors, h_dirs,
+                                 &no, field, out);
+      if (s != BRC_OK) return s;
+      if (o->linear_iterations > 0) {
+        BRC_TRY(ctx, brc::add_affine_to_field(field, W2, H2, D2, &total[12 * (size_t)b], st), "field");
+        BRC_TRY(ctx, brc::warp_field(res.as<float>() + V2 * b, W2, H2, D2, field, field + V2, field + 2 * V2, out,
+                                     st),
+                "warp");
+        ctx->launches += 2;
+      }
+      if (d_aligned_nonlinear)
+        BRC_TRY(ctx, cudaMemcpyAsync(d_aligned_nonlinear + V2 * b, out, sizeof(float) * V2, cudaMemcpyDeviceToDevice,
+                                     st),
+                "copy");
+    }
   }
   BRC_TRY(ctx, cudaStreamSynchronize(st), "sync");
   return BRC_OK;

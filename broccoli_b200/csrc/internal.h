@@ -53,6 +53,15 @@ cudaError_t resize_to_grid(const float* src, int W, int H, int D, float vx, floa
                            int W2, int H2, int D2, float nvx, float nvy, float nvz, int mm_z_cut,
                            cudaStream_t st);
 cudaError_t mass_moments(const float* vol, int W, int H, int D, double* sums, cudaStream_t st);
+// Ragged batch of resamples onto one grid, one launch: subject b (device
+// pointer srcs[b], size dims3n[3b..3b+2], voxel size vox3n[3b..3b+2]) into
+// out + b W2 H2 D2.  h_jobs / d_jobs: n * resize_job_bytes() of host and
+// device staging for the per-subject descriptors (pageable host memory is
+// fine: the copy is staged before the call returns).
+size_t resize_job_bytes();
+cudaError_t resize_to_grid_ragged(int n, const float* const* srcs, const int* dims3n, const float* vox3n,
+                                  void* h_jobs, void* d_jobs, float* out, int W2, int H2, int D2,
+                                  const float* new_vox3, int mm_z_cut, cudaStream_t st);
 cudaError_t add_affine_to_field(float* field, int W, int H, int D, const float* p12, cudaStream_t st);
 }  // namespace brc
 

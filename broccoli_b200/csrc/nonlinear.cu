@@ -280,6 +280,30 @@ resize_to_grid_kernel(const float* __restrict__ src, int W, int H, int D, float*
   out[i] = v;
 }
 
+// One subject of a ragged batch: its own source volume and size, resampled
+// onto the shared new grid (same arithmetic as resize_to_grid_kernel).
+struct ResizeJob {
+  const float* src;
+  int W, H, D;
+  ResizeGeom g;
+};
+
+__global__ void __launch_bounds__(256)
+resize_to_grid_ragged_kernel(const ResizeJob* __restrict__ jobs, float* __restrict__ out, int W2, int H2,
+                             int D2) {
+  const long long V2 = (long long)W2 * H2 * D2;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V2) return;
+  const ResizeJob& j = jobs[blockIdx.y];
+  const int xn = (int)(i % W2), yn = (int)((i / W2) % H2), zn = (int)(i / ((long long)W2 * H2));
+  const int x = xn - j.g.offn[0], y = yn - j.g.offn[1], z = zn - j.g.offn[2];
+  const int xi = x + j.g.offi[0], yi = y + j.g.offi[1], zi = z + j.g.offi[2];
+  float v = 0.f;
+  if (x >= 0 && y >= 0 && z >= 0 && xi >= 0 && yi >= 0 && zi >= 0 && xi < j.g.Wi && yi < j.g.Hi && zi < j.g.Di)
+    v = sample_lin(j.src, j.W, j.H, j.D, xi * j.g.vd[0] + 0.5f, yi * j.g.vd[1] + 0.5f, zi * j.g.vd[2] + 0.5f);
+  out[(long long)blockIdx.y * V2 + i] = v;
+}
+
 // Sums of m, m x, m y, m z over the volume in FP64 (centre of mass;
 // CalculateCenterOfMass, broccoli_lib.cpp:6763-6800, accumulates in float
 // on the host after a full device-to-host copy).
@@ -339,14 +363,14 @@ static unsigned grid1(long long n) { return (unsigned)((n + 255) / 256); }
 
 static int round_half_away(float v) { return (int)roundf(v); }
 
-cudaError_t resize_to_grid(const float* src, int W, int H, int D, float vx, float vy, float vz, float* out,
-                           int W2, int H2, int D2, float nvx, float nvy, float nvz, int mm_z_cut,
-                           cudaStream_t st) {
-  ResizeGeom g;
+// Geometry of ChangeVolumesResolutionAndSize for one volume; false if the
+// interpolated size is below 2 voxels along an axis.
+static bool resize_geom(int W, int H, int D, float vx, float vy, float vz, int W2, int H2, int D2, float nvx,
+                        float nvy, float nvz, int mm_z_cut, ResizeGeom& g) {
   g.Wi = (int)floorf((float)W * vx / nvx + 0.5f);
   g.Hi = (int)floorf((float)H * vy / nvy + 0.5f);
   g.Di = (int)floorf((float)D * vz / nvz + 0.5f);
-  if (g.Wi < 2 || g.Hi < 2 || g.Di < 2) return cudaErrorInvalidValue;
+  if (g.Wi < 2 || g.Hi < 2 || g.Di < 2) return false;
   const int diff[3] = {g.Wi - W2, g.Hi - H2, g.Di - D2};
   const int zcut = (int)round((float)mm_z_cut / nvz);
   for (int a = 0; a < 3; a++) {
@@ -363,7 +387,38 @@ cudaError_t resize_to_grid(const float* src, int W, int H, int D, float vx, floa
   g.vd[0] = (float)(W - 1) / (float)(g.Wi - 1);
   g.vd[1] = (float)(H - 1) / (float)(g.Hi - 1);
   g.vd[2] = (float)(D - 1) / (float)(g.Di - 1);
+  return true;
+}
+
+cudaError_t resize_to_grid(const float* src, int W, int H, int D, float vx, float vy, float vz, float* out,
+                           int W2, int H2, int D2, float nvx, float nvy, float nvz, int mm_z_cut,
+                           cudaStream_t st) {
+  ResizeGeom g;
+  if (!resize_geom(W, H, D, vx, vy, vz, W2, H2, D2, nvx, nvy, nvz, mm_z_cut, g)) return cudaErrorInvalidValue;
   resize_to_grid_kernel<<<grid1((long long)W2 * H2 * D2), 256, 0, st>>>(src, W, H, D, out, W2, H2, D2, g);
+  return cudaGetLastError();
+}
+
+size_t resize_job_bytes() { return sizeof(ResizeJob); }
+
+cudaError_t resize_to_grid_ragged(int n, const float* const* srcs, const int* dims3n, const float* vox3n,
+                                  void* h_jobs, void* d_jobs, float* out, int W2, int H2, int D2,
+                                  const float* new_vox3, int mm_z_cut, cudaStream_t st) {
+  ResizeJob* jobs = static_cast<ResizeJob*>(h_jobs);
+  for (int b = 0; b < n; b++) {
+    ResizeJob& j = jobs[b];
+    j.src = srcs[b];
+    j.W = dims3n[3 * b];
+    j.H = dims3n[3 * b + 1];
+    j.D = dims3n[3 * b + 2];
+    if (!resize_geom(j.W, j.H, j.D, vox3n[3 * b], vox3n[3 * b + 1], vox3n[3 * b + 2], W2, H2, D2, new_vox3[0],
+                     new_vox3[1], new_vox3[2], mm_z_cut, j.g))
+      return cudaErrorInvalidValue;
+  }
+  cudaError_t e = cudaMemcpyAsync(d_jobs, jobs, sizeof(ResizeJob) * n, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return e;
+  dim3 grid(grid1((long long)W2 * H2 * D2), n);
+  resize_to_grid_ragged_kernel<<<grid, 256, 0, st>>>(static_cast<const ResizeJob*>(d_jobs), out, W2, H2, D2);
   return cudaGetLastError();
 }
 

@@ -375,6 +375,27 @@ int brc_register_two_volumes(brc_ctx* ctx, const float* d_in, int W, int H, int 
                              float* d_interpolated, float* d_aligned_linear,
                              float* d_aligned_nonlinear, float* d_field);
 
+/* T1-to-template normalisation of a cohort of n subjects of different sizes
+ * (the reference normalises one subject per PerformRegistrationTwoVolumes-
+ * Wrapper call, broccoli_lib.cpp:7973-8112).  d_subjects is a host array of
+ * n device pointers; subject b has size sizes3n[3b..3b+2] (W, H, D) and
+ * voxel size voxel_sizes3n[3b..3b+2].  All subjects are resampled onto the
+ * template grid in one launch (ChangeVolumesResolutionAndSize,
+ * :6950-7100), centred by their centres of mass (MatchVolumeMasses,
+ * :6876-6948) with one batched warp, registered affinely as one batch
+ * over the scales, then registered nonlinearly one by one (each at
+ * template size).  Per subject b the results equal those of
+ * brc_register_two_volumes: h_params12n[12b..] (host), d_aligned_linear +
+ * b V2, d_aligned_nonlinear + b V2, d_fields + 3 b V2 (V2 = W2 H2 D2;
+ * volumes optional, NULL to skip; d_fields required when the nonlinear
+ * stage runs).  Synchronises before returning. */
+int brc_register_cohort(brc_ctx* ctx, int n, const float* const* d_subjects, const int* sizes3n,
+                        const float* voxel_sizes3n, const float* d_tpl, int W2, int H2, int D2,
+                        const float* tpl_voxel_size3, const float* h_filters3, const float* h_filters6,
+                        const float* h_tensors, const float* h_dirs, const brc_two_volume_opts* opts,
+                        float* h_params12n, float* d_aligned_linear, float* d_aligned_nonlinear,
+                        float* d_fields);
+
 #ifdef __cplusplus
 }
 #endif

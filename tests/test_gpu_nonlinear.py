@@ -10,6 +10,7 @@ import torch
 
 from conftest import rel_err
 from broccoli_b200 import _lib as L
+from broccoli_b200 import synthetic as S
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-4
@@ -104,3 +105,27 @@ def test_register_two_volumes_matches_golden(ctx, golden, bank):
     assert param_err(r["params"], golden["r2v_params"]) < TOL
     for k in ("interpolated", "aligned_linear", "aligned_nonlinear", "field"):
         assert rel_err(r[k].cpu().numpy(), golden["r2v_" + k]) < TOL, k
+
+
+@pytest.mark.parametrize("prec", [L.PREC_FP32, L.PREC_BF16X3])
+def test_cohort_equals_two_volumes_per_subject(ctx, golden, bank, prec):
+    """brc_register_cohort: three subjects of different sizes and voxel
+    sizes (one ragged resample launch, one batched affine stage, nonlinear
+    per subject) give, subject by subject, exactly what
+    brc_register_two_volumes gives."""
+    tpl = golden["r2v_template"]
+    subs, vox = [], []
+    for i, (shape, vs) in enumerate((((30, 36, 34), (1.1, 0.9, 1.2)), ((27, 40, 31), (1.2, 1.0, 1.0)),
+                                     ((33, 34, 37), (0.9, 1.1, 0.95)))):
+        sub, _, _ = S.t1_template_pair(shape, tpl.shape, seed=10 + i)
+        subs.append(sub.astype(np.float32))
+        vox.append(vs)
+    c = ctx.register_cohort([cuda(v) for v in subs], vox, cuda(tpl), (1.0, 1.0, 1.0), bank, 6, 3, 2, mm_z_cut=3,
+                            precision=prec)
+    for i in range(3):
+        r = ctx.register_two_volumes(cuda(subs[i]), vox[i], cuda(tpl), (1.0, 1.0, 1.0), bank, 6, 3, 2, mm_z_cut=3,
+                                     precision=prec)
+        assert np.array_equal(c["params"][i], r["params"]), i
+        assert np.array_equal(c["aligned_linear"][i].cpu().numpy(), r["aligned_linear"].cpu().numpy()), i
+        assert np.array_equal(c["aligned_nonlinear"][i].cpu().numpy(), r["aligned_nonlinear"].cpu().numpy()), i
+        assert np.array_equal(c["fields"][i].cpu().numpy(), r["field"].cpu().numpy()), i
