@@ -380,10 +380,14 @@ def run_gpu(args, rank, world, local_rank):
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     sm_max = clocks.get("sm_max_mhz") if clocks else None
     fp32_peak = 148 * 128 * 2 * (sm_max or 1965.0) * 1e6 / 1e12
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "filter3d_fp32_traffic.json")
-    if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get("dram_bytes_per_launch")
+    # DRAM bytes (read + write) per filtered volume of 64x64x33 from one ncu
+    # capture of each kernel on 63 volumes (profiles/filter3d_tc_motion_
+    # correction.md, profiles/filter3d_sym_motion_correction.md), scaled to
+    # this launch by the volume count (traffic grows with the volumes)
+    tc_bytes_per_vol = (34574592 + 149403392) / 63
+    sym_bytes_per_vol = (34094848 + 147386624) / 63
+    traffic = sym_bytes_per_vol * (T - 1) if symmetric_bank(fl) and tuple(SHAPE) == (33, 64, 64) else None
+    tc_traffic = tc_bytes_per_vol * (T - 1) if tuple(SHAPE) == (33, 64, 64) else None
     achieved = f_flop / (f_ms / 1000.0) / 1e12
     if prec == L.PREC_BF16X3:
         peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
@@ -399,7 +403,10 @@ def run_gpu(args, rank, world, local_rank):
                     "flop_note": "3 split products x the 343-tap convolution of 3 complex filters; "
                                  "the banded-Toeplitz zeros the GEMMs also issue are not counted",
                     "launch_ms": f_ms, "fp32_equiv_tflops": achieved,
-                    "fp32_filter_launch_ms": f32_ms, "traffic": None}
+                    "fp32_filter_launch_ms": f32_ms, "traffic": tc_traffic,
+                    "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on 63 "
+                                    "volumes, scaled by the volume count; algorithmic: 4 B in + 24 B out "
+                                    "per voxel"}
     else:
         roofline = {"kernel": ("filter3d_sym_kernel<3,8,3> (even/odd half-tap form; FLOP counted "
                                "as the full 343-tap convolution)") if symmetric_bank(fl) else

@@ -456,8 +456,7 @@ struct RegPlan {
   int* conv_iter;
   int* iters_ws;
   int* status;
-  int nblk, zpb;
-  float* cert;  // [batch][3][V] certainty volumes when smoothing them, else null
+  int nblk;  // partial rows per instance of the normal-equation kernel
   FilterPath fpath;
 };
 
@@ -489,11 +488,10 @@ long long enqueue_registration(brc_ctx* ctx, const RegPlan& p, cudaStream_t st) 
     const float* cur = it == 0 ? p.moving : p.aligned;
     if ((e = run_filter(p.fpath, cur, p.W, p.H, p.D, p.batch, V, p.q2, p.conv_iter, it, st)) != cudaSuccess)
       return ctx->cuda(e, "filter3d");
-    if ((e = brc::normal_eq_partials(p.q1, p.ref_stride ? 6 * V : 0, p.q2, p.W, p.H, p.D, p.batch,
-                                     p.partials, p.nblk, p.zpb, p.conv_iter, it, st, p.cert,
-                                     p.opts.certainty_sigma_x100 / 100.0f)) != cudaSuccess)
+    if ((e = brc::normal_eq_march(p.q1, p.ref_stride ? 6 * V : 0, p.q2, p.W, p.H, p.D, p.batch, p.partials,
+                                  p.nblk, p.conv_iter, it, st, p.opts.certainty_sigma_x100 / 100.0f)) !=
+        cudaSuccess)
       return ctx->cuda(e, "normal_eq");
-    if (p.cert) kernels++;
     if ((e = brc::solve_update(p.partials, p.nblk, p.batch, p.opts.type, p.opts.tolerance, p.W, p.H,
                                p.D, p.params, p.rotations, p.conv_iter, p.iters_ws, p.status, it,
                                st)) != cudaSuccess)
@@ -547,9 +545,10 @@ extern "C" int brc_register_linear_batched(brc_ctx* ctx, const float* d_ref, lon
   p.params = d_params;
   p.rotations = d_rotations;
   p.iterations = d_iterations;
-  p.zpb = pick_zpb(W, H);
-  const int nint = D - 6 > 0 ? D - 6 : 1;
-  p.nblk = (nint + p.zpb - 1) / p.zpb;
+  {
+    int ntx, nty, zs;
+    p.nblk = brc::normal_eq_march_blocks(W, H, D, &ntx, &nty, &zs);
+  }
 
   const size_t q1n = sizeof(float) * 6 * V * (ref_stride ? batch : 1);
   const size_t q2n = sizeof(float) * 6 * V * batch;
@@ -569,11 +568,6 @@ extern "C" int brc_register_linear_batched(brc_ctx* ctx, const float* d_ref, lon
     const int ps = make_filter_path(ctx, h_filters, 3, opts->precision, W, H, D, &p.fpath);
     if (ps != BRC_OK) return ps;
   }
-  p.cert = nullptr;
-  if (opts->certainty_sigma_x100 > 0) {
-    BRC_TRY(ctx, ctx->cert.ensure(sizeof(float) * 3 * V * batch), "alloc certainty");
-    p.cert = ctx->cert.as<float>();
-  }
 
   const cudaStream_t user = ctx->stream();
   if (!opts->use_graph) {
@@ -588,7 +582,7 @@ extern "C" int brc_register_linear_batched(brc_ctx* ctx, const float* d_ref, lon
              (uint64_t)fnv1a(&opts->tolerance, sizeof(float)), (uint64_t)d_params,
              (uint64_t)p.aligned, (uint64_t)d_rotations, (uint64_t)d_iterations,
              (uint64_t)ctx->q1.ptr, (uint64_t)ctx->q2.ptr, (uint64_t)ctx->partials.ptr,
-             (uint64_t)ctx->ctl.ptr, (uint64_t)p.cert, (uint64_t)opts->certainty_sigma_x100,
+             (uint64_t)ctx->ctl.ptr, (uint64_t)opts->certainty_sigma_x100,
              (uint64_t)opts->precision, (uint64_t)p.fpath.d_taps};
     auto itg = ctx->graphs.find(key);
     GraphEntry* ge = nullptr;

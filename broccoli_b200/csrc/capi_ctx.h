@@ -63,7 +63,7 @@ struct brc_ctx {
   cudaEvent_t ev_chunk_in[kMaxChunks] = {}, ev_chunk_done[kMaxChunks] = {};
   std::string last_error;
   unsigned long long launches = 0;
-  DevBuf q1, q2, aligned, partials, ctl, tmp1, tmp2, series, corrected, params, rot, nl, pyr, cert;
+  DevBuf q1, q2, aligned, partials, ctl, tmp1, tmp2, series, corrected, params, rot, nl, pyr;
   std::map<GraphKey, std::unique_ptr<GraphEntry>> graphs;
   // packed split-BF16 taps of the tensor-core filtering, per filter bank
   // (key: hash of the bank and its size); graphs may hold these pointers,

@@ -10,12 +10,17 @@ cudaError_t filter3d_fp32(const float* vol, int W, int H, int D, int batch, long
                           const float* h_filters, int nfilt, float* out, const int* conv_iter,
                           int it, cudaStream_t st, bool allow_symmetric = true);
 // registration.cu
-// cert != nullptr: certainty volumes [batch][3][V] are computed into `cert`
-// and the sums use their 3x3x3 Gaussian smoothing (sigma cert_sigma).
+// Normal equations of batch instances, one CTA per `zpb` interior slices of
+// an instance (the single-call and allocation-free entry points).
 cudaError_t normal_eq_partials(const float* q1, long long q1_stride_floats, const float* q2, int W,
                                int H, int D, int batch, double* partials, int nblk, int zpb,
-                               const int* conv_iter, int it, cudaStream_t st, const float* cert = nullptr,
-                               float cert_sigma = 0.f);
+                               const int* conv_iter, int it, cudaStream_t st);
+// Normal equations in the z-marching form (certainty smoothing fused in when
+// cert_sigma > 0): partial rows per instance and the launch.
+int normal_eq_march_blocks(int W, int H, int D, int* ntx, int* nty, int* zs);
+cudaError_t normal_eq_march(const float* q1, long long q1_stride_floats, const float* q2, int W, int H, int D,
+                            int batch, double* partials, int nblk, const int* conv_iter, int it, cudaStream_t st,
+                            float cert_sigma);
 cudaError_t assemble_normal_eq(const double* partials, int nblk, int batch, double* A, double* h,
                                cudaStream_t st);
 cudaError_t solve_update(const double* partials, int nblk, int batch, int type, float tol, int W,

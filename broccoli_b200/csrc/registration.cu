@@ -55,90 +55,6 @@ __device__ __forceinline__ float phase_grad(float2 a_p, float2 a_c, float2 a_m, 
   return atan2f(ti, tr);
 }
 
-// Certainties |q1 q2| cos^2(dphi/2) of the three filter pairs smoothed along
-// x and then y by the 3-tap Gaussian (w1, w0, w1): the first two passes of
-// the separable 3x3x3 certainty smoothing, in the order x, y, z.  Computed
-// where the z pass of the interior voxels reads them: planes 2..D-3, rows
-// and columns 3..N-4 (their x/y neighbours 2..N-3 are inside the volume).
-// One CTA: a 32x8 patch of one instance through all those planes; the
-// certainties of the patch and its 1-voxel halo are staged in shared
-// memory, and each thread holds the responses of its (at most two) halo
-// cells for the next plane in registers while the current one is smoothed,
-// so every plane's loads overlap the previous plane's work.
-constexpr int kCxyTX = 32, kCxyTY = 8, kCxyCells = (kCxyTX + 2) * (kCxyTY + 2);
-
-__global__ void __launch_bounds__(256)
-cert_xy_kernel(const float2* __restrict__ q1, long long q1_stride, const float2* __restrict__ q2, int W, int H,
-               int D, int ntx, float* __restrict__ cxy, const int* __restrict__ conv_iter, int it, float w0,
-               float w1) {
-  const int b = blockIdx.y;
-  if (instance_done(conv_iter, b, it)) return;
-  __shared__ float c[3][kCxyTY + 2][kCxyTX + 2];
-  __shared__ float sx[3][kCxyTY + 2][kCxyTX];
-  const long long V = (long long)W * H * D;
-  const long long WH = (long long)W * H;
-  const int tx0 = 3 + (blockIdx.x % ntx) * kCxyTX, ty0 = 3 + (blockIdx.x / ntx) * kCxyTY;
-  const float2* Q1 = q1 + (long long)b * q1_stride;
-  const float2* Q2 = q2 + (long long)b * 3 * V;
-  // the (at most two) halo cells of this thread
-  int cell[2];
-  bool in[2];
-  long long off[2];
-#pragma unroll
-  for (int h = 0; h < 2; h++) {
-    cell[h] = threadIdx.x + h * 256;
-    const int ly = cell[h] / (kCxyTX + 2), lx = cell[h] - ly * (kCxyTX + 2);
-    const int x = tx0 - 1 + lx, y = ty0 - 1 + ly;
-    in[h] = cell[h] < kCxyCells && x <= W - 3 && y <= H - 3;
-    off[h] = (long long)y * W + x;
-  }
-  float2 qa[2][3], qc[2][3];
-  auto load_plane = [&](int z) {
-#pragma unroll
-    for (int h = 0; h < 2; h++)
-#pragma unroll
-      for (int k = 0; k < 3; k++)
-        if (in[h]) {
-          const long long i = (long long)z * WH + off[h];
-          qa[h][k] = __ldg(Q1 + k * V + i);
-          qc[h][k] = __ldg(Q2 + k * V + i);
-        }
-  };
-  load_plane(2);
-  for (int z = 2; z <= D - 3; z++) {
-#pragma unroll
-    for (int h = 0; h < 2; h++) {
-      if (cell[h] >= kCxyCells) continue;
-      const int ly = cell[h] / (kCxyTX + 2), lx = cell[h] - ly * (kCxyTX + 2);
-#pragma unroll
-      for (int k = 0; k < 3; k++) {
-        float pd, cv = 0.f;
-        if (in[h]) phase_diff_cert(qa[h][k], qc[h][k], pd, cv);
-        c[k][ly][lx] = cv;
-      }
-    }
-    if (z < D - 3) load_plane(z + 1);  // in flight during the smoothing below
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < (kCxyTY + 2) * kCxyTX; idx += blockDim.x) {
-      const int ly = idx / kCxyTX, lx = idx - ly * kCxyTX;
-#pragma unroll
-      for (int k = 0; k < 3; k++) sx[k][ly][lx] = w1 * c[k][ly][lx] + w0 * c[k][ly][lx + 1] + w1 * c[k][ly][lx + 2];
-    }
-    __syncthreads();
-    const int ly = threadIdx.x / kCxyTX, lx = threadIdx.x - ly * kCxyTX;
-    const int x = tx0 + lx, y = ty0 + ly;
-    if (ly < kCxyTY && x < W - 3 && y < H - 3) {
-      const long long i = (long long)z * WH + (long long)y * W + x;
-#pragma unroll
-      for (int k = 0; k < 3; k++)
-        cxy[((long long)b * 3 + k) * V + i] = w1 * sx[k][ly][lx] + w0 * sx[k][ly + 1][lx] + w1 * sx[k][ly + 2][lx];
-    }
-    // next plane: c is rewritten at once (its last reader, the x pass, is
-    // behind the second barrier); sx only after the next plane's first
-    // barrier, which every thread reaches after this y pass
-  }
-}
-
 // Sum e (0..13) of one axis as (row moment) x y^py x z^pz: moments
 // [sum w, sum w x, sum w x^2, sum v, sum v x] of the row, y and z relative
 // to the volume centre.
@@ -180,8 +96,7 @@ __device__ __forceinline__ double zpow(double z, int e) {
 __global__ void __launch_bounds__(kNEThreads, 4)
 normal_eq_partial_kernel(const float2* __restrict__ q1, long long q1_stride,
                          const float2* __restrict__ q2, int W, int H, int D, int zpb,
-                         double* __restrict__ partials, const int* __restrict__ conv_iter, int it,
-                         const float* __restrict__ cert_in, float cw0, float cw1) {
+                         double* __restrict__ partials, const int* __restrict__ conv_iter, int it) {
   const int b = blockIdx.y;
   if (instance_done(conv_iter, b, it)) return;
   const long long V = (long long)W * H * D;
@@ -251,11 +166,6 @@ normal_eq_partial_kernel(const float2* __restrict__ q1, long long q1_stride,
         }
         float pd, cert;
         phase_diff_cert(a, c, pd, cert);
-        if (cert_in != nullptr) {
-          // z pass of the separable smoothing over the x/y-smoothed certainties
-          const float* cz = cert_in + ((long long)b * 3 + k) * V + i;
-          cert = act ? cw1 * __ldg(cz - WH) + cw0 * __ldg(cz) + cw1 * __ldg(cz + WH) : 0.f;
-        }
         const float g = phase_grad(ap, a, am, cp, c, cm);
         const float cg = act ? cert * g : 0.f;
         const float w = cg * g;
@@ -290,6 +200,200 @@ normal_eq_partial_kernel(const float2* __restrict__ q1, long long q1_stride,
     double v = 0.0;
 #pragma unroll
     for (int w = 0; w < kNEThreads / 32; w++) v += s_part[w][threadIdx.x];
+    partials[((long long)b * gridDim.x + blockIdx.x) * kNSums + threadIdx.x] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Normal equations, z-marching form: certainty smoothing fused in.
+//
+// One CTA of 10 warps x 32 lanes covers a patch of 30 x 8 interior voxels
+// (x, y) with a one-voxel halo (lanes 0 and 31, warps 0 and 9) and walks a
+// slab of interior planes z0..z1-1, reading each plane's responses once:
+//   * certainties of a plane are smoothed along x by shuffles, along y
+//     through shared memory and along z through a three-plane window kept
+//     in shared memory (the separable 3x3x3 Gaussian in the order x, y, z);
+//   * phase-gradient neighbours come from the adjacent lanes (x), from the
+//     shared-memory copy of the axis-1 responses of the adjacent warps (y)
+//     and from the previous / next plane held in registers (z);
+//   * each lane accumulates, over the planes, the FP32 moments
+//     sum w [1, z, z^2] and sum v [1, z] of its (x, y) column per axis and
+//     expands them once into the 42 FP64 sums with its x and y.
+// The next plane's responses are loaded while the current plane's sums are
+// computed.  Without smoothing, the same sums as normal_eq_partial_kernel
+// up to FP32 summation order.
+// ---------------------------------------------------------------------------
+
+constexpr int kMarchWarps = 10;              // 8 output rows + 2 halo rows
+constexpr int kMarchCols = 30;               // output columns per warp
+constexpr int kMarchZs = 16;                 // at most this many planes per slab
+
+struct PlaneQ {
+  float2 a[3], c[3];  // q1, q2 of the three filters at this lane's (x, y)
+};
+
+__device__ __forceinline__ void load_plane_q(const float2* __restrict__ Q1, const float2* __restrict__ Q2,
+                                             long long V, long long i, bool in, PlaneQ& q) {
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    q.a[k] = in ? __ldg(Q1 + k * V + i) : make_float2(0.f, 0.f);
+    q.c[k] = in ? __ldg(Q2 + k * V + i) : make_float2(0.f, 0.f);
+  }
+}
+
+template <bool SMOOTH>
+__global__ void __launch_bounds__(kMarchWarps * 32, 2)
+normal_eq_march_kernel(const float2* __restrict__ q1, long long q1_stride, const float2* __restrict__ q2, int W,
+                       int H, int D, int ntx, int nty, int zs, double* __restrict__ partials,
+                       const int* __restrict__ conv_iter, int it, float cw0, float cw1) {
+  const int b = blockIdx.y;
+  if (instance_done(conv_iter, b, it)) return;
+  __shared__ float sxr[kMarchWarps][3][32];     // x-smoothed certainties of the newest plane
+  // x/y-smoothed certainties of the last three planes (slot p % 3); each
+  // thread reads back only its own entries, so no barrier guards them
+  __shared__ float cxr[SMOOTH ? 3 : 1][kMarchWarps][3][32];
+  __shared__ float2 qy1[2][kMarchWarps][32];    // axis-1 responses (q1) of the last two planes
+  __shared__ float2 qy2[2][kMarchWarps][32];    // axis-1 responses (q2)
+  __shared__ double s_part[kMarchWarps][kNSums];
+  const long long V = (long long)W * H * D;
+  const long long WH = (long long)W * H;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nzs = gridDim.x / (ntx * nty);
+  const int zsl = blockIdx.x / (ntx * nty), rem = blockIdx.x - zsl * (ntx * nty);
+  const int yt = rem / ntx, xt = rem - yt * ntx;
+  const int x = 3 + xt * kMarchCols - 1 + lane;  // lanes 0 and 31: halo columns
+  const int y = 3 + yt * 8 - 1 + warp;           // warps 0 and 9: halo rows
+  const int z0 = 3 + zsl * zs;
+  const int z1 = min(D - 3, z0 + zs);
+  (void)nzs;
+  const bool empty = W <= 6 || H <= 6 || z1 <= z0;  // no interior voxel: zero sums
+  const float2* Q1 = q1 + (long long)b * q1_stride;
+  const float2* Q2 = q2 + (long long)b * 3 * V;
+  const bool in = x < W && y < H;                         // loads stay inside the volume
+  const bool cin = x <= W - 3 && y <= H - 3;              // certainty defined (smoothing support)
+  const bool out = lane >= 1 && lane <= kMarchCols && warp >= 1 && warp <= 8 && x <= W - 4 && y <= H - 4;
+  const long long col = (long long)y * W + x;
+  const float xf = (float)x - 0.5f * (float)(W - 1);
+  const float w0 = cw0, w1 = cw1;
+
+  // per-lane moments over the planes: [k][sum w, sum w z, sum w z^2, sum v, sum v z]
+  float m[3][5];
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+#pragma unroll
+    for (int q = 0; q < 5; q++) m[k][q] = 0.f;
+
+  PlaneQ cur, nw, nxt;
+  float2 prev_a2 = make_float2(0.f, 0.f), prev_c2 = make_float2(0.f, 0.f);  // axis 2 at z - 1
+#pragma unroll
+  for (int k = 0; k < 3; k++) cur.a[k] = cur.c[k] = nw.a[k] = nw.c[k] = make_float2(0.f, 0.f);
+  if (!empty) load_plane_q(Q1, Q2, V, (long long)(z0 - 1) * WH + col, in, nw);
+
+  for (int p = z0 - 1; !empty && p <= z1; p++) {
+    // [A] certainties of plane p, x pass, axis-1 responses to shared memory
+    if (SMOOTH) {
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        float pd, cv = 0.f;
+        phase_diff_cert(nw.a[k], nw.c[k], pd, cv);
+        cv = cin ? cv : 0.f;
+        const float cl = __shfl_up_sync(0xffffffffu, cv, 1), cr = __shfl_down_sync(0xffffffffu, cv, 1);
+        sxr[warp][k][lane] = w1 * cl + w0 * cv + w1 * cr;
+      }
+    }
+    qy1[p & 1][warp][lane] = nw.a[1];
+    qy2[p & 1][warp][lane] = nw.c[1];
+    __syncthreads();
+    // next plane in flight during the rest of this step
+    if (p + 1 <= z1) load_plane_q(Q1, Q2, V, (long long)(p + 1) * WH + col, in, nxt);
+    // [B] y pass: smoothed certainty of plane p in the register window
+    if (SMOOTH && warp >= 1 && warp <= 8) {
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+        cxr[SMOOTH ? p % 3 : 0][warp][k][lane] =
+            w1 * sxr[warp - 1][k][lane] + w0 * sxr[warp][k][lane] + w1 * sxr[warp + 1][k][lane];
+    }
+    // [C] sums of output plane z = p - 1
+    if (p >= z0 + 1) {
+      const int z = p - 1;
+      const float zf = (float)z - 0.5f * (float)(D - 1);
+      // x neighbours of axis 0 from the adjacent lanes (all lanes shuffle)
+      const float2 a0p = make_float2(__shfl_down_sync(0xffffffffu, cur.a[0].x, 1),
+                                     __shfl_down_sync(0xffffffffu, cur.a[0].y, 1));
+      const float2 c0p = make_float2(__shfl_down_sync(0xffffffffu, cur.c[0].x, 1),
+                                     __shfl_down_sync(0xffffffffu, cur.c[0].y, 1));
+      const float2 a0m = make_float2(__shfl_up_sync(0xffffffffu, cur.a[0].x, 1),
+                                     __shfl_up_sync(0xffffffffu, cur.a[0].y, 1));
+      const float2 c0m = make_float2(__shfl_up_sync(0xffffffffu, cur.c[0].x, 1),
+                                     __shfl_up_sync(0xffffffffu, cur.c[0].y, 1));
+      if (out) {
+        const int sl = z & 1;  // slot of plane z = p - 1
+        float2 ap[3], am[3], cp[3], cm[3];
+        ap[0] = a0p; am[0] = a0m; cp[0] = c0p; cm[0] = c0m;
+        ap[1] = qy1[sl][warp + 1][lane]; am[1] = qy1[sl][warp - 1][lane];
+        cp[1] = qy2[sl][warp + 1][lane]; cm[1] = qy2[sl][warp - 1][lane];
+        ap[2] = nw.a[2]; am[2] = prev_a2; cp[2] = nw.c[2]; cm[2] = prev_c2;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+          float pd, cert;
+          phase_diff_cert(cur.a[k], cur.c[k], pd, cert);
+          if (SMOOTH)
+            cert = w1 * cxr[SMOOTH ? (p + 1) % 3 : 0][warp][k][lane] + w0 * cxr[SMOOTH ? (p + 2) % 3 : 0][warp][k][lane] +
+                   w1 * cxr[SMOOTH ? p % 3 : 0][warp][k][lane];  // planes z - 1, z, z + 1
+          const float g = phase_grad(ap[k], cur.a[k], am[k], cp[k], cur.c[k], cm[k]);
+          const float cg = cert * g;
+          const float wv = cg * g;
+          const float vv = cg * pd;
+          m[k][0] += wv;
+          m[k][1] += wv * zf;
+          m[k][2] += wv * zf * zf;
+          m[k][3] += vv;
+          m[k][4] += vv * zf;
+        }
+      }
+    }
+    // [D] rotate the plane registers
+    prev_a2 = cur.a[2];
+    prev_c2 = cur.c[2];
+    cur = nw;
+    if (p + 1 <= z1) nw = nxt;
+    __syncthreads();  // sxr and the qy slot of plane p - 1 are rewritten next step
+  }
+
+  // expand the column moments into the 42 sums (FP64), warp sums, block sum
+  const double xd = (double)xf, yd = (double)y - 0.5 * (double)(H - 1);
+#pragma unroll
+  for (int j = 0; j < kNSums; j++) {
+    const int k = j / 14, e = j % 14;
+    double v = 0.0;
+    if (out) {
+      const double s0 = m[k][0], sz = m[k][1], szz = m[k][2], v0 = m[k][3], vz = m[k][4];
+      switch (e) {
+        case 0: v = s0; break;
+        case 1: v = xd * s0; break;
+        case 2: v = yd * s0; break;
+        case 3: v = sz; break;
+        case 4: v = xd * xd * s0; break;
+        case 5: v = xd * yd * s0; break;
+        case 6: v = xd * sz; break;
+        case 7: v = yd * yd * s0; break;
+        case 8: v = yd * sz; break;
+        case 9: v = szz; break;
+        case 10: v = v0; break;
+        case 11: v = xd * v0; break;
+        case 12: v = yd * v0; break;
+        default: v = vz; break;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) s_part[warp][j] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < kNSums) {
+    double v = 0.0;
+#pragma unroll
+    for (int w = 0; w < kMarchWarps; w++) v += s_part[w][threadIdx.x];
     partials[((long long)b * gridDim.x + blockIdx.x) * kNSums + threadIdx.x] = v;
   }
 }
@@ -776,26 +880,41 @@ smooth_pass_kernel(const float* __restrict__ in, long long in_stride, const floa
 
 cudaError_t normal_eq_partials(const float* q1, long long q1_stride_floats, const float* q2, int W,
                                int H, int D, int batch, double* partials, int nblk, int zpb,
-                               const int* conv_iter, int it, cudaStream_t st, const float* cert,
-                               float cert_sigma) {
-  float w0 = 1.f, w1 = 0.f;
-  if (cert != nullptr) {
-    // 3-tap Gaussian, weights normalised to sum 1
-    const float e = (float)exp(-1.0 / (2.0 * (double)cert_sigma * (double)cert_sigma));
-    w0 = 1.0f / (1.0f + 2.0f * e);
-    w1 = e * w0;
-    const int ntx = (W - 6 + kCxyTX - 1) / kCxyTX, nty = (H - 6 + kCxyTY - 1) / kCxyTY;
-    if (W > 6 && H > 6 && D > 6) {
-      dim3 cgrid((unsigned)(ntx * nty), batch);
-      cert_xy_kernel<<<cgrid, kCxyTX * kCxyTY, 0, st>>>(reinterpret_cast<const float2*>(q1), q1_stride_floats / 2,
-                                                          reinterpret_cast<const float2*>(q2), W, H, D, ntx,
-                                                          const_cast<float*>(cert), conv_iter, it, w0, w1);
-    }
-  }
+                               const int* conv_iter, int it, cudaStream_t st) {
   dim3 grid(nblk, batch);
   normal_eq_partial_kernel<<<grid, kNEThreads, 0, st>>>(
       reinterpret_cast<const float2*>(q1), q1_stride_floats / 2, reinterpret_cast<const float2*>(q2),
-      W, H, D, zpb, partials, conv_iter, it, cert, w0, w1);
+      W, H, D, zpb, partials, conv_iter, it);
+  return cudaGetLastError();
+}
+
+int normal_eq_march_blocks(int W, int H, int D, int* ntx, int* nty, int* zs) {
+  const int nx = W - 6, ny = H - 6, nz = D - 6;
+  *ntx = nx > 0 ? (nx + kMarchCols - 1) / kMarchCols : 1;
+  *nty = ny > 0 ? (ny + 7) / 8 : 1;
+  const int nzs = nz > 0 ? (nz + kMarchZs - 1) / kMarchZs : 1;
+  *zs = nz > 0 ? (nz + nzs - 1) / nzs : 0;
+  return *ntx * *nty * nzs;
+}
+
+cudaError_t normal_eq_march(const float* q1, long long q1_stride_floats, const float* q2, int W, int H, int D,
+                            int batch, double* partials, int nblk, const int* conv_iter, int it, cudaStream_t st,
+                            float cert_sigma) {
+  int ntx, nty, zs;
+  if (normal_eq_march_blocks(W, H, D, &ntx, &nty, &zs) != nblk) return cudaErrorInvalidValue;
+  dim3 grid((unsigned)nblk, (unsigned)batch);
+  const float2* a = reinterpret_cast<const float2*>(q1);
+  const float2* c = reinterpret_cast<const float2*>(q2);
+  if (cert_sigma > 0.f) {
+    // 3-tap Gaussian, weights normalised to sum 1
+    const float e = (float)exp(-1.0 / (2.0 * (double)cert_sigma * (double)cert_sigma));
+    const float w0 = 1.0f / (1.0f + 2.0f * e), w1 = e * w0;
+    normal_eq_march_kernel<true><<<grid, kMarchWarps * 32, 0, st>>>(a, q1_stride_floats / 2, c, W, H, D, ntx, nty,
+                                                                     zs, partials, conv_iter, it, w0, w1);
+  } else {
+    normal_eq_march_kernel<false><<<grid, kMarchWarps * 32, 0, st>>>(a, q1_stride_floats / 2, c, W, H, D, ntx,
+                                                                      nty, zs, partials, conv_iter, it, 1.f, 0.f);
+  }
   return cudaGetLastError();
 }
 
