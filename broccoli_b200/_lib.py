@@ -86,6 +86,7 @@ _SIGS = {
     "brc_ctx_stream": ([_P], _P),
     "brc_ctx_synchronize": ([_P], _I),
     "brc_selftest_bounded_wait": ([_P, _I], _I),
+    "brc_selftest_phase_atan2": ([_P, _P, _P, _P, _LL], _I),
     "brc_ctx_workspace_bytes": ([_P], ctypes.c_size_t),
     "brc_ctx_kernel_launches": ([_P], ctypes.c_ulonglong),
     "brc_filter3d": ([_P, _P, _I, _I, _I, _I, _LL, _P, _I, _I, _P], _I),

@@ -94,6 +94,20 @@ class Context:
         self._bind_stream()
         _check(self, L.lib().brc_selftest_bounded_wait(self.handle, int(wait_ms)))
 
+    def phase_atan2(self, y: torch.Tensor, x: torch.Tensor) -> torch.Tensor:
+        """The arctangent of the phase kernels, element-wise on two float32
+        device tensors of one shape."""
+        for t in (y, x):
+            if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != torch.float32:
+                raise TypeError("phase_atan2: float32 CUDA tensors")
+        if y.shape != x.shape:
+            raise ValueError("phase_atan2: y and x differ in shape")
+        y, x = y.contiguous(), x.contiguous()
+        out = torch.empty_like(y)
+        self._bind_stream()
+        _check(self, L.lib().brc_selftest_phase_atan2(self.handle, _p(y), _p(x), _p(out), y.numel()))
+        return out
+
     # ---- kernels ---------------------------------------------------------
 
     def filter3d(self, vol: torch.Tensor, filters, precision: int = L.PREC_FP32) -> torch.Tensor:

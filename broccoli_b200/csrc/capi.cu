@@ -260,6 +260,16 @@ int brc_selftest_bounded_wait(brc_ctx* ctx, int wait_ms) {
   return BRC_OK;
 }
 
+int brc_selftest_phase_atan2(brc_ctx* ctx, const float* d_y, const float* d_x, float* d_out, long long n) {
+  BRC_CHECK_CTX(ctx);
+  if (n < 0 || (n > 0 && (!d_y || !d_x || !d_out)))
+    return ctx->fail(BRC_ERR_INVALID, "brc_selftest_phase_atan2: bad pointer or size");
+  cudaSetDevice(ctx->device);
+  BRC_TRY(ctx, brc::phase_atan2_eval(d_y, d_x, d_out, n, ctx->stream()), "phase_atan2");
+  ctx->launches += n > 0 ? 1 : 0;
+  return BRC_OK;
+}
+
 size_t brc_ctx_workspace_bytes(const brc_ctx* ctx) { return ctx ? ctx->workspace() : 0; }
 
 unsigned long long brc_ctx_kernel_launches(const brc_ctx* ctx) { return ctx ? ctx->launches : 0; }

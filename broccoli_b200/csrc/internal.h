@@ -37,6 +37,8 @@ cudaError_t rescale_linear(const float* src, int W, int H, int D, float* out, in
 cudaError_t smooth3d(const float* vol, int W, int H, int D, int batch, const float* fx,
                      const float* fy, const float* fz, const float* cert, const float* scert,
                      float* tmp1, float* tmp2, float* out, cudaStream_t st, int accumulate = 0);
+// out[i] = phase_atan2(y[i], x[i]) (the arctangent of the phase kernels).
+cudaError_t phase_atan2_eval(const float* y, const float* x, float* out, long long n, cudaStream_t st);
 cudaError_t multiply_mask(float* vols, const float* mask, long long V, int batch, cudaStream_t st);
 // nonlinear.cu
 cudaError_t tensor_norm_max(const float* t6, long long V, float* a11, unsigned int* maxbits,

@@ -78,10 +78,10 @@ nonlinear_ah_kernel(const float2* __restrict__ q1, const float2* __restrict__ q2
     const float2 a = __ldg(q1 + k * V + i), c = __ldg(q2 + k * V + i);
     const float qr = __fadd_rn(__fmul_rn(a.x, c.x), __fmul_rn(a.y, c.y));
     const float qi = __fadd_rn(-__fmul_rn(a.x, c.y), __fmul_rn(a.y, c.x));
-    const float pd = atan2f(qi, qr);
-    const float aqq = sqrtf(qr * qr + qi * qi);
-    const float cs = cosf(pd / 2.0f);
-    const float cert = sqrtf(aqq) * cs * cs;
+    const float pd = phase_atan2(qi, qr);
+    // sqrt|q1 q2*| cos^2(pd/2) with cos^2(pd/2) = (1 + qr/|q1 q2*|)/2
+    const float aqq = sqrt_approx(qr * qr + qi * qi);
+    const float cert = aqq > 0.f ? 0.5f * (aqq + qr) * rsqrtf(aqq) : 0.f;
     a11 += cert * tt11;
     a12 += cert * tt12;
     a13 += cert * tt13;

@@ -315,6 +315,14 @@ int brc_warp_field_backward(brc_ctx* ctx, const float* d_src, int W, int H, int 
  * context stays usable. */
 int brc_selftest_bounded_wait(brc_ctx* ctx, int wait_ms);
 
+/* Evaluates the four-quadrant arctangent that the phase-difference and
+ * phase-gradient kernels use (a polynomial fit with the hardware reciprocal
+ * in place of atan2f): d_out[i] = angle of (d_x[i], d_y[i]) for n >= 0
+ * device floats, so that its error can be checked against atan2.  No
+ * counterpart in the reference, whose kernels call OpenCL's atan2
+ * (kernelRegistration.cpp:173-382). */
+int brc_selftest_phase_atan2(brc_ctx* ctx, const float* d_y, const float* d_x, float* d_out, long long n);
+
 /* ---- device memory and host copies (for hosts without a CUDA runtime) --- */
 
 /* cudaMalloc / cudaFree on the context's device.  Replaces the clCreateBuffer
