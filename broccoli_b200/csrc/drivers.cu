@@ -120,14 +120,14 @@ static int nonlinear_scale(brc_ctx* ctx, const float* ref, float* aligned, const
   smoothing_taps(o->esigma, fe);
   smoothing_taps(o->dsigma, fd);
   FilterPath fp;
-  s = make_filter_path(ctx, filters6, 6, o->precision, W, H, D, &fp);
+  s = make_filter_path(ctx, filters6, 6, o->precision, W, H, D, 1, &fp);
   if (s != BRC_OK) return s;
   BRC_TRY(ctx, run_filter(fp, ref, W, H, D, 1, V, q1, nullptr, 0, st), "filter ref");
-  ctx->launches += 1;
+  ctx->launches += filter_launches(fp);
   BRC_TRY(ctx, cudaMemsetAsync(field, 0, sizeof(float) * 3 * V, st), "memset field");
   for (int it = 0; it < iterations; it++) {
     BRC_TRY(ctx, run_filter(fp, aligned, W, H, D, 1, V, q2, nullptr, 0, st), "filter");
-    ctx->launches += 1;
+    ctx->launches += filter_launches(fp);
     s = nonlinear_step(ctx, q1, q2, W, H, D, m36, dirs18, ft, fe, fd, o->solve_fp64, field);
     if (s != BRC_OK) return s;
     BRC_TRY(ctx, brc::warp_field(original, W, H, D, field, field + V, field + 2 * V, aligned, st), "warp");

@@ -37,6 +37,8 @@
 // CTAs per SM overlap one tile's staging/epilogue with the other's GEMMs.
 // Every wait is bounded (about 2 s); a CTA that gives up sets *err, still
 // waits (bounded) for its GEMMs and copies, frees its TMEM and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -363,6 +365,383 @@ filter3d_tc_kernel(const float* __restrict__ vol, int W, int H, int D, long long
   if (tid == 0 && (!ok || !dok)) atomicExch(err, 1);
 }
 
+// ---------------------------------------------------------------------------
+// Persistent form: one CTA per SM walks the tiles of the launch with its
+// warps specialised.  The input comes pre-converted (pack_windows_kernel)
+// so that a tile's B operand is eight TMA box loads, and two TMEM
+// accumulators let the epilogue of one tile run under the GEMMs of the next.
+//
+//   warp 0, lane 0   TMA loads of the packed input tile (two buffers)
+//   warp 1, lane 0   tcgen05.mma issue (the 3 split products of each stage)
+//   warp 2, lane 0   tap stages through the ring (cp.async.bulk)
+//   warps 4-7        epilogue: tcgen05.ld of TMEM lanes 32 (warp - 4) ..,
+//                    transpose through shared memory, 16-byte stores
+//
+// Packed layout (uint16 BF16): element e of row (b, part, xc, z, y) at
+// ((((b * 2 + part) * nxc + xc) * Dp + z) * H + y) * 16 + e is the
+// sample x = 10 xc - 3 + e of plane z, row y (part 0 the BF16 rounding of
+// the sample, part 1 the BF16 rounding of the remainder; zero outside the
+// volume, Dp = D rounded up to SP).  Its tensor map has five dimensions
+// (e: 16, y: H, plane parity: SP, plane pair: Dp / SP, (b, part, xc)), so
+// one box {8, Hp, 1, NQ / SP, 1} brings the 16-byte K-half rows of one plane
+// parity of a tile in the order (plane slot, row) the GEMMs read them.
+// ---------------------------------------------------------------------------
+
+struct PArgs {
+  int W, H, D, Dp, nxc, nyt, nzt, batch, nfilt, ntiles;
+  int nqp;                 // planes per parity in a tile (NQ / SP)
+  uint32_t in_off;         // shared offset of the input buffers
+  uint32_t e_off;          // shared offset of the epilogue transpose buffer
+  uint32_t bar_off;        // shared offset of the barriers
+  int ecols;               // accumulator columns per epilogue chunk
+};
+
+constexpr int kPThreads = 256;
+constexpr int kPRing = 8;
+constexpr uint32_t kPTmemCols = 512;  // two accumulators of up to 256 columns
+// barrier block: full_in, empty_in, acc_full, acc_empty (2 each), the ring's
+// full / empty (kPRing each), done; then the TMEM address and 6 flags
+constexpr int kPBarBytes = ((8 + 2 * kPRing + 1) * 8 + 4 + 6 * 4 + 15) / 16 * 16;
+
+__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            int c4, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+      "%5, %6}], [%7];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+// Tile t -> (b, zt, yt, xc), xc fastest.
+__device__ __forceinline__ void decode_tile(const PArgs& a, int t, int& b, int& zt, int& yt, int& xc) {
+  xc = t % a.nxc;
+  int r = t / a.nxc;
+  yt = r % a.nyt;
+  r /= a.nyt;
+  zt = r % a.nzt;
+  b = r / a.nzt;
+}
+
+__global__ void __launch_bounds__(kPThreads, 1)
+filter3d_tcp_kernel(const __grid_constant__ CUtensorMap tmap, const uint16_t* __restrict__ taps,
+                    float* __restrict__ out, const PArgs a, const Geometry g, const int* __restrict__ conv_iter,
+                    int it, int* __restrict__ err) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  uint8_t* ring = smem;
+  uint8_t* inb = smem + a.in_off;
+  float* E = reinterpret_cast<float*>(smem + a.e_off);
+  uint64_t* full_in = reinterpret_cast<uint64_t*>(smem + a.bar_off);
+  uint64_t* empty_in = full_in + 2;
+  uint64_t* acc_full = empty_in + 2;
+  uint64_t* acc_empty = acc_full + 2;
+  uint64_t* tfull = acc_empty + 2;
+  uint64_t* tempty = tfull + kPRing;
+  uint64_t* done = tempty + kPRing;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  // [0] tiles produced, [1] tiles consumed, [2] tap stages loaded, [3] consumed,
+  // [4] a wait gave up, [5] epilogue: accumulator ready
+  int* flags = reinterpret_cast<int*>(tmem_slot + 1);
+
+  const uint32_t rowbytes = 16u * (uint32_t)g.NR;  // one K half of one part of one buffer
+  const int nst = g.nstage;
+  const long long V = (long long)a.W * a.H * a.D;
+
+  if (tid == 0) {
+    for (int i = 0; i < 2; i++) {
+      mbar_init(&full_in[i], 1);
+      mbar_init(&empty_in[i], 1);
+      mbar_init(&acc_full[i], 1);
+      mbar_init(&acc_empty[i], 128);
+    }
+    for (int s = 0; s < kPRing; s++) {
+      mbar_init(&tfull[s], 1);
+      mbar_init(&tempty[s], 1);
+    }
+    mbar_init(done, 1);
+    for (int i = 0; i < 6; i++) flags[i] = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kPTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // ---- producer: packed input tiles by TMA
+    const uint32_t tx = 64u * (uint32_t)g.SP * (uint32_t)g.Hp * (uint32_t)a.nqp;
+    int i = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+      int b, zt, yt, xc;
+      decode_tile(a, t, b, zt, yt, xc);
+      if (instance_done(conv_iter, b, it)) continue;
+      const int buf = i & 1;
+      if (i >= 2 && !mbar_wait(&empty_in[buf], (uint32_t)((i >> 1) - 1) & 1u)) {
+        ok = false;
+        break;
+      }
+      mbar_expect_tx(&full_in[buf], tx);
+      const int z0 = zt * g.SP * g.J, y0 = yt * g.Ty;
+      for (int part = 0; part < 2; part++)
+        for (int kh = 0; kh < 2; kh++)
+          for (int p = 0; p < g.SP; p++) {
+            uint8_t* dst = inb + (uint32_t)((buf * 2 + part) * 2 + kh) * rowbytes + (uint32_t)(p * g.RP) * 16u;
+            const int gpar = g.SP == 2 ? ((p + 1) & 1) : 0;
+            const int zp0 = g.SP == 2 ? (z0 / 2 - 2 + p) : (z0 - 3);
+            tma_load_5d(dst, &tmap, 8 * kh, y0 - 3, gpar, zp0, (b * 2 + part) * a.nxc + xc, &full_in[buf]);
+          }
+      i++;
+    }
+    flags[0] = i;
+    if (!ok) flags[4] = 1;
+  } else if (warp == 1 && lane == 0) {
+    // ---- GEMM issue.  The descriptors are built once; a stage only adds
+    // offsets to their start-address fields (one 16-byte row = 1), so that
+    // the issuing thread spends its time in tcgen05.mma, not in address
+    // arithmetic (which delays every GEMM it precedes).
+    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(g.N >> 3) << 17) |
+                           ((uint32_t)(kM >> 4) << 24);
+    const uint64_t da0 = sdesc(smem_u32(ring), kM * 16, 128);  // slot 0, hi taps
+    const uint64_t db0 = sdesc(smem_u32(inb), rowbytes, 128);  // buffer 0, hi part, row 0
+    const uint64_t dslot = kStageBytes >> 4, dalo = kStageBytes >> 5;
+    const uint64_t dbuf = (4u * rowbytes) >> 4, dblo = (2u * rowbytes) >> 4;
+    const int ncq = nst / 7;
+    int i = 0, slot = 0;
+    uint32_t ph = 0, G = 0;
+    uint64_t ah = da0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < a.ntiles && ok; t += gridDim.x) {
+      int b, zt, yt, xc;
+      decode_tile(a, t, b, zt, yt, xc);
+      if (instance_done(conv_iter, b, it)) continue;
+      const int buf = i & 1, acc = i & 1;
+      if (!mbar_wait(&full_in[buf], (uint32_t)(i >> 1) & 1u) ||
+          (i >= 2 && !mbar_wait(&acc_empty[acc], (uint32_t)((i >> 1) - 1) & 1u))) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const uint64_t bh0 = db0 + (uint64_t)buf * dbuf;
+      const uint32_t dcol = tmem + (uint32_t)(acc * 256);
+      uint32_t accf = 0;
+      for (int cq = 0; cq < ncq && ok; cq++) {
+        // rows of input-plane offset c = cq - 3: parity array cq % SP, plane slot cq / SP
+        const uint64_t bh = bh0 + (uint64_t)((cq % g.SP) * g.RP + (cq / g.SP) * g.Hp), bl = bh + dblo;
+#pragma unroll
+        for (int dyq = 0; dyq < 7; dyq++) {
+          if (!mbar_wait(&tfull[slot], ph)) {
+            ok = false;
+            break;
+          }
+          mma_bf16(dcol, ah, bh + dyq, idesc, accf);
+          mma_bf16(dcol, ah, bl + dyq, idesc, 1u);
+          mma_bf16(dcol, ah + dalo, bh + dyq, idesc, 1u);
+          mma_commit(&tempty[slot]);
+          accf = 1u;
+          G++;
+          ah += dslot;
+          if (++slot == kPRing) {
+            slot = 0;
+            ph ^= 1u;
+            ah = da0;
+          }
+        }
+      }
+      if (!ok) break;
+      mma_commit(&empty_in[buf]);
+      mma_commit(&acc_full[acc]);
+      i++;
+    }
+    flags[1] = i;
+    flags[3] = (int)G;
+    if (!ok) flags[4] = 1;
+    mma_commit(done);
+    if (!mbar_wait(done, 0)) flags[4] = 1;
+  } else if (warp == 2 && lane == 0) {
+    // ---- tap stages
+    uint32_t G = 0, ph = 0;
+    int slot = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < a.ntiles && ok; t += gridDim.x) {
+      int b, zt, yt, xc;
+      decode_tile(a, t, b, zt, yt, xc);
+      if (instance_done(conv_iter, b, it)) continue;
+      const uint16_t* src = taps;
+      for (int s = 0; s < nst; s++, G++) {
+        // the slot's previous stage (G - kPRing) must have been consumed
+        if (G >= (uint32_t)kPRing && !mbar_wait(&tempty[slot], ph ^ 1u)) {
+          ok = false;
+          break;
+        }
+        mbar_expect_tx(&tfull[slot], kStageBytes);
+        bulk_load(ring + slot * kStageBytes, src, kStageBytes, &tfull[slot]);
+        src += kStageBytes / 2;
+        if (++slot == kPRing) {
+          slot = 0;
+          ph ^= 1u;
+        }
+      }
+    }
+    flags[2] = (int)G;
+    if (!ok) flags[4] = 1;
+  } else if (warp >= 4) {
+    // ---- epilogue
+    const int q = warp - 4;
+    const int r = q * 32 + lane;
+    int sp, f, xo;
+    bool rvalid;
+    if (g.SP == 2) {
+      sp = r >> 6;
+      const int rr = r & 63;
+      f = rr / kXo;
+      xo = rr - f * kXo;
+      rvalid = rr < 2 * a.nfilt * kXo;
+    } else {
+      sp = 0;
+      f = r / kXo;
+      xo = r - f * kXo;
+      rvalid = r < 2 * a.nfilt * kXo;
+    }
+    const int rowf = 20 * a.nfilt;
+    const int ke = (f >> 1) * 20 + xo * 2 + (f & 1);
+    const int et = tid - 128;
+    // stores: SP * nfilt * 5 = 30 16-byte pieces per accumulator column
+    // (plane s2, filter k, x pair); threads et < 120 take piece et % 30 of
+    // every fourth column, starting at column et / 30
+    const int piece = et % 30, cgrp = et / 30;
+    const int part = piece % 5, sk = piece / 5;
+    const int s2 = sk / a.nfilt, k = sk - s2 * a.nfilt;
+    const bool vec16 = ((a.W & 1) == 0) && ((V & 1) == 0) && ((reinterpret_cast<uintptr_t>(out) & 15) == 0);
+    int i = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+      int b, zt, yt, xc;
+      decode_tile(a, t, b, zt, yt, xc);
+      if (instance_done(conv_iter, b, it)) continue;
+      const int acc = i & 1;
+      // one thread waits and tells the other 127, so that all of them leave
+      // together if the wait gives up (they meet at named barriers below)
+      if (et == 0) flags[5] = mbar_wait(&acc_full[acc], (uint32_t)(i >> 1) & 1u) ? 1 : 0;
+      epi_sync();
+      const bool ready = *reinterpret_cast<volatile int*>(&flags[5]) != 0;
+      epi_sync();
+      if (!ready) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const int x0 = xc * kXo, y0 = yt * g.Ty, z0 = zt * g.SP * g.J;
+      const uint32_t lanecol = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * 256);
+      for (int cbase = 0; cbase < g.N; cbase += a.ecols) {
+        const int cend = cbase + a.ecols < g.N ? cbase + a.ecols : g.N;
+        for (int c0 = cbase; c0 < cend; c0 += 16) {
+          uint32_t v[16];
+          tmem_ld16(lanecol + (uint32_t)c0, v);
+          if (rvalid) {
+#pragma unroll
+            for (int e = 0; e < 16; e++) E[((c0 + e - cbase) * g.SP + sp) * rowf + ke] = __uint_as_float(v[e]);
+          }
+        }
+        if (cend >= g.N) {
+          // this accumulator is read out: the GEMMs of tile i + 2 may start
+          tc_fence_before();
+          mbar_arrive(&acc_empty[acc]);
+        }
+        epi_sync();
+        if (et < 120) {
+          int nl = cgrp;
+          int j = (cbase + nl) / g.Hp, yl = cbase + nl - j * g.Hp;
+          const int xs = x0 + 2 * part;
+          for (; nl < cend - cbase; nl += 4) {
+            const int z = z0 + j * g.SP + s2, y = y0 + yl;
+            if (j < g.J && yl < g.Ty && y < a.H && z < a.D && xs < a.W) {
+              const float4 qv = *reinterpret_cast<const float4*>(E + (nl * g.SP + s2) * rowf + k * 20 + part * 4);
+              float* dst = out + (((long long)b * a.nfilt + k) * V + ((long long)z * a.H + y) * a.W + xs) * 2;
+              if (xs + 1 < a.W && vec16) {
+                *reinterpret_cast<float4*>(dst) = qv;
+              } else {
+                *reinterpret_cast<float2*>(dst) = make_float2(qv.x, qv.y);
+                if (xs + 1 < a.W) *reinterpret_cast<float2*>(dst + 2) = make_float2(qv.z, qv.w);
+              }
+            }
+            yl += 4;  // Hp >= 7 > 4: at most one wrap
+            if (yl >= g.Hp) {
+              yl -= g.Hp;
+              j++;
+            }
+          }
+        }
+        epi_sync();
+      }
+      i++;
+    }
+    if (!ok) flags[4] = 1;
+  }
+
+  __syncthreads();
+  // a wait gave up somewhere: bounded drain of the copies nothing consumed
+  if (tid == 0)
+    for (int j = flags[1]; j < flags[0]; j++) mbar_wait(&full_in[j & 1], (uint32_t)(j >> 1) & 1u);
+  if (tid == 64)
+    for (int s = flags[3]; s < flags[2]; s++) mbar_wait(&tfull[s % kPRing], (uint32_t)(s / kPRing) & 1u);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kPTmemCols) : "memory");
+  if (tid == 0 && flags[4]) atomicExch(err, 1);
+}
+
+// One thread per packed row (b, xc, z, y), y fastest: the 16 samples of the
+// window, split into BF16 hi and lo.
+__global__ void pack_windows_kernel(const float* __restrict__ vol, long long vstride, int W, int H, int D, int Dp,
+                                    int nxc, uint4* __restrict__ packed, const int* __restrict__ conv_iter,
+                                    int it) {
+  const int b = blockIdx.y;
+  if (instance_done(conv_iter, b, it)) return;
+  const long long rows = (long long)nxc * Dp * H;
+  const float* src = vol + (long long)b * vstride;
+  for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < rows;
+       r += (long long)gridDim.x * blockDim.x) {
+    const int y = (int)(r % H);
+    const long long t = r / H;
+    const int z = (int)(t % Dp), xc = (int)(t / Dp);
+    const int xs = xc * kXo - 3;
+    const bool rowok = z < D;
+    const float* rp = src + ((long long)(rowok ? z : 0) * H + y) * W;
+    uint32_t ph[8], pl[8];
+#pragma unroll
+    for (int e = 0; e < 16; e += 2) {
+      const int xa = xs + e, xb = xs + e + 1;
+      const float va = (rowok && xa >= 0 && xa < W) ? __ldg(rp + xa) : 0.f;
+      const float vb = (rowok && xb >= 0 && xb < W) ? __ldg(rp + xb) : 0.f;
+      const __nv_bfloat16 ha = __float2bfloat16_rn(va), hb = __float2bfloat16_rn(vb);
+      const __nv_bfloat16 la = __float2bfloat16_rn(va - __bfloat162float(ha));
+      const __nv_bfloat16 lb = __float2bfloat16_rn(vb - __bfloat162float(hb));
+      ph[e / 2] = pack_bf16(ha, hb);
+      pl[e / 2] = pack_bf16(la, lb);
+    }
+    const long long hrow = (((long long)(b * 2) * nxc + xc) * Dp + z) * H + y;
+    const long long lrow = hrow + (long long)nxc * Dp * H;
+    packed[2 * hrow] = make_uint4(ph[0], ph[1], ph[2], ph[3]);
+    packed[2 * hrow + 1] = make_uint4(ph[4], ph[5], ph[6], ph[7]);
+    packed[2 * lrow] = make_uint4(pl[0], pl[1], pl[2], pl[3]);
+    packed[2 * lrow + 1] = make_uint4(pl[4], pl[5], pl[6], pl[7]);
+  }
+}
+
 // Self-test of the bounded wait and the error flag: thread 0 waits on an
 // mbarrier that nothing arrives on, gives up after limit_ns and sets *err,
 // as a CTA of filter3d_tc_kernel does when a wait runs out.
@@ -462,15 +841,19 @@ bool geometry_ok(const Geometry& g) {
 // Cost model of a tile shape: GEMM columns issued over the volume (tiles x
 // (N + 32), the 32 standing for a tile's staging and epilogue), x1.3 when
 // the tile leaves no room for a second CTA on the SM.
-static long long tile_cost(const Geometry& g, int H, int D) {
+static long long tile_cost(const Geometry& g, int H, int D, bool persistent) {
   const long long ny = (H + g.Ty - 1) / g.Ty;
   const long long nz = (D + g.SP * g.J - 1) / (g.SP * g.J);
+  if (persistent) return ny * nz * (g.N + 16);
   long long cost = ny * nz * (g.N + 32);
   if (g.smem > 113 * 1024) cost = cost * 13 / 10;
   return cost;
 }
 
-int candidate_tys(int nfilt, int H, int D, int* tys, int max_n) {
+int persistent_smem(const Geometry& g);
+bool persistent_ok(const Geometry& g);
+
+int candidate_tys(int nfilt, int H, int D, int* tys, int max_n, bool persistent) {
   // the cheapest tile height for each plane-group count J (ties to the
   // taller tile), then the max_n cheapest of those
   long long best_cost[kMaxN + 1];
@@ -480,8 +863,8 @@ int candidate_tys(int nfilt, int H, int D, int* tys, int max_n) {
   const int hi = H < kMaxN - 6 ? H : kMaxN - 6;
   for (int ty = hi; ty >= lo; ty--) {
     const Geometry g = make_geometry(nfilt, H, D, ty);
-    if (!geometry_ok(g)) continue;
-    const long long c = tile_cost(g, H, D);
+    if (persistent ? !persistent_ok(g) : !geometry_ok(g)) continue;
+    const long long c = tile_cost(g, H, D, persistent);
     if (best_ty[g.J] < 0 || c < best_cost[g.J]) {
       best_ty[g.J] = g.Ty;
       best_cost[g.J] = c;
@@ -499,9 +882,89 @@ int candidate_tys(int nfilt, int H, int D, int* tys, int max_n) {
   return n;
 }
 
-int pick_ty(int nfilt, int H, int D) {
+int pick_ty(int nfilt, int H, int D, bool persistent) {
   int ty = -1;
-  return candidate_tys(nfilt, H, D, &ty, 1) == 1 ? ty : -1;
+  return candidate_tys(nfilt, H, D, &ty, 1, persistent) == 1 ? ty : -1;
+}
+
+// ---- persistent form -------------------------------------------------------
+
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+static int g_num_sms = 0;
+
+static int dpad(int D, int SP) { return (D + SP - 1) / SP * SP; }
+
+size_t packed_bytes(int W, int H, int D, int batch, int nfilt) {
+  const int SP = stacked_planes(nfilt);
+  const long long nxc = (W + kXo - 1) / kXo;
+  return (size_t)batch * 2 * (size_t)nxc * (size_t)dpad(D, SP) * (size_t)H * 32u;
+}
+
+static int epi_cols() { return 64; }
+
+int persistent_smem(const Geometry& g) {
+  const int ebytes = epi_cols() * 6 * 20 * 4;  // SP * nfilt = 6 for both banks
+  const int need = kPRing * kStageBytes + 128 * g.NR + ebytes + kPBarBytes;
+  return need > 116 * 1024 ? need : 116 * 1024;  // one CTA (and 512 TMEM columns) per SM
+}
+
+bool persistent_ok(const Geometry& g) {
+  return g.Hp <= kMaxN && g.N >= 16 && g.N <= kMaxN && persistent_smem(g) <= 227 * 1024;
+}
+
+cudaError_t pack(const float* vol, int W, int H, int D, int batch, long long stride, int nfilt, uint16_t* packed,
+                 const int* conv_iter, int it, cudaStream_t st) {
+  if (batch <= 0 || batch > 65535 || (nfilt != 3 && nfilt != 6)) return cudaErrorInvalidValue;
+  const int SP = stacked_planes(nfilt);
+  const int nxc = (W + kXo - 1) / kXo, Dp = dpad(D, SP);
+  const long long rows = (long long)nxc * Dp * H;
+  long long nb = (rows + 255) / 256;
+  const long long cap = 4LL * (g_num_sms > 0 ? g_num_sms : 148);
+  if (nb > cap) nb = cap;
+  dim3 grid((unsigned)nb, (unsigned)batch);
+  pack_windows_kernel<<<grid, 256, 0, st>>>(vol, stride, W, H, D, Dp, nxc, reinterpret_cast<uint4*>(packed),
+                                            conv_iter, it);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_packed(const uint16_t* packed, int W, int H, int D, int batch, const uint16_t* d_taps, int nfilt,
+                          float* out, const int* conv_iter, int it, int* d_err, const Geometry& g, cudaStream_t st) {
+  if (!g_encode || g_num_sms <= 0) return cudaErrorInitializationError;
+  if (!persistent_ok(g) || (nfilt != 3 && nfilt != 6) || g.SP != stacked_planes(nfilt)) return cudaErrorInvalidValue;
+  if ((reinterpret_cast<uintptr_t>(packed) & 15) != 0 || batch <= 0) return cudaErrorInvalidValue;
+  PArgs a;
+  a.W = W;
+  a.H = H;
+  a.D = D;
+  a.Dp = dpad(D, g.SP);
+  a.nxc = (W + kXo - 1) / kXo;
+  a.nyt = (H + g.Ty - 1) / g.Ty;
+  a.nzt = (D + g.SP * g.J - 1) / (g.SP * g.J);
+  a.batch = batch;
+  a.nfilt = nfilt;
+  const long long ntiles = (long long)a.nxc * a.nyt * a.nzt * batch;
+  if (ntiles > 0x7fffffffLL || (long long)batch * 2 * a.nxc > 0x7fffffffLL) return cudaErrorInvalidValue;
+  a.ntiles = (int)ntiles;
+  a.nqp = (g.SP * g.J + 6) / g.SP;
+  a.ecols = epi_cols();
+  a.in_off = (uint32_t)(kPRing * kStageBytes);
+  a.e_off = a.in_off + 128u * (uint32_t)g.NR;
+  a.bar_off = a.e_off + (uint32_t)(a.ecols * 6 * 20 * 4);
+  const int smem = persistent_smem(g);
+
+  CUtensorMap map;
+  const cuuint64_t dims[5] = {16, (cuuint64_t)H, (cuuint64_t)g.SP, (cuuint64_t)(a.Dp / g.SP),
+                              (cuuint64_t)batch * 2 * (cuuint64_t)a.nxc};
+  const cuuint64_t strides[4] = {32, 32 * (cuuint64_t)H, 32 * (cuuint64_t)H * g.SP, 32 * (cuuint64_t)H * a.Dp};
+  const cuuint32_t box[5] = {8, (cuuint32_t)g.Hp, 1, (cuuint32_t)a.nqp, 1};
+  const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+  const CUresult cr = g_encode(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<uint16_t*>(packed), dims,
+                               strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (cr != CUDA_SUCCESS) return cudaErrorInvalidValue;
+  const int grid = a.ntiles < g_num_sms ? a.ntiles : g_num_sms;
+  filter3d_tcp_kernel<<<grid, kPThreads, smem, st>>>(map, d_taps, out, a, g, conv_iter, it, d_err);
+  return cudaGetLastError();
 }
 
 cudaError_t bounded_wait_probe(int wait_ms, int* d_err, cudaStream_t st) {
@@ -511,7 +974,21 @@ cudaError_t bounded_wait_probe(int wait_ms, int* d_err, cudaStream_t st) {
 }
 
 cudaError_t init() {
-  return cudaFuncSetAttribute(filter3d_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  cudaError_t e = cudaFuncSetAttribute(filter3d_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(filter3d_tcp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  if (e != cudaSuccess) return e;
+  int dev = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  if (!g_encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+    if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) return e != cudaSuccess ? e : cudaErrorNotSupported;
+    g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  return cudaSuccess;
 }
 
 cudaError_t launch(const float* vol, int W, int H, int D, int batch, long long stride, const uint16_t* d_taps,
