@@ -82,7 +82,7 @@ int brc_ctx::tune_tc(int nfilt, int W, int H, int D, const uint16_t* d_taps, int
     return BRC_OK;
   }
   int tys[3];
-  const int n = brc::tc::candidate_tys(nfilt, H, D, tys, 3, true);
+  const int n = brc::tc::candidate_tys(nfilt, H, D, tys, 3);
   if (n <= 0) return fail(BRC_ERR_UNSUPPORTED, "volume shape not supported by the BF16X3 filtering");
   *ty = tys[0];
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
@@ -97,10 +97,7 @@ int brc_ctx::tune_tc(int nfilt, int W, int H, int D, const uint16_t* d_taps, int
     BRC_TRY(this, cudaStreamSynchronize(stream()), "synchronize");
     BRC_TRY(this, tmp1.ensure(sizeof(float) * (size_t)(V * nb)), "alloc");
     BRC_TRY(this, tmp2.ensure(sizeof(float) * (size_t)(V * nb) * 2 * nfilt), "alloc");
-    BRC_TRY(this, packed.ensure(brc::tc::packed_bytes(W, H, D, (int)nb, nfilt)), "alloc");
     BRC_TRY(this, cudaMemsetAsync(tmp1.ptr, 0, sizeof(float) * (size_t)(V * nb), own_stream), "memset");
-    BRC_TRY(this, brc::tc::pack(tmp1.as<float>(), W, H, D, (int)nb, V, nfilt, packed.as<uint16_t>(), nullptr, 0,
-                                own_stream), "pack");
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     BRC_TRY(this, cudaEventCreate(&e0), "event");
     if (cudaEventCreate(&e1) != cudaSuccess) {
@@ -115,8 +112,8 @@ int brc_ctx::tune_tc(int nfilt, int W, int H, int D, const uint16_t* d_taps, int
       for (int rep = 0; rep < 4 && err == cudaSuccess; rep++) {
         err = cudaEventRecord(e0, own_stream);
         if (err == cudaSuccess)
-          err = brc::tc::launch_packed(packed.as<uint16_t>(), W, H, D, (int)nb, d_taps, nfilt, tmp2.as<float>(),
-                                       nullptr, 0, tc_err.as<int>(), g, own_stream);
+          err = brc::tc::launch(tmp1.as<float>(), W, H, D, (int)nb, V, d_taps, nfilt, tmp2.as<float>(), nullptr, 0,
+                                tc_err.as<int>(), g, own_stream);
         if (err == cudaSuccess) err = cudaEventRecord(e1, own_stream);
         if (err == cudaSuccess) err = cudaEventSynchronize(e1);
         float ms = 0.f;
@@ -137,7 +134,7 @@ int brc_ctx::tune_tc(int nfilt, int W, int H, int D, const uint16_t* d_taps, int
 }
 
 int make_filter_path(brc_ctx* ctx, const float* h_filters, int nfilt, int precision, int W, int H, int D,
-                     int batch, FilterPath* fp) {
+                     FilterPath* fp) {
   if (nfilt != 3 && nfilt != 6) return ctx->fail(BRC_ERR_INVALID, "filtering needs 3 or 6 filters");
   fp->precision = precision;
   fp->h_filters = h_filters;
@@ -152,22 +149,14 @@ int make_filter_path(brc_ctx* ctx, const float* h_filters, int nfilt, int precis
   st = ctx->tune_tc(nfilt, W, H, D, fp->d_taps, &ty);
   if (st != BRC_OK) return st;
   fp->g = brc::tc::make_geometry(nfilt, H, D, ty);
-  const size_t pb = brc::tc::packed_bytes(W, H, D, batch > 0 ? batch : 1, nfilt);
-  BRC_TRY(ctx, ctx->packed.ensure(pb), "alloc packed windows");
-  fp->d_packed = ctx->packed.as<uint16_t>();
-  fp->packed_cap = ctx->packed.bytes;
   return BRC_OK;
 }
 
 cudaError_t run_filter(const FilterPath& fp, const float* vol, int W, int H, int D, int batch, long long stride,
                        float* out, const int* conv_iter, int it, cudaStream_t st) {
-  if (fp.precision == BRC_PREC_BF16X3) {
-    if (!fp.d_packed || brc::tc::packed_bytes(W, H, D, batch, fp.nfilt) > fp.packed_cap) return cudaErrorInvalidValue;
-    const cudaError_t e = brc::tc::pack(vol, W, H, D, batch, stride, fp.nfilt, fp.d_packed, conv_iter, it, st);
-    if (e != cudaSuccess) return e;
-    return brc::tc::launch_packed(fp.d_packed, W, H, D, batch, fp.d_taps, fp.nfilt, out, conv_iter, it, fp.d_err,
-                                  fp.g, st);
-  }
+  if (fp.precision == BRC_PREC_BF16X3)
+    return brc::tc::launch(vol, W, H, D, batch, stride, fp.d_taps, fp.nfilt, out, conv_iter, it, fp.d_err, fp.g,
+                           st);
   return brc::filter3d_fp32(vol, W, H, D, batch, stride, fp.h_filters, fp.nfilt, out, conv_iter, it, st,
                             fp.precision == BRC_PREC_FP32);
 }
@@ -296,7 +285,7 @@ int brc_filter3d(brc_ctx* ctx, const float* d_vol, int W, int H, int D, int batc
     return ctx->fail(BRC_ERR_INVALID, "brc_filter3d: vol_stride smaller than a volume");
   cudaSetDevice(ctx->device);
   FilterPath fp;
-  const int ps = make_filter_path(ctx, h_filters, nfilt, precision, W, H, D, batch, &fp);
+  const int ps = make_filter_path(ctx, h_filters, nfilt, precision, W, H, D, &fp);
   if (ps != BRC_OK) return ps;
   BRC_TRY(ctx, run_filter(fp, d_vol, W, H, D, batch, vol_stride, d_out, nullptr, 0, ctx->stream()), "filter3d");
   ctx->launches += filter_launches(fp);
@@ -586,7 +575,7 @@ extern "C" int brc_register_linear_batched(brc_ctx* ctx, const float* d_ref, lon
   p.iters_ws = p.conv_iter + batch;
   p.status = p.iters_ws + batch;
   {
-    const int ps = make_filter_path(ctx, h_filters, 3, opts->precision, W, H, D, batch, &p.fpath);
+    const int ps = make_filter_path(ctx, h_filters, 3, opts->precision, W, H, D, &p.fpath);
     if (ps != BRC_OK) return ps;
   }
 
@@ -604,7 +593,7 @@ extern "C" int brc_register_linear_batched(brc_ctx* ctx, const float* d_ref, lon
              (uint64_t)p.aligned, (uint64_t)d_rotations, (uint64_t)d_iterations,
              (uint64_t)ctx->q1.ptr, (uint64_t)ctx->q2.ptr, (uint64_t)ctx->partials.ptr,
              (uint64_t)ctx->ctl.ptr, (uint64_t)opts->certainty_sigma_x100,
-             (uint64_t)opts->precision, (uint64_t)p.fpath.d_taps, (uint64_t)p.fpath.d_packed};
+             (uint64_t)opts->precision, (uint64_t)p.fpath.d_taps};
     auto itg = ctx->graphs.find(key);
     GraphEntry* ge = nullptr;
     if (itg == ctx->graphs.end()) {

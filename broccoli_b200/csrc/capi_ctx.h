@@ -71,7 +71,6 @@ struct brc_ctx {
   std::map<uint64_t, std::unique_ptr<DevBuf>> tc_taps;
   DevBuf tc_err;  // device int: a bounded wait of a tensor-core kernel gave up
   DevBuf smask;   // smoothed certainty of brc_smooth_normalized
-  DevBuf packed;  // BF16 windows of the volumes the tensor-core filtering reads
   // tensor-core tile height chosen by timing, per (nfilt, W, H, D)
   std::map<std::tuple<int, int, int, int>, int> tc_tuned;
 
@@ -127,14 +126,11 @@ struct FilterPath {
   const uint16_t* d_taps = nullptr;
   brc::tc::Geometry g{};
   int* d_err = nullptr;
-  uint16_t* d_packed = nullptr;  // BF16 window scratch of the persistent tensor-core form
-  size_t packed_cap = 0;         // its bytes
 };
-// batch: the most volumes one run_filter call of this path filters.
 int make_filter_path(brc_ctx* ctx, const float* h_filters, int nfilt, int precision, int W, int H, int D,
-                     int batch, FilterPath* fp);
-// Kernels one run_filter call launches (BF16X3: the window packing and the filtering).
-inline int filter_launches(const FilterPath& fp) { return fp.precision == BRC_PREC_BF16X3 ? 2 : 1; }
+                     FilterPath* fp);
+// Kernels one run_filter call launches.
+inline int filter_launches(const FilterPath&) { return 1; }
 cudaError_t run_filter(const FilterPath& fp, const float* vol, int W, int H, int D, int batch, long long stride,
                        float* out, const int* conv_iter, int it, cudaStream_t st);
 

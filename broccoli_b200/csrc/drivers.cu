@@ -120,7 +120,7 @@ static int nonlinear_scale(brc_ctx* ctx, const float* ref, float* aligned, const
   smoothing_taps(o->esigma, fe);
   smoothing_taps(o->dsigma, fd);
   FilterPath fp;
-  s = make_filter_path(ctx, filters6, 6, o->precision, W, H, D, 1, &fp);
+  s = make_filter_path(ctx, filters6, 6, o->precision, W, H, D, &fp);
   if (s != BRC_OK) return s;
   BRC_TRY(ctx, run_filter(fp, ref, W, H, D, 1, V, q1, nullptr, 0, st), "filter ref");
   ctx->launches += filter_launches(fp);

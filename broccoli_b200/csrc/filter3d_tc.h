@@ -13,7 +13,8 @@ constexpr int kK = 16;     // GEMM K: input samples along x per window
 constexpr int kXo = 10;    // outputs along x per window (kK - 6)
 constexpr int kMaxN = 256; // GEMM N limit (rows of one tile)
 
-// Tile geometry of one launch, chosen on the host.
+// Tile geometry of one launch, chosen on the host.  The kernel is
+// persistent (one CTA per SM over all tiles of the launch).
 struct Geometry {
   int SP;      // output planes stacked along M (2 for 3 filters, 1 for 6)
   int Ty;      // output rows along y per tile
@@ -23,7 +24,7 @@ struct Geometry {
   int RP;      // shared-memory rows per plane-parity array
   int NR;      // SP * RP
   int nstage;  // GEMMs per tile: (7 + SP - 1) * 7
-  int smem;    // dynamic shared memory bytes
+  int smem;    // dynamic shared memory bytes of a CTA
 };
 
 int stacked_planes(int nfilt);
@@ -37,22 +38,11 @@ Geometry make_geometry(int nfilt, int H, int D, int Ty);
 bool geometry_ok(const Geometry& g);
 // The max_n cheapest tile heights by the cost model, cheapest first; returns
 // how many were found.  pick_ty is the cheapest.
-// persistent: the cost model and shared-memory limit of the persistent form.
-int candidate_tys(int nfilt, int H, int D, int* tys, int max_n, bool persistent = false);
-int pick_ty(int nfilt, int H, int D, bool persistent = false);
+int candidate_tys(int nfilt, int H, int D, int* tys, int max_n);
+int pick_ty(int nfilt, int H, int D);
 cudaError_t init();
 // One CTA waits wait_ms (1..1000) on a barrier nothing completes, then sets *d_err.
 cudaError_t bounded_wait_probe(int wait_ms, int* d_err, cudaStream_t st);
-// Persistent form: pack() converts a batch of FP32 volumes into the
-// BF16 hi/lo window layout (packed_bytes of scratch) that launch_packed()
-// filters; one CTA per SM, two TMEM accumulators.
-size_t packed_bytes(int W, int H, int D, int batch, int nfilt);
-int persistent_smem(const Geometry& g);
-bool persistent_ok(const Geometry& g);
-cudaError_t pack(const float* vol, int W, int H, int D, int batch, long long stride, int nfilt, uint16_t* packed,
-                 const int* conv_iter, int it, cudaStream_t st);
-cudaError_t launch_packed(const uint16_t* packed, int W, int H, int D, int batch, const uint16_t* d_taps, int nfilt,
-                          float* out, const int* conv_iter, int it, int* d_err, const Geometry& g, cudaStream_t st);
 cudaError_t launch(const float* vol, int W, int H, int D, int batch, long long stride, const uint16_t* d_taps,
                    int nfilt, float* out, const int* conv_iter, int it, int* d_err, const Geometry& g,
                    cudaStream_t st);
