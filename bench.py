@@ -383,8 +383,11 @@ def run_gpu(args, rank, world, local_rank):
     # DRAM bytes (read + write) per filtered volume of 64x64x33 from one ncu
     # capture of each kernel on 63 volumes (profiles/filter3d_tc_motion_
     # correction.md, profiles/filter3d_sym_motion_correction.md), scaled to
-    # this launch by the volume count (traffic grows with the volumes)
-    tc_bytes_per_vol = (34574592 + 149403392) / 63
+    # this launch by the volume count (traffic grows with the volumes).  The
+    # tensor-core figure is below the algorithmic bytes: the input comes
+    # partly from L2 (written by the preceding resampling) and part of the
+    # output is still in L2 when the kernel ends.
+    tc_bytes_per_vol = (17850368 + 48461056) / 63
     sym_bytes_per_vol = (34094848 + 147386624) / 63
     traffic = sym_bytes_per_vol * (T - 1) if symmetric_bank(fl) and tuple(SHAPE) == (33, 64, 64) else None
     tc_traffic = tc_bytes_per_vol * (T - 1) if tuple(SHAPE) == (33, 64, 64) else None
