@@ -771,28 +771,29 @@ __device__ __forceinline__ float sample_linear(const float* __restrict__ T, int 
   const int r10 = yj1 * W + zk0 * WH;
   const int r01 = yj0 * W + zk1 * WH;
   const int r11 = yj1 * W + zk1 * WH;
-  return (1.f - a) * (1.f - bb) * (1.f - c) * __ldg(T + xi0 + r00) +
-         a * (1.f - bb) * (1.f - c) * __ldg(T + xi1 + r00) +
-         (1.f - a) * bb * (1.f - c) * __ldg(T + xi0 + r10) +
-         a * bb * (1.f - c) * __ldg(T + xi1 + r10) +
-         (1.f - a) * (1.f - bb) * c * __ldg(T + xi0 + r01) +
-         a * (1.f - bb) * c * __ldg(T + xi1 + r01) +
-         (1.f - a) * bb * c * __ldg(T + xi0 + r11) + a * bb * c * __ldg(T + xi1 + r11);
+  // trilinear weights applied as seven linear interpolations
+  const float t000 = __ldg(T + xi0 + r00), t100 = __ldg(T + xi1 + r00);
+  const float t010 = __ldg(T + xi0 + r10), t110 = __ldg(T + xi1 + r10);
+  const float t001 = __ldg(T + xi0 + r01), t101 = __ldg(T + xi1 + r01);
+  const float t011 = __ldg(T + xi0 + r11), t111 = __ldg(T + xi1 + r11);
+  const float c00 = fmaf(a, t100 - t000, t000), c10 = fmaf(a, t110 - t010, t010);
+  const float c01 = fmaf(a, t101 - t001, t001), c11 = fmaf(a, t111 - t011, t011);
+  const float c0 = fmaf(bb, c10 - c00, c00), c1 = fmaf(bb, c11 - c01, c01);
+  return fmaf(c, c1 - c0, c0);
 }
 
 // out_b(x) = src_b(x + t + (A - I)(x - centre)), params_b of instance b
 // (InterpolateVolumeLinearLinear, kernelRegistration.cpp:1066-1101).
 __global__ void __launch_bounds__(256)
-warp_affine_kernel(const float* __restrict__ src, long long src_stride, int W, int H, int D,
+warp_affine_kernel(const float* __restrict__ src, long long src_stride, int W, int H, int D, int ntx,
                    const float* __restrict__ params, float* __restrict__ out, long long out_stride,
                    const int* __restrict__ conv_iter, int it) {
-  const int b = blockIdx.y;
+  // block: 32 x 8 voxels of one plane; grid (x-y tiles, planes, instances)
+  const int b = blockIdx.z;
   if (instance_done(conv_iter, b, it)) return;
-  const int V = W * H * D;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= V) return;
-  const int r = i / W;
-  const int x = i - r * W, y = r % H, z = r / H;
+  const int ty = blockIdx.x / ntx, tx = blockIdx.x - ty * ntx;
+  const int x = tx * 32 + threadIdx.x, y = ty * 8 + threadIdx.y, z = blockIdx.y;
+  if (x >= W || y >= H) return;
   const float* p = params + (long long)b * 12;
   const float xf = (float)x - ((float)W - 1.0f) * 0.5f;
   const float yf = (float)y - ((float)H - 1.0f) * 0.5f;
@@ -800,7 +801,8 @@ warp_affine_kernel(const float* __restrict__ src, long long src_stride, int W, i
   const float u = (float)x + p[0] + p[3] * xf + p[4] * yf + p[5] * zf + 0.5f;
   const float v = (float)y + p[1] + p[6] * xf + p[7] * yf + p[8] * zf + 0.5f;
   const float w = (float)z + p[2] + p[9] * xf + p[10] * yf + p[11] * zf + 0.5f;
-  out[(long long)b * out_stride + i] = sample_linear(src + (long long)b * src_stride, W, H, D, u, v, w);
+  out[(long long)b * out_stride + ((long long)z * H + y) * W + x] =
+      sample_linear(src + (long long)b * src_stride, W, H, D, u, v, w);
 }
 
 // Displacement-field warp (InterpolateVolumeLinearNonLinear,
@@ -942,9 +944,11 @@ cudaError_t warp_affine(const float* src, long long src_stride, int W, int H, in
                         int it, cudaStream_t st) {
   const long long V = (long long)W * H * D;
   if (V > kMaxVoxels) return cudaErrorInvalidValue;
-  dim3 grid((unsigned)((V + 255) / 256), batch);
-  warp_affine_kernel<<<grid, 256, 0, st>>>(src, src_stride, W, H, D, params, out, out_stride,
-                                           conv_iter, it);
+  if (D > 65535 || batch > 65535) return cudaErrorInvalidValue;
+  const int ntx = (W + 31) / 32, nty = (H + 7) / 8;
+  dim3 grid((unsigned)(ntx * nty), (unsigned)D, (unsigned)batch);
+  warp_affine_kernel<<<grid, dim3(32, 8), 0, st>>>(src, src_stride, W, H, D, ntx, params, out, out_stride,
+                                                   conv_iter, it);
   return cudaGetLastError();
 }
 
