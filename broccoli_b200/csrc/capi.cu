@@ -656,15 +656,23 @@ extern "C" int brc_motion_correct(brc_ctx* ctx, float* h_volumes, int W, int H, 
   BRC_TRY(ctx, ctx->rot.ensure(sizeof(float) * 3 * batch), "alloc rot");
   float* d_series = ctx->series.as<float>();
   BRC_TRY(ctx, ctx->ensure_copy_streams(), "copy streams");
-  // Series of 64 or more volumes are registered in two chunks so that the
-  // upload of the second chunk and the download of the first run on the
-  // copy engines while a chunk registers.  (Measured on 199 volumes of
-  // 64x64x33: 1 chunk 29.2 ms, 2 chunks 27.5, 4 chunks 28.5, 8 chunks 31.3
-  // per call -- smaller batches lose more compute efficiency than the
-  // overlap gains.)  Chunk 0's upload includes the reference (volume 0, or
+  // Series of 64 or more volumes are registered in three chunks, a tenth,
+  // the rest and a tenth, so that only a small upload precedes the first
+  // registration and a small download follows the last, while the other
+  // copies run on the copy engines under registration.  (Measured per call
+  // on 199 volumes of 64x64x33: one chunk 18.3 ms, two equal chunks 16.9,
+  // 20/159/20 16.1, 30/139/30 16.3, 12/175/12 16.4, 20/80/79/20 16.6 --
+  // each chunk is a registration of its own, and small ones use the GPU
+  // less well.)  Chunk 0's upload includes the reference (volume 0, or
   // h_reference).
-  const int nchunk = batch >= 64 ? 2 : 1;
-  const int per = (batch + nchunk - 1) / nchunk;
+  int nchunk = 1, csz[3] = {batch, 0, 0};
+  if (batch >= 64) {
+    nchunk = 3;
+    csz[0] = csz[2] = batch / 10;
+    csz[1] = batch - 2 * csz[0];
+  }
+  int cst[4] = {0, 0, 0, 0};
+  for (int c = 0; c < nchunk; c++) cst[c + 1] = cst[c] + csz[c];
   // the copy streams start after work the caller queued before this call
   BRC_TRY(ctx, cudaEventRecord(ctx->ev_in, st), "event");
   BRC_TRY(ctx, cudaStreamWaitEvent(ctx->copy_in, ctx->ev_in, 0), "wait");
@@ -676,8 +684,8 @@ extern "C" int brc_motion_correct(brc_ctx* ctx, float* h_volumes, int W, int H, 
     d_ref = d_series + V * T;
   }
   for (int c = 0; c < nchunk; c++) {
-    const long long lo = c == 0 ? 0 : first + (long long)c * per;
-    const long long hi = std::min<long long>(T, first + (long long)(c + 1) * per);
+    const long long lo = c == 0 ? 0 : first + (long long)cst[c];
+    const long long hi = first + (long long)cst[c + 1];
     if (hi > lo)
       BRC_TRY(ctx, cudaMemcpyAsync(d_series + V * lo, h_volumes + V * lo, sizeof(float) * V * (hi - lo),
                                    cudaMemcpyHostToDevice, ctx->copy_in), "H2D");
@@ -686,8 +694,8 @@ extern "C" int brc_motion_correct(brc_ctx* ctx, float* h_volumes, int W, int H, 
   brc_linear_opts o = *opts;
   o.type = BRC_RIGID;
   for (int c = 0; c < nchunk; c++) {
-    const int i0 = c * per;
-    const int nb = std::min(batch, i0 + per) - i0;
+    const int i0 = cst[c];
+    const int nb = csz[c];
     BRC_TRY(ctx, cudaStreamWaitEvent(st, ctx->ev_chunk_in[c], 0), "wait");
     if (nb > 0) {
       int s = brc_register_linear_batched(ctx, d_ref, 0, d_series + V * (first + i0), W, H, D, nb, h_filters, &o,

@@ -83,8 +83,9 @@ def test_motion_correction_matches_golden(ctx, golden, lin_filters):
 
 @pytest.mark.parametrize("prec", [L.PREC_FP32, L.PREC_BF16X3])
 def test_chunked_host_motion_correction_equals_device_batch(ctx, lin_filters, prec):
-    """A 70-volume series goes through brc_motion_correct in two chunks with
-    overlapped copies; every volume's parameters and corrected volume equal
+    """A 70-volume series goes through brc_motion_correct in three chunks
+    (6 / 57 / 6 registrations) with overlapped copies; every volume's
+    parameters and corrected volume equal
     those of the device-resident batch of all 69 registrations (the
     instances are independent, so the split does not change any result)."""
     vols, _ = S.motion_series(T=70, shape=(13, 18, 20), snr=50.0)
