@@ -112,8 +112,8 @@ int brc_ctx::tune_tc(int nfilt, int W, int H, int D, const uint16_t* d_taps, int
       for (int rep = 0; rep < 4 && err == cudaSuccess; rep++) {
         err = cudaEventRecord(e0, own_stream);
         if (err == cudaSuccess)
-          err = brc::tc::launch(tmp1.as<float>(), W, H, D, (int)nb, V, d_taps, nfilt, tmp2.as<float>(), nullptr, 0,
-                                tc_err.as<int>(), g, own_stream);
+          err = brc::tc::launch(tmp1.as<float>(), W, H, D, (int)nb, V, d_taps, nfilt, tmp2.as<float>(),
+                                brc::all_instances(), tc_err.as<int>(), g, own_stream);
         if (err == cudaSuccess) err = cudaEventRecord(e1, own_stream);
         if (err == cudaSuccess) err = cudaEventSynchronize(e1);
         float ms = 0.f;
@@ -153,11 +153,10 @@ int make_filter_path(brc_ctx* ctx, const float* h_filters, int nfilt, int precis
 }
 
 cudaError_t run_filter(const FilterPath& fp, const float* vol, int W, int H, int D, int batch, long long stride,
-                       float* out, const int* conv_iter, int it, cudaStream_t st) {
+                       float* out, brc::ActiveSet act, cudaStream_t st) {
   if (fp.precision == BRC_PREC_BF16X3)
-    return brc::tc::launch(vol, W, H, D, batch, stride, fp.d_taps, fp.nfilt, out, conv_iter, it, fp.d_err, fp.g,
-                           st);
-  return brc::filter3d_fp32(vol, W, H, D, batch, stride, fp.h_filters, fp.nfilt, out, conv_iter, it, st,
+    return brc::tc::launch(vol, W, H, D, batch, stride, fp.d_taps, fp.nfilt, out, act, fp.d_err, fp.g, st);
+  return brc::filter3d_fp32(vol, W, H, D, batch, stride, fp.h_filters, fp.nfilt, out, act, st,
                             fp.precision == BRC_PREC_FP32);
 }
 
@@ -287,7 +286,8 @@ int brc_filter3d(brc_ctx* ctx, const float* d_vol, int W, int H, int D, int batc
   FilterPath fp;
   const int ps = make_filter_path(ctx, h_filters, nfilt, precision, W, H, D, &fp);
   if (ps != BRC_OK) return ps;
-  BRC_TRY(ctx, run_filter(fp, d_vol, W, H, D, batch, vol_stride, d_out, nullptr, 0, ctx->stream()), "filter3d");
+  BRC_TRY(ctx, run_filter(fp, d_vol, W, H, D, batch, vol_stride, d_out, brc::all_instances(), ctx->stream()),
+          "filter3d");
   ctx->launches += filter_launches(fp);
   return BRC_OK;
 }
@@ -303,7 +303,7 @@ int brc_normal_equations(brc_ctx* ctx, const float* d_q1, long long q1_stride, c
   const int nblk = (nint + zpb - 1) / zpb;
   BRC_TRY(ctx, ctx->partials.ensure(sizeof(double) * brc::kNSums * nblk * (size_t)batch), "alloc");
   BRC_TRY(ctx, brc::normal_eq_partials(d_q1, q1_stride, d_q2, W, H, D, batch,
-                                       ctx->partials.as<double>(), nblk, zpb, nullptr, 0, ctx->stream()),
+                                       ctx->partials.as<double>(), nblk, zpb, ctx->stream()),
           "normal_eq_partials");
   BRC_TRY(ctx, brc::assemble_normal_eq(ctx->partials.as<double>(), nblk, batch, d_A, d_h, ctx->stream()),
           "assemble");
@@ -328,7 +328,7 @@ int brc_warp_affine(brc_ctx* ctx, const float* d_src, int W, int H, int D, int b
   if (d_src == d_out) return ctx->fail(BRC_ERR_INVALID, "brc_warp_affine: in-place warp not supported");
   cudaSetDevice(ctx->device);
   const long long V = (long long)W * H * D;
-  BRC_TRY(ctx, brc::warp_affine(d_src, V, W, H, D, batch, d_params, d_out, V, nullptr, 0, ctx->stream()),
+  BRC_TRY(ctx, brc::warp_affine(d_src, V, W, H, D, batch, d_params, d_out, V, brc::all_instances(), ctx->stream()),
           "warp_affine");
   ctx->launches += 1;
   return BRC_OK;
@@ -466,7 +466,9 @@ struct RegPlan {
   int* conv_iter;
   int* iters_ws;
   int* status;
-  int nblk;  // partial rows per instance of the normal-equation kernel
+  int* lists;   // 3 x batch: active instances of iterations it % 3
+  int* counts;  // their lengths
+  int nblk;     // partial rows per instance of the normal-equation kernel
   FilterPath fpath;
 };
 
@@ -484,10 +486,12 @@ long long enqueue_registration(brc_ctx* ctx, const RegPlan& p, cudaStream_t st) 
   if ((e = cudaMemsetAsync(p.iters_ws, 0, sizeof(int) * p.batch, st)) != cudaSuccess)
     return ctx->cuda(e, "memset ctl");
   if ((e = cudaMemsetAsync(p.status, 0, sizeof(int), st)) != cudaSuccess) return ctx->cuda(e, "memset");
+  if ((e = brc::active_init(p.lists, p.counts, p.batch, st)) != cudaSuccess) return ctx->cuda(e, "active set");
+  kernels++;
   if (p.rotations && (e = cudaMemsetAsync(p.rotations, 0, sizeof(float) * 3 * p.batch, st)) != cudaSuccess)
     return ctx->cuda(e, "memset rot");
-  if ((e = run_filter(p.fpath, p.ref, p.W, p.H, p.D, ref_batch, p.ref_stride ? p.ref_stride : V, p.q1, nullptr,
-                      0, st)) != cudaSuccess)
+  if ((e = run_filter(p.fpath, p.ref, p.W, p.H, p.D, ref_batch, p.ref_stride ? p.ref_stride : V, p.q1,
+                      brc::all_instances(), st)) != cudaSuccess)
     return ctx->cuda(e, "filter3d(ref)");
   kernels += filter_launches(p.fpath);
   if (p.opts.iterations == 0 &&
@@ -496,18 +500,22 @@ long long enqueue_registration(brc_ctx* ctx, const RegPlan& p, cudaStream_t st) 
     return ctx->cuda(e, "copy");
   for (int it = 0; it < p.opts.iterations; it++) {
     const float* cur = it == 0 ? p.moving : p.aligned;
-    if ((e = run_filter(p.fpath, cur, p.W, p.H, p.D, p.batch, V, p.q2, p.conv_iter, it, st)) != cudaSuccess)
+    // iteration it works on list it % 3; its solve fills list (it + 1) % 3
+    // and empties list (it + 2) % 3 (the one iteration it - 1 used)
+    const int c0 = it % 3, c1 = (it + 1) % 3, c2 = (it + 2) % 3;
+    const brc::ActiveSet act{p.lists + (long long)c0 * p.batch, p.counts + c0};
+    if ((e = run_filter(p.fpath, cur, p.W, p.H, p.D, p.batch, V, p.q2, act, st)) != cudaSuccess)
       return ctx->cuda(e, "filter3d");
     if ((e = brc::normal_eq_march(p.q1, p.ref_stride ? 6 * V : 0, p.q2, p.W, p.H, p.D, p.batch, p.partials,
-                                  p.nblk, p.conv_iter, it, st, p.opts.certainty_sigma_x100 / 100.0f)) !=
-        cudaSuccess)
+                                  p.nblk, act, st, p.opts.certainty_sigma_x100 / 100.0f)) != cudaSuccess)
       return ctx->cuda(e, "normal_eq");
-    if ((e = brc::solve_update(p.partials, p.nblk, p.batch, p.opts.type, p.opts.tolerance, p.W, p.H,
-                               p.D, p.params, p.rotations, p.conv_iter, p.iters_ws, p.status, it,
-                               st)) != cudaSuccess)
+    if ((e = brc::solve_update(p.partials, p.nblk, p.batch, p.opts.type, p.opts.tolerance, p.W, p.H, p.D,
+                               p.params, p.rotations, p.conv_iter, p.iters_ws, p.status, it, act,
+                               p.lists + (long long)c1 * p.batch, p.counts + c1, p.counts + c2, st)) !=
+        cudaSuccess)
       return ctx->cuda(e, "solve");
-    if ((e = brc::warp_affine(p.moving, V, p.W, p.H, p.D, p.batch, p.params, p.aligned, V,
-                              p.conv_iter, it, st)) != cudaSuccess)
+    if ((e = brc::warp_affine(p.moving, V, p.W, p.H, p.D, p.batch, p.params, p.aligned, V, act, st)) !=
+        cudaSuccess)
       return ctx->cuda(e, "warp");
     kernels += 3 + filter_launches(p.fpath);
   }
@@ -565,7 +573,7 @@ extern "C" int brc_register_linear_batched(brc_ctx* ctx, const float* d_ref, lon
   BRC_TRY(ctx, ctx->q1.ensure(q1n), "alloc q1");
   BRC_TRY(ctx, ctx->q2.ensure(q2n), "alloc q2");
   BRC_TRY(ctx, ctx->partials.ensure(sizeof(double) * brc::kNSums * p.nblk * (size_t)batch), "alloc");
-  BRC_TRY(ctx, ctx->ctl.ensure(sizeof(int) * (2 * (size_t)batch + 4)), "alloc ctl");
+  BRC_TRY(ctx, ctx->ctl.ensure(sizeof(int) * (5 * (size_t)batch + 8)), "alloc ctl");
   if (!d_aligned) BRC_TRY(ctx, ctx->aligned.ensure(sizeof(float) * V * batch), "alloc aligned");
   p.aligned = d_aligned ? d_aligned : ctx->aligned.as<float>();
   p.q1 = ctx->q1.as<float>();
@@ -574,6 +582,8 @@ extern "C" int brc_register_linear_batched(brc_ctx* ctx, const float* d_ref, lon
   p.conv_iter = ctx->ctl.as<int>();
   p.iters_ws = p.conv_iter + batch;
   p.status = p.iters_ws + batch;
+  p.lists = p.status + 4;
+  p.counts = p.lists + 3 * (size_t)batch;
   {
     const int ps = make_filter_path(ctx, h_filters, 3, opts->precision, W, H, D, &p.fpath);
     if (ps != BRC_OK) return ps;

@@ -132,7 +132,7 @@ int make_filter_path(brc_ctx* ctx, const float* h_filters, int nfilt, int precis
 // Kernels one run_filter call launches.
 inline int filter_launches(const FilterPath&) { return 1; }
 cudaError_t run_filter(const FilterPath& fp, const float* vol, int W, int H, int D, int batch, long long stride,
-                       float* out, const int* conv_iter, int it, cudaStream_t st);
+                       float* out, brc::ActiveSet act, cudaStream_t st);
 
 #define BRC_CHECK_CTX(ctx) \
   do {                     \

@@ -22,18 +22,19 @@ struct FilterBank {
   float coef[kTaps * 2 * NF];
 };
 
-// Per-instance iteration control for batched registration.  An instance is
-// skipped by every kernel of iteration `it` once conv_iter[b] < it; the solve
-// kernel sets conv_iter[b] = it when that iteration's update fell below the
-// tolerance, so the warp of that iteration still runs.
-struct IterCtl {
-  int* conv_iter;   // [batch], INT_MAX while active
-  int* iterations;  // [batch], iterations run
+// The instances a kernel of the batched registration loop works on: the
+// first *count entries of list, written by the solve of the previous
+// iteration (instances whose update has not yet fallen below the
+// tolerance), or every instance 0 .. batch-1 when list is null.
+struct ActiveSet {
+  const int* list;
+  const int* count;
 };
 
-__device__ __forceinline__ bool instance_done(const int* conv_iter, int b, int it) {
-  return conv_iter != nullptr && __ldg(conv_iter + b) < it;
-}
+inline ActiveSet all_instances() { return ActiveSet{nullptr, nullptr}; }
+
+__device__ __forceinline__ int active_count(const ActiveSet& a, int batch) { return a.list ? *a.count : batch; }
+__device__ __forceinline__ int active_instance(const ActiveSet& a, int i) { return a.list ? a.list[i] : i; }
 
 // Four-quadrant arctangent of the phase kernels.  t = min(|x|,|y|) /
 // max(|x|,|y|) with the hardware reciprocal (rcp.approx, about 1 ulp), atan(t)

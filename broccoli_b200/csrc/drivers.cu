@@ -122,11 +122,11 @@ static int nonlinear_scale(brc_ctx* ctx, const float* ref, float* aligned, const
   FilterPath fp;
   s = make_filter_path(ctx, filters6, 6, o->precision, W, H, D, &fp);
   if (s != BRC_OK) return s;
-  BRC_TRY(ctx, run_filter(fp, ref, W, H, D, 1, V, q1, nullptr, 0, st), "filter ref");
+  BRC_TRY(ctx, run_filter(fp, ref, W, H, D, 1, V, q1, brc::all_instances(), st), "filter ref");
   ctx->launches += filter_launches(fp);
   BRC_TRY(ctx, cudaMemsetAsync(field, 0, sizeof(float) * 3 * V, st), "memset field");
   for (int it = 0; it < iterations; it++) {
-    BRC_TRY(ctx, run_filter(fp, aligned, W, H, D, 1, V, q2, nullptr, 0, st), "filter");
+    BRC_TRY(ctx, run_filter(fp, aligned, W, H, D, 1, V, q2, brc::all_instances(), st), "filter");
     ctx->launches += filter_launches(fp);
     s = nonlinear_step(ctx, q1, q2, W, H, D, m36, dirs18, ft, fe, fd, o->solve_fp64, field);
     if (s != BRC_OK) return s;
@@ -291,7 +291,7 @@ extern "C" int brc_register_two_volumes(brc_ctx* ctx, const float* d_in, int W, 
   float match[12] = {0};
   for (int k = 0; k < 3; k++) match[k] = -(float)myround(c2[k] - c1[k]);
   BRC_TRY(ctx, cudaMemcpyAsync(dparams, match, sizeof(match), cudaMemcpyHostToDevice, st), "H2D");
-  BRC_TRY(ctx, brc::warp_affine(w, V2, W2, H2, D2, 1, dparams, a, V2, nullptr, 0, st), "match");
+  BRC_TRY(ctx, brc::warp_affine(w, V2, W2, H2, D2, 1, dparams, a, V2, brc::all_instances(), st), "match");
   ctx->launches += 1;
   if (d_interpolated)
     BRC_TRY(ctx, cudaMemcpyAsync(d_interpolated, a, sizeof(float) * V2, cudaMemcpyDeviceToDevice, st), "copy");
@@ -440,8 +440,7 @@ extern "C" int brc_register_cohort(brc_ctx* ctx, int n, const float* const* d_su
     for (int k = 0; k < 3; k++) match[12 * b + k] = -(float)myround(ct[k] - cs[k]);
   }
   BRC_TRY(ctx, cudaMemcpyAsync(prm.ptr, match.data(), sizeof(float) * 12 * n, cudaMemcpyHostToDevice, st), "H2D");
-  BRC_TRY(ctx, brc::warp_affine(res.as<float>(), V2, W2, H2, D2, n, prm.as<float>(), mat.as<float>(), V2, nullptr,
-                                0, st),
+  BRC_TRY(ctx, brc::warp_affine(res.as<float>(), V2, W2, H2, D2, n, prm.as<float>(), mat.as<float>(), V2, brc::all_instances(), st),
           "match");
   ctx->launches += 1;
   // 3. affine stage of all subjects as one batched multi-scale registration
@@ -535,7 +534,7 @@ extern "C" int brc_register_linear_scales(brc_ctx* ctx, const float* d_ref, cons
       BRC_TRY(ctx, brc::rescale_batch(d_moving, W, H, D, batch, o_s, cw, ch, cd, 1.0f, st), "rescale");
     } else {
       BRC_TRY(ctx, brc::rescale_batch(d_moving, W, H, D, batch, m_s, cw, ch, cd, 1.0f, st), "rescale");
-      BRC_TRY(ctx, brc::warp_affine(m_s, vs, cw, ch, cd, batch, d_params, o_s, vs, nullptr, 0, st), "prewarp");
+      BRC_TRY(ctx, brc::warp_affine(m_s, vs, cw, ch, cd, batch, d_params, o_s, vs, brc::all_instances(), st), "prewarp");
       ctx->launches += 1;
     }
     ctx->launches += 2;
@@ -555,7 +554,7 @@ extern "C" int brc_register_linear_scales(brc_ctx* ctx, const float* d_ref, cons
       cd = myround((float)D / ((float)scale / 2.0f));
     }
   }
-  BRC_TRY(ctx, brc::warp_affine(d_moving, V, W, H, D, batch, d_params, d_aligned, V, nullptr, 0, st), "warp");
+  BRC_TRY(ctx, brc::warp_affine(d_moving, V, W, H, D, batch, d_params, d_aligned, V, brc::all_instances(), st), "warp");
   ctx->launches += 1;
   return BRC_OK;
 }

@@ -39,14 +39,14 @@ template <int NF, int R, int TZ>
 __global__ void __launch_bounds__(Filter3dCfg<NF, R, TZ>::kThreads)
 filter3d_fp32_kernel(const float* __restrict__ vol, int W, int H, int D, long long vol_stride,
                      const __grid_constant__ FilterBank<NF> bank, float* __restrict__ out,
-                     const int* __restrict__ conv_iter, int it) {
+                     const ActiveSet act) {
   using Cfg = Filter3dCfg<NF, R, TZ>;
   extern __shared__ __align__(16) float smem[];
   float* s_vol = smem;
   float* s_coef = smem + Cfg::kVolFloats;
 
-  const int b = blockIdx.z;
-  if (instance_done(conv_iter, b, it)) return;
+  if ((int)blockIdx.z >= active_count(act, (int)gridDim.z)) return;
+  const int b = active_instance(act, blockIdx.z);
   const int z_tiles = (D + TZ - 1) / TZ;
   const int tile_x0 = blockIdx.x * kTX;
   const int tile_y0 = (blockIdx.y / z_tiles) * kTY;
@@ -175,15 +175,15 @@ template <int NF, int R, int TZ>
 __global__ void __launch_bounds__(Filter3dCfg<NF, R, TZ>::kThreads)
 filter3d_sym_kernel(const float* __restrict__ vol, int W, int H, int D, long long vol_stride,
                     const __grid_constant__ SymBank<NF> bank, float* __restrict__ out,
-                    const int* __restrict__ conv_iter, int it) {
+                    const ActiveSet act) {
   using Cfg = Filter3dCfg<NF, R, TZ>;
   constexpr int kTapsSym = 24 * 7 + 4;
   extern __shared__ __align__(16) float smem[];
   float* s_vol = smem;
   float* s_coef = smem + Cfg::kVolFloats;  // kTapsSym x kCP
 
-  const int b = blockIdx.z;
-  if (instance_done(conv_iter, b, it)) return;
+  if ((int)blockIdx.z >= active_count(act, (int)gridDim.z)) return;
+  const int b = active_instance(act, blockIdx.z);
   const int z_tiles = (D + TZ - 1) / TZ;
   const int tile_x0 = blockIdx.x * kTX;
   const int tile_y0 = (blockIdx.y / z_tiles) * kTY;
@@ -380,25 +380,25 @@ static void pack_bank(const float* h_filters, FilterBank<NF>& bank) {
 
 template <int NF, int R, int TZ>
 static cudaError_t launch_fp32(const float* vol, int W, int H, int D, int batch, long long stride,
-                               const FilterBank<NF>& bank, float* out, const int* conv_iter, int it,
+                               const FilterBank<NF>& bank, float* out, ActiveSet act,
                                cudaStream_t st) {
   using Cfg = Filter3dCfg<NF, R, TZ>;
   const int z_tiles = (D + TZ - 1) / TZ;
   dim3 grid((W + kTX - 1) / kTX, ((H + kTY - 1) / kTY) * z_tiles, batch);
   filter3d_fp32_kernel<NF, R, TZ><<<grid, Cfg::kThreads, Cfg::kSmemBytes, st>>>(
-      vol, W, H, D, stride, bank, out, conv_iter, it);
+      vol, W, H, D, stride, bank, out, act);
   return cudaGetLastError();
 }
 
 template <int NF, int R, int TZ>
 static cudaError_t launch_sym(const float* vol, int W, int H, int D, int batch, long long stride,
-                              const SymBank<NF>& bank, float* out, const int* conv_iter, int it,
+                              const SymBank<NF>& bank, float* out, ActiveSet act,
                               cudaStream_t st) {
   using Cfg = Filter3dCfg<NF, R, TZ>;
   const int z_tiles = (D + TZ - 1) / TZ;
   dim3 grid((W + kTX - 1) / kTX, ((H + kTY - 1) / kTY) * z_tiles, batch);
   filter3d_sym_kernel<NF, R, TZ><<<grid, Cfg::kThreads, Cfg::kSmemBytes, st>>>(
-      vol, W, H, D, stride, bank, out, conv_iter, it);
+      vol, W, H, D, stride, bank, out, act);
   return cudaGetLastError();
 }
 
@@ -427,32 +427,32 @@ cudaError_t filter3d_init() {
 static int pick_tz(int D) { return (D % 4 != 0 && D % 3 == 0) ? 3 : 4; }
 
 cudaError_t filter3d_fp32(const float* vol, int W, int H, int D, int batch, long long stride,
-                          const float* h_filters, int nfilt, float* out, const int* conv_iter,
-                          int it, cudaStream_t st, bool allow_symmetric) {
+                          const float* h_filters, int nfilt, float* out, ActiveSet act, cudaStream_t st,
+                          bool allow_symmetric) {
   const int tz = pick_tz(D);
   if (allow_symmetric && nfilt == 3) {
     SymBank<3> sb;
     if (pack_sym_bank<3>(h_filters, sb))
-      return tz == 3 ? launch_sym<3, 8, 3>(vol, W, H, D, batch, stride, sb, out, conv_iter, it, st)
-                     : launch_sym<3, 8, 4>(vol, W, H, D, batch, stride, sb, out, conv_iter, it, st);
+      return tz == 3 ? launch_sym<3, 8, 3>(vol, W, H, D, batch, stride, sb, out, act, st)
+                     : launch_sym<3, 8, 4>(vol, W, H, D, batch, stride, sb, out, act, st);
   }
   if (allow_symmetric && nfilt == 6) {
     SymBank<6> sb;
     if (pack_sym_bank<6>(h_filters, sb))
-      return tz == 3 ? launch_sym<6, 4, 3>(vol, W, H, D, batch, stride, sb, out, conv_iter, it, st)
-                     : launch_sym<6, 4, 4>(vol, W, H, D, batch, stride, sb, out, conv_iter, it, st);
+      return tz == 3 ? launch_sym<6, 4, 3>(vol, W, H, D, batch, stride, sb, out, act, st)
+                     : launch_sym<6, 4, 4>(vol, W, H, D, batch, stride, sb, out, act, st);
   }
   if (nfilt == 3) {
     FilterBank<3> bank;
     pack_bank<3>(h_filters, bank);
-    return tz == 3 ? launch_fp32<3, 8, 3>(vol, W, H, D, batch, stride, bank, out, conv_iter, it, st)
-                   : launch_fp32<3, 8, 4>(vol, W, H, D, batch, stride, bank, out, conv_iter, it, st);
+    return tz == 3 ? launch_fp32<3, 8, 3>(vol, W, H, D, batch, stride, bank, out, act, st)
+                   : launch_fp32<3, 8, 4>(vol, W, H, D, batch, stride, bank, out, act, st);
   }
   if (nfilt == 6) {
     FilterBank<6> bank;
     pack_bank<6>(h_filters, bank);
-    return tz == 3 ? launch_fp32<6, 4, 3>(vol, W, H, D, batch, stride, bank, out, conv_iter, it, st)
-                   : launch_fp32<6, 4, 4>(vol, W, H, D, batch, stride, bank, out, conv_iter, it, st);
+    return tz == 3 ? launch_fp32<6, 4, 3>(vol, W, H, D, batch, stride, bank, out, act, st)
+                   : launch_fp32<6, 4, 4>(vol, W, H, D, batch, stride, bank, out, act, st);
   }
   return cudaErrorInvalidValue;
 }

@@ -176,27 +176,30 @@ __device__ __forceinline__ void stage_sync() { asm volatile("bar.sync 2, 128;" :
 
 struct TileArgs {
   long long vstride;       // floats between volumes
-  int W, H, D, nxc, nyt, nzt, nfilt, ntiles;
+  int W, H, D, nxc, nyt, nzt, nfilt, batch;
+  int tiles_per;           // tiles of one volume
   int nqp;                 // input plane slots per parity array: (SP J + 6) / SP
   uint32_t in_off;         // shared offsets: input buffers, epilogue buffer, barriers
   uint32_t e_off;
   uint32_t bar_off;
 };
 
-// Tile t -> (b, zt, yt, xc), xc fastest.
-__device__ __forceinline__ void decode_tile(const TileArgs& a, int t, int& b, int& zt, int& yt, int& xc) {
-  xc = t % a.nxc;
-  int r = t / a.nxc;
+// Tile t of the launch -> (instance b, zt, yt, xc), xc fastest; the
+// instances are those of the active set, in its order.
+__device__ __forceinline__ void decode_tile(const TileArgs& a, const ActiveSet& act, int t, int& b, int& zt,
+                                            int& yt, int& xc) {
+  const int li = t / a.tiles_per;
+  int r = t - li * a.tiles_per;
+  xc = r % a.nxc;
+  r /= a.nxc;
   yt = r % a.nyt;
-  r /= a.nyt;
-  zt = r % a.nzt;
-  b = r / a.nzt;
+  zt = r / a.nyt;
+  b = active_instance(act, li);
 }
 
 __global__ void __launch_bounds__(kThreads, 1)
 filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ taps, float* __restrict__ out,
-                   const TileArgs a, const Geometry g, const int* __restrict__ conv_iter, int it,
-                   int* __restrict__ err) {
+                   const TileArgs a, const Geometry g, const ActiveSet act, int* __restrict__ err) {
   extern __shared__ __align__(1024) uint8_t smem[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   uint8_t* ring = smem;
@@ -218,6 +221,8 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
   const uint32_t rowbytes = 16u * (uint32_t)g.NR;
   const int nst = g.nstage;
   const long long V = (long long)a.W * a.H * a.D;
+  // every role walks the same tiles: those of the active instances
+  const int ntiles = active_count(act, a.batch) * a.tiles_per;
 
   if (tid == 0) {
     for (int i = 0; i < 2; i++) {
@@ -254,10 +259,9 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
     const int nrows = g.SP * prow;   // staged rows per K half
     int i = 0;
     bool ok = true;
-    for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
       int b, zt, yt, xc;
-      decode_tile(a, t, b, zt, yt, xc);
-      if (instance_done(conv_iter, b, it)) continue;
+      decode_tile(a, act, t, b, zt, yt, xc);
       const int buf = i & 1;
       // one thread waits for the buffer and tells the others
       if (st == 0) flags[6] = (i < 2 || mbar_wait(&empty_in[buf], (uint32_t)((i >> 1) - 1) & 1u)) ? 1 : 0;
@@ -333,10 +337,9 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
     uint32_t ph = 0, G = 0;
     uint64_t ah = da0;
     bool ok = true;
-    for (int t = blockIdx.x; t < a.ntiles && ok; t += gridDim.x) {
+    for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
       int b, zt, yt, xc;
-      decode_tile(a, t, b, zt, yt, xc);
-      if (instance_done(conv_iter, b, it)) continue;
+      decode_tile(a, act, t, b, zt, yt, xc);
       const int buf = i & 1, acc = i & 1;
       if (!mbar_wait(&full_in[buf], (uint32_t)(i >> 1) & 1u) ||
           (i >= 2 && !mbar_wait(&acc_empty[acc], (uint32_t)((i >> 1) - 1) & 1u))) {
@@ -385,10 +388,9 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
     uint32_t G = 0, ph = 0;
     int slot = 0;
     bool ok = true;
-    for (int t = blockIdx.x; t < a.ntiles && ok; t += gridDim.x) {
+    for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
       int b, zt, yt, xc;
-      decode_tile(a, t, b, zt, yt, xc);
-      if (instance_done(conv_iter, b, it)) continue;
+      decode_tile(a, act, t, b, zt, yt, xc);
       const uint16_t* src = taps;
       for (int s = 0; s < nst; s++, G++) {
         // the slot's previous stage (G - kRing) must have been consumed
@@ -437,10 +439,9 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
     const bool vec16 = ((a.W & 1) == 0) && ((V & 1) == 0) && ((reinterpret_cast<uintptr_t>(out) & 15) == 0);
     int i = 0;
     bool ok = true;
-    for (int t = blockIdx.x; t < a.ntiles; t += gridDim.x) {
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
       int b, zt, yt, xc;
-      decode_tile(a, t, b, zt, yt, xc);
-      if (instance_done(conv_iter, b, it)) continue;
+      decode_tile(a, act, t, b, zt, yt, xc);
       const int acc = i & 1;
       // one thread waits and tells the other 127, so that all of them leave
       // together if the wait gives up (they meet at named barriers below)
@@ -677,8 +678,7 @@ cudaError_t init() {
 }
 
 cudaError_t launch(const float* vol, int W, int H, int D, int batch, long long stride, const uint16_t* d_taps,
-                   int nfilt, float* out, const int* conv_iter, int it, int* d_err, const Geometry& g,
-                   cudaStream_t st) {
+                   int nfilt, float* out, ActiveSet act, int* d_err, const Geometry& g, cudaStream_t st) {
   if (g_num_sms <= 0) return cudaErrorInitializationError;
   if (!geometry_ok(g) || (nfilt != 3 && nfilt != 6) || g.SP != stacked_planes(nfilt) || batch <= 0)
     return cudaErrorInvalidValue;
@@ -691,15 +691,16 @@ cudaError_t launch(const float* vol, int W, int H, int D, int batch, long long s
   a.nyt = (H + g.Ty - 1) / g.Ty;
   a.nzt = (D + g.SP * g.J - 1) / (g.SP * g.J);
   a.nfilt = nfilt;
+  a.batch = batch;
   const long long ntiles = (long long)a.nxc * a.nyt * a.nzt * batch;
   if (ntiles > 0x7fffffffLL) return cudaErrorInvalidValue;
-  a.ntiles = (int)ntiles;
+  a.tiles_per = a.nxc * a.nyt * a.nzt;
   a.nqp = (g.SP * g.J + 6) / g.SP;
   a.in_off = (uint32_t)(kRing * kStageBytes);
   a.e_off = a.in_off + 128u * (uint32_t)g.NR;
   a.bar_off = a.e_off + (uint32_t)kEpiBytes;
-  const int grid = a.ntiles < g_num_sms ? a.ntiles : g_num_sms;
-  filter3d_tc_kernel<<<grid, kThreads, g.smem, st>>>(vol, d_taps, out, a, g, conv_iter, it, d_err);
+  const int grid = ntiles < g_num_sms ? (int)ntiles : g_num_sms;
+  filter3d_tc_kernel<<<grid, kThreads, g.smem, st>>>(vol, d_taps, out, a, g, act, d_err);
   return cudaGetLastError();
 }
 

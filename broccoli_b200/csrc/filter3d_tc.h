@@ -5,6 +5,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include "common.cuh"
+
 namespace brc {
 namespace tc {
 
@@ -44,8 +46,7 @@ cudaError_t init();
 // One CTA waits wait_ms (1..1000) on a barrier nothing completes, then sets *d_err.
 cudaError_t bounded_wait_probe(int wait_ms, int* d_err, cudaStream_t st);
 cudaError_t launch(const float* vol, int W, int H, int D, int batch, long long stride, const uint16_t* d_taps,
-                   int nfilt, float* out, const int* conv_iter, int it, int* d_err, const Geometry& g,
-                   cudaStream_t st);
+                   int nfilt, float* out, ActiveSet act, int* d_err, const Geometry& g, cudaStream_t st);
 
 }  // namespace tc
 }  // namespace brc

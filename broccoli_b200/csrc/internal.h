@@ -3,33 +3,41 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "common.cuh"
+
 namespace brc {
 // filter3d.cu
 cudaError_t filter3d_init();
 cudaError_t filter3d_fp32(const float* vol, int W, int H, int D, int batch, long long stride,
-                          const float* h_filters, int nfilt, float* out, const int* conv_iter,
-                          int it, cudaStream_t st, bool allow_symmetric = true);
+                          const float* h_filters, int nfilt, float* out, ActiveSet act, cudaStream_t st,
+                          bool allow_symmetric = true);
 // registration.cu
 // Normal equations of batch instances, one CTA per `zpb` interior slices of
 // an instance (the single-call and allocation-free entry points).
 cudaError_t normal_eq_partials(const float* q1, long long q1_stride_floats, const float* q2, int W,
-                               int H, int D, int batch, double* partials, int nblk, int zpb,
-                               const int* conv_iter, int it, cudaStream_t st);
+                               int H, int D, int batch, double* partials, int nblk, int zpb, cudaStream_t st);
 // Normal equations in the z-marching form (certainty smoothing fused in when
 // cert_sigma > 0): partial rows per instance and the launch.
 int normal_eq_march_blocks(int W, int H, int D, int* ntx, int* nty, int* zs);
 cudaError_t normal_eq_march(const float* q1, long long q1_stride_floats, const float* q2, int W, int H, int D,
-                            int batch, double* partials, int nblk, const int* conv_iter, int it, cudaStream_t st,
+                            int batch, double* partials, int nblk, ActiveSet act, cudaStream_t st,
                             float cert_sigma);
 cudaError_t assemble_normal_eq(const double* partials, int nblk, int batch, double* A, double* h,
                                cudaStream_t st);
+// One iteration's solve and update of the instances in `act`; those whose
+// update is not yet below tol are appended to next_list / *next_count (and
+// conv_iter[b] = it records the others); *stale_count is reset for the
+// iteration after next.  Lists and counts may be null (no early exit).
 cudaError_t solve_update(const double* partials, int nblk, int batch, int type, float tol, int W,
                          int H, int D, float* params, float* rotations, int* conv_iter,
-                         int* iterations, int* status, int it, cudaStream_t st);
+                         int* iterations, int* status, int it, ActiveSet act, int* next_list,
+                         int* next_count, int* stale_count, cudaStream_t st);
+// list0[i] = i for i < batch, counts[0] = batch, counts[1] = counts[2] = 0.
+cudaError_t active_init(int* list0, int* counts, int batch, cudaStream_t st);
 cudaError_t solve_given(const double* A, const double* h, int batch, float* p, cudaStream_t st);
 cudaError_t warp_affine(const float* src, long long src_stride, int W, int H, int D, int batch,
-                        const float* params, float* out, long long out_stride, const int* conv_iter,
-                        int it, cudaStream_t st);
+                        const float* params, float* out, long long out_stride, ActiveSet act,
+                        cudaStream_t st);
 cudaError_t warp_field(const float* src, int W, int H, int D, const float* dx, const float* dy,
                        const float* dz, float* out, cudaStream_t st);
 cudaError_t rescale_linear(const float* src, int W, int H, int D, float* out, int W2, int H2, int D2,

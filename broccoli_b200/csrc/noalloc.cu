@@ -69,7 +69,7 @@ extern "C" int brc_normal_equations_noalloc(void* cuda_stream, const float* d_q1
   double* partials = nullptr;
   if (scratch_address(device, &partials) != cudaSuccess) return BRC_ERR_CUDA;
   cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
-  if (brc::normal_eq_partials(d_q1, q1_stride, d_q2, W, H, D, batch, partials, nblk, zpb, nullptr, 0, st) !=
+  if (brc::normal_eq_partials(d_q1, q1_stride, d_q2, W, H, D, batch, partials, nblk, zpb, st) !=
       cudaSuccess)
     return BRC_ERR_CUDA;
   if (brc::assemble_normal_eq(partials, nblk, batch, d_A, d_h, st) != cudaSuccess) return BRC_ERR_CUDA;

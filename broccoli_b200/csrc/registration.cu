@@ -96,9 +96,8 @@ __device__ __forceinline__ double zpow(double z, int e) {
 __global__ void __launch_bounds__(kNEThreads, 4)
 normal_eq_partial_kernel(const float2* __restrict__ q1, long long q1_stride,
                          const float2* __restrict__ q2, int W, int H, int D, int zpb,
-                         double* __restrict__ partials, const int* __restrict__ conv_iter, int it) {
+                         double* __restrict__ partials) {
   const int b = blockIdx.y;
-  if (instance_done(conv_iter, b, it)) return;
   const long long V = (long long)W * H * D;
   const long long WH = (long long)W * H;
   const float2* Q1 = q1 + (long long)b * q1_stride;
@@ -245,9 +244,9 @@ template <bool SMOOTH>
 __global__ void __launch_bounds__(kMarchWarps * 32, 2)
 normal_eq_march_kernel(const float2* __restrict__ q1, long long q1_stride, const float2* __restrict__ q2, int W,
                        int H, int D, int ntx, int nty, int zs, double* __restrict__ partials,
-                       const int* __restrict__ conv_iter, int it, float cw0, float cw1) {
-  const int b = blockIdx.y;
-  if (instance_done(conv_iter, b, it)) return;
+                       const ActiveSet act, float cw0, float cw1) {
+  if ((int)blockIdx.y >= active_count(act, (int)gridDim.y)) return;
+  const int b = active_instance(act, blockIdx.y);
   __shared__ float sxr[kMarchWarps][3][32];     // x-smoothed certainties of the newest plane
   // x/y-smoothed certainties of the last three planes (slot p % 3); each
   // thread reads back only its own entries, so no barrier guards them
@@ -644,10 +643,14 @@ __device__ double update_magnitude(const float* p, int W, int H, int D) {
 __global__ void solve_update_kernel(const double* __restrict__ partials, int nblk, int type,
                                     float tol, int W, int H, int D, float* __restrict__ params,
                                     float* __restrict__ rotations, int* __restrict__ conv_iter,
-                                    int* __restrict__ iterations, int* __restrict__ status, int it) {
+                                    int* __restrict__ iterations, int* __restrict__ status, int it,
+                                    const ActiveSet act, int* __restrict__ next_list,
+                                    int* __restrict__ next_count, int* __restrict__ stale_count) {
   __shared__ double s[kNSums];
-  const int b = blockIdx.x;
-  if (conv_iter != nullptr && conv_iter[b] < it) return;
+  // the list of iteration it + 2 is refilled by the next solve
+  if (blockIdx.x == 0 && threadIdx.x == 0 && stale_count) *stale_count = 0;
+  if ((int)blockIdx.x >= active_count(act, (int)gridDim.x)) return;
+  const int b = active_instance(act, blockIdx.x);
   reduce_partials(partials, nblk, b, s);
   if (threadIdx.x != 0) return;
   float p[12];
@@ -676,8 +679,18 @@ __global__ void solve_update_kernel(const double* __restrict__ partials, int nbl
   for (int i = 0; i < 12; i++) tot[i] = t[i];
   if (iterations) iterations[b] = it + 1;
   if (rotations && type == 1) rotation_angles(t, rotations + (long long)b * 3);
-  if (conv_iter != nullptr && tol > 0.f && update_magnitude(p, W, H, D) < (double)tol)
-    conv_iter[b] = it;
+  const bool converged = tol > 0.f && update_magnitude(p, W, H, D) < (double)tol;
+  if (converged && conv_iter != nullptr) conv_iter[b] = it;
+  if (!converged && next_list != nullptr) next_list[atomicAdd(next_count, 1)] = b;
+}
+
+__global__ void active_init_kernel(int* __restrict__ list0, int* __restrict__ counts, int batch) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < batch; i += gridDim.x * blockDim.x) list0[i] = i;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    counts[0] = batch;
+    counts[1] = 0;
+    counts[2] = 0;
+  }
 }
 
 // Plain solve of given A/h (brc_solve_affine_fp64): A column-major 12x12.
@@ -785,24 +798,27 @@ __device__ __forceinline__ float sample_linear(const float* __restrict__ T, int 
 // out_b(x) = src_b(x + t + (A - I)(x - centre)), params_b of instance b
 // (InterpolateVolumeLinearLinear, kernelRegistration.cpp:1066-1101).
 __global__ void __launch_bounds__(256)
-warp_affine_kernel(const float* __restrict__ src, long long src_stride, int W, int H, int D, int ntx,
+warp_affine_kernel(const float* __restrict__ src, long long src_stride, int W, int H, int D, int ntx, int batch,
                    const float* __restrict__ params, float* __restrict__ out, long long out_stride,
-                   const int* __restrict__ conv_iter, int it) {
-  // block: 32 x 8 voxels of one plane; grid (x-y tiles, planes, instances)
-  const int b = blockIdx.z;
-  if (instance_done(conv_iter, b, it)) return;
+                   const ActiveSet act) {
+  // block: 32 x 8 voxels of one plane; grid (x-y tiles, planes, a share of
+  // the instances: blockIdx.z, + gridDim.z, ...)
   const int ty = blockIdx.x / ntx, tx = blockIdx.x - ty * ntx;
   const int x = tx * 32 + threadIdx.x, y = ty * 8 + threadIdx.y, z = blockIdx.y;
   if (x >= W || y >= H) return;
-  const float* p = params + (long long)b * 12;
   const float xf = (float)x - ((float)W - 1.0f) * 0.5f;
   const float yf = (float)y - ((float)H - 1.0f) * 0.5f;
   const float zf = (float)z - ((float)D - 1.0f) * 0.5f;
-  const float u = (float)x + p[0] + p[3] * xf + p[4] * yf + p[5] * zf + 0.5f;
-  const float v = (float)y + p[1] + p[6] * xf + p[7] * yf + p[8] * zf + 0.5f;
-  const float w = (float)z + p[2] + p[9] * xf + p[10] * yf + p[11] * zf + 0.5f;
-  out[(long long)b * out_stride + ((long long)z * H + y) * W + x] =
-      sample_linear(src + (long long)b * src_stride, W, H, D, u, v, w);
+  const int n = active_count(act, batch);
+  for (int li = blockIdx.z; li < n; li += gridDim.z) {
+    const int b = active_instance(act, li);
+    const float* p = params + (long long)b * 12;
+    const float u = (float)x + p[0] + p[3] * xf + p[4] * yf + p[5] * zf + 0.5f;
+    const float v = (float)y + p[1] + p[6] * xf + p[7] * yf + p[8] * zf + 0.5f;
+    const float w = (float)z + p[2] + p[9] * xf + p[10] * yf + p[11] * zf + 0.5f;
+    out[(long long)b * out_stride + ((long long)z * H + y) * W + x] =
+        sample_linear(src + (long long)b * src_stride, W, H, D, u, v, w);
+  }
 }
 
 // Displacement-field warp (InterpolateVolumeLinearNonLinear,
@@ -881,12 +897,11 @@ smooth_pass_kernel(const float* __restrict__ in, long long in_stride, const floa
 // ---------------------------------------------------------------------------
 
 cudaError_t normal_eq_partials(const float* q1, long long q1_stride_floats, const float* q2, int W,
-                               int H, int D, int batch, double* partials, int nblk, int zpb,
-                               const int* conv_iter, int it, cudaStream_t st) {
+                               int H, int D, int batch, double* partials, int nblk, int zpb, cudaStream_t st) {
   dim3 grid(nblk, batch);
   normal_eq_partial_kernel<<<grid, kNEThreads, 0, st>>>(
       reinterpret_cast<const float2*>(q1), q1_stride_floats / 2, reinterpret_cast<const float2*>(q2),
-      W, H, D, zpb, partials, conv_iter, it);
+      W, H, D, zpb, partials);
   return cudaGetLastError();
 }
 
@@ -900,7 +915,7 @@ int normal_eq_march_blocks(int W, int H, int D, int* ntx, int* nty, int* zs) {
 }
 
 cudaError_t normal_eq_march(const float* q1, long long q1_stride_floats, const float* q2, int W, int H, int D,
-                            int batch, double* partials, int nblk, const int* conv_iter, int it, cudaStream_t st,
+                            int batch, double* partials, int nblk, ActiveSet act, cudaStream_t st,
                             float cert_sigma) {
   int ntx, nty, zs;
   if (normal_eq_march_blocks(W, H, D, &ntx, &nty, &zs) != nblk) return cudaErrorInvalidValue;
@@ -912,10 +927,10 @@ cudaError_t normal_eq_march(const float* q1, long long q1_stride_floats, const f
     const float e = (float)exp(-1.0 / (2.0 * (double)cert_sigma * (double)cert_sigma));
     const float w0 = 1.0f / (1.0f + 2.0f * e), w1 = e * w0;
     normal_eq_march_kernel<true><<<grid, kMarchWarps * 32, 0, st>>>(a, q1_stride_floats / 2, c, W, H, D, ntx, nty,
-                                                                     zs, partials, conv_iter, it, w0, w1);
+                                                                     zs, partials, act, w0, w1);
   } else {
     normal_eq_march_kernel<false><<<grid, kMarchWarps * 32, 0, st>>>(a, q1_stride_floats / 2, c, W, H, D, ntx,
-                                                                      nty, zs, partials, conv_iter, it, 1.f, 0.f);
+                                                                      nty, zs, partials, act, 1.f, 0.f);
   }
   return cudaGetLastError();
 }
@@ -928,9 +943,16 @@ cudaError_t assemble_normal_eq(const double* partials, int nblk, int batch, doub
 
 cudaError_t solve_update(const double* partials, int nblk, int batch, int type, float tol, int W,
                          int H, int D, float* params, float* rotations, int* conv_iter,
-                         int* iterations, int* status, int it, cudaStream_t st) {
+                         int* iterations, int* status, int it, ActiveSet act, int* next_list,
+                         int* next_count, int* stale_count, cudaStream_t st) {
   solve_update_kernel<<<batch, 64, 0, st>>>(partials, nblk, type, tol, W, H, D, params, rotations,
-                                            conv_iter, iterations, status, it);
+                                            conv_iter, iterations, status, it, act, next_list, next_count,
+                                            stale_count);
+  return cudaGetLastError();
+}
+
+cudaError_t active_init(int* list0, int* counts, int batch, cudaStream_t st) {
+  active_init_kernel<<<(batch + 255) / 256, 256, 0, st>>>(list0, counts, batch);
   return cudaGetLastError();
 }
 
@@ -940,15 +962,17 @@ cudaError_t solve_given(const double* A, const double* h, int batch, float* p, c
 }
 
 cudaError_t warp_affine(const float* src, long long src_stride, int W, int H, int D, int batch,
-                        const float* params, float* out, long long out_stride, const int* conv_iter,
-                        int it, cudaStream_t st) {
+                        const float* params, float* out, long long out_stride, ActiveSet act,
+                        cudaStream_t st) {
   const long long V = (long long)W * H * D;
   if (V > kMaxVoxels) return cudaErrorInvalidValue;
-  if (D > 65535 || batch > 65535) return cudaErrorInvalidValue;
+  if (D > 65535 || batch > 65535 || batch <= 0) return cudaErrorInvalidValue;
   const int ntx = (W + 31) / 32, nty = (H + 7) / 8;
-  dim3 grid((unsigned)(ntx * nty), (unsigned)D, (unsigned)batch);
-  warp_affine_kernel<<<grid, dim3(32, 8), 0, st>>>(src, src_stride, W, H, D, ntx, params, out, out_stride,
-                                                   conv_iter, it);
+  // at most 16 instance shares: a launch whose instances have mostly
+  // converged does not pay for blocks with nothing to do
+  dim3 grid((unsigned)(ntx * nty), (unsigned)D, (unsigned)(batch < 16 ? batch : 16));
+  warp_affine_kernel<<<grid, dim3(32, 8), 0, st>>>(src, src_stride, W, H, D, ntx, batch, params, out, out_stride,
+                                                   act);
   return cudaGetLastError();
 }
 

@@ -162,7 +162,9 @@ def test_kernel_launch_counter(ctx, lin_filters):
     before = ctx.kernel_launches
     ctx.register_linear(v, v[None], lin_filters, 4, L.AFFINE)
     torch.cuda.synchronize()
-    assert ctx.kernel_launches - before == 1 + 4 * 4
+    # active-set initialisation, reference filtering, 4 x (filter, normal
+    # equations, solve, warp)
+    assert ctx.kernel_launches - before == 2 + 4 * 4
 
 
 def test_certainty_smoothing_one_iteration_matches_oracle(ctx, orc, golden, lin_filters):
