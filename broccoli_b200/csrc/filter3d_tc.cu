@@ -36,8 +36,9 @@
 //   warp 1, lane 0 issues the tcgen05.mma's: three split products per stage,
 //                  descriptors built once and advanced by adds (every cycle
 //                  of address arithmetic in this thread delays the GEMMs)
-//   warp 2, lane 0 streams the packed taps of each stage (8 KB, hi + lo)
-//                  through an 8-slot ring with cp.async.bulk + mbarriers
+//   warp 2, lane 0 streams the packed taps, two stages (16 KB: hi + lo of
+//                  each) per slot, through a 4-slot ring with cp.async.bulk
+//                  + mbarriers (one wait and one commit per six GEMMs)
 //   warps 4-7      epilogue: tcgen05.ld of the accumulator (TMEM lanes
 //                  32 (warp - 4) ..), transposed through shared memory into
 //                  16-byte stores of the complex outputs
@@ -59,11 +60,13 @@ namespace tc {
 
 constexpr int kThreads = 384;        // 12 warps, roles above
 constexpr int kStageWarp = 8;        // first staging warp
-constexpr int kRing = 8;             // tap stages in flight
+constexpr int kRing = 4;             // tap slots in flight (two stages each)
 constexpr int kEpiCols = 64;         // accumulator columns per epilogue chunk
 constexpr uint32_t kTmemCols = 512;  // two accumulators of up to 256 columns
 constexpr int kStageHalves = kM * kK;              // BF16 elements of one A (hi or lo)
 constexpr int kStageBytes = 2 * kStageHalves * 2;  // hi + lo
+constexpr int kSlotBytes = 2 * kStageBytes;        // a ring slot: two stages
+constexpr int kSlotsPerTile = 28;                  // 7 dy x 4 pairs of input-plane offsets
 constexpr int kEpiBytes = kEpiCols * 6 * 20 * 4;   // SP * nfilt = 6 for both banks
 // barrier block: full_in, empty_in, acc_full, acc_empty (2 each), the ring's
 // full / empty (kRing each), done; then the TMEM address and 7 flags
@@ -219,7 +222,6 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
 
   // one K half of one part (hi or lo) of one input buffer: NR 16-byte rows
   const uint32_t rowbytes = 16u * (uint32_t)g.NR;
-  const int nst = g.nstage;
   const long long V = (long long)a.W * a.H * a.D;
   // every role walks the same tiles: those of the active instances
   const int ntiles = active_count(act, a.batch) * a.tiles_per;
@@ -330,9 +332,19 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
                            ((uint32_t)(kM >> 4) << 24);
     const uint64_t da0 = sdesc(smem_u32(ring), kM * 16, 128);  // slot 0, hi taps
     const uint64_t db0 = sdesc(smem_u32(inb), rowbytes, 128);  // buffer 0, hi part, row 0
-    const uint64_t dslot = kStageBytes >> 4, dalo = kStageBytes >> 5;
+    const uint64_t dslot = kSlotBytes >> 4, dstage = kStageBytes >> 4, dalo = kStageBytes >> 5;
     const uint64_t dbuf = (4u * rowbytes) >> 4, dblo = (2u * rowbytes) >> 4;
-    const int ncq = nst / 7;
+    // slot m of dy row dyq holds the taps of input-plane offsets cq = 2m and
+    // 2m + 1 (c = cq - 3); their B rows start at parity array cq % SP, plane
+    // slot cq / SP, row dyq.  The last slot's second stage (cq = 7) exists
+    // only with two stacked planes.
+    uint64_t offa[4], offb[4];
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+      offa[m] = (uint64_t)(((2 * m) % g.SP) * g.RP + ((2 * m) / g.SP) * g.Hp);
+      offb[m] = (uint64_t)(((2 * m + 1) % g.SP) * g.RP + ((2 * m + 1) / g.SP) * g.Hp);
+    }
+    const bool last_pair = g.SP == 2;
     int i = 0, slot = 0;
     uint32_t ph = 0, G = 0;
     uint64_t ah = da0;
@@ -350,20 +362,25 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
       const uint64_t bh0 = db0 + (uint64_t)buf * dbuf;
       const uint32_t dcol = tmem + (uint32_t)(acc * 256);
       uint32_t accf = 0;
-      for (int cq = 0; cq < ncq && ok; cq++) {
-        // rows of input-plane offset c = cq - 3: parity array cq % SP, plane slot cq / SP
-        const uint64_t bh = bh0 + (uint64_t)((cq % g.SP) * g.RP + (cq / g.SP) * g.Hp), bl = bh + dblo;
+      for (int dyq = 0; dyq < 7 && ok; dyq++) {
 #pragma unroll
-        for (int dyq = 0; dyq < 7; dyq++) {
+        for (int m = 0; m < 4; m++) {
           if (!mbar_wait(&tfull[slot], ph)) {
             ok = false;
             break;
           }
-          mma_bf16(dcol, ah, bh + dyq, idesc, accf);
-          mma_bf16(dcol, ah, bl + dyq, idesc, 1u);
-          mma_bf16(dcol, ah + dalo, bh + dyq, idesc, 1u);
-          mma_commit(&tempty[slot]);
+          const uint64_t b1 = bh0 + offa[m] + (uint64_t)dyq;
+          mma_bf16(dcol, ah, b1, idesc, accf);
+          mma_bf16(dcol, ah, b1 + dblo, idesc, 1u);
+          mma_bf16(dcol, ah + dalo, b1, idesc, 1u);
           accf = 1u;
+          if (m < 3 || last_pair) {
+            const uint64_t b2 = bh0 + offb[m] + (uint64_t)dyq, a2 = ah + dstage;
+            mma_bf16(dcol, a2, b2, idesc, 1u);
+            mma_bf16(dcol, a2, b2 + dblo, idesc, 1u);
+            mma_bf16(dcol, a2 + dalo, b2, idesc, 1u);
+          }
+          mma_commit(&tempty[slot]);
           G++;
           ah += dslot;
           if (++slot == kRing) {
@@ -392,15 +409,15 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
       int b, zt, yt, xc;
       decode_tile(a, act, t, b, zt, yt, xc);
       const uint16_t* src = taps;
-      for (int s = 0; s < nst; s++, G++) {
-        // the slot's previous stage (G - kRing) must have been consumed
+      for (int s = 0; s < kSlotsPerTile; s++, G++) {
+        // the slot's previous pair (G - kRing) must have been consumed
         if (G >= (uint32_t)kRing && !mbar_wait(&tempty[slot], ph ^ 1u)) {
           ok = false;
           break;
         }
-        mbar_expect_tx(&tfull[slot], kStageBytes);
-        bulk_load(ring + slot * kStageBytes, src, kStageBytes, &tfull[slot]);
-        src += kStageBytes / 2;
+        mbar_expect_tx(&tfull[slot], kSlotBytes);
+        bulk_load(ring + slot * kSlotBytes, src, kSlotBytes, &tfull[slot]);
+        src += kSlotBytes / 2;
         if (++slot == kRing) {
           slot = 0;
           ph ^= 1u;
@@ -546,44 +563,52 @@ static float bf16_to_f(uint16_t h) {
 
 int stacked_planes(int nfilt) { return nfilt == 3 ? 2 : 1; }
 int num_stages(int nfilt) { return (7 + stacked_planes(nfilt) - 1) * 7; }
-size_t packed_tap_bytes(int nfilt) { return (size_t)num_stages(nfilt) * kStageBytes; }
+size_t packed_tap_bytes(int nfilt) {
+  (void)nfilt;
+  return (size_t)kSlotsPerTile * kSlotBytes;
+}
 
+// Stage (input-plane offset c = cq - 3, dy = dyq - 3) goes to ring slot
+// dyq * 4 + cq / 2, half cq % 2; each half is hi (kM x 16 BF16) then lo, as
+// two K-major 8-row x 16-byte core-matrix blocks.  Halves without a stage
+// (cq = 7 with one stacked plane) stay zero.
 void pack_taps(const float* h_filters, int nfilt, uint16_t* dst) {
   const int SP = stacked_planes(nfilt);
-  const int nst = num_stages(nfilt);
-  memset(dst, 0, (size_t)nst * kStageBytes);
-  for (int st = 0; st < nst; st++) {
-    const int c = st / 7 - 3, dy = st % 7 - 3;
-    uint16_t* hi = dst + (size_t)st * 2 * kStageHalves;
-    uint16_t* lo = hi + kStageHalves;
-    for (int r = 0; r < kM; r++) {
-      int s, f, xo;
-      if (SP == 2) {
-        s = r >> 6;
-        const int rr = r & 63;
-        if (rr >= 2 * nfilt * kXo) continue;
-        f = rr / kXo;
-        xo = rr % kXo;
-      } else {
-        s = 0;
-        if (r >= 2 * nfilt * kXo) continue;
-        f = r / kXo;
-        xo = r % kXo;
-      }
-      const int dz = c - s;
-      if (dz < -3 || dz > 3) continue;
-      const float* F = h_filters + (size_t)(f >> 1) * kFilterFloats + (f & 1) * kTaps;
-      for (int kx = xo; kx <= xo + 6; kx++) {
-        const int dx = kx - 3 - xo;
-        const float w = F[(3 - dz) * 49 + (3 - dy) * 7 + (3 - dx)];
-        const uint16_t wh = bf16_rn(w);
-        const uint16_t wl = bf16_rn(w - bf16_to_f(wh));
-        const size_t e = (size_t)(kx / 8) * (kM * 8) + (size_t)r * 8 + (kx % 8);
-        hi[e] = wh;
-        lo[e] = wl;
+  const int ncq = 6 + SP;
+  memset(dst, 0, packed_tap_bytes(nfilt));
+  for (int cq = 0; cq < ncq; cq++)
+    for (int dyq = 0; dyq < 7; dyq++) {
+      const int c = cq - 3, dy = dyq - 3;
+      uint16_t* hi = dst + ((size_t)(dyq * 4 + cq / 2) * 2 + (cq & 1)) * 2 * kStageHalves;
+      uint16_t* lo = hi + kStageHalves;
+      for (int r = 0; r < kM; r++) {
+        int s, f, xo;
+        if (SP == 2) {
+          s = r >> 6;
+          const int rr = r & 63;
+          if (rr >= 2 * nfilt * kXo) continue;
+          f = rr / kXo;
+          xo = rr % kXo;
+        } else {
+          s = 0;
+          if (r >= 2 * nfilt * kXo) continue;
+          f = r / kXo;
+          xo = r % kXo;
+        }
+        const int dz = c - s;
+        if (dz < -3 || dz > 3) continue;
+        const float* F = h_filters + (size_t)(f >> 1) * kFilterFloats + (f & 1) * kTaps;
+        for (int kx = xo; kx <= xo + 6; kx++) {
+          const int dx = kx - 3 - xo;
+          const float w = F[(3 - dz) * 49 + (3 - dy) * 7 + (3 - dx)];
+          const uint16_t wh = bf16_rn(w);
+          const uint16_t wl = bf16_rn(w - bf16_to_f(wh));
+          const size_t e = (size_t)(kx / 8) * (kM * 8) + (size_t)r * 8 + (kx % 8);
+          hi[e] = wh;
+          lo[e] = wl;
+        }
       }
     }
-  }
 }
 
 static int g_num_sms = 0;
@@ -592,7 +617,7 @@ static int g_num_sms = 0;
 // lo, two K halves each), epilogue transpose buffer, barriers; at least
 // 116 KB, so that one CTA (and its 512 TMEM columns) is alone on its SM.
 static int smem_bytes(int NR) {
-  const int need = kRing * kStageBytes + 128 * NR + kEpiBytes + kBarBytes;
+  const int need = kRing * kSlotBytes + 128 * NR + kEpiBytes + kBarBytes;
   return need > 116 * 1024 ? need : 116 * 1024;
 }
 
@@ -696,7 +721,7 @@ cudaError_t launch(const float* vol, int W, int H, int D, int batch, long long s
   if (ntiles > 0x7fffffffLL) return cudaErrorInvalidValue;
   a.tiles_per = a.nxc * a.nyt * a.nzt;
   a.nqp = (g.SP * g.J + 6) / g.SP;
-  a.in_off = (uint32_t)(kRing * kStageBytes);
+  a.in_off = (uint32_t)(kRing * kSlotBytes);
   a.e_off = a.in_off + 128u * (uint32_t)g.NR;
   a.bar_off = a.e_off + (uint32_t)kEpiBytes;
   const int grid = ntiles < g_num_sms ? (int)ntiles : g_num_sms;
