@@ -25,6 +25,7 @@ BRC_ERR_NONFINITE = -7
 
 TRANSLATION, RIGID, AFFINE = 0, 1, 2
 PREC_FP32, PREC_BF16X3, PREC_FP32_GENERAL = 0, 1, 2
+INTERP_NEAREST, INTERP_LINEAR, INTERP_CUBIC = 0, 1, 2
 
 
 class BrcError(RuntimeError):
@@ -111,6 +112,11 @@ _SIGS = {
         [_P, _P, _P, _I, _I, _I, _P, _P, _P, ctypes.POINTER(NonlinearOpts), _P, _P], _I),
     "brc_change_resolution_and_size": ([_P, _P, _I, _I, _I, _P, _P, _I, _I, _I, _P, _I], _I),
     "brc_center_of_mass": ([_P, _P, _I, _I, _I, _P], _I),
+    "brc_change_resolution_and_size_batch": ([_P, _P, _I, _I, _I, _I, _P, _P, _I, _I, _I, _P, _I, _I], _I),
+    "brc_transform_volumes_linear": ([_P, _P, _I, _I, _I, _I, _P, _I, _P], _I),
+    "brc_transform_volumes_nonlinear": ([_P, _P, _I, _I, _I, _I, _P, _P, _P, _I, _P], _I),
+    "brc_combine_displacement_field": ([_P, _P, _P, _P, _I, _I, _I, _P], _I),
+    "brc_center_volumes": ([_P, _P, _I, _I, _I, _I, _I, _P, _P], _I),
     "brc_two_volume_opts_default": ([ctypes.POINTER(TwoVolumeOpts)], None),
     "brc_register_two_volumes": (
         [_P, _P, _I, _I, _I, _P, _P, _I, _I, _I, _P, _P, _P, _P, _P, ctypes.POINTER(TwoVolumeOpts), _P, _P,

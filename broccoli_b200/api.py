@@ -318,6 +318,84 @@ class Context:
             nvs.ctypes.data_as(ctypes.c_void_p), mm_z_cut))
         return out
 
+    # ---- 4D transforms (NEAREST = 0, LINEAR = 1) ------------------------------
+
+    @staticmethod
+    def _vols4(t: torch.Tensor) -> torch.Tensor:
+        if not isinstance(t, torch.Tensor) or not t.is_cuda or t.dtype != torch.float32:
+            raise TypeError("volumes must be float32 CUDA tensors")
+        if t.dim() == 3:
+            t = t.unsqueeze(0)
+        if t.dim() != 4:
+            raise ValueError("volumes must be (D,H,W) or (T,D,H,W)")
+        return t.contiguous()
+
+    def change_resolution_and_size_batch(self, src: torch.Tensor, voxel_size, shape, new_voxel_size,
+                                         mm_z_cut: int = 0, interpolation: int = L.INTERP_LINEAR) -> torch.Tensor:
+        """ChangeVolumesResolutionAndSize of (T, D, H, W) volumes onto a
+        (D2, H2, W2) grid; returns (T, D2, H2, W2)."""
+        v = self._vols4(src)
+        T, D, H, W = v.shape
+        D2, H2, W2 = shape
+        out = torch.empty((T, D2, H2, W2), dtype=torch.float32, device=v.device)
+        vs = np.ascontiguousarray(voxel_size, np.float32)
+        nvs = np.ascontiguousarray(new_voxel_size, np.float32)
+        self._bind_stream()
+        _check(self, L.lib().brc_change_resolution_and_size_batch(
+            self.handle, _p(v), W, H, D, T, vs.ctypes.data_as(ctypes.c_void_p), _p(out), W2, H2, D2,
+            nvs.ctypes.data_as(ctypes.c_void_p), int(mm_z_cut), int(interpolation)))
+        return out
+
+    def transform_volumes_linear(self, src: torch.Tensor, params,
+                                 interpolation: int = L.INTERP_LINEAR) -> torch.Tensor:
+        """TransformVolumesLinear: one 12-parameter vector applied to every
+        volume of (T, D, H, W)."""
+        v = self._vols4(src)
+        T, D, H, W = v.shape
+        p = np.ascontiguousarray(np.asarray(params, np.float32).reshape(12))
+        out = torch.empty_like(v)
+        self._bind_stream()
+        _check(self, L.lib().brc_transform_volumes_linear(self.handle, _p(v), W, H, D, T,
+                                                          p.ctypes.data_as(ctypes.c_void_p), int(interpolation),
+                                                          _p(out)))
+        return out
+
+    def transform_volumes_nonlinear(self, src: torch.Tensor, dx, dy, dz,
+                                    interpolation: int = L.INTERP_LINEAR) -> torch.Tensor:
+        """TransformVolumesNonLinear: one displacement field (voxels) applied
+        to every volume of (T, D, H, W)."""
+        v = self._vols4(src)
+        T, D, H, W = v.shape
+        fx, fy, fz = (f.contiguous().to(torch.float32) for f in (dx, dy, dz))
+        out = torch.empty_like(v)
+        self._bind_stream()
+        _check(self, L.lib().brc_transform_volumes_nonlinear(self.handle, _p(v), W, H, D, T, _p(fx), _p(fy),
+                                                             _p(fz), int(interpolation), _p(out)))
+        return out
+
+    def combine_displacement_field(self, dx: torch.Tensor, dy: torch.Tensor, dz: torch.Tensor, params) -> None:
+        """CreateCombinedDisplacementField: adds the affine displacement of
+        params to the field (dx, dy, dz) in place."""
+        for f in (dx, dy, dz):
+            if not f.is_contiguous() or f.dtype != torch.float32 or not f.is_cuda:
+                raise TypeError("field components must be contiguous float32 CUDA tensors")
+        D, H, W = dx.shape
+        p = np.ascontiguousarray(np.asarray(params, np.float32).reshape(12))
+        self._bind_stream()
+        _check(self, L.lib().brc_combine_displacement_field(self.handle, _p(dx), _p(dy), _p(dz), W, H, D,
+                                                            p.ctypes.data_as(ctypes.c_void_p)))
+
+    def center_volumes(self, src: torch.Tensor, interpolation: int = L.INTERP_LINEAR):
+        """CenterVolumesWrapper: (centred (T, D, H, W) volumes, 12 parameters)."""
+        v = self._vols4(src)
+        T, D, H, W = v.shape
+        out = torch.empty_like(v)
+        p = np.zeros(12, np.float32)
+        self._bind_stream()
+        _check(self, L.lib().brc_center_volumes(self.handle, _p(v), W, H, D, T, int(interpolation), _p(out),
+                                                p.ctypes.data_as(ctypes.c_void_p)))
+        return out, p
+
     def center_of_mass(self, vol: torch.Tensor) -> np.ndarray:
         v = vol.contiguous()
         D, H, W = v.shape

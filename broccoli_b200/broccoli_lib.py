@@ -41,6 +41,9 @@ class BROCCOLI_LIB:
         self._input_arrays = []
         self.epi = [0, 0, 0, 1]
         self.t1 = [0, 0, 0]
+        self.t1_t = 1
+        self.interpolation = LINEAR
+        self.center_parameters = np.zeros(12, np.float32)
         self.mni = [0, 0, 0]
         self.epi_vox = [1.0, 1.0, 1.0]
         self.t1_vox = [1.0, 1.0, 1.0]
@@ -229,8 +232,12 @@ class BROCCOLI_LIB:
     def SetCoarsestScaleT1MNI(self, n): self.coarsest = int(n)
     def SetMMT1ZCUT(self, mm): self.mm_z_cut = int(mm)
     def SetInterpolationMode(self, mode):
-        if mode != LINEAR:
-            raise ValueError("only LINEAR interpolation is implemented")
+        # the registration loops resample linearly whatever the mode (as the
+        # reference's loops do); the transform wrappers take NEAREST or LINEAR
+        if mode not in (NEAREST, LINEAR):
+            raise ValueError("NEAREST or LINEAR interpolation (the reference's CUBIC kernels are not usable)")
+        self.interpolation = int(mode)
+    def SetT1Timepoints(self, t): self.t1_t = int(t)
     def SetTsigma(self, s): self.sigmas[0] = float(s)
     def SetEsigma(self, s): self.sigmas[1] = float(s)
     def SetDsigma(self, s): self.sigmas[2] = float(s)
@@ -324,6 +331,55 @@ class BROCCOLI_LIB:
             f = r["field"].cpu().numpy()
             for a in range(3):
                 self.out["field"][a][...] = f[a].reshape(self.out["field"][a].shape)
+        ctx.close()
+
+
+    # ---- 4D transforms (TransformVolumesLinear/NonLinearWrapper,
+    # CenterVolumesWrapper, broccoli_lib.cpp:8145-8245) ------------------------
+
+    def _t1_volumes(self, ctx):
+        import torch
+        W, H, D = self.t1
+        a = np.ascontiguousarray(self.t1_volume, np.float32).reshape(self.t1_t, D, H, W)
+        return torch.from_numpy(a).cuda()
+
+    def _t1_to_mni(self, ctx, vols):
+        W2, H2, D2 = self.mni
+        return ctx.change_resolution_and_size_batch(vols, self.t1_vox, (D2, H2, W2), self.mni_vox, self.mm_z_cut,
+                                                    self.interpolation)
+
+    def TransformVolumesLinearWrapper(self):
+        """The T1 volumes resampled onto the MNI grid, then transformed by the
+        parameters of SetOutputT1MNIRegistrationParameters; result in the
+        array of SetOutputInterpolatedT1Volume."""
+        from .api import Context
+        ctx = Context(0)
+        mni = self._t1_to_mni(ctx, self._t1_volumes(ctx))
+        out = ctx.transform_volumes_linear(mni, np.asarray(self.out["params"], np.float32)[:12], self.interpolation)
+        self.out["interpolated"][...] = out.cpu().numpy().reshape(self.out["interpolated"].shape)
+        ctx.close()
+
+    def TransformVolumesNonLinearWrapper(self):
+        """As TransformVolumesLinearWrapper with the displacement field of
+        SetOutputDisplacementField."""
+        import torch
+        from .api import Context
+        ctx = Context(0)
+        W2, H2, D2 = self.mni
+        mni = self._t1_to_mni(ctx, self._t1_volumes(ctx))
+        f = [torch.from_numpy(np.ascontiguousarray(a, np.float32).reshape(D2, H2, W2)).cuda()
+             for a in self.out["field"]]
+        out = ctx.transform_volumes_nonlinear(mni, *f, interpolation=self.interpolation)
+        self.out["interpolated"][...] = out.cpu().numpy().reshape(self.out["interpolated"].shape)
+        ctx.close()
+
+    def CenterVolumesWrapper(self):
+        """The T1 volumes centred by the first one's centre of mass (T1 size)."""
+        from .api import Context
+        ctx = Context(0)
+        out, p = ctx.center_volumes(self._t1_volumes(ctx), self.interpolation)
+        self.center_parameters[:] = p
+        self.out["interpolated"][...] = out.cpu().numpy().reshape(self.out["interpolated"].shape)
         ctx.close()
 
 

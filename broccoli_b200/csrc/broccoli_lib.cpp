@@ -338,6 +338,78 @@ void BROCCOLI_LIB::smooth_normalized(const float* h_mask, float* h_out, const ch
 }
 
 // PerformRegistrationTwoVolumesWrapper, broccoli_lib.cpp:7973-8112.
+// h_T1_Volume (T1 grid, t1_t_ volumes) resampled onto the MNI grid with the
+// interpolation mode (ChangeVolumesResolutionAndSize), into d_out.
+bool BROCCOLI_LIB::t1_to_mni(const float* d_t1, float* d_out, const char* where) {
+  return check(brc_change_resolution_and_size_batch(ctx_, d_t1, (int)t1_w_, (int)t1_h_, (int)t1_d_, (int)t1_t_,
+                                                    t1_vox_, d_out, (int)mni_w_, (int)mni_h_, (int)mni_d_, mni_vox_,
+                                                    mm_z_cut_, interpolation_),
+               where);
+}
+
+void BROCCOLI_LIB::TransformVolumesLinearWrapper() {
+  if (!initiated_ && !check(BRC_ERR_NODEVICE, "TransformVolumesLinearWrapper")) return;
+  if (!h_t1_ || !out_params_ || !out_interpolated_) {
+    check(BRC_ERR_INVALID, "TransformVolumesLinearWrapper: T1 volumes, parameters or output not set");
+    return;
+  }
+  const size_t V1 = t1_w_ * t1_h_ * t1_d_ * t1_t_, V2 = mni_w_ * mni_h_ * mni_d_ * t1_t_;
+  DeviceArray d_in(ctx_, sizeof(float) * V1), d_mni(ctx_, sizeof(float) * V2), d_out(ctx_, sizeof(float) * V2);
+  for (const DeviceArray* a : {&d_in, &d_mni, &d_out})
+    if (!check(a->status, "alloc")) return;
+  if (!check(brc_copy_to_device(ctx_, d_in.ptr, h_t1_, sizeof(float) * V1), "H2D")) return;
+  if (!t1_to_mni(d_in.f(), d_mni.f(), "TransformVolumesLinearWrapper: resample")) return;
+  // the parameters are read from the array given to
+  // SetOutputT1MNIRegistrationParameters, as in the reference
+  if (!check(brc_transform_volumes_linear(ctx_, d_mni.f(), (int)mni_w_, (int)mni_h_, (int)mni_d_, (int)t1_t_,
+                                          out_params_, interpolation_, d_out.f()),
+             "TransformVolumesLinearWrapper"))
+    return;
+  check(brc_copy_to_host(ctx_, out_interpolated_, d_out.ptr, sizeof(float) * V2), "D2H");
+}
+
+void BROCCOLI_LIB::TransformVolumesNonLinearWrapper() {
+  if (!initiated_ && !check(BRC_ERR_NODEVICE, "TransformVolumesNonLinearWrapper")) return;
+  if (!h_t1_ || !out_field_[0] || !out_field_[1] || !out_field_[2] || !out_interpolated_) {
+    check(BRC_ERR_INVALID, "TransformVolumesNonLinearWrapper: T1 volumes, displacement field or output not set");
+    return;
+  }
+  const size_t V1 = t1_w_ * t1_h_ * t1_d_ * t1_t_, V3 = mni_w_ * mni_h_ * mni_d_, V2 = V3 * t1_t_;
+  DeviceArray d_in(ctx_, sizeof(float) * V1), d_mni(ctx_, sizeof(float) * V2), d_out(ctx_, sizeof(float) * V2),
+      d_field(ctx_, sizeof(float) * 3 * V3);
+  for (const DeviceArray* a : {&d_in, &d_mni, &d_out, &d_field})
+    if (!check(a->status, "alloc")) return;
+  if (!check(brc_copy_to_device(ctx_, d_in.ptr, h_t1_, sizeof(float) * V1), "H2D")) return;
+  // the field is read from the arrays given to SetOutputDisplacementField
+  for (int a = 0; a < 3; a++)
+    if (!check(brc_copy_to_device(ctx_, d_field.f() + a * V3, out_field_[a], sizeof(float) * V3), "H2D")) return;
+  if (!t1_to_mni(d_in.f(), d_mni.f(), "TransformVolumesNonLinearWrapper: resample")) return;
+  if (!check(brc_transform_volumes_nonlinear(ctx_, d_mni.f(), (int)mni_w_, (int)mni_h_, (int)mni_d_, (int)t1_t_,
+                                             d_field.f(), d_field.f() + V3, d_field.f() + 2 * V3, interpolation_,
+                                             d_out.f()),
+             "TransformVolumesNonLinearWrapper"))
+    return;
+  check(brc_copy_to_host(ctx_, out_interpolated_, d_out.ptr, sizeof(float) * V2), "D2H");
+}
+
+void BROCCOLI_LIB::CenterVolumesWrapper() {
+  if (!initiated_ && !check(BRC_ERR_NODEVICE, "CenterVolumesWrapper")) return;
+  if (!h_t1_ || !out_interpolated_) {
+    check(BRC_ERR_INVALID, "CenterVolumesWrapper: T1 volumes or output not set");
+    return;
+  }
+  const size_t V = t1_w_ * t1_h_ * t1_d_ * t1_t_;
+  DeviceArray d_in(ctx_, sizeof(float) * V), d_out(ctx_, sizeof(float) * V);
+  for (const DeviceArray* a : {&d_in, &d_out})
+    if (!check(a->status, "alloc")) return;
+  if (!check(brc_copy_to_device(ctx_, d_in.ptr, h_t1_, sizeof(float) * V), "H2D")) return;
+  if (!check(brc_center_volumes(ctx_, d_in.f(), (int)t1_w_, (int)t1_h_, (int)t1_d_, (int)t1_t_, interpolation_,
+                                d_out.f(), center_params_),
+             "CenterVolumesWrapper"))
+    return;
+  check(brc_copy_to_host(ctx_, out_interpolated_, d_out.ptr, sizeof(float) * V), "D2H");
+}
+
 void BROCCOLI_LIB::PerformRegistrationTwoVolumesWrapper() {
   if (!initiated_ && !check(BRC_ERR_NODEVICE, "PerformRegistrationTwoVolumesWrapper")) return;
   float bank3[3 * 686], bank6[6 * 686], dirs[18];

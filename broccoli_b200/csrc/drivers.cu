@@ -223,6 +223,78 @@ extern "C" int brc_change_resolution_and_size(brc_ctx* ctx, const float* d_src, 
   return BRC_OK;
 }
 
+// Interpolation modes of the transform entries: the reference's NEAREST and
+// LINEAR.  Its CUBIC kernels sum into an uninitialised variable
+// (kernelRegistration.cpp:1230, :1284, :1396), so CUBIC is refused.
+static int check_interp(brc_ctx* ctx, int interpolation, const char* where) {
+  if (interpolation == BRC_INTERP_NEAREST || interpolation == BRC_INTERP_LINEAR) return BRC_OK;
+  if (interpolation == BRC_INTERP_CUBIC)
+    return ctx->fail(BRC_ERR_UNSUPPORTED, std::string(where) + ": CUBIC interpolation is not supported");
+  return ctx->fail(BRC_ERR_INVALID, std::string(where) + ": unknown interpolation mode");
+}
+
+extern "C" int brc_change_resolution_and_size_batch(brc_ctx* ctx, const float* d_src, int W, int H, int D, int T,
+                                                    const float* voxel_size3, float* d_out, int W2, int H2, int D2,
+                                                    const float* new_voxel_size3, int mm_z_cut, int interpolation) {
+  if (!ctx) return BRC_ERR_INVALID;
+  if (!d_src || !d_out || !voxel_size3 || !new_voxel_size3 || W <= 0 || H <= 0 || D <= 0 || W2 <= 0 ||
+      H2 <= 0 || D2 <= 0 || T <= 0 || T > 65535 || d_src == d_out)
+    return ctx->fail(BRC_ERR_INVALID, "brc_change_resolution_and_size_batch: bad argument");
+  for (int a = 0; a < 3; a++)
+    if (!(voxel_size3[a] > 0) || !(new_voxel_size3[a] > 0))
+      return ctx->fail(BRC_ERR_INVALID, "brc_change_resolution_and_size_batch: voxel sizes must be positive");
+  const int s = check_interp(ctx, interpolation, "brc_change_resolution_and_size_batch");
+  if (s != BRC_OK) return s;
+  cudaSetDevice(ctx->device);
+  BRC_TRY(ctx, brc::resize_to_grid_batch(d_src, W, H, D, T, voxel_size3[0], voxel_size3[1], voxel_size3[2], d_out,
+                                         W2, H2, D2, new_voxel_size3[0], new_voxel_size3[1], new_voxel_size3[2],
+                                         mm_z_cut, interpolation, ctx->stream()),
+          "resize");
+  ctx->launches += 1;
+  return BRC_OK;
+}
+
+extern "C" int brc_transform_volumes_linear(brc_ctx* ctx, const float* d_src, int W, int H, int D, int T,
+                                            const float* h_params12, int interpolation, float* d_out) {
+  if (!ctx) return BRC_ERR_INVALID;
+  if (!d_src || !d_out || !h_params12 || W <= 0 || H <= 0 || D <= 0 || T <= 0 || T > 65535 || d_src == d_out)
+    return ctx->fail(BRC_ERR_INVALID, "brc_transform_volumes_linear: bad argument");
+  const int s = check_interp(ctx, interpolation, "brc_transform_volumes_linear");
+  if (s != BRC_OK) return s;
+  cudaSetDevice(ctx->device);
+  BRC_TRY(ctx, brc::transform_affine(d_src, W, H, D, T, h_params12, interpolation, d_out, ctx->stream()),
+          "transform_affine");
+  ctx->launches += 1;
+  return BRC_OK;
+}
+
+extern "C" int brc_transform_volumes_nonlinear(brc_ctx* ctx, const float* d_src, int W, int H, int D, int T,
+                                               const float* d_dx, const float* d_dy, const float* d_dz,
+                                               int interpolation, float* d_out) {
+  if (!ctx) return BRC_ERR_INVALID;
+  if (!d_src || !d_out || !d_dx || !d_dy || !d_dz || W <= 0 || H <= 0 || D <= 0 || T <= 0 || T > 65535 ||
+      d_src == d_out)
+    return ctx->fail(BRC_ERR_INVALID, "brc_transform_volumes_nonlinear: bad argument");
+  const int s = check_interp(ctx, interpolation, "brc_transform_volumes_nonlinear");
+  if (s != BRC_OK) return s;
+  cudaSetDevice(ctx->device);
+  BRC_TRY(ctx, brc::transform_field(d_src, W, H, D, T, d_dx, d_dy, d_dz, interpolation, d_out, ctx->stream()),
+          "transform_field");
+  ctx->launches += 1;
+  return BRC_OK;
+}
+
+extern "C" int brc_combine_displacement_field(brc_ctx* ctx, float* d_dx, float* d_dy, float* d_dz, int W, int H,
+                                              int D, const float* h_params12) {
+  if (!ctx) return BRC_ERR_INVALID;
+  if (!d_dx || !d_dy || !d_dz || !h_params12 || W <= 0 || H <= 0 || D <= 0)
+    return ctx->fail(BRC_ERR_INVALID, "brc_combine_displacement_field: bad argument");
+  cudaSetDevice(ctx->device);
+  BRC_TRY(ctx, brc::combine_field(d_dx, d_dy, d_dz, W, H, D, h_params12, ctx->stream()), "combine_field");
+  ctx->launches += 1;
+  return BRC_OK;
+}
+
 extern "C" int brc_center_of_mass(brc_ctx* ctx, const float* d_vol, int W, int H, int D, float* h_com3) {
   if (!ctx) return BRC_ERR_INVALID;
   if (!d_vol || !h_com3 || W <= 0 || H <= 0 || D <= 0)
@@ -236,6 +308,26 @@ extern "C" int brc_center_of_mass(brc_ctx* ctx, const float* d_vol, int W, int H
   BRC_TRY(ctx, cudaMemcpyAsync(h, sums, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream()), "D2H");
   BRC_TRY(ctx, cudaStreamSynchronize(ctx->stream()), "sync");
   for (int a = 0; a < 3; a++) h_com3[a] = (float)(h[a + 1] / h[0]);
+  return BRC_OK;
+}
+
+extern "C" int brc_center_volumes(brc_ctx* ctx, const float* d_src, int W, int H, int D, int T, int interpolation,
+                                  float* d_out, float* h_params12) {
+  if (!ctx) return BRC_ERR_INVALID;
+  if (!d_src || !d_out || W <= 0 || H <= 0 || D <= 0 || T <= 0 || T > 65535 || d_src == d_out)
+    return ctx->fail(BRC_ERR_INVALID, "brc_center_volumes: bad argument");
+  int s = check_interp(ctx, interpolation, "brc_center_volumes");
+  if (s != BRC_OK) return s;
+  float com[3];
+  if ((s = brc_center_of_mass(ctx, d_src, W, H, D, com)) != BRC_OK) return s;
+  // CenterVolumeMass (broccoli_lib.cpp:6839-6874): integer translation that
+  // moves the first volume's centre of mass to (W/2, H/2, D/2)
+  float p[12] = {0};
+  p[0] = -floorf((float)W / 2.0f - com[0] + 0.5f);
+  p[1] = -floorf((float)H / 2.0f - com[1] + 0.5f);
+  p[2] = -floorf((float)D / 2.0f - com[2] + 0.5f);
+  if ((s = brc_transform_volumes_linear(ctx, d_src, W, H, D, T, p, interpolation, d_out)) != BRC_OK) return s;
+  if (h_params12) memcpy(h_params12, p, sizeof(p));
   return BRC_OK;
 }
 

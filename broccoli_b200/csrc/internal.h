@@ -77,6 +77,16 @@ size_t resize_job_bytes();
 cudaError_t resize_to_grid_ragged(int n, const float* const* srcs, const int* dims3n, const float* vox3n,
                                   void* h_jobs, void* d_jobs, float* out, int W2, int H2, int D2,
                                   const float* new_vox3, int mm_z_cut, cudaStream_t st);
+// 4D transforms with interpolation 0 (NEAREST) or 1 (LINEAR), T volumes of
+// W x H x D one after another; the affine parameters are host values.
+cudaError_t resize_to_grid_batch(const float* src, int W, int H, int D, int T, float vx, float vy, float vz,
+                                 float* out, int W2, int H2, int D2, float nvx, float nvy, float nvz, int mm_z_cut,
+                                 int interp, cudaStream_t st);
+cudaError_t transform_affine(const float* src, int W, int H, int D, int T, const float* p12, int interp,
+                             float* out, cudaStream_t st);
+cudaError_t transform_field(const float* src, int W, int H, int D, int T, const float* dx, const float* dy,
+                            const float* dz, int interp, float* out, cudaStream_t st);
+cudaError_t combine_field(float* dx, float* dy, float* dz, int W, int H, int D, const float* p12, cudaStream_t st);
 cudaError_t add_affine_to_field(float* field, int W, int H, int D, const float* p12, cudaStream_t st);
 }  // namespace brc
 

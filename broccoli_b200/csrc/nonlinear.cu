@@ -359,6 +359,149 @@ add_affine_to_field_kernel(float* __restrict__ field, int W, int H, int D, Param
 
 // ---------------------------------------------------------------------------
 
+// ---------------------------------------------------------------------------
+// Transforms of 4D data with NEAREST (0) or LINEAR (1) interpolation
+// (TransformVolumesLinear / NonLinear, broccoli_lib.cpp:8267-8451,
+// ChangeVolumesResolutionAndSize :6950-7100, CreateCombinedDisplacementField
+// :8115-8143).  Coordinates and weights are computed in the reference's
+// operation order with every product and sum rounded (no contraction into
+// FMAs), so that nearest sampling picks the reference's voxel and linear
+// sampling reproduces its arithmetic.
+// ---------------------------------------------------------------------------
+
+// OpenCL 1.2 section 8.2 nearest filtering, unnormalised coordinates,
+// clamp-to-edge: i = floor(u) (volume_sampler_nearest,
+// kernelRegistration.cpp:992).
+__device__ __forceinline__ float sample_near(const float* __restrict__ T, int W, int H, int D, float u, float v,
+                                             float w) {
+  const int i = min(max((int)floorf(u), 0), W - 1);
+  const int j = min(max((int)floorf(v), 0), H - 1);
+  const int k = min(max((int)floorf(w), 0), D - 1);
+  return __ldg(T + i + (long long)j * W + (long long)k * W * H);
+}
+
+// Linear filtering with the 8 weights formed and summed as in the
+// reference's sampler, each operation rounded.
+__device__ __forceinline__ float sample_lin_exact(const float* __restrict__ T, int W, int H, int D, float u,
+                                                  float v, float w) {
+  const float uu = __fsub_rn(u, 0.5f), vv = __fsub_rn(v, 0.5f), ww = __fsub_rn(w, 0.5f);
+  const float fu = floorf(uu), fv = floorf(vv), fw = floorf(ww);
+  const float a = __fsub_rn(uu, fu), b = __fsub_rn(vv, fv), c = __fsub_rn(ww, fw);
+  const float a0 = __fsub_rn(1.f, a), b0 = __fsub_rn(1.f, b), c0 = __fsub_rn(1.f, c);
+  const int i0 = (int)fu, j0 = (int)fv, k0 = (int)fw;
+  const int x0 = min(max(i0, 0), W - 1), x1 = min(max(i0 + 1, 0), W - 1);
+  const int y0 = min(max(j0, 0), H - 1), y1 = min(max(j0 + 1, 0), H - 1);
+  const int z0 = min(max(k0, 0), D - 1), z1 = min(max(k0 + 1, 0), D - 1);
+  const long long WH = (long long)W * H;
+#define TX(i, j, k) __ldg(T + (i) + (long long)(j) * W + (long long)(k) * WH)
+  float r = __fmul_rn(__fmul_rn(__fmul_rn(a0, b0), c0), TX(x0, y0, z0));
+  r = __fadd_rn(r, __fmul_rn(__fmul_rn(__fmul_rn(a, b0), c0), TX(x1, y0, z0)));
+  r = __fadd_rn(r, __fmul_rn(__fmul_rn(__fmul_rn(a0, b), c0), TX(x0, y1, z0)));
+  r = __fadd_rn(r, __fmul_rn(__fmul_rn(__fmul_rn(a, b), c0), TX(x1, y1, z0)));
+  r = __fadd_rn(r, __fmul_rn(__fmul_rn(__fmul_rn(a0, b0), c), TX(x0, y0, z1)));
+  r = __fadd_rn(r, __fmul_rn(__fmul_rn(__fmul_rn(a, b0), c), TX(x1, y0, z1)));
+  r = __fadd_rn(r, __fmul_rn(__fmul_rn(__fmul_rn(a0, b), c), TX(x0, y1, z1)));
+  r = __fadd_rn(r, __fmul_rn(__fmul_rn(__fmul_rn(a, b), c), TX(x1, y1, z1)));
+#undef TX
+  return r;
+}
+
+template <int MODE>
+__device__ __forceinline__ float sample_mode(const float* __restrict__ T, int W, int H, int D, float u, float v,
+                                             float w) {
+  return MODE == 0 ? sample_near(T, W, H, D, u, v, w) : sample_lin_exact(T, W, H, D, u, v, w);
+}
+
+// pos + t + a xf + b yf + c zf, left to right, each operation rounded
+__device__ __forceinline__ float affine_sum(float pos, float t, float a, float b, float c, float xf, float yf,
+                                            float zf) {
+  float r = __fadd_rn(pos, t);
+  r = __fadd_rn(r, __fmul_rn(a, xf));
+  r = __fadd_rn(r, __fmul_rn(b, yf));
+  return __fadd_rn(r, __fmul_rn(c, zf));
+}
+
+// Volume t = blockIdx.y of the batch: out_t(x) = src_t(x + t + (A - I)(x - c))
+// (InterpolateVolumeNearestLinear / LinearLinear, kernelRegistration.cpp:
+// 995-1031, :1066-1101).
+template <int MODE>
+__global__ void __launch_bounds__(256)
+transform_affine_kernel(const float* __restrict__ src, int W, int H, int D, Params12 prm,
+                        float* __restrict__ out) {
+  const long long V = (long long)W * H * D;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V) return;
+  const int x = (int)(i % W), y = (int)((i / W) % H), z = (int)(i / ((long long)W * H));
+  const float* p = prm.p;
+  const float xf = (float)x - ((float)W - 1.0f) * 0.5f;
+  const float yf = (float)y - ((float)H - 1.0f) * 0.5f;
+  const float zf = (float)z - ((float)D - 1.0f) * 0.5f;
+  const float u = __fadd_rn(affine_sum((float)x, p[0], p[3], p[4], p[5], xf, yf, zf), 0.5f);
+  const float v = __fadd_rn(affine_sum((float)y, p[1], p[6], p[7], p[8], xf, yf, zf), 0.5f);
+  const float w = __fadd_rn(affine_sum((float)z, p[2], p[9], p[10], p[11], xf, yf, zf), 0.5f);
+  const long long t = blockIdx.y;
+  out[t * V + i] = sample_mode<MODE>(src + t * V, W, H, D, u, v, w);
+}
+
+// Volume t = blockIdx.y warped by one displacement field
+// (InterpolateVolumeNearestNonLinear / LinearNonLinear,
+// kernelRegistration.cpp:1032-1061, :1111-1140).
+template <int MODE>
+__global__ void __launch_bounds__(256)
+transform_field_kernel(const float* __restrict__ src, int W, int H, int D, const float* __restrict__ dx,
+                       const float* __restrict__ dy, const float* __restrict__ dz, float* __restrict__ out) {
+  const long long V = (long long)W * H * D;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V) return;
+  const int x = (int)(i % W), y = (int)((i / W) % H), z = (int)(i / ((long long)W * H));
+  const float u = __fadd_rn(__fadd_rn((float)x, __ldg(dx + i)), 0.5f);
+  const float v = __fadd_rn(__fadd_rn((float)y, __ldg(dy + i)), 0.5f);
+  const float w = __fadd_rn(__fadd_rn((float)z, __ldg(dz + i)), 0.5f);
+  const long long t = blockIdx.y;
+  out[t * V + i] = sample_mode<MODE>(src + t * V, W, H, D, u, v, w);
+}
+
+// (dx, dy, dz) += t + (A - I)(x - c) (AddLinearAndNonLinearDisplacement,
+// kernelRegistration.cpp:1142-1178), each operation rounded.
+__global__ void __launch_bounds__(256)
+combine_field_kernel(float* __restrict__ dx, float* __restrict__ dy, float* __restrict__ dz, int W, int H, int D,
+                     Params12 prm) {
+  const long long V = (long long)W * H * D;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V) return;
+  const int x = (int)(i % W), y = (int)((i / W) % H), z = (int)(i / ((long long)W * H));
+  const float* p = prm.p;
+  const float xf = (float)x - ((float)W - 1.0f) * 0.5f;
+  const float yf = (float)y - ((float)H - 1.0f) * 0.5f;
+  const float zf = (float)z - ((float)D - 1.0f) * 0.5f;
+  dx[i] = __fadd_rn(dx[i], affine_sum(p[0], 0.f, p[3], p[4], p[5], xf, yf, zf));
+  dy[i] = __fadd_rn(dy[i], affine_sum(p[1], 0.f, p[6], p[7], p[8], xf, yf, zf));
+  dz[i] = __fadd_rn(dz[i], affine_sum(p[2], 0.f, p[9], p[10], p[11], xf, yf, zf));
+}
+
+// Volume t = blockIdx.y of a batch resampled as resize_to_grid_kernel does,
+// with NEAREST (0) or LINEAR (1) interpolation and the reference's rounding
+// (RescaleVolumeNearest / Linear, kernelRegistration.cpp:1312-1366, then
+// CopyVolumeToNew, :1593-1678).
+template <int MODE>
+__global__ void __launch_bounds__(256)
+resize_to_grid_mode_kernel(const float* __restrict__ src, int W, int H, int D, float* __restrict__ out, int W2,
+                           int H2, int D2, ResizeGeom g) {
+  const long long V2 = (long long)W2 * H2 * D2;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V2) return;
+  const long long t = blockIdx.y;
+  const int xn = (int)(i % W2), yn = (int)((i / W2) % H2), zn = (int)(i / ((long long)W2 * H2));
+  const int x = xn - g.offn[0], y = yn - g.offn[1], z = zn - g.offn[2];
+  const int xi = x + g.offi[0], yi = y + g.offi[1], zi = z + g.offi[2];
+  float v = 0.f;
+  if (x >= 0 && y >= 0 && z >= 0 && xi >= 0 && yi >= 0 && zi >= 0 && xi < g.Wi && yi < g.Hi && zi < g.Di)
+    v = sample_mode<MODE>(src + t * W * H * D, W, H, D, __fadd_rn(__fmul_rn((float)xi, g.vd[0]), 0.5f),
+                          __fadd_rn(__fmul_rn((float)yi, g.vd[1]), 0.5f),
+                          __fadd_rn(__fmul_rn((float)zi, g.vd[2]), 0.5f));
+  out[t * V2 + i] = v;
+}
+
 static unsigned grid1(long long n) { return (unsigned)((n + 255) / 256); }
 
 static int round_half_away(float v) { return (int)roundf(v); }
@@ -396,6 +539,51 @@ cudaError_t resize_to_grid(const float* src, int W, int H, int D, float vx, floa
   ResizeGeom g;
   if (!resize_geom(W, H, D, vx, vy, vz, W2, H2, D2, nvx, nvy, nvz, mm_z_cut, g)) return cudaErrorInvalidValue;
   resize_to_grid_kernel<<<grid1((long long)W2 * H2 * D2), 256, 0, st>>>(src, W, H, D, out, W2, H2, D2, g);
+  return cudaGetLastError();
+}
+
+cudaError_t resize_to_grid_batch(const float* src, int W, int H, int D, int T, float vx, float vy, float vz,
+                                 float* out, int W2, int H2, int D2, float nvx, float nvy, float nvz, int mm_z_cut,
+                                 int interp, cudaStream_t st) {
+  ResizeGeom g;
+  if (T <= 0 || T > 65535 || (interp != 0 && interp != 1)) return cudaErrorInvalidValue;
+  if (!resize_geom(W, H, D, vx, vy, vz, W2, H2, D2, nvx, nvy, nvz, mm_z_cut, g)) return cudaErrorInvalidValue;
+  const dim3 grid(grid1((long long)W2 * H2 * D2), (unsigned)T);
+  if (interp == 0)
+    resize_to_grid_mode_kernel<0><<<grid, 256, 0, st>>>(src, W, H, D, out, W2, H2, D2, g);
+  else
+    resize_to_grid_mode_kernel<1><<<grid, 256, 0, st>>>(src, W, H, D, out, W2, H2, D2, g);
+  return cudaGetLastError();
+}
+
+cudaError_t transform_affine(const float* src, int W, int H, int D, int T, const float* p12, int interp,
+                             float* out, cudaStream_t st) {
+  if (T <= 0 || T > 65535 || (interp != 0 && interp != 1)) return cudaErrorInvalidValue;
+  Params12 prm;
+  for (int i = 0; i < 12; i++) prm.p[i] = p12[i];
+  const dim3 grid(grid1((long long)W * H * D), (unsigned)T);
+  if (interp == 0)
+    transform_affine_kernel<0><<<grid, 256, 0, st>>>(src, W, H, D, prm, out);
+  else
+    transform_affine_kernel<1><<<grid, 256, 0, st>>>(src, W, H, D, prm, out);
+  return cudaGetLastError();
+}
+
+cudaError_t transform_field(const float* src, int W, int H, int D, int T, const float* dx, const float* dy,
+                            const float* dz, int interp, float* out, cudaStream_t st) {
+  if (T <= 0 || T > 65535 || (interp != 0 && interp != 1)) return cudaErrorInvalidValue;
+  const dim3 grid(grid1((long long)W * H * D), (unsigned)T);
+  if (interp == 0)
+    transform_field_kernel<0><<<grid, 256, 0, st>>>(src, W, H, D, dx, dy, dz, out);
+  else
+    transform_field_kernel<1><<<grid, 256, 0, st>>>(src, W, H, D, dx, dy, dz, out);
+  return cudaGetLastError();
+}
+
+cudaError_t combine_field(float* dx, float* dy, float* dz, int W, int H, int D, const float* p12, cudaStream_t st) {
+  Params12 prm;
+  for (int i = 0; i < 12; i++) prm.p[i] = p12[i];
+  combine_field_kernel<<<grid1((long long)W * H * D), 256, 0, st>>>(dx, dy, dz, W, H, D, prm);
   return cudaGetLastError();
 }
 

@@ -347,6 +347,56 @@ int brc_change_resolution_and_size(brc_ctx* ctx, const float* d_src, int W, int 
                                    const float* voxel_size3, float* d_out, int W2, int H2, int D2,
                                    const float* new_voxel_size3, int mm_z_cut);
 
+/* Interpolation modes of the transform and resample entries: the values of
+ * the reference's INTERPOLATION_MODE (broccoli_constants.h:97-99).  CUBIC
+ * is refused with BRC_ERR_UNSUPPORTED: the reference's cubic kernels sum
+ * into an uninitialised variable (kernelRegistration.cpp:1230, :1284,
+ * :1396), so there is no defined result to reproduce. */
+#define BRC_INTERP_NEAREST 0
+#define BRC_INTERP_LINEAR 1
+#define BRC_INTERP_CUBIC 2
+
+/* brc_change_resolution_and_size for T volumes (d_src: T x W x H x D one
+ * after another, d_out: T x W2 x H2 x D2) with NEAREST or LINEAR
+ * interpolation.  Replaces ChangeVolumesResolutionAndSize with
+ * NUMBER_OF_VOLUMES = T and INTERPOLATION_MODE (broccoli_lib.cpp:6950-7100;
+ * RescaleVolumeNearest / Linear and CopyVolumeToNew,
+ * kernelRegistration.cpp:1312-1366, :1593-1678). */
+int brc_change_resolution_and_size_batch(brc_ctx* ctx, const float* d_src, int W, int H, int D, int T,
+                                         const float* voxel_size3, float* d_out, int W2, int H2, int D2,
+                                         const float* new_voxel_size3, int mm_z_cut, int interpolation);
+
+/* One parameter vector (h_params12, host, the 12-parameter layout above)
+ * applied to T volumes: out_t(x) = src_t(x + t + (A - I)(x - centre)),
+ * NEAREST or LINEAR.  d_src and d_out must differ.  Replaces
+ * TransformVolumesLinear (broccoli_lib.cpp:8267-8359; InterpolateVolume-
+ * NearestLinear / LinearLinear, kernelRegistration.cpp:995-1031, :1066-1101). */
+int brc_transform_volumes_linear(brc_ctx* ctx, const float* d_src, int W, int H, int D, int T,
+                                 const float* h_params12, int interpolation, float* d_out);
+
+/* One displacement field (voxels, three W x H x D volumes) applied to T
+ * volumes: out_t(x) = src_t(x + d(x)).  Replaces TransformVolumesNonLinear
+ * (broccoli_lib.cpp:8361-8451; InterpolateVolumeNearestNonLinear /
+ * LinearNonLinear, kernelRegistration.cpp:1032-1061, :1111-1140). */
+int brc_transform_volumes_nonlinear(brc_ctx* ctx, const float* d_src, int W, int H, int D, int T,
+                                    const float* d_dx, const float* d_dy, const float* d_dz, int interpolation,
+                                    float* d_out);
+
+/* d += t + (A - I)(x - centre) in place: the displacement of an affine
+ * parameter vector (host) added to a field.  Replaces
+ * CreateCombinedDisplacementField (broccoli_lib.cpp:8115-8143;
+ * AddLinearAndNonLinearDisplacement, kernelRegistration.cpp:1142-1178). */
+int brc_combine_displacement_field(brc_ctx* ctx, float* d_dx, float* d_dy, float* d_dz, int W, int H, int D,
+                                   const float* h_params12);
+
+/* Centres T volumes by the first one's centre of mass: the translation
+ * -round(N/2 - com) per axis (returned in h_params12 when not NULL)
+ * applied to all T volumes with the given interpolation; synchronises.
+ * Replaces CenterVolumesWrapper with CenterVolumeMass (broccoli_lib.cpp:
+ * 8225-8245, :6839-6874). */
+int brc_center_volumes(brc_ctx* ctx, const float* d_src, int W, int H, int D, int T, int interpolation,
+                       float* d_out, float* h_params12);
+
 /* Centre of mass (voxel coordinates) of a volume, FP64 reduction on the
  * device; synchronises.  Replaces CalculateCenterOfMass
  * (broccoli_lib.cpp:6763-6800, a host loop after a full device-to-host

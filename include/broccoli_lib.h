@@ -162,6 +162,16 @@ class BROCCOLI_LIB {
   void PerformSmoothingWrapper();
   void PerformSmoothingNormalizedWrapper();
   void PerformSmoothingNormalizedHostWrapper();  // smooths the fMRI volumes in place
+  // 4D transforms of h_T1_Volume (t1 timepoints) into the array of
+  // SetOutputInterpolatedT1Volume: resampled onto the MNI grid, then the
+  // parameters of SetOutputT1MNIRegistrationParameters (Linear) or the field
+  // of SetOutputDisplacementField (NonLinear) applied; CenterVolumes centres
+  // the T1 volumes by the first one's centre of mass at T1 size.  NEAREST or
+  // LINEAR (SetInterpolationMode); CUBIC fails with BRC_ERR_UNSUPPORTED.
+  void TransformVolumesLinearWrapper();
+  void TransformVolumesNonLinearWrapper();
+  void CenterVolumesWrapper();
+  const float* GetCenterParameters() const { return center_params_; }  // of the last CenterVolumesWrapper
 
   int GetLastStatus() const { return last_status_; }
 
@@ -216,6 +226,8 @@ class BROCCOLI_LIB {
   bool auto_mask_ = false;
   cl_float2* out_q_[3] = {nullptr};
 
+  float center_params_[12] = {0};
+  bool t1_to_mni(const float* d_t1, float* d_out, const char* where);
   bool check(int status, const char* where);
   bool pack_linear(float* bank3);
   bool pack_nonlinear(float* bank6, float* dirs18);

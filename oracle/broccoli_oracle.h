@@ -95,6 +95,17 @@ enum { ORC_TRANSLATION = 0, ORC_RIGID = 1, ORC_AFFINE = 2 };
       const real* src, int W, int H, int D, float vx, float vy, float vz,       \
       real* out, int W2, int H2, int D2, float nvx, float nvy, float nvz,       \
       int mm_z_cut);                                                            \
+  void orc_change_resolution_and_size_interp##SFX(                              \
+      const real* src, int W, int H, int D, float vx, float vy, float vz,       \
+      real* out, int W2, int H2, int D2, float nvx, float nvy, float nvz,       \
+      int mm_z_cut, int interp);                                                \
+  void orc_transform_affine##SFX(const real* src, int W, int H, int D, int T,   \
+                                 const real* p, int interp, real* out);         \
+  void orc_transform_field##SFX(const real* src, int W, int H, int D, int T,    \
+                                const real* dx, const real* dy,                 \
+                                const real* dz, int interp, real* out);         \
+  void orc_center_volumes##SFX(const real* src, int W, int H, int D, int T,     \
+                               int interp, real* out, real* p12);               \
   void orc_center_of_mass##SFX(const real* vol, int W, int H, int D, real* c3); \
   void orc_match_volume_masses##SFX(real* v1, const real* v2, int W, int H,     \
                                     int D, real* p12);                          \

@@ -576,3 +576,104 @@ def registration_objective(moving, ref, filters, sigma, params=None, field=None,
     qr = filter3d(sr, filters, prec=prec)
     d = qm - qr
     return float((d.real ** 2 + d.imag ** 2).sum())
+
+
+# ---- 4D transforms with NEAREST (0) / LINEAR (1) interpolation ------------
+
+def _vols4(src):
+    v = np.asarray(src)
+    return v[None] if v.ndim == 3 else v
+
+
+def transform_affine(src, p12, interp=1, prec="f32"):
+    """TransformVolumesLinear: one parameter vector applied to (T, D, H, W)."""
+    dt, s = _dt(prec)
+    v = _arr(_vols4(src), dt)
+    T, D, H, W = v.shape
+    p = _arr(p12, dt)
+    out = np.empty_like(v)
+    getattr(orc_lib(), "orc_transform_affine" + s)(_ptr(v), W, H, D, T, _ptr(p), int(interp), _ptr(out))
+    return out
+
+
+def transform_field(src, dx, dy, dz, interp=1, prec="f32"):
+    """TransformVolumesNonLinear: one displacement field applied to (T, D, H, W)."""
+    dt, s = _dt(prec)
+    v = _arr(_vols4(src), dt)
+    T, D, H, W = v.shape
+    fx, fy, fz = (_arr(a, dt) for a in (dx, dy, dz))
+    out = np.empty_like(v)
+    getattr(orc_lib(), "orc_transform_field" + s)(_ptr(v), W, H, D, T, _ptr(fx), _ptr(fy), _ptr(fz),
+                                                   int(interp), _ptr(out))
+    return out
+
+
+def center_volumes(src, interp=1, prec="f32"):
+    """CenterVolumesWrapper: (centred volumes, 12 parameters)."""
+    dt, s = _dt(prec)
+    v = _arr(_vols4(src), dt)
+    T, D, H, W = v.shape
+    out = np.empty_like(v)
+    p = np.zeros(12, dt)
+    getattr(orc_lib(), "orc_center_volumes" + s)(_ptr(v), W, H, D, T, int(interp), _ptr(out), _ptr(p))
+    return out, p
+
+
+def change_resolution_and_size_interp(src, vin, shape, vnew, mm_z_cut=0, interp=1, prec="f32"):
+    """ChangeVolumesResolutionAndSize of (T, D, H, W) volumes with an interpolation mode."""
+    dt, s = _dt(prec)
+    v = _arr(_vols4(src), dt)
+    T, D, H, W = v.shape
+    D2, H2, W2 = shape
+    out = np.zeros((T, D2, H2, W2), dt)
+    fn = getattr(orc_lib(), "orc_change_resolution_and_size_interp" + s)
+    fn.argtypes = [_P, _I, _I, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float, _P, _I, _I, _I,
+                   ctypes.c_float, ctypes.c_float, ctypes.c_float, _I, _I]
+    V, V2 = D * H * W, D2 * H2 * W2
+    for t in range(T):
+        src_t = v[t]
+        out_t = np.zeros((D2, H2, W2), dt)
+        fn(_ptr(src_t), W, H, D, *[float(a) for a in vin], _ptr(out_t), W2, H2, D2, *[float(a) for a in vnew],
+           int(mm_z_cut), int(interp))
+        out[t] = out_t
+    return out
+
+
+def ref_transform_affine(src, p12, interp=1):
+    v = _arr(_vols4(src), np.float32)
+    T, D, H, W = v.shape
+    p = _arr(p12, np.float32)
+    out = np.empty_like(v)
+    ref_lib().ref_transform_linear(_ptr(v), W, H, D, T, _ptr(p), int(interp), _ptr(out))
+    return out
+
+
+def ref_transform_field(src, dx, dy, dz, interp=1):
+    v = _arr(_vols4(src), np.float32)
+    T, D, H, W = v.shape
+    fx, fy, fz = (_arr(a, np.float32) for a in (dx, dy, dz))
+    out = np.empty_like(v)
+    ref_lib().ref_transform_nonlinear(_ptr(v), W, H, D, T, _ptr(fx), _ptr(fy), _ptr(fz), int(interp), _ptr(out))
+    return out
+
+
+def ref_center_volumes(src, interp=1):
+    v = _arr(_vols4(src), np.float32)
+    T, D, H, W = v.shape
+    out = np.empty_like(v)
+    p = np.zeros(12, np.float32)
+    ref_lib().ref_center_volumes(_ptr(v), W, H, D, T, int(interp), _ptr(out), _ptr(p))
+    return out, p
+
+
+def ref_change_resolution_and_size_interp(src, vin, shape, vnew, mm_z_cut=0, interp=1):
+    v = _arr(_vols4(src), np.float32)
+    T, D, H, W = v.shape
+    D2, H2, W2 = shape
+    out = np.zeros((T, D2, H2, W2), np.float32)
+    fn = ref_lib().ref_change_resolution_and_size_interp
+    fn.argtypes = [_P, _I, _I, _I, _I, ctypes.c_float, ctypes.c_float, ctypes.c_float, _P, _I, _I, _I,
+                   ctypes.c_float, ctypes.c_float, ctypes.c_float, _I, _I]
+    fn(_ptr(v), W, H, D, T, *[float(a) for a in vin], _ptr(out), W2, H2, D2, *[float(a) for a in vnew],
+       int(mm_z_cut), int(interp))
+    return out

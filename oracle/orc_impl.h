@@ -507,6 +507,24 @@ static REAL FN(orc_sample_linear)(const REAL* T, int W, int H, int D, REAL u,
 #undef TV
 }
 
+/* OpenCL 1.2 (section 8.2) nearest filtering with CLK_ADDRESS_CLAMP_TO_EDGE
+ * and unnormalised coordinates: i = floor(u), clamped to the edge. */
+static REAL FN(orc_sample_nearest)(const REAL* T, int W, int H, int D, REAL u,
+                                   REAL v, REAL w) {
+  int i = (int)RFLOOR(u), j = (int)RFLOOR(v), k = (int)RFLOOR(w);
+  i = i < 0 ? 0 : (i > W - 1 ? W - 1 : i);
+  j = j < 0 ? 0 : (j > H - 1 ? H - 1 : j);
+  k = k < 0 ? 0 : (k > D - 1 ? D - 1 : k);
+  return T[i + (long)j * W + (long)k * W * H];
+}
+
+/* Sample with INTERPOLATION_MODE 0 (NEAREST) or 1 (LINEAR). */
+static REAL FN(orc_sample)(int interp, const REAL* T, int W, int H, int D, REAL u,
+                           REAL v, REAL w) {
+  return interp == 0 ? FN(orc_sample_nearest)(T, W, H, D, u, v, w)
+                     : FN(orc_sample_linear)(T, W, H, D, u, v, w);
+}
+
 /* Affine warp: out(x) = linear sample of src at
  * x + t + (A - I)(x - c), c the volume centre.
  * InterpolateVolumeLinearLinear, kernelRegistration.cpp:1066-1101. */
@@ -540,6 +558,52 @@ void FN(orc_warp_field)(const REAL* src, int W, int H, int D, const REAL* dx,
         const REAL w = (REAL)z + dz[i] + RHALF;
         out[i] = FN(orc_sample_linear)(src, W, H, D, u, v, w);
       }
+}
+
+/* One parameter vector applied to T consecutive volumes with NEAREST (0) or
+ * LINEAR (1) interpolation.  TransformVolumesLinear, broccoli_lib.cpp:
+ * 8267-8359 (InterpolateVolumeNearestLinear / LinearLinear,
+ * kernelRegistration.cpp:995-1031, :1066-1101). */
+void FN(orc_transform_affine)(const REAL* src, int W, int H, int D, int T, const REAL* p, int interp,
+                              REAL* out) {
+  const long V = (long)W * H * D;
+  for (int t = 0; t < T; t++) {
+    const REAL* s = src + t * V;
+    REAL* o = out + t * V;
+#pragma omp parallel for schedule(static)
+    for (int z = 0; z < D; z++)
+      for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++) {
+          const REAL xf = (REAL)x - ((REAL)W - RONE) * RHALF;
+          const REAL yf = (REAL)y - ((REAL)H - RONE) * RHALF;
+          const REAL zf = (REAL)z - ((REAL)D - RONE) * RHALF;
+          const REAL u = (REAL)x + p[0] + p[3] * xf + p[4] * yf + p[5] * zf + RHALF;
+          const REAL v = (REAL)y + p[1] + p[6] * xf + p[7] * yf + p[8] * zf + RHALF;
+          const REAL w = (REAL)z + p[2] + p[9] * xf + p[10] * yf + p[11] * zf + RHALF;
+          o[x + (long)y * W + (long)z * W * H] = FN(orc_sample)(interp, s, W, H, D, u, v, w);
+        }
+  }
+}
+
+/* One displacement field applied to T consecutive volumes.
+ * TransformVolumesNonLinear, broccoli_lib.cpp:8361-8451
+ * (InterpolateVolumeNearestNonLinear / LinearNonLinear,
+ * kernelRegistration.cpp:1032-1061, :1111-1140). */
+void FN(orc_transform_field)(const REAL* src, int W, int H, int D, int T, const REAL* dx,
+                             const REAL* dy, const REAL* dz, int interp, REAL* out) {
+  const long V = (long)W * H * D;
+  for (int t = 0; t < T; t++) {
+    const REAL* s = src + t * V;
+    REAL* o = out + t * V;
+#pragma omp parallel for schedule(static)
+    for (int z = 0; z < D; z++)
+      for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++) {
+          const long i = x + (long)y * W + (long)z * W * H;
+          o[i] = FN(orc_sample)(interp, s, W, H, D, (REAL)x + dx[i] + RHALF, (REAL)y + dy[i] + RHALF,
+                                (REAL)z + dz[i] + RHALF);
+        }
+  }
 }
 
 /* Linear registration of `aligned` (warped from `original`) to `ref` over a
@@ -725,8 +789,8 @@ void FN(orc_smooth3d)(const REAL* vol, const REAL* cert, const REAL* scert,
 /* Resample to a new grid size by linear interpolation with sample spacing
  * (N-1)/(N'-1) per axis.  RescaleVolumeLinear, kernelRegistration.cpp:
  * 1340-1366, driven by ChangeVolumeSize, broccoli_lib.cpp:6247-6388. */
-void FN(orc_rescale_linear)(const REAL* src, int W, int H, int D, int W2,
-                            int H2, int D2, REAL* out) {
+static void FN(orc_rescale_interp)(const REAL* src, int W, int H, int D, int W2,
+                                   int H2, int D2, int interp, REAL* out) {
   const REAL dx = (REAL)(W - 1) / (REAL)(W2 - 1);
   const REAL dy = (REAL)(H - 1) / (REAL)(H2 - 1);
   const REAL dz = (REAL)(D - 1) / (REAL)(D2 - 1);
@@ -734,8 +798,13 @@ void FN(orc_rescale_linear)(const REAL* src, int W, int H, int D, int W2,
   for (int z = 0; z < D2; z++)
     for (int y = 0; y < H2; y++)
       for (int x = 0; x < W2; x++)
-        out[x + (long)y * W2 + (long)z * W2 * H2] = FN(orc_sample_linear)(
-            src, W, H, D, (REAL)x * dx + RHALF, (REAL)y * dy + RHALF, (REAL)z * dz + RHALF);
+        out[x + (long)y * W2 + (long)z * W2 * H2] = FN(orc_sample)(
+            interp, src, W, H, D, (REAL)x * dx + RHALF, (REAL)y * dy + RHALF, (REAL)z * dz + RHALF);
+}
+
+void FN(orc_rescale_linear)(const REAL* src, int W, int H, int D, int W2,
+                            int H2, int D2, REAL* out) {
+  FN(orc_rescale_interp)(src, W, H, D, W2, H2, D2, 1, out);
 }
 
 /* myround, broccoli_lib.cpp:94-97. */
@@ -1013,14 +1082,15 @@ void FN(orc_align_nonlinear_scales)(const REAL* ref, REAL* aligned, int W, int H
  * ChangeVolumesResolutionAndSize, broccoli_lib.cpp:6950-7100, with
  * RescaleVolumeLinear and CopyVolumeToNew (kernelRegistration.cpp:
  * 1340-1366, :1593-1678).  Voxels of the new grid not covered stay 0. */
-void FN(orc_change_resolution_and_size)(const REAL* src, int W, int H, int D, float vx, float vy,
-                                        float vz, REAL* out, int W2, int H2, int D2, float nvx,
-                                        float nvy, float nvz, int mm_z_cut) {
+void FN(orc_change_resolution_and_size_interp)(const REAL* src, int W, int H, int D, float vx,
+                                               float vy, float vz, REAL* out, int W2, int H2, int D2,
+                                               float nvx, float nvy, float nvz, int mm_z_cut,
+                                               int mode) {
   const int Wi = FN(orc_myround)((float)W * vx / nvx);
   const int Hi = FN(orc_myround)((float)H * vy / nvy);
   const int Di = FN(orc_myround)((float)D * vz / nvz);
   REAL* interp = (REAL*)malloc(sizeof(REAL) * (long)Wi * Hi * Di);
-  FN(orc_rescale_linear)(src, W, H, D, Wi, Hi, Di, interp);
+  FN(orc_rescale_interp)(src, W, H, D, Wi, Hi, Di, mode, interp);
   for (long i = 0; i < (long)W2 * H2 * D2; i++) out[i] = RZERO;
   const int xd = Wi - W2, yd = Hi - H2, zd = Di - D2;
   const int zcut = (int)round((float)mm_z_cut / nvz);
@@ -1042,6 +1112,13 @@ void FN(orc_change_resolution_and_size)(const REAL* src, int W, int H, int D, fl
   free(interp);
 }
 
+void FN(orc_change_resolution_and_size)(const REAL* src, int W, int H, int D, float vx, float vy,
+                                        float vz, REAL* out, int W2, int H2, int D2, float nvx,
+                                        float nvy, float nvz, int mm_z_cut) {
+  FN(orc_change_resolution_and_size_interp)(src, W, H, D, vx, vy, vz, out, W2, H2, D2, nvx, nvy, nvz,
+                                            mm_z_cut, 1);
+}
+
 /* Centre of mass (voxels), float accumulation in x-fastest order.
  * CalculateCenterOfMass, broccoli_lib.cpp:6763-6800. */
 void FN(orc_center_of_mass)(const REAL* vol, int W, int H, int D, REAL* c3) {
@@ -1058,6 +1135,21 @@ void FN(orc_center_of_mass)(const REAL* vol, int W, int H, int D, REAL* c3) {
   c3[0] = rx / tm;
   c3[1] = ry / tm;
   c3[2] = rz / tm;
+}
+
+/* Centre T volumes by the centre of mass of the first: the integer
+ * translation -myround(N/2 - com) per axis, applied to all T volumes with
+ * the given interpolation.  CenterVolumesWrapper / CenterVolumeMass,
+ * broccoli_lib.cpp:6839-6874, :8225-8245. */
+void FN(orc_center_volumes)(const REAL* src, int W, int H, int D, int T, int interp, REAL* out,
+                            REAL* p12) {
+  REAL c[3];
+  FN(orc_center_of_mass)(src, W, H, D, c);
+  for (int i = 0; i < 12; i++) p12[i] = RZERO;
+  p12[0] = -(REAL)FN(orc_myround)((float)W / 2.0f - (float)c[0]);
+  p12[1] = -(REAL)FN(orc_myround)((float)H / 2.0f - (float)c[1]);
+  p12[2] = -(REAL)FN(orc_myround)((float)D / 2.0f - (float)c[2]);
+  FN(orc_transform_affine)(src, W, H, D, T, p12, interp, out);
 }
 
 /* Translate v1 by the rounded difference of the centres of mass so that it

@@ -223,6 +223,39 @@ void ref_rescale_linear(const float* src, int W, int H, int D, int W2, int H2, i
           [&] { clr::RescaleVolumeLinear(out, im, vx, vy, vz, W2, H2, D2); });
 }
 
+// TransformVolumesLinear, broccoli_lib.cpp:8267-8359: the volumes one after
+// another through InterpolateVolumeNearestLinear (interp 0) or
+// InterpolateVolumeLinearLinear (1), kernelRegistration.cpp:995-1101.
+void ref_transform_linear(const float* src, int W, int H, int D, int T, const float* p12, int interp,
+                          float* out) {
+  const long V = (long)W * H * D;
+  for (int t = 0; t < T; t++) {
+    const image3d_t im{src + t * V, W, H, D};
+    ndrange(roundup(W, 16), roundup(H, 16), D, 16, 16, 1, [&] {
+      if (interp == 0)
+        clr::InterpolateVolumeNearestLinear(out, im, p12, W, H, D, t);
+      else
+        clr::InterpolateVolumeLinearLinear(out, im, p12, W, H, D, t);
+    });
+  }
+}
+
+// TransformVolumesNonLinear, broccoli_lib.cpp:8361-8451
+// (InterpolateVolumeNearestNonLinear / LinearNonLinear).
+void ref_transform_nonlinear(const float* src, int W, int H, int D, int T, const float* dx, const float* dy,
+                             const float* dz, int interp, float* out) {
+  const long V = (long)W * H * D;
+  for (int t = 0; t < T; t++) {
+    const image3d_t im{src + t * V, W, H, D};
+    ndrange(roundup(W, 16), roundup(H, 16), D, 16, 16, 1, [&] {
+      if (interp == 0)
+        clr::InterpolateVolumeNearestNonLinear(out, im, dx, dy, dz, W, H, D, t);
+      else
+        clr::InterpolateVolumeLinearNonLinear(out, im, dx, dy, dz, W, H, D, t);
+    });
+  }
+}
+
 // AlignTwoVolumesLinear, broccoli_lib.cpp:5273-5437 (type 0 TRANSLATION,
 // 1 RIGID, 2 AFFINE).  `aligned` is updated in place; `original` is the
 // image that is re-sampled each iteration.
@@ -404,6 +437,36 @@ void ref_change_resolution_and_size(const float* src, int W, int H, int D, float
   });
 }
 
+// ChangeVolumesResolutionAndSize with INTERPOLATION_MODE 0 (RescaleVolumeNearest,
+// kernelRegistration.cpp:1312-1338) or 1 (RescaleVolumeLinear) for T volumes,
+// broccoli_lib.cpp:6950-7100.
+void ref_change_resolution_and_size_interp(const float* src, int W, int H, int D, int T, float vx, float vy,
+                                           float vz, float* out, int W2, int H2, int D2, float nvx, float nvy,
+                                           float nvz, int mm_z_cut, int interp) {
+  const int Wi = myround_((float)W * vx / nvx), Hi = myround_((float)H * vy / nvy),
+            Di = myround_((float)D * vz / nvz);
+  const float rx = (float)(W - 1) / (float)(Wi - 1), ry = (float)(H - 1) / (float)(Hi - 1),
+              rz = (float)(D - 1) / (float)(Di - 1);
+  const long V = (long)W * H * D, V2 = (long)W2 * H2 * D2;
+  std::vector<float> interp_v((long)Wi * Hi * Di, 0.f);
+  for (int t = 0; t < T; t++) {
+    const image3d_t im{src + t * V, W, H, D};
+    ndrange(roundup(Wi, 16), roundup(Hi, 16), Di, 16, 16, 1, [&] {
+      if (interp == 0)
+        clr::RescaleVolumeNearest(interp_v.data(), im, rx, ry, rz, Wi, Hi, Di);
+      else
+        clr::RescaleVolumeLinear(interp_v.data(), im, rx, ry, rz, Wi, Hi, Di);
+    });
+    float* o = out + t * V2;
+    std::memset(o, 0, sizeof(float) * V2);
+    const int gx = W2 > Wi ? W2 : Wi, gy = H2 > Hi ? H2 : Hi, gz = D2 > Di ? D2 : Di;
+    ndrange(roundup(gx, 16), roundup(gy, 16), gz, 16, 16, 1, [&] {
+      clr::CopyVolumeToNew(o, interp_v.data(), W2, H2, D2, Wi, Hi, Di, Wi - W2, Hi - H2, Di - D2, mm_z_cut,
+                           nvz, 0);
+    });
+  }
+}
+
 // CalculateCenterOfMass, broccoli_lib.cpp:6763-6800 (host loop).
 static void com_(const float* v, int W, int H, int D, float* c) {
   float tm = 0.f, rx = 0.f, ry = 0.f, rz = 0.f;
@@ -433,6 +496,19 @@ void ref_match_volume_masses(float* v1, const float* v2, int W, int H, int D, fl
   p12[2] = -(float)myround_(c2[2] - c1[2]);
   std::vector<float> tmp(v1, v1 + (long)W * H * D);
   ref_warp_affine(tmp.data(), W, H, D, p12, v1);
+}
+
+// CenterVolumesWrapper, broccoli_lib.cpp:8225-8245, with CenterVolumeMass
+// (:6839-6874): translation from the first volume's centre of mass, then
+// TransformVolumesLinear of all T volumes.
+void ref_center_volumes(const float* src, int W, int H, int D, int T, int interp, float* out, float* p12) {
+  float c[3];
+  com_(src, W, H, D, c);
+  for (int i = 0; i < 12; i++) p12[i] = 0.f;
+  p12[0] = -(float)myround_((float)W / 2.0f - c[0]);
+  p12[1] = -(float)myround_((float)H / 2.0f - c[1]);
+  p12[2] = -(float)myround_((float)D / 2.0f - c[2]);
+  ref_transform_linear(src, W, H, D, T, p12, interp, out);
 }
 
 // CreateCombinedDisplacementField, broccoli_lib.cpp:8115-8150, with

@@ -146,6 +146,36 @@ def main_smooth_normalized() -> None:
     print("wrote smooth_normalized.npz; NaN voxels per volume:", int(np.isnan(out[0]).sum()))
 
 
+def main_transforms() -> None:
+    """The 4D transforms on the reference's kernels (TransformVolumesLinear /
+    NonLinear, CenterVolumesWrapper, ChangeVolumesResolutionAndSize with
+    NEAREST = 0 and LINEAR = 1), on a short series of smooth volumes with
+    an off-centre blob."""
+    shape = (11, 14, 17)
+    rng = np.random.Generator(np.random.PCG64(21))
+    z, y, x = np.meshgrid(*[np.arange(n) for n in shape], indexing="ij")
+    blob = np.exp(-(((z - 3.5) / 3.0) ** 2 + ((y - 9.0) / 4.0) ** 2 + ((x - 5.0) / 3.5) ** 2)) * 500.0
+    vols = (blob[None] + rng.standard_normal((3,) + shape) * 5 + 100).astype(np.float32)
+    p12 = np.array([1.37, -0.81, 0.55, 0.031, -0.012, 0.024, 0.018, -0.027, 0.011, -0.022, 0.016, 0.013],
+                   np.float32)
+    field = (rng.standard_normal((3,) + shape) * 1.7).astype(np.float32)
+    vin, vnew, shape2, zcut = (2.0, 2.5, 3.0), (1.5, 2.0, 3.5), (14, 12, 10), 2
+    g = {"vols": vols, "p12": p12, "field": field, "vin": np.array(vin, np.float32),
+         "vnew": np.array(vnew, np.float32), "shape2": np.array(shape2, np.int32), "zcut": np.int32(zcut)}
+    for interp, tag in ((0, "nearest"), (1, "linear")):
+        g["affine_" + tag] = O.ref_transform_affine(vols, p12, interp)
+        g["field_" + tag] = O.ref_transform_field(vols, *field, interp=interp)
+        g["center_" + tag], g["center_p12_" + tag] = O.ref_center_volumes(vols, interp)
+        g["resize_" + tag] = O.ref_change_resolution_and_size_interp(vols, vin, shape2, vnew, zcut, interp)
+    f2 = field.copy()
+    O.ref_lib().ref_add_linear_nonlinear(f2.ctypes.data_as(O._P), shape[2], shape[1], shape[0],
+                                         p12.ctypes.data_as(O._P))
+    g["combined_field"] = f2
+    np.savez_compressed(os.path.join(HERE, "transforms.npz"), **g)
+    print("wrote transforms.npz")
+
+
 if __name__ == "__main__":
     main()
     main_smooth_normalized()
+    main_transforms()

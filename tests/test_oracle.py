@@ -162,3 +162,35 @@ def test_smooth_normalized_matches_reference_kernels():
     out = O.smooth_normalized(g["vols"], g["mask"], fs, fs, fs)
     assert np.array_equal(out, g["out"], equal_nan=True)
     assert np.isnan(out).any() and np.isfinite(out[:, 8, 9, 10]).all()
+
+
+@pytest.fixture(scope="module")
+def golden_tf():
+    import os
+    from conftest import GOLDEN
+    return dict(np.load(os.path.join(GOLDEN, "transforms.npz")))
+
+
+@pytest.mark.parametrize("interp,tag", [(0, "nearest"), (1, "linear")])
+def test_transforms_match_reference_kernels(orc, golden_tf, interp, tag):
+    """TransformVolumesLinear / NonLinear, CenterVolumesWrapper and
+    ChangeVolumesResolutionAndSize of a 3-volume series: the restatement
+    equals the reference's kernels (golden vectors) bit for bit."""
+    g = golden_tf
+    v = g["vols"]
+    assert np.array_equal(orc.transform_affine(v, g["p12"], interp), g["affine_" + tag])
+    assert np.array_equal(orc.transform_field(v, *g["field"], interp=interp), g["field_" + tag])
+    c, p = orc.center_volumes(v, interp)
+    assert np.array_equal(p, g["center_p12_" + tag])
+    assert np.array_equal(c, g["center_" + tag])
+    r = orc.change_resolution_and_size_interp(v, g["vin"], tuple(g["shape2"]), g["vnew"], int(g["zcut"]), interp)
+    assert np.array_equal(r, g["resize_" + tag])
+
+
+def test_combined_field_matches_reference_kernel(orc, golden_tf):
+    g = golden_tf
+    f = np.ascontiguousarray(g["field"], np.float32).copy()
+    D, H, W = f.shape[1:]
+    orc.orc_lib().orc_add_linear_nonlinear_f32(f.ctypes.data_as(orc._P), W, H, D,
+                                               np.ascontiguousarray(g["p12"]).ctypes.data_as(orc._P))
+    assert np.array_equal(f, g["combined_field"])
