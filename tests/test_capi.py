@@ -20,6 +20,15 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_library_exports_the_nifti_header():
+    import os
+    path = os.path.join(os.path.dirname(L.HEADER_PATH), "broccoli_nifti.h")
+    syms = L.header_symbols(path)
+    assert {"brc_nifti_read", "brc_nifti_write", "brc_nifti_free", "brc_nifti_error"} <= set(syms)
+    lib = L.lib()
+    assert all(hasattr(lib, s) for s in syms)
+
+
 def test_status_strings_and_version():
     assert L.status_string(L.BRC_OK) == "ok"
     assert "invalid" in L.status_string(L.BRC_ERR_INVALID)
