@@ -175,6 +175,59 @@ def cpu_reference_rate(vols, flt, n_regs: int, iters: int = ITERS):
     return n_regs / dt, kind, oracle.num_threads(), dt
 
 
+def normalisation_rates(ctx, prec) -> dict:
+    """T1-to-template normalisation (affine, then nonlinear over the scales
+    8, 4, 2, 1 with the six nonlinear filters; 10 + 10 iterations) timed with
+    CUDA events: one subject of 256 x 256 x 170 1-mm voxels (a head phantom
+    warped by a smooth 6-mm field) and a cohort of 64 subjects with per-axis
+    sizes U{160..256} (seeds 300 + i, crops of one 256^3 phantom), both onto a
+    182 x 218 x 182 1-mm template phantom.  Filters: the reference's shipped
+    linear and nonlinear banks (tests/golden/filters)."""
+    import torch
+    from broccoli_b200 import filters as F
+    from broccoli_b200 import synthetic as S
+    bank = F.load_filter_dir(os.path.join(ROOT, "tests", "golden", "filters"))
+    tpl = torch.from_numpy(S.head_phantom((182, 218, 182), seed=2)).cuda()
+    subj_np = S.warp_with_field(S.head_phantom((170, 256, 256), seed=1),
+                                S.smooth_field((170, 256, 256), seed=200, max_mm=6.0))
+    subj = torch.from_numpy(np.ascontiguousarray(subj_np, np.float32)).cuda()
+    one = (1.0, 1.0, 1.0)
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    two = lambda: ctx.register_two_volumes(subj, one, tpl, one, bank, 10, 10, 8, precision=prec)  # noqa: E731
+    timed(two)
+    ms1 = min(timed(two) for _ in range(3))
+    big = S.head_phantom((256, 256, 256), seed=3)
+    subjects, sizes = [], []
+    for i in range(64):
+        rng = np.random.Generator(np.random.PCG64(300 + i))
+        d, h, w = (int(v) for v in rng.integers(160, 257, 3))
+        z0, y0, x0 = (256 - d) // 2, (256 - h) // 2, (256 - w) // 2
+        subjects.append(torch.from_numpy(np.ascontiguousarray(big[z0:z0 + d, y0:y0 + h, x0:x0 + w])).cuda())
+        sizes.append((w, h, d))
+    coh = lambda: ctx.register_cohort(subjects, [one] * 64, tpl, one, bank, 10, 10, 8, precision=prec)  # noqa: E731
+    timed(coh)
+    ms64 = timed(coh)
+    return {
+        "t1_to_template": {"value": 1000.0 / ms1, "unit": "subjects/s", "ms_per_subject": ms1,
+                           "config": {"subject": [256, 256, 170], "template": [182, 218, 182], "voxel_mm": 1.0,
+                                      "linear_iterations": 10, "nonlinear_iterations": 10,
+                                      "scales": [8, 4, 2, 1]}},
+        "cohort": {"value": 64 * 1000.0 / ms64, "unit": "subjects/s", "ms": ms64,
+                   "config": {"subjects": 64, "sizes": "U{160..256} per axis (seeds 300 + i)",
+                              "template": [182, 218, 182], "linear_iterations": 10,
+                              "nonlinear_iterations": 10, "scales": [8, 4, 2, 1]}},
+    }
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -448,6 +501,8 @@ def run_gpu(args, rank, world, local_rank):
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
+    if not args.skip_normalisation:
+        line.update(normalisation_rates(ctx, prec))
     print(json.dumps(line))
 
 
@@ -459,6 +514,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-accuracy", action="store_true")
+    ap.add_argument("--skip-normalisation", action="store_true",
+                    help="skip the T1-to-template and cohort timings (configs 2 and 4)")
     ap.add_argument("--series", type=int, default=T, help="series length (volumes)")
     ap.add_argument("--precision", default="bf16x3", choices=["fp32", "bf16x3"],
                     help="filtering precision of the timed path (bf16x3: tensor-core split BF16)")
