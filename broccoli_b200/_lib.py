@@ -71,6 +71,56 @@ class TwoVolumeOpts(ctypes.Structure):
     ]
 
 
+_F3 = ctypes.c_float * 3
+
+
+class FirstLevelInput(ctypes.Structure):
+    _fields_ = [
+        ("fmri", ctypes.c_void_p),
+        ("epi_w", ctypes.c_int), ("epi_h", ctypes.c_int), ("epi_d", ctypes.c_int), ("epi_t", ctypes.c_int),
+        ("epi_voxel", _F3),
+        ("t1", ctypes.c_void_p),
+        ("t1_w", ctypes.c_int), ("t1_h", ctypes.c_int), ("t1_d", ctypes.c_int),
+        ("t1_voxel", _F3),
+        ("mni", ctypes.c_void_p),
+        ("mni_w", ctypes.c_int), ("mni_h", ctypes.c_int), ("mni_d", ctypes.c_int),
+        ("mni_voxel", _F3),
+        ("filters3", ctypes.c_void_p),
+        ("filters6", ctypes.c_void_p),
+        ("tensors", ctypes.c_void_p),
+        ("dirs", ctypes.c_void_p),
+    ]
+
+
+class FirstLevelOpts(ctypes.Structure):
+    _fields_ = [
+        ("linear_iterations", ctypes.c_int),
+        ("nonlinear_iterations", ctypes.c_int),
+        ("motion_iterations", ctypes.c_int),
+        ("coarsest_scale_t1_mni", ctypes.c_int),
+        ("coarsest_scale_epi_t1", ctypes.c_int),
+        ("mm_t1_z_cut", ctypes.c_int),
+        ("apply_motion_correction", ctypes.c_int),
+        ("apply_smoothing", ctypes.c_int),
+        ("smoothing_fwhm", ctypes.c_float),
+        ("tsigma", ctypes.c_float),
+        ("esigma", ctypes.c_float),
+        ("dsigma", ctypes.c_float),
+        ("precision", ctypes.c_int),
+        ("solve_fp64", ctypes.c_int),
+    ]
+
+
+FIRST_LEVEL_OUTPUTS = ("params_t1_mni", "params_epi_t1", "params_epi_mni", "motion_parameters", "interpolated_t1",
+                       "aligned_t1_linear", "aligned_t1_nonlinear", "field", "aligned_epi_t1",
+                       "aligned_epi_mni_linear", "aligned_epi_mni_nonlinear", "motion_corrected", "epi_mask",
+                       "smoothed")
+
+
+class FirstLevelOutput(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in FIRST_LEVEL_OUTPUTS]
+
+
 _lib = None
 
 _P = ctypes.c_void_p
@@ -121,6 +171,12 @@ _SIGS = {
     "brc_register_two_volumes": (
         [_P, _P, _I, _I, _I, _P, _P, _I, _I, _I, _P, _P, _P, _P, _P, ctypes.POINTER(TwoVolumeOpts), _P, _P,
          _P, _P, _P], _I),
+    "brc_smoothing_filters_fwhm": ([ctypes.c_float, _P, _P, _P, _P], None),
+    "brc_tensor_magnitude": ([_P, _P, _I, _I, _I, _P, _P, _I, _P], _I),
+    "brc_segment_epi": ([_P, _P, _I, _I, _I, _P, _P], _I),
+    "brc_first_level_opts_default": ([ctypes.POINTER(FirstLevelOpts)], None),
+    "brc_first_level_preprocess": ([_P, ctypes.POINTER(FirstLevelInput), ctypes.POINTER(FirstLevelOpts),
+                                    ctypes.POINTER(FirstLevelOutput)], _I),
     "brc_register_cohort": (
         [_P, _I, _P, _P, _P, _P, _I, _I, _I, _P, _P, _P, _P, _P, ctypes.POINTER(TwoVolumeOpts), _P, _P, _P, _P],
         _I),

@@ -505,3 +505,82 @@ class Context:
             f.ctypes.data_as(ctypes.c_void_p), ctypes.byref(opts), refp,
             motion.ctypes.data_as(ctypes.c_void_p)))
         return v, motion.reshape(6, T)
+
+    @staticmethod
+    def smoothing_filters_fwhm(fwhm: float, voxel_size):
+        """Gaussian filters (9 taps per axis) from a FWHM in mm: (fx, fy, fz)."""
+        vs = np.ascontiguousarray(voxel_size, np.float32)
+        f = [np.zeros(9, np.float32) for _ in range(3)]
+        L.lib().brc_smoothing_filters_fwhm(float(fwhm), vs.ctypes.data_as(ctypes.c_void_p),
+                                           *[a.ctypes.data_as(ctypes.c_void_p) for a in f])
+        return tuple(f)
+
+    def tensor_magnitude(self, vol: torch.Tensor, bank: dict, precision: int = L.PREC_FP32) -> torch.Tensor:
+        """Frobenius norm of the structure tensor of one (D,H,W) volume."""
+        v = vol.contiguous()
+        D, H, W = v.shape
+        f6, m, _ = self._nl_consts(bank)
+        out = torch.empty_like(v)
+        self._bind_stream()
+        _check(self, L.lib().brc_tensor_magnitude(self.handle, _p(v), W, H, D, f6.ctypes.data_as(ctypes.c_void_p),
+                                                  m.ctypes.data_as(ctypes.c_void_p), precision, _p(out)))
+        return out
+
+    def segment_epi(self, vol: torch.Tensor, voxel_size) -> torch.Tensor:
+        """Brain mask (1 / 0.001) of one (D,H,W) EPI volume."""
+        v = vol.contiguous()
+        D, H, W = v.shape
+        vs = np.ascontiguousarray(voxel_size, np.float32)
+        out = torch.empty_like(v)
+        self._bind_stream()
+        _check(self, L.lib().brc_segment_epi(self.handle, _p(v), W, H, D, vs.ctypes.data_as(ctypes.c_void_p),
+                                             _p(out)))
+        return out
+
+    def first_level_preprocess(self, fmri: np.ndarray, epi_voxel_size, t1: np.ndarray, t1_voxel_size,
+                               mni: np.ndarray, mni_voxel_size, bank: dict, linear_iterations: int = 10,
+                               nonlinear_iterations: int = 10, motion_iterations: int = 5,
+                               coarsest_scale_t1_mni: int = 4, coarsest_scale_epi_t1: int = 4,
+                               mm_t1_z_cut: int = 0, apply_motion_correction: bool = True,
+                               apply_smoothing: bool = True, smoothing_fwhm: float = 6.0, tsigma=5.0, esigma=5.0,
+                               dsigma=5.0, solve_fp64: bool = False, precision: int = L.PREC_FP32):
+        """The preprocessing stages of a first-level analysis on host arrays:
+        fmri (T,D,H,W), t1 and mni (D,H,W), voxel sizes (x, y, z) in mm.
+        Returns a dict of every output of brc_first_level_preprocess (as
+        numpy arrays) plus "fmri", the preprocessed series (the input array
+        is not modified)."""
+        v = np.ascontiguousarray(fmri, np.float32).copy()
+        T, D1, H1, W1 = v.shape
+        t = np.ascontiguousarray(t1, np.float32)
+        m = np.ascontiguousarray(mni, np.float32)
+        D2, H2, W2 = t.shape
+        D3, H3, W3 = m.shape
+        f3 = np.ascontiguousarray(bank["linear"], np.float32)
+        f6, mt, d = self._nl_consts(bank)
+        cp = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+        inp = L.FirstLevelInput(cp(v), W1, H1, D1, T, L._F3(*epi_voxel_size), cp(t), W2, H2, D2,
+                                L._F3(*t1_voxel_size), cp(m), W3, H3, D3, L._F3(*mni_voxel_size), cp(f3), cp(f6),
+                                cp(mt), cp(d))
+        o = L.FirstLevelOpts()
+        L.lib().brc_first_level_opts_default(ctypes.byref(o))
+        o.linear_iterations, o.nonlinear_iterations = linear_iterations, nonlinear_iterations
+        o.motion_iterations = motion_iterations
+        o.coarsest_scale_t1_mni, o.coarsest_scale_epi_t1 = coarsest_scale_t1_mni, coarsest_scale_epi_t1
+        o.mm_t1_z_cut = mm_t1_z_cut
+        o.apply_motion_correction, o.apply_smoothing = int(apply_motion_correction), int(apply_smoothing)
+        o.smoothing_fwhm = smoothing_fwhm
+        o.tsigma, o.esigma, o.dsigma = tsigma, esigma, dsigma
+        o.precision, o.solve_fp64 = precision, int(solve_fp64)
+        shapes = {"params_t1_mni": (12,), "params_epi_t1": (12,), "params_epi_mni": (12,),
+                  "motion_parameters": (6, T), "interpolated_t1": (D3, H3, W3),
+                  "aligned_t1_linear": (D3, H3, W3), "aligned_t1_nonlinear": (D3, H3, W3),
+                  "field": (3, D3, H3, W3), "aligned_epi_t1": (D3, H3, W3), "aligned_epi_mni_linear": (D3, H3, W3),
+                  "aligned_epi_mni_nonlinear": (D3, H3, W3), "motion_corrected": (T, D1, H1, W1),
+                  "epi_mask": (D1, H1, W1), "smoothed": (T, D1, H1, W1)}
+        res = {k: np.zeros(shapes[k], np.float32) for k in L.FIRST_LEVEL_OUTPUTS}
+        out = L.FirstLevelOutput(*[cp(res[k]) for k in L.FIRST_LEVEL_OUTPUTS])
+        self._bind_stream()
+        _check(self, L.lib().brc_first_level_preprocess(self.handle, ctypes.byref(inp), ctypes.byref(o),
+                                                        ctypes.byref(out)))
+        res["fmri"] = v
+        return res

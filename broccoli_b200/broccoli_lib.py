@@ -62,6 +62,10 @@ class BROCCOLI_LIB:
         self.mc_tolerance = 0.0
         self.precision = L.PREC_FP32
         self.out = {}
+        self.save = {}
+        self.coarsest_epi_t1 = 4
+        self.apply_mc, self.apply_smoothing, self.apply_slice_timing = True, True, False
+        self.preprocessing_only = False
         if len(args) == 2:
             self.OpenCLInitiate(*args)
 
@@ -230,6 +234,25 @@ class BROCCOLI_LIB:
     def SetNumberOfIterationsForNonParametricImageRegistration(self, n): self.it_nonlinear = int(n)
     def SetNumberOfIterationsForMotionCorrection(self, n): self.it_mc = int(n)
     def SetCoarsestScaleT1MNI(self, n): self.coarsest = int(n)
+    def SetCoarsestScaleEPIT1(self, n): self.coarsest_epi_t1 = int(n)
+    def SetApplyMotionCorrection(self, b): self.apply_mc = bool(b)
+    def SetApplySmoothing(self, b): self.apply_smoothing = bool(b)
+    def SetApplySliceTimingCorrection(self, b): self.apply_slice_timing = bool(b)
+    def SetPreprocessingOnly(self, b): self.preprocessing_only = bool(b)
+    def SetOutputEPIT1RegistrationParameters(self, a): self.out["params_epi_t1"] = a
+    def SetOutputEPIMNIRegistrationParameters(self, a): self.out["params_epi_mni"] = a
+    def SetOutputAlignedEPIVolumeT1(self, a): self.out["aligned_epi_t1"] = a
+    def SetOutputAlignedEPIVolumeMNILinear(self, a): self.out["aligned_epi_mni_linear"] = a
+    def SetOutputAlignedEPIVolumeMNINonlinear(self, a): self.out["aligned_epi_mni_nonlinear"] = a
+    def SetOutputEPIMask(self, a): self.out["epi_mask"] = a
+    def SetSaveInterpolatedT1(self, b): self.save["interpolated_t1"] = bool(b)
+    def SetSaveAlignedT1MNILinear(self, b): self.save["aligned_t1_linear"] = bool(b)
+    def SetSaveAlignedT1MNINonLinear(self, b): self.save["aligned_t1_nonlinear"] = bool(b)
+    def SetSaveAlignedEPIT1(self, b): self.save["aligned_epi_t1"] = bool(b)
+    def SetSaveAlignedEPIMNI(self, b): self.save["aligned_epi_mni"] = bool(b)
+    def SetSaveEPIMask(self, b): self.save["epi_mask"] = bool(b)
+    def SetSaveMotionCorrected(self, b): self.save["motion_corrected"] = bool(b)
+    def SetSaveSmoothed(self, b): self.save["smoothed"] = bool(b)
     def SetMMT1ZCUT(self, mm): self.mm_z_cut = int(mm)
     def SetInterpolationMode(self, mode):
         # the registration loops resample linearly whatever the mode (as the
@@ -333,6 +356,53 @@ class BROCCOLI_LIB:
                 self.out["field"][a][...] = f[a].reshape(self.out["field"][a].shape)
         ctx.close()
 
+    def PerformFirstLevelAnalysisWrapper(self):
+        """The preprocessing of PerformFirstLevelAnalysisWrapper
+        (broccoli_lib.cpp:8466-8733) on brc_first_level_preprocess: the
+        fMRI volumes are replaced by the preprocessed series; the parameter
+        vectors and motion parameters are written always, the volumes when
+        their SetSave* flag is on.  The statistics are not part of this
+        library (SetPreprocessingOnly(True) is required) and slice-timing
+        correction must be off."""
+        from .api import Context
+        if not self.preprocessing_only:
+            raise L.BrcError(L.BRC_ERR_UNSUPPORTED, "PerformFirstLevelAnalysisWrapper: the statistical analysis "
+                                                    "is not part of this library; call SetPreprocessingOnly(True)")
+        if self.apply_slice_timing:
+            raise L.BrcError(L.BRC_ERR_UNSUPPORTED,
+                             "PerformFirstLevelAnalysisWrapper: slice-timing correction is not supported")
+        W, H, D, T = self.epi
+        W2, H2, D2 = self.t1
+        W3, H3, D3 = self.mni
+        ctx = Context(0)
+        bank = {"linear": self.linear_filters, "nonlinear": self.nonlinear_filters,
+                "projection_tensors": self.projection_tensors, "directions": self.directions}
+        r = ctx.first_level_preprocess(
+            np.asarray(self.fmri, np.float32).reshape(T, D, H, W), self.epi_vox,
+            np.asarray(self.t1_volume, np.float32).reshape(D2, H2, W2), self.t1_vox,
+            np.asarray(self.mni_volume, np.float32).reshape(D3, H3, W3), self.mni_vox, bank, self.it_linear,
+            self.it_nonlinear, self.it_mc, self.coarsest, self.coarsest_epi_t1, self.mm_z_cut, self.apply_mc,
+            self.apply_smoothing, getattr(self, "epi_fwhm", 8.0), *self.sigmas, precision=self.precision)
+        ctx.close()
+        self.fmri[...] = r["fmri"].reshape(self.fmri.shape)
+        written = {"params": "params_t1_mni", "params_epi_t1": "params_epi_t1", "params_epi_mni": "params_epi_mni"}
+        if self.apply_mc:
+            written["motion"] = "motion_parameters"
+        flags = {"interpolated": ("interpolated_t1", "interpolated_t1"),
+                 "aligned_linear": ("aligned_t1_linear", "aligned_t1_linear"),
+                 "aligned_nonlinear": ("aligned_t1_nonlinear", "aligned_t1_nonlinear"),
+                 "aligned_epi_t1": ("aligned_epi_t1", "aligned_epi_t1"),
+                 "aligned_epi_mni_linear": ("aligned_epi_mni", "aligned_epi_mni_linear"),
+                 "aligned_epi_mni_nonlinear": ("aligned_epi_mni", "aligned_epi_mni_nonlinear"),
+                 "epi_mask": ("epi_mask", "epi_mask"), "mc": ("motion_corrected", "motion_corrected"),
+                 "smoothed": ("smoothed", "smoothed")}
+        for k, (flag, key) in flags.items():
+            if self.save.get(flag, False):
+                written[k] = key
+        for k, key in written.items():
+            if k in self.out:
+                dst = self.out[k]
+                dst[...] = np.asarray(r[key], np.float32).reshape(-1)[: dst.size].reshape(dst.shape)
 
     # ---- 4D transforms (TransformVolumesLinear/NonLinearWrapper,
     # CenterVolumesWrapper, broccoli_lib.cpp:8145-8245) ------------------------
@@ -438,3 +508,74 @@ def performMotionCorrection(h_fMRI_Volumes, h_fMRI_Voxel_Sizes, h_Quadrature_Fil
     B.SetOutputMotionParameters(motion)
     B.PerformMotionCorrectionWrapper()
     return B.unpackOutputVolume(corrected, shape), B.unpackOutputArray(motion, (6, T))
+
+
+def performFirstLevelPreprocessing(fMRI_data, fMRI_voxel_sizes, T1_data, T1_voxel_sizes, MNI_brain_data,
+                                   MNI_voxel_sizes, parametric_filters, nonparametric_filters, projection_tensor,
+                                   filter_directions, iterations_parametric, iterations_nonparametric,
+                                   iterations_motion_correction, coarsest_scale_T1_MNI, coarsest_scale_EPI_T1,
+                                   mm_T1_z_cut, EPI_smoothing, opencl_platform=0, opencl_device=0):
+    """The registration, motion-correction and smoothing stages of
+    firstlevel.py:performFirstLevelAnalysis (Python_Wrapper/broccoli/
+    firstlevel.py:21-181) through the wrapper class with
+    SetPreprocessingOnly(True): the same packing (fMRI flipped up-down, the
+    template brain divided by its maximum) and parameter setters.  Returns a
+    dict: T1_MNI_registration_parameters, EPI_T1_registration_parameters,
+    EPI_MNI_registration_parameters, motion_parameters (6, T),
+    motion_corrected_fMRI_data, smoothed_fMRI_data, EPI_mask,
+    aligned_T1_volume, aligned_T1_volume_nonparametric and
+    aligned_EPI_volume (template space, linear)."""
+    B = BROCCOLI_LIB(opencl_platform, opencl_device)
+    if not B.GetOpenCLInitiated():
+        raise RuntimeError("initialisation failed: " + B.GetOpenCLInitializationError())
+    fMRI_data = np.flipud(fMRI_data)
+    MNI_brain_data = MNI_brain_data / MNI_brain_data.max()
+    B.SetfMRIData(fMRI_data, fMRI_voxel_sizes)
+    B.SetT1Data(T1_data, T1_voxel_sizes)
+    B.SetMNIData(MNI_brain_data, MNI_voxel_sizes)
+    B.SetInputMNIBrainVolume(B.packVolume(MNI_brain_data))
+    B.SetNumberOfIterationsForParametricImageRegistration(iterations_parametric)
+    B.SetNumberOfIterationsForNonParametricImageRegistration(iterations_nonparametric)
+    B.SetImageRegistrationFilterSize(parametric_filters[0][0].shape[0])
+    B.SetParametricImageRegistrationFilters(parametric_filters)
+    B.SetNonParametricImageRegistrationFilters(nonparametric_filters)
+    B.SetProjectionTensorMatrixFilters(projection_tensor)
+    B.SetFilterDirections(*[B.packArray(f) for f in filter_directions])
+    B.SetNumberOfIterationsForMotionCorrection(iterations_motion_correction)
+    B.SetCoarsestScaleT1MNI(coarsest_scale_T1_MNI)
+    B.SetCoarsestScaleEPIT1(coarsest_scale_EPI_T1)
+    B.SetMMT1ZCUT(mm_T1_z_cut)
+    B.SetEPISmoothingAmount(EPI_smoothing)
+    B.SetPreprocessingOnly(True)
+    T = fMRI_data.shape[3]
+    r = {"T1_MNI_registration_parameters": B.createOutputArray(12),
+         "EPI_T1_registration_parameters": B.createOutputArray(12),
+         "EPI_MNI_registration_parameters": B.createOutputArray(12),
+         "motion_parameters": B.createOutputArray(6 * T),
+         "motion_corrected_fMRI_data": B.createOutputArray(fMRI_data.shape),
+         "smoothed_fMRI_data": B.createOutputArray(fMRI_data.shape),
+         "EPI_mask": B.createOutputArray(fMRI_data.shape[0:3]),
+         "aligned_T1_volume": B.createOutputArray(MNI_brain_data.shape),
+         "aligned_T1_volume_nonparametric": B.createOutputArray(MNI_brain_data.shape),
+         "aligned_EPI_volume": B.createOutputArray(MNI_brain_data.shape)}
+    B.SetOutputT1MNIRegistrationParameters(r["T1_MNI_registration_parameters"])
+    B.SetOutputEPIT1RegistrationParameters(r["EPI_T1_registration_parameters"])
+    B.SetOutputEPIMNIRegistrationParameters(r["EPI_MNI_registration_parameters"])
+    B.SetOutputMotionParameters(r["motion_parameters"])
+    B.SetOutputMotionCorrectedfMRIVolumes(r["motion_corrected_fMRI_data"])
+    B.SetOutputSmoothedfMRIVolumes(r["smoothed_fMRI_data"])
+    B.SetOutputEPIMask(r["EPI_mask"])
+    B.SetOutputAlignedT1VolumeLinear(r["aligned_T1_volume"])
+    B.SetOutputAlignedT1VolumeNonLinear(r["aligned_T1_volume_nonparametric"])
+    B.SetOutputAlignedEPIVolumeMNILinear(r["aligned_EPI_volume"])
+    for save in (B.SetSaveMotionCorrected, B.SetSaveSmoothed, B.SetSaveEPIMask, B.SetSaveAlignedT1MNILinear,
+                 B.SetSaveAlignedT1MNINonLinear, B.SetSaveAlignedEPIMNI):
+        save(True)
+    B.PerformFirstLevelAnalysisWrapper()
+    r["motion_parameters"] = B.unpackOutputArray(r["motion_parameters"], (6, T))
+    for k in ("motion_corrected_fMRI_data", "smoothed_fMRI_data"):
+        r[k] = B.unpackOutputVolume(r[k], fMRI_data.shape)
+    r["EPI_mask"] = B.unpackOutputVolume(r["EPI_mask"], fMRI_data.shape[0:3])
+    for k in ("aligned_T1_volume", "aligned_T1_volume_nonparametric", "aligned_EPI_volume"):
+        r[k] = B.unpackOutputVolume(r[k], MNI_brain_data.shape)
+    return r

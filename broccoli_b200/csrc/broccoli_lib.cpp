@@ -14,18 +14,7 @@ namespace {
 // normalised by their float sums (CreateSmoothingFilters,
 // broccoli_lib.cpp:11055-11091).
 void fwhm_filters(float fwhm, const float* vox, float* fx, float* fy, float* fz) {
-  float* f[3] = {fx, fy, fz};
-  for (int a = 0; a < 3; a++) {
-    const double sigma = (double)fwhm / 2.354 / (double)vox[a];
-    const double s2 = 2.0 * sigma * sigma;
-    float sum = 0.0f;
-    for (int i = 0; i < 9; i++) {
-      const double u = (double)(i - 4);
-      f[a][i] = (float)exp(-pow(u, 2.0) / s2);
-      sum += f[a][i];
-    }
-    for (int i = 0; i < 9; i++) f[a][i] /= sum;
-  }
+  brc_smoothing_filters_fwhm(fwhm, vox, fx, fy, fz);
 }
 
 // RAII device buffer over brc_device_alloc / brc_device_free.
@@ -157,6 +146,11 @@ void BROCCOLI_LIB::SetNumberOfIterationsForMotionCorrection(int N) { it_mc_ = N;
 void BROCCOLI_LIB::SetChangeMotionCorrectionReferenceVolume(bool c) { change_mc_reference_ = c; }
 void BROCCOLI_LIB::SetMotionCorrectionReferenceVolume(float* r) { h_mc_reference_ = r; }
 void BROCCOLI_LIB::SetCoarsestScaleT1MNI(int N) { coarsest_ = N; }
+void BROCCOLI_LIB::SetCoarsestScaleEPIT1(int N) { coarsest_epi_t1_ = N; }
+void BROCCOLI_LIB::SetApplyMotionCorrection(bool b) { apply_mc_ = b; }
+void BROCCOLI_LIB::SetApplySmoothing(bool b) { apply_smoothing_ = b; }
+void BROCCOLI_LIB::SetApplySliceTimingCorrection(bool b) { apply_slice_timing_ = b; }
+void BROCCOLI_LIB::SetPreprocessingOnly(bool b) { preprocessing_only_ = b; }
 void BROCCOLI_LIB::SetMMT1ZCUT(int mm) { mm_z_cut_ = mm; }
 void BROCCOLI_LIB::SetInterpolationMode(int m) { interpolation_ = m; }
 void BROCCOLI_LIB::SetTsigma(float s) { tsigma_ = s; }
@@ -193,6 +187,20 @@ void BROCCOLI_LIB::SetOutputQuadratureFilterResponses(cl_float2* a, cl_float2* b
   out_q_[1] = b;
   out_q_[2] = c;
 }
+void BROCCOLI_LIB::SetOutputEPIT1RegistrationParameters(float* o) { out_params_epi_t1_ = o; }
+void BROCCOLI_LIB::SetOutputEPIMNIRegistrationParameters(float* o) { out_params_epi_mni_ = o; }
+void BROCCOLI_LIB::SetOutputAlignedEPIVolumeT1(float* o) { out_aligned_epi_t1_ = o; }
+void BROCCOLI_LIB::SetOutputAlignedEPIVolumeMNILinear(float* o) { out_aligned_epi_mni_lin_ = o; }
+void BROCCOLI_LIB::SetOutputAlignedEPIVolumeMNINonlinear(float* o) { out_aligned_epi_mni_nonlin_ = o; }
+void BROCCOLI_LIB::SetOutputEPIMask(float* o) { out_epi_mask_ = o; }
+void BROCCOLI_LIB::SetSaveInterpolatedT1(bool b) { save_interpolated_t1_ = b; }
+void BROCCOLI_LIB::SetSaveAlignedT1MNILinear(bool b) { save_t1_lin_ = b; }
+void BROCCOLI_LIB::SetSaveAlignedT1MNINonLinear(bool b) { save_t1_nonlin_ = b; }
+void BROCCOLI_LIB::SetSaveAlignedEPIT1(bool b) { save_epi_t1_ = b; }
+void BROCCOLI_LIB::SetSaveAlignedEPIMNI(bool b) { save_epi_mni_ = b; }
+void BROCCOLI_LIB::SetSaveEPIMask(bool b) { save_epi_mask_ = b; }
+void BROCCOLI_LIB::SetSaveMotionCorrected(bool b) { save_mc_ = b; }
+void BROCCOLI_LIB::SetSaveSmoothed(bool b) { save_smoothed_ = b; }
 
 bool BROCCOLI_LIB::check(int status, const char* where) {
   last_status_ = status;
@@ -298,13 +306,21 @@ void BROCCOLI_LIB::PerformSmoothingNormalizedWrapper() {
 // volumes go through one batched call.
 void BROCCOLI_LIB::PerformSmoothingNormalizedHostWrapper() {
   if (!initiated_ && !check(BRC_ERR_NODEVICE, "PerformSmoothingNormalizedHostWrapper")) return;
-  if (auto_mask_) {
-    check(BRC_ERR_UNSUPPORTED, "PerformSmoothingNormalizedHostWrapper: automatic EPI mask not available");
-    return;
-  }
   if (!h_fmri_ || !h_certainty_) {
     check(BRC_ERR_INVALID, "PerformSmoothingNormalizedHostWrapper: input or certainty not set");
     return;
+  }
+  if (auto_mask_) {
+    // the certainty is the mask of the first fMRI volume, written back to
+    // the host certainty array (SegmentEPIData, broccoli_lib.cpp:11008-11030)
+    const size_t V = epi_w_ * epi_h_ * epi_d_;
+    DeviceArray vol(ctx_, sizeof(float) * V), mask(ctx_, sizeof(float) * V);
+    if (!check(vol.status, "alloc") || !check(mask.status, "alloc")) return;
+    if (!check(brc_copy_to_device(ctx_, vol.ptr, h_fmri_, sizeof(float) * V), "H2D")) return;
+    if (!check(brc_segment_epi(ctx_, vol.f(), (int)epi_w_, (int)epi_h_, (int)epi_d_, epi_vox_, mask.f()),
+               "brc_segment_epi"))
+      return;
+    if (!check(brc_copy_to_host(ctx_, h_certainty_, mask.ptr, sizeof(float) * V), "D2H")) return;
   }
   const int keep = smoothing_type_;
   smoothing_type_ = LOWPASS;
@@ -460,4 +476,83 @@ void BROCCOLI_LIB::PerformRegistrationTwoVolumesWrapper() {
           !check(brc_copy_to_host(ctx_, out_field_[a], d_field.f() + a * V2, sizeof(float) * V2), "D2H"))
         return;
   }
+}
+
+// PerformFirstLevelAnalysisWrapper, broccoli_lib.cpp:8466-8733, up to the
+// statistics (PREPROCESSING_ONLY): one brc_first_level_preprocess call.
+// The parameter vectors and motion parameters are written always, the
+// volumes when their SetSave* flag is on and the array is set.
+void BROCCOLI_LIB::PerformFirstLevelAnalysisWrapper() {
+  if (!initiated_ && !check(BRC_ERR_NODEVICE, "PerformFirstLevelAnalysisWrapper")) return;
+  if (!preprocessing_only_) {
+    check(BRC_ERR_UNSUPPORTED,
+          "PerformFirstLevelAnalysisWrapper: the statistical analysis is not part of this library; "
+          "call SetPreprocessingOnly(true)");
+    return;
+  }
+  if (apply_slice_timing_) {
+    check(BRC_ERR_UNSUPPORTED, "PerformFirstLevelAnalysisWrapper: slice-timing correction is not supported");
+    return;
+  }
+  float bank3[3 * 686], bank6[6 * 686], dirs[18];
+  const float* tpl = h_mni_brain_ ? h_mni_brain_ : h_mni_;
+  if (!h_fmri_ || !h_t1_ || !tpl || !pack_linear(bank3) || !pack_nonlinear(bank6, dirs)) {
+    check(BRC_ERR_INVALID, "PerformFirstLevelAnalysisWrapper: inputs or filters not set");
+    return;
+  }
+  brc_first_level_input in;
+  in.fmri = h_fmri_;
+  in.epi_w = (int)epi_w_;
+  in.epi_h = (int)epi_h_;
+  in.epi_d = (int)epi_d_;
+  in.epi_t = (int)epi_t_;
+  in.t1 = h_t1_;
+  in.t1_w = (int)t1_w_;
+  in.t1_h = (int)t1_h_;
+  in.t1_d = (int)t1_d_;
+  in.mni = tpl;
+  in.mni_w = (int)mni_w_;
+  in.mni_h = (int)mni_h_;
+  in.mni_d = (int)mni_d_;
+  for (int a = 0; a < 3; a++) {
+    in.epi_voxel[a] = epi_vox_[a];
+    in.t1_voxel[a] = t1_vox_[a];
+    in.mni_voxel[a] = mni_vox_[a];
+  }
+  in.filters3 = bank3;
+  in.filters6 = bank6;
+  in.tensors = tensors_;
+  in.dirs = dirs;
+  brc_first_level_opts o;
+  brc_first_level_opts_default(&o);
+  o.linear_iterations = it_linear_;
+  o.nonlinear_iterations = it_nonlinear_;
+  o.motion_iterations = it_mc_;
+  o.coarsest_scale_t1_mni = coarsest_;
+  o.coarsest_scale_epi_t1 = coarsest_epi_t1_;
+  o.mm_t1_z_cut = mm_z_cut_;
+  o.apply_motion_correction = apply_mc_ ? 1 : 0;
+  o.apply_smoothing = apply_smoothing_ ? 1 : 0;
+  o.smoothing_fwhm = epi_fwhm_;
+  o.tsigma = tsigma_;
+  o.esigma = esigma_;
+  o.dsigma = dsigma_;
+  o.precision = precision_;
+  o.solve_fp64 = solve_fp64_ ? 1 : 0;
+  brc_first_level_output out;
+  memset(&out, 0, sizeof(out));
+  out.params_t1_mni = out_params_;
+  out.params_epi_t1 = out_params_epi_t1_;
+  out.params_epi_mni = out_params_epi_mni_;
+  out.motion_parameters = apply_mc_ ? out_motion_ : nullptr;
+  out.interpolated_t1 = save_interpolated_t1_ ? out_interpolated_ : nullptr;
+  out.aligned_t1_linear = save_t1_lin_ ? out_aligned_lin_ : nullptr;
+  out.aligned_t1_nonlinear = save_t1_nonlin_ ? out_aligned_nonlin_ : nullptr;
+  out.aligned_epi_t1 = save_epi_t1_ ? out_aligned_epi_t1_ : nullptr;
+  out.aligned_epi_mni_linear = save_epi_mni_ ? out_aligned_epi_mni_lin_ : nullptr;
+  out.aligned_epi_mni_nonlinear = save_epi_mni_ ? out_aligned_epi_mni_nonlin_ : nullptr;
+  out.motion_corrected = save_mc_ && out_mc_ != h_fmri_ ? out_mc_ : nullptr;
+  out.epi_mask = save_epi_mask_ ? out_epi_mask_ : nullptr;
+  out.smoothed = save_smoothed_ && out_smoothed_ != h_fmri_ ? out_smoothed_ : nullptr;
+  check(brc_first_level_preprocess(ctx_, &in, &o, &out), "brc_first_level_preprocess");
 }

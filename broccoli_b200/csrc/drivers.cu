@@ -458,11 +458,12 @@ extern "C" int brc_register_two_volumes(brc_ctx* ctx, const float* d_in, int W, 
   return BRC_OK;
 }
 
-// Composition total = match * linear of two parameter vectors in double
-// (AddAffineRegistrationParameters(total, match), broccoli_lib.cpp:7252-7340).
-static void compose_params(const float* linear, const float* match, float* total) {
+// Composition of two parameter vectors in double, total = new * old as 4x4
+// affine matrices (AddAffineRegistrationParameters, broccoli_lib.cpp:
+// 7252-7340 and :7433-7520).  `total` may alias `old12`.
+void brc::host_add_affine(const float* old12, const float* new12, float* total) {
   double O[16] = {0}, N[16] = {0}, T[16];
-  const float* src[2] = {linear, match};
+  const float* src[2] = {old12, new12};
   double* dst[2] = {O, N};
   for (int m = 0; m < 2; m++) {
     const float* p = src[m];
@@ -550,7 +551,8 @@ extern "C" int brc_register_cohort(brc_ctx* ctx, int n, const float* const* d_su
   } else {
     BRC_TRY(ctx, cudaMemcpyAsync(lin.ptr, mat.ptr, sizeof(float) * V2 * n, cudaMemcpyDeviceToDevice, st), "copy");
   }
-  for (int b = 0; b < n; b++) compose_params(&linp[12 * (size_t)b], &match[12 * (size_t)b], &total[12 * (size_t)b]);
+  for (int b = 0; b < n; b++)
+    brc::host_add_affine(&linp[12 * (size_t)b], &match[12 * (size_t)b], &total[12 * (size_t)b]);
   memcpy(h_params12n, total.data(), sizeof(float) * 12 * n);
   if (d_aligned_linear)
     BRC_TRY(ctx, cudaMemcpyAsync(d_aligned_linear, lin.ptr, sizeof(float) * V2 * n, cudaMemcpyDeviceToDevice, st),

@@ -88,6 +88,9 @@ cudaError_t transform_field(const float* src, int W, int H, int D, int T, const 
                             const float* dz, int interp, float* out, cudaStream_t st);
 cudaError_t combine_field(float* dx, float* dy, float* dz, int W, int H, int D, const float* p12, cudaStream_t st);
 cudaError_t add_affine_to_field(float* field, int W, int H, int D, const float* p12, cudaStream_t st);
+// Host composition total = new * old of two parameter vectors (4x4 affine
+// matrices in double); total may alias old12.
+void host_add_affine(const float* old12, const float* new12, float* total);
 }  // namespace brc
 
 namespace brc {

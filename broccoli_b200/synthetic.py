@@ -101,14 +101,19 @@ def affine_pair(shape=(33, 64, 64), base_seed: int = 0, motion_seed: int = 1):
 
 
 def motion_series(T: int = 200, shape=(33, 64, 64), base_seed: int = 0, snr: float = 50.0,
-                  max_translation: float = 2.0, max_rotation_deg: float = 2.0, noise: bool = True):
+                  max_translation: float = 2.0, max_rotation_deg: float = 2.0, noise: bool = True,
+                  base: np.ndarray = None):
     """fMRI-like series: volume t is the base volume under a rigid motion
     drawn from seed 100 + t (translations U(+-2) voxels, rotations U(+-2)
     degrees) plus Rician noise at the given SNR (noise std = mean
     foreground intensity / snr; magnitude of a complex signal with
     independent Gaussian noise in both channels).  Returns (series (T,D,H,W),
-    true parameters (T,12) of each volume's own motion)."""
-    base = base_volume(shape, base_seed)
+    true parameters (T,12) of each volume's own motion).  `base` replaces
+    the generated base volume (its shape is then the series' shape)."""
+    if base is None:
+        base = base_volume(shape, base_seed)
+    base = np.asarray(base, np.float32)
+    shape = base.shape
     fg = base[base > 100.0]
     s = (fg.mean() if fg.size else np.abs(base).mean()) / snr
     vols = np.empty((T,) + tuple(shape), np.float32)
@@ -207,3 +212,24 @@ def relative_params(p_ref, p_t) -> np.ndarray:
     out[:3] = M[:3, 3]
     out[3:] = (M[:3, :3] - np.eye(3)).reshape(-1)
     return out
+
+
+def first_level_dataset(T: int = 20, epi_shape=(33, 64, 64), epi_voxel=(3.0, 3.0, 3.5), t1_shape=(170, 256, 256),
+                        t1_voxel=(1.0, 1.0, 1.0), mni_shape=(182, 218, 182), mni_voxel=(1.0, 1.0, 1.0),
+                        seed: int = 0):
+    """Inputs of the first-level preprocessing: one head drawn three times.
+    The template is head_phantom(mni_shape, seed + 1); the T1 and the EPI
+    base are head_phantom(seed) with the template head's size in mm at
+    their own voxel sizes, so a T1 and an EPI of the same head overlap the
+    template after resampling; the EPI series is that base under rigid
+    motion (motion_series, translations up to 1 voxel, rotations up to 1
+    degree) with Rician noise at SNR 50.  Shapes are (D, H, W), voxel sizes
+    (x, y, z) in mm.  Returns (fmri (T, D, H, W), t1, mni, true motion
+    (T, 12))."""
+    mni = head_phantom(mni_shape, seed=seed + 1)
+    radii_mm = np.array([0.40 * mni_shape[2] * mni_voxel[0], 0.42 * mni_shape[1] * mni_voxel[1],
+                         0.40 * mni_shape[0] * mni_voxel[2]])
+    t1 = head_phantom(t1_shape, seed=seed, scale=radii_mm / np.asarray(t1_voxel, np.float64))
+    epi = head_phantom(epi_shape, seed=seed, scale=radii_mm / np.asarray(epi_voxel, np.float64))
+    fmri, truth = motion_series(T, base=epi, max_translation=1.0, max_rotation_deg=1.0)
+    return fmri, t1, mni, truth

@@ -454,6 +454,108 @@ int brc_register_cohort(brc_ctx* ctx, int n, const float* const* d_subjects, con
                         float* h_params12n, float* d_aligned_linear, float* d_aligned_nonlinear,
                         float* d_fields);
 
+/* ---- first-level preprocessing ----------------------------------------- */
+
+/* Gaussian smoothing filters of 9 taps per axis from a FWHM in mm and the
+ * voxel sizes (x, y, z), each normalised by its float sum.  Host only.
+ * Replaces CreateSmoothingFilters(..., FWHM, voxel sizes)
+ * (broccoli_lib.cpp:11055-11091). */
+void brc_smoothing_filters_fwhm(float fwhm_mm, const float* voxel_size3, float* h_fx, float* h_fy,
+                                float* h_fz);
+
+/* Tensor magnitude of one volume: its six nonlinear filter responses
+ * (h_filters6: 6 x 686 floats), the structure tensor T = sum_k |q_k| M_k
+ * (h_tensors: 6 x {m11 m12 m13 m22 m23 m33}) and the Frobenius norm of T
+ * into d_out.  Replaces CalculateTensorMagnitude (broccoli_lib.cpp:
+ * 5658-5746) with CalculateTensorComponents and CalculateTensorNorms
+ * (kernelRegistration.cpp:806-875). */
+int brc_tensor_magnitude(brc_ctx* ctx, const float* d_vol, int W, int H, int D, const float* h_filters6,
+                         const float* h_tensors, int precision, float* d_out);
+
+/* Brain mask of one EPI volume: smoothing with a 4 mm FWHM Gaussian, the
+ * sum of the smoothed volume in the reference's order (rows over x, then
+ * over y per plane, then over z on the host), and d_mask = 1 where the
+ * smoothed value exceeds 0.9 x sum / (W H D), 0.001 elsewhere.
+ * Synchronises.  Replaces SegmentEPIData (broccoli_lib.cpp:11008-11030)
+ * with CalculateSum (:10846-10886) and ThresholdVolume (kernelMisc.cpp:
+ * 305-327). */
+int brc_segment_epi(brc_ctx* ctx, const float* d_vol, int W, int H, int D, const float* voxel_size3,
+                    float* d_mask);
+
+typedef struct {
+  float* fmri;               /* host, T EPI volumes; replaced in place by the
+                                preprocessed series                         */
+  int epi_w, epi_h, epi_d, epi_t;
+  float epi_voxel[3];        /* mm (x, y, z)                                 */
+  const float* t1;           /* host, one T1 volume                          */
+  int t1_w, t1_h, t1_d;
+  float t1_voxel[3];
+  const float* mni;          /* host, the template brain volume              */
+  int mni_w, mni_h, mni_d;
+  float mni_voxel[3];
+  const float* filters3;     /* 3 x 686: linear registration filters         */
+  const float* filters6;     /* 6 x 686: nonlinear registration filters      */
+  const float* tensors;      /* 6 x 6 projection tensors                     */
+  const float* dirs;         /* filter directions x[6] y[6] z[6]             */
+} brc_first_level_input;
+
+typedef struct {
+  int linear_iterations;     /* NUMBER_OF_ITERATIONS_FOR_LINEAR_IMAGE_REGISTRATION */
+  int nonlinear_iterations;  /* ... _NONLINEAR_ ...; 0 skips the nonlinear stage   */
+  int motion_iterations;     /* NUMBER_OF_ITERATIONS_FOR_MOTION_CORRECTION         */
+  int coarsest_scale_t1_mni; /* COARSEST_SCALE_T1_MNI                              */
+  int coarsest_scale_epi_t1; /* COARSEST_SCALE_EPI_T1                              */
+  int mm_t1_z_cut;           /* MM_T1_Z_CUT                                        */
+  int apply_motion_correction;
+  int apply_smoothing;
+  float smoothing_fwhm;      /* EPI smoothing, mm                                  */
+  float tsigma, esigma, dsigma;
+  int precision;             /* filtering: BRC_PREC_FP32 / BRC_PREC_BF16X3         */
+  int solve_fp64;
+} brc_first_level_opts;
+
+/* Defaults of the reference's FirstLevelAnalysis tool
+ * (Bash_Wrapper/FirstLevelAnalysis.cpp:133-158): 10 linear and 10 nonlinear
+ * iterations, 5 motion-correction iterations, coarsest scales 4, no z cut,
+ * motion correction and 6 mm smoothing on, sigmas 5, FP32. */
+void brc_first_level_opts_default(brc_first_level_opts* opts);
+
+typedef struct {             /* host outputs, each may be NULL               */
+  float* params_t1_mni;      /* 12 */
+  float* params_epi_t1;      /* 12: EPI to the original T1                   */
+  float* params_epi_mni;     /* 12 */
+  float* motion_parameters;  /* 6 x T, [t + k*T]: mm then degrees            */
+  float* interpolated_t1;    /* template size                                */
+  float* aligned_t1_linear;
+  float* aligned_t1_nonlinear;
+  float* field;              /* 3 template-size volumes x, y, z              */
+  float* aligned_epi_t1;     /* template size                                */
+  float* aligned_epi_mni_linear;
+  float* aligned_epi_mni_nonlinear;
+  float* motion_corrected;   /* T EPI volumes                                */
+  float* epi_mask;           /* EPI size                                     */
+  float* smoothed;           /* T EPI volumes                                */
+} brc_first_level_output;
+
+/* The preprocessing stages of a first-level analysis, in the reference's
+ * order: T1 to template (centring, resampling onto the template grid with
+ * the z cut, mass match, multi-scale affine, multi-scale nonlinear); the
+ * first EPI volume to the resampled T1 on the template grid (centring,
+ * resampling, mass match, multi-scale affine) and through the T1's
+ * transforms to the template; the first EPI volume to the original T1
+ * (translation and rigid on the volumes, rigid and affine on their tensor
+ * magnitudes); rigid motion correction of the series; the EPI mask of the
+ * first corrected volume; normalised smoothing of the series with the mask.
+ * Slice-timing correction and the statistics are not part of this entry.
+ * Synchronises before returning.  Replaces the preprocessing of
+ * PerformFirstLevelAnalysisWrapper (broccoli_lib.cpp:8480-8733) with
+ * PerformRegistrationT1MNINoSkullstrip (:8226-8273),
+ * PerformRegistrationEPIT1 (:7853-7915), PerformRegistrationEPIT1Original
+ * (:7917-7970), PerformMotionCorrectionHost (:10723-10787), SegmentEPIData
+ * (:11008-11030) and PerformSmoothingNormalizedHost (:11628-11727). */
+int brc_first_level_preprocess(brc_ctx* ctx, const brc_first_level_input* in, const brc_first_level_opts* opts,
+                               const brc_first_level_output* out);
+
 #ifdef __cplusplus
 }
 #endif

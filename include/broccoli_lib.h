@@ -21,6 +21,13 @@
  *   - PerformRegistrationTwoVolumesWrapper: T1 -> MNI, single volume.
  *   - PerformSmoothingWrapper: LOWPASS (from SetEPISmoothingAmount, FWHM in
  *     mm) or RANDOM (filters from SetSmoothingFilters).
+ *   - PerformFirstLevelAnalysisWrapper: the preprocessing stages only
+ *     (SetPreprocessingOnly(true)); outputs are written where the reference
+ *     writes them: the three parameter vectors and the motion parameters
+ *     always, the volumes when their SetSave* flag is on.
+ *   - SetAutoMask(true): PerformSmoothingNormalizedHostWrapper makes the
+ *     certainty from the first fMRI volume (SegmentEPIData) and writes it
+ *     to the SetInputCertainty array.
  *   - Extensions (new setters): SetPrecision, SetMotionCorrectionTolerance,
  *     SetSolveFP64.
  */
@@ -128,6 +135,11 @@ class BROCCOLI_LIB {
   void SetChangeMotionCorrectionReferenceVolume(bool change);
   void SetMotionCorrectionReferenceVolume(float* reference);
   void SetCoarsestScaleT1MNI(int N);
+  void SetCoarsestScaleEPIT1(int N);
+  void SetApplyMotionCorrection(bool apply);
+  void SetApplySmoothing(bool apply);
+  void SetApplySliceTimingCorrection(bool apply);  // true is not supported
+  void SetPreprocessingOnly(bool only);            // PerformFirstLevelAnalysisWrapper needs true
   void SetMMT1ZCUT(int mm);
   void SetInterpolationMode(int mode);
   void SetTsigma(float s);
@@ -138,7 +150,7 @@ class BROCCOLI_LIB {
   void SetEPISmoothingAmount(float fwhm_mm);
   void SetEPIMask(float* mask);  // certainty of PerformSmoothingNormalizedWrapper
   void SetInputCertainty(float* certainty);  // certainty of PerformSmoothingNormalizedHostWrapper
-  void SetAutoMask(bool automask);  // true is not supported (EPI segmentation is not built)
+  void SetAutoMask(bool automask);  // certainty from SegmentEPIData of the first fMRI volume
 
   // extensions of this implementation
   void SetPrecision(int precision);             // BRC_PREC_FP32 / BRC_PREC_BF16X3
@@ -155,6 +167,20 @@ class BROCCOLI_LIB {
   void SetOutputDisplacementField(float* x, float* y, float* z);
   void SetOutputSmoothedfMRIVolumes(float* output);
   void SetOutputQuadratureFilterResponses(cl_float2* q1, cl_float2* q2, cl_float2* q3);
+  void SetOutputEPIT1RegistrationParameters(float* output);
+  void SetOutputEPIMNIRegistrationParameters(float* output);
+  void SetOutputAlignedEPIVolumeT1(float* output);
+  void SetOutputAlignedEPIVolumeMNILinear(float* output);
+  void SetOutputAlignedEPIVolumeMNINonlinear(float* output);
+  void SetOutputEPIMask(float* output);
+  void SetSaveInterpolatedT1(bool save);
+  void SetSaveAlignedT1MNILinear(bool save);
+  void SetSaveAlignedT1MNINonLinear(bool save);
+  void SetSaveAlignedEPIT1(bool save);
+  void SetSaveAlignedEPIMNI(bool save);
+  void SetSaveEPIMask(bool save);
+  void SetSaveMotionCorrected(bool save);
+  void SetSaveSmoothed(bool save);
 
   // entry points
   void PerformMotionCorrectionWrapper();
@@ -171,6 +197,12 @@ class BROCCOLI_LIB {
   void TransformVolumesLinearWrapper();
   void TransformVolumesNonLinearWrapper();
   void CenterVolumesWrapper();
+  // The preprocessing of a first-level analysis (brc_first_level_preprocess):
+  // T1 -> MNI, EPI -> T1, motion correction, EPI mask and normalised
+  // smoothing; h_fMRI_Volumes is replaced by the preprocessed series.  The
+  // statistics are not part of this library: SetPreprocessingOnly(true) is
+  // required, and slice-timing correction must be off.
+  void PerformFirstLevelAnalysisWrapper();
   const float* GetCenterParameters() const { return center_params_; }  // of the last CenterVolumesWrapper
 
   int GetLastStatus() const { return last_status_; }
@@ -225,6 +257,17 @@ class BROCCOLI_LIB {
   float* h_certainty_ = nullptr;
   bool auto_mask_ = false;
   cl_float2* out_q_[3] = {nullptr};
+
+  int coarsest_epi_t1_ = 4;
+  bool apply_mc_ = true, apply_smoothing_ = true, apply_slice_timing_ = false, preprocessing_only_ = false;
+  float* out_params_epi_t1_ = nullptr;
+  float* out_params_epi_mni_ = nullptr;
+  float* out_aligned_epi_t1_ = nullptr;
+  float* out_aligned_epi_mni_lin_ = nullptr;
+  float* out_aligned_epi_mni_nonlin_ = nullptr;
+  float* out_epi_mask_ = nullptr;
+  bool save_interpolated_t1_ = false, save_t1_lin_ = false, save_t1_nonlin_ = false, save_epi_t1_ = false,
+       save_epi_mni_ = false, save_epi_mask_ = false, save_mc_ = false, save_smoothed_ = false;
 
   float center_params_[12] = {0};
   bool t1_to_mni(const float* d_t1, float* d_out, const char* where);

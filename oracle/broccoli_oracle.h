@@ -117,7 +117,12 @@ enum { ORC_TRANSLATION = 0, ORC_RIGID = 1, ORC_AFFINE = 2 };
       int lin_iter, int nl_iter, const real* filters3, const real* filters6,    \
       const real* tensors, const real* dirs, double tsigma, double esigma,      \
       double dsigma, real* p12, real* interpolated, real* aligned_linear,       \
-      real* aligned_nonlinear, real* field);
+      real* aligned_nonlinear, real* field);                                    \
+  void orc_tensor_magnitude##SFX(const real* vol, int W, int H, int D,          \
+                                 const real* filters6, const real* tensors,     \
+                                 real* out);                                    \
+  void orc_segment_epi##SFX(const real* vol, int W, int H, int D, double vx,    \
+                            double vy, double vz, real* mask);
 
 ORC_DECLARE(float, _f32)
 ORC_DECLARE(double, _f64)

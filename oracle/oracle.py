@@ -677,3 +677,203 @@ def ref_change_resolution_and_size_interp(src, vin, shape, vnew, mm_z_cut=0, int
     fn(_ptr(v), W, H, D, T, *[float(a) for a in vin], _ptr(out), W2, H2, D2, *[float(a) for a in vnew],
        int(mm_z_cut), int(interp))
     return out
+
+
+def match_volume_masses(v1, v2, prec="f32"):
+    """MatchVolumeMasses: (v1 translated so its centre of mass meets v2's, 12 parameters)."""
+    dt, s = _dt(prec)
+    D, H, W = v1.shape
+    a = _arr(v1, dt).copy()
+    b = _arr(v2, dt)
+    p = np.zeros(12, dt)
+    getattr(orc_lib(), "orc_match_volume_masses" + s)(_ptr(a), _ptr(b), W, H, D, _ptr(p))
+    return a, p
+
+
+def smoothing_filter_fwhm(fwhm, voxel_size, size=9, prec="f32"):
+    """CreateSmoothingFilters from a FWHM in mm: (fx, fy, fz)."""
+    dt, s = _dt(prec)
+    f = [np.zeros(size, dt) for _ in range(3)]
+    fn = getattr(orc_lib(), "orc_smoothing_filter_fwhm" + s)
+    fn.argtypes = [_I, _D, _D, _D, _D, _P, _P, _P]
+    fn(size, float(fwhm), *[float(v) for v in voxel_size], *[_ptr(a) for a in f])
+    return tuple(f)
+
+
+def tensor_magnitude(vol, bank, prec="f32"):
+    """CalculateTensorMagnitude of one (D, H, W) volume."""
+    dt, s = _dt(prec)
+    D, H, W = vol.shape
+    v = _arr(vol, dt)
+    f6, m, _ = _nl_args(bank, dt)
+    out = np.zeros_like(v)
+    getattr(orc_lib(), "orc_tensor_magnitude" + s)(_ptr(v), W, H, D, _ptr(f6), _ptr(m), _ptr(out))
+    return out
+
+
+def segment_epi(vol, voxel_size, prec="f32"):
+    """SegmentEPIData of one (D, H, W) volume: the 1 / 0.001 mask."""
+    dt, s = _dt(prec)
+    D, H, W = vol.shape
+    v = _arr(vol, dt)
+    out = np.zeros_like(v)
+    fn = getattr(orc_lib(), "orc_segment_epi" + s)
+    fn.argtypes = [_P, _I, _I, _I, _D, _D, _D, _P]
+    fn(_ptr(v), W, H, D, *[float(a) for a in voxel_size], _ptr(out))
+    return out
+
+
+def ref_match_volume_masses(v1, v2):
+    D, H, W = v1.shape
+    a = _arr(v1, np.float32).copy()
+    b = _arr(v2, np.float32)
+    p = np.zeros(12, np.float32)
+    ref_lib().ref_match_volume_masses(_ptr(a), _ptr(b), W, H, D, _ptr(p))
+    return a, p
+
+
+def ref_tensor_magnitude(vol, bank):
+    D, H, W = vol.shape
+    v = _arr(vol, np.float32)
+    f6, m, _ = _nl_args(bank, np.float32)
+    out = np.zeros_like(v)
+    ref_lib().ref_tensor_magnitude(_ptr(v), W, H, D, _ptr(f6), _ptr(m), _ptr(out))
+    return out
+
+
+def ref_segment_epi(vol, voxel_size):
+    D, H, W = vol.shape
+    v = _arr(vol, np.float32)
+    out = np.zeros_like(v)
+    fn = ref_lib().ref_segment_epi
+    fn.argtypes = [_P, _I, _I, _I, _D, _D, _D, _P]
+    fn(_ptr(v), W, H, D, *[float(a) for a in voxel_size], _ptr(out))
+    return out
+
+
+class _Steps:
+    """The steps of the first-level preprocessing chain, from the C
+    restatement (prec "f32" / "f64") or from the reference's own kernels
+    (prec "ref", float)."""
+
+    def __init__(self, prec):
+        self.ref = prec == "ref"
+        self.prec = "f32" if self.ref else prec
+        self.dt = np.float32 if self.ref else _dt(prec)[0]
+
+    def center(self, v):
+        return (ref_center_volumes(v, 1) if self.ref else center_volumes(v, 1, self.prec))[0][0]
+
+    def resize(self, v, vin, shape, vnew, zcut):
+        if self.ref:
+            return ref_change_resolution_and_size(v, vin, shape, vnew, zcut)
+        return change_resolution_and_size(v, vin, shape, vnew, zcut, self.prec)
+
+    def match(self, v1, v2):
+        return ref_match_volume_masses(v1, v2) if self.ref else match_volume_masses(v1, v2, self.prec)
+
+    def scales(self, ref, moving, filters, niter, coarsest, type_):
+        if self.ref:
+            return ref_align_linear_scales(ref, moving, filters, niter, coarsest, type_)
+        return align_linear_scales(ref, moving, filters, niter, coarsest, type_, self.prec)
+
+    def nonlinear(self, ref, moving, bank, niter, coarsest, ts, es, ds):
+        if self.ref:
+            return ref_align_nonlinear_scales(ref, moving, bank, niter, coarsest, ts, es, ds)
+        return align_nonlinear_scales(ref, moving, bank, niter, coarsest, ts, es, ds, self.prec)
+
+    def compose(self, old, new):
+        return ref_add_affine(old, new) if self.ref else add_affine(old, new, self.prec)
+
+    def affine(self, v, p):
+        return (ref_transform_affine(v, p, 1) if self.ref else transform_affine(v, p, 1, self.prec))[0]
+
+    def field(self, v, f):
+        if self.ref:
+            return ref_transform_field(v, f[0], f[1], f[2], 1)[0]
+        return transform_field(v, f[0], f[1], f[2], 1, self.prec)[0]
+
+    def tensor_magnitude(self, v, bank):
+        return ref_tensor_magnitude(v, bank) if self.ref else tensor_magnitude(v, bank, self.prec)
+
+    def motion(self, vols, vs, filters, niter):
+        return ref_motion_correct(vols, vs, filters, niter) if self.ref else motion_correct(vols, vs, filters,
+                                                                                             niter, self.prec)
+
+    def segment(self, v, vs):
+        return ref_segment_epi(v, vs) if self.ref else segment_epi(v, vs, self.prec)
+
+    def smooth(self, vols, mask, f):
+        if self.ref:
+            return ref_smooth_normalized(vols, mask, *f)
+        return smooth_normalized(vols, mask, *f, prec=self.prec).astype(self.dt)
+
+
+def first_level_preprocess(fmri, vs_epi, t1, vs_t1, mni, vs_mni, bank, lin_iter=10, nl_iter=10,
+                           coarsest_t1_mni=4, coarsest_epi_t1=4, mm_t1_z_cut=0, motion_iter=5,
+                           smoothing_fwhm=6.0, apply_motion=True, apply_smoothing=True, tsigma=5.0,
+                           esigma=5.0, dsigma=5.0, prec="f32"):
+    """The registration, motion-correction, segmentation and smoothing stages
+    of PerformFirstLevelAnalysisWrapper (broccoli_lib.cpp:8480-8733), with
+    slice-timing correction off, composed in the reference's order from the
+    oracle's steps (prec "f32" / "f64") or from the reference's kernels
+    (prec "ref").  fmri (T, D, H, W), t1 and mni (D, H, W) volumes; voxel
+    sizes (x, y, z) in mm.  Returns a dict of the outputs."""
+    op = _Steps(prec)
+    lin = bank["linear"]
+    out = {}
+    # T1 to MNI: PerformRegistrationT1MNINoSkullstrip, :8226-8273
+    mni_t1 = op.resize(op.center(t1), vs_t1, mni.shape, vs_mni, mm_t1_z_cut)
+    mni_t1, start_t1_mni = op.match(mni_t1, mni)
+    skull = mni_t1.copy()
+    out["interpolated_t1"] = skull
+    p_t1_mni, mni_t1, _ = op.scales(mni, mni_t1, lin, lin_iter, coarsest_t1_mni, AFFINE)
+    out["aligned_t1_linear"] = mni_t1
+    field = None
+    if nl_iter > 0:
+        field, out["aligned_t1_nonlinear"] = op.nonlinear(mni, mni_t1, bank, nl_iter, coarsest_t1_mni, tsigma,
+                                                          esigma, dsigma)
+        out["field"] = field
+    out["params_t1_mni"] = op.compose(p_t1_mni, start_t1_mni)  # :8510
+    # EPI to T1 on the MNI grid: PerformRegistrationEPIT1, :7853-7915
+    epi0 = np.asarray(fmri[0])
+    t1_epi = op.resize(op.center(epi0), vs_epi, mni.shape, vs_mni, 0)
+    t1_epi, start_epi_t1 = op.match(t1_epi, skull)
+    p_epi_t1, t1_epi, _ = op.scales(skull, t1_epi, lin, lin_iter, coarsest_epi_t1, AFFINE)
+    out["aligned_epi_t1"] = t1_epi
+    epi_mni = op.affine(t1_epi, p_t1_mni)  # :8547-8556
+    out["aligned_epi_mni_linear"] = epi_mni
+    if field is not None:
+        out["aligned_epi_mni_nonlinear"] = op.field(epi_mni, field)
+    epi_t1_out = op.compose(p_epi_t1, start_epi_t1)  # :8574-8575
+    out["params_epi_mni"] = op.compose(p_t1_mni, epi_t1_out)
+    # EPI to the original T1: PerformRegistrationEPIT1Original, :7917-7970
+    t1o = np.asarray(t1)
+    t1_epi_o = op.resize(epi0, vs_epi, t1o.shape, vs_t1, 0)
+    t1_epi_o, start_o = op.match(t1_epi_o, t1o)
+    tm_epi = op.tensor_magnitude(t1_epi_o, bank)
+    tm_t1 = op.tensor_magnitude(t1o, bank)
+    aff = np.zeros(12, op.dt)
+    for type_ in (TRANSLATION, RIGID):
+        p, t1_epi_o, _ = op.scales(t1o, t1_epi_o, lin, lin_iter, coarsest_epi_t1 * 2, type_)
+        tm_epi = op.affine(tm_epi, p)
+        aff = op.compose(aff, p)
+    for type_ in (RIGID, AFFINE):
+        p, tm_epi, _ = op.scales(tm_t1, tm_epi, lin, lin_iter, 2, type_)
+        t1_epi_o = op.affine(t1_epi_o, p)
+        aff = op.compose(aff, p)
+    out["params_epi_t1"] = op.compose(aff, start_o)  # :8601
+    # motion correction (PerformMotionCorrectionHost, :10723-10787), the EPI
+    # mask of the first corrected volume (SegmentEPIData, :11008-11030) and
+    # normalised smoothing with that mask (:8700-8733)
+    vols = _arr(fmri, op.dt).copy()
+    if apply_motion:
+        vols, out["motion_parameters"] = op.motion(vols, vs_epi, lin, motion_iter)
+        out["motion_corrected"] = vols.copy()
+    mask = op.segment(vols[0], vs_epi)
+    out["epi_mask"] = mask
+    if apply_smoothing:
+        vols = op.smooth(vols, mask, smoothing_filter_fwhm(smoothing_fwhm, vs_epi, 9, op.prec))
+        out["smoothed"] = vols
+    out["fmri"] = vols
+    return out

@@ -1222,6 +1222,55 @@ void FN(orc_register_two_volumes)(const REAL* in, int W, int H, int D, const flo
   free(work);
 }
 
+/* Tensor magnitude of one volume: its six nonlinear filter responses, the
+ * structure tensor T = sum_k |q_k| M_k and the Frobenius norm of T.
+ * CalculateTensorMagnitude, broccoli_lib.cpp:5658-5746 (responses of the
+ * volume in the q2 slots; CalculateTensorComponents,
+ * kernelRegistration.cpp:806-845, reads only q2; CalculateTensorNorms,
+ * :847-875). */
+void FN(orc_tensor_magnitude)(const REAL* vol, int W, int H, int D, const REAL* filters6,
+                              const REAL* tensors, REAL* out) {
+  const long V = (long)W * H * D;
+  REAL* q = (REAL*)malloc(sizeof(REAL) * 12 * V);
+  REAL* t6 = (REAL*)calloc(6 * V, sizeof(REAL));
+  FN(orc_filter3d)(vol, W, H, D, filters6, 6, q);
+  for (int k = 0; k < 6; k++) FN(orc_tensor_components)(q + 2 * V * k, V, tensors + 6 * k, t6);
+  FN(orc_tensor_norms)(t6, V, out);
+  free(q);
+  free(t6);
+}
+
+/* Brain mask of one EPI volume.  SegmentEPIData, broccoli_lib.cpp:
+ * 11008-11030: smoothing with a 4 mm FWHM Gaussian of 9 taps per axis
+ * (CreateSmoothingFilters from the voxel sizes, :11055-11091); the sum of
+ * the smoothed volume in the reference's order -- over x for every (y, z)
+ * (CalculateColumnSums, kernelMisc.cpp:193-212), over y for every z
+ * (CalculateRowSums, :214-231), over z on the host (CalculateSum,
+ * broccoli_lib.cpp:10846-10886); threshold 0.9 x sum / (W H D); mask 1
+ * where the smoothed value is above it and 0.001 elsewhere
+ * (ThresholdVolume, kernelMisc.cpp:305-327). */
+void FN(orc_segment_epi)(const REAL* vol, int W, int H, int D, double vx, double vy, double vz,
+                         REAL* mask) {
+  const long V = (long)W * H * D;
+  REAL fx[9], fy[9], fz[9];
+  FN(orc_smoothing_filter_fwhm)(9, 4.0, vx, vy, vz, fx, fy, fz);
+  REAL* sm = (REAL*)malloc(sizeof(REAL) * V);
+  FN(orc_smooth3d)(vol, NULL, NULL, W, H, D, fx, fy, fz, sm);
+  REAL sum = RZERO;
+  for (int z = 0; z < D; z++) {
+    REAL zs = RZERO;
+    for (int y = 0; y < H; y++) {
+      REAL ys = RZERO;
+      for (int x = 0; x < W; x++) ys += sm[x + (long)y * W + (long)z * W * H];
+      zs += ys;
+    }
+    sum += zs;
+  }
+  const REAL thr = (REAL)0.9f * sum / ((REAL)W * (REAL)H * (REAL)D);
+  for (long i = 0; i < V; i++) mask[i] = sm[i] > thr ? RONE : (REAL)0.001f;
+  free(sm);
+}
+
 #undef RSQRT
 #undef RATAN2
 #undef RCOS

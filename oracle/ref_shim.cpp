@@ -628,4 +628,56 @@ void ref_register_two_volumes(const float* in, int W, int H, int D, const float*
   ref_warp_field(work.data(), W2, H2, D2, field, field + V2, field + 2 * V2, aligned_nonlinear);
 }
 
+// CalculateTensorMagnitude, broccoli_lib.cpp:5658-5746, with the
+// reference's CalculateTensorComponents and CalculateTensorNorms kernels.
+void ref_tensor_magnitude(const float* vol, int W, int H, int D, const float* filters6, const float* tensors,
+                          float* out) {
+  const long V = (long)W * H * D;
+  std::vector<float> q(12 * V), t(6 * V, 0.f);
+  ref_filter3d(vol, W, H, D, filters6, q.data());
+  ref_filter3d(vol, W, H, D, filters6 + 3 * 686, q.data() + 6 * V);
+  const float2* Q = reinterpret_cast<const float2*>(q.data());
+  float *t11 = t.data(), *t12 = t11 + V, *t13 = t12 + V, *t22 = t13 + V, *t23 = t22 + V, *t33 = t23 + V;
+  const int gx = roundup(W, 16), gy = roundup(H, 16);
+  for (int k = 0; k < 6; k++) {
+    const float* m = tensors + 6 * k;
+    ndrange(gx, gy, D, 16, 16, 1, [&] {
+      clr::CalculateTensorComponents(t11, t12, t13, t22, t23, t33, Q + k * V, Q + k * V, m[0], m[1], m[2], m[3],
+                                     m[4], m[5], W, H, D);
+    });
+  }
+  ndrange(gx, gy, D, 16, 16, 1, [&] { clr::CalculateTensorNorms(out, t11, t12, t13, t22, t23, t33, W, H, D); });
+}
+
+// SegmentEPIData, broccoli_lib.cpp:11008-11030: 4 mm FWHM smoothing
+// (CreateSmoothingFilters, :11055-11091, restated), CalculateSum
+// (:10846-10886) on the reference's CalculateColumnSums / CalculateRowSums
+// kernels, and its ThresholdVolume kernel at 0.9 x the mean.
+void ref_segment_epi(const float* vol, int W, int H, int D, double vx, double vy, double vz, float* mask) {
+  const long V = (long)W * H * D;
+  float f[3][9];
+  const double vs[3] = {vx, vy, vz};
+  for (int a = 0; a < 3; a++) {
+    const double s = 4.0 / 2.354 / vs[a];
+    const double s2 = 2.0 * s * s;
+    float sum = 0.0f;
+    for (int i = 0; i < 9; i++) {
+      const double u = (double)(i - 4);
+      f[a][i] = (float)exp(-pow(u, 2.0) / s2);
+      sum += f[a][i];
+    }
+    for (int i = 0; i < 9; i++) f[a][i] /= sum;
+  }
+  std::vector<float> sm(V), cols((long)H * D), rows(D);
+  ref_smooth3d(vol, nullptr, nullptr, W, H, D, f[0], f[1], f[2], sm.data());
+  ndrange(roundup(H, 16), roundup(D, 16), 1, 16, 16, 1,
+          [&] { clm::CalculateColumnSums(cols.data(), sm.data(), W, H, D); }, false);
+  ndrange(roundup(D, 16), 1, 1, 16, 1, 1, [&] { clm::CalculateRowSums(rows.data(), cols.data(), H, D); }, false);
+  float sum = 0.0f;
+  for (int z = 0; z < D; z++) sum += rows[z];
+  const float thr = 0.9f * sum / ((float)W * H * D);
+  ndrange(roundup(W, 16), roundup(H, 16), D, 16, 16, 1,
+          [&] { clm::ThresholdVolume(mask, sm.data(), thr, W, H, D); });
+}
+
 }  // extern "C"

@@ -3,10 +3,11 @@
 // sizes and voxel sizes, then PerformSmoothingNormalizedHostWrapper, which
 // smooths the volumes in place.  Test program: reads a raw float32 series
 // and certainty volume, writes the smoothed series.
-//   broccoli_lib_smooth <series.f32> <certainty.f32> W H D T vx vy vz fwhm_mm <out.f32>
+//   broccoli_lib_smooth <series.f32> <certainty.f32 | auto> W H D T vx vy vz fwhm_mm <out.f32>
 #include <stdio.h>
 #include <stdlib.h>
 
+#include <string>
 #include <vector>
 
 #include "broccoli_lib.h"
@@ -30,7 +31,10 @@ int main(int argc, char** argv) {
   const int W = atoi(argv[3]), H = atoi(argv[4]), D = atoi(argv[5]), T = atoi(argv[6]);
   const size_t V = (size_t)W * H * D;
   std::vector<float> series = read_floats(argv[1], V * T);
-  std::vector<float> certainty = read_floats(argv[2], V);
+  // certainty "auto": SetAutoMask(true), the mask of the first volume is
+  // made by the library and written to <out>.mask
+  const bool automask = std::string(argv[2]) == "auto";
+  std::vector<float> certainty = automask ? std::vector<float>(V, 0.f) : read_floats(argv[2], V);
 
   BROCCOLI_LIB broccoli(0, 0, BASH, false);
   if (!broccoli.GetOpenCLInitiated()) {
@@ -38,7 +42,7 @@ int main(int argc, char** argv) {
     return 1;
   }
   broccoli.SetInputfMRIVolumes(series.data());
-  broccoli.SetAutoMask(false);
+  broccoli.SetAutoMask(automask);
   broccoli.SetInputCertainty(certainty.data());
   broccoli.SetEPISmoothingAmount((float)atof(argv[10]));
   broccoli.SetEPIWidth(W);
@@ -59,5 +63,14 @@ int main(int argc, char** argv) {
     return 2;
   }
   fclose(f);
+  if (automask) {
+    const std::string mp = std::string(argv[11]) + ".mask";
+    FILE* m = fopen(mp.c_str(), "wb");
+    if (!m || fwrite(certainty.data(), sizeof(float), V, m) != V) {
+      fprintf(stderr, "cannot write %s\n", mp.c_str());
+      return 2;
+    }
+    fclose(m);
+  }
   return 0;
 }

@@ -175,7 +175,37 @@ def main_transforms() -> None:
     print("wrote transforms.npz")
 
 
+FIRST_LEVEL = dict(epi_shape=(12, 14, 14), epi_voxel=(3.0, 3.0, 3.0), t1_shape=(24, 28, 26),
+                   t1_voxel=(1.5, 1.5, 1.5), mni_shape=(18, 22, 20), mni_voxel=(2.0, 2.0, 2.0), T=4, seed=2,
+                   lin_iter=4, nl_iter=2, coarsest_t1_mni=2, coarsest_epi_t1=2, mm_t1_z_cut=0, motion_iter=4,
+                   smoothing_fwhm=6.0)
+
+
+def main_first_level() -> None:
+    """The preprocessing stages of a first-level analysis (T1 to template,
+    EPI to T1 on the template grid and to the original T1, motion
+    correction, EPI mask, normalised smoothing) composed from the
+    reference's kernels (oracle.first_level_preprocess with prec "ref") on
+    first_level_dataset inputs, plus the tensor magnitude of the T1 and the
+    mask of the first EPI volume on their own."""
+    c = FIRST_LEVEL
+    fmri, t1, mni, _ = S.first_level_dataset(c["T"], c["epi_shape"], c["epi_voxel"], c["t1_shape"], c["t1_voxel"],
+                                             c["mni_shape"], c["mni_voxel"], seed=c["seed"])
+    bank = F.load_filter_dir(os.path.join(HERE, "filters"))
+    out = O.first_level_preprocess(fmri, c["epi_voxel"], t1, c["t1_voxel"], mni, c["mni_voxel"], bank,
+                                   c["lin_iter"], c["nl_iter"], c["coarsest_t1_mni"], c["coarsest_epi_t1"],
+                                   c["mm_t1_z_cut"], c["motion_iter"], c["smoothing_fwhm"], prec="ref")
+    g = {"in_fmri": fmri, "in_t1": t1, "in_mni": mni,
+         "tensor_magnitude_t1": O.ref_tensor_magnitude(t1, bank),
+         "segment_epi0": O.ref_segment_epi(fmri[0], c["epi_voxel"])}
+    g.update({"cfg_" + k: np.asarray(v) for k, v in c.items() if not k.endswith("_shape")})
+    g.update({"out_" + k: np.asarray(v, np.float32) for k, v in out.items()})
+    np.savez_compressed(os.path.join(HERE, "first_level.npz"), **g)
+    print("wrote first_level.npz")
+
+
 if __name__ == "__main__":
     main()
     main_smooth_normalized()
     main_transforms()
+    main_first_level()

@@ -83,3 +83,37 @@ def test_perform_smoothing_normalized_matches_golden():
     assert np.array_equal(np.isnan(got), np.isnan(ref))
     fin = np.isfinite(ref)
     assert np.abs(got[fin] - ref[fin]).max() <= 1e-4 * np.abs(ref[fin]).max()
+
+
+@pytest.mark.gpu
+def test_perform_first_level_preprocessing_equals_library(bank):
+    """firstlevel.py's preprocessing through the wrapper class (fMRI flipped
+    up-down, template brain divided by its maximum, packVolume layouts)
+    equals brc_first_level_preprocess on the same volumes."""
+    import os
+    from conftest import GOLDEN
+    from test_first_level import cfg
+    from broccoli_b200.api import Context
+    fl = dict(np.load(os.path.join(GOLDEN, "first_level.npz")))
+    c = cfg(fl)
+    fmri, t1, mni = fl["in_fmri"], fl["in_t1"], fl["in_mni"]
+    wrap3 = to_wrapper_layout
+    filters = {k: [to_wrapper_layout(bank[k][i, 0]) + 1j * to_wrapper_layout(bank[k][i, 1])
+                   for i in range(len(bank[k]))] for k in ("linear", "nonlinear")}
+    # performFirstLevelAnalysis flips the fMRI data up-down before packing it
+    r = BL.performFirstLevelPreprocessing(
+        np.flipud(to_wrapper_layout(fmri)), c["epi_voxel"], wrap3(t1), c["t1_voxel"], wrap3(mni), c["mni_voxel"],
+        filters["linear"], filters["nonlinear"], bank["projection_tensors"], list(bank["directions"]),
+        c["lin_iter"], c["nl_iter"], c["motion_iter"], c["coarsest_t1_mni"], c["coarsest_epi_t1"], 0,
+        c["smoothing_fwhm"])
+    ctx = Context(0)
+    want = ctx.first_level_preprocess(fmri, c["epi_voxel"], t1, c["t1_voxel"], mni / mni.max(), c["mni_voxel"],
+                                      bank, c["lin_iter"], c["nl_iter"], c["motion_iter"], c["coarsest_t1_mni"],
+                                      c["coarsest_epi_t1"], 0, smoothing_fwhm=c["smoothing_fwhm"])
+    ctx.close()
+    assert np.array_equal(r["T1_MNI_registration_parameters"], want["params_t1_mni"])
+    assert np.array_equal(r["EPI_T1_registration_parameters"], want["params_epi_t1"])
+    assert np.array_equal(r["EPI_MNI_registration_parameters"], want["params_epi_mni"])
+    assert np.array_equal(r["motion_parameters"], want["motion_parameters"])
+    assert np.array_equal(r["EPI_mask"], wrap3(want["epi_mask"]))
+    assert np.array_equal(r["aligned_T1_volume"], wrap3(want["aligned_t1_linear"]))
