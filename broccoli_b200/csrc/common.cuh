@@ -74,4 +74,47 @@ __device__ __forceinline__ float sqrt_approx(float v) {
   return r;
 }
 
+// OpenCL 1.2 section 8.2 linear filtering with unnormalised coordinates and
+// clamp-to-edge addressing, exact float weights (the sampler of
+// kernelRegistration.cpp:1064).  u, v, w include the +0.5 texel offset.
+__device__ __forceinline__ float sample_linear(const float* __restrict__ T, int W, int H, int D,
+                                              float u, float v, float w) {
+  // volumes hold fewer than 2^31 voxels (checked by the launchers)
+  const float uu = u - 0.5f, vv = v - 0.5f, ww = w - 0.5f;
+  const float fu = floorf(uu), fv = floorf(vv), fw = floorf(ww);
+  const float a = uu - fu, bb = vv - fv, c = ww - fw;
+  const int i0 = (int)fu, j0 = (int)fv, k0 = (int)fw;
+  const int xi0 = min(max(i0, 0), W - 1), xi1 = min(max(i0 + 1, 0), W - 1);
+  const int yj0 = min(max(j0, 0), H - 1), yj1 = min(max(j0 + 1, 0), H - 1);
+  const int zk0 = min(max(k0, 0), D - 1), zk1 = min(max(k0 + 1, 0), D - 1);
+  const int WH = W * H;
+  const int r00 = yj0 * W + zk0 * WH;
+  const int r10 = yj1 * W + zk0 * WH;
+  const int r01 = yj0 * W + zk1 * WH;
+  const int r11 = yj1 * W + zk1 * WH;
+  // trilinear weights applied as seven linear interpolations
+  const float t000 = __ldg(T + xi0 + r00), t100 = __ldg(T + xi1 + r00);
+  const float t010 = __ldg(T + xi0 + r10), t110 = __ldg(T + xi1 + r10);
+  const float t001 = __ldg(T + xi0 + r01), t101 = __ldg(T + xi1 + r01);
+  const float t011 = __ldg(T + xi0 + r11), t111 = __ldg(T + xi1 + r11);
+  const float c00 = fmaf(a, t100 - t000, t000), c10 = fmaf(a, t110 - t010, t010);
+  const float c01 = fmaf(a, t101 - t001, t001), c11 = fmaf(a, t111 - t011, t011);
+  const float c0 = fmaf(bb, c10 - c00, c00), c1 = fmaf(bb, c11 - c01, c01);
+  return fmaf(c, c1 - c0, c0);
+}
+
+// The affine warp's sample of voxel (x, y, z): src at x + t + (A - I)(x -
+// centre) with p = {t, A - I} (InterpolateVolumeLinearLinear,
+// kernelRegistration.cpp:1066-1101).
+__device__ __forceinline__ float affine_sample(const float* __restrict__ src, int W, int H, int D,
+                                               const float* __restrict__ p, int x, int y, int z) {
+  const float xf = (float)x - ((float)W - 1.0f) * 0.5f;
+  const float yf = (float)y - ((float)H - 1.0f) * 0.5f;
+  const float zf = (float)z - ((float)D - 1.0f) * 0.5f;
+  const float u = (float)x + p[0] + p[3] * xf + p[4] * yf + p[5] * zf + 0.5f;
+  const float v = (float)y + p[1] + p[6] * xf + p[7] * yf + p[8] * zf + 0.5f;
+  const float w = (float)z + p[2] + p[9] * xf + p[10] * yf + p[11] * zf + 0.5f;
+  return sample_linear(src, W, H, D, u, v, w);
+}
+
 }  // namespace brc

@@ -766,35 +766,6 @@ __global__ void solve_given_kernel(const double* __restrict__ A, const double* _
 // Trilinear sampling
 // ---------------------------------------------------------------------------
 
-// OpenCL 1.2 section 8.2 linear filtering with unnormalised coordinates and
-// clamp-to-edge addressing, exact float weights (the sampler of
-// kernelRegistration.cpp:1064).  u, v, w include the +0.5 texel offset.
-__device__ __forceinline__ float sample_linear(const float* __restrict__ T, int W, int H, int D,
-                                              float u, float v, float w) {
-  // volumes hold fewer than 2^31 voxels (checked by the launchers)
-  const float uu = u - 0.5f, vv = v - 0.5f, ww = w - 0.5f;
-  const float fu = floorf(uu), fv = floorf(vv), fw = floorf(ww);
-  const float a = uu - fu, bb = vv - fv, c = ww - fw;
-  const int i0 = (int)fu, j0 = (int)fv, k0 = (int)fw;
-  const int xi0 = min(max(i0, 0), W - 1), xi1 = min(max(i0 + 1, 0), W - 1);
-  const int yj0 = min(max(j0, 0), H - 1), yj1 = min(max(j0 + 1, 0), H - 1);
-  const int zk0 = min(max(k0, 0), D - 1), zk1 = min(max(k0 + 1, 0), D - 1);
-  const int WH = W * H;
-  const int r00 = yj0 * W + zk0 * WH;
-  const int r10 = yj1 * W + zk0 * WH;
-  const int r01 = yj0 * W + zk1 * WH;
-  const int r11 = yj1 * W + zk1 * WH;
-  // trilinear weights applied as seven linear interpolations
-  const float t000 = __ldg(T + xi0 + r00), t100 = __ldg(T + xi1 + r00);
-  const float t010 = __ldg(T + xi0 + r10), t110 = __ldg(T + xi1 + r10);
-  const float t001 = __ldg(T + xi0 + r01), t101 = __ldg(T + xi1 + r01);
-  const float t011 = __ldg(T + xi0 + r11), t111 = __ldg(T + xi1 + r11);
-  const float c00 = fmaf(a, t100 - t000, t000), c10 = fmaf(a, t110 - t010, t010);
-  const float c01 = fmaf(a, t101 - t001, t001), c11 = fmaf(a, t111 - t011, t011);
-  const float c0 = fmaf(bb, c10 - c00, c00), c1 = fmaf(bb, c11 - c01, c01);
-  return fmaf(c, c1 - c0, c0);
-}
-
 // out_b(x) = src_b(x + t + (A - I)(x - centre)), params_b of instance b
 // (InterpolateVolumeLinearLinear, kernelRegistration.cpp:1066-1101).
 __global__ void __launch_bounds__(256)
@@ -806,18 +777,11 @@ warp_affine_kernel(const float* __restrict__ src, long long src_stride, int W, i
   const int ty = blockIdx.x / ntx, tx = blockIdx.x - ty * ntx;
   const int x = tx * 32 + threadIdx.x, y = ty * 8 + threadIdx.y, z = blockIdx.y;
   if (x >= W || y >= H) return;
-  const float xf = (float)x - ((float)W - 1.0f) * 0.5f;
-  const float yf = (float)y - ((float)H - 1.0f) * 0.5f;
-  const float zf = (float)z - ((float)D - 1.0f) * 0.5f;
   const int n = active_count(act, batch);
   for (int li = blockIdx.z; li < n; li += gridDim.z) {
     const int b = active_instance(act, li);
-    const float* p = params + (long long)b * 12;
-    const float u = (float)x + p[0] + p[3] * xf + p[4] * yf + p[5] * zf + 0.5f;
-    const float v = (float)y + p[1] + p[6] * xf + p[7] * yf + p[8] * zf + 0.5f;
-    const float w = (float)z + p[2] + p[9] * xf + p[10] * yf + p[11] * zf + 0.5f;
     out[(long long)b * out_stride + ((long long)z * H + y) * W + x] =
-        sample_linear(src + (long long)b * src_stride, W, H, D, u, v, w);
+        affine_sample(src + (long long)b * src_stride, W, H, D, params + (long long)b * 12, x, y, z);
   }
 }
 
