@@ -106,3 +106,97 @@ def test_cli_errors(tmp_path):
     r = subprocess.run([os.path.join(BIN, "RegisterTwoVolumes"), bad, bad, "-mask", "m.nii"],
                        capture_output=True, text=True, timeout=60)
     assert r.returncode != 0 and "not supported" in r.stderr
+
+
+@pytest.mark.parametrize("mode", ["ones", "mask", "automask"])
+def test_smoothing_cli_equals_library(ctx, tmp_path, mode):
+    """Smoothing (Bash_Wrapper/Smoothing.cpp): normalised smoothing with a
+    mask, with the all-ones certainty, or with the library's EPI mask
+    (written as _mask)."""
+    vols, _ = S.motion_series(T=3, shape=(12, 16, 14), snr=50.0)
+    vs = (3.0, 3.0, 3.5)
+    path = os.path.join(tmp_path, "epi.nii")
+    nifti.write(path, vols, header_with_voxels(vs))
+    args = [os.path.join(BIN, "Smoothing"), path, "-fwhm", "8", "-quiet"]
+    mask = np.ones(vols.shape[1:], np.float32)
+    if mode == "mask":
+        mask = (S.head_phantom(vols.shape[1:], seed=3) > 200).astype(np.float32)
+        nifti.write(os.path.join(tmp_path, "mask.nii"), mask, header_with_voxels(vs))
+        args += ["-mask", os.path.join(tmp_path, "mask.nii")]
+    if mode == "automask":
+        args += ["-automask"]
+        mask = ctx.segment_epi(torch.from_numpy(vols[0]).cuda(), vs).cpu().numpy()
+    run(args)
+    fx, fy, fz = ctx.smoothing_filters_fwhm(8.0, vs)
+    want = ctx.smooth_normalized(torch.from_numpy(vols).cuda(), torch.from_numpy(mask).cuda(), fx, fy, fz)
+    out = nifti.read(os.path.join(tmp_path, "epi_sm.nii"))
+    assert np.array_equal(out.data, want.cpu().numpy(), equal_nan=True)
+    assert out.voxel_size == vs
+    if mode == "automask":
+        assert np.array_equal(nifti.read(os.path.join(tmp_path, "epi_mask.nii")).data, mask)
+
+
+def test_transform_volume_cli_equals_library(ctx, tmp_path):
+    """TransformVolume (Bash_Wrapper/TransformVolume.cpp): a 4x4 matrix file,
+    a scaling, a centring and a displacement field, each on the reference
+    volume's grid, equal to the library's transform calls."""
+    from broccoli_b200 import _lib as L
+    rng = np.random.default_rng(7)
+    vols = np.stack([S.head_phantom((20, 24, 22), seed=s) for s in (1, 2)]).astype(np.float32)
+    vin, vref = (2.0, 2.0, 2.5), (2.5, 2.2, 2.4)
+    ref = np.zeros((18, 22, 20), np.float32)
+    src = os.path.join(tmp_path, "vol.nii")
+    refp = os.path.join(tmp_path, "ref.nii.gz")
+    nifti.write(src, vols, header_with_voxels(vin))
+    nifti.write(refp, ref, header_with_voxels(vref))
+    resampled = ctx.change_resolution_and_size_batch(torch.from_numpy(vols).cuda(), vin, ref.shape, vref, 0,
+                                                     L.INTERP_LINEAR)
+    # matrix (rows a11 a12 a13 tx ...), nearest neighbour
+    p = np.array([1.5, -0.75, 0.5, 0.02, -0.01, 0.015, 0.01, -0.02, 0.005, -0.012, 0.01, 0.018], np.float32)
+    mat = np.array([[p[3] + 1, p[4], p[5], p[0]], [p[6], p[7] + 1, p[8], p[1]], [p[9], p[10], p[11] + 1, p[2]],
+                    [0, 0, 0, 1]])
+    np.savetxt(os.path.join(tmp_path, "m.txt"), mat, fmt="%.9g")
+    run([os.path.join(BIN, "TransformVolume"), src, refp, "-matrix", os.path.join(tmp_path, "m.txt"),
+         "-interpolation", "0", "-quiet"])
+    resampled0 = ctx.change_resolution_and_size_batch(torch.from_numpy(vols).cuda(), vin, ref.shape, vref, 0,
+                                                      L.INTERP_NEAREST)
+    pm = np.array([mat[0, 3], mat[1, 3], mat[2, 3], mat[0, 0] - 1, mat[0, 1], mat[0, 2], mat[1, 0], mat[1, 1] - 1,
+                   mat[1, 2], mat[2, 0], mat[2, 1], mat[2, 2] - 1], np.float32)
+    want = ctx.transform_volumes_linear(resampled0, pm, L.INTERP_NEAREST).cpu().numpy()
+    out = nifti.read(os.path.join(tmp_path, "vol_warped.nii"))
+    assert np.array_equal(out.data, want) and out.voxel_size == tuple(np.float32(vref))
+    # scaling on the input's own grid
+    run([os.path.join(BIN, "TransformVolume"), src, src, "-scaling", "1.25", "-output",
+         os.path.join(tmp_path, "scaled.nii"), "-quiet"])
+    same = ctx.change_resolution_and_size_batch(torch.from_numpy(vols).cuda(), vin, vols.shape[1:], vin, 0,
+                                                L.INTERP_LINEAR)
+    ps = np.zeros(12, np.float32)
+    ps[[3, 7, 11]] = np.float32(1.0) / np.float32(1.25) - np.float32(1.0)
+    want = ctx.transform_volumes_linear(same, ps, L.INTERP_LINEAR).cpu().numpy()
+    assert np.array_equal(nifti.read(os.path.join(tmp_path, "scaled.nii")).data, want)
+    # centring (input grid)
+    run([os.path.join(BIN, "TransformVolume"), src, src, "-centering", "-quiet"])
+    want, _ = ctx.center_volumes(torch.from_numpy(vols).cuda())
+    assert np.array_equal(nifti.read(os.path.join(tmp_path, "vol_centered.nii")).data, want.cpu().numpy())
+    # displacement field on the reference grid
+    field = (rng.standard_normal((3,) + ref.shape) * 0.8).astype(np.float32)
+    fps = []
+    for a, ax in enumerate("xyz"):
+        fps.append(os.path.join(tmp_path, f"f_{ax}.nii"))
+        nifti.write(fps[-1], field[a], header_with_voxels(vref))
+    run([os.path.join(BIN, "TransformVolume"), src, refp, "-field", *fps, "-output",
+         os.path.join(tmp_path, "fw.nii.gz"), "-quiet"])
+    f = torch.from_numpy(field).cuda()
+    want = ctx.transform_volumes_nonlinear(resampled, f[0], f[1], f[2], L.INTERP_LINEAR).cpu().numpy()
+    assert np.array_equal(nifti.read(os.path.join(tmp_path, "fw.nii.gz")).data, want)
+
+
+def test_new_cli_errors(tmp_path):
+    vol = os.path.join(tmp_path, "v.nii")
+    nifti.write(vol, np.ones((4, 5, 6), np.float32), header_with_voxels((1.0, 1.0, 1.0)))
+    r = subprocess.run([os.path.join(BIN, "TransformVolume"), vol, vol, "-scaling", "2", "-centering"],
+                       capture_output=True, text=True, timeout=60)
+    assert r.returncode != 0 and "exactly one" in r.stderr
+    r = subprocess.run([os.path.join(BIN, "Smoothing"), vol, "-fwhm", "-1"], capture_output=True, text=True,
+                       timeout=60)
+    assert r.returncode != 0 and "positive" in r.stderr
