@@ -200,3 +200,43 @@ def test_new_cli_errors(tmp_path):
     r = subprocess.run([os.path.join(BIN, "Smoothing"), vol, "-fwhm", "-1"], capture_output=True, text=True,
                        timeout=60)
     assert r.returncode != 0 and "positive" in r.stderr
+
+
+def test_first_level_cli_preprocessing_equals_library(ctx, tmp_path, bank):
+    """FirstLevelAnalysis -preprocessingonly (Bash_Wrapper/FirstLevelAnalysis.cpp)
+    on NIfTI files: the saved matrices, motion parameters and volumes equal
+    brc_first_level_preprocess on the same data (coarsest scale 1 for this
+    template: fewer than 32 voxels along an axis)."""
+    fmri, t1, mni, _ = S.first_level_dataset(4, (12, 14, 14), (3.0, 3.0, 3.0), (24, 28, 26), (1.5, 1.5, 1.5),
+                                             (18, 22, 20), (2.0, 2.0, 2.0), seed=2)
+    fp, tp, mp = (os.path.join(tmp_path, n) for n in ("run.nii", "t1.nii.gz", "mni.nii"))
+    nifti.write(fp, fmri, header_with_voxels((3.0, 3.0, 3.0)))
+    nifti.write(tp, t1, header_with_voxels((1.5, 1.5, 1.5)))
+    nifti.write(mp, mni, header_with_voxels((2.0, 2.0, 2.0)))
+    run([os.path.join(BIN, "FirstLevelAnalysis"), fp, tp, mp, "-preprocessingonly", "-filters", FILTERS,
+         "-iterationslinear", "3", "-iterationsnonlinear", "2", "-iterationsmc", "3", "-smoothing", "6",
+         "-saveall", "-quiet"])
+    want = ctx.first_level_preprocess(fmri, (3.0, 3.0, 3.0), t1, (1.5, 1.5, 1.5), mni, (2.0, 2.0, 2.0), bank, 3, 2,
+                                      3, 1, 1, smoothing_fwhm=6.0)
+    vols = {"t1_interpolated.nii.gz": "interpolated_t1", "t1_aligned_mni_linear.nii.gz": "aligned_t1_linear",
+            "t1_aligned_mni_nonlinear.nii.gz": "aligned_t1_nonlinear", "run_aligned_t1.nii": "aligned_epi_t1",
+            "run_aligned_mni_linear.nii": "aligned_epi_mni_linear",
+            "run_aligned_mni_nonlinear.nii": "aligned_epi_mni_nonlinear", "run_motion_corrected.nii": "motion_corrected",
+            "run_smoothed.nii": "smoothed", "run_mask.nii": "epi_mask"}
+    for name, k in vols.items():
+        got = nifti.read(os.path.join(tmp_path, name)).data
+        assert np.array_equal(got, want[k]), name
+    for name, k in (("t1_affinematrix_t1_mni.txt", "params_t1_mni"), ("run_affinematrix_epi_t1.txt", "params_epi_t1"),
+                    ("run_affinematrix_epi_mni.txt", "params_epi_mni")):
+        m = np.loadtxt(os.path.join(tmp_path, name))
+        p = want[k]
+        expect = np.array([[p[3] + 1, p[4], p[5], p[0]], [p[6], p[7] + 1, p[8], p[1]],
+                           [p[9], p[10], p[11] + 1, p[2]], [0, 0, 0, 1]])
+        np.testing.assert_allclose(m, expect, rtol=1e-5, atol=1e-6)
+    cols = np.loadtxt(os.path.join(tmp_path, "run_motionparameters.1D"))
+    mo = want["motion_parameters"]
+    np.testing.assert_allclose(cols, np.stack([mo[4], -mo[3], mo[5], -mo[2], -mo[0], -mo[1]], 1), rtol=1e-5,
+                               atol=1e-6)
+    r = subprocess.run([os.path.join(BIN, "FirstLevelAnalysis"), fp, tp, mp, "regressors.txt"], capture_output=True,
+                       text=True, timeout=60)
+    assert r.returncode != 0 and "statistical analysis" in r.stderr
