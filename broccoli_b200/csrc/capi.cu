@@ -369,7 +369,7 @@ int brc_smooth3d(brc_ctx* ctx, const float* d_vol, int W, int H, int D, int batc
   BRC_TRY(ctx, brc::smooth3d(d_vol, W, H, D, batch, h_fx, h_fy, h_fz, d_cert, d_scert,
                              ctx->tmp1.as<float>(), ctx->tmp2.as<float>(), d_out, ctx->stream()),
           "smooth3d");
-  ctx->launches += 3;
+  ctx->launches += 1;
   return BRC_OK;
 }
 
@@ -394,7 +394,7 @@ int brc_smooth_normalized(brc_ctx* ctx, const float* d_vols, int W, int H, int D
                              ctx->tmp1.as<float>(), ctx->tmp2.as<float>(), d_out, st),
           "smooth volumes");
   BRC_TRY(ctx, brc::multiply_mask(d_out, d_mask, V, T, st), "multiply mask");
-  ctx->launches += 7;
+  ctx->launches += 3;
   return BRC_OK;
 }
 

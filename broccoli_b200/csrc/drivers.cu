@@ -48,20 +48,21 @@ static int nonlinear_step(brc_ctx* ctx, const float* q1, const float* q2, int W,
   float* ah = t6 + 6 * V;  // a6 then h3, contiguous (9 volumes)
   float* d3 = ah + 9 * V;
   unsigned int* maxbits = reinterpret_cast<unsigned int*>(d3 + 3 * V);
-  BRC_TRY(ctx, brc::tensor_components(q2, V, m36, t6, st), "tensor_components");
-  BRC_TRY(ctx, brc::smooth3d(t6, W, H, D, 6, ft, ft, ft, nullptr, nullptr, ctx->tmp1.as<float>(),
-                             ctx->tmp2.as<float>(), t6, st),
+  // the unsmoothed T and A, h go to tmp2, so every smoothing writes a
+  // buffer it does not read
+  float* raw = ctx->tmp2.as<float>();
+  BRC_TRY(ctx, brc::tensor_components(q2, V, m36, raw, st), "tensor_components");
+  BRC_TRY(ctx, brc::smooth3d(raw, W, H, D, 6, ft, ft, ft, nullptr, nullptr, ctx->tmp1.as<float>(), nullptr, t6, st),
           "smooth T");
-  BRC_TRY(ctx, brc::tensor_norm_max(t6, V, ah, maxbits, st), "tensor_norm_max");
-  BRC_TRY(ctx, brc::nonlinear_ah(q1, q2, t6, V, maxbits, m36, dirs18, ah, ah + 6 * V, st), "nonlinear_ah");
-  BRC_TRY(ctx, brc::smooth3d(ah, W, H, D, 9, fe, fe, fe, nullptr, nullptr, ctx->tmp1.as<float>(),
-                             ctx->tmp2.as<float>(), ah, st),
+  BRC_TRY(ctx, brc::tensor_norm_max(t6, V, raw, maxbits, st), "tensor_norm_max");
+  BRC_TRY(ctx, brc::nonlinear_ah(q1, q2, t6, V, maxbits, m36, dirs18, raw, raw + 6 * V, st), "nonlinear_ah");
+  BRC_TRY(ctx, brc::smooth3d(raw, W, H, D, 9, fe, fe, fe, nullptr, nullptr, ctx->tmp1.as<float>(), nullptr, ah, st),
           "smooth A,h");
   BRC_TRY(ctx, brc::displacement_update(ah, ah + 6 * V, V, fp64, d3, st), "displacement_update");
-  BRC_TRY(ctx, brc::smooth3d(d3, W, H, D, 3, fd, fd, fd, nullptr, nullptr, ctx->tmp1.as<float>(),
-                             ctx->tmp2.as<float>(), field, st, 1),
+  BRC_TRY(ctx, brc::smooth3d(d3, W, H, D, 3, fd, fd, fd, nullptr, nullptr, ctx->tmp1.as<float>(), nullptr, field, st,
+                             1),
           "smooth update");
-  ctx->launches += 1 + 3 + 1 + 1 + 3 + 1 + 3;
+  ctx->launches += 7;
   return BRC_OK;
 }
 

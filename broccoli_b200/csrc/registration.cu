@@ -14,6 +14,7 @@
 #include <math.h>
 
 #include "common.cuh"
+#include "internal.h"
 
 namespace brc {
 
@@ -820,40 +821,79 @@ struct Taps9 {
   float f[9];
 };
 
-// axis 1 (y): out = sum (vol * cert)[y+o] f[4-o]; axis 0 (x): along x;
-// axis 2 (z): along z, then divided by the smoothed certainty.
-// SeparableConvolutionRows / Columns / Rods, kernelConvolution.cpp:52-91,
-// :531-569, :1201-1240.
-template <int AXIS>
+// The three separable 9-tap passes in one kernel: y over (vol * cert), then
+// x, then z, divided by the smoothed certainty (SeparableConvolutionRows /
+// Columns / Rods, kernelConvolution.cpp:52-91, :531-569, :1201-1240, zero
+// padding).  A block owns a 32 x 8 column tile and marches along z through
+// a chunk of planes: per plane it stages the 40 x 16 input window (tile
+// plus 4-voxel halo) in shared memory, runs the y and x passes there, and
+// keeps the last nine xy results of its column in registers for the z
+// pass.  Each output is the same sequence of float operations as three
+// separate passes (terms o = -4..4 in order, out-of-volume terms 0), and
+// the volume is read from HBM once and written once instead of three times
+// each way.  `out` must not overlap the inputs.
+constexpr int kSmTX = 32, kSmTY = 8, kSmZC = 32;
+
+template <bool CERT>
 __global__ void __launch_bounds__(256)
-smooth_pass_kernel(const float* __restrict__ in, long long in_stride, const float* __restrict__ cert,
-                   const float* __restrict__ scert, int W, int H, int D, Taps9 taps,
-                   float* __restrict__ out, long long out_stride, int accumulate) {
-  const int b = blockIdx.y;
-  const long long V = (long long)W * H * D;
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= V) return;
-  const int x = (int)(i % W), y = (int)((i / W) % H), z = (int)(i / ((long long)W * H));
-  const float* src = in + (long long)b * in_stride;
-  const int c = AXIS == 0 ? x : (AXIS == 1 ? y : z);
-  const int n = AXIS == 0 ? W : (AXIS == 1 ? H : D);
-  const long long s = AXIS == 0 ? 1 : (AXIS == 1 ? (long long)W : (long long)W * H);
-  float sum = 0.f;
+smooth3d_kernel(const float* __restrict__ in, long long in_stride, const float* __restrict__ cert,
+                const float* __restrict__ scert, int W, int H, int D, Taps9 tx, Taps9 ty, Taps9 tz,
+                float* __restrict__ out, long long out_stride, int accumulate) {
+  __shared__ float s_in[kSmTY + 8][kSmTX + 9];
+  __shared__ float s_y[kSmTY][kSmTX + 9];
+  const int tid = threadIdx.x, lx = tid & 31, ly = tid >> 5;
+  const int ntx = (W + kSmTX - 1) / kSmTX;
+  const int x0 = (int)(blockIdx.x % ntx) * kSmTX, y0 = (int)(blockIdx.x / ntx) * kSmTY;
+  const int z0 = blockIdx.y * kSmZC, z1 = min(D, z0 + kSmZC);
+  const long long WH = (long long)W * H;
+  const float* src = in + (long long)blockIdx.z * in_stride;
+  const int x = x0 + lx, y = y0 + ly;
+  float ring[9];
 #pragma unroll
-  for (int o = -4; o <= 4; o++) {
-    float px = 0.f;
-    if (c + o >= 0 && c + o < n) {
-      const long long j = i + o * s;
-      px = __ldg(src + j);
-      if (AXIS == 1 && cert != nullptr) px *= __ldg(cert + j);
+  for (int k = 0; k < 9; k++) ring[k] = 0.f;
+  for (int p = z0 - 4; p < z1 + 4; p++) {
+    float xy = 0.f;
+    if (p >= 0 && p < D) {  // uniform over the block
+      for (int e = tid; e < (kSmTY + 8) * (kSmTX + 8); e += 256) {
+        const int r = e / (kSmTX + 8), c = e - r * (kSmTX + 8);
+        const int gx = x0 - 4 + c, gy = y0 - 4 + r;
+        float v = 0.f;
+        if (gx >= 0 && gx < W && gy >= 0 && gy < H) {
+          const long long j = (long long)p * WH + (long long)gy * W + gx;
+          v = __ldg(src + j);
+          if (CERT) v *= __ldg(cert + j);
+        }
+        s_in[r][c] = v;
+      }
+      __syncthreads();
+      // y pass on the tile rows, over the tile columns plus the x halo
+      // (0 outside the volume: the x pass pads with zeros)
+      for (int e = tid; e < kSmTY * (kSmTX + 8); e += 256) {
+        const int r = e / (kSmTX + 8), c = e - r * (kSmTX + 8);
+        const int gx = x0 - 4 + c;
+        float sum = 0.f;
+#pragma unroll
+        for (int o = -4; o <= 4; o++) sum += s_in[r + 4 + o][c] * ty.f[4 - o];
+        s_y[r][c] = (gx >= 0 && gx < W) ? sum : 0.f;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int o = -4; o <= 4; o++) xy += s_y[ly][lx + 4 + o] * tx.f[4 - o];
     }
-    sum += px * taps.f[4 - o];
+#pragma unroll
+    for (int k = 0; k < 8; k++) ring[k] = ring[k + 1];
+    ring[8] = xy;  // plane p; ring[4] is plane p - 4
+    const int z = p - 4;
+    if (z >= z0 && x < W && y < H) {
+      float sum = 0.f;
+#pragma unroll
+      for (int o = -4; o <= 4; o++) sum += ring[4 + o] * tz.f[4 - o];
+      const long long i = (long long)z * WH + (long long)y * W + x;
+      if (scert != nullptr) sum = sum / __ldg(scert + i);
+      float* o = out + (long long)blockIdx.z * out_stride + i;
+      *o = accumulate ? *o + sum : sum;
+    }
   }
-  if (AXIS == 2 && scert != nullptr) sum = sum / __ldg(scert + i);
-  float* o = out + (long long)b * out_stride + i;
-  // accumulate: the field update of the nonlinear step (AddVolumes after
-  // the smoothing, broccoli_lib.cpp:6021-6025) folded into the last pass
-  *o = accumulate ? *o + sum : sum;
 }
 
 // ---------------------------------------------------------------------------
@@ -992,17 +1032,35 @@ cudaError_t smooth3d(const float* vol, int W, int H, int D, int batch, const flo
                      const float* fy, const float* fz, const float* cert, const float* scert,
                      float* tmp1, float* tmp2, float* out, cudaStream_t st, int accumulate) {
   const long long V = (long long)W * H * D;
-  dim3 grid((unsigned)((V + 255) / 256), batch);
   Taps9 tx, ty, tz;
   for (int i = 0; i < 9; i++) {
     tx.f[i] = fx[i];
     ty.f[i] = fy[i];
     tz.f[i] = fz[i];
   }
-  smooth_pass_kernel<1><<<grid, 256, 0, st>>>(vol, V, cert, nullptr, W, H, D, ty, tmp1, V, 0);
-  smooth_pass_kernel<0><<<grid, 256, 0, st>>>(tmp1, V, nullptr, nullptr, W, H, D, tx, tmp2, V, 0);
-  smooth_pass_kernel<2><<<grid, 256, 0, st>>>(tmp2, V, nullptr, scert, W, H, D, tz, out, V, accumulate);
-  return cudaGetLastError();
+  (void)tmp2;  // the fused kernel needs no second temporary
+  // an output overlapping an input is computed into tmp1, then moved
+  const size_t bytes = sizeof(float) * (size_t)V * batch;
+  auto overlaps = [&](const float* a, size_t na) {
+    const char *o0 = reinterpret_cast<const char*>(out), *a0 = reinterpret_cast<const char*>(a);
+    return a != nullptr && o0 < a0 + na && a0 < o0 + bytes;
+  };
+  const bool alias = overlaps(vol, bytes) || overlaps(cert, sizeof(float) * (size_t)V) ||
+                     overlaps(scert, sizeof(float) * (size_t)V);
+  float* dst = alias ? tmp1 : out;
+  const long long ntiles = (long long)((W + kSmTX - 1) / kSmTX) * ((H + kSmTY - 1) / kSmTY);
+  if (ntiles > 0x7fffffffLL || batch > 65535) return cudaErrorInvalidValue;
+  const dim3 grid((unsigned)ntiles, (unsigned)((D + kSmZC - 1) / kSmZC), (unsigned)batch);
+  if (cert)
+    smooth3d_kernel<true><<<grid, 256, 0, st>>>(vol, V, cert, scert, W, H, D, tx, ty, tz, dst, V,
+                                                alias ? 0 : accumulate);
+  else
+    smooth3d_kernel<false><<<grid, 256, 0, st>>>(vol, V, nullptr, scert, W, H, D, tx, ty, tz, dst, V,
+                                                 alias ? 0 : accumulate);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || !alias) return e;
+  if (accumulate) return add_volumes(out, out, tmp1, V * batch, st);
+  return cudaMemcpyAsync(out, tmp1, bytes, cudaMemcpyDeviceToDevice, st);
 }
 
 }  // namespace brc
