@@ -851,21 +851,43 @@ smooth3d_kernel(const float* __restrict__ in, long long in_stride, const float* 
   float ring[9];
 #pragma unroll
   for (int k = 0; k < 9; k++) ring[k] = 0.f;
+  // the thread's (up to) three elements of the 16 x 40 window: their window
+  // positions and in-plane offsets (-1: outside the volume)
+  constexpr int kWin = (kSmTY + 8) * (kSmTX + 8);
+  int woff[3];
+  long long goff[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const int e = tid + 256 * k;
+    const int r = e / (kSmTX + 8), c = e - r * (kSmTX + 8);
+    const int gx = x0 - 4 + c, gy = y0 - 4 + r;
+    woff[k] = e < kWin ? r * (kSmTX + 9) + c : -1;
+    goff[k] = (e < kWin && gx >= 0 && gx < W && gy >= 0 && gy < H) ? (long long)gy * W + gx : -1;
+  }
+  // the next plane's elements are loaded while the current plane is
+  // smoothed
+  float pre[3];
+  auto load = [&](int q) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      float v = 0.f;
+      if (q >= 0 && q < D && goff[k] >= 0) {
+        const long long j = (long long)q * WH + goff[k];
+        v = __ldg(src + j);
+        if (CERT) v *= __ldg(cert + j);
+      }
+      pre[k] = v;
+    }
+  };
+  load(z0 - 4);
   for (int p = z0 - 4; p < z1 + 4; p++) {
     float xy = 0.f;
     if (p >= 0 && p < D) {  // uniform over the block
-      for (int e = tid; e < (kSmTY + 8) * (kSmTX + 8); e += 256) {
-        const int r = e / (kSmTX + 8), c = e - r * (kSmTX + 8);
-        const int gx = x0 - 4 + c, gy = y0 - 4 + r;
-        float v = 0.f;
-        if (gx >= 0 && gx < W && gy >= 0 && gy < H) {
-          const long long j = (long long)p * WH + (long long)gy * W + gx;
-          v = __ldg(src + j);
-          if (CERT) v *= __ldg(cert + j);
-        }
-        s_in[r][c] = v;
-      }
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+        if (woff[k] >= 0) (&s_in[0][0])[woff[k]] = pre[k];
       __syncthreads();
+      load(p + 1);
       // y pass on the tile rows, over the tile columns plus the x halo
       // (0 outside the volume: the x pass pads with zeros)
       for (int e = tid; e < kSmTY * (kSmTX + 8); e += 256) {
@@ -879,6 +901,8 @@ smooth3d_kernel(const float* __restrict__ in, long long in_stride, const float* 
       __syncthreads();
 #pragma unroll
       for (int o = -4; o <= 4; o++) xy += s_y[ly][lx + 4 + o] * tx.f[4 - o];
+    } else {
+      load(p + 1);
     }
 #pragma unroll
     for (int k = 0; k < 8; k++) ring[k] = ring[k + 1];
