@@ -215,7 +215,7 @@ def normalisation_rates(ctx, prec) -> dict:
         sizes.append((w, h, d))
     coh = lambda: ctx.register_cohort(subjects, [one] * 64, tpl, one, bank, 10, 10, 8, precision=prec)  # noqa: E731
     timed(coh)
-    ms64 = timed(coh)
+    ms64 = min(timed(coh) for _ in range(2))
     return {
         "t1_to_template": {"value": 1000.0 / ms1, "unit": "subjects/s", "ms_per_subject": ms1,
                            "config": {"subject": [256, 256, 170], "template": [182, 218, 182], "voxel_mm": 1.0,
