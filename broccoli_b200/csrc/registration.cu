@@ -868,17 +868,23 @@ smooth3d_kernel(const float* __restrict__ in, long long in_stride, const float* 
   // smoothed
   float pre[3];
   auto load = [&](int q) {
+    const bool qin = q >= 0 && q < D;
+    const long long base = (long long)q * WH;
 #pragma unroll
     for (int k = 0; k < 3; k++) {
       float v = 0.f;
-      if (q >= 0 && q < D && goff[k] >= 0) {
-        const long long j = (long long)q * WH + goff[k];
-        v = __ldg(src + j);
-        if (CERT) v *= __ldg(cert + j);
+      if (qin && goff[k] >= 0) {
+        v = __ldg(src + base + goff[k]);
+        if (CERT) v *= __ldg(cert + base + goff[k]);
       }
       pre[k] = v;
     }
   };
+  // y-pass outputs of this thread: the tile column above it, and for the
+  // first 64 threads one of the 8 halo columns of a row (4 on each side)
+  const int hr = tid >> 3, hk = tid & 7, hc = hk < 4 ? hk : hk + kSmTX;
+  const bool halo = tid < 8 * kSmTY;
+  const bool hin = x0 - 4 + hc >= 0 && x0 - 4 + hc < W;
   load(z0 - 4);
   for (int p = z0 - 4; p < z1 + 4; p++) {
     float xy = 0.f;
@@ -890,13 +896,17 @@ smooth3d_kernel(const float* __restrict__ in, long long in_stride, const float* 
       load(p + 1);
       // y pass on the tile rows, over the tile columns plus the x halo
       // (0 outside the volume: the x pass pads with zeros)
-      for (int e = tid; e < kSmTY * (kSmTX + 8); e += 256) {
-        const int r = e / (kSmTX + 8), c = e - r * (kSmTX + 8);
-        const int gx = x0 - 4 + c;
+      {
         float sum = 0.f;
 #pragma unroll
-        for (int o = -4; o <= 4; o++) sum += s_in[r + 4 + o][c] * ty.f[4 - o];
-        s_y[r][c] = (gx >= 0 && gx < W) ? sum : 0.f;
+        for (int o = -4; o <= 4; o++) sum += s_in[ly + 4 + o][lx + 4] * ty.f[4 - o];
+        s_y[ly][lx + 4] = x < W ? sum : 0.f;
+      }
+      if (halo) {
+        float sum = 0.f;
+#pragma unroll
+        for (int o = -4; o <= 4; o++) sum += s_in[hr + 4 + o][hc] * ty.f[4 - o];
+        s_y[hr][hc] = hin ? sum : 0.f;
       }
       __syncthreads();
 #pragma unroll
