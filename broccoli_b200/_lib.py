@@ -22,6 +22,7 @@ BRC_ERR_TIMEOUT = -4
 BRC_ERR_NODEVICE = -5
 BRC_ERR_UNSUPPORTED = -6
 BRC_ERR_NONFINITE = -7
+BRC_ERR_SCRATCH_LIMIT = -8
 
 TRANSLATION, RIGID, AFFINE = 0, 1, 2
 PREC_FP32, PREC_BF16X3, PREC_FP32_GENERAL = 0, 1, 2
@@ -68,6 +69,16 @@ class TwoVolumeOpts(ctypes.Structure):
         ("dsigma", ctypes.c_float),
         ("precision", ctypes.c_int),
         ("solve_fp64", ctypes.c_int),
+        ("precenter", ctypes.c_int),
+    ]
+
+
+class DebugOutputs(ctypes.Structure):
+    _fields_ = [
+        ("quadrature_responses", ctypes.c_void_p * 6),
+        ("phase_differences", ctypes.c_void_p),
+        ("phase_certainties", ctypes.c_void_p),
+        ("phase_gradients", ctypes.c_void_p),
     ]
 
 
@@ -177,6 +188,10 @@ _SIGS = {
     "brc_first_level_opts_default": ([ctypes.POINTER(FirstLevelOpts)], None),
     "brc_first_level_preprocess": ([_P, ctypes.POINTER(FirstLevelInput), ctypes.POINTER(FirstLevelOpts),
                                     ctypes.POINTER(FirstLevelOutput)], _I),
+    "brc_ctx_set_debug_outputs": ([_P, ctypes.POINTER(DebugOutputs)], _I),
+    "brc_phase_volumes": ([_P, _P, _P, _I, _I, _I, _I, _P, _P, _P], _I),
+    "brc_multiply_volumes": ([_P, _P, _I, _I, _I, _I, _P], _I),
+    "brc_invert_affine_parameters": ([_P, _P], None),
     "brc_register_cohort": (
         [_P, _I, _P, _P, _P, _P, _I, _I, _I, _P, _P, _P, _P, _P, ctypes.POINTER(TwoVolumeOpts), _P, _P, _P, _P],
         _I),

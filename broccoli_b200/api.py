@@ -404,14 +404,69 @@ class Context:
         _check(self, L.lib().brc_center_of_mass(self.handle, _p(v), W, H, D, c.ctypes.data_as(ctypes.c_void_p)))
         return c
 
+    def phase_volumes(self, q1: torch.Tensor, q2: torch.Tensor, axis: int = 2):
+        """Phase difference, certainty and phase gradient along `axis` of one
+        pair of complex (D,H,W) responses (the reference's linear formulas)."""
+        a = torch.view_as_real(q1.contiguous()).contiguous() if q1.is_complex() else q1.contiguous()
+        c = torch.view_as_real(q2.contiguous()).contiguous() if q2.is_complex() else q2.contiguous()
+        D, H, W = a.shape[:3]
+        out = torch.empty((3, D, H, W), dtype=torch.float32, device=a.device)
+        self._bind_stream()
+        _check(self, L.lib().brc_phase_volumes(self.handle, _p(a), _p(c), W, H, D, axis, _p(out[0]), _p(out[1]),
+                                               _p(out[2])))
+        return out[0], out[1], out[2]
+
+    def multiply_volumes(self, vols: torch.Tensor, mask: torch.Tensor) -> None:
+        """vols (T,D,H,W) or (D,H,W) *= mask (D,H,W), in place."""
+        v = vols if vols.dim() == 4 else vols[None]
+        assert v.is_contiguous() and mask.is_contiguous()
+        T, D, H, W = v.shape
+        self._bind_stream()
+        _check(self, L.lib().brc_multiply_volumes(self.handle, _p(v), W, H, D, T, _p(mask)))
+
+    def set_debug_outputs(self, outputs) -> None:
+        """Host numpy arrays the linear (and, with six responses, nonlinear)
+        registrations fill as the reference does with DEBUG set: a dict with
+        any of 'quadrature_responses' (list of 3 or 6 complex64 arrays),
+        'phase_differences', 'phase_certainties', 'phase_gradients'
+        (float32).  None turns them off.  The arrays must stay alive while
+        debug outputs are on."""
+        if outputs is None:
+            _check(self, L.lib().brc_ctx_set_debug_outputs(self.handle, None))
+            self._debug_keep = None
+            return
+        d = L.DebugOutputs()
+        keep = []
+        for k, a in enumerate(outputs.get("quadrature_responses", []) or []):
+            if a is not None:
+                assert a.dtype == np.complex64 and a.flags.c_contiguous
+                d.quadrature_responses[k] = a.ctypes.data
+                keep.append(a)
+        for name in ("phase_differences", "phase_certainties", "phase_gradients"):
+            a = outputs.get(name)
+            if a is not None:
+                assert a.dtype == np.float32 and a.flags.c_contiguous
+                setattr(d, name, a.ctypes.data)
+                keep.append(a)
+        self._debug_keep = keep
+        _check(self, L.lib().brc_ctx_set_debug_outputs(self.handle, ctypes.byref(d)))
+
+    @staticmethod
+    def invert_affine_parameters(params) -> np.ndarray:
+        p = np.ascontiguousarray(params, np.float32)
+        out = np.zeros(12, np.float32)
+        L.lib().brc_invert_affine_parameters(p.ctypes.data_as(ctypes.c_void_p), out.ctypes.data_as(ctypes.c_void_p))
+        return out
+
     def register_two_volumes(self, subject: torch.Tensor, voxel_size, template: torch.Tensor,
                              template_voxel_size, bank: dict, linear_iterations: int,
                              nonlinear_iterations: int, coarsest_scale: int, mm_z_cut: int = 0,
                              tsigma=5.0, esigma=5.0, dsigma=5.0, solve_fp64: bool = False,
-                             precision: int = L.PREC_FP32):
+                             precision: int = L.PREC_FP32, precenter: bool = False):
         """T1-to-template normalisation.  Returns dict: params (12,),
         interpolated, aligned_linear, aligned_nonlinear (template size) and
-        field (3, D, H, W)."""
+        field (3, D, H, W).  precenter: centre the subject by its centre of
+        mass at its own size first (PRECENTER_REGISTRATION)."""
         s = subject.contiguous()
         t = template.contiguous()
         D, H, W = s.shape
@@ -425,6 +480,7 @@ class Context:
         o.tsigma, o.esigma, o.dsigma = tsigma, esigma, dsigma
         o.solve_fp64 = 1 if solve_fp64 else 0
         o.precision = precision
+        o.precenter = 1 if precenter else 0
         vs = np.ascontiguousarray(voxel_size, np.float32)
         tvs = np.ascontiguousarray(template_voxel_size, np.float32)
         params = np.zeros(12, np.float32)
@@ -444,7 +500,7 @@ class Context:
     def register_cohort(self, subjects, voxel_sizes, template: torch.Tensor, template_voxel_size, bank: dict,
                         linear_iterations: int, nonlinear_iterations: int, coarsest_scale: int,
                         mm_z_cut: int = 0, tsigma=5.0, esigma=5.0, dsigma=5.0, solve_fp64: bool = False,
-                        precision: int = L.PREC_FP32):
+                        precision: int = L.PREC_FP32, precenter: bool = False):
         """T1-to-template normalisation of a cohort: `subjects` is a list of
         (D,H,W) device volumes of any sizes, `voxel_sizes` a matching list of
         (vx, vy, vz).  Returns dict: params (n,12), aligned_linear,
@@ -462,6 +518,7 @@ class Context:
         o.tsigma, o.esigma, o.dsigma = tsigma, esigma, dsigma
         o.solve_fp64 = 1 if solve_fp64 else 0
         o.precision = precision
+        o.precenter = 1 if precenter else 0
         ptrs = (ctypes.c_void_p * n)(*[v.data_ptr() for v in subs])
         sizes = np.ascontiguousarray([[v.shape[2], v.shape[1], v.shape[0]] for v in subs], np.int32)
         vs = np.ascontiguousarray(voxel_sizes, np.float32).reshape(n, 3)

@@ -5,7 +5,10 @@
 // :1086-1143, affine matrix file :1220-1246, volumes :1250-1302): outputs
 // at the reference's size under its header, input_aligned_linear.nii,
 // input_aligned_nonlinear.nii and, on request, input_interpolated.nii,
-// input_displacement_{x,y,z}.nii and input_affinematrix.txt.
+// input_displacement_{x,y,z}.nii, input_affinematrix.txt, input_masked.nii
+// (-mask / -maskoriginal, :1292-1295) and the debug volumes of -debug
+// (:1304-1318: phase differences, certainties and gradients, the three
+// quadrature filter responses as real and imaginary volumes).
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -34,6 +37,11 @@ static void usage() {
   printf(" -output                 Output base filename (default: the input's)\n");
   printf(" -filters                Directory of the filter files (default $BROCCOLI_DIR/filters)\n");
   printf(" -precision              fp32 (default) or bf16x3 (tensor-core filtering)\n");
+  printf(" -precenter              Centre the input volume by its centre of mass first (default off)\n");
+  printf(" -mask                   Mask (reference size) applied after the registration, e.g. a skull strip\n");
+  printf(" -maskoriginal           Mask applied to the interpolated, unregistered input through the inverse\n");
+  printf("                         affine transform\n");
+  printf(" -debug                  Save the phase differences, certainties, gradients and filter responses\n");
   printf(" -quiet                  Print nothing\n");
   printf(" -verbose                Print extra information\n\n");
 }
@@ -46,6 +54,8 @@ int main(int argc, char** argv) {
   int device = 0, it_lin = 10, it_nonlin = 10, coarsest = 4, zcut = 0, precision = BRC_PREC_FP32;
   float sigma = 5.0f;
   bool save_matrix = false, save_field = false, save_interp = false, quiet = false, verbose = false;
+  bool precenter = false, debug = false, mask_original = false;
+  const char* mask_name = nullptr;
   const char* out_opt = nullptr;
   const char* filters_opt = nullptr;
   for (int i = 3; i < argc; i++) {
@@ -82,9 +92,14 @@ int main(int argc, char** argv) {
           return EXIT_FAILURE;
         }
       }
-    } else if (o == "-precenter" || o == "-mask" || o == "-maskoriginal" || o == "-debug") {
-      fprintf(stderr, "Option %s is not supported by this build\n", argv[i]);
-      return EXIT_FAILURE;
+    } else if (o == "-precenter") {
+      precenter = true;
+    } else if (o == "-debug") {
+      debug = true;
+    } else if (o == "-mask" || o == "-maskoriginal") {
+      if (!cli::has_value(i, argc, argv)) return EXIT_FAILURE;
+      mask_name = argv[++i];
+      mask_original = o == "-maskoriginal";
     } else {
       fprintf(stderr, "Unknown option %s\n", argv[i]);
       return EXIT_FAILURE;
@@ -96,11 +111,20 @@ int main(int argc, char** argv) {
     return EXIT_FAILURE;
   }
 
-  brc_nifti t1, mni;
+  brc_nifti t1, mni, mask;
+  memset(&mask, 0, sizeof(mask));
   if (!cli::read_nifti(argv[1], &t1) || !cli::read_nifti(argv[2], &mni)) return EXIT_FAILURE;
   const int W = t1.dim[1], H = t1.dim[2], D = t1.dim[3];
   const int W2 = mni.dim[1], H2 = mni.dim[2], D2 = mni.dim[3];
   const size_t V2 = (size_t)W2 * H2 * D2;
+  if (mask_name) {
+    if (!cli::read_nifti(mask_name, &mask)) return EXIT_FAILURE;
+    if (mask.dim[1] != W2 || mask.dim[2] != H2 || mask.dim[3] != D2) {
+      fprintf(stderr, "Reference volume has the dimensions %d x %d x %d, while the mask volume has the dimensions "
+                      "%d x %d x %d. Aborting!\n", W2, H2, D2, mask.dim[1], mask.dim[2], mask.dim[3]);
+      return EXIT_FAILURE;
+    }
+  }
   const std::string dir = cli::filter_dir(filters_opt);
   if (dir.empty()) {
     fprintf(stderr, "Give -filters DIR or set BROCCOLI_DIR\n");
@@ -167,6 +191,23 @@ int main(int argc, char** argv) {
   broccoli.SetOutputAlignedT1VolumeNonLinear(nonlin.data());
   broccoli.SetOutputT1MNIRegistrationParameters(params.data());
   broccoli.SetOutputDisplacementField(fx.data(), fy.data(), fz.data());
+  broccoli.SetPrecenterRegistration(precenter);
+  std::vector<float> masked(mask_name ? V2 : 0), pd(debug ? V2 : 0), pc(debug ? V2 : 0), pg(debug ? V2 : 0);
+  std::vector<cl_float2> q[3];
+  if (mask_name) {
+    broccoli.SetInputMNIBrainMask(mask.data);
+    broccoli.SetOutputSkullstrippedT1Volume(masked.data());
+    broccoli.SetDoSkullstrip(!mask_original);
+    broccoli.SetDoSkullstripOriginal(mask_original);
+  }
+  if (debug) {
+    for (int k = 0; k < 3; k++) q[k].resize(V2);
+    broccoli.SetDebug(true);
+    broccoli.SetOutputQuadratureFilterResponses(q[0].data(), q[1].data(), q[2].data());
+    broccoli.SetOutputPhaseDifferences(pd.data());
+    broccoli.SetOutputPhaseCertainties(pc.data());
+    broccoli.SetOutputPhaseGradients(pg.data());
+  }
   broccoli.PerformRegistrationTwoVolumesWrapper();
   if (broccoli.GetLastStatus() != BRC_OK) {
     fprintf(stderr, "Registration failed: %s\n", broccoli.GetOpenCLError());
@@ -207,7 +248,25 @@ int main(int argc, char** argv) {
       ok = cli::write_nifti(cli::with_suffix(base, "_displacement_z"), &mni, fz.data(), W2, H2, D2, 1, quiet) && ok;
     }
   }
+  if (mask_name && (!mask_original || it_lin > 0))
+    ok = cli::write_nifti(cli::with_suffix(base, "_masked"), &mni, masked.data(), W2, H2, D2, 1, quiet) && ok;
+  if (debug) {
+    ok = cli::write_nifti(cli::with_suffix(base, "_phase_gradients"), &mni, pg.data(), W2, H2, D2, 1, quiet) && ok;
+    ok = cli::write_nifti(cli::with_suffix(base, "_phase_certainties"), &mni, pc.data(), W2, H2, D2, 1, quiet) && ok;
+    ok = cli::write_nifti(cli::with_suffix(base, "_phase_differences"), &mni, pd.data(), W2, H2, D2, 1, quiet) && ok;
+    std::vector<float> re(V2), im(V2);
+    for (int k = 0; k < 3; k++) {
+      for (size_t i = 0; i < V2; i++) {
+        re[i] = q[k][i].x;
+        im[i] = q[k][i].y;
+      }
+      const std::string n = "_quadrature_filter_response_" + std::to_string(k + 1);
+      ok = cli::write_nifti(cli::with_suffix(base, n + "_real"), &mni, re.data(), W2, H2, D2, 1, quiet) && ok;
+      ok = cli::write_nifti(cli::with_suffix(base, n + "_imag"), &mni, im.data(), W2, H2, D2, 1, quiet) && ok;
+    }
+  }
   brc_nifti_free(&t1);
   brc_nifti_free(&mni);
+  if (mask_name) brc_nifti_free(&mask);
   return ok ? EXIT_SUCCESS : EXIT_FAILURE;
 }

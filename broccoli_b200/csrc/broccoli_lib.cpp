@@ -71,13 +71,18 @@ bool BROCCOLI_LIB::OpenCLInitiate(cl_uint platform, cl_uint device) {
 
 bool BROCCOLI_LIB::GetOpenCLInitiated() { return initiated_; }
 std::string BROCCOLI_LIB::GetOpenCLInitializationError() { return init_error_; }
-const char* BROCCOLI_LIB::GetOpenCLError() { return ctx_ ? brc_last_error(ctx_) : init_error_.c_str(); }
+const char* BROCCOLI_LIB::GetOpenCLError() {
+  if (!last_error_.empty()) return last_error_.c_str();
+  return ctx_ ? brc_last_error(ctx_) : init_error_.c_str();
+}
 const char* BROCCOLI_LIB::GetOpenCLErrorMessage(int error) { return brc_status_string(error); }
 int* BROCCOLI_LIB::GetOpenCLRunKernelErrors() { return run_errors_; }
+int* BROCCOLI_LIB::GetOpenCLCreateKernelErrors() { return create_kernel_errors_; }
+int* BROCCOLI_LIB::GetOpenCLCreateBufferErrors() { return create_buffer_errors_; }
 
 void BROCCOLI_LIB::SetWrapper(int w) { wrapper_ = w; }
 void BROCCOLI_LIB::SetVerbose(bool v) { verbose_ = v; }
-void BROCCOLI_LIB::SetDebug(bool) {}
+void BROCCOLI_LIB::SetDebug(bool d) { debug_ = d; }
 
 void BROCCOLI_LIB::SetEPIWidth(size_t w) { epi_w_ = w; }
 void BROCCOLI_LIB::SetEPIHeight(size_t h) { epi_h_ = h; }
@@ -106,6 +111,10 @@ void BROCCOLI_LIB::SetInputT1Volume(float* p) { h_t1_ = p; }
 void BROCCOLI_LIB::SetInputMNIVolume(float* p) { h_mni_ = p; }
 void BROCCOLI_LIB::SetInputMNIBrainVolume(float* p) { h_mni_brain_ = p; }
 
+void BROCCOLI_LIB::SetPrecenterRegistration(bool c) { precenter_ = c; }
+void BROCCOLI_LIB::SetDoSkullstrip(bool b) { do_skullstrip_ = b; }
+void BROCCOLI_LIB::SetDoSkullstripOriginal(bool b) { do_skullstrip_original_ = b; }
+void BROCCOLI_LIB::SetInputMNIBrainMask(float* m) { h_mni_mask_ = m; }
 void BROCCOLI_LIB::SetImageRegistrationFilterSize(int N) { filter_size_ = N; }
 void BROCCOLI_LIB::SetLinearImageRegistrationFilters(float* a, float* b, float* c, float* d, float* e,
                                                      float* f) {
@@ -186,7 +195,17 @@ void BROCCOLI_LIB::SetOutputQuadratureFilterResponses(cl_float2* a, cl_float2* b
   out_q_[0] = a;
   out_q_[1] = b;
   out_q_[2] = c;
+  out_q_[3] = out_q_[4] = out_q_[5] = nullptr;
 }
+void BROCCOLI_LIB::SetOutputQuadratureFilterResponses(cl_float2* a, cl_float2* b, cl_float2* c, cl_float2* d,
+                                                      cl_float2* e, cl_float2* f) {
+  cl_float2* q[6] = {a, b, c, d, e, f};
+  for (int k = 0; k < 6; k++) out_q_[k] = q[k];
+}
+void BROCCOLI_LIB::SetOutputPhaseDifferences(float* p) { out_pd_ = p; }
+void BROCCOLI_LIB::SetOutputPhaseCertainties(float* p) { out_pc_ = p; }
+void BROCCOLI_LIB::SetOutputPhaseGradients(float* p) { out_pg_ = p; }
+void BROCCOLI_LIB::SetOutputSkullstrippedT1Volume(float* p) { out_skullstripped_ = p; }
 void BROCCOLI_LIB::SetOutputEPIT1RegistrationParameters(float* o) { out_params_epi_t1_ = o; }
 void BROCCOLI_LIB::SetOutputEPIMNIRegistrationParameters(float* o) { out_params_epi_mni_ = o; }
 void BROCCOLI_LIB::SetOutputAlignedEPIVolumeT1(float* o) { out_aligned_epi_t1_ = o; }
@@ -204,11 +223,28 @@ void BROCCOLI_LIB::SetSaveSmoothed(bool b) { save_smoothed_ = b; }
 
 bool BROCCOLI_LIB::check(int status, const char* where) {
   last_status_ = status;
-  if (status == BRC_OK) return true;
+  if (status == BRC_OK) {
+    last_error_.clear();
+    return true;
+  }
   run_errors_[0] = status;
-  init_error_ = std::string(where) + ": " + brc_status_string(status) + (ctx_ ? std::string(" (") +
+  if (status == BRC_ERR_NOMEM) create_buffer_errors_[0] = status;
+  last_error_ = std::string(where) + ": " + brc_status_string(status) + (ctx_ ? std::string(" (") +
                 brc_last_error(ctx_) + ")" : std::string());
   return false;
+}
+
+// The DEBUG outputs of the registrations (SetDebug, broccoli_lib.cpp:
+// 5285-5289, :5349-5354) handed to the context before each entry point.
+bool BROCCOLI_LIB::apply_debug() {
+  if (!debug_) return check(brc_ctx_set_debug_outputs(ctx_, nullptr), "SetDebug");
+  brc_debug_outputs d;
+  memset(&d, 0, sizeof(d));
+  for (int k = 0; k < 6; k++) d.quadrature_responses[k] = out_q_[k];
+  d.phase_differences = out_pd_;
+  d.phase_certainties = out_pc_;
+  d.phase_gradients = out_pg_;
+  return check(brc_ctx_set_debug_outputs(ctx_, &d), "SetDebug");
 }
 
 bool BROCCOLI_LIB::pack_linear(float* bank) {
@@ -248,6 +284,7 @@ void BROCCOLI_LIB::PerformMotionCorrectionWrapper() {
   o.type = BRC_RIGID;
   o.precision = precision_;
   o.tolerance = mc_tolerance_;
+  if (!apply_debug()) return;
   const int W = (int)epi_w_, H = (int)epi_h_, D = (int)epi_d_, T = (int)epi_t_;
   std::vector<float> motion(6 * (size_t)T);
   const float* ref = change_mc_reference_ ? h_mc_reference_ : nullptr;
@@ -454,6 +491,14 @@ void BROCCOLI_LIB::PerformRegistrationTwoVolumesWrapper() {
   o.dsigma = dsigma_;
   o.precision = precision_;
   o.solve_fp64 = solve_fp64_ ? 1 : 0;
+  o.precenter = precenter_ ? 1 : 0;
+  const bool strip = do_skullstrip_ || (do_skullstrip_original_ && it_linear_ > 0);
+  if (strip && (!h_mni_mask_ || !out_skullstripped_)) {
+    check(BRC_ERR_INVALID, "PerformRegistrationTwoVolumesWrapper: skull strip needs SetInputMNIBrainMask and "
+                           "SetOutputSkullstrippedT1Volume");
+    return;
+  }
+  if (!apply_debug()) return;
   float params[12];
   if (!check(brc_register_two_volumes(ctx_, d_in.f(), (int)t1_w_, (int)t1_h_, (int)t1_d_, t1_vox_, d_tpl.f(),
                                       (int)mni_w_, (int)mni_h_, (int)mni_d_, mni_vox_, bank3,
@@ -475,6 +520,30 @@ void BROCCOLI_LIB::PerformRegistrationTwoVolumesWrapper() {
       if (out_field_[a] &&
           !check(brc_copy_to_host(ctx_, out_field_[a], d_field.f() + a * V2, sizeof(float) * V2), "D2H"))
         return;
+  }
+  if (strip) {
+    // broccoli_lib.cpp:8064-8105: DO_SKULLSTRIP multiplies the last aligned
+    // volume by the brain mask; DO_SKULLSTRIP_ORIGINAL carries the mask back
+    // by the inverse affine transform (NEAREST) and multiplies the
+    // interpolated volume by it
+    DeviceArray d_mask(ctx_, sizeof(float) * V2);
+    if (!check(d_mask.status, "alloc")) return;
+    if (!check(brc_copy_to_device(ctx_, d_mask.ptr, h_mni_mask_, sizeof(float) * V2), "H2D")) return;
+    float* vol = nonlinear ? d_nonlin.f() : d_lin.f();
+    const float* mask = d_mask.f();
+    if (!do_skullstrip_) {
+      float inv[12];
+      brc_invert_affine_parameters(params, inv);
+      if (!check(brc_transform_volumes_linear(ctx_, d_mask.f(), (int)mni_w_, (int)mni_h_, (int)mni_d_, 1, inv,
+                                              BRC_INTERP_NEAREST, d_field.f()),
+                 "skull strip: mask to the original space"))
+        return;
+      vol = d_interp.f();
+      mask = d_field.f();
+    }
+    if (!check(brc_multiply_volumes(ctx_, vol, (int)mni_w_, (int)mni_h_, (int)mni_d_, 1, mask), "skull strip"))
+      return;
+    check(brc_copy_to_host(ctx_, out_skullstripped_, vol, sizeof(float) * V2), "D2H");
   }
 }
 
@@ -554,5 +623,6 @@ void BROCCOLI_LIB::PerformFirstLevelAnalysisWrapper() {
   out.motion_corrected = save_mc_ && out_mc_ != h_fmri_ ? out_mc_ : nullptr;
   out.epi_mask = save_epi_mask_ ? out_epi_mask_ : nullptr;
   out.smoothed = save_smoothed_ && out_smoothed_ != h_fmri_ ? out_smoothed_ : nullptr;
+  if (!apply_debug()) return;
   check(brc_first_level_preprocess(ctx_, &in, &o, &out), "brc_first_level_preprocess");
 }

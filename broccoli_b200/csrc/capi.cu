@@ -434,6 +434,41 @@ int brc_copy_to_host(brc_ctx* ctx, void* h_dst, const void* d_src, size_t bytes)
   return BRC_OK;
 }
 
+int brc_ctx_set_debug_outputs(brc_ctx* ctx, const brc_debug_outputs* outs) {
+  BRC_CHECK_CTX(ctx);
+  if (outs) {
+    ctx->dbg = *outs;
+    ctx->dbg_on = true;
+  } else {
+    ctx->dbg = brc_debug_outputs{};
+    ctx->dbg_on = false;
+  }
+  return BRC_OK;
+}
+
+int brc_phase_volumes(brc_ctx* ctx, const float* d_q1, const float* d_q2, int W, int H, int D, int axis,
+                      float* d_phase_diff, float* d_cert, float* d_grad) {
+  BRC_CHECK_CTX(ctx);
+  if (!d_q1 || !d_q2 || bad_dims(W, H, D) || axis < 0 || axis > 2)
+    return ctx->fail(BRC_ERR_INVALID, "brc_phase_volumes: bad pointer, size or axis");
+  if (!d_phase_diff && !d_cert && !d_grad) return BRC_OK;
+  cudaSetDevice(ctx->device);
+  BRC_TRY(ctx, brc::phase_volumes(d_q1, d_q2, W, H, D, axis, d_phase_diff, d_cert, d_grad, ctx->stream()),
+          "phase_volumes");
+  ctx->launches += 1;
+  return BRC_OK;
+}
+
+int brc_multiply_volumes(brc_ctx* ctx, float* d_vols, int W, int H, int D, int T, const float* d_mask) {
+  BRC_CHECK_CTX(ctx);
+  if (!d_vols || !d_mask || bad_dims(W, H, D) || T <= 0 || T > 65535)
+    return ctx->fail(BRC_ERR_INVALID, "brc_multiply_volumes: bad pointer or size");
+  cudaSetDevice(ctx->device);
+  BRC_TRY(ctx, brc::multiply_mask(d_vols, d_mask, (long long)W * H * D, T, ctx->stream()), "multiply");
+  ctx->launches += 1;
+  return BRC_OK;
+}
+
 void brc_linear_opts_default(brc_linear_opts* o, int iterations) {
   if (!o) return;
   o->iterations = iterations;
@@ -526,7 +561,50 @@ long long enqueue_registration(brc_ctx* ctx, const RegPlan& p, cudaStream_t st) 
   return kernels;
 }
 
+// The reference's DEBUG reads of one AlignTwoVolumesLinear call
+// (broccoli_lib.cpp:5285-5289, :5349-5354), for the last instance of the
+// batch: the reference volume's three responses, and the z-axis phase
+// difference, certainty and gradient of iteration 0, whose aligned volume
+// is the moving volume itself (the parameters start at 0).  Synchronises.
+int debug_linear(brc_ctx* ctx, const RegPlan& p, cudaStream_t st) {
+  int s = debug_capture_check(ctx, "debug outputs");
+  if (s != BRC_OK) return s;
+  const long long V = (long long)p.W * p.H * p.D;
+  const int b = p.batch - 1;
+  const float* qref = p.q1 + (p.ref_stride ? 6 * V * b : 0);
+  for (int k = 0; k < 3; k++)
+    if (ctx->dbg.quadrature_responses[k])
+      BRC_TRY(ctx, cudaMemcpyAsync(ctx->dbg.quadrature_responses[k], qref + 2 * V * k, sizeof(float) * 2 * V,
+                                   cudaMemcpyDeviceToHost, st), "debug D2H");
+  float* outs[3] = {ctx->dbg.phase_differences, ctx->dbg.phase_certainties, ctx->dbg.phase_gradients};
+  if (p.opts.iterations > 0 && (outs[0] || outs[1] || outs[2])) {
+    BRC_TRY(ctx, ctx->dbg_q.ensure(sizeof(float) * 6 * V), "alloc debug");
+    BRC_TRY(ctx, ctx->dbg_v.ensure(sizeof(float) * 3 * V), "alloc debug");
+    float* q = ctx->dbg_q.as<float>();
+    float* v = ctx->dbg_v.as<float>();
+    BRC_TRY(ctx, run_filter(p.fpath, p.moving + V * b, p.W, p.H, p.D, 1, V, q, brc::all_instances(), st),
+            "debug filter");
+    BRC_TRY(ctx, brc::phase_volumes(qref + 4 * V, q + 4 * V, p.W, p.H, p.D, 2, v, v + V, v + 2 * V, st),
+            "debug phase");
+    ctx->launches += 1 + filter_launches(p.fpath);
+    for (int k = 0; k < 3; k++)
+      if (outs[k])
+        BRC_TRY(ctx, cudaMemcpyAsync(outs[k], v + V * k, sizeof(float) * V, cudaMemcpyDeviceToHost, st),
+                "debug D2H");
+  }
+  BRC_TRY(ctx, cudaStreamSynchronize(st), "debug synchronize");
+  return BRC_OK;
+}
+
 }  // namespace
+
+int debug_capture_check(brc_ctx* ctx, const char* where) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  BRC_TRY(ctx, cudaStreamIsCapturing(ctx->stream(), &cs), "capture status");
+  if (cs != cudaStreamCaptureStatusNone)
+    return ctx->fail(BRC_ERR_UNSUPPORTED, std::string(where) + ": not available under stream capture");
+  return BRC_OK;
+}
 
 extern "C" int brc_register_linear_batched(brc_ctx* ctx, const float* d_ref, long long ref_stride,
                                            const float* d_moving, int W, int H, int D, int batch,
@@ -640,6 +718,7 @@ extern "C" int brc_register_linear_batched(brc_ctx* ctx, const float* d_ref, lon
     }
     ctx->launches += ge->kernels;
   }
+  if (ctx->dbg_on) return debug_linear(ctx, p, user);
   return BRC_OK;
 }
 

@@ -73,6 +73,10 @@ struct brc_ctx {
   DevBuf smask;   // smoothed certainty of brc_smooth_normalized
   // tensor-core tile height chosen by timing, per (nfilt, W, H, D)
   std::map<std::tuple<int, int, int, int>, int> tc_tuned;
+  // host arrays of the debug outputs (brc_ctx_set_debug_outputs)
+  bool dbg_on = false;
+  brc_debug_outputs dbg{};
+  DevBuf dbg_q, dbg_v;  // device staging of the debug outputs
 
   cudaStream_t stream() const { return use_user_stream ? user_stream : own_stream; }
 
@@ -133,6 +137,8 @@ int make_filter_path(brc_ctx* ctx, const float* h_filters, int nfilt, int precis
 inline int filter_launches(const FilterPath&) { return 1; }
 cudaError_t run_filter(const FilterPath& fp, const float* vol, int W, int H, int D, int batch, long long stride,
                        float* out, brc::ActiveSet act, cudaStream_t st);
+// Refuses debug writes while the context's stream is being captured.
+int debug_capture_check(brc_ctx* ctx, const char* where);
 
 #define BRC_CHECK_CTX(ctx) \
   do {                     \

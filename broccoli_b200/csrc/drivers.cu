@@ -202,6 +202,20 @@ extern "C" int brc_register_nonlinear(brc_ctx* ctx, const float* d_ref, const fl
       ctx->launches += 1;
     }
   }
+  if (ctx->dbg_on) {
+    bool six = true;
+    for (int k = 0; k < 6; k++) six = six && ctx->dbg.quadrature_responses[k] != nullptr;
+    if (six) {
+      // the finest scale's reference responses, still in q1 (the reads kept
+      // commented out at broccoli_lib.cpp:5754-5759)
+      int s = debug_capture_check(ctx, "debug outputs");
+      if (s != BRC_OK) return s;
+      for (int k = 0; k < 6; k++)
+        BRC_TRY(ctx, cudaMemcpyAsync(ctx->dbg.quadrature_responses[k], ctx->q1.as<float>() + 2 * V * k,
+                                     sizeof(float) * 2 * V, cudaMemcpyDeviceToHost, st), "debug D2H");
+      BRC_TRY(ctx, cudaStreamSynchronize(st), "debug synchronize");
+    }
+  }
   return BRC_OK;
 }
 
@@ -343,10 +357,22 @@ extern "C" void brc_two_volume_opts_default(brc_two_volume_opts* o) {
   o->dsigma = 5.0f;
   o->precision = BRC_PREC_FP32;
   o->solve_fp64 = 0;
+  o->precenter = 0;
+}
+
+// PRECENTER_REGISTRATION (broccoli_lib.cpp:8003-8007): the input centred by
+// its centre of mass at its own size, twice (the two CenterVolumeMass calls,
+// both LINEAR), into `out` (a buffer of the input's size); `tmp` is a second
+// such buffer.
+static int precenter_volume(brc_ctx* ctx, const float* d_in, int W, int H, int D, float* tmp, float* out) {
+  int s = brc_center_volumes(ctx, d_in, W, H, D, 1, BRC_INTERP_LINEAR, tmp, nullptr);
+  if (s != BRC_OK) return s;
+  return brc_center_volumes(ctx, tmp, W, H, D, 1, BRC_INTERP_LINEAR, out, nullptr);
 }
 
 // PerformRegistrationTwoVolumesWrapper, broccoli_lib.cpp:7973-8112 (single
-// volume, no pre-centring, no skull strip): resample to the template grid,
+// volume; the skull strip is left to the caller, which holds the mask):
+// optional pre-centring of the input, resample to the template grid,
 // match centres of mass, multi-scale affine, compose with the mass match,
 // multi-scale nonlinear, add the affine motion to the field, resample the
 // input again and warp it once by the combined field.
@@ -375,8 +401,16 @@ extern "C" int brc_register_two_volumes(brc_ctx* ctx, const float* d_in, int W, 
   float* w = work.as<float>();
   float* a = lin.as<float>();
   float* dparams = a + V2;
-  int s = brc_change_resolution_and_size(ctx, d_in, W, H, D, voxel_size3, w, W2, H2, D2, tpl_voxel_size3,
-                                         o->mm_z_cut);
+  int s;
+  DevBuf cen;
+  if (o->precenter && o->linear_iterations > 0) {
+    const long long V1 = (long long)W * H * D;
+    BRC_TRY(ctx, cen.ensure(sizeof(float) * 2 * V1), "alloc");
+    if ((s = precenter_volume(ctx, d_in, W, H, D, cen.as<float>() + V1, cen.as<float>())) != BRC_OK) return s;
+    d_in = cen.as<float>();  // the centred input replaces the input throughout
+  }
+  s = brc_change_resolution_and_size(ctx, d_in, W, H, D, voxel_size3, w, W2, H2, D2, tpl_voxel_size3,
+                                     o->mm_z_cut);
   if (s != BRC_OK) return s;
   float c1[3], c2[3];
   if ((s = brc_center_of_mass(ctx, w, W2, H2, D2, c1)) != BRC_OK) return s;
@@ -486,6 +520,59 @@ void brc::host_add_affine(const float* old12, const float* new12, float* total) 
   total[9] = (float)T[8]; total[10] = (float)T[9]; total[11] = (float)(T[10] - 1.0);
 }
 
+// 4x4 inverse of a parameter vector's affine matrix in double by
+// Gauss-Jordan elimination with partial pivoting, rounded to float
+// (InvertAffineRegistrationParameters, broccoli_lib.cpp:7186-7250).
+void brc::host_invert_affine(const float* p, float* inv) {
+  double M[4][8] = {{(double)(p[3] + 1.0f), p[4], p[5], p[0]},
+                    {p[6], (double)(p[7] + 1.0f), p[8], p[1]},
+                    {p[9], p[10], (double)(p[11] + 1.0f), p[2]},
+                    {0.0, 0.0, 0.0, 1.0}};
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) M[i][4 + j] = i == j ? 1.0 : 0.0;
+  for (int c = 0; c < 4; c++) {
+    int piv = c;
+    for (int r = c + 1; r < 4; r++)
+      if (fabs(M[r][c]) > fabs(M[piv][c])) piv = r;
+    if (piv != c)
+      for (int j = 0; j < 8; j++) {
+        const double t = M[c][j];
+        M[c][j] = M[piv][j];
+        M[piv][j] = t;
+      }
+    const double d = M[c][c];
+    for (int j = 0; j < 8; j++) M[c][j] /= d;
+    for (int r = 0; r < 4; r++)
+      if (r != c) {
+        const double f = M[r][c];
+        if (f != 0.0)
+          for (int j = 0; j < 8; j++) M[r][j] -= f * M[c][j];
+      }
+  }
+  double I[4][4];
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) I[i][j] = M[i][4 + j];
+  inv[0] = (float)I[0][3];
+  inv[1] = (float)I[1][3];
+  inv[2] = (float)I[2][3];
+  inv[3] = (float)(I[0][0] - 1.0);
+  inv[4] = (float)I[0][1];
+  inv[5] = (float)I[0][2];
+  inv[6] = (float)I[1][0];
+  inv[7] = (float)(I[1][1] - 1.0);
+  inv[8] = (float)I[1][2];
+  inv[9] = (float)I[2][0];
+  inv[10] = (float)I[2][1];
+  inv[11] = (float)(I[2][2] - 1.0);
+}
+
+extern "C" void brc_invert_affine_parameters(const float* h_params12, float* h_inverse12) {
+  if (!h_params12 || !h_inverse12) return;
+  float tmp[12];
+  brc::host_invert_affine(h_params12, tmp);
+  memcpy(h_inverse12, tmp, sizeof(tmp));
+}
+
 extern "C" int brc_register_cohort(brc_ctx* ctx, int n, const float* const* d_subjects, const int* sizes3n,
                                    const float* voxel_sizes3n, const float* d_tpl, int W2, int H2, int D2,
                                    const float* tpl_voxel_size3, const float* h_filters3, const float* h_filters6,
@@ -518,6 +605,21 @@ extern "C" int brc_register_cohort(brc_ctx* ctx, int n, const float* const* d_su
   BRC_TRY(ctx, prm.ensure(sizeof(float) * 12 * n), "alloc");
   BRC_TRY(ctx, jobs.ensure(brc::resize_job_bytes() * n), "alloc");
   std::vector<unsigned char> h_jobs(brc::resize_job_bytes() * n);
+  // 0. optional pre-centring of every subject at its own size
+  std::vector<const float*> srcs(d_subjects, d_subjects + n);
+  std::vector<std::unique_ptr<DevBuf>> centred;
+  if (o->precenter && o->linear_iterations > 0) {
+    for (int b = 0; b < n; b++) {
+      const long long V1 = (long long)sizes3n[3 * b] * sizes3n[3 * b + 1] * sizes3n[3 * b + 2];
+      centred.emplace_back(new DevBuf());
+      BRC_TRY(ctx, centred.back()->ensure(sizeof(float) * 2 * V1), "alloc");
+      float* c = centred.back()->as<float>();
+      int s0 = precenter_volume(ctx, d_subjects[b], sizes3n[3 * b], sizes3n[3 * b + 1], sizes3n[3 * b + 2], c + V1, c);
+      if (s0 != BRC_OK) return s0;
+      srcs[b] = c;
+    }
+  }
+  d_subjects = srcs.data();
   // 1. every subject onto the template grid in one ragged launch
   BRC_TRY(ctx, brc::resize_to_grid_ragged(n, d_subjects, sizes3n, voxel_sizes3n, h_jobs.data(), jobs.ptr,
                                           res.as<float>(), W2, H2, D2, tpl_voxel_size3, o->mm_z_cut, st),

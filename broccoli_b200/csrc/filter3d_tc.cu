@@ -45,8 +45,9 @@
 //
 // Two TMEM accumulators (2 x 256 of the SM's 512 columns) let the epilogue
 // of tile i run under the GEMMs of tile i + 1.  Every wait is bounded
-// (about 2 s); a CTA that gives up sets *err, drains its copies in flight,
-// frees its TMEM and returns.
+// (about 2 s); a CTA that gives up sets *err, waits (bounded) for its MMAs
+// and copies in flight, frees its TMEM and returns.  The responses of a
+// launch that timed out are undefined.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -398,6 +399,9 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
     flags[1] = i;
     flags[3] = (int)G;
     if (!ok) flags[4] = 1;
+    // on every exit, the give-up path included: one commit that tracks all
+    // MMAs this thread issued, waited on (bounded) before the TMEM and the
+    // shared-memory stages are released below
     mma_commit(done);
     if (!mbar_wait(done, 0)) flags[4] = 1;
   } else if (warp == 2 && lane == 0) {

@@ -48,6 +48,10 @@ cudaError_t smooth3d(const float* vol, int W, int H, int D, int batch, const flo
 // out[i] = phase_atan2(y[i], x[i]) (the arctangent of the phase kernels).
 cudaError_t phase_atan2_eval(const float* y, const float* x, float* out, long long n, cudaStream_t st);
 cudaError_t multiply_mask(float* vols, const float* mask, long long V, int batch, cudaStream_t st);
+// Phase difference, certainty and phase gradient along `axis` of one filter
+// pair (the reference's linear formulas; outputs may be null).
+cudaError_t phase_volumes(const float* q1, const float* q2, int W, int H, int D, int axis, float* pd, float* cert,
+                          float* grad, cudaStream_t st);
 // nonlinear.cu
 cudaError_t tensor_norm_max(const float* t6, long long V, float* a11, unsigned int* maxbits,
                             cudaStream_t st);
@@ -91,6 +95,8 @@ cudaError_t add_affine_to_field(float* field, int W, int H, int D, const float* 
 // Host composition total = new * old of two parameter vectors (4x4 affine
 // matrices in double); total may alias old12.
 void host_add_affine(const float* old12, const float* new12, float* total);
+// Host inverse of a parameter vector (4x4 affine matrix in double).
+void host_invert_affine(const float* p12, float* inv12);
 }  // namespace brc
 
 namespace brc {

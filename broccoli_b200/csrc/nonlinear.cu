@@ -114,8 +114,8 @@ nonlinear_ah_kernel(const float2* __restrict__ q1, const float2* __restrict__ q2
 
 // d = A^-1 h per voxel.  fp64 = 0: cofactors in FP32 with det + 1e-16f
 // (CalculateDisplacementUpdate, kernelRegistration.cpp:948-988); fp64 = 1:
-// the same cofactor solve in FP64 (no regularising 1e-16, a singular system
-// gives d = 0).
+// the same regularised cofactor solve, det + 1e-16, in FP64 (a non-finite
+// inverse gives d = 0).
 __global__ void __launch_bounds__(256)
 displacement_update_kernel(const float* __restrict__ a6, const float* __restrict__ h3, long long V,
                            int fp64, float* __restrict__ d3) {
@@ -139,14 +139,17 @@ displacement_update_kernel(const float* __restrict__ a6, const float* __restrict
     const double h1 = h3[i], h2 = h3[V + i], hh3 = h3[2 * V + i];
     const double c11 = a22 * a33 - a23 * a23, c12 = a13 * a23 - a12 * a33, c13 = a12 * a23 - a13 * a22;
     const double c22 = a11 * a33 - a13 * a13, c23 = a12 * a13 - a11 * a23, c33 = a11 * a22 - a12 * a12;
+    // the reference's regularised inverse, det + 1e-16, evaluated in double:
+    // in near-singular (background) voxels the 1e-16 damps the update, and
+    // the exact inverse there would be a different algorithm
     const double det = a11 * c11 + a12 * c12 + a13 * c13;
-    if (det == 0.0 || !isfinite(det)) {
+    const double r = 1.0 / (det + 1e-16);
+    if (!isfinite(r)) {
       d3[i] = 0.f;
       d3[V + i] = 0.f;
       d3[2 * V + i] = 0.f;
       return;
     }
-    const double r = 1.0 / det;
     d3[i] = (float)(r * (c11 * h1 + c12 * h2 + c13 * hh3));
     d3[V + i] = (float)(r * (c12 * h1 + c22 * h2 + c23 * hh3));
     d3[2 * V + i] = (float)(r * (c13 * h1 + c23 * h2 + c33 * hh3));

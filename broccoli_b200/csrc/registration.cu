@@ -1049,6 +1049,63 @@ __global__ void phase_atan2_kernel(const float* __restrict__ y, const float* __r
     out[i] = phase_atan2(y[i], x[i]);
 }
 
+// The reference's linear phase quantities of one filter pair, volume by
+// volume (CalculatePhaseDifferencesAndCertainties, CalculatePhaseGradients
+// X/Y/Z, kernelRegistration.cpp:173-382), with the library's own atan2f,
+// cosf and sqrtf and no contraction into FMAs (the reference's order of
+// operations).  Used for the debug outputs, not in the registration loop.
+__global__ void __launch_bounds__(256)
+phase_volumes_kernel(const float2* __restrict__ q1, const float2* __restrict__ q2, int W, int H, int D, int axis,
+                     float* __restrict__ pd, float* __restrict__ cert, float* __restrict__ grad) {
+  const long long V = (long long)W * H * D;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V) return;
+  if (pd || cert) {
+    const float2 a = q1[i], c = q2[i];
+    const float re = __fadd_rn(__fmul_rn(a.x, c.x), __fmul_rn(a.y, c.y));
+    const float im = __fsub_rn(__fmul_rn(a.y, c.x), __fmul_rn(a.x, c.y));
+    const float d = atan2f(im, re);
+    if (pd) pd[i] = d;
+    if (cert) {
+      const float pr = __fsub_rn(__fmul_rn(a.x, c.x), __fmul_rn(a.y, c.y));
+      const float pi = __fadd_rn(__fmul_rn(a.y, c.x), __fmul_rn(a.x, c.y));
+      const float cc = cosf(__fmul_rn(d, 0.5f));
+      cert[i] = __fmul_rn(__fmul_rn(sqrtf(__fadd_rn(__fmul_rn(pr, pr), __fmul_rn(pi, pi))), cc), cc);
+    }
+  }
+  if (grad) {
+    const int x = (int)(i % W), y = (int)((i / W) % H), z = (int)(i / ((long long)W * H));
+    const int c = axis == 0 ? x : (axis == 1 ? y : z);
+    const int n = axis == 0 ? W : (axis == 1 ? H : D);
+    const long long step = axis == 0 ? 1 : (axis == 1 ? (long long)W : (long long)W * H);
+    if (c - 1 < 0 || c + 1 >= n) {
+      grad[i] = 0.f;
+      return;
+    }
+    float tr = 0.f, ti = 0.f;
+    const float2* qs[2] = {q1, q2};
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      const float2 p = qs[k][i + step], o = qs[k][i], m = qs[k][i - step];
+      tr = __fadd_rn(tr, __fadd_rn(__fmul_rn(p.x, o.x), __fmul_rn(p.y, o.y)));
+      ti = __fadd_rn(ti, __fsub_rn(__fmul_rn(p.y, o.x), __fmul_rn(p.x, o.y)));
+      tr = __fadd_rn(tr, __fadd_rn(__fmul_rn(o.x, m.x), __fmul_rn(o.y, m.y)));
+      ti = __fadd_rn(ti, __fsub_rn(__fmul_rn(o.y, m.x), __fmul_rn(o.x, m.y)));
+    }
+    grad[i] = atan2f(ti, tr);
+  }
+}
+
+cudaError_t phase_volumes(const float* q1, const float* q2, int W, int H, int D, int axis, float* pd, float* cert,
+                          float* grad, cudaStream_t st) {
+  const long long V = (long long)W * H * D;
+  if (V <= 0 || V > kMaxVoxels || axis < 0 || axis > 2) return cudaErrorInvalidValue;
+  phase_volumes_kernel<<<(unsigned)((V + 255) / 256), 256, 0, st>>>(reinterpret_cast<const float2*>(q1),
+                                                                   reinterpret_cast<const float2*>(q2), W, H, D,
+                                                                   axis, pd, cert, grad);
+  return cudaGetLastError();
+}
+
 cudaError_t phase_atan2_eval(const float* y, const float* x, float* out, long long n, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
   const long long nb = (n + 255) / 256;

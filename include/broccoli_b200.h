@@ -124,11 +124,19 @@ int brc_normal_equations(brc_ctx* ctx, const float* d_q1, long long q1_stride,
  * A call needs ceil((D-6)/zpb) x batch rows, zpb = max(1, 4096 /
  * ((W-6)(H-6))) interior slices per row (64x64x33: 27 rows per volume,
  * batch <= 113); larger requests return BRC_ERR_SCRATCH_LIMIT and do
- * nothing.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture.  All calls share the array: calls that overlap
- * on the GPU race and must be ordered by the caller.  No cudaMalloc,
- * cudaFree or allocating library routine is called. */
+ * nothing.  The stream must belong to the current device (BRC_ERR_INVALID
+ * otherwise).  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) with that device current and caches it;
+ * make that first call before any stream capture.  Under lazy module loading
+ * (the CUDA 12.2+ default) that lookup is also what allocates the array, so
+ * a process that gives its HBM to a pool should make a set-up call first:
+ * batch = 0 (other arguments ignored) only resolves the array on the current
+ * device and returns; BRC_ERR_NOMEM there means the device had no room left.
+ * CUDA_MODULE_LOADING=EAGER allocates it when the library loads instead.
+ * After cudaDeviceReset, repeat the set-up call before the next call.  All
+ * calls share the array: calls that overlap on the GPU race and must be
+ * ordered by the caller.  No cudaMalloc, cudaFree or allocating library
+ * routine is called. */
 #define BRC_NOALLOC_PARTIAL_ROWS 3072
 int brc_normal_equations_noalloc(void* cuda_stream, const float* d_q1, long long q1_stride,
                                  const float* d_q2, int W, int H, int D, int batch,
@@ -248,7 +256,8 @@ typedef struct {
   float esigma;        /* smoothing of A and h (voxels)                     */
   float dsigma;        /* smoothing of the field update (voxels)            */
   int precision;       /* BRC_PREC_FP32 / BRC_PREC_BF16X3 (filtering)        */
-  int solve_fp64;      /* 0: FP32 cofactors + 1e-16 (reference); 1: FP64    */
+  int solve_fp64;      /* 0: FP32 cofactors + 1e-16 (reference); 1: the same
+                          in FP64 (det + 1e-16 in double)                  */
 } brc_nonlinear_opts;
 
 /* Defaults of SetStartValues (broccoli_lib.cpp:325-355): sigmas 5,
@@ -411,12 +420,17 @@ typedef struct {
   float tsigma, esigma, dsigma;
   int precision;
   int solve_fp64;
+  int precenter;             /* PRECENTER_REGISTRATION: centre the input by its
+                                centre of mass at its own size first          */
 } brc_two_volume_opts;
 
 void brc_two_volume_opts_default(brc_two_volume_opts* opts);
 
-/* T1-to-template normalisation of one volume: resample onto the template
- * grid, match centres of mass, multi-scale affine registration, parameters
+/* T1-to-template normalisation of one volume: (with opts->precenter and a
+ * linear stage: the input centred twice by its centre of mass at its own
+ * size, as CenterVolumeMass is called twice at broccoli_lib.cpp:8003-8007;
+ * the centred input then replaces the input throughout) resample onto the
+ * template grid, match centres of mass, multi-scale affine registration, parameters
  * composed with the mass match (h_params12, host), multi-scale nonlinear
  * registration, affine motion added to the field, and one final warp of a
  * fresh resample by the combined field.  Output volumes are template size
@@ -453,6 +467,57 @@ int brc_register_cohort(brc_ctx* ctx, int n, const float* const* d_subjects, con
                         const float* h_tensors, const float* h_dirs, const brc_two_volume_opts* opts,
                         float* h_params12n, float* d_aligned_linear, float* d_aligned_nonlinear,
                         float* d_fields);
+
+/* ---- debug outputs, masks and parameter inversion ------------------------ */
+
+/* Host arrays the linear registration fills as the reference does with
+ * DEBUG set (broccoli_lib.cpp:5285-5289, :5349-5354): every call of
+ * brc_register_linear_batched (and so of the pyramid, motion-correction and
+ * T1-to-template entry points built on it) writes, for its last instance,
+ *   quadrature_responses[0..2]  the reference volume's three complex
+ *                               responses (interleaved re, im; W H D pairs),
+ *   phase_differences / phase_certainties / phase_gradients
+ *                               of iteration 0 along z: arg(q1 conj q2),
+ *                               |q1| |q2| cos^2(dphi/2) and the z phase
+ *                               gradient of the third filter pair (the
+ *                               first and last plane, which the reference
+ *                               leaves unwritten, are 0 here),
+ * so that after a pyramid the finest scale's values remain.  When all six
+ * quadrature_responses are set, brc_register_nonlinear also writes the six
+ * responses of its reference volume at the finest scale (the reads the
+ * reference keeps commented out at broccoli_lib.cpp:5754-5759).  Any
+ * pointer may be NULL.  Debug writes synchronise the stream and are refused
+ * (BRC_ERR_UNSUPPORTED) while the context's stream is being captured.
+ * outs = NULL turns them off.  No counterpart function in the reference: it
+ * replaces SetDebug plus the SetOutputQuadratureFilterResponses /
+ * SetOutputPhaseDifferences / Certainties / Gradients pointers
+ * (broccoli_lib.h:299-304). */
+typedef struct {
+  void* quadrature_responses[6];
+  float* phase_differences;
+  float* phase_certainties;
+  float* phase_gradients;
+} brc_debug_outputs;
+int brc_ctx_set_debug_outputs(brc_ctx* ctx, const brc_debug_outputs* outs);
+
+/* The reference's linear phase quantities of one pair of complex responses
+ * (one filter): d_phase_diff = arg(q1 conj q2), d_cert = |q1 q2| cos^2(
+ * dphi/2), d_grad = the phase gradient along `axis` (0 x, 1 y, 2 z; the
+ * first and last sample along the axis are 0).  Any output may be NULL.
+ * Replaces CalculatePhaseDifferencesAndCertainties and CalculatePhase-
+ * GradientsX/Y/Z (kernelRegistration.cpp:173-382). */
+int brc_phase_volumes(brc_ctx* ctx, const float* d_q1, const float* d_q2, int W, int H, int D, int axis,
+                      float* d_phase_diff, float* d_cert, float* d_grad);
+
+/* d_vols[t][i] *= d_mask[i] for T volumes of W x H x D, in place.  Replaces
+ * MultiplyVolumes (kernelMisc.cpp; the skull strip of
+ * PerformRegistrationTwoVolumesWrapper, broccoli_lib.cpp:8066-8105). */
+int brc_multiply_volumes(brc_ctx* ctx, float* d_vols, int W, int H, int D, int T, const float* d_mask);
+
+/* Inverse of a 12-parameter affine transform (4x4 inverse in double, result
+ * rounded to float).  Host only.  Replaces InvertAffineRegistrationParameters
+ * (broccoli_lib.cpp:7186-7250). */
+void brc_invert_affine_parameters(const float* h_params12, float* h_inverse12);
 
 /* ---- first-level preprocessing ----------------------------------------- */
 

@@ -28,6 +28,26 @@
  *   - SetAutoMask(true): PerformSmoothingNormalizedHostWrapper makes the
  *     certainty from the first fMRI volume (SegmentEPIData) and writes it
  *     to the SetInputCertainty array.
+ *   - SetDebug(true): the registrations fill the arrays of
+ *     SetOutputQuadratureFilterResponses (the reference volume's responses)
+ *     and SetOutputPhaseDifferences / Certainties / Gradients (iteration 0,
+ *     z axis), the last AlignTwoVolumesLinear call's values, as the reference
+ *     does (broccoli_lib.cpp:5285-5289, :5349-5354); the six-array form of
+ *     SetOutputQuadratureFilterResponses receives instead, after a nonlinear
+ *     registration, the six responses of its reference volume at the
+ *     finest scale (the reads the reference keeps commented out at
+ *     :5754-5759).  Gradient samples on the first and last z plane, which
+ *     the reference leaves unwritten, are 0.
+ *   - SetDoSkullstrip / SetDoSkullstripOriginal with SetInputMNIBrainMask
+ *     and SetOutputSkullstrippedT1Volume: PerformRegistrationTwoVolumesWrapper
+ *     multiplies the aligned volume by the mask, or the interpolated volume
+ *     by the mask carried back by the inverse affine transform (NEAREST), as
+ *     at broccoli_lib.cpp:8064-8105; a missing mask or output array is an
+ *     error (BRC_ERR_INVALID), not ignored.
+ *   - GetOpenCLCreateKernelErrors / GetOpenCLCreateBufferErrors: kernels are
+ *     compiled into the library, so no kernel is created at run time (all
+ *     zeros); element 0 of the buffer array holds BRC_ERR_NOMEM when a call
+ *     failed to allocate device memory.
  *   - Extensions (new setters): SetPrecision, SetMotionCorrectionTolerance,
  *     SetSolveFP64.
  */
@@ -81,6 +101,8 @@ class BROCCOLI_LIB {
   const char* GetOpenCLError();
   const char* GetOpenCLErrorMessage(int error);
   int* GetOpenCLRunKernelErrors();
+  int* GetOpenCLCreateKernelErrors();
+  int* GetOpenCLCreateBufferErrors();
 
   void SetWrapper(int wrapper);
   void SetVerbose(bool verbos);
@@ -116,6 +138,10 @@ class BROCCOLI_LIB {
   void SetInputMNIBrainVolume(float* input);
 
   // filters and algorithm settings
+  void SetPrecenterRegistration(bool center);
+  void SetDoSkullstrip(bool doskullstrip);
+  void SetDoSkullstripOriginal(bool doskullstriporiginal);
+  void SetInputMNIBrainMask(float* mask);
   void SetImageRegistrationFilterSize(int N);
   void SetLinearImageRegistrationFilters(float* qf1r, float* qf1i, float* qf2r, float* qf2i, float* qf3r,
                                          float* qf3i);
@@ -167,6 +193,12 @@ class BROCCOLI_LIB {
   void SetOutputDisplacementField(float* x, float* y, float* z);
   void SetOutputSmoothedfMRIVolumes(float* output);
   void SetOutputQuadratureFilterResponses(cl_float2* q1, cl_float2* q2, cl_float2* q3);
+  void SetOutputQuadratureFilterResponses(cl_float2* q1, cl_float2* q2, cl_float2* q3, cl_float2* q4,
+                                          cl_float2* q5, cl_float2* q6);
+  void SetOutputPhaseDifferences(float* pd);
+  void SetOutputPhaseCertainties(float* pc);
+  void SetOutputPhaseGradients(float* pg);
+  void SetOutputSkullstrippedT1Volume(float* skullstripped);
   void SetOutputEPIT1RegistrationParameters(float* output);
   void SetOutputEPIMNIRegistrationParameters(float* output);
   void SetOutputAlignedEPIVolumeT1(float* output);
@@ -211,8 +243,18 @@ class BROCCOLI_LIB {
   brc_ctx* ctx_ = nullptr;
   bool initiated_ = false;
   std::string init_error_;
+  std::string last_error_;  // message of the last failed call (GetOpenCLError)
   int last_status_ = BRC_OK;
   int run_errors_[200] = {0};
+  int create_kernel_errors_[200] = {0};
+  int create_buffer_errors_[200] = {0};
+  bool debug_ = false;
+  bool precenter_ = false, do_skullstrip_ = false, do_skullstrip_original_ = false;
+  float* h_mni_mask_ = nullptr;
+  float* out_skullstripped_ = nullptr;
+  float* out_pd_ = nullptr;
+  float* out_pc_ = nullptr;
+  float* out_pg_ = nullptr;
   int wrapper_ = BASH;
   bool verbose_ = false;
 
@@ -256,7 +298,7 @@ class BROCCOLI_LIB {
   float* h_epi_mask_ = nullptr;
   float* h_certainty_ = nullptr;
   bool auto_mask_ = false;
-  cl_float2* out_q_[3] = {nullptr};
+  cl_float2* out_q_[6] = {nullptr};
 
   int coarsest_epi_t1_ = 4;
   bool apply_mc_ = true, apply_smoothing_ = true, apply_slice_timing_ = false, preprocessing_only_ = false;
@@ -272,6 +314,7 @@ class BROCCOLI_LIB {
   float center_params_[12] = {0};
   bool t1_to_mni(const float* d_t1, float* d_out, const char* where);
   bool check(int status, const char* where);
+  bool apply_debug();
   bool pack_linear(float* bank3);
   bool pack_nonlinear(float* bank6, float* dirs18);
 };

@@ -35,3 +35,13 @@ int orc_num_threads(void) {
   return 1;
 #endif
 }
+
+/* Threads of the following OpenMP regions (the process's OpenMP runtime is
+ * shared with the reference-kernel build, so this also sets its count). */
+void orc_set_num_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+#else
+  (void)n;
+#endif
+}

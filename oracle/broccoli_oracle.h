@@ -128,6 +128,7 @@ ORC_DECLARE(float, _f32)
 ORC_DECLARE(double, _f64)
 
 int orc_num_threads(void);
+void orc_set_num_threads(int n);
 
 #ifdef __cplusplus
 }

@@ -79,6 +79,15 @@ def num_threads() -> int:
     return orc_lib().orc_num_threads()
 
 
+def set_num_threads(n: int) -> None:
+    """OpenMP threads of the oracle and of the reference-kernel build (one
+    OpenMP runtime per process)."""
+    fn = orc_lib().orc_set_num_threads
+    fn.argtypes = [_I]
+    fn.restype = None
+    fn(int(n))
+
+
 # --------------------------------------------------------------------------
 # restatement (liborc.so)
 # --------------------------------------------------------------------------
@@ -876,4 +885,52 @@ def first_level_preprocess(fmri, vs_epi, t1, vs_t1, mni, vs_mni, bank, lin_iter=
         vols = op.smooth(vols, mask, smoothing_filter_fwhm(smoothing_fwhm, vs_epi, 9, op.prec))
         out["smoothed"] = vols
     out["fmri"] = vols
+    return out
+
+
+# --------------------------------------------------------------------------
+# debug outputs and parameter inversion
+# --------------------------------------------------------------------------
+
+def phase_volumes(q1: np.ndarray, q2: np.ndarray, axis: int = 2, prec: str = "f32"):
+    """Phase difference, certainty and phase gradient along `axis` of one pair
+    of complex (D,H,W) responses (restatement; kernelRegistration.cpp:173-382),
+    zeros where the gradient kernels write nothing."""
+    dt, s = _dt(prec)
+    D, H, W = q1.shape
+    a = _interleave(q1, dt)
+    c = _interleave(q2, dt)
+    V = D * H * W
+    pd = np.zeros(V, dt)
+    cert = np.zeros(V, dt)
+    grad = np.zeros(V, dt)
+    fn = getattr(orc_lib(), "orc_phase_diff_cert" + s)
+    fn.argtypes = [_P, _P, _L, _P, _P]
+    fn(_ptr(a), _ptr(c), V, _ptr(pd), _ptr(cert))
+    fn = getattr(orc_lib(), "orc_phase_grad" + s)
+    fn.argtypes = [_P, _P, _I, _I, _I, _I, _P]
+    fn(_ptr(a), _ptr(c), int(axis), W, H, D, _ptr(grad))
+    return pd.reshape(D, H, W), cert.reshape(D, H, W), grad.reshape(D, H, W)
+
+
+def ref_phase_volumes(q1: np.ndarray, q2: np.ndarray, axis: int = 2):
+    """The same with the reference's kernels (zero-filled outputs)."""
+    D, H, W = q1.shape
+    a = _interleave(q1, np.float32)
+    c = _interleave(q2, np.float32)
+    out = [np.empty((D, H, W), np.float32) for _ in range(3)]
+    fn = ref_lib().ref_phase_volumes
+    fn.argtypes = [_P, _P, _I, _I, _I, _I, _P, _P, _P]
+    fn(_ptr(a), _ptr(c), W, H, D, int(axis), *(_ptr(o) for o in out))
+    return tuple(out)
+
+
+def ref_invert_affine(p12) -> np.ndarray:
+    """InvertAffineRegistrationParameters (broccoli_lib.cpp:7186-7250) with
+    the reference's Eigen."""
+    p = _arr(p12, np.float32)
+    out = np.zeros(12, np.float32)
+    fn = ref_lib().ref_invert_affine
+    fn.argtypes = [_P, _P]
+    fn(_ptr(p), _ptr(out))
     return out

@@ -177,6 +177,36 @@ void ref_add_affine(float* old12, const float* new12) {
   from_affine(T, old12);
 }
 
+// InvertAffineRegistrationParameters, broccoli_lib.cpp:7186-7250 (Eigen's
+// 4x4 inverse in double).
+void ref_invert_affine(const float* p12, float* inv12) {
+  Eigen::MatrixXd M = to_affine(p12, 1.0f);
+  Eigen::MatrixXd I = M.inverse();
+  from_affine(I, inv12);
+}
+
+// The DEBUG outputs of AlignTwoVolumesLinear (broccoli_lib.cpp:5315-5354)
+// for one filter pair: CalculatePhaseDifferencesAndCertainties and
+// CalculatePhaseGradientsX/Y/Z (kernelRegistration.cpp:173-382) into
+// zero-filled outputs (the gradient kernels leave the first and last sample
+// along the axis unwritten).
+void ref_phase_volumes(const float* q1, const float* q2, int W, int H, int D, int axis, float* pd,
+                       float* cert, float* grad) {
+  const long V = (long)W * H * D;
+  std::memset(pd, 0, sizeof(float) * V);
+  std::memset(cert, 0, sizeof(float) * V);
+  std::memset(grad, 0, sizeof(float) * V);
+  const float2* a = reinterpret_cast<const float2*>(q1);
+  const float2* c = reinterpret_cast<const float2*>(q2);
+  const int gx = roundup(W, 16), gy = roundup(H, 16);
+  ndrange(gx, gy, D, 16, 16, 1, [&] { clr::CalculatePhaseDifferencesAndCertainties(pd, cert, a, c, W, H, D); });
+  ndrange(gx, gy, D, 16, 16, 1, [&] {
+    if (axis == 0) clr::CalculatePhaseGradientsX(grad, a, c, W, H, D);
+    if (axis == 1) clr::CalculatePhaseGradientsY(grad, a, c, W, H, D);
+    if (axis == 2) clr::CalculatePhaseGradientsZ(grad, a, c, W, H, D);
+  });
+}
+
 // AddAffineRegistrationParametersNextScale, broccoli_lib.cpp:7344-7431.
 void ref_add_affine_next_scale(float* old12, const float* new12) {
   Eigen::MatrixXd T = to_affine(new12, 2.0f) * to_affine(old12, 2.0f);

@@ -1,9 +1,9 @@
 """Generates the golden fixtures of this directory from the reference itself.
 
-Run in a tree where the BROCCOLI sources are present (default
-/root/reference, override with BROCCOLI_REF):
+Run where the BROCCOLI sources are present, naming their root in
+BROCCOLI_REF (the directory holding code/ and filters/):
 
-    python tests/golden/make_golden.py
+    BROCCOLI_REF=/path/to/BROCCOLI python tests/golden/make_golden.py
 
 1. Copies the reference's shipped filter coefficients (``filters/*.bin``:
    quadrature filters, projection tensors, filter directions) into
@@ -36,10 +36,12 @@ import oracle as O  # noqa: E402
 from broccoli_b200 import filters as F  # noqa: E402
 from broccoli_b200 import synthetic as S  # noqa: E402
 
-REF = os.environ.get("BROCCOLI_REF", "/root/reference")
+REF = os.environ.get("BROCCOLI_REF", "")
 
 
 def main() -> None:
+    if not REF or not os.path.isdir(os.path.join(REF, "code", "Kernels")):
+        sys.exit("make_golden.py: set BROCCOLI_REF to the root of the BROCCOLI sources")
     src = os.path.join(REF, "filters")
     dst = os.path.join(HERE, "filters")
     os.makedirs(dst, exist_ok=True)

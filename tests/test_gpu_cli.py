@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 import torch
 
-from conftest import GOLDEN, ROOT
+from conftest import GOLDEN, ROOT, rel_err
 from broccoli_b200 import _lib as L
 from broccoli_b200 import nifti
 from broccoli_b200 import synthetic as S
@@ -105,7 +105,52 @@ def test_cli_errors(tmp_path):
     assert r.returncode != 0 and "Could not read" in r.stderr
     r = subprocess.run([os.path.join(BIN, "RegisterTwoVolumes"), bad, bad, "-mask", "m.nii"],
                        capture_output=True, text=True, timeout=60)
-    assert r.returncode != 0 and "not supported" in r.stderr
+    assert r.returncode != 0 and "Could not read" in r.stderr
+
+
+@pytest.mark.parametrize("maskopt", ["-mask", "-maskoriginal"])
+def test_register_two_volumes_cli_precenter_mask_debug(ctx, tmp_path, bank, maskopt):
+    """-precenter, -mask / -maskoriginal and -debug (RegisterTwoVolumes.cpp:
+    364-392, :410, :1088-1160, :1292-1318): the masked volume is the
+    library's aligned (or interpolated) volume times the (carried back)
+    mask, and the debug volumes are the template's responses."""
+    subj = S.head_phantom((22, 26, 24), seed=4).astype(np.float32)
+    tpl = np.ascontiguousarray(subj[1:-1, 2:-1, 1:-2])
+    mask = (tpl > 400).astype(np.float32)
+    vin, vtpl = (2.0, 2.0, 2.0), (2.2, 2.1, 2.3)
+    sp = os.path.join(tmp_path, "t1.nii")
+    tp = os.path.join(tmp_path, "template.nii")
+    mp = os.path.join(tmp_path, "mask.nii")
+    nifti.write(sp, subj, header_with_voxels(vin))
+    nifti.write(tp, tpl, header_with_voxels(vtpl))
+    nifti.write(mp, mask, header_with_voxels(vtpl))
+    run([os.path.join(BIN, "RegisterTwoVolumes"), sp, tp, "-filters", FILTERS, "-iterationslinear", "4",
+         "-iterationsnonlinear", "2", "-lowestscale", "2", "-sigma", "4.0", "-precenter", maskopt, mp, "-debug",
+         "-quiet"])
+    r = ctx.register_two_volumes(torch.from_numpy(subj).cuda(), vin, torch.from_numpy(tpl).cuda(), vtpl, bank,
+                                 4, 2, 2, 0, 4.0, 4.0, 4.0, precenter=True)
+    lin = nifti.read(os.path.join(tmp_path, "t1_aligned_linear.nii")).data
+    assert np.array_equal(lin, r["aligned_linear"].cpu().numpy())
+    masked = nifti.read(os.path.join(tmp_path, "t1_masked.nii")).data
+    m = torch.from_numpy(mask).cuda()
+    if maskopt == "-mask":
+        expect = r["aligned_nonlinear"] * m
+    else:
+        from broccoli_b200.api import Context
+        inv = Context.invert_affine_parameters(r["params"])
+        back = ctx.transform_volumes_linear(m, inv, 0)
+        expect = r["interpolated"] * back.reshape(m.shape)
+    assert np.array_equal(masked, expect.cpu().numpy())
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "..", "oracle"))
+    import oracle
+    qt = oracle.filter3d(tpl, bank["linear"])
+    for k in range(3):
+        re = nifti.read(os.path.join(tmp_path, f"t1_quadrature_filter_response_{k + 1}_real.nii")).data
+        im = nifti.read(os.path.join(tmp_path, f"t1_quadrature_filter_response_{k + 1}_imag.nii")).data
+        assert rel_err(re + 1j * im, qt[k]) < 1e-4
+    for n in ("phase_differences", "phase_certainties", "phase_gradients"):
+        assert os.path.exists(os.path.join(tmp_path, f"t1_{n}.nii"))
 
 
 @pytest.mark.parametrize("mode", ["ones", "mask", "automask"])
