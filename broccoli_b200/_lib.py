@@ -25,7 +25,7 @@ BRC_ERR_NONFINITE = -7
 BRC_ERR_SCRATCH_LIMIT = -8
 
 TRANSLATION, RIGID, AFFINE = 0, 1, 2
-PREC_FP32, PREC_BF16X3, PREC_FP32_GENERAL = 0, 1, 2
+PREC_FP32, PREC_BF16X3, PREC_FP32_GENERAL, PREC_TF32 = 0, 1, 2, 3
 INTERP_NEAREST, INTERP_LINEAR, INTERP_CUBIC = 0, 1, 2
 
 

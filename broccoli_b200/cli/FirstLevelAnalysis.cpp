@@ -38,7 +38,7 @@ static void usage() {
   printf(" -saveallaligned, -saveallpreprocessed, -saveall\n");
   printf(" -output                    Base name of the outputs\n");
   printf(" -filters                   Directory of the filter files (default $BROCCOLI_DIR/filters)\n");
-  printf(" -precision                 fp32 (default) or bf16x3 (tensor-core filtering)\n");
+  printf(" -precision                 fp32 (default), bf16x3 or tf32 (tensor-core filtering)\n");
   printf(" -quiet                     Print nothing\n");
   printf(" -verbose                   Print extra information\n\n");
 }
@@ -129,6 +129,8 @@ int main(int argc, char** argv) {
           precision = BRC_PREC_FP32;
         } else if (strcmp(v, "bf16x3") == 0) {
           precision = BRC_PREC_BF16X3;
+        } else if (strcmp(v, "tf32") == 0) {
+          precision = BRC_PREC_TF32;
         } else {
           fprintf(stderr, "Unknown precision %s\n", v);
           return EXIT_FAILURE;

@@ -25,7 +25,7 @@ static void usage() {
   printf(" -iterations         Iterations of the registration per volume (default 5)\n");
   printf(" -output             Output filename (default input_mc.nii)\n");
   printf(" -filters            Directory of the filter files (default $BROCCOLI_DIR/filters)\n");
-  printf(" -precision          fp32 (default) or bf16x3 (tensor-core filtering)\n");
+  printf(" -precision          fp32 (default), bf16x3 or tf32 (tensor-core filtering)\n");
   printf(" -tolerance          Stop a volume's iterations once its update is below this many voxels (default 0: off)\n");
   printf(" -quiet              Print nothing\n");
   printf(" -verbose            Print extra information\n\n");
@@ -63,6 +63,8 @@ int main(int argc, char** argv) {
           precision = BRC_PREC_FP32;
         } else if (strcmp(v, "bf16x3") == 0) {
           precision = BRC_PREC_BF16X3;
+        } else if (strcmp(v, "tf32") == 0) {
+          precision = BRC_PREC_TF32;
         } else {
           fprintf(stderr, "Unknown precision %s\n", v);
           return EXIT_FAILURE;

@@ -36,7 +36,7 @@ static void usage() {
   printf(" -saveinterpolated       Save the input resampled onto the reference grid, before alignment\n");
   printf(" -output                 Output base filename (default: the input's)\n");
   printf(" -filters                Directory of the filter files (default $BROCCOLI_DIR/filters)\n");
-  printf(" -precision              fp32 (default) or bf16x3 (tensor-core filtering)\n");
+  printf(" -precision              fp32 (default), bf16x3 or tf32 (tensor-core filtering)\n");
   printf(" -precenter              Centre the input volume by its centre of mass first (default off)\n");
   printf(" -mask                   Mask (reference size) applied after the registration, e.g. a skull strip\n");
   printf(" -maskoriginal           Mask applied to the interpolated, unregistered input through the inverse\n");
@@ -87,6 +87,8 @@ int main(int argc, char** argv) {
           precision = BRC_PREC_FP32;
         } else if (strcmp(v, "bf16x3") == 0) {
           precision = BRC_PREC_BF16X3;
+        } else if (strcmp(v, "tf32") == 0) {
+          precision = BRC_PREC_TF32;
         } else {
           fprintf(stderr, "Unknown precision %s\n", v);
           return EXIT_FAILURE;

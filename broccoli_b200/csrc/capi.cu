@@ -47,8 +47,9 @@ static bool bad_dims(int W, int H, int D) {
   return W <= 0 || H <= 0 || D <= 0 || (long long)W * H * D > (1ll << 31);
 }
 
-int brc_ctx::taps_for(const float* h_filters, int nfilt, const uint16_t** d_taps) {
-  const uint64_t key = fnv1a(h_filters, sizeof(float) * brc::kFilterFloats * (size_t)nfilt, 1469598103934665603ull ^ (uint64_t)nfilt);
+int brc_ctx::taps_for(const float* h_filters, int nfilt, bool tf32, const uint16_t** d_taps) {
+  const uint64_t key = fnv1a(h_filters, sizeof(float) * brc::kFilterFloats * (size_t)nfilt,
+                             1469598103934665603ull ^ (uint64_t)nfilt ^ (tf32 ? 0x100ull : 0ull));
   auto it = tc_taps.find(key);
   if (it == tc_taps.end()) {
     if (tc_taps.size() >= 16) {
@@ -56,7 +57,7 @@ int brc_ctx::taps_for(const float* h_filters, int nfilt, const uint16_t** d_taps
       tc_taps.clear();
     }
     std::vector<uint16_t> packed(brc::tc::packed_tap_bytes(nfilt) / 2);
-    brc::tc::pack_taps(h_filters, nfilt, packed.data());
+    brc::tc::pack_taps(h_filters, nfilt, packed.data(), tf32);
     std::unique_ptr<DevBuf> buf(new DevBuf());
     BRC_TRY(this, buf->ensure(packed.size() * 2), "alloc taps");
     BRC_TRY(this, cudaMemcpy(buf->ptr, packed.data(), packed.size() * 2, cudaMemcpyHostToDevice), "upload taps");
@@ -74,8 +75,8 @@ int brc_ctx::check_tc_err() {
   return fail(BRC_ERR_TIMEOUT, "a bounded wait of the tensor-core filtering kernel gave up");
 }
 
-int brc_ctx::tune_tc(int nfilt, int W, int H, int D, const uint16_t* d_taps, int* ty) {
-  const auto key = std::make_tuple(nfilt, W, H, D);
+int brc_ctx::tune_tc(int nfilt, int W, int H, int D, const uint16_t* d_taps, bool tf32, int* ty) {
+  const auto key = std::make_tuple(nfilt + (tf32 ? 100 : 0), W, H, D);
   auto it = tc_tuned.find(key);
   if (it != tc_tuned.end()) {
     *ty = it->second;
@@ -83,7 +84,7 @@ int brc_ctx::tune_tc(int nfilt, int W, int H, int D, const uint16_t* d_taps, int
   }
   int tys[3];
   const int n = brc::tc::candidate_tys(nfilt, H, D, tys, 3);
-  if (n <= 0) return fail(BRC_ERR_UNSUPPORTED, "volume shape not supported by the BF16X3 filtering");
+  if (n <= 0) return fail(BRC_ERR_UNSUPPORTED, "volume shape not supported by the tensor-core filtering");
   *ty = tys[0];
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   BRC_TRY(this, cudaStreamIsCapturing(stream(), &cap), "capture status");
@@ -113,7 +114,7 @@ int brc_ctx::tune_tc(int nfilt, int W, int H, int D, const uint16_t* d_taps, int
         err = cudaEventRecord(e0, own_stream);
         if (err == cudaSuccess)
           err = brc::tc::launch(tmp1.as<float>(), W, H, D, (int)nb, V, d_taps, nfilt, tmp2.as<float>(),
-                                brc::all_instances(), tc_err.as<int>(), g, own_stream);
+                                brc::all_instances(), tc_err.as<int>(), g, own_stream, tf32);
         if (err == cudaSuccess) err = cudaEventRecord(e1, own_stream);
         if (err == cudaSuccess) err = cudaEventSynchronize(e1);
         float ms = 0.f;
@@ -142,11 +143,13 @@ int make_filter_path(brc_ctx* ctx, const float* h_filters, int nfilt, int precis
   fp->d_taps = nullptr;
   fp->d_err = ctx->tc_err.as<int>();
   if (precision == BRC_PREC_FP32 || precision == BRC_PREC_FP32_GENERAL) return BRC_OK;
-  if (precision != BRC_PREC_BF16X3) return ctx->fail(BRC_ERR_UNSUPPORTED, "unknown precision");
-  int st = ctx->taps_for(h_filters, nfilt, &fp->d_taps);
+  if (precision != BRC_PREC_BF16X3 && precision != BRC_PREC_TF32)
+    return ctx->fail(BRC_ERR_UNSUPPORTED, "unknown precision");
+  const bool tf32 = precision == BRC_PREC_TF32;
+  int st = ctx->taps_for(h_filters, nfilt, tf32, &fp->d_taps);
   if (st != BRC_OK) return st;
   int ty = 0;
-  st = ctx->tune_tc(nfilt, W, H, D, fp->d_taps, &ty);
+  st = ctx->tune_tc(nfilt, W, H, D, fp->d_taps, tf32, &ty);
   if (st != BRC_OK) return st;
   fp->g = brc::tc::make_geometry(nfilt, H, D, ty);
   return BRC_OK;
@@ -154,8 +157,9 @@ int make_filter_path(brc_ctx* ctx, const float* h_filters, int nfilt, int precis
 
 cudaError_t run_filter(const FilterPath& fp, const float* vol, int W, int H, int D, int batch, long long stride,
                        float* out, brc::ActiveSet act, cudaStream_t st) {
-  if (fp.precision == BRC_PREC_BF16X3)
-    return brc::tc::launch(vol, W, H, D, batch, stride, fp.d_taps, fp.nfilt, out, act, fp.d_err, fp.g, st);
+  if (fp.precision == BRC_PREC_BF16X3 || fp.precision == BRC_PREC_TF32)
+    return brc::tc::launch(vol, W, H, D, batch, stride, fp.d_taps, fp.nfilt, out, act, fp.d_err, fp.g, st,
+                           fp.precision == BRC_PREC_TF32);
   return brc::filter3d_fp32(vol, W, H, D, batch, stride, fp.h_filters, fp.nfilt, out, act, st,
                             fp.precision == BRC_PREC_FP32);
 }
@@ -618,8 +622,7 @@ extern "C" int brc_register_linear_batched(brc_ctx* ctx, const float* d_ref, lon
   if (opts->iterations < 0 || opts->iterations > 10000 || opts->type < 0 || opts->type > 2 ||
       !(opts->tolerance >= 0.f))
     return ctx->fail(BRC_ERR_INVALID, "brc_register_linear_batched: bad options");
-  if (opts->precision != BRC_PREC_FP32 && opts->precision != BRC_PREC_FP32_GENERAL &&
-      opts->precision != BRC_PREC_BF16X3)
+  if (!brc_precision_valid(opts->precision))
     return ctx->fail(BRC_ERR_UNSUPPORTED, "brc_register_linear_batched: unknown precision");
   if (opts->certainty_sigma_x100 < 0)
     return ctx->fail(BRC_ERR_INVALID, "brc_register_linear_batched: negative certainty sigma");

@@ -106,13 +106,13 @@ struct brc_ctx {
   }
   // Device copy of the packed taps of a bank (uploaded on first use; call
   // outside stream capture).
-  int taps_for(const float* h_filters, int nfilt, const uint16_t** d_taps);
+  int taps_for(const float* h_filters, int nfilt, bool tf32, const uint16_t** d_taps);
   // Reads and clears the tensor-core wait flag (synchronises the device).
   int check_tc_err();
   // Tile height of the tensor-core filtering for a shape: the fastest of the
   // cost model's candidates, timed once per shape (outside stream capture;
   // under capture the cost model's first choice).
-  int tune_tc(int nfilt, int W, int H, int D, const uint16_t* d_taps, int* ty);
+  int tune_tc(int nfilt, int W, int H, int D, const uint16_t* d_taps, bool tf32, int* ty);
 
   size_t workspace() const {
     return q1.bytes + q2.bytes + aligned.bytes + partials.bytes + ctl.bytes + tmp1.bytes +
@@ -133,6 +133,9 @@ struct FilterPath {
 };
 int make_filter_path(brc_ctx* ctx, const float* h_filters, int nfilt, int precision, int W, int H, int D,
                      FilterPath* fp);
+inline bool brc_precision_valid(int p) {
+  return p == BRC_PREC_FP32 || p == BRC_PREC_FP32_GENERAL || p == BRC_PREC_BF16X3 || p == BRC_PREC_TF32;
+}
 // Kernels one run_filter call launches.
 inline int filter_launches(const FilterPath&) { return 1; }
 cudaError_t run_filter(const FilterPath& fp, const float* vol, int W, int H, int D, int batch, long long stride,

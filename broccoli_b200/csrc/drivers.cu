@@ -146,7 +146,7 @@ extern "C" int brc_register_nonlinear(brc_ctx* ctx, const float* d_ref, const fl
       W <= 0 || H <= 0 || D <= 0 || o->iterations < 0 || o->coarsest_scale < 1 ||
       !(o->tsigma > 0) || !(o->esigma > 0) || !(o->dsigma > 0))
     return ctx->fail(BRC_ERR_INVALID, "brc_register_nonlinear: bad argument");
-  if (o->precision != BRC_PREC_FP32 && o->precision != BRC_PREC_FP32_GENERAL && o->precision != BRC_PREC_BF16X3)
+  if (!brc_precision_valid(o->precision))
     return ctx->fail(BRC_ERR_UNSUPPORTED, "brc_register_nonlinear: unknown precision");
   if (d_aligned == d_moving)
     return ctx->fail(BRC_ERR_INVALID, "brc_register_nonlinear: d_aligned must not alias d_moving");

@@ -1,5 +1,6 @@
 // filter3d_tc.cu -- 7x7x7 complex filtering on the tcgen05 tensor cores in
-// BF16 split precision with FP32 accumulation (BRC_PREC_BF16X3).
+// BF16 split precision (BRC_PREC_BF16X3) or TF32 (BRC_PREC_TF32), with FP32
+// accumulation.
 //
 // The contraction q_f(z,y,x) = sum_{dz,dy,dx} F_f[3-dz][3-dy][3-dx] V(z+dz,
 // y+dy, x+dx) (NonseparableConvolution3D, broccoli_lib.cpp:4974-5027, true
@@ -27,6 +28,12 @@
 // rounding of x - x_hi), for the data and the taps; each GEMM is issued as
 // A_hi B_hi + A_hi B_lo + A_lo B_hi into the same FP32 TMEM accumulator
 // (relative error of a product ~2^-16; the dropped A_lo B_lo ~2^-18).
+// TF32: data and taps rounded to TF32 (10-bit mantissa, round to nearest,
+// ties away), one product per tap, as two K = 8 MMAs of kind::tf32 per GEMM
+// instead of three K = 16 BF16 ones (relative error of a product ~2^-10).
+// The 16 K samples of a row then sit in four 4-sample 16-byte quarters
+// where the BF16 form keeps a hi and a lo part of two 8-sample halves: the
+// same bytes and the same descriptor strides.
 //
 // One persistent CTA per SM walks the tiles of the launch (10 x positions x
 // Ty rows x SP*J planes of one volume each) with its warps specialised:
@@ -201,6 +208,24 @@ __device__ __forceinline__ void decode_tile(const TileArgs& a, const ActiveSet& 
   b = active_instance(act, li);
 }
 
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+  const uint32_t z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
+      "}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+__device__ __forceinline__ uint32_t tf32_rna(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+template <bool TF32>
 __global__ void __launch_bounds__(kThreads, 1)
 filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ taps, float* __restrict__ out,
                    const TileArgs a, const Geometry g, const ActiveSet act, int* __restrict__ err) {
@@ -305,18 +330,27 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
             v[e] = (rowok && xg >= 0 && xg < a.W) ? __ldg(rp + xg) : 0.f;
           }
         }
-        uint32_t ph4[4], pl4[4];
+        const uint32_t rowoff = (uint32_t)(par * g.RP + qq * g.Hp + yl) * 16u;
+        if (TF32) {
+          // quarters 2 kh and 2 kh + 1 (samples 0-3 and 4-7 of this half)
+          uint8_t* q0 = hi + (uint32_t)(2 * kh) * rowbytes + rowoff;
+          *reinterpret_cast<uint4*>(q0) = make_uint4(tf32_rna(v[0]), tf32_rna(v[1]), tf32_rna(v[2]), tf32_rna(v[3]));
+          *reinterpret_cast<uint4*>(q0 + rowbytes) =
+              make_uint4(tf32_rna(v[4]), tf32_rna(v[5]), tf32_rna(v[6]), tf32_rna(v[7]));
+        } else {
+          uint32_t ph4[4], pl4[4];
 #pragma unroll
-        for (int e = 0; e < 8; e += 2) {
-          const __nv_bfloat16 h0 = __float2bfloat16_rn(v[e]), h1 = __float2bfloat16_rn(v[e + 1]);
-          const __nv_bfloat16 l0 = __float2bfloat16_rn(v[e] - __bfloat162float(h0));
-          const __nv_bfloat16 l1 = __float2bfloat16_rn(v[e + 1] - __bfloat162float(h1));
-          ph4[e / 2] = pack_bf16(h0, h1);
-          pl4[e / 2] = pack_bf16(l0, l1);
+          for (int e = 0; e < 8; e += 2) {
+            const __nv_bfloat16 h0 = __float2bfloat16_rn(v[e]), h1 = __float2bfloat16_rn(v[e + 1]);
+            const __nv_bfloat16 l0 = __float2bfloat16_rn(v[e] - __bfloat162float(h0));
+            const __nv_bfloat16 l1 = __float2bfloat16_rn(v[e + 1] - __bfloat162float(h1));
+            ph4[e / 2] = pack_bf16(h0, h1);
+            pl4[e / 2] = pack_bf16(l0, l1);
+          }
+          const uint32_t off = (uint32_t)kh * rowbytes + rowoff;
+          *reinterpret_cast<uint4*>(hi + off) = make_uint4(ph4[0], ph4[1], ph4[2], ph4[3]);
+          *reinterpret_cast<uint4*>(lo + off) = make_uint4(pl4[0], pl4[1], pl4[2], pl4[3]);
         }
-        const uint32_t off = (uint32_t)kh * rowbytes + (uint32_t)(par * g.RP + qq * g.Hp + yl) * 16u;
-        *reinterpret_cast<uint4*>(hi + off) = make_uint4(ph4[0], ph4[1], ph4[2], ph4[3]);
-        *reinterpret_cast<uint4*>(lo + off) = make_uint4(pl4[0], pl4[1], pl4[2], pl4[3]);
       }
       // the GEMMs read the buffer through the async proxy
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -329,7 +363,9 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
     // offsets to their start-address fields (one 16-byte row = 1), so that
     // the issuing thread spends its time in tcgen05.mma, not in address
     // arithmetic (which delays every GEMM it precedes).
-    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(g.N >> 3) << 17) |
+    // D F32; A, B BF16 (1) or TF32 (2); K-major; N, M
+    const uint32_t ab = TF32 ? 2u : 1u;
+    const uint32_t idesc = (1u << 4) | (ab << 7) | (ab << 10) | ((uint32_t)(g.N >> 3) << 17) |
                            ((uint32_t)(kM >> 4) << 24);
     const uint64_t da0 = sdesc(smem_u32(ring), kM * 16, 128);  // slot 0, hi taps
     const uint64_t db0 = sdesc(smem_u32(inb), rowbytes, 128);  // buffer 0, hi part, row 0
@@ -371,15 +407,26 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
             break;
           }
           const uint64_t b1 = bh0 + offa[m] + (uint64_t)dyq;
-          mma_bf16(dcol, ah, b1, idesc, accf);
-          mma_bf16(dcol, ah, b1 + dblo, idesc, 1u);
-          mma_bf16(dcol, ah + dalo, b1, idesc, 1u);
+          if (TF32) {
+            // K samples 0-7 (quarters 0, 1), then 8-15 (quarters 2, 3)
+            mma_tf32(dcol, ah, b1, idesc, accf);
+            mma_tf32(dcol, ah + dalo, b1 + dblo, idesc, 1u);
+          } else {
+            mma_bf16(dcol, ah, b1, idesc, accf);
+            mma_bf16(dcol, ah, b1 + dblo, idesc, 1u);
+            mma_bf16(dcol, ah + dalo, b1, idesc, 1u);
+          }
           accf = 1u;
           if (m < 3 || last_pair) {
             const uint64_t b2 = bh0 + offb[m] + (uint64_t)dyq, a2 = ah + dstage;
-            mma_bf16(dcol, a2, b2, idesc, 1u);
-            mma_bf16(dcol, a2, b2 + dblo, idesc, 1u);
-            mma_bf16(dcol, a2 + dalo, b2, idesc, 1u);
+            if (TF32) {
+              mma_tf32(dcol, a2, b2, idesc, 1u);
+              mma_tf32(dcol, a2 + dalo, b2 + dblo, idesc, 1u);
+            } else {
+              mma_bf16(dcol, a2, b2, idesc, 1u);
+              mma_bf16(dcol, a2, b2 + dblo, idesc, 1u);
+              mma_bf16(dcol, a2 + dalo, b2, idesc, 1u);
+            }
           }
           mma_commit(&tempty[slot]);
           G++;
@@ -572,11 +619,20 @@ size_t packed_tap_bytes(int nfilt) {
   return (size_t)kSlotsPerTile * kSlotBytes;
 }
 
+static uint32_t tf32_rna_host(float f) {
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u) return u & 0xffffe000u;  // inf / nan
+  return (u + 0x1000u) & 0xffffe000u;  // nearest, ties away from zero
+}
+
 // Stage (input-plane offset c = cq - 3, dy = dyq - 3) goes to ring slot
 // dyq * 4 + cq / 2, half cq % 2; each half is hi (kM x 16 BF16) then lo, as
-// two K-major 8-row x 16-byte core-matrix blocks.  Halves without a stage
-// (cq = 7 with one stacked plane) stay zero.
-void pack_taps(const float* h_filters, int nfilt, uint16_t* dst) {
+// two K-major 8-row x 16-byte core-matrix blocks, or (tf32) four K quarters
+// of kM x 4 TF32 values, each a K-major block of 8-row x 16-byte core
+// matrices.  Halves without a stage (cq = 7 with one stacked plane) stay
+// zero.
+void pack_taps(const float* h_filters, int nfilt, uint16_t* dst, bool tf32) {
   const int SP = stacked_planes(nfilt);
   const int ncq = 6 + SP;
   memset(dst, 0, packed_tap_bytes(nfilt));
@@ -605,11 +661,17 @@ void pack_taps(const float* h_filters, int nfilt, uint16_t* dst) {
         for (int kx = xo; kx <= xo + 6; kx++) {
           const int dx = kx - 3 - xo;
           const float w = F[(3 - dz) * 49 + (3 - dy) * 7 + (3 - dx)];
-          const uint16_t wh = bf16_rn(w);
-          const uint16_t wl = bf16_rn(w - bf16_to_f(wh));
-          const size_t e = (size_t)(kx / 8) * (kM * 8) + (size_t)r * 8 + (kx % 8);
-          hi[e] = wh;
-          lo[e] = wl;
+          if (tf32) {
+            const uint32_t t = tf32_rna_host(w);
+            const size_t e = (size_t)(kx / 4) * (kM * 4) + (size_t)r * 4 + (kx % 4);
+            memcpy(hi + 2 * e, &t, 4);
+          } else {
+            const uint16_t wh = bf16_rn(w);
+            const uint16_t wl = bf16_rn(w - bf16_to_f(wh));
+            const size_t e = (size_t)(kx / 8) * (kM * 8) + (size_t)r * 8 + (kx % 8);
+            hi[e] = wh;
+            lo[e] = wl;
+          }
         }
       }
     }
@@ -699,7 +761,10 @@ cudaError_t bounded_wait_probe(int wait_ms, int* d_err, cudaStream_t st) {
 }
 
 cudaError_t init() {
-  cudaError_t e = cudaFuncSetAttribute(filter3d_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  cudaError_t e = cudaFuncSetAttribute(filter3d_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       227 * 1024);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(filter3d_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
   if (e != cudaSuccess) return e;
   int dev = 0;
   if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
@@ -707,7 +772,7 @@ cudaError_t init() {
 }
 
 cudaError_t launch(const float* vol, int W, int H, int D, int batch, long long stride, const uint16_t* d_taps,
-                   int nfilt, float* out, ActiveSet act, int* d_err, const Geometry& g, cudaStream_t st) {
+                   int nfilt, float* out, ActiveSet act, int* d_err, const Geometry& g, cudaStream_t st, bool tf32) {
   if (g_num_sms <= 0) return cudaErrorInitializationError;
   if (!geometry_ok(g) || (nfilt != 3 && nfilt != 6) || g.SP != stacked_planes(nfilt) || batch <= 0)
     return cudaErrorInvalidValue;
@@ -729,7 +794,10 @@ cudaError_t launch(const float* vol, int W, int H, int D, int batch, long long s
   a.e_off = a.in_off + 128u * (uint32_t)g.NR;
   a.bar_off = a.e_off + (uint32_t)kEpiBytes;
   const int grid = ntiles < g_num_sms ? (int)ntiles : g_num_sms;
-  filter3d_tc_kernel<<<grid, kThreads, g.smem, st>>>(vol, d_taps, out, a, g, act, d_err);
+  if (tf32)
+    filter3d_tc_kernel<true><<<grid, kThreads, g.smem, st>>>(vol, d_taps, out, a, g, act, d_err);
+  else
+    filter3d_tc_kernel<false><<<grid, kThreads, g.smem, st>>>(vol, d_taps, out, a, g, act, d_err);
   return cudaGetLastError();
 }
 

@@ -1,5 +1,5 @@
-// filter3d_tc.h -- host interface of the tcgen05 split-BF16 filtering kernel
-// (filter3d_tc.cu).
+// filter3d_tc.h -- host interface of the tcgen05 filtering kernel (split
+// BF16 or TF32; filter3d_tc.cu).
 #pragma once
 #include <cuda_runtime.h>
 #include <stddef.h>
@@ -31,11 +31,11 @@ struct Geometry {
 
 int stacked_planes(int nfilt);
 int num_stages(int nfilt);
-// Bytes of the packed split-BF16 Toeplitz taps of a bank of nfilt (3 or 6)
-// complex filters, and the packing itself (dst holds packed_tap_bytes/2
-// 16-bit words).
+// Bytes of the packed Toeplitz taps (split BF16, or TF32: the same size) of
+// a bank of nfilt (3 or 6) complex filters, and the packing itself (dst
+// holds packed_tap_bytes/2 16-bit words).
 size_t packed_tap_bytes(int nfilt);
-void pack_taps(const float* h_filters, int nfilt, uint16_t* dst);
+void pack_taps(const float* h_filters, int nfilt, uint16_t* dst, bool tf32);
 Geometry make_geometry(int nfilt, int H, int D, int Ty);
 bool geometry_ok(const Geometry& g);
 // The max_n cheapest tile heights by the cost model, cheapest first; returns
@@ -46,7 +46,8 @@ cudaError_t init();
 // One CTA waits wait_ms (1..1000) on a barrier nothing completes, then sets *d_err.
 cudaError_t bounded_wait_probe(int wait_ms, int* d_err, cudaStream_t st);
 cudaError_t launch(const float* vol, int W, int H, int D, int batch, long long stride, const uint16_t* d_taps,
-                   int nfilt, float* out, ActiveSet act, int* d_err, const Geometry& g, cudaStream_t st);
+                   int nfilt, float* out, ActiveSet act, int* d_err, const Geometry& g, cudaStream_t st,
+                   bool tf32);
 
 }  // namespace tc
 }  // namespace brc

@@ -83,7 +83,7 @@ extern "C" int brc_tensor_magnitude(brc_ctx* ctx, const float* d_vol, int W, int
   if (!ctx) return BRC_ERR_INVALID;
   if (!d_vol || !h_filters6 || !h_tensors || !d_out || bad_size(W, H, D))
     return ctx->fail(BRC_ERR_INVALID, "brc_tensor_magnitude: bad argument");
-  if (precision != BRC_PREC_FP32 && precision != BRC_PREC_FP32_GENERAL && precision != BRC_PREC_BF16X3)
+  if (!brc_precision_valid(precision))
     return ctx->fail(BRC_ERR_UNSUPPORTED, "brc_tensor_magnitude: unknown precision");
   cudaSetDevice(ctx->device);
   cudaStream_t st = ctx->stream();

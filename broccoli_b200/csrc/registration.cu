@@ -824,110 +824,237 @@ struct Taps9 {
 // The three separable 9-tap passes in one kernel: y over (vol * cert), then
 // x, then z, divided by the smoothed certainty (SeparableConvolutionRows /
 // Columns / Rods, kernelConvolution.cpp:52-91, :531-569, :1201-1240, zero
-// padding).  A block owns a 32 x 8 column tile and marches along z through
-// a chunk of planes: per plane it stages the 40 x 16 input window (tile
-// plus 4-voxel halo) in shared memory, runs the y and x passes there, and
-// keeps the last nine xy results of its column in registers for the z
-// pass.  Each output is the same sequence of float operations as three
-// separate passes (terms o = -4..4 in order, out-of-volume terms 0), and
-// the volume is read from HBM once and written once instead of three times
-// each way.  `out` must not overlap the inputs.
-constexpr int kSmTX = 32, kSmTY = 8, kSmZC = 32;
+// padding).  Each output is the same sequence of terms as three separate
+// passes (o = -4..4 in order, out-of-volume terms 0), and the volume is read
+// from HBM once and written once.
+//
+// A block owns a 56 x 16 column tile and marches along z through a chunk of
+// planes.  Per plane, the 64 x 24 input window (tile plus 4-voxel halo) is
+// copied into shared memory with cp.async (zero-filled outside the volume)
+// into a four-stage ring, three planes ahead of its use; with an even W the
+// copies move 8-byte pairs (a pair never straddles the volume's edge), and a
+// thread's copies lie in one window column, so its addresses advance by a
+// constant.  Every thread then computes four y outputs of one window column
+// (12 shared loads, 36 FMAs), and 224 of the 256 threads four consecutive x
+// outputs of one tile row (three 16-byte shared loads, 36 FMAs), which enter
+// a nine-plane register ring; the z pass (36 FMAs) writes the output plane
+// to shared memory, from which all threads store it coalesced in the next
+// phase.  The ring slot of a plane is its index modulo 9, dispatched by a
+// switch over nine copies of the z pass so that every register index is a
+// constant.  The y pass of plane k, the x and z passes of plane k - 1 and
+// the stores of plane k - 2 run in the same phase (the y results and the
+// output plane are double-buffered), so one barrier per plane separates
+// every producer from its consumer.  With a certainty, its window is copied
+// beside the volume's and the product is formed in the y pass.  `out` must
+// not overlap the inputs.
+constexpr int kSmTX = 56, kSmTY = 16;            // output tile
+constexpr int kSmWX = kSmTX + 8, kSmWY = kSmTY + 8;  // input window 64 x 24
+constexpr int kSmPitch = 68;                     // shared row pitch (floats, 16-byte rows)
+constexpr int kSmThreads = 256;
+constexpr int kSmXQ = kSmTX / 4;                 // 14 quads of x outputs per row
+constexpr int kSmOwners = kSmXQ * kSmTY;         // 224 threads own outputs
+constexpr int kSmStages = 4;                     // window ring (planes in flight + 1)
+constexpr int kSmWin = kSmWY * kSmPitch;         // floats per window stage
+constexpr int kSmYBuf = kSmTY * kSmPitch;        // floats per y-result buffer
+constexpr int kSmOut = kSmTY * kSmTX;            // floats per output plane
+static_assert(kSmWX == 64 && kSmTY == 16, "mappings assume 64 window columns and 16 tile rows");
 
-template <bool CERT>
-__global__ void __launch_bounds__(256)
+inline size_t smooth_smem_bytes(bool cert) {
+  return sizeof(float) * ((size_t)(cert ? 2 : 1) * kSmStages * kSmWin + 2 * kSmYBuf + 2 * kSmOut);
+}
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async(uint32_t dst, const float* src, uint32_t n) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(dst), "l"(src), "n"(BYTES), "r"(n)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// VEC: floats per copy (2 needs an even W and 8-byte aligned volumes); DIV:
+// divide by the smoothed certainty scert; ACC: add into `out`.
+template <bool CERT, int VEC, bool DIV, bool ACC>
+__global__ void __launch_bounds__(kSmThreads, 3)
 smooth3d_kernel(const float* __restrict__ in, long long in_stride, const float* __restrict__ cert,
-                const float* __restrict__ scert, int W, int H, int D, Taps9 tx, Taps9 ty, Taps9 tz,
-                float* __restrict__ out, long long out_stride, int accumulate) {
-  __shared__ float s_in[kSmTY + 8][kSmTX + 9];
-  __shared__ float s_y[kSmTY][kSmTX + 9];
-  const int tid = threadIdx.x, lx = tid & 31, ly = tid >> 5;
+                const float* __restrict__ scert, int W, int H, int D, int zc, Taps9 tx, Taps9 ty, Taps9 tz,
+                float* __restrict__ out, long long out_stride) {
+  extern __shared__ __align__(16) float smem[];
+  float* s_in = smem;                                       // kSmStages windows (+ certainty windows)
+  float* s_y = smem + (CERT ? 2 : 1) * kSmStages * kSmWin;  // 2 y-result buffers
+  float* s_o = s_y + 2 * kSmYBuf;                           // 2 output planes
+  const int tid = threadIdx.x;
   const int ntx = (W + kSmTX - 1) / kSmTX;
   const int x0 = (int)(blockIdx.x % ntx) * kSmTX, y0 = (int)(blockIdx.x / ntx) * kSmTY;
-  const int z0 = blockIdx.y * kSmZC, z1 = min(D, z0 + kSmZC);
+  const int z0 = blockIdx.y * zc, z1 = min(D, z0 + zc);
+  const int np = z1 - z0 + 8;  // planes z0 - 4 .. z1 + 3
   const long long WH = (long long)W * H;
   const float* src = in + (long long)blockIdx.z * in_stride;
-  const int x = x0 + lx, y = y0 + ly;
-  float ring[9];
+
+  // copies: window column wc (VEC wide), rows wr0 + RS m for m < NC
+  constexpr int CPR = kSmWX / VEC;            // copies per window row
+  constexpr int RS = kSmThreads / CPR;        // row step between a thread's copies
+  constexpr int NC = kSmWY / RS;              // copies per thread
+  static_assert(NC * RS == kSmWY, "window rows / thread mismatch");
+  const int wc = (tid % CPR) * VEC, wr0 = tid / CPR;
+  const int gx = x0 - 4 + wc;
+  const bool xin = gx >= 0 && gx < W;  // with VEC 2 and W even, gx + 1 < W too
+  unsigned rowmask = 0;
 #pragma unroll
-  for (int k = 0; k < 9; k++) ring[k] = 0.f;
-  // the thread's (up to) three elements of the 16 x 40 window: their window
-  // positions and in-plane offsets (-1: outside the volume)
-  constexpr int kWin = (kSmTY + 8) * (kSmTX + 8);
-  int woff[3];
-  long long goff[3];
-#pragma unroll
-  for (int k = 0; k < 3; k++) {
-    const int e = tid + 256 * k;
-    const int r = e / (kSmTX + 8), c = e - r * (kSmTX + 8);
-    const int gx = x0 - 4 + c, gy = y0 - 4 + r;
-    woff[k] = e < kWin ? r * (kSmTX + 9) + c : -1;
-    goff[k] = (e < kWin && gx >= 0 && gx < W && gy >= 0 && gy < H) ? (long long)gy * W + gx : -1;
+  for (int m = 0; m < NC; m++) {
+    const int gy = y0 - 4 + wr0 + RS * m;
+    if (xin && gy >= 0 && gy < H) rowmask |= 1u << m;
   }
-  // the next plane's elements are loaded while the current plane is
-  // smoothed
-  float pre[3];
-  auto load = [&](int q) {
-    const bool qin = q >= 0 && q < D;
-    const long long base = (long long)q * WH;
+  // in-plane offset of copy 0 (outside the volume when its row is; only
+  // copies of rows inside the volume use it)
+  const long long off0 = (long long)(y0 - 4 + wr0) * W + gx;
+  const long long rstep = (long long)RS * W;
+  const uint32_t sdst0 = static_cast<uint32_t>(__cvta_generic_to_shared(s_in)) + 4u * (wr0 * kSmPitch + wc);
+  auto issue = [&](int k) {
+    const int p = z0 - 4 + k;
+    const bool pin = p >= 0 && p < D;
+    const unsigned mask = pin ? rowmask : 0u;
+    const long long poff = (long long)(pin ? p : 0) * WH;
+    const uint32_t d = sdst0 + 4u * (uint32_t)(((unsigned)k % kSmStages) * kSmWin);
 #pragma unroll
-    for (int k = 0; k < 3; k++) {
-      float v = 0.f;
-      if (qin && goff[k] >= 0) {
-        v = __ldg(src + base + goff[k]);
-        if (CERT) v *= __ldg(cert + base + goff[k]);
-      }
-      pre[k] = v;
+    for (int m = 0; m < NC; m++) {
+      const bool v = (mask >> m) & 1u;
+      // copies outside the volume read nothing (size 0) from the volume's start
+      const long long o = v ? poff + off0 + m * rstep : 0;
+      cp_async<4 * VEC>(d + 4u * (uint32_t)(RS * m * kSmPitch), src + o, v ? 4u * VEC : 0u);
+      if (CERT) cp_async<4 * VEC>(d + 4u * (uint32_t)(kSmStages * kSmWin + RS * m * kSmPitch), cert + o,
+                                   v ? 4u * VEC : 0u);
     }
+    cp_async_commit();
   };
-  // y-pass outputs of this thread: the tile column above it, and for the
-  // first 64 threads one of the 8 halo columns of a row (4 on each side)
-  const int hr = tid >> 3, hk = tid & 7, hc = hk < 4 ? hk : hk + kSmTX;
-  const bool halo = tid < 8 * kSmTY;
-  const bool hin = x0 - 4 + hc >= 0 && x0 - 4 + hc < W;
-  load(z0 - 4);
-  for (int p = z0 - 4; p < z1 + 4; p++) {
-    float xy = 0.f;
-    if (p >= 0 && p < D) {  // uniform over the block
+  // y pass: window column yc, tile rows 4 yg .. 4 yg + 3
+  const int yc = tid & 63, yg = tid >> 6;
+  auto ypass = [&](int k) {
+    const float* w = s_in + ((unsigned)k % kSmStages) * kSmWin + (4 * yg) * kSmPitch + yc;
+    float* yb = s_y + (k & 1) * kSmYBuf + (4 * yg) * kSmPitch + yc;
+    float a[12];
 #pragma unroll
-      for (int k = 0; k < 3; k++)
-        if (woff[k] >= 0) (&s_in[0][0])[woff[k]] = pre[k];
-      __syncthreads();
-      load(p + 1);
-      // y pass on the tile rows, over the tile columns plus the x halo
-      // (0 outside the volume: the x pass pads with zeros)
-      {
-        float sum = 0.f;
-#pragma unroll
-        for (int o = -4; o <= 4; o++) sum += s_in[ly + 4 + o][lx + 4] * ty.f[4 - o];
-        s_y[ly][lx + 4] = x < W ? sum : 0.f;
-      }
-      if (halo) {
-        float sum = 0.f;
-#pragma unroll
-        for (int o = -4; o <= 4; o++) sum += s_in[hr + 4 + o][hc] * ty.f[4 - o];
-        s_y[hr][hc] = hin ? sum : 0.f;
-      }
-      __syncthreads();
-#pragma unroll
-      for (int o = -4; o <= 4; o++) xy += s_y[ly][lx + 4 + o] * tx.f[4 - o];
-    } else {
-      load(p + 1);
+    for (int i = 0; i < 12; i++) {
+      a[i] = w[i * kSmPitch];
+      if (CERT) a[i] *= w[kSmStages * kSmWin + i * kSmPitch];
     }
 #pragma unroll
-    for (int k = 0; k < 8; k++) ring[k] = ring[k + 1];
-    ring[8] = xy;  // plane p; ring[4] is plane p - 4
-    const int z = p - 4;
-    if (z >= z0 && x < W && y < H) {
+    for (int i = 0; i < 4; i++) {
       float sum = 0.f;
 #pragma unroll
-      for (int o = -4; o <= 4; o++) sum += ring[4 + o] * tz.f[4 - o];
-      const long long i = (long long)z * WH + (long long)y * W + x;
-      if (scert != nullptr) sum = sum / __ldg(scert + i);
-      float* o = out + (long long)blockIdx.z * out_stride + i;
-      *o = accumulate ? *o + sum : sum;
+      for (int o = -4; o <= 4; o++) sum += a[i + 4 + o] * ty.f[4 - o];
+      yb[i * kSmPitch] = sum;
     }
+  };
+  // x and z passes: tile row xr, outputs x0 + 4 xq .. + 3
+  const bool owner = tid < kSmOwners;
+  const int xr = tid / kSmXQ, xq = tid - (tid / kSmXQ) * kSmXQ;
+  float ring[9][4];
+#pragma unroll
+  for (int u = 0; u < 9; u++)
+#pragma unroll
+    for (int i = 0; i < 4; i++) ring[u][i] = 0.f;
+  // stores: tile row sr = tid / 16, columns sc + 16 i (i < 4, < 56)
+  const int sr = tid >> 4, sc = tid & 15;
+  unsigned colmask = 0;
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+    if (sc + 16 * i < kSmTX && x0 + sc + 16 * i < W) colmask |= 1u << i;
+  if (y0 + sr >= H) colmask = 0;
+  float* dst_row = out + (long long)blockIdx.z * out_stride + (long long)(y0 + sr) * W + x0 + sc;
+  const float* scert_row = DIV ? scert + (long long)(y0 + sr) * W + x0 + sc : nullptr;
+  auto store = [&](int j) {
+    const long long zoff = (long long)(z0 + j - 8) * WH;
+    const float* so = s_o + (j & 1) * kSmOut + sr * kSmTX + sc;
+    float* o = dst_row + zoff;
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+      if ((colmask >> i) & 1u) {
+        float q = so[16 * i];
+        if (DIV) q = q / __ldg(scert_row + zoff + 16 * i);
+        o[16 * i] = ACC ? o[16 * i] + q : q;
+      }
+  };
+
+  // planes 0 .. kSmStages - 2 in flight; plane 0 complete and visible
+#pragma unroll
+  for (int k = 0; k < kSmStages - 1; k++) {
+    if (k < np) issue(k);
+    else cp_async_commit();
   }
+  cp_async_wait<kSmStages - 2>();
+  __syncthreads();
+  // phase k: copies of plane k + 3 issued, y pass of plane k, x and z passes
+  // of plane k - 1 (ring slot (k - 1) % 9), stores of plane k - 2; then plane
+  // k + 1 complete and visible
+  int slot = 0;
+  for (int k = 0; k <= np + 1; k++) {
+    if (k + kSmStages - 1 < np) issue(k + kSmStages - 1);
+    else cp_async_commit();
+    if (k < np) ypass(k);
+    if (k >= 1 && k <= np) {
+      if (owner) {
+        const int j = k - 1;
+        const float4* r4 = reinterpret_cast<const float4*>(s_y + (j & 1) * kSmYBuf + xr * kSmPitch + 4 * xq);
+        const float4 f0 = r4[0], f1 = r4[1], f2 = r4[2];
+        const float a[12] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, f1.z, f1.w, f2.x, f2.y, f2.z, f2.w};
+        float v[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          float sum = 0.f;
+#pragma unroll
+          for (int o = -4; o <= 4; o++) sum += a[i + 4 + o] * tx.f[4 - o];
+          v[i] = sum;
+        }
+        float4* od = reinterpret_cast<float4*>(s_o + (j & 1) * kSmOut + xr * kSmTX + 4 * xq);
+        // slot S holds plane j; the output plane z0 + j - 8 sums planes
+        // j - 8 .. j, held in slots S + 1 .. S + 9 (mod 9), oldest first
+#define BRC_SMOOTH_Z(S)                                                              \
+  case S: {                                                                          \
+    _Pragma("unroll") for (int i = 0; i < 4; i++) ring[S][i] = v[i];                 \
+    if (j >= 8) {                                                                    \
+      float zs[4];                                                                   \
+      _Pragma("unroll") for (int i = 0; i < 4; i++) {                                \
+        float sum = 0.f;                                                             \
+        _Pragma("unroll") for (int jj = 0; jj < 9; jj++) sum += ring[(S + 1 + jj) % 9][i] * tz.f[8 - jj]; \
+        zs[i] = sum;                                                                 \
+      }                                                                              \
+      *od = make_float4(zs[0], zs[1], zs[2], zs[3]);                                 \
+    }                                                                                \
+  } break;
+        switch (slot) {
+          BRC_SMOOTH_Z(0)
+          BRC_SMOOTH_Z(1)
+          BRC_SMOOTH_Z(2)
+          BRC_SMOOTH_Z(3)
+          BRC_SMOOTH_Z(4)
+          BRC_SMOOTH_Z(5)
+          BRC_SMOOTH_Z(6)
+          BRC_SMOOTH_Z(7)
+          BRC_SMOOTH_Z(8)
+        }
+#undef BRC_SMOOTH_Z
+      }
+      slot = slot == 8 ? 0 : slot + 1;
+    }
+    if (k >= 10) store(k - 2);
+    cp_async_wait<kSmStages - 2>();
+    __syncthreads();
+  }
+  cp_async_wait<0>();
+}
+
+// Planes per z chunk of smooth3d_kernel: enough chunks that the grid fills
+// the 148 SMs about six blocks deep, at least 16 planes per chunk.
+static int smooth_chunk(int D, long long tiles_x_batch) {
+  const long long want = 148LL * 6;
+  long long chunks = (want + tiles_x_batch - 1) / tiles_x_batch;
+  const long long maxc = (D + 15) / 16;
+  if (chunks > maxc) chunks = maxc;
+  if (chunks < 1) chunks = 1;
+  return (int)((D + chunks - 1) / chunks);
 }
 
 // ---------------------------------------------------------------------------
@@ -1119,6 +1246,21 @@ cudaError_t multiply_mask(float* vols, const float* mask, long long V, int batch
   return cudaGetLastError();
 }
 
+// smooth3d_kernel instantiations indexed by (cert << 3) | (pairs << 2) |
+// (divide << 1) | accumulate.
+static const void* smooth_kernel_of(int v) {
+#define BRC_SK(C, P, Q, A) reinterpret_cast<const void*>(smooth3d_kernel<C, (P) ? 2 : 1, Q, A>)
+  static const void* const table[16] = {
+      BRC_SK(false, false, false, false), BRC_SK(false, false, false, true), BRC_SK(false, false, true, false),
+      BRC_SK(false, false, true, true),   BRC_SK(false, true, false, false), BRC_SK(false, true, false, true),
+      BRC_SK(false, true, true, false),   BRC_SK(false, true, true, true),   BRC_SK(true, false, false, false),
+      BRC_SK(true, false, false, true),   BRC_SK(true, false, true, false),  BRC_SK(true, false, true, true),
+      BRC_SK(true, true, false, false),   BRC_SK(true, true, false, true),   BRC_SK(true, true, true, false),
+      BRC_SK(true, true, true, true)};
+#undef BRC_SK
+  return table[v];
+}
+
 cudaError_t smooth3d(const float* vol, int W, int H, int D, int batch, const float* fx,
                      const float* fy, const float* fz, const float* cert, const float* scert,
                      float* tmp1, float* tmp2, float* out, cudaStream_t st, int accumulate) {
@@ -1140,14 +1282,33 @@ cudaError_t smooth3d(const float* vol, int W, int H, int D, int batch, const flo
                      overlaps(scert, sizeof(float) * (size_t)V);
   float* dst = alias ? tmp1 : out;
   const long long ntiles = (long long)((W + kSmTX - 1) / kSmTX) * ((H + kSmTY - 1) / kSmTY);
-  if (ntiles > 0x7fffffffLL || batch > 65535) return cudaErrorInvalidValue;
-  const dim3 grid((unsigned)ntiles, (unsigned)((D + kSmZC - 1) / kSmZC), (unsigned)batch);
-  if (cert)
-    smooth3d_kernel<true><<<grid, 256, 0, st>>>(vol, V, cert, scert, W, H, D, tx, ty, tz, dst, V,
-                                                alias ? 0 : accumulate);
-  else
-    smooth3d_kernel<false><<<grid, 256, 0, st>>>(vol, V, nullptr, scert, W, H, D, tx, ty, tz, dst, V,
-                                                 alias ? 0 : accumulate);
+  if (ntiles > 0x7fffffffLL || batch > 65535 || V > kMaxVoxels) return cudaErrorInvalidValue;
+  const int zc = smooth_chunk(D, ntiles * batch);
+  const dim3 grid((unsigned)ntiles, (unsigned)((D + zc - 1) / zc), (unsigned)batch);
+  // the dynamic shared memory above 48 KB is a per-device function attribute
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  // 8-byte copies need an even W (pairs never straddle the edge) and 8-byte
+  // aligned volumes
+  const bool pairs = (W & 1) == 0 && ((reinterpret_cast<uintptr_t>(vol) | reinterpret_cast<uintptr_t>(cert)) & 7) == 0;
+  const bool acc = !alias && accumulate != 0;
+  const int variant = (cert ? 8 : 0) | (pairs ? 4 : 0) | (scert ? 2 : 0) | (acc ? 1 : 0);
+  if (!attr_set[dev]) {
+    for (int v = 0; v < 16; v++) {
+      const cudaError_t e0 = cudaFuncSetAttribute(smooth_kernel_of(v), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)smooth_smem_bytes((v & 8) != 0));
+      if (e0 != cudaSuccess) return e0;
+    }
+    attr_set[dev] = true;
+  }
+  void* args[] = {(void*)&vol, (void*)&V, (void*)&cert, (void*)&scert, (void*)&W, (void*)&H, (void*)&D, (void*)&zc,
+                  (void*)&tx, (void*)&ty, (void*)&tz, (void*)&dst, (void*)&V};
+  {
+    const cudaError_t e0 = cudaLaunchKernel(smooth_kernel_of(variant), grid, dim3(kSmThreads), args,
+                                            smooth_smem_bytes(cert != nullptr), st);
+    if (e0 != cudaSuccess) return e0;
+  }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || !alias) return e;
   if (accumulate) return add_volumes(out, out, tmp1, V * batch, st);

@@ -19,7 +19,7 @@ Bars
   FP32 parity (the reference's 1e-4 relative):
     parameters  max |p - p_oracle| <= 1e-4 * max(1, max |p_oracle|)
     volumes and displacement fields  max |v - v_oracle| <= 1e-4 * max |v_oracle|
-  mixed precision (BF16X3 filtering, FP64 solves) against the FP64 oracle:
+  mixed precision (BF16X3 or TF32 filtering, FP64 solves) against the FP64 oracle:
     RMS displacement error <= 0.05 voxel (affine: over all voxels of the
     grid; nonlinear: RMS over voxels of the length of the difference of the
     combined affine + nonlinear displacement fields)
@@ -75,11 +75,12 @@ def test_affine_64x64x33_fp32_matches_oracle(ctx, orc, bank, affine_case, which)
     assert S.rms_displacement_error(p, truth, base.shape) < 0.2 * err0
 
 
+@pytest.mark.parametrize("prec", [L.PREC_BF16X3, L.PREC_TF32], ids=["bf16x3", "tf32"])
 @pytest.mark.parametrize("which", ["shipped", "lognormal"])
-def test_affine_64x64x33_bf16x3_vs_fp64_oracle(ctx, orc, bank, affine_case, which):
+def test_affine_64x64x33_mixed_vs_fp64_oracle(ctx, orc, bank, affine_case, which, prec):
     base, moved, _ = affine_case
     flt = bank["linear"] if which == "shipped" else F.linear_registration_filters()
-    r = ctx.register_linear(cuda(base), cuda(moved)[None], flt, 20, L.AFFINE, precision=L.PREC_BF16X3)
+    r = ctx.register_linear(cuda(base), cuda(moved)[None], flt, 20, L.AFFINE, precision=prec)
     p = r["params"].cpu().numpy()[0]
     p64, _, _ = orc.align_linear(base, moved, flt, 20, orc.AFFINE, prec="f64")
     assert S.rms_displacement_error(p, p64, base.shape) < RMS_BAR
@@ -106,14 +107,15 @@ def test_motion_batch_64x64x33_fp32_matches_oracle(ctx, orc, series8, cert_sigma
         assert rel_err(al[i], a32) < TOL, i
 
 
-def test_motion_batch_64x64x33_workload_vs_fp64_oracle(ctx, orc, series8):
-    """The timed workload's form (BF16X3 filtering, certainty smoothing
+@pytest.mark.parametrize("prec", [L.PREC_BF16X3, L.PREC_TF32], ids=["bf16x3", "tf32"])
+def test_motion_batch_64x64x33_workload_vs_fp64_oracle(ctx, orc, series8, prec):
+    """The timed workload's form (tensor-core filtering, certainty smoothing
     sigma 1, early exit at 1e-3 voxel) against the FP64 oracle running all
     20 iterations."""
     flt = F.linear_registration_filters()
     vols = series8
     r = ctx.register_linear(cuda(vols[0]), cuda(vols[1:]), flt, 20, L.RIGID, tolerance=1e-3,
-                            precision=L.PREC_BF16X3, certainty_sigma=1.0)
+                            precision=prec, certainty_sigma=1.0)
     got = r["params"].cpu().numpy()
     for i in range(vols.shape[0] - 1):
         p64, _, _ = orc.align_linear(vols[0], vols[i + 1], flt, 20, orc.RIGID, prec="f64", cert_sigma=1.0)
@@ -146,11 +148,12 @@ def test_t1_to_template_half_size_fp32_matches_oracle(ctx, bank, t1_half, t1_hal
         assert rel_err(r[k].cpu().numpy(), o[k]) < TOL, k
 
 
-def test_t1_to_template_half_size_mixed_vs_fp64_oracle(ctx, bank, t1_half, t1_half_oracle):
+@pytest.mark.parametrize("prec", [L.PREC_BF16X3, L.PREC_TF32], ids=["bf16x3", "tf32"])
+def test_t1_to_template_half_size_mixed_vs_fp64_oracle(ctx, bank, t1_half, t1_half_oracle, prec):
     sub, tpl = t1_half
     two = (2.0, 2.0, 2.0)
     o = t1_half_oracle["f64"]
-    r = ctx.register_two_volumes(cuda(sub), two, cuda(tpl), two, bank, 10, 10, 8, precision=L.PREC_BF16X3,
+    r = ctx.register_two_volumes(cuda(sub), two, cuda(tpl), two, bank, 10, 10, 8, precision=prec,
                                  solve_fp64=True)
     f = r["field"].cpu().numpy()
     assert field_rms(f, o["field"]) < RMS_BAR
