@@ -359,7 +359,8 @@ def normalisation_rates(ctx, L, prec, sampler, accuracy_on: bool, reps: int = 5)
     sizes U{160..256} (seeds 300 + i, crops of one 256^3 phantom), both onto a
     182 x 218 x 182 1-mm template phantom.  Filters: the reference's shipped
     linear and nonlinear banks (tests/golden/filters).  The mixed-precision
-    form (BF16X3 filtering, FP64 per-voxel 3x3 solves, FP64 12x12 solves) and
+    form (tensor-core filtering in the timed precision, TF32 or BF16X3, FP64
+    per-voxel 3x3 solves, FP64 12x12 solves) and
     the plain FP32 form (FP32 filtering, the reference's FP32 cofactor
     solves); medians of `reps` runs; the cohort also one subject at a time in
     plain FP32."""
@@ -374,7 +375,8 @@ def normalisation_rates(ctx, L, prec, sampler, accuracy_on: bool, reps: int = 5)
                                    np.float32)
     subj = torch.from_numpy(subj_np).cuda()
     one = (1.0, 1.0, 1.0)
-    mixed = prec == L.PREC_BF16X3
+    mixed = prec in (L.PREC_BF16X3, L.PREC_TF32)
+    pname = {L.PREC_BF16X3: "bf16x3", L.PREC_TF32: "tf32"}.get(prec, "fp32")
     forms = [("mixed" if mixed else "fp32", prec, mixed)] + ([("fp32", L.PREC_FP32, False)] if mixed else [])
 
     def two(p, fp64):
@@ -396,7 +398,7 @@ def normalisation_rates(ctx, L, prec, sampler, accuracy_on: bool, reps: int = 5)
             ms += [cuda_ms(lambda: two(p, fp64)) for _ in range(reps - 1)]
         med = float(np.median(ms))
         t1[name] = clocked({"value": 1000.0 / med, "unit": "subjects/s", "ms_per_subject": med,
-                            "runs_ms": [float(v) for v in ms], "precision": "bf16x3 + fp64 solves" if fp64 else
+                            "runs_ms": [float(v) for v in ms], "precision": pname + " + fp64 solves" if fp64 else
                             "fp32"}, sampler, "t1_" + name, med)
 
     big = S.head_phantom((256, 256, 256), seed=3)
@@ -416,7 +418,7 @@ def normalisation_rates(ctx, L, prec, sampler, accuracy_on: bool, reps: int = 5)
             ms = [cuda_ms(run) for _ in range(reps)]
         med = float(np.median(ms))
         coh[name] = clocked({"value": 64 * 1000.0 / med, "unit": "subjects/s", "ms": med,
-                             "runs_ms": [float(v) for v in ms], "precision": "bf16x3 + fp64 solves" if fp64 else
+                             "runs_ms": [float(v) for v in ms], "precision": pname + " + fp64 solves" if fp64 else
                              "fp32"}, sampler, "cohort_" + name, med)
 
     def serial():
@@ -506,7 +508,7 @@ def run_gpu(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     ctx = Context(local_rank)
     flt = filters()
-    prec = L.PREC_BF16X3 if args.precision == "bf16x3" else L.PREC_FP32
+    prec = {"bf16x3": L.PREC_BF16X3, "tf32": L.PREC_TF32}.get(args.precision, L.PREC_FP32)
     vols, truth = make_series(rank)
     D, H, W = SHAPE
     V = D * H * W
@@ -626,14 +628,18 @@ def run_gpu(args, rank, world, local_rank):
     with Section(sampler, "serial"):
         serial_rate = n_serial / (cuda_ms(serial, st) / 1000.0)
 
-    # ---- the same batched step with FP32 filtering (when timing BF16X3) ----
-    fp32_batched = None
-    if prec != L.PREC_FP32:
-        with Section(sampler, "fp32_batched"):
+    # ---- the same batched step with the other filtering precisions ----
+    other_arms = {}
+    for name, p2 in (("fp32_batched", L.PREC_FP32), ("bf16x3_batched", L.PREC_BF16X3), ("tf32_batched", L.PREC_TF32)):
+        if p2 == prec:
+            continue
+        with Section(sampler, name):
             for _ in range(2):
-                step(L.PREC_FP32)
-            _, b_times = timed_steps(lambda: step(L.PREC_FP32), args.steps)
-        fp32_batched = (T - 1) * args.steps / (float(np.sum(b_times)) / 1000.0)
+                step(p2)
+            o2, b_times = timed_steps(lambda: step(p2), args.steps)
+        other_arms[name] = {"value": (T - 1) * args.steps / (float(np.sum(b_times)) / 1000.0), "unit": UNIT,
+                            "mean_iterations": float(o2["iterations"].float().mean()),
+                            "sample": f"the same batched step with {name.split('_')[0].upper()} filtering"}
 
     # ---- dominant kernel alone: 7^3 filtering of the 199 moving volumes
     # (inputs 107 MB + responses 640 MB per launch, larger than L2) ----
@@ -653,7 +659,8 @@ def run_gpu(args, rank, world, local_rank):
 
     with Section(sampler, "filter"):
         f_ms = time_filter(prec)
-        f32_ms = time_filter(L.PREC_FP32) if prec != L.PREC_FP32 else f_ms
+        filter_ms = {n: (time_filter(p2) if p2 != prec else f_ms)
+                     for n, p2 in (("fp32", L.PREC_FP32), ("bf16x3", L.PREC_BF16X3), ("tf32", L.PREC_TF32))}
     ctx.synchronize()
     del q
     f_flop = FLOP_PER_VOXEL_FILTER * 3 * V * (T - 1)
@@ -693,25 +700,37 @@ def run_gpu(args, rank, world, local_rank):
     # is below the algorithmic bytes: the input comes partly from L2 (written
     # by the preceding resampling) and part of the output is still in L2
     # when the kernel ends.
-    tc_bytes_per_vol = (17850368 + 48461056) / 63
+    tc_bytes_per_vol = ((34571776 + 150313472) if prec == L.PREC_TF32 else (17850368 + 48461056)) / 63
     sym_bytes_per_vol = (34094848 + 147386624) / 63
     traffic = sym_bytes_per_vol * (T - 1) if symmetric_bank(fl) and tuple(SHAPE) == (33, 64, 64) else None
     tc_traffic = tc_bytes_per_vol * (T - 1) if tuple(SHAPE) == (33, 64, 64) else None
     achieved = f_flop / (f_ms / 1000.0) / 1e12
-    if prec == L.PREC_BF16X3:
-        tc_peak = peaks.get("bf16_tflops", 1590.0)
-        roofline = {"kernel": "filter3d_tc_kernel (tcgen05.mma kind::f16, split BF16 x3, FP32 accumulate in TMEM)",
-                    "bound": "tensor", "achieved": achieved, "peak": tc_peak, "unit": "TFLOP/s",
-                    "frac": achieved / tc_peak,
-                    "peak_source": ("MEASURED_PEAKS.json bf16_tflops (burst, measured)" if "bf16_tflops" in peaks
-                                    else "fallback 1.59 PFLOP/s"),
-                    "flop_per_launch": f_flop,
-                    "flop_note": "algorithmic: 1,372 FLOP per voxel per complex filter (343 taps x 2 real MACs "
-                                 "x 2) x 3 filters x the voxels of the 199 volumes; the three split products and "
-                                 "the banded-Toeplitz zeros the GEMMs also issue are not counted",
-                    "split_products": {"achieved": 3 * achieved, "frac": 3 * achieved / tc_peak,
+    bf16_peak = peaks.get("bf16_tflops", 1590.0)
+    peak_src = "MEASURED_PEAKS.json bf16_tflops (burst, measured)" if "bf16_tflops" in peaks else "fallback 1.59 PFLOP/s"
+    alg_note = ("algorithmic: 1,372 FLOP per voxel per complex filter (343 taps x 2 real MACs x 2) x 3 filters x the "
+                "voxels of the 199 volumes; the split products and the banded-Toeplitz, row and halo padding the "
+                "GEMMs also issue are not counted")
+    if prec == L.PREC_TF32:
+        tf32_peak = bf16_peak / 2.0
+        roofline = {"kernel": "filter3d_tc_kernel<TF32> (tcgen05.mma kind::tf32, FP32 accumulate in TMEM)",
+                    "bound": "tensor", "achieved": achieved, "peak": tf32_peak, "unit": "TFLOP/s",
+                    "frac": achieved / tf32_peak,
+                    "peak_source": peak_src + " / 2: the dense kind::tf32 rate is half the kind::f16 rate",
+                    "frac_of_bf16_peak": achieved / bf16_peak,
+                    "flop_per_launch": f_flop, "flop_note": alg_note, "launch_ms": f_ms,
+                    "filter_launch_ms": filter_ms, "traffic": tc_traffic,
+                    "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on 63 "
+                                    "volumes, scaled by the volume count; algorithmic: 4 B in + 24 B out "
+                                    "per voxel"}
+    elif prec == L.PREC_BF16X3:
+        roofline = {"kernel": "filter3d_tc_kernel<BF16X3> (tcgen05.mma kind::f16, split BF16 x3, FP32 accumulate "
+                              "in TMEM)",
+                    "bound": "tensor", "achieved": achieved, "peak": bf16_peak, "unit": "TFLOP/s",
+                    "frac": achieved / bf16_peak, "peak_source": peak_src,
+                    "flop_per_launch": f_flop, "flop_note": alg_note,
+                    "split_products": {"achieved": 3 * achieved, "frac": 3 * achieved / bf16_peak,
                                        "note": "the 3 BF16 products per tap the split form executes"},
-                    "launch_ms": f_ms, "fp32_filter_launch_ms": f32_ms, "traffic": tc_traffic,
+                    "launch_ms": f_ms, "filter_launch_ms": filter_ms, "traffic": tc_traffic,
                     "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on 63 "
                                     "volumes, scaled by the volume count; algorithmic: 4 B in + 24 B out "
                                     "per voxel"}
@@ -723,7 +742,7 @@ def run_gpu(args, rank, world, local_rank):
                     "frac": achieved / fp32_peak,
                     "peak_source": "nominal FP32 FMA rate 148 SMs x 128 lanes x 2 at the sampled max SM clock "
                                    "(MEASURED_PEAKS.json has no FP32 figure)",
-                    "flop_per_launch": f_flop, "launch_ms": f_ms, "traffic": traffic}
+                    "flop_per_launch": f_flop, "launch_ms": f_ms, "filter_launch_ms": filter_ms, "traffic": traffic}
     acc = (accuracy(vols, truth, out["params"].cpu().numpy(), flt, cert_sigma=cs)
            if not args.skip_accuracy else None)
     cpu = cpu_baseline_protocol(vols, flt) if not args.skip_cpu else None
@@ -731,7 +750,8 @@ def run_gpu(args, rank, world, local_rank):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3" if prec == L.PREC_BF16X3 else "f32",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": {L.PREC_BF16X3: "bf16x3", L.PREC_TF32: "tf32"}.get(prec, "f32"),
         "data": "synthetic",
         "config": workload_config(world, {"mean_iterations": float(iters_used.mean()),
                                           "precision": args.precision}, cert_sigma=cs),
@@ -748,8 +768,7 @@ def run_gpu(args, rank, world, local_rank):
                               "sample": f"{n_serial} volumes of the series registered one at a time "
                                         "(batch 1, eager launches)",
                               "batched_over_serial": value / serial_rate},
-        "fp32_batched": ({"value": fp32_batched, "unit": UNIT,
-                          "sample": "the same batched step with FP32 filtering"} if fp32_batched else None),
+        "other_precisions": other_arms,
         "clocks": clocks,
         "clocks_all_sections": sampler.summary() if sampler else None,
         "cpu_baseline": cpu,
@@ -772,8 +791,9 @@ def main():
                     help="skip the single FP32 affine registration and the differentiable objective "
                          "(configs 0 and 3)")
     ap.add_argument("--series", type=int, default=T, help="series length (volumes)")
-    ap.add_argument("--precision", default="bf16x3", choices=["fp32", "bf16x3"],
-                    help="filtering precision of the timed path (bf16x3: tensor-core split BF16)")
+    ap.add_argument("--precision", default="tf32", choices=["fp32", "bf16x3", "tf32"],
+                    help="filtering precision of the timed path (tf32: tensor-core TF32; bf16x3: tensor-core "
+                         "split BF16)")
     ap.add_argument("--certainty-sigma", type=float, default=1.0,
                     help="sigma (voxels) of the 3x3x3 certainty smoothing; 0 = off")
     ap.add_argument("--only-steps", action="store_true",
