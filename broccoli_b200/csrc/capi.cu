@@ -688,7 +688,7 @@ extern "C" int brc_register_linear_batched(brc_ctx* ctx, const float* d_ref, lon
     auto itg = ctx->graphs.find(key);
     GraphEntry* ge = nullptr;
     if (itg == ctx->graphs.end()) {
-      if (ctx->graphs.size() >= 16) ctx->graphs.clear();
+      if (ctx->graphs.size() >= 64) ctx->graphs.clear();  // a bounded cache of instantiated graphs
       std::unique_ptr<GraphEntry> ne(new GraphEntry());
       cudaStream_t cs = ctx->own_stream;
       BRC_TRY(ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "begin capture");

@@ -64,6 +64,10 @@ struct brc_ctx {
   std::string last_error;
   unsigned long long launches = 0;
   DevBuf q1, q2, aligned, partials, ctl, tmp1, tmp2, series, corrected, params, rot, nl, pyr;
+  // working volumes of the T1-to-template and cohort drivers, kept across
+  // calls so that their addresses (and the captured graphs keyed by them)
+  // stay the same from one call to the next
+  DevBuf r2v_work, r2v_lin, r2v_prm, coh_res, coh_mat, coh_lin, coh_prm, coh_jobs;
   std::map<GraphKey, std::unique_ptr<GraphEntry>> graphs;
   // packed split-BF16 taps of the tensor-core filtering, per filter bank
   // (key: hash of the bank and its size); graphs may hold these pointers,
@@ -116,7 +120,9 @@ struct brc_ctx {
 
   size_t workspace() const {
     return q1.bytes + q2.bytes + aligned.bytes + partials.bytes + ctl.bytes + tmp1.bytes +
-           tmp2.bytes + series.bytes + corrected.bytes + params.bytes + rot.bytes + nl.bytes + pyr.bytes;
+           tmp2.bytes + series.bytes + corrected.bytes + params.bytes + rot.bytes + nl.bytes + pyr.bytes +
+           r2v_work.bytes + r2v_lin.bytes + r2v_prm.bytes + coh_res.bytes + coh_mat.bytes + coh_lin.bytes +
+           coh_prm.bytes + coh_jobs.bytes;
   }
 };
 

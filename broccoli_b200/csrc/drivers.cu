@@ -35,41 +35,46 @@ int myround(float a) { return (int)floorf(a + 0.5f); }
 
 }  // namespace
 
-// One nonlinear update from given responses: T, its smoothing, norm and
-// max, A and h, their smoothing, the per-voxel solve, the smoothing of the
-// update and its addition into the field (AlignTwoVolumesNonLinear loop
-// body, broccoli_lib.cpp:5784-6025).
-static int nonlinear_step(brc_ctx* ctx, const float* q1, const float* q2, int W, int H, int D,
+// One nonlinear update of G instances from given responses (q1, the
+// reference's, shared; q2 6 complex volumes per instance): T, its
+// smoothing, norm and max, A and h, their smoothing, the per-voxel solve,
+// the smoothing of the update and its addition into the fields (3 volumes
+// per instance) -- the AlignTwoVolumesNonLinear loop body,
+// broccoli_lib.cpp:5784-6025, every launch covering all G instances.
+static int nonlinear_step(brc_ctx* ctx, const float* q1, const float* q2, int G, int W, int H, int D,
                           const float* m36, const float* dirs18, const float* ft, const float* fe,
                           const float* fd, int fp64, float* field) {
   const long long V = (long long)W * H * D;
   cudaStream_t st = ctx->stream();
-  float* t6 = ctx->nl.as<float>();
-  float* ah = t6 + 6 * V;  // a6 then h3, contiguous (9 volumes)
-  float* d3 = ah + 9 * V;
-  unsigned int* maxbits = reinterpret_cast<unsigned int*>(d3 + 3 * V);
-  // the unsmoothed T and A, h go to tmp2, so every smoothing writes a
-  // buffer it does not read
+  float* t6 = ctx->nl.as<float>();        // [G][6][V] smoothed T
+  float* ah = t6 + 6 * V * G;             // [G][9][V] smoothed a6 then h3
+  float* d3 = ah + 9 * V * G;             // [G][3][V] update
+  unsigned int* maxbits = reinterpret_cast<unsigned int*>(d3 + 3 * V * G);  // G words
+  // the unsmoothed T ([G][6][V]) and then A, h ([G][9][V]) go to tmp2, so
+  // every smoothing writes a buffer it does not read
   float* raw = ctx->tmp2.as<float>();
-  BRC_TRY(ctx, brc::tensor_components(q2, V, m36, raw, st), "tensor_components");
-  BRC_TRY(ctx, brc::smooth3d(raw, W, H, D, 6, ft, ft, ft, nullptr, nullptr, ctx->tmp1.as<float>(), nullptr, t6, st),
+  BRC_TRY(ctx, brc::tensor_components(q2, V, m36, raw, st, G), "tensor_components");
+  BRC_TRY(ctx, brc::smooth3d(raw, W, H, D, 6 * G, ft, ft, ft, nullptr, nullptr, ctx->tmp1.as<float>(), nullptr, t6,
+                             st),
           "smooth T");
-  BRC_TRY(ctx, brc::tensor_norm_max(t6, V, raw, maxbits, st), "tensor_norm_max");
-  BRC_TRY(ctx, brc::nonlinear_ah(q1, q2, t6, V, maxbits, m36, dirs18, raw, raw + 6 * V, st), "nonlinear_ah");
-  BRC_TRY(ctx, brc::smooth3d(raw, W, H, D, 9, fe, fe, fe, nullptr, nullptr, ctx->tmp1.as<float>(), nullptr, ah, st),
+  BRC_TRY(ctx, brc::tensor_norm_max(t6, V, raw, maxbits, st, G, 6 * V, 9 * V), "tensor_norm_max");
+  BRC_TRY(ctx, brc::nonlinear_ah(q1, q2, t6, V, maxbits, m36, dirs18, raw, raw + 6 * V, st, G, 9 * V),
+          "nonlinear_ah");
+  BRC_TRY(ctx, brc::smooth3d(raw, W, H, D, 9 * G, fe, fe, fe, nullptr, nullptr, ctx->tmp1.as<float>(), nullptr, ah,
+                             st),
           "smooth A,h");
-  BRC_TRY(ctx, brc::displacement_update(ah, ah + 6 * V, V, fp64, d3, st), "displacement_update");
-  BRC_TRY(ctx, brc::smooth3d(d3, W, H, D, 3, fd, fd, fd, nullptr, nullptr, ctx->tmp1.as<float>(), nullptr, field, st,
-                             1),
+  BRC_TRY(ctx, brc::displacement_update(ah, ah + 6 * V, V, fp64, d3, st, G, 9 * V), "displacement_update");
+  BRC_TRY(ctx, brc::smooth3d(d3, W, H, D, 3 * G, fd, fd, fd, nullptr, nullptr, ctx->tmp1.as<float>(), nullptr, field,
+                             st, 1),
           "smooth update");
   ctx->launches += 7;
   return BRC_OK;
 }
 
-static int ensure_nonlinear_ws(brc_ctx* ctx, long long V) {
-  BRC_TRY(ctx, ctx->nl.ensure(sizeof(float) * (18 * V + 64)), "alloc nonlinear");
+static int ensure_nonlinear_ws(brc_ctx* ctx, long long V, int G = 1) {
+  BRC_TRY(ctx, ctx->nl.ensure(sizeof(float) * (18 * V * G + 64 + G)), "alloc nonlinear");
   BRC_TRY(ctx, ctx->tmp1.ensure(sizeof(float) * 9 * V), "alloc tmp");
-  BRC_TRY(ctx, ctx->tmp2.ensure(sizeof(float) * 9 * V), "alloc tmp");
+  BRC_TRY(ctx, ctx->tmp2.ensure(sizeof(float) * 9 * V * G), "alloc tmp");
   return BRC_OK;
 }
 
@@ -99,21 +104,22 @@ extern "C" int brc_nonlinear_step(brc_ctx* ctx, const float* d_q1, const float* 
   smoothing_taps(tsigma, ft);
   smoothing_taps(esigma, fe);
   smoothing_taps(dsigma, fd);
-  return nonlinear_step(ctx, d_q1, d_q2, W, H, D, h_tensors, h_dirs, ft, fe, fd, solve_fp64, d_field);
+  return nonlinear_step(ctx, d_q1, d_q2, 1, W, H, D, h_tensors, h_dirs, ft, fe, fd, solve_fp64, d_field);
 }
 
-// One scale of nonlinear registration: `aligned` (in: start volume, out:
-// last warp) and `original` (the volume the field warps) at size W,H,D;
-// `field` receives this scale's total update (zeroed first).
-static int nonlinear_scale(brc_ctx* ctx, const float* ref, float* aligned, const float* original, int W,
+// One scale of nonlinear registration of G instances: `aligned` (in: start
+// volumes, out: last warps) and `original` (the volumes the fields warp), G
+// volumes of W,H,D each, one shared reference; `field` (3 volumes per
+// instance) receives this scale's total update (zeroed first).
+static int nonlinear_scale(brc_ctx* ctx, const float* ref, float* aligned, const float* original, int G, int W,
                            int H, int D, const float* filters6, const float* m36, const float* dirs18,
                            int iterations, const brc_nonlinear_opts* o, float* field) {
   const long long V = (long long)W * H * D;
   cudaStream_t st = ctx->stream();
-  int s = ensure_nonlinear_ws(ctx, V);
+  int s = ensure_nonlinear_ws(ctx, V, G);
   if (s != BRC_OK) return s;
   BRC_TRY(ctx, ctx->q1.ensure(sizeof(float) * 12 * V), "alloc q1");
-  BRC_TRY(ctx, ctx->q2.ensure(sizeof(float) * 12 * V), "alloc q2");
+  BRC_TRY(ctx, ctx->q2.ensure(sizeof(float) * 12 * V * G), "alloc q2");
   float* q1 = ctx->q1.as<float>();
   float* q2 = ctx->q2.as<float>();
   float ft[9], fe[9], fd[9];
@@ -125,62 +131,58 @@ static int nonlinear_scale(brc_ctx* ctx, const float* ref, float* aligned, const
   if (s != BRC_OK) return s;
   BRC_TRY(ctx, run_filter(fp, ref, W, H, D, 1, V, q1, brc::all_instances(), st), "filter ref");
   ctx->launches += filter_launches(fp);
-  BRC_TRY(ctx, cudaMemsetAsync(field, 0, sizeof(float) * 3 * V, st), "memset field");
+  BRC_TRY(ctx, cudaMemsetAsync(field, 0, sizeof(float) * 3 * V * G, st), "memset field");
   for (int it = 0; it < iterations; it++) {
-    BRC_TRY(ctx, run_filter(fp, aligned, W, H, D, 1, V, q2, brc::all_instances(), st), "filter");
+    BRC_TRY(ctx, run_filter(fp, aligned, W, H, D, G, V, q2, brc::all_instances(), st), "filter");
     ctx->launches += filter_launches(fp);
-    s = nonlinear_step(ctx, q1, q2, W, H, D, m36, dirs18, ft, fe, fd, o->solve_fp64, field);
+    s = nonlinear_step(ctx, q1, q2, G, W, H, D, m36, dirs18, ft, fe, fd, o->solve_fp64, field);
     if (s != BRC_OK) return s;
-    BRC_TRY(ctx, brc::warp_field(original, W, H, D, field, field + V, field + 2 * V, aligned, st), "warp");
+    BRC_TRY(ctx, brc::warp_field(original, W, H, D, field, field + V, field + 2 * V, aligned, st, G, V, 3 * V, V),
+            "warp");
     ctx->launches += 1;
   }
   return BRC_OK;
 }
 
-extern "C" int brc_register_nonlinear(brc_ctx* ctx, const float* d_ref, const float* d_moving, int W,
-                                      int H, int D, const float* h_filters6, const float* h_tensors,
-                                      const float* h_dirs, const brc_nonlinear_opts* o, float* d_field,
-                                      float* d_aligned) {
-  if (!ctx) return BRC_ERR_INVALID;
-  if (!d_ref || !d_moving || !h_filters6 || !h_tensors || !h_dirs || !o || !d_field || !d_aligned ||
-      W <= 0 || H <= 0 || D <= 0 || o->iterations < 0 || o->coarsest_scale < 1 ||
-      !(o->tsigma > 0) || !(o->esigma > 0) || !(o->dsigma > 0))
-    return ctx->fail(BRC_ERR_INVALID, "brc_register_nonlinear: bad argument");
-  if (!brc_precision_valid(o->precision))
-    return ctx->fail(BRC_ERR_UNSUPPORTED, "brc_register_nonlinear: unknown precision");
-  if (d_aligned == d_moving)
-    return ctx->fail(BRC_ERR_INVALID, "brc_register_nonlinear: d_aligned must not alias d_moving");
-  cudaSetDevice(ctx->device);
+// AlignTwoVolumesNonLinearSeveralScales (broccoli_lib.cpp:6516-6665) for G
+// moving volumes (d_moving, G volumes one after another) and one reference:
+// d_field receives 3 volumes per instance, d_aligned one.  Every launch of
+// the pyramid covers all G instances; per instance the arithmetic is that
+// of a single registration.
+static int register_nonlinear_group(brc_ctx* ctx, const float* d_ref, const float* d_moving, int G, int W, int H,
+                                    int D, const float* h_filters6, const float* h_tensors, const float* h_dirs,
+                                    const brc_nonlinear_opts* o, float* d_field, float* d_aligned) {
   cudaStream_t st = ctx->stream();
   const long long V = (long long)W * H * D;
-  // scale buffers: ref, original, aligned at the scale, two field sets
-  BRC_TRY(ctx, ctx->pyr.ensure(sizeof(float) * 10 * V), "alloc pyramid");
+  // scale buffers: reference (1), originals and aligned (G each), two field
+  // sets (3G each)
+  BRC_TRY(ctx, ctx->pyr.ensure(sizeof(float) * (V + 8 * V * G)), "alloc pyramid");
   float* r_s = ctx->pyr.as<float>();
   float* o_s = r_s + V;
-  float* a_s = o_s + V;
-  float* tot = a_s + V;       // 3V
-  float* upd = tot + 3 * V;   // 3V
+  float* a_s = o_s + V * G;
+  float* tot = a_s + V * G;       // [G][3][vs]
+  float* upd = tot + 3 * V * G;   // [G][3][vs]
   int cw = myround((float)W / (float)o->coarsest_scale);
   int ch = myround((float)H / (float)o->coarsest_scale);
   int cd = myround((float)D / (float)o->coarsest_scale);
   if (cw < 2 || ch < 2 || cd < 2)
     return ctx->fail(BRC_ERR_INVALID, "brc_register_nonlinear: coarsest scale leaves fewer than 2 voxels");
   if (o->coarsest_scale == 1) {
-    BRC_TRY(ctx, cudaMemcpyAsync(o_s, d_moving, sizeof(float) * V, cudaMemcpyDeviceToDevice, st), "copy");
+    BRC_TRY(ctx, cudaMemcpyAsync(o_s, d_moving, sizeof(float) * V * G, cudaMemcpyDeviceToDevice, st), "copy");
     BRC_TRY(ctx, cudaMemcpyAsync(r_s, d_ref, sizeof(float) * V, cudaMemcpyDeviceToDevice, st), "copy");
   } else {
-    BRC_TRY(ctx, brc::rescale_batch(d_moving, W, H, D, 1, o_s, cw, ch, cd, 1.0f, st), "rescale");
+    BRC_TRY(ctx, brc::rescale_batch(d_moving, W, H, D, G, o_s, cw, ch, cd, 1.0f, st), "rescale");
     BRC_TRY(ctx, brc::rescale_batch(d_ref, W, H, D, 1, r_s, cw, ch, cd, 1.0f, st), "rescale");
     ctx->launches += 2;
   }
-  BRC_TRY(ctx, cudaMemsetAsync(tot, 0, sizeof(float) * 3 * (long long)cw * ch * cd, st), "memset");
+  BRC_TRY(ctx, cudaMemsetAsync(tot, 0, sizeof(float) * 3 * (long long)cw * ch * cd * G, st), "memset");
   for (int scale = o->coarsest_scale; scale >= 1; scale /= 2) {
     const long long vs = (long long)cw * ch * cd;
-    BRC_TRY(ctx, cudaMemcpyAsync(a_s, o_s, sizeof(float) * vs, cudaMemcpyDeviceToDevice, st), "copy");
+    BRC_TRY(ctx, cudaMemcpyAsync(a_s, o_s, sizeof(float) * vs * G, cudaMemcpyDeviceToDevice, st), "copy");
     const int iters = scale == 1 ? (int)ceilf((float)o->iterations / 2.0f) : o->iterations;
-    int s = nonlinear_scale(ctx, r_s, a_s, o_s, cw, ch, cd, h_filters6, h_tensors, h_dirs, iters, o, upd);
+    int s = nonlinear_scale(ctx, r_s, a_s, o_s, G, cw, ch, cd, h_filters6, h_tensors, h_dirs, iters, o, upd);
     if (s != BRC_OK) return s;
-    BRC_TRY(ctx, brc::add_volumes(tot, tot, upd, 3 * vs, st), "add");
+    BRC_TRY(ctx, brc::add_volumes(tot, tot, upd, 3 * vs * G, st), "add");
     ctx->launches += 1;
     if (scale != 1) {
       const int pw = cw, ph = ch, pd = cd;
@@ -188,16 +190,18 @@ extern "C" int brc_register_nonlinear(brc_ctx* ctx, const float* d_ref, const fl
       ch = myround((float)H / ((float)scale / 2.0f));
       cd = myround((float)D / ((float)scale / 2.0f));
       const long long nv = (long long)cw * ch * cd;
-      // field to the finer grid, doubled (voxel units), via the upd buffer
-      BRC_TRY(ctx, brc::rescale_batch(tot, pw, ph, pd, 3, upd, cw, ch, cd, 2.0f, st), "rescale field");
-      BRC_TRY(ctx, cudaMemcpyAsync(tot, upd, sizeof(float) * 3 * nv, cudaMemcpyDeviceToDevice, st), "copy");
+      // fields to the finer grid, doubled (voxel units), via the upd buffer
+      BRC_TRY(ctx, brc::rescale_batch(tot, pw, ph, pd, 3 * G, upd, cw, ch, cd, 2.0f, st), "rescale field");
+      BRC_TRY(ctx, cudaMemcpyAsync(tot, upd, sizeof(float) * 3 * nv * G, cudaMemcpyDeviceToDevice, st), "copy");
       BRC_TRY(ctx, brc::rescale_batch(d_ref, W, H, D, 1, r_s, cw, ch, cd, 1.0f, st), "rescale");
-      BRC_TRY(ctx, brc::rescale_batch(d_moving, W, H, D, 1, a_s, cw, ch, cd, 1.0f, st), "rescale");
-      BRC_TRY(ctx, brc::warp_field(a_s, cw, ch, cd, tot, tot + nv, tot + 2 * nv, o_s, st), "warp");
+      BRC_TRY(ctx, brc::rescale_batch(d_moving, W, H, D, G, a_s, cw, ch, cd, 1.0f, st), "rescale");
+      BRC_TRY(ctx, brc::warp_field(a_s, cw, ch, cd, tot, tot + nv, tot + 2 * nv, o_s, st, G, nv, 3 * nv, nv),
+              "warp");
       ctx->launches += 4;
     } else {
-      BRC_TRY(ctx, cudaMemcpyAsync(d_field, tot, sizeof(float) * 3 * V, cudaMemcpyDeviceToDevice, st), "copy");
-      BRC_TRY(ctx, brc::warp_field(d_moving, W, H, D, d_field, d_field + V, d_field + 2 * V, d_aligned, st),
+      BRC_TRY(ctx, cudaMemcpyAsync(d_field, tot, sizeof(float) * 3 * V * G, cudaMemcpyDeviceToDevice, st), "copy");
+      BRC_TRY(ctx, brc::warp_field(d_moving, W, H, D, d_field, d_field + V, d_field + 2 * V, d_aligned, st, G, V,
+                                   3 * V, V),
               "warp");
       ctx->launches += 1;
     }
@@ -217,6 +221,24 @@ extern "C" int brc_register_nonlinear(brc_ctx* ctx, const float* d_ref, const fl
     }
   }
   return BRC_OK;
+}
+
+extern "C" int brc_register_nonlinear(brc_ctx* ctx, const float* d_ref, const float* d_moving, int W,
+                                      int H, int D, const float* h_filters6, const float* h_tensors,
+                                      const float* h_dirs, const brc_nonlinear_opts* o, float* d_field,
+                                      float* d_aligned) {
+  if (!ctx) return BRC_ERR_INVALID;
+  if (!d_ref || !d_moving || !h_filters6 || !h_tensors || !h_dirs || !o || !d_field || !d_aligned ||
+      W <= 0 || H <= 0 || D <= 0 || o->iterations < 0 || o->coarsest_scale < 1 ||
+      !(o->tsigma > 0) || !(o->esigma > 0) || !(o->dsigma > 0))
+    return ctx->fail(BRC_ERR_INVALID, "brc_register_nonlinear: bad argument");
+  if (!brc_precision_valid(o->precision))
+    return ctx->fail(BRC_ERR_UNSUPPORTED, "brc_register_nonlinear: unknown precision");
+  if (d_aligned == d_moving)
+    return ctx->fail(BRC_ERR_INVALID, "brc_register_nonlinear: d_aligned must not alias d_moving");
+  cudaSetDevice(ctx->device);
+  return register_nonlinear_group(ctx, d_ref, d_moving, 1, W, H, D, h_filters6, h_tensors, h_dirs, o, d_field,
+                                  d_aligned);
 }
 
 extern "C" int brc_change_resolution_and_size(brc_ctx* ctx, const float* d_src, int W, int H, int D,
@@ -395,7 +417,8 @@ extern "C" int brc_register_two_volumes(brc_ctx* ctx, const float* d_in, int W, 
   cudaStream_t st = ctx->stream();
   const long long V2 = (long long)W2 * H2 * D2;
   // own buffers for the template-size working volumes
-  DevBuf work, lin;
+  DevBuf& work = ctx->r2v_work;
+  DevBuf& lin = ctx->r2v_lin;
   BRC_TRY(ctx, work.ensure(sizeof(float) * V2), "alloc");
   BRC_TRY(ctx, lin.ensure(sizeof(float) * (V2 + 12)), "alloc");
   float* w = work.as<float>();
@@ -428,7 +451,7 @@ extern "C" int brc_register_two_volumes(brc_ctx* ctx, const float* d_in, int W, 
     brc_linear_opts_default(&lo, o->linear_iterations);
     lo.type = BRC_AFFINE;
     lo.precision = o->precision;
-    DevBuf prm;
+    DevBuf& prm = ctx->r2v_prm;
     BRC_TRY(ctx, prm.ensure(sizeof(float) * 12), "alloc");
     s = brc_register_linear_scales(ctx, d_tpl, a, W2, H2, D2, 1, h_filters3, &lo, o->coarsest_scale,
                                    prm.as<float>(), w, nullptr);
@@ -598,7 +621,11 @@ extern "C" int brc_register_cohort(brc_ctx* ctx, int n, const float* const* d_su
   const long long V2 = (long long)W2 * H2 * D2;
   // template-grid working volumes of all subjects: resampled originals,
   // centred copies, linear results; parameters; resample descriptors
-  DevBuf res, mat, lin, prm, jobs;
+  DevBuf& res = ctx->coh_res;
+  DevBuf& mat = ctx->coh_mat;
+  DevBuf& lin = ctx->coh_lin;
+  DevBuf& prm = ctx->coh_prm;
+  DevBuf& jobs = ctx->coh_jobs;
   BRC_TRY(ctx, res.ensure(sizeof(float) * V2 * n), "alloc");
   BRC_TRY(ctx, mat.ensure(sizeof(float) * V2 * n), "alloc");
   BRC_TRY(ctx, lin.ensure(sizeof(float) * V2 * n), "alloc");
@@ -660,7 +687,8 @@ extern "C" int brc_register_cohort(brc_ctx* ctx, int n, const float* const* d_su
   if (d_aligned_linear)
     BRC_TRY(ctx, cudaMemcpyAsync(d_aligned_linear, lin.ptr, sizeof(float) * V2 * n, cudaMemcpyDeviceToDevice, st),
             "copy");
-  // 4. nonlinear stage per subject (each runs at template size)
+  // 4. nonlinear stage in groups of subjects (each at template size): every
+  // launch of the pyramid covers the whole group
   if (o->nonlinear_iterations > 0) {
     brc_nonlinear_opts no;
     brc_nonlinear_opts_default(&no, o->nonlinear_iterations);
@@ -670,22 +698,33 @@ extern "C" int brc_register_cohort(brc_ctx* ctx, int n, const float* const* d_su
     no.dsigma = o->dsigma;
     no.precision = o->precision;
     no.solve_fp64 = o->solve_fp64;
-    for (int b = 0; b < n; b++) {
-      float* field = d_fields + 3 * V2 * b;
-      float* out = mat.as<float>() + V2 * b;  // the centred copy is no longer needed
-      s = brc_register_nonlinear(ctx, d_tpl, lin.as<float>() + V2 * b, W2, H2, D2, h_filters6, h_tensors, h_dirs,
-                                 &no, field, out);
+    // group size: about half the free device memory for the group's
+    // workspace (~190 bytes per voxel and subject), at most 16 subjects
+    size_t freeb = 0, totalb = 0;
+    BRC_TRY(ctx, cudaMemGetInfo(&freeb, &totalb), "memory info");
+    const double per = 190.0 * (double)V2;
+    int G = (int)((0.5 * (double)freeb) / per);
+    G = G < 1 ? 1 : (G > 16 ? 16 : G);
+    if (G > n) G = n;
+    for (int g0 = 0; g0 < n; g0 += G) {
+      const int g = n - g0 < G ? n - g0 : G;
+      float* fields = d_fields + 3 * V2 * g0;
+      float* outs = mat.as<float>() + V2 * g0;  // the centred copies are no longer needed
+      s = register_nonlinear_group(ctx, d_tpl, lin.as<float>() + V2 * g0, g, W2, H2, D2, h_filters6, h_tensors,
+                                   h_dirs, &no, fields, outs);
       if (s != BRC_OK) return s;
       if (o->linear_iterations > 0) {
-        BRC_TRY(ctx, brc::add_affine_to_field(field, W2, H2, D2, &total[12 * (size_t)b], st), "field");
-        BRC_TRY(ctx, brc::warp_field(res.as<float>() + V2 * b, W2, H2, D2, field, field + V2, field + 2 * V2, out,
-                                     st),
+        for (int b = 0; b < g; b++)
+          BRC_TRY(ctx, brc::add_affine_to_field(fields + 3 * V2 * b, W2, H2, D2, &total[12 * (size_t)(g0 + b)], st),
+                  "field");
+        BRC_TRY(ctx, brc::warp_field(res.as<float>() + V2 * g0, W2, H2, D2, fields, fields + V2, fields + 2 * V2, outs,
+                                     st, g, V2, 3 * V2, V2),
                 "warp");
-        ctx->launches += 2;
+        ctx->launches += g + 1;
       }
       if (d_aligned_nonlinear)
-        BRC_TRY(ctx, cudaMemcpyAsync(d_aligned_nonlinear + V2 * b, out, sizeof(float) * V2, cudaMemcpyDeviceToDevice,
-                                     st),
+        BRC_TRY(ctx, cudaMemcpyAsync(d_aligned_nonlinear + V2 * g0, outs, sizeof(float) * V2 * g,
+                                     cudaMemcpyDeviceToDevice, st),
                 "copy");
     }
   }

@@ -38,8 +38,11 @@ cudaError_t solve_given(const double* A, const double* h, int batch, float* p, c
 cudaError_t warp_affine(const float* src, long long src_stride, int W, int H, int D, int batch,
                         const float* params, float* out, long long out_stride, ActiveSet act,
                         cudaStream_t st);
+// batch instances blockIdx.y: src, field (dx, dy, dz) and out advance by
+// their strides (floats) per instance.
 cudaError_t warp_field(const float* src, int W, int H, int D, const float* dx, const float* dy,
-                       const float* dz, float* out, cudaStream_t st);
+                       const float* dz, float* out, cudaStream_t st, int batch = 1, long long src_stride = 0,
+                       long long field_stride = 0, long long out_stride = 0);
 cudaError_t rescale_linear(const float* src, int W, int H, int D, float* out, int W2, int H2, int D2,
                            cudaStream_t st);
 cudaError_t smooth3d(const float* vol, int W, int H, int D, int batch, const float* fx,
@@ -53,14 +56,19 @@ cudaError_t multiply_mask(float* vols, const float* mask, long long V, int batch
 cudaError_t phase_volumes(const float* q1, const float* q2, int W, int H, int D, int axis, float* pd, float* cert,
                           float* grad, cudaStream_t st);
 // nonlinear.cu
-cudaError_t tensor_norm_max(const float* t6, long long V, float* a11, unsigned int* maxbits,
-                            cudaStream_t st);
+// The per-voxel steps of a nonlinear iteration for `batch` instances (grid
+// dimension y): t6 / q2 hold 6 (complex) volumes per instance, a6 and h3
+// advance by ah_stride floats per instance, d3 by 3 volumes, maxbits by one
+// word; q1 (the reference's responses) is shared.
+cudaError_t tensor_norm_max(const float* t6, long long V, float* a11, unsigned int* maxbits, cudaStream_t st,
+                            int batch = 1, long long t_stride = 0, long long a_stride = 0);
 cudaError_t nonlinear_ah(const float* q1, const float* q2, float* t6, long long V,
                          const unsigned int* maxbits, const float* m36, const float* dirs18, float* a6,
-                         float* h3, cudaStream_t st);
-cudaError_t tensor_components(const float* q2, long long V, const float* m36, float* t6, cudaStream_t st);
+                         float* h3, cudaStream_t st, int batch = 1, long long ah_stride = 0);
+cudaError_t tensor_components(const float* q2, long long V, const float* m36, float* t6, cudaStream_t st,
+                              int batch = 1);
 cudaError_t displacement_update(const float* a6, const float* h3, long long V, int fp64, float* d3,
-                                cudaStream_t st);
+                                cudaStream_t st, int batch = 1, long long ah_stride = 0);
 cudaError_t rescale_batch(const float* src, int W, int H, int D, int batch, float* out, int W2, int H2,
                           int D2, float factor, cudaStream_t st);
 cudaError_t compose(float* total, const float* add, int batch, float tscale, cudaStream_t st);

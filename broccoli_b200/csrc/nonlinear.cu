@@ -31,7 +31,11 @@ struct NonlinearConsts {
 // CalculateMax (broccoli_lib.cpp:10889-10928).
 __global__ void __launch_bounds__(256)
 tensor_norm_max_kernel(const float* __restrict__ t6, long long V, float* __restrict__ a11,
-                       unsigned int* __restrict__ maxbits) {
+                       unsigned int* __restrict__ maxbits, long long t_stride, long long a_stride) {
+  // instance blockIdx.y: its tensor, norm volume and maximum
+  t6 += (long long)blockIdx.y * t_stride;
+  a11 += (long long)blockIdx.y * a_stride;
+  maxbits += blockIdx.y;
   float mx = 0.f;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < V;
        i += (long long)gridDim.x * blockDim.x) {
@@ -58,9 +62,17 @@ tensor_norm_max_kernel(const float* __restrict__ t6, long long V, float* __restr
 __global__ void __launch_bounds__(256)
 nonlinear_ah_kernel(const float2* __restrict__ q1, const float2* __restrict__ q2,
                     float* __restrict__ t6, long long V, const unsigned int* __restrict__ maxbits,
-                    NonlinearConsts cst, float* __restrict__ a6, float* __restrict__ h3) {
+                    NonlinearConsts cst, float* __restrict__ a6, float* __restrict__ h3, long long ah_stride) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= V) return;
+  // instance blockIdx.y (q1, the reference's responses, is shared): q2 6
+  // complex volumes, t6 6 volumes, a6 / h3 ah_stride floats apart
+  const int b = blockIdx.y;
+  q2 += (long long)b * 6 * V;
+  t6 += (long long)b * 6 * V;
+  maxbits += b;
+  a6 += (long long)b * ah_stride;
+  h3 += (long long)b * ah_stride;
   const float mx = fmaxf(__uint_as_float(*maxbits), 1.17549435e-38f);
   const float f = 1.0f / mx;
   const float t11 = t6[i] * f, t12 = t6[V + i] * f, t13 = t6[2 * V + i] * f;
@@ -118,9 +130,13 @@ nonlinear_ah_kernel(const float2* __restrict__ q1, const float2* __restrict__ q2
 // inverse gives d = 0).
 __global__ void __launch_bounds__(256)
 displacement_update_kernel(const float* __restrict__ a6, const float* __restrict__ h3, long long V,
-                           int fp64, float* __restrict__ d3) {
+                           int fp64, float* __restrict__ d3, long long ah_stride) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= V) return;
+  // instance blockIdx.y: a6 / h3 ah_stride floats apart, d3 3 volumes
+  a6 += (long long)blockIdx.y * ah_stride;
+  h3 += (long long)blockIdx.y * ah_stride;
+  d3 += (long long)blockIdx.y * 3 * V;
   if (!fp64) {
     const float a11 = a6[i], a12 = a6[V + i], a13 = a6[2 * V + i], a22 = a6[3 * V + i],
                 a23 = a6[4 * V + i], a33 = a6[5 * V + i];
@@ -164,6 +180,9 @@ tensor_components_kernel(const float2* __restrict__ q2, long long V, NonlinearCo
                          float* __restrict__ t6) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= V) return;
+  // instance blockIdx.y: 6 complex responses in, 6 tensor volumes out
+  q2 += (long long)blockIdx.y * 6 * V;
+  t6 += (long long)blockIdx.y * 6 * V;
   float t[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll
   for (int k = 0; k < 6; k++) {
@@ -629,40 +648,49 @@ cudaError_t add_affine_to_field(float* field, int W, int H, int D, const float* 
   return cudaGetLastError();
 }
 
-cudaError_t tensor_norm_max(const float* t6, long long V, float* a11, unsigned int* maxbits,
-                            cudaStream_t st) {
-  cudaError_t e = cudaMemsetAsync(maxbits, 0, sizeof(unsigned int), st);
+cudaError_t tensor_norm_max(const float* t6, long long V, float* a11, unsigned int* maxbits, cudaStream_t st,
+                            int batch, long long t_stride, long long a_stride) {
+  if (batch <= 0 || batch > 65535) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(maxbits, 0, sizeof(unsigned int) * batch, st);
   if (e != cudaSuccess) return e;
   long long blocks = (V + 255) / 256;
-  if (blocks > 148 * 8) blocks = 148 * 8;
-  tensor_norm_max_kernel<<<(unsigned)blocks, 256, 0, st>>>(t6, V, a11, maxbits);
+  const long long cap = (148 * 8 + batch - 1) / batch;
+  if (blocks > cap) blocks = cap;
+  tensor_norm_max_kernel<<<dim3((unsigned)blocks, (unsigned)batch), 256, 0, st>>>(t6, V, a11, maxbits, t_stride,
+                                                                                  a_stride);
   return cudaGetLastError();
 }
 
 cudaError_t nonlinear_ah(const float* q1, const float* q2, float* t6, long long V, const unsigned int* maxbits,
-                         const float* m36, const float* dirs18, float* a6, float* h3, cudaStream_t st) {
+                         const float* m36, const float* dirs18, float* a6, float* h3, cudaStream_t st, int batch,
+                         long long ah_stride) {
+  if (batch <= 0 || batch > 65535) return cudaErrorInvalidValue;
   NonlinearConsts c;
   for (int k = 0; k < 6; k++)
     for (int j = 0; j < 6; j++) c.m[k][j] = m36[6 * k + j];
   for (int a = 0; a < 3; a++)
     for (int k = 0; k < 6; k++) c.dir[a][k] = dirs18[6 * a + k];
-  nonlinear_ah_kernel<<<grid1(V), 256, 0, st>>>(reinterpret_cast<const float2*>(q1),
-                                                 reinterpret_cast<const float2*>(q2), t6, V, maxbits, c,
-                                                 a6, h3);
+  nonlinear_ah_kernel<<<dim3(grid1(V), (unsigned)batch), 256, 0, st>>>(reinterpret_cast<const float2*>(q1),
+                                                                        reinterpret_cast<const float2*>(q2), t6, V,
+                                                                        maxbits, c, a6, h3, ah_stride);
   return cudaGetLastError();
 }
 
-cudaError_t tensor_components(const float* q2, long long V, const float* m36, float* t6, cudaStream_t st) {
+cudaError_t tensor_components(const float* q2, long long V, const float* m36, float* t6, cudaStream_t st,
+                              int batch) {
+  if (batch <= 0 || batch > 65535) return cudaErrorInvalidValue;
   NonlinearConsts c;
   for (int k = 0; k < 6; k++)
     for (int j = 0; j < 6; j++) c.m[k][j] = m36[6 * k + j];
-  tensor_components_kernel<<<grid1(V), 256, 0, st>>>(reinterpret_cast<const float2*>(q2), V, c, t6);
+  tensor_components_kernel<<<dim3(grid1(V), (unsigned)batch), 256, 0, st>>>(reinterpret_cast<const float2*>(q2),
+                                                                             V, c, t6);
   return cudaGetLastError();
 }
 
 cudaError_t displacement_update(const float* a6, const float* h3, long long V, int fp64, float* d3,
-                                cudaStream_t st) {
-  displacement_update_kernel<<<grid1(V), 256, 0, st>>>(a6, h3, V, fp64, d3);
+                                cudaStream_t st, int batch, long long ah_stride) {
+  if (batch <= 0 || batch > 65535) return cudaErrorInvalidValue;
+  displacement_update_kernel<<<dim3(grid1(V), (unsigned)batch), 256, 0, st>>>(a6, h3, V, fp64, d3, ah_stride);
   return cudaGetLastError();
 }
 

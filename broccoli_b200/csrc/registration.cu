@@ -790,10 +790,18 @@ warp_affine_kernel(const float* __restrict__ src, long long src_stride, int W, i
 // kernelRegistration.cpp:1111-1140).
 __global__ void __launch_bounds__(256)
 warp_field_kernel(const float* __restrict__ src, int W, int H, int D, const float* __restrict__ dx,
-                  const float* __restrict__ dy, const float* __restrict__ dz, float* __restrict__ out) {
+                  const float* __restrict__ dy, const float* __restrict__ dz, float* __restrict__ out,
+                  long long src_stride, long long field_stride, long long out_stride) {
   const int V = W * H * D;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= V) return;
+  // instance blockIdx.y
+  const long long b = blockIdx.y;
+  src += b * src_stride;
+  dx += b * field_stride;
+  dy += b * field_stride;
+  dz += b * field_stride;
+  out += b * out_stride;
   const int r = i / W;
   const int x = i - r * W, y = r % H, z = r / H;
   out[i] = sample_linear(src, W, H, D, (float)x + dx[i] + 0.5f, (float)y + dy[i] + 0.5f,
@@ -1142,10 +1150,12 @@ cudaError_t warp_affine(const float* src, long long src_stride, int W, int H, in
 }
 
 cudaError_t warp_field(const float* src, int W, int H, int D, const float* dx, const float* dy,
-                       const float* dz, float* out, cudaStream_t st) {
+                       const float* dz, float* out, cudaStream_t st, int batch, long long src_stride,
+                       long long field_stride, long long out_stride) {
   const long long V = (long long)W * H * D;
-  if (V > kMaxVoxels) return cudaErrorInvalidValue;
-  warp_field_kernel<<<(unsigned)((V + 255) / 256), 256, 0, st>>>(src, W, H, D, dx, dy, dz, out);
+  if (V > kMaxVoxels || batch <= 0 || batch > 65535) return cudaErrorInvalidValue;
+  warp_field_kernel<<<dim3((unsigned)((V + 255) / 256), (unsigned)batch), 256, 0, st>>>(
+      src, W, H, D, dx, dy, dz, out, src_stride, field_stride, out_stride);
   return cudaGetLastError();
 }
 
