@@ -266,6 +266,50 @@ class BROCCOLI_LIB:
     def SetDsigma(self, s): self.sigmas[2] = float(s)
     def SetMotionCorrectionTolerance(self, v): self.mc_tolerance = float(v)
     def SetPrecision(self, p): self.precision = int(p)
+    def SetSolveFP64(self, b): self.solve_fp64 = bool(b)
+    def SetPrecenterRegistration(self, b): self.precenter = bool(b)
+    def SetDoSkullstrip(self, b): self.do_skullstrip = bool(b)
+    def SetDoSkullstripOriginal(self, b): self.do_skullstrip_original = bool(b)
+    def SetInputMNIBrainMask(self, a): self.mni_mask = a
+    def SetOutputSkullstrippedT1Volume(self, a): self.out["skullstripped"] = a
+    def SetDebug(self, b): self.debug = bool(b)
+    def SetOutputQuadratureFilterResponses(self, *arrays):
+        """Three arrays (the last linear call's reference responses) or six
+        (the nonlinear reference's responses at the finest scale)."""
+        if len(arrays) not in (3, 6):
+            raise ValueError("SetOutputQuadratureFilterResponses takes 3 or 6 arrays")
+        self.out["q"] = list(arrays)
+    def SetOutputPhaseDifferences(self, a): self.out["phase_differences"] = a
+    def SetOutputPhaseCertainties(self, a): self.out["phase_certainties"] = a
+    def SetOutputPhaseGradients(self, a): self.out["phase_gradients"] = a
+
+    def _debug_arrays(self, ctx):
+        """Host arrays for the context's debug outputs when SetDebug(True):
+        the caller's own arrays where they are contiguous of the right type,
+        else staging arrays copied back by _debug_copy_back."""
+        if not getattr(self, "debug", False):
+            ctx.set_debug_outputs(None)
+            return None
+        stage = {}
+
+        def host(a, dtype):
+            if a is None:
+                return None
+            if isinstance(a, np.ndarray) and a.dtype == dtype and a.flags.c_contiguous:
+                return a
+            t = np.zeros(np.asarray(a).size, dtype)
+            stage[id(t)] = (t, a)
+            return t
+        outs = {"quadrature_responses": [host(a, np.complex64) for a in self.out.get("q", [])]}
+        for k in ("phase_differences", "phase_certainties", "phase_gradients"):
+            outs[k] = host(self.out.get(k), np.float32)
+        ctx.set_debug_outputs(outs)
+        return stage
+
+    @staticmethod
+    def _debug_copy_back(stage):
+        for t, a in (stage or {}).values():
+            a[...] = t.reshape(np.asarray(a).shape).astype(np.asarray(a).dtype)
     def SetOutputMotionParameters(self, a): self.out["motion"] = a
     def SetOutputMotionCorrectedfMRIVolumes(self, a): self.out["mc"] = a
     def SetOutputT1MNIRegistrationParameters(self, a): self.out["params"] = a
@@ -283,6 +327,8 @@ class BROCCOLI_LIB:
     # ---- entry points -------------------------------------------------------
 
     def PerformMotionCorrectionWrapper(self):
+        if getattr(self, "debug", False):
+            return self._motion_correction_debug()
         W, H, D, T = self.epi
         vols = np.ascontiguousarray(self.fmri, np.float32)
         opts = L.LinearOpts()
@@ -301,6 +347,24 @@ class BROCCOLI_LIB:
             self.out["motion"][...] = motion.reshape(self.out["motion"].shape)
         if "mc" in self.out:
             self.out["mc"][...] = vols.reshape(self.out["mc"].shape)
+
+    def _motion_correction_debug(self):
+        """Motion correction through a Context, so that SetDebug's outputs
+        are filled (the last volume's registration to volume 0)."""
+        from .api import Context
+        W, H, D, T = self.epi
+        ctx = Context(0)
+        stage = self._debug_arrays(ctx)
+        vols = np.ascontiguousarray(self.fmri, np.float32).reshape(T, D, H, W)
+        corrected, motion = ctx.motion_correct(vols, self.epi_vox, self.linear_filters, self.it_mc,
+                                               precision=self.precision, tolerance=self.mc_tolerance)
+        ctx.close()
+        self._debug_copy_back(stage)
+        self.fmri[...] = np.asarray(corrected, np.float32).reshape(self.fmri.shape)
+        if "motion" in self.out:
+            self.out["motion"][...] = np.asarray(motion, np.float32).reshape(self.out["motion"].shape)
+        if "mc" in self.out:
+            self.out["mc"][...] = np.asarray(corrected, np.float32).reshape(self.out["mc"].shape)
 
     def _smoothing_taps(self):
         if getattr(self, "smoothing_type", LOWPASS) == RANDOM:
@@ -342,9 +406,18 @@ class BROCCOLI_LIB:
         tpl = torch.from_numpy(np.ascontiguousarray(self.mni_volume, np.float32).reshape(D2, H2, W2)).cuda()
         bank = {"linear": self.linear_filters, "nonlinear": self.nonlinear_filters,
                 "projection_tensors": self.projection_tensors, "directions": self.directions}
-        r = ctx.register_two_volumes(sub, self.t1_vox, tpl, self.mni_vox, bank, self.it_linear,
-                                     self.it_nonlinear if self.nonlinear_filters is not None else 0,
-                                     self.coarsest, self.mm_z_cut, *self.sigmas)
+        nonlinear = self.it_nonlinear if self.nonlinear_filters is not None else 0
+        strip = getattr(self, "do_skullstrip", False) or (getattr(self, "do_skullstrip_original", False) and
+                                                            self.it_linear > 0)
+        if strip and (getattr(self, "mni_mask", None) is None or "skullstripped" not in self.out):
+            raise L.BrcError(L.BRC_ERR_INVALID, "PerformRegistrationTwoVolumesWrapper: skull strip needs "
+                                                "SetInputMNIBrainMask and SetOutputSkullstrippedT1Volume")
+        stage = self._debug_arrays(ctx)
+        r = ctx.register_two_volumes(sub, self.t1_vox, tpl, self.mni_vox, bank, self.it_linear, nonlinear,
+                                     self.coarsest, self.mm_z_cut, *self.sigmas,
+                                     solve_fp64=getattr(self, "solve_fp64", False), precision=self.precision,
+                                     precenter=getattr(self, "precenter", False))
+        self._debug_copy_back(stage)
         if "params" in self.out:
             self.out["params"][: 12] = r["params"]
         for k in ("aligned_linear", "aligned_nonlinear", "interpolated"):
@@ -354,6 +427,18 @@ class BROCCOLI_LIB:
             f = r["field"].cpu().numpy()
             for a in range(3):
                 self.out["field"][a][...] = f[a].reshape(self.out["field"][a].shape)
+        if strip:
+            # broccoli_lib.cpp:8064-8105: the aligned volume times the mask, or
+            # the interpolated volume times the mask carried back (NEAREST)
+            mask = torch.from_numpy(np.ascontiguousarray(self.mni_mask, np.float32).reshape(D2, H2, W2)).cuda()
+            if getattr(self, "do_skullstrip", False):
+                vol = (r["aligned_nonlinear"] if nonlinear > 0 else r["aligned_linear"]).clone()
+            else:
+                inv = Context.invert_affine_parameters(r["params"])
+                mask = ctx.transform_volumes_linear(mask, inv, L.INTERP_NEAREST).reshape(D2, H2, W2).contiguous()
+                vol = r["interpolated"].clone()
+            ctx.multiply_volumes(vol, mask)
+            self.out["skullstripped"][...] = vol.cpu().numpy().reshape(self.out["skullstripped"].shape)
         ctx.close()
 
     def PerformFirstLevelAnalysisWrapper(self):

@@ -117,3 +117,63 @@ def test_perform_first_level_preprocessing_equals_library(bank):
     assert np.array_equal(r["motion_parameters"], want["motion_parameters"])
     assert np.array_equal(r["EPI_mask"], wrap3(want["epi_mask"]))
     assert np.array_equal(r["aligned_T1_volume"], wrap3(want["aligned_t1_linear"]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("strip", ["mask", "original"])
+def test_two_volumes_precenter_skull_strip_debug(golden, bank, strip):
+    """The Python mirror's SetPrecenterRegistration, SetDoSkullstrip(Original)
+    with SetInputMNIBrainMask / SetOutputSkullstrippedT1Volume, and SetDebug
+    with three response arrays, against the reference kernels' fixtures
+    (tests/golden/boundary.npz; 6 linear and 4 nonlinear iterations, coarsest
+    scale 2, 3 mm z cut as there)."""
+    import os
+    import oracle
+    from conftest import GOLDEN
+    bd = dict(np.load(os.path.join(GOLDEN, "boundary.npz")))
+    sub, tpl = golden["r2v_subject"], golden["r2v_template"]
+    D, H, W = sub.shape
+    D2, H2, W2 = tpl.shape
+    B = BL.BROCCOLI_LIB(0, 0)
+    B.SetT1Width(W), B.SetT1Height(H), B.SetT1Depth(D)
+    vs = golden["r2v_voxel"]
+    B.SetT1VoxelSizeX(vs[0]), B.SetT1VoxelSizeY(vs[1]), B.SetT1VoxelSizeZ(vs[2])
+    B.SetMNIWidth(W2), B.SetMNIHeight(H2), B.SetMNIDepth(D2)
+    B.SetInputT1Volume(np.ascontiguousarray(sub).reshape(-1))
+    B.SetInputMNIBrainVolume(np.ascontiguousarray(tpl).reshape(-1))
+    B.linear_filters = np.ascontiguousarray(bank["linear"], np.float32)
+    B.nonlinear_filters = np.ascontiguousarray(bank["nonlinear"], np.float32)
+    B.projection_tensors = np.asarray(bank["projection_tensors"], np.float32).reshape(6, 6)
+    B.directions = np.asarray(bank["directions"], np.float32).reshape(3, 6)
+    B.SetNumberOfIterationsForLinearImageRegistration(6)
+    B.SetNumberOfIterationsForNonLinearImageRegistration(4)
+    B.SetCoarsestScaleT1MNI(2)
+    B.SetMMT1ZCUT(3)
+    B.SetPrecenterRegistration(True)
+    params = np.zeros(12, np.float32)
+    nonlin = np.zeros(D2 * H2 * W2, np.float32)
+    interp = np.zeros(D2 * H2 * W2, np.float32)
+    skull = np.zeros(D2 * H2 * W2, np.float32)
+    B.SetOutputT1MNIRegistrationParameters(params)
+    B.SetOutputAlignedT1VolumeNonLinear(nonlin)
+    B.SetOutputInterpolatedT1Volume(interp)
+    B.SetInputMNIBrainMask(bd["r2v_mask"].reshape(-1))
+    B.SetOutputSkullstrippedT1Volume(skull)
+    B.SetDoSkullstrip(strip == "mask")
+    B.SetDoSkullstripOriginal(strip == "original")
+    q = [np.zeros(D2 * H2 * W2, np.complex64) for _ in range(3)]
+    B.SetDebug(True)
+    B.SetOutputQuadratureFilterResponses(*q)
+    B.PerformRegistrationTwoVolumesWrapper()
+    assert np.abs(params - bd["pc_params"]).max() < 1e-4 * max(1.0, np.abs(bd["pc_params"]).max())
+    assert rel_err(nonlin.reshape(D2, H2, W2), bd["pc_aligned_nonlinear"]) < 1e-4
+    mask = bd["r2v_mask"]
+    if strip == "mask":
+        assert np.array_equal(skull, nonlin * mask.reshape(-1))
+    else:
+        from broccoli_b200.api import Context
+        back = oracle.transform_affine(mask, Context.invert_affine_parameters(params), interp=0)[0]
+        assert np.array_equal(skull, interp * back.reshape(-1))
+    qt = oracle.filter3d(tpl, bank["linear"])
+    for k in range(3):
+        assert rel_err(q[k].reshape(D2, H2, W2), qt[k]) < 1e-4
