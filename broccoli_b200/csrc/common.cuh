@@ -84,19 +84,39 @@ __device__ __forceinline__ float sample_linear(const float* __restrict__ T, int 
   const float fu = floorf(uu), fv = floorf(vv), fw = floorf(ww);
   const float a = uu - fu, bb = vv - fv, c = ww - fw;
   const int i0 = (int)fu, j0 = (int)fv, k0 = (int)fw;
-  const int xi0 = min(max(i0, 0), W - 1), xi1 = min(max(i0 + 1, 0), W - 1);
-  const int yj0 = min(max(j0, 0), H - 1), yj1 = min(max(j0 + 1, 0), H - 1);
-  const int zk0 = min(max(k0, 0), D - 1), zk1 = min(max(k0 + 1, 0), D - 1);
   const int WH = W * H;
-  const int r00 = yj0 * W + zk0 * WH;
-  const int r10 = yj1 * W + zk0 * WH;
-  const int r01 = yj0 * W + zk1 * WH;
-  const int r11 = yj1 * W + zk1 * WH;
+  float t000, t100, t010, t110, t001, t101, t011, t111;
+  if ((unsigned)i0 < (unsigned)(W - 1) && (unsigned)j0 < (unsigned)(H - 1) && (unsigned)k0 < (unsigned)(D - 1)) {
+    // all eight neighbours inside the volume (the clamps below leave them
+    // as they are): one base address and constant offsets
+    const float* p0 = T + (i0 + j0 * W + k0 * WH);
+    const float* p1 = p0 + WH;
+    t000 = __ldg(p0);
+    t100 = __ldg(p0 + 1);
+    t010 = __ldg(p0 + W);
+    t110 = __ldg(p0 + W + 1);
+    t001 = __ldg(p1);
+    t101 = __ldg(p1 + 1);
+    t011 = __ldg(p1 + W);
+    t111 = __ldg(p1 + W + 1);
+  } else {
+    const int xi0 = min(max(i0, 0), W - 1), xi1 = min(max(i0 + 1, 0), W - 1);
+    const int yj0 = min(max(j0, 0), H - 1), yj1 = min(max(j0 + 1, 0), H - 1);
+    const int zk0 = min(max(k0, 0), D - 1), zk1 = min(max(k0 + 1, 0), D - 1);
+    const int r00 = yj0 * W + zk0 * WH;
+    const int r10 = yj1 * W + zk0 * WH;
+    const int r01 = yj0 * W + zk1 * WH;
+    const int r11 = yj1 * W + zk1 * WH;
+    t000 = __ldg(T + xi0 + r00);
+    t100 = __ldg(T + xi1 + r00);
+    t010 = __ldg(T + xi0 + r10);
+    t110 = __ldg(T + xi1 + r10);
+    t001 = __ldg(T + xi0 + r01);
+    t101 = __ldg(T + xi1 + r01);
+    t011 = __ldg(T + xi0 + r11);
+    t111 = __ldg(T + xi1 + r11);
+  }
   // trilinear weights applied as seven linear interpolations
-  const float t000 = __ldg(T + xi0 + r00), t100 = __ldg(T + xi1 + r00);
-  const float t010 = __ldg(T + xi0 + r10), t110 = __ldg(T + xi1 + r10);
-  const float t001 = __ldg(T + xi0 + r01), t101 = __ldg(T + xi1 + r01);
-  const float t011 = __ldg(T + xi0 + r11), t111 = __ldg(T + xi1 + r11);
   const float c00 = fmaf(a, t100 - t000, t000), c10 = fmaf(a, t110 - t010, t010);
   const float c01 = fmaf(a, t101 - t001, t001), c11 = fmaf(a, t111 - t011, t011);
   const float c0 = fmaf(bb, c10 - c00, c00), c1 = fmaf(bb, c11 - c01, c01);

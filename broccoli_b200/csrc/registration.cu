@@ -769,6 +769,9 @@ __global__ void solve_given_kernel(const double* __restrict__ A, const double* _
 
 // out_b(x) = src_b(x + t + (A - I)(x - centre)), params_b of instance b
 // (InterpolateVolumeLinearLinear, kernelRegistration.cpp:1066-1101).
+// VEC: params is 16-byte aligned, and the 12 parameters of an instance are
+// read as three 16-byte loads.
+template <bool VEC>
 __global__ void __launch_bounds__(256)
 warp_affine_kernel(const float* __restrict__ src, long long src_stride, int W, int H, int D, int ntx, int batch,
                    const float* __restrict__ params, float* __restrict__ out, long long out_stride,
@@ -781,8 +784,23 @@ warp_affine_kernel(const float* __restrict__ src, long long src_stride, int W, i
   const int n = active_count(act, batch);
   for (int li = blockIdx.z; li < n; li += gridDim.z) {
     const int b = active_instance(act, li);
+    float p[12];
+    if (VEC) {
+      const float4* p4 = reinterpret_cast<const float4*>(params + (long long)b * 12);
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        const float4 v = __ldg(p4 + q);
+        p[4 * q] = v.x;
+        p[4 * q + 1] = v.y;
+        p[4 * q + 2] = v.z;
+        p[4 * q + 3] = v.w;
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < 12; q++) p[q] = __ldg(params + (long long)b * 12 + q);
+    }
     out[(long long)b * out_stride + ((long long)z * H + y) * W + x] =
-        affine_sample(src + (long long)b * src_stride, W, H, D, params + (long long)b * 12, x, y, z);
+        affine_sample(src + (long long)b * src_stride, W, H, D, p, x, y, z);
   }
 }
 
@@ -1144,8 +1162,12 @@ cudaError_t warp_affine(const float* src, long long src_stride, int W, int H, in
   // at most 16 instance shares: a launch whose instances have mostly
   // converged does not pay for blocks with nothing to do
   dim3 grid((unsigned)(ntx * nty), (unsigned)D, (unsigned)(batch < 16 ? batch : 16));
-  warp_affine_kernel<<<grid, dim3(32, 8), 0, st>>>(src, src_stride, W, H, D, ntx, batch, params, out, out_stride,
-                                                   act);
+  if ((reinterpret_cast<uintptr_t>(params) & 15) == 0)
+    warp_affine_kernel<true><<<grid, dim3(32, 8), 0, st>>>(src, src_stride, W, H, D, ntx, batch, params, out,
+                                                         out_stride, act);
+  else
+    warp_affine_kernel<false><<<grid, dim3(32, 8), 0, st>>>(src, src_stride, W, H, D, ntx, batch, params, out,
+                                                          out_stride, act);
   return cudaGetLastError();
 }
 
