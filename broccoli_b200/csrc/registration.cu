@@ -13,6 +13,8 @@
 //                             original volume with the total parameters.
 #include <math.h>
 
+#include <type_traits>
+
 #include "common.cuh"
 #include "internal.h"
 
@@ -248,12 +250,14 @@ normal_eq_march_kernel(const float2* __restrict__ q1, long long q1_stride, const
                        const ActiveSet act, float cw0, float cw1) {
   if ((int)blockIdx.y >= active_count(act, (int)gridDim.y)) return;
   const int b = active_instance(act, blockIdx.y);
+  // Shared slots are numbered by step: the plane of step s (p = z0 - 1 + s)
+  // uses slot s % 3, a constant in each of the three unrolled copies below.
   __shared__ float sxr[kMarchWarps][3][32];     // x-smoothed certainties of the newest plane
-  // x/y-smoothed certainties of the last three planes (slot p % 3); each
-  // thread reads back only its own entries, so no barrier guards them
+  // x/y-smoothed certainties of the last three planes; each thread reads
+  // back only its own entries, so no barrier guards them
   __shared__ float cxr[SMOOTH ? 3 : 1][kMarchWarps][3][32];
-  __shared__ float2 qy1[2][kMarchWarps][32];    // axis-1 responses (q1) of the last two planes
-  __shared__ float2 qy2[2][kMarchWarps][32];    // axis-1 responses (q2)
+  __shared__ float2 qy1[3][kMarchWarps][32];    // axis-1 responses (q1) of the last planes
+  __shared__ float2 qy2[3][kMarchWarps][32];    // axis-1 responses (q2)
   __shared__ double s_part[kMarchWarps][kNSums];
   const long long V = (long long)W * H * D;
   const long long WH = (long long)W * H;
@@ -283,13 +287,20 @@ normal_eq_march_kernel(const float2* __restrict__ q1, long long q1_stride, const
 #pragma unroll
     for (int q = 0; q < 5; q++) m[k][q] = 0.f;
 
-  PlaneQ cur, nw, nxt;
+  // Three plane buffers whose roles rotate by step: at step s (plane p) the
+  // current one holds plane p - 1 (the output plane), the newest plane p,
+  // and the third, which held plane p - 2, receives plane p + 1.  The loop
+  // is unrolled three times so that the rotation costs no register moves.
+  PlaneQ pb0, pb1, pb2;
   float2 prev_a2 = make_float2(0.f, 0.f), prev_c2 = make_float2(0.f, 0.f);  // axis 2 at z - 1
 #pragma unroll
-  for (int k = 0; k < 3; k++) cur.a[k] = cur.c[k] = nw.a[k] = nw.c[k] = make_float2(0.f, 0.f);
-  if (!empty) load_plane_q(Q1, Q2, V, (long long)(z0 - 1) * WH + col, in, nw);
+  for (int k = 0; k < 3; k++) pb0.a[k] = pb0.c[k] = pb2.a[k] = pb2.c[k] = make_float2(0.f, 0.f);
+  if (!empty) load_plane_q(Q1, Q2, V, (long long)(z0 - 1) * WH + col, in, pb1);
 
-  for (int p = z0 - 1; !empty && p <= z1; p++) {
+  auto step = [&](auto slot, int p, PlaneQ& cur, PlaneQ& nw, PlaneQ& nxt) {
+    constexpr int j = decltype(slot)::value;  // slot of plane p
+    constexpr int j1 = (j + 2) % 3;            // plane p - 1
+    constexpr int j2 = (j + 1) % 3;            // plane p - 2
     // [A] certainties of plane p, x pass, axis-1 responses to shared memory
     if (SMOOTH) {
 #pragma unroll
@@ -301,16 +312,19 @@ normal_eq_march_kernel(const float2* __restrict__ q1, long long q1_stride, const
         sxr[warp][k][lane] = w1 * cl + w0 * cv + w1 * cr;
       }
     }
-    qy1[p & 1][warp][lane] = nw.a[1];
-    qy2[p & 1][warp][lane] = nw.c[1];
+    qy1[j][warp][lane] = nw.a[1];
+    qy2[j][warp][lane] = nw.c[1];
     __syncthreads();
-    // next plane in flight during the rest of this step
+    // axis 2 of plane p - 2, then the next plane in flight during the rest
+    // of this step
+    prev_a2 = nxt.a[2];
+    prev_c2 = nxt.c[2];
     if (p + 1 <= z1) load_plane_q(Q1, Q2, V, (long long)(p + 1) * WH + col, in, nxt);
     // [B] y pass: smoothed certainty of plane p in the register window
     if (SMOOTH && warp >= 1 && warp <= 8) {
 #pragma unroll
       for (int k = 0; k < 3; k++)
-        cxr[SMOOTH ? p % 3 : 0][warp][k][lane] =
+        cxr[SMOOTH ? j : 0][warp][k][lane] =
             w1 * sxr[warp - 1][k][lane] + w0 * sxr[warp][k][lane] + w1 * sxr[warp + 1][k][lane];
     }
     // [C] sums of output plane z = p - 1
@@ -327,19 +341,18 @@ normal_eq_march_kernel(const float2* __restrict__ q1, long long q1_stride, const
       const float2 c0m = make_float2(__shfl_up_sync(0xffffffffu, cur.c[0].x, 1),
                                      __shfl_up_sync(0xffffffffu, cur.c[0].y, 1));
       if (out) {
-        const int sl = z & 1;  // slot of plane z = p - 1
         float2 ap[3], am[3], cp[3], cm[3];
         ap[0] = a0p; am[0] = a0m; cp[0] = c0p; cm[0] = c0m;
-        ap[1] = qy1[sl][warp + 1][lane]; am[1] = qy1[sl][warp - 1][lane];
-        cp[1] = qy2[sl][warp + 1][lane]; cm[1] = qy2[sl][warp - 1][lane];
+        ap[1] = qy1[j1][warp + 1][lane]; am[1] = qy1[j1][warp - 1][lane];
+        cp[1] = qy2[j1][warp + 1][lane]; cm[1] = qy2[j1][warp - 1][lane];
         ap[2] = nw.a[2]; am[2] = prev_a2; cp[2] = nw.c[2]; cm[2] = prev_c2;
 #pragma unroll
         for (int k = 0; k < 3; k++) {
           float pd, cert;
           phase_diff_cert(cur.a[k], cur.c[k], pd, cert);
           if (SMOOTH)
-            cert = w1 * cxr[SMOOTH ? (p + 1) % 3 : 0][warp][k][lane] + w0 * cxr[SMOOTH ? (p + 2) % 3 : 0][warp][k][lane] +
-                   w1 * cxr[SMOOTH ? p % 3 : 0][warp][k][lane];  // planes z - 1, z, z + 1
+            cert = w1 * cxr[SMOOTH ? j2 : 0][warp][k][lane] + w0 * cxr[SMOOTH ? j1 : 0][warp][k][lane] +
+                   w1 * cxr[SMOOTH ? j : 0][warp][k][lane];  // planes z - 1, z, z + 1
           const float g = phase_grad(ap[k], cur.a[k], am[k], cp[k], cur.c[k], cm[k]);
           const float cg = cert * g;
           const float wv = cg * g;
@@ -352,12 +365,18 @@ normal_eq_march_kernel(const float2* __restrict__ q1, long long q1_stride, const
         }
       }
     }
-    // [D] rotate the plane registers
-    prev_a2 = cur.a[2];
-    prev_c2 = cur.c[2];
-    cur = nw;
-    if (p + 1 <= z1) nw = nxt;
-    __syncthreads();  // sxr and the qy slot of plane p - 1 are rewritten next step
+    __syncthreads();  // sxr and the qy slot of plane p - 2 are rewritten next step
+  };
+
+  if (!empty) {
+    for (int p = z0 - 1;; p += 3) {
+      step(std::integral_constant<int, 0>(), p, pb0, pb1, pb2);
+      if (p + 1 > z1) break;
+      step(std::integral_constant<int, 1>(), p + 1, pb1, pb2, pb0);
+      if (p + 2 > z1) break;
+      step(std::integral_constant<int, 2>(), p + 2, pb2, pb0, pb1);
+      if (p + 3 > z1) break;
+    }
   }
 
   // expand the column moments into the 42 sums (FP64), warp sums, block sum
