@@ -134,6 +134,63 @@ int brc_ctx::tune_tc(int nfilt, int W, int H, int D, const uint16_t* d_taps, boo
   return BRC_OK;
 }
 
+int brc_ctx::tune_fp32(const float* h_filters, int nfilt, bool sym, int W, int H, int D, int* tz) {
+  sym = sym && brc::filter3d_bank_symmetric(h_filters, nfilt);  // the kernel the launches will take
+  const auto key = std::make_tuple(nfilt + (sym ? 100 : 0), W, H, D);
+  auto it = fp32_tuned.find(key);
+  if (it != fp32_tuned.end()) {
+    *tz = it->second;
+    return BRC_OK;
+  }
+  *tz = brc::filter3d_default_tz(D);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  BRC_TRY(this, cudaStreamIsCapturing(stream(), &cap), "capture status");
+  if (cap != cudaStreamCaptureStatusNone) return BRC_OK;  // no timing inside a capture
+  int cand[8];
+  const int n = brc::filter3d_tz_candidates(cand, 8);
+  // time each z depth on zero-filled scratch volumes (the kernels' work does
+  // not depend on the data, only on the shape and on whether the bank is
+  // even/odd symmetric): one warm launch, best of three
+  const long long V = (long long)W * H * D;
+  long long nb = (1ll << 24) / (V > 0 ? V : 1);
+  nb = nb < 1 ? 1 : (nb > 32 ? 32 : nb);
+  BRC_TRY(this, cudaStreamSynchronize(stream()), "synchronize");
+  BRC_TRY(this, tmp1.ensure(sizeof(float) * (size_t)(V * nb)), "alloc");
+  BRC_TRY(this, tmp2.ensure(sizeof(float) * (size_t)(V * nb) * 2 * nfilt), "alloc");
+  BRC_TRY(this, cudaMemsetAsync(tmp1.ptr, 0, sizeof(float) * (size_t)(V * nb), own_stream), "memset");
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  BRC_TRY(this, cudaEventCreate(&e0), "event");
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return fail(BRC_ERR_CUDA, "event");
+  }
+  float best = -1.f;
+  cudaError_t err = cudaSuccess;
+  for (int c = 0; c < n && err == cudaSuccess; c++) {
+    float ms_best = -1.f;
+    for (int rep = 0; rep < 4 && err == cudaSuccess; rep++) {
+      err = cudaEventRecord(e0, own_stream);
+      if (err == cudaSuccess)
+        err = brc::filter3d_fp32(tmp1.as<float>(), W, H, D, (int)nb, V, h_filters, nfilt, tmp2.as<float>(),
+                                 brc::all_instances(), own_stream, sym, cand[c]);
+      if (err == cudaSuccess) err = cudaEventRecord(e1, own_stream);
+      if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+      if (err == cudaSuccess && rep > 0 && (ms_best < 0.f || ms < ms_best)) ms_best = ms;
+    }
+    if (err == cudaSuccess && (best < 0.f || ms_best < best)) {
+      best = ms_best;
+      *tz = cand[c];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  BRC_TRY(this, err, "z-depth timing");
+  fp32_tuned[key] = *tz;
+  return BRC_OK;
+}
+
 int make_filter_path(brc_ctx* ctx, const float* h_filters, int nfilt, int precision, int W, int H, int D,
                      FilterPath* fp) {
   if (nfilt != 3 && nfilt != 6) return ctx->fail(BRC_ERR_INVALID, "filtering needs 3 or 6 filters");
@@ -142,7 +199,8 @@ int make_filter_path(brc_ctx* ctx, const float* h_filters, int nfilt, int precis
   fp->nfilt = nfilt;
   fp->d_taps = nullptr;
   fp->d_err = ctx->tc_err.as<int>();
-  if (precision == BRC_PREC_FP32 || precision == BRC_PREC_FP32_GENERAL) return BRC_OK;
+  if (precision == BRC_PREC_FP32 || precision == BRC_PREC_FP32_GENERAL)
+    return ctx->tune_fp32(h_filters, nfilt, precision == BRC_PREC_FP32, W, H, D, &fp->tz);
   if (precision != BRC_PREC_BF16X3 && precision != BRC_PREC_TF32)
     return ctx->fail(BRC_ERR_UNSUPPORTED, "unknown precision");
   const bool tf32 = precision == BRC_PREC_TF32;
@@ -161,7 +219,7 @@ cudaError_t run_filter(const FilterPath& fp, const float* vol, int W, int H, int
     return brc::tc::launch(vol, W, H, D, batch, stride, fp.d_taps, fp.nfilt, out, act, fp.d_err, fp.g, st,
                            fp.precision == BRC_PREC_TF32);
   return brc::filter3d_fp32(vol, W, H, D, batch, stride, fp.h_filters, fp.nfilt, out, act, st,
-                            fp.precision == BRC_PREC_FP32);
+                            fp.precision == BRC_PREC_FP32, fp.tz);
 }
 
 extern "C" {

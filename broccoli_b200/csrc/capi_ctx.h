@@ -77,6 +77,7 @@ struct brc_ctx {
   DevBuf smask;   // smoothed certainty of brc_smooth_normalized
   // tensor-core tile height chosen by timing, per (nfilt, W, H, D)
   std::map<std::tuple<int, int, int, int>, int> tc_tuned;
+  std::map<std::tuple<int, int, int, int>, int> fp32_tuned;  // (nfilt + 100 sym, W, H, D) -> z depth
   // host arrays of the debug outputs (brc_ctx_set_debug_outputs)
   bool dbg_on = false;
   brc_debug_outputs dbg{};
@@ -117,6 +118,10 @@ struct brc_ctx {
   // cost model's candidates, timed once per shape (outside stream capture;
   // under capture the cost model's first choice).
   int tune_tc(int nfilt, int W, int H, int D, const uint16_t* d_taps, bool tf32, int* ty);
+  // z depth of the FP32 filtering's output block for this shape and kind
+  // of kernel (even/odd when sym and the bank is symmetric, else general):
+  // the candidates timed once (outside stream capture), then cached.
+  int tune_fp32(const float* h_filters, int nfilt, bool sym, int W, int H, int D, int* tz);
 
   size_t workspace() const {
     return q1.bytes + q2.bytes + aligned.bytes + partials.bytes + ctl.bytes + tmp1.bytes +
@@ -136,6 +141,7 @@ struct FilterPath {
   const uint16_t* d_taps = nullptr;
   brc::tc::Geometry g{};
   int* d_err = nullptr;
+  int tz = 0;  // FP32 filtering: z depth of the output block (0: untimed choice)
 };
 int make_filter_path(brc_ctx* ctx, const float* h_filters, int nfilt, int precision, int W, int H, int D,
                      FilterPath* fp);

@@ -15,6 +15,8 @@
 // Algorithm (what is computed, not how): NonseparableConvolution3D,
 // broccoli_lib.cpp:4974-5027, with the 2D passes of
 // kernelConvolution.cpp:2802-3693.
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace brc {
@@ -412,47 +414,94 @@ static cudaError_t set_smem_attr() {
                               (int)Filter3dCfg<NF, R, TZ>::kSmemBytes);
 }
 
+// z depths of the output block the kernels are instantiated for; the
+// context's tuner times them per volume shape (pick_tz is the untimed
+// choice).
+constexpr int kTzCandidates[] = {2, 3, 4, 6, 8};
+
 // Raises the dynamic shared-memory limit of every instantiation; called
 // once per device when a context is created.
 cudaError_t filter3d_init() {
   cudaError_t e;
-  if ((e = set_smem_attr<3, 8, 3>()) != cudaSuccess) return e;
-  if ((e = set_smem_attr<3, 8, 4>()) != cudaSuccess) return e;
-  if ((e = set_smem_attr<6, 4, 3>()) != cudaSuccess) return e;
-  return set_smem_attr<6, 4, 4>();
+#define BRC_TZ_ATTR(TZ)                                                \
+  if ((e = set_smem_attr<3, 8, TZ>()) != cudaSuccess) return e;        \
+  if ((e = set_smem_attr<6, 4, TZ>()) != cudaSuccess) return e;
+  BRC_TZ_ATTR(2)
+  BRC_TZ_ATTR(3)
+  BRC_TZ_ATTR(4)
+  BRC_TZ_ATTR(6)
+  BRC_TZ_ATTR(8)
+#undef BRC_TZ_ATTR
+  return cudaSuccess;
 }
 
-// Chooses the z depth of the tile: 3 when it divides D exactly and 4 does
-// not (e.g. D = 33), else 4.
+// Chooses the z depth of the tile without timing: 3 when it divides D
+// exactly and 4 does not (e.g. D = 33), else 4.
 static int pick_tz(int D) { return (D % 4 != 0 && D % 3 == 0) ? 3 : 4; }
+
+int filter3d_tz_candidates(int* tz, int max_n) {
+  const int n = (int)(sizeof(kTzCandidates) / sizeof(kTzCandidates[0]));
+  for (int i = 0; i < n && i < max_n; i++) tz[i] = kTzCandidates[i];
+  return n < max_n ? n : max_n;
+}
+
+int filter3d_default_tz(int D) { return pick_tz(D); }
+
+bool filter3d_bank_symmetric(const float* h_filters, int nfilt) {
+  if (nfilt == 3) {
+    SymBank<3> sb;
+    return pack_sym_bank<3>(h_filters, sb);
+  }
+  if (nfilt == 6) {
+    SymBank<6> sb;
+    return pack_sym_bank<6>(h_filters, sb);
+  }
+  return false;
+}
+
+template <typename Launch>
+static cudaError_t dispatch_tz(int tz, Launch launch) {
+  switch (tz) {
+    case 2: return launch(std::integral_constant<int, 2>());
+    case 3: return launch(std::integral_constant<int, 3>());
+    case 4: return launch(std::integral_constant<int, 4>());
+    case 6: return launch(std::integral_constant<int, 6>());
+    case 8: return launch(std::integral_constant<int, 8>());
+    default: return cudaErrorInvalidValue;
+  }
+}
 
 cudaError_t filter3d_fp32(const float* vol, int W, int H, int D, int batch, long long stride,
                           const float* h_filters, int nfilt, float* out, ActiveSet act, cudaStream_t st,
-                          bool allow_symmetric) {
-  const int tz = pick_tz(D);
+                          bool allow_symmetric, int tz) {
+  if (tz <= 0) tz = pick_tz(D);
   if (allow_symmetric && nfilt == 3) {
     SymBank<3> sb;
     if (pack_sym_bank<3>(h_filters, sb))
-      return tz == 3 ? launch_sym<3, 8, 3>(vol, W, H, D, batch, stride, sb, out, act, st)
-                     : launch_sym<3, 8, 4>(vol, W, H, D, batch, stride, sb, out, act, st);
+      return dispatch_tz(tz, [&](auto T) {
+        return launch_sym<3, 8, decltype(T)::value>(vol, W, H, D, batch, stride, sb, out, act, st);
+      });
   }
   if (allow_symmetric && nfilt == 6) {
     SymBank<6> sb;
     if (pack_sym_bank<6>(h_filters, sb))
-      return tz == 3 ? launch_sym<6, 4, 3>(vol, W, H, D, batch, stride, sb, out, act, st)
-                     : launch_sym<6, 4, 4>(vol, W, H, D, batch, stride, sb, out, act, st);
+      return dispatch_tz(tz, [&](auto T) {
+        return launch_sym<6, 4, decltype(T)::value>(vol, W, H, D, batch, stride, sb, out, act, st);
+      });
   }
   if (nfilt == 3) {
     FilterBank<3> bank;
     pack_bank<3>(h_filters, bank);
-    return tz == 3 ? launch_fp32<3, 8, 3>(vol, W, H, D, batch, stride, bank, out, act, st)
-                   : launch_fp32<3, 8, 4>(vol, W, H, D, batch, stride, bank, out, act, st);
+    return dispatch_tz(tz, [&](auto T) {
+      return launch_fp32<3, 8, decltype(T)::value>(vol, W, H, D, batch, stride, bank, out, act, st);
+    });
   }
   if (nfilt == 6) {
     FilterBank<6> bank;
     pack_bank<6>(h_filters, bank);
-    return tz == 3 ? launch_fp32<6, 4, 3>(vol, W, H, D, batch, stride, bank, out, act, st)
-                   : launch_fp32<6, 4, 4>(vol, W, H, D, batch, stride, bank, out, act, st);
+    return dispatch_tz(tz, [&](auto T) {
+      return launch_fp32<6, 4, decltype(T)::value>(vol, W, H, D, batch, stride, bank, out, act, st);
+    });
   }
   return cudaErrorInvalidValue;
 }

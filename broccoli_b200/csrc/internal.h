@@ -8,9 +8,15 @@
 namespace brc {
 // filter3d.cu
 cudaError_t filter3d_init();
+// tz: z depth of the output block (filter3d_tz_candidates), 0 for the
+// untimed choice filter3d_default_tz(D).
 cudaError_t filter3d_fp32(const float* vol, int W, int H, int D, int batch, long long stride,
                           const float* h_filters, int nfilt, float* out, ActiveSet act, cudaStream_t st,
-                          bool allow_symmetric = true);
+                          bool allow_symmetric = true, int tz = 0);
+int filter3d_tz_candidates(int* tz, int max_n);
+int filter3d_default_tz(int D);
+// The bank is even/odd symmetric (the even/odd kernel can take it).
+bool filter3d_bank_symmetric(const float* h_filters, int nfilt);
 // registration.cu
 // Normal equations of batch instances, one CTA per `zpb` interior slices of
 // an instance (the single-call and allocation-free entry points).
