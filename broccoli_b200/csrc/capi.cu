@@ -134,6 +134,67 @@ int brc_ctx::tune_tc(int nfilt, int W, int H, int D, const uint16_t* d_taps, boo
   return BRC_OK;
 }
 
+int brc_ctx::smooth(const float* vol, int W, int H, int D, int batch, const float* fx, const float* fy,
+                    const float* fz, const float* cert, const float* scert, float* tmp1, float* tmp2, float* out,
+                    cudaStream_t st, int accumulate) {
+  const auto key = std::make_tuple(W, H, D, batch, (cert ? 1 : 0) + (scert ? 2 : 0));
+  auto it = smooth_tuned.find(key);
+  if (it != smooth_tuned.end()) {
+    BRC_TRY(this, brc::smooth3d(vol, W, H, D, batch, fx, fy, fz, cert, scert, tmp1, tmp2, out, st, accumulate,
+                                it->second),
+            "smooth3d");
+    return BRC_OK;
+  }
+  const long long V = (long long)W * H * D;
+  const size_t bytes = sizeof(float) * (size_t)V * batch;
+  auto overlaps = [&](const float* a, size_t na) {
+    const char *o0 = reinterpret_cast<const char*>(out), *a0 = reinterpret_cast<const char*>(a);
+    return a != nullptr && o0 < a0 + na && a0 < o0 + bytes;
+  };
+  const bool alias = overlaps(vol, bytes) || overlaps(cert, sizeof(float) * (size_t)V) ||
+                     overlaps(scert, sizeof(float) * (size_t)V);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  BRC_TRY(this, cudaStreamIsCapturing(st, &cap), "capture status");
+  int cand[8];
+  const int n = brc::smooth3d_chunk_candidates(D, cand, 8);
+  if (alias || accumulate || cap != cudaStreamCaptureStatusNone || n < 2) {
+    BRC_TRY(this, brc::smooth3d(vol, W, H, D, batch, fx, fy, fz, cert, scert, tmp1, tmp2, out, st, accumulate),
+            "smooth3d");
+    return BRC_OK;
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  BRC_TRY(this, cudaEventCreate(&e0), "event");
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return fail(BRC_ERR_CUDA, "event");
+  }
+  float best = -1.f;
+  int zbest = cand[0];
+  cudaError_t err = cudaSuccess;
+  for (int c = 0; c < n && err == cudaSuccess; c++) {
+    float ms_best = -1.f;
+    for (int rep = 0; rep < 3 && err == cudaSuccess; rep++) {
+      err = cudaEventRecord(e0, st);
+      if (err == cudaSuccess)
+        err = brc::smooth3d(vol, W, H, D, batch, fx, fy, fz, cert, scert, tmp1, tmp2, out, st, 0, cand[c]);
+      if (err == cudaSuccess) err = cudaEventRecord(e1, st);
+      if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+      if (err == cudaSuccess && rep > 0 && (ms_best < 0.f || ms < ms_best)) ms_best = ms;
+    }
+    if (err == cudaSuccess && (best < 0.f || ms_best < best)) {
+      best = ms_best;
+      zbest = cand[c];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  BRC_TRY(this, err, "z-chunk timing");
+  smooth_tuned[key] = zbest;
+  return BRC_OK;
+}
+
 int brc_ctx::tune_fp32(const float* h_filters, int nfilt, bool sym, int W, int H, int D, int* tz) {
   sym = sym && brc::filter3d_bank_symmetric(h_filters, nfilt);  // the kernel the launches will take
   const auto key = std::make_tuple(nfilt + (sym ? 100 : 0), W, H, D);
@@ -428,9 +489,11 @@ int brc_smooth3d(brc_ctx* ctx, const float* d_vol, int W, int H, int D, int batc
   const size_t bytes = sizeof(float) * (size_t)W * H * D * batch;
   BRC_TRY(ctx, ctx->tmp1.ensure(bytes), "alloc");
   BRC_TRY(ctx, ctx->tmp2.ensure(bytes), "alloc");
-  BRC_TRY(ctx, brc::smooth3d(d_vol, W, H, D, batch, h_fx, h_fy, h_fz, d_cert, d_scert,
-                             ctx->tmp1.as<float>(), ctx->tmp2.as<float>(), d_out, ctx->stream()),
-          "smooth3d");
+  {
+    const int s = ctx->smooth(d_vol, W, H, D, batch, h_fx, h_fy, h_fz, d_cert, d_scert, ctx->tmp1.as<float>(),
+                              ctx->tmp2.as<float>(), d_out, ctx->stream());
+    if (s != BRC_OK) return s;
+  }
   ctx->launches += 1;
   return BRC_OK;
 }
@@ -449,12 +512,12 @@ int brc_smooth_normalized(brc_ctx* ctx, const float* d_vols, int W, int H, int D
   const cudaStream_t st = ctx->stream();
   // smoothed certainty (all-ones certainty), then the certainty-weighted
   // smoothing of every volume divided by it, then the mask product
-  BRC_TRY(ctx, brc::smooth3d(d_mask, W, H, D, 1, h_fx, h_fy, h_fz, nullptr, nullptr, ctx->tmp1.as<float>(),
-                             ctx->tmp2.as<float>(), ctx->smask.as<float>(), st),
-          "smooth mask");
-  BRC_TRY(ctx, brc::smooth3d(d_vols, W, H, D, T, h_fx, h_fy, h_fz, d_mask, ctx->smask.as<float>(),
-                             ctx->tmp1.as<float>(), ctx->tmp2.as<float>(), d_out, st),
-          "smooth volumes");
+  int s = ctx->smooth(d_mask, W, H, D, 1, h_fx, h_fy, h_fz, nullptr, nullptr, ctx->tmp1.as<float>(),
+                      ctx->tmp2.as<float>(), ctx->smask.as<float>(), st);
+  if (s != BRC_OK) return s;
+  s = ctx->smooth(d_vols, W, H, D, T, h_fx, h_fy, h_fz, d_mask, ctx->smask.as<float>(), ctx->tmp1.as<float>(),
+                  ctx->tmp2.as<float>(), d_out, st);
+  if (s != BRC_OK) return s;
   BRC_TRY(ctx, brc::multiply_mask(d_out, d_mask, V, T, st), "multiply mask");
   ctx->launches += 3;
   return BRC_OK;

@@ -78,6 +78,7 @@ struct brc_ctx {
   // tensor-core tile height chosen by timing, per (nfilt, W, H, D)
   std::map<std::tuple<int, int, int, int>, int> tc_tuned;
   std::map<std::tuple<int, int, int, int>, int> fp32_tuned;  // (nfilt + 100 sym, W, H, D) -> z depth
+  std::map<std::tuple<int, int, int, int, int>, int> smooth_tuned;  // (W, H, D, batch, cert kind) -> z chunk
   // host arrays of the debug outputs (brc_ctx_set_debug_outputs)
   bool dbg_on = false;
   brc_debug_outputs dbg{};
@@ -122,6 +123,14 @@ struct brc_ctx {
   // of kernel (even/odd when sym and the bank is symmetric, else general):
   // the candidates timed once (outside stream capture), then cached.
   int tune_fp32(const float* h_filters, int nfilt, bool sym, int W, int H, int D, int* tz);
+  // brc::smooth3d with the z chunk tuned per (shape, batch, certainty
+  // kind): the first call of a key that writes a buffer it does not read
+  // and does not accumulate (outside stream capture) runs every candidate
+  // on its own buffers (the result is the same for each) and keeps the
+  // fastest; other calls take the tuned or the untimed choice.
+  int smooth(const float* vol, int W, int H, int D, int batch, const float* fx, const float* fy, const float* fz,
+             const float* cert, const float* scert, float* tmp1, float* tmp2, float* out, cudaStream_t st,
+             int accumulate = 0);
 
   size_t workspace() const {
     return q1.bytes + q2.bytes + aligned.bytes + partials.bytes + ctl.bytes + tmp1.bytes +

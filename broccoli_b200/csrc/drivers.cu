@@ -54,19 +54,16 @@ static int nonlinear_step(brc_ctx* ctx, const float* q1, const float* q2, int G,
   // every smoothing writes a buffer it does not read
   float* raw = ctx->tmp2.as<float>();
   BRC_TRY(ctx, brc::tensor_components(q2, V, m36, raw, st, G), "tensor_components");
-  BRC_TRY(ctx, brc::smooth3d(raw, W, H, D, 6 * G, ft, ft, ft, nullptr, nullptr, ctx->tmp1.as<float>(), nullptr, t6,
-                             st),
-          "smooth T");
+  int s = ctx->smooth(raw, W, H, D, 6 * G, ft, ft, ft, nullptr, nullptr, ctx->tmp1.as<float>(), nullptr, t6, st);
+  if (s != BRC_OK) return s;
   BRC_TRY(ctx, brc::tensor_norm_max(t6, V, raw, maxbits, st, G, 6 * V, 9 * V), "tensor_norm_max");
   BRC_TRY(ctx, brc::nonlinear_ah(q1, q2, t6, V, maxbits, m36, dirs18, raw, raw + 6 * V, st, G, 9 * V),
           "nonlinear_ah");
-  BRC_TRY(ctx, brc::smooth3d(raw, W, H, D, 9 * G, fe, fe, fe, nullptr, nullptr, ctx->tmp1.as<float>(), nullptr, ah,
-                             st),
-          "smooth A,h");
+  s = ctx->smooth(raw, W, H, D, 9 * G, fe, fe, fe, nullptr, nullptr, ctx->tmp1.as<float>(), nullptr, ah, st);
+  if (s != BRC_OK) return s;
   BRC_TRY(ctx, brc::displacement_update(ah, ah + 6 * V, V, fp64, d3, st, G, 9 * V), "displacement_update");
-  BRC_TRY(ctx, brc::smooth3d(d3, W, H, D, 3 * G, fd, fd, fd, nullptr, nullptr, ctx->tmp1.as<float>(), nullptr, field,
-                             st, 1),
-          "smooth update");
+  s = ctx->smooth(d3, W, H, D, 3 * G, fd, fd, fd, nullptr, nullptr, ctx->tmp1.as<float>(), nullptr, field, st, 1);
+  if (s != BRC_OK) return s;
   ctx->launches += 7;
   return BRC_OK;
 }

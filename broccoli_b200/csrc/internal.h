@@ -51,9 +51,13 @@ cudaError_t warp_field(const float* src, int W, int H, int D, const float* dx, c
                        long long field_stride = 0, long long out_stride = 0);
 cudaError_t rescale_linear(const float* src, int W, int H, int D, float* out, int W2, int H2, int D2,
                            cudaStream_t st);
+// zchunk: planes per z chunk of a CTA (0: the untimed choice
+// smooth3d_default_chunk); every choice gives the same result.
 cudaError_t smooth3d(const float* vol, int W, int H, int D, int batch, const float* fx,
                      const float* fy, const float* fz, const float* cert, const float* scert,
-                     float* tmp1, float* tmp2, float* out, cudaStream_t st, int accumulate = 0);
+                     float* tmp1, float* tmp2, float* out, cudaStream_t st, int accumulate = 0, int zchunk = 0);
+int smooth3d_default_chunk(int W, int H, int D, int batch);
+int smooth3d_chunk_candidates(int D, int* zc, int max_n);
 // out[i] = phase_atan2(y[i], x[i]) (the arctangent of the phase kernels).
 cudaError_t phase_atan2_eval(const float* y, const float* x, float* out, long long n, cudaStream_t st);
 cudaError_t multiply_mask(float* vols, const float* mask, long long V, int batch, cudaStream_t st);

@@ -1312,9 +1312,26 @@ static const void* smooth_kernel_of(int v) {
   return table[v];
 }
 
+int smooth3d_default_chunk(int W, int H, int D, int batch) {
+  const long long ntiles = (long long)((W + kSmTX - 1) / kSmTX) * ((H + kSmTY - 1) / kSmTY);
+  return smooth_chunk(D, ntiles * batch);
+}
+
+int smooth3d_chunk_candidates(int D, int* zc, int max_n) {
+  // D split into 1, 2, 3, 4, 6 or 8 chunks of at least 8 planes
+  static const int parts[] = {1, 2, 3, 4, 6, 8};
+  int n = 0;
+  for (int c : parts) {
+    const int z = (D + c - 1) / c;
+    if (n >= max_n || (c > 1 && z < 8)) break;
+    if (n == 0 || zc[n - 1] != z) zc[n++] = z;
+  }
+  return n;
+}
+
 cudaError_t smooth3d(const float* vol, int W, int H, int D, int batch, const float* fx,
                      const float* fy, const float* fz, const float* cert, const float* scert,
-                     float* tmp1, float* tmp2, float* out, cudaStream_t st, int accumulate) {
+                     float* tmp1, float* tmp2, float* out, cudaStream_t st, int accumulate, int zchunk) {
   const long long V = (long long)W * H * D;
   Taps9 tx, ty, tz;
   for (int i = 0; i < 9; i++) {
@@ -1334,7 +1351,7 @@ cudaError_t smooth3d(const float* vol, int W, int H, int D, int batch, const flo
   float* dst = alias ? tmp1 : out;
   const long long ntiles = (long long)((W + kSmTX - 1) / kSmTX) * ((H + kSmTY - 1) / kSmTY);
   if (ntiles > 0x7fffffffLL || batch > 65535 || V > kMaxVoxels) return cudaErrorInvalidValue;
-  const int zc = smooth_chunk(D, ntiles * batch);
+  const int zc = zchunk > 0 ? (zchunk < D ? zchunk : D) : smooth_chunk(D, ntiles * batch);
   const dim3 grid((unsigned)ntiles, (unsigned)((D + zc - 1) / zc), (unsigned)batch);
   // the dynamic shared memory above 48 KB is a per-device function attribute
   static bool attr_set[64] = {false};
