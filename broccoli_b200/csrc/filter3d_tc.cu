@@ -44,7 +44,7 @@
 //                  descriptors built once and advanced by adds (every cycle
 //                  of address arithmetic in this thread delays the GEMMs)
 //   warp 2, lane 0 streams the packed taps, two stages (16 KB: hi + lo of
-//                  each) per slot, through a 4-slot ring with cp.async.bulk
+//                  each) per slot, through a 3-slot ring with cp.async.bulk
 //                  + mbarriers (one wait and one commit per six GEMMs)
 //   warps 4-7      epilogue: tcgen05.ld of the accumulator (TMEM lanes
 //                  32 (warp - 4) ..), transposed through shared memory into
@@ -68,7 +68,7 @@ namespace tc {
 
 constexpr int kThreads = 384;        // 12 warps, roles above
 constexpr int kStageWarp = 8;        // first staging warp
-constexpr int kRing = 4;             // tap slots in flight (two stages each)
+constexpr int kRing = 3;             // tap slots in flight (two stages each; 2, 4, 5, 6 measured slower)
 constexpr int kEpiCols = 64;         // accumulator columns per epilogue chunk
 constexpr uint32_t kTmemCols = 512;  // two accumulators of up to 256 columns
 constexpr int kStageHalves = kM * kK;              // BF16 elements of one A (hi or lo)
