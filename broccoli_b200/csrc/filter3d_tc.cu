@@ -38,17 +38,19 @@
 // One persistent CTA per SM walks the tiles of the launch (10 x positions x
 // Ty rows x SP*J planes of one volume each) with its warps specialised:
 //
-//   warps 8-11     stage a tile's input (FP32 -> BF16 hi/lo rows) into one
-//                  of two shared-memory buffers while the GEMMs read the other
+//   warps 12-19    stage a tile's input (FP32 -> BF16 hi/lo or TF32 rows)
+//                  into one of two shared-memory buffers while the GEMMs
+//                  read the other
 //   warp 1, lane 0 issues the tcgen05.mma's: three split products per stage,
 //                  descriptors built once and advanced by adds (every cycle
 //                  of address arithmetic in this thread delays the GEMMs)
 //   warp 2, lane 0 streams the packed taps, two stages (16 KB: hi + lo of
 //                  each) per slot, through a 3-slot ring with cp.async.bulk
 //                  + mbarriers (one wait and one commit per six GEMMs)
-//   warps 4-7      epilogue: tcgen05.ld of the accumulator (TMEM lanes
-//                  32 (warp - 4) ..), transposed through shared memory into
-//                  16-byte stores of the complex outputs
+//   warps 4-11     epilogue: tcgen05.ld of the accumulator (TMEM lanes
+//                  32 (warp % 4) .., the two warps of a lane quarter on
+//                  alternate 16-column groups), transposed through shared
+//                  memory into 16-byte stores of the complex outputs
 //
 // Two TMEM accumulators (2 x 256 of the SM's 512 columns) let the epilogue
 // of tile i run under the GEMMs of tile i + 1.  Every wait is bounded
@@ -66,8 +68,15 @@
 namespace brc {
 namespace tc {
 
-constexpr int kThreads = 384;        // 12 warps, roles above
-constexpr int kStageWarp = 8;        // first staging warp
+// Group sizes measured on 199 volumes of 64x64x33 (TF32 / BF16X3 ms):
+// 4 + 4 warps 0.58 / 0.72, 8 + 4 0.57 / 0.74, 4 + 8 0.66 / 0.72, 8 + 8
+// 0.534 / 0.696, 12 + 8 and 8 + 12 0.54-0.55 / 0.70.
+constexpr int kEpiWarps = 8;         // epilogue warps (a multiple of 4: kEpiWarps / 4 per TMEM lane quarter)
+constexpr int kStageWarps = 8;       // staging warps
+constexpr int kStageWarp = 4 + kEpiWarps;                    // first staging warp
+constexpr int kThreads = 32 * (4 + kEpiWarps + kStageWarps);  // roles above
+constexpr int kEpiThreads = 32 * kEpiWarps, kStageThreads = 32 * kStageWarps;
+constexpr int kEpiGroups = kEpiThreads / 30;  // accumulator columns stored at once (30 pieces each)
 constexpr int kRing = 3;             // tap slots in flight (two stages each; 2, 4, 5, 6 measured slower)
 constexpr int kEpiCols = 64;         // accumulator columns per epilogue chunk
 constexpr uint32_t kTmemCols = 512;  // two accumulators of up to 256 columns
@@ -182,8 +191,8 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
 }
 
 // Named barriers of the 128-thread groups (0 is __syncthreads).
-__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
-__device__ __forceinline__ void stage_sync() { asm volatile("bar.sync 2, 128;" ::: "memory"); }
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kEpiThreads) : "memory"); }
+__device__ __forceinline__ void stage_sync() { asm volatile("bar.sync 2, %0;" ::"n"(kStageThreads) : "memory"); }
 
 struct TileArgs {
   long long vstride;       // floats between volumes
@@ -254,10 +263,10 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
 
   if (tid == 0) {
     for (int i = 0; i < 2; i++) {
-      mbar_init(&full_in[i], 128);
+      mbar_init(&full_in[i], kStageThreads);
       mbar_init(&empty_in[i], 1);
       mbar_init(&acc_full[i], 1);
-      mbar_init(&acc_empty[i], 128);
+      mbar_init(&acc_empty[i], kEpiThreads);
     }
     for (int s = 0; s < kRing; s++) {
       mbar_init(&tfull[s], 1);
@@ -307,7 +316,7 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
       const bool vec_rows = (a.W & 3) == 0 && (reinterpret_cast<uintptr_t>(src) & 15) == 0;
       uint8_t* hi = inb + (uint32_t)(buf * 4) * rowbytes;
       uint8_t* lo = hi + 2u * rowbytes;
-      for (int item = st; item < 2 * nrows; item += 128) {
+      for (int item = st; item < 2 * nrows; item += kStageThreads) {
         const int kh = item >= nrows ? 1 : 0, row = item - kh * nrows;
         const int par = row / prow, rr = row - par * prow;
         const int qq = rr / g.Hp, yl = rr - qq * g.Hp;
@@ -477,9 +486,10 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
     }
     flags[2] = (int)G;
     if (!ok) flags[4] = 1;
-  } else if (warp >= 4 && warp < 8) {
-    // ---- epilogue
-    const int q = warp - 4;
+  } else if (warp >= 4 && warp < 4 + kEpiWarps) {
+    // ---- epilogue: warp w reads TMEM lane quarter w % 4; with 8 warps the
+    // two of a quarter take alternate 16-column groups
+    const int q = (warp - 4) & 3, half = (warp - 4) >> 2;
     const int r = q * 32 + lane;
     int sp, f, xo;
     bool rvalid;
@@ -499,8 +509,8 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
     const int ke = (f >> 1) * 20 + xo * 2 + (f & 1);
     const int et = tid - 128;
     // stores: SP * nfilt * 5 = 30 16-byte pieces per accumulator column
-    // (plane s2, filter k, x pair); threads et < 120 take piece et % 30 of
-    // every fourth column, starting at column et / 30
+    // (plane s2, filter k, x pair); threads et < 30 kEpiGroups take piece
+    // et % 30 of every kEpiGroups-th column, starting at column et / 30
     const int piece = et % 30, cgrp = et / 30;
     const int part = piece % 5, sk = piece / 5;
     const int s2 = sk / a.nfilt, k = sk - s2 * a.nfilt;
@@ -511,7 +521,7 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
       int b, zt, yt, xc;
       decode_tile(a, act, t, b, zt, yt, xc);
       const int acc = i & 1;
-      // one thread waits and tells the other 127, so that all of them leave
+      // one thread waits and tells the others, so that all of them leave
       // together if the wait gives up (they meet at named barriers below)
       if (et == 0) flags[5] = mbar_wait(&acc_full[acc], (uint32_t)(i >> 1) & 1u) ? 1 : 0;
       epi_sync();
@@ -526,7 +536,7 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
       const uint32_t lanecol = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * 256);
       for (int cbase = 0; cbase < g.N; cbase += kEpiCols) {
         const int cend = cbase + kEpiCols < g.N ? cbase + kEpiCols : g.N;
-        for (int c0 = cbase; c0 < cend; c0 += 16) {
+        for (int c0 = cbase + 16 * half; c0 < cend; c0 += 16 * (kEpiWarps / 4)) {
           uint32_t v[16];
           tmem_ld16(lanecol + (uint32_t)c0, v);
           if (rvalid) {
@@ -540,11 +550,11 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
           mbar_arrive(&acc_empty[acc]);
         }
         epi_sync();
-        if (et < 120) {
+        if (et < 30 * kEpiGroups) {
           int nl = cgrp;
           int j = (cbase + nl) / g.Hp, yl = cbase + nl - j * g.Hp;
           const int xs = x0 + 2 * part;
-          for (; nl < cend - cbase; nl += 4) {
+          for (; nl < cend - cbase; nl += kEpiGroups) {
             const int z = z0 + j * g.SP + s2, y = y0 + yl;
             if (j < g.J && yl < g.Ty && y < a.H && z < a.D && xs < a.W) {
               const float4 qv = *reinterpret_cast<const float4*>(E + (nl * g.SP + s2) * rowf + k * 20 + part * 4);
@@ -556,10 +566,14 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
                 if (xs + 1 < a.W) *reinterpret_cast<float2*>(dst + 2) = make_float2(qv.z, qv.w);
               }
             }
-            yl += 4;  // Hp >= 7 > 4: at most one wrap
+            yl += kEpiGroups;  // Hp >= 7 and kEpiGroups <= 12: at most two wraps
             if (yl >= g.Hp) {
               yl -= g.Hp;
               j++;
+              if (yl >= g.Hp) {
+                yl -= g.Hp;
+                j++;
+              }
             }
           }
         }
