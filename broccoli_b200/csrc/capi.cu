@@ -136,7 +136,7 @@ int brc_ctx::tune_tc(int nfilt, int W, int H, int D, const uint16_t* d_taps, boo
 
 int brc_ctx::smooth(const float* vol, int W, int H, int D, int batch, const float* fx, const float* fy,
                     const float* fz, const float* cert, const float* scert, float* tmp1, float* tmp2, float* out,
-                    cudaStream_t st, int accumulate) {
+                    cudaStream_t st, int accumulate, float* tune_out) {
   const auto key = std::make_tuple(W, H, D, batch, (cert ? 1 : 0) + (scert ? 2 : 0));
   auto it = smooth_tuned.find(key);
   if (it != smooth_tuned.end()) {
@@ -147,17 +147,20 @@ int brc_ctx::smooth(const float* vol, int W, int H, int D, int batch, const floa
   }
   const long long V = (long long)W * H * D;
   const size_t bytes = sizeof(float) * (size_t)V * batch;
+  // the timing runs write `dst`: the output itself, or tune_out for an
+  // accumulating call
+  float* dst = accumulate ? tune_out : out;
   auto overlaps = [&](const float* a, size_t na) {
-    const char *o0 = reinterpret_cast<const char*>(out), *a0 = reinterpret_cast<const char*>(a);
+    const char *o0 = reinterpret_cast<const char*>(dst), *a0 = reinterpret_cast<const char*>(a);
     return a != nullptr && o0 < a0 + na && a0 < o0 + bytes;
   };
-  const bool alias = overlaps(vol, bytes) || overlaps(cert, sizeof(float) * (size_t)V) ||
-                     overlaps(scert, sizeof(float) * (size_t)V);
+  const bool alias = dst == nullptr || overlaps(vol, bytes) || overlaps(cert, sizeof(float) * (size_t)V) ||
+                     overlaps(scert, sizeof(float) * (size_t)V) || (accumulate && overlaps(out, bytes));
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   BRC_TRY(this, cudaStreamIsCapturing(st, &cap), "capture status");
   int cand[8];
   const int n = brc::smooth3d_chunk_candidates(D, cand, 8);
-  if (alias || accumulate || cap != cudaStreamCaptureStatusNone || n < 2) {
+  if (alias || cap != cudaStreamCaptureStatusNone || n < 2) {
     BRC_TRY(this, brc::smooth3d(vol, W, H, D, batch, fx, fy, fz, cert, scert, tmp1, tmp2, out, st, accumulate),
             "smooth3d");
     return BRC_OK;
@@ -176,7 +179,7 @@ int brc_ctx::smooth(const float* vol, int W, int H, int D, int batch, const floa
     for (int rep = 0; rep < 3 && err == cudaSuccess; rep++) {
       err = cudaEventRecord(e0, st);
       if (err == cudaSuccess)
-        err = brc::smooth3d(vol, W, H, D, batch, fx, fy, fz, cert, scert, tmp1, tmp2, out, st, 0, cand[c]);
+        err = brc::smooth3d(vol, W, H, D, batch, fx, fy, fz, cert, scert, tmp1, tmp2, dst, st, 0, cand[c]);
       if (err == cudaSuccess) err = cudaEventRecord(e1, st);
       if (err == cudaSuccess) err = cudaEventSynchronize(e1);
       float ms = 0.f;
@@ -192,6 +195,9 @@ int brc_ctx::smooth(const float* vol, int W, int H, int D, int batch, const floa
   cudaEventDestroy(e1);
   BRC_TRY(this, err, "z-chunk timing");
   smooth_tuned[key] = zbest;
+  if (accumulate)
+    BRC_TRY(this, brc::smooth3d(vol, W, H, D, batch, fx, fy, fz, cert, scert, tmp1, tmp2, out, st, accumulate, zbest),
+            "smooth3d");
   return BRC_OK;
 }
 

@@ -127,10 +127,13 @@ struct brc_ctx {
   // kind): the first call of a key that writes a buffer it does not read
   // and does not accumulate (outside stream capture) runs every candidate
   // on its own buffers (the result is the same for each) and keeps the
-  // fastest; other calls take the tuned or the untimed choice.
+  // fastest; an accumulating call given tune_out (batch volumes that
+  // overlap nothing and may be overwritten) times the candidates without
+  // accumulation into tune_out first.  Other calls take the tuned or the
+  // untimed choice.
   int smooth(const float* vol, int W, int H, int D, int batch, const float* fx, const float* fy, const float* fz,
              const float* cert, const float* scert, float* tmp1, float* tmp2, float* out, cudaStream_t st,
-             int accumulate = 0);
+             int accumulate = 0, float* tune_out = nullptr);
 
   size_t workspace() const {
     return q1.bytes + q2.bytes + aligned.bytes + partials.bytes + ctl.bytes + tmp1.bytes +

@@ -62,7 +62,10 @@ static int nonlinear_step(brc_ctx* ctx, const float* q1, const float* q2, int G,
   s = ctx->smooth(raw, W, H, D, 9 * G, fe, fe, fe, nullptr, nullptr, ctx->tmp1.as<float>(), nullptr, ah, st);
   if (s != BRC_OK) return s;
   BRC_TRY(ctx, brc::displacement_update(ah, ah + 6 * V, V, fp64, d3, st, G, 9 * V), "displacement_update");
-  s = ctx->smooth(d3, W, H, D, 3 * G, fd, fd, fd, nullptr, nullptr, ctx->tmp1.as<float>(), nullptr, field, st, 1);
+  // the unsmoothed A, h in raw are consumed: raw takes the chunk timing of
+  // the accumulating smoothing
+  s = ctx->smooth(d3, W, H, D, 3 * G, fd, fd, fd, nullptr, nullptr, ctx->tmp1.as<float>(), nullptr, field, st, 1,
+                  raw);
   if (s != BRC_OK) return s;
   ctx->launches += 7;
   return BRC_OK;
