@@ -330,6 +330,8 @@ int brc_ctx_create(int device, brc_ctx** out) {
   if (brc::filter3d_init() != cudaSuccess || brc::tc::init() != cudaSuccess) return BRC_ERR_CUDA;
   if (ctx->tc_err.ensure(16) != cudaSuccess || cudaMemset(ctx->tc_err.ptr, 0, 16) != cudaSuccess)
     return BRC_ERR_NOMEM;
+  if (ctx->iters_run.ensure(16) != cudaSuccess || cudaMemset(ctx->iters_run.ptr, 0, 16) != cudaSuccess)
+    return BRC_ERR_NOMEM;
   *out = ctx.release();
   return BRC_OK;
 }
@@ -355,6 +357,7 @@ int brc_ctx_destroy(brc_ctx* ctx) {
     cudaStreamDestroy(ctx->copy_out);
   }
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  if (ctx->body_stream) cudaStreamDestroy(ctx->body_stream);
   delete ctx;
   return BRC_OK;
 }
@@ -400,7 +403,18 @@ int brc_selftest_phase_atan2(brc_ctx* ctx, const float* d_y, const float* d_x, f
 
 size_t brc_ctx_workspace_bytes(const brc_ctx* ctx) { return ctx ? ctx->workspace() : 0; }
 
-unsigned long long brc_ctx_kernel_launches(const brc_ctx* ctx) { return ctx ? ctx->launches : 0; }
+unsigned long long brc_ctx_kernel_launches(const brc_ctx* ctx) {
+  if (!ctx) return 0;
+  // the kernels of the graph-run loop iterations: 5 per iteration the
+  // device ran (filtering, normal equations, solve, warp, control)
+  unsigned long long it = 0;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream());
+  cudaStreamSynchronize(ctx->own_stream);
+  if (ctx->iters_run.ptr && cudaMemcpy(&it, ctx->iters_run.ptr, sizeof(it), cudaMemcpyDeviceToHost) != cudaSuccess)
+    it = 0;
+  return ctx->launches + 5ull * it;
+}
 
 int brc_filter3d(brc_ctx* ctx, const float* d_vol, int W, int H, int D, int batch,
                  long long vol_stride, const float* h_filters, int nfilt, int precision,
@@ -634,6 +648,7 @@ struct RegPlan {
   int* status;
   int* lists;   // 3 x batch: active instances of iterations it % 3
   int* counts;  // their lengths
+  const int* iter;  // the iteration being run (device counter)
   int nblk;     // partial rows per instance of the normal-equation kernel
   FilterPath fpath;
 };
@@ -651,7 +666,7 @@ long long enqueue_registration(brc_ctx* ctx, const RegPlan& p, cudaStream_t st) 
     return ctx->cuda(e, "memset ctl");
   if ((e = cudaMemsetAsync(p.iters_ws, 0, sizeof(int) * p.batch, st)) != cudaSuccess)
     return ctx->cuda(e, "memset ctl");
-  if ((e = cudaMemsetAsync(p.status, 0, sizeof(int), st)) != cudaSuccess) return ctx->cuda(e, "memset");
+  if ((e = cudaMemsetAsync(p.status, 0, sizeof(int) * 2, st)) != cudaSuccess) return ctx->cuda(e, "memset");
   if ((e = brc::active_init(p.lists, p.counts, p.batch, st)) != cudaSuccess) return ctx->cuda(e, "active set");
   kernels++;
   if (p.rotations && (e = cudaMemsetAsync(p.rotations, 0, sizeof(float) * 3 * p.batch, st)) != cudaSuccess)
@@ -664,26 +679,76 @@ long long enqueue_registration(brc_ctx* ctx, const RegPlan& p, cudaStream_t st) 
       (e = cudaMemcpyAsync(p.aligned, p.moving, sizeof(float) * V * p.batch, cudaMemcpyDeviceToDevice,
                            st)) != cudaSuccess)
     return ctx->cuda(e, "copy");
-  for (int it = 0; it < p.opts.iterations; it++) {
-    const float* cur = it == 0 ? p.moving : p.aligned;
-    // iteration it works on list it % 3; its solve fills list (it + 1) % 3
-    // and empties list (it + 2) % 3 (the one iteration it - 1 used)
-    const int c0 = it % 3, c1 = (it + 1) % 3, c2 = (it + 2) % 3;
-    const brc::ActiveSet act{p.lists + (long long)c0 * p.batch, p.counts + c0};
-    if ((e = run_filter(p.fpath, cur, p.W, p.H, p.D, p.batch, V, p.q2, act, st)) != cudaSuccess)
-      return ctx->cuda(e, "filter3d");
-    if ((e = brc::normal_eq_march(p.q1, p.ref_stride ? 6 * V : 0, p.q2, p.W, p.H, p.D, p.batch, p.partials,
-                                  p.nblk, act, st, p.opts.certainty_sigma_x100 / 100.0f)) != cudaSuccess)
-      return ctx->cuda(e, "normal_eq");
-    if ((e = brc::solve_update(p.partials, p.nblk, p.batch, p.opts.type, p.opts.tolerance, p.W, p.H, p.D,
-                               p.params, p.rotations, p.conv_iter, p.iters_ws, p.status, it, act,
-                               p.lists + (long long)c1 * p.batch, p.counts + c1, p.counts + c2, st)) !=
-        cudaSuccess)
-      return ctx->cuda(e, "solve");
-    if ((e = brc::warp_affine(p.moving, V, p.W, p.H, p.D, p.batch, p.params, p.aligned, V, act, st)) !=
-        cudaSuccess)
-      return ctx->cuda(e, "warp");
-    kernels += 3 + filter_launches(p.fpath);
+  if (p.opts.iterations > 0) {
+    // the iteration runs on the device's counter p.iter (set to 0 above);
+    // iteration 0 filters the moving volumes themselves, later ones their
+    // warps: the first iteration is enqueued on its own
+    const brc::ActiveSet act{p.lists, p.counts, p.iter, p.batch};
+    int* iter = const_cast<int*>(p.iter);
+    auto one_iteration = [&](cudaStream_t s, const float* cur, bool cond_node, cudaGraphConditionalHandle h) -> long long {
+      cudaError_t ee;
+      if ((ee = run_filter(p.fpath, cur, p.W, p.H, p.D, p.batch, V, p.q2, act, s)) != cudaSuccess)
+        return ctx->cuda(ee, "filter3d");
+      if ((ee = brc::normal_eq_march(p.q1, p.ref_stride ? 6 * V : 0, p.q2, p.W, p.H, p.D, p.batch, p.partials,
+                                     p.nblk, act, s, p.opts.certainty_sigma_x100 / 100.0f)) != cudaSuccess)
+        return ctx->cuda(ee, "normal_eq");
+      if ((ee = brc::solve_update(p.partials, p.nblk, p.batch, p.opts.type, p.opts.tolerance, p.W, p.H, p.D,
+                                  p.params, p.rotations, p.conv_iter, p.iters_ws, p.status, act, p.lists, p.counts,
+                                  s)) != cudaSuccess)
+        return ctx->cuda(ee, "solve");
+      if ((ee = brc::warp_affine(p.moving, V, p.W, p.H, p.D, p.batch, p.params, p.aligned, V, act, s)) !=
+          cudaSuccess)
+        return ctx->cuda(ee, "warp");
+      if ((ee = brc::iteration_control(iter, p.counts, p.opts.iterations, h, cond_node,
+                                       ctx->iters_run.as<unsigned long long>(), s)) != cudaSuccess)
+        return ctx->cuda(ee, "iteration control");
+      return 4 + filter_launches(p.fpath);
+    };
+    long long k0 = one_iteration(st, p.moving, false, 0);
+    if (k0 < 0) return k0;
+    kernels += k0;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if ((e = cudaStreamIsCapturing(st, &cs)) != cudaSuccess) return ctx->cuda(e, "capture status");
+    if (cs == cudaStreamCaptureStatusActive && p.opts.iterations > 1) {
+      // iterations 1 .. while instances remain: one conditional WHILE node
+      // whose body is one iteration, its condition set on the device by the
+      // control kernel (the loop stops as soon as every instance converged)
+      cudaGraph_t graph = nullptr;
+      const cudaGraphNode_t* deps = nullptr;
+      size_t ndeps = 0;
+      if ((e = cudaStreamGetCaptureInfo(st, &cs, nullptr, &graph, &deps, &ndeps)) != cudaSuccess)
+        return ctx->cuda(e, "capture info");
+      cudaGraphConditionalHandle h;
+      if ((e = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess)
+        return ctx->cuda(e, "conditional handle");
+      cudaGraphNodeParams cp = {};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = h;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      cudaGraphNode_t node;
+      if ((e = cudaGraphAddNode(&node, graph, deps, ndeps, &cp)) != cudaSuccess) return ctx->cuda(e, "while node");
+      if ((e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies)) != cudaSuccess)
+        return ctx->cuda(e, "capture dependencies");
+      if (!ctx->body_stream &&
+          (e = cudaStreamCreateWithFlags(&ctx->body_stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return ctx->cuda(e, "body stream");
+      if ((e = cudaStreamBeginCaptureToGraph(ctx->body_stream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                             cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+        return ctx->cuda(e, "body capture");
+      const long long kb = one_iteration(ctx->body_stream, p.aligned, true, h);
+      cudaGraph_t body = nullptr;
+      e = cudaStreamEndCapture(ctx->body_stream, &body);
+      if (kb < 0) return kb;
+      if (e != cudaSuccess) return ctx->cuda(e, "end body capture");
+      // the kernels the body runs are counted on the device (iters_run)
+    } else {
+      for (int it = 1; it < p.opts.iterations; it++) {
+        const long long k = one_iteration(st, p.aligned, false, 0);
+        if (k < 0) return k;
+        kernels += k;
+      }
+    }
   }
   if (p.iterations &&
       (e = cudaMemcpyAsync(p.iterations, p.iters_ws, sizeof(int) * p.batch, cudaMemcpyDeviceToDevice,
@@ -790,6 +855,7 @@ extern "C" int brc_register_linear_batched(brc_ctx* ctx, const float* d_ref, lon
   p.conv_iter = ctx->ctl.as<int>();
   p.iters_ws = p.conv_iter + batch;
   p.status = p.iters_ws + batch;
+  p.iter = p.status + 1;
   p.lists = p.status + 4;
   p.counts = p.lists + 3 * (size_t)batch;
   {

@@ -53,6 +53,8 @@ struct GraphEntry {
 struct brc_ctx {
   int device = 0;
   cudaStream_t own_stream = nullptr;
+  // stream on which the body of a registration graph's WHILE node is captured
+  cudaStream_t body_stream = nullptr;
   cudaStream_t user_stream = nullptr;
   bool use_user_stream = false;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
@@ -74,6 +76,9 @@ struct brc_ctx {
   // so an entry lives as long as the graphs do
   std::map<uint64_t, std::unique_ptr<DevBuf>> tc_taps;
   DevBuf tc_err;  // device int: a bounded wait of a tensor-core kernel gave up
+  // device count of the iterations that registration graphs ran (their
+  // loops stop on the device, so their kernel count is known only there)
+  DevBuf iters_run;
   DevBuf smask;   // smoothed certainty of brc_smooth_normalized
   // tensor-core tile height chosen by timing, per (nfilt, W, H, D)
   std::map<std::tuple<int, int, int, int>, int> tc_tuned;

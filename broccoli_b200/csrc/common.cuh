@@ -22,19 +22,27 @@ struct FilterBank {
   float coef[kTaps * 2 * NF];
 };
 
-// The instances a kernel of the batched registration loop works on: the
-// first *count entries of list, written by the solve of the previous
-// iteration (instances whose update has not yet fallen below the
-// tolerance), or every instance 0 .. batch-1 when list is null.
+// The instances a kernel of the batched registration loop works on.  The
+// loop keeps three lists of `stride` entries and their lengths; iteration
+// it (read from device memory, so that one captured iteration serves every
+// iteration of the loop) works on list it % 3, written by the solve of the
+// previous iteration (instances whose update has not yet fallen below the
+// tolerance).  With list null: every instance 0 .. batch-1.
 struct ActiveSet {
   const int* list;
   const int* count;
+  const int* iter;
+  int stride;
 };
 
-inline ActiveSet all_instances() { return ActiveSet{nullptr, nullptr}; }
+inline ActiveSet all_instances() { return ActiveSet{nullptr, nullptr, nullptr, 0}; }
 
-__device__ __forceinline__ int active_count(const ActiveSet& a, int batch) { return a.list ? *a.count : batch; }
-__device__ __forceinline__ int active_instance(const ActiveSet& a, int i) { return a.list ? a.list[i] : i; }
+__device__ __forceinline__ int active_count(const ActiveSet& a, int batch) {
+  return a.list ? a.count[*a.iter % 3] : batch;
+}
+__device__ __forceinline__ int active_instance(const ActiveSet& a, int i) {
+  return a.list ? a.list[(*a.iter % 3) * a.stride + i] : i;
+}
 
 // Four-quadrant arctangent of the phase kernels.  t = min(|x|,|y|) /
 // max(|x|,|y|) with the hardware reciprocal (rcp.approx, about 1 ulp), atan(t)

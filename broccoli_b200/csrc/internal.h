@@ -30,14 +30,19 @@ cudaError_t normal_eq_march(const float* q1, long long q1_stride_floats, const f
                             float cert_sigma);
 cudaError_t assemble_normal_eq(const double* partials, int nblk, int batch, double* A, double* h,
                                cudaStream_t st);
-// One iteration's solve and update of the instances in `act`; those whose
-// update is not yet below tol are appended to next_list / *next_count (and
-// conv_iter[b] = it records the others); *stale_count is reset for the
-// iteration after next.  Lists and counts may be null (no early exit).
+// One iteration's solve and update of the instances in `act` (iteration
+// *act.iter; act.list and act.iter not null); those whose update is not yet
+// below tol are appended to list (it + 1) % 3 of `lists` / `counts` (and
+// conv_iter[b] = it records the others); count (it + 2) % 3 is reset for
+// the iteration after next.
 cudaError_t solve_update(const double* partials, int nblk, int batch, int type, float tol, int W,
                          int H, int D, float* params, float* rotations, int* conv_iter,
-                         int* iterations, int* status, int it, ActiveSet act, int* next_list,
-                         int* next_count, int* stale_count, cudaStream_t st);
+                         int* iterations, int* status, ActiveSet act, int* lists, int* counts, cudaStream_t st);
+// *iter += 1; with use_cond, the condition of the WHILE node that runs the
+// loop is set (continue while *iter < max_it and count *iter % 3 > 0) and
+// *iters_run counts the iteration.
+cudaError_t iteration_control(int* iter, const int* counts, int max_it, cudaGraphConditionalHandle cond,
+                              bool use_cond, unsigned long long* iters_run, cudaStream_t st);
 // list0[i] = i for i < batch, counts[0] = batch, counts[1] = counts[2] = 0.
 cudaError_t active_init(int* list0, int* counts, int batch, cudaStream_t st);
 cudaError_t solve_given(const double* A, const double* h, int batch, float* p, cudaStream_t st);

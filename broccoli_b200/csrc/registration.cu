@@ -659,16 +659,20 @@ __device__ double update_magnitude(const float* p, int W, int H, int D) {
 }
 
 // One iteration's solve and parameter update for every active instance
-// (AlignTwoVolumesLinear, broccoli_lib.cpp:5380-5421).
+// (AlignTwoVolumesLinear, broccoli_lib.cpp:5380-5421).  The iteration it is
+// *act.iter; instances whose update is not yet below tol go to list
+// (it + 1) % 3, and list (it + 2) % 3 (the one iteration it - 1 used) is
+// emptied for the next solve.
 __global__ void solve_update_kernel(const double* __restrict__ partials, int nblk, int type,
                                     float tol, int W, int H, int D, float* __restrict__ params,
                                     float* __restrict__ rotations, int* __restrict__ conv_iter,
-                                    int* __restrict__ iterations, int* __restrict__ status, int it,
-                                    const ActiveSet act, int* __restrict__ next_list,
-                                    int* __restrict__ next_count, int* __restrict__ stale_count) {
+                                    int* __restrict__ iterations, int* __restrict__ status,
+                                    const ActiveSet act, int* __restrict__ lists, int* __restrict__ counts) {
   __shared__ double s[kNSums];
-  // the list of iteration it + 2 is refilled by the next solve
-  if (blockIdx.x == 0 && threadIdx.x == 0 && stale_count) *stale_count = 0;
+  const int it = *act.iter;
+  int* next_list = lists + ((it + 1) % 3) * act.stride;
+  int* next_count = counts + (it + 1) % 3;
+  if (blockIdx.x == 0 && threadIdx.x == 0) counts[(it + 2) % 3] = 0;
   if ((int)blockIdx.x >= active_count(act, (int)gridDim.x)) return;
   const int b = active_instance(act, blockIdx.x);
   reduce_partials(partials, nblk, b, s);
@@ -701,7 +705,22 @@ __global__ void solve_update_kernel(const double* __restrict__ partials, int nbl
   if (rotations && type == 1) rotation_angles(t, rotations + (long long)b * 3);
   const bool converged = tol > 0.f && update_magnitude(p, W, H, D) < (double)tol;
   if (converged && conv_iter != nullptr) conv_iter[b] = it;
-  if (!converged && next_list != nullptr) next_list[atomicAdd(next_count, 1)] = b;
+  if (!converged) next_list[atomicAdd(next_count, 1)] = b;
+}
+
+// End of an iteration of the loop: advances the device iteration counter,
+// and, when the loop runs as a graph's conditional WHILE node, sets its
+// condition: another iteration while iterations remain and the list the
+// solve just filled is not empty (then *iters_run counts the iteration).
+__global__ void iteration_control_kernel(int* __restrict__ iter, const int* __restrict__ counts, int max_it,
+                                         cudaGraphConditionalHandle cond, int use_cond,
+                                         unsigned long long* __restrict__ iters_run) {
+  const int next = *iter + 1;
+  *iter = next;
+  if (use_cond) {
+    atomicAdd(iters_run, 1ull);
+    cudaGraphSetConditional(cond, (next < max_it && counts[next % 3] > 0) ? 1u : 0u);
+  }
 }
 
 __global__ void active_init_kernel(int* __restrict__ list0, int* __restrict__ counts, int batch) {
@@ -1153,11 +1172,16 @@ cudaError_t assemble_normal_eq(const double* partials, int nblk, int batch, doub
 
 cudaError_t solve_update(const double* partials, int nblk, int batch, int type, float tol, int W,
                          int H, int D, float* params, float* rotations, int* conv_iter,
-                         int* iterations, int* status, int it, ActiveSet act, int* next_list,
-                         int* next_count, int* stale_count, cudaStream_t st) {
+                         int* iterations, int* status, ActiveSet act, int* lists, int* counts, cudaStream_t st) {
+  if (!act.list || !act.iter) return cudaErrorInvalidValue;
   solve_update_kernel<<<batch, 64, 0, st>>>(partials, nblk, type, tol, W, H, D, params, rotations,
-                                            conv_iter, iterations, status, it, act, next_list, next_count,
-                                            stale_count);
+                                            conv_iter, iterations, status, act, lists, counts);
+  return cudaGetLastError();
+}
+
+cudaError_t iteration_control(int* iter, const int* counts, int max_it, cudaGraphConditionalHandle cond,
+                              bool use_cond, unsigned long long* iters_run, cudaStream_t st) {
+  iteration_control_kernel<<<1, 1, 0, st>>>(iter, counts, max_it, cond, use_cond ? 1 : 0, iters_run);
   return cudaGetLastError();
 }
 

@@ -79,7 +79,9 @@ int brc_ctx_synchronize(brc_ctx* ctx);
 /* Bytes of device workspace the context currently holds. */
 size_t brc_ctx_workspace_bytes(const brc_ctx* ctx);
 /* Number of kernels this context has launched so far (graph replays count
- * every kernel node).  Used by benchmarks to report launch counts. */
+ * every kernel node they ran; the iterations of a registration graph's loop
+ * are counted on the device, so this call first synchronises the context's
+ * streams).  Used by benchmarks to report launch counts. */
 unsigned long long brc_ctx_kernel_launches(const brc_ctx* ctx);
 /* Replaces GetOpenCLErrorMessage / the INITIALIZATION_ERROR getters
  * (broccoli_lib.h:399-413). */
