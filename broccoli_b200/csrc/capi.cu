@@ -680,12 +680,14 @@ long long enqueue_registration(brc_ctx* ctx, const RegPlan& p, cudaStream_t st) 
                            st)) != cudaSuccess)
     return ctx->cuda(e, "copy");
   if (p.opts.iterations > 0) {
-    // the iteration runs on the device's counter p.iter (set to 0 above);
-    // iteration 0 filters the moving volumes themselves, later ones their
-    // warps: the first iteration is enqueued on its own
-    const brc::ActiveSet act{p.lists, p.counts, p.iter, p.batch};
-    int* iter = const_cast<int*>(p.iter);
-    auto one_iteration = [&](cudaStream_t s, const float* cur, bool cond_node, cudaGraphConditionalHandle h) -> long long {
+    // one iteration: filtering (of the moving volumes themselves at
+    // iteration 0, of their warps later), normal equations, solve, warp;
+    // with device_iter, the kernels read the iteration from the device
+    // counter p.iter and a control kernel advances it
+    auto one_iteration = [&](cudaStream_t s, int it, bool device_iter, bool cond_node,
+                             cudaGraphConditionalHandle h) -> long long {
+      const brc::ActiveSet act{p.lists, p.counts, device_iter ? p.iter : nullptr, it, p.batch};
+      const float* cur = it == 0 ? p.moving : p.aligned;
       cudaError_t ee;
       if ((ee = run_filter(p.fpath, cur, p.W, p.H, p.D, p.batch, V, p.q2, act, s)) != cudaSuccess)
         return ctx->cuda(ee, "filter3d");
@@ -699,20 +701,23 @@ long long enqueue_registration(brc_ctx* ctx, const RegPlan& p, cudaStream_t st) 
       if ((ee = brc::warp_affine(p.moving, V, p.W, p.H, p.D, p.batch, p.params, p.aligned, V, act, s)) !=
           cudaSuccess)
         return ctx->cuda(ee, "warp");
-      if ((ee = brc::iteration_control(iter, p.counts, p.opts.iterations, h, cond_node,
+      if (!device_iter) return 3 + filter_launches(p.fpath);
+      if ((ee = brc::iteration_control(const_cast<int*>(p.iter), p.counts, p.opts.iterations, h, cond_node,
                                        ctx->iters_run.as<unsigned long long>(), s)) != cudaSuccess)
         return ctx->cuda(ee, "iteration control");
       return 4 + filter_launches(p.fpath);
     };
-    long long k0 = one_iteration(st, p.moving, false, 0);
-    if (k0 < 0) return k0;
-    kernels += k0;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if ((e = cudaStreamIsCapturing(st, &cs)) != cudaSuccess) return ctx->cuda(e, "capture status");
-    if (cs == cudaStreamCaptureStatusActive && p.opts.iterations > 1) {
-      // iterations 1 .. while instances remain: one conditional WHILE node
-      // whose body is one iteration, its condition set on the device by the
-      // control kernel (the loop stops as soon as every instance converged)
+    if (cs == cudaStreamCaptureStatusActive && p.opts.tolerance > 0.f && p.opts.iterations > 1) {
+      // a graph with early exit: iteration 0, then one conditional WHILE
+      // node whose body is one iteration on the device counter (set to 1 by
+      // iteration 0's control kernel), its condition set on the device by
+      // the control kernel: the loop stops as soon as every instance
+      // converged, with no host round trip
+      const long long k0 = one_iteration(st, 0, true, false, 0);
+      if (k0 < 0) return k0;
+      kernels += k0;
       cudaGraph_t graph = nullptr;
       const cudaGraphNode_t* deps = nullptr;
       size_t ndeps = 0;
@@ -736,15 +741,17 @@ long long enqueue_registration(brc_ctx* ctx, const RegPlan& p, cudaStream_t st) 
       if ((e = cudaStreamBeginCaptureToGraph(ctx->body_stream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
                                              cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
         return ctx->cuda(e, "body capture");
-      const long long kb = one_iteration(ctx->body_stream, p.aligned, true, h);
+      const long long kb = one_iteration(ctx->body_stream, 1, true, true, h);
       cudaGraph_t body = nullptr;
       e = cudaStreamEndCapture(ctx->body_stream, &body);
       if (kb < 0) return kb;
       if (e != cudaSuccess) return ctx->cuda(e, "end body capture");
       // the kernels the body runs are counted on the device (iters_run)
     } else {
-      for (int it = 1; it < p.opts.iterations; it++) {
-        const long long k = one_iteration(st, p.aligned, false, 0);
+      // every iteration enqueued with its number (a graph without early
+      // exit runs all of them anyway; without a graph the host loops)
+      for (int it = 0; it < p.opts.iterations; it++) {
+        const long long k = one_iteration(st, it, false, false, 0);
         if (k < 0) return k;
         kernels += k;
       }

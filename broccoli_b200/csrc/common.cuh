@@ -24,24 +24,27 @@ struct FilterBank {
 
 // The instances a kernel of the batched registration loop works on.  The
 // loop keeps three lists of `stride` entries and their lengths; iteration
-// it (read from device memory, so that one captured iteration serves every
-// iteration of the loop) works on list it % 3, written by the solve of the
-// previous iteration (instances whose update has not yet fallen below the
-// tolerance).  With list null: every instance 0 .. batch-1.
+// it works on list it % 3, written by the solve of the previous iteration
+// (instances whose update has not yet fallen below the tolerance).  The
+// iteration is `it`, or *iter when iter is set (a device counter, so that
+// one captured iteration serves every iteration of a graph's loop).  With
+// list null: every instance 0 .. batch-1.
 struct ActiveSet {
   const int* list;
   const int* count;
   const int* iter;
+  int it;
   int stride;
 };
 
-inline ActiveSet all_instances() { return ActiveSet{nullptr, nullptr, nullptr, 0}; }
+inline ActiveSet all_instances() { return ActiveSet{nullptr, nullptr, nullptr, 0, 0}; }
 
+__device__ __forceinline__ int active_iteration(const ActiveSet& a) { return a.iter ? *a.iter : a.it; }
 __device__ __forceinline__ int active_count(const ActiveSet& a, int batch) {
-  return a.list ? a.count[*a.iter % 3] : batch;
+  return a.list ? a.count[active_iteration(a) % 3] : batch;
 }
 __device__ __forceinline__ int active_instance(const ActiveSet& a, int i) {
-  return a.list ? a.list[(*a.iter % 3) * a.stride + i] : i;
+  return a.list ? a.list[(active_iteration(a) % 3) * a.stride + i] : i;
 }
 
 // Four-quadrant arctangent of the phase kernels.  t = min(|x|,|y|) /

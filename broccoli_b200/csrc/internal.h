@@ -30,8 +30,8 @@ cudaError_t normal_eq_march(const float* q1, long long q1_stride_floats, const f
                             float cert_sigma);
 cudaError_t assemble_normal_eq(const double* partials, int nblk, int batch, double* A, double* h,
                                cudaStream_t st);
-// One iteration's solve and update of the instances in `act` (iteration
-// *act.iter; act.list and act.iter not null); those whose update is not yet
+// One iteration's solve and update of the instances in `act` (its
+// iteration it; act.list not null); those whose update is not yet
 // below tol are appended to list (it + 1) % 3 of `lists` / `counts` (and
 // conv_iter[b] = it records the others); count (it + 2) % 3 is reset for
 // the iteration after next.

@@ -659,8 +659,8 @@ __device__ double update_magnitude(const float* p, int W, int H, int D) {
 }
 
 // One iteration's solve and parameter update for every active instance
-// (AlignTwoVolumesLinear, broccoli_lib.cpp:5380-5421).  The iteration it is
-// *act.iter; instances whose update is not yet below tol go to list
+// (AlignTwoVolumesLinear, broccoli_lib.cpp:5380-5421), iteration it of
+// act; instances whose update is not yet below tol go to list
 // (it + 1) % 3, and list (it + 2) % 3 (the one iteration it - 1 used) is
 // emptied for the next solve.
 __global__ void solve_update_kernel(const double* __restrict__ partials, int nblk, int type,
@@ -669,7 +669,7 @@ __global__ void solve_update_kernel(const double* __restrict__ partials, int nbl
                                     int* __restrict__ iterations, int* __restrict__ status,
                                     const ActiveSet act, int* __restrict__ lists, int* __restrict__ counts) {
   __shared__ double s[kNSums];
-  const int it = *act.iter;
+  const int it = active_iteration(act);
   int* next_list = lists + ((it + 1) % 3) * act.stride;
   int* next_count = counts + (it + 1) % 3;
   if (blockIdx.x == 0 && threadIdx.x == 0) counts[(it + 2) % 3] = 0;
@@ -1173,7 +1173,7 @@ cudaError_t assemble_normal_eq(const double* partials, int nblk, int batch, doub
 cudaError_t solve_update(const double* partials, int nblk, int batch, int type, float tol, int W,
                          int H, int D, float* params, float* rotations, int* conv_iter,
                          int* iterations, int* status, ActiveSet act, int* lists, int* counts, cudaStream_t st) {
-  if (!act.list || !act.iter) return cudaErrorInvalidValue;
+  if (!act.list) return cudaErrorInvalidValue;
   solve_update_kernel<<<batch, 64, 0, st>>>(partials, nblk, type, tol, W, H, D, params, rotations,
                                             conv_iter, iterations, status, act, lists, counts);
   return cudaGetLastError();

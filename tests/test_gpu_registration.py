@@ -163,22 +163,24 @@ def test_kernel_launch_counter(ctx, lin_filters):
     ctx.register_linear(v, v[None], lin_filters, 4, L.AFFINE)
     torch.cuda.synchronize()
     # active-set initialisation, reference filtering, 4 x (filter, normal
-    # equations, solve, warp, iteration control)
-    assert ctx.kernel_launches - before == 2 + 4 * 5
+    # equations, solve, warp): without early exit every iteration is a node
+    assert ctx.kernel_launches - before == 2 + 4 * 4
 
 
 @pytest.mark.parametrize("use_graph", [True, False])
 def test_loop_stops_when_every_instance_converged(ctx, lin_filters, use_graph):
-    """A volume registered to itself converges at iteration 0.  As a graph,
-    the loop's WHILE node then runs one more (empty) iteration and stops on
-    the device; the eager loop runs all iterations over an empty active set.
-    Both give the same (zero) parameters and one iteration per instance."""
+    """A volume registered to itself converges at iteration 0.  As a graph
+    with early exit, iteration 0 and the loop's WHILE node, which runs one
+    more (empty) iteration and stops on the device (five kernels each, with
+    the control kernel); the eager loop runs all ten iterations (four
+    kernels each) over an empty active set.  Both give the same (zero)
+    parameters and one iteration per instance."""
     v = cuda(np.random.default_rng(3).standard_normal((12, 14, 13)))
     before = ctx.kernel_launches
     r = ctx.register_linear(v, torch.stack([v, v]), lin_filters, 10, L.AFFINE, tolerance=1e-3, use_graph=use_graph)
     torch.cuda.synchronize()
     n = ctx.kernel_launches - before
-    assert n == (2 + 2 * 5 if use_graph else 2 + 10 * 5)
+    assert n == (2 + 2 * 5 if use_graph else 2 + 10 * 4)
     assert np.array_equal(r["iterations"].cpu().numpy(), [1, 1])
     assert np.abs(r["params"].cpu().numpy()).max() == 0.0
 
