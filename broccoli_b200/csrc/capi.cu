@@ -948,19 +948,20 @@ extern "C" int brc_motion_correct(brc_ctx* ctx, float* h_volumes, int W, int H, 
   BRC_TRY(ctx, ctx->rot.ensure(sizeof(float) * 3 * batch), "alloc rot");
   float* d_series = ctx->series.as<float>();
   BRC_TRY(ctx, ctx->ensure_copy_streams(), "copy streams");
-  // Series of 64 or more volumes are registered in three chunks, a tenth,
-  // the rest and a tenth, so that only a small upload precedes the first
+  // Series of 64 or more volumes are registered in three chunks, an eighth,
+  // the rest and an eighth, so that only a small upload precedes the first
   // registration and a small download follows the last, while the other
   // copies run on the copy engines under registration.  (Measured per call
-  // on 199 volumes of 64x64x33: one chunk 18.3 ms, two equal chunks 16.9,
-  // 20/159/20 16.1, 30/139/30 16.3, 12/175/12 16.4, 20/80/79/20 16.6 --
-  // each chunk is a registration of its own, and small ones use the GPU
-  // less well.)  Chunk 0's upload includes the reference (volume 0, or
-  // h_reference).
+  // on 199 volumes of 64x64x33, TF32, with the registration loop stopping on
+  // the device: one chunk 13.2 ms; 19/161/19 11.27-11.40, 22/156/21 11.10,
+  // 25/150/24 10.98-11.07, 28/144/27 11.04-11.06, 32/136/31 11.23-11.28;
+  // four chunks 11.37-11.74, five 12.15 -- each chunk is a registration of
+  // its own, and small ones use the GPU less well.)  Chunk 0's upload
+  // includes the reference (volume 0, or h_reference).
   int nchunk = 1, csz[3] = {batch, 0, 0};
   if (batch >= 64) {
     nchunk = 3;
-    csz[0] = csz[2] = batch / 10;
+    csz[0] = csz[2] = batch / 8;
     csz[1] = batch - 2 * csz[0];
   }
   int cst[4] = {0, 0, 0, 0};
