@@ -56,7 +56,7 @@ int brc_ctx::taps_for(const float* h_filters, int nfilt, bool tf32, const uint16
       graphs.clear();  // graphs may hold the pointers released here
       tc_taps.clear();
     }
-    std::vector<uint16_t> packed(brc::tc::packed_tap_bytes(nfilt) / 2);
+    std::vector<uint16_t> packed(brc::tc::packed_tap_bytes(nfilt, tf32) / 2);
     brc::tc::pack_taps(h_filters, nfilt, packed.data(), tf32);
     std::unique_ptr<DevBuf> buf(new DevBuf());
     BRC_TRY(this, buf->ensure(packed.size() * 2), "alloc taps");
@@ -83,7 +83,7 @@ int brc_ctx::tune_tc(int nfilt, int W, int H, int D, const uint16_t* d_taps, boo
     return BRC_OK;
   }
   int tys[3];
-  const int n = brc::tc::candidate_tys(nfilt, H, D, tys, 3);
+  const int n = brc::tc::candidate_tys(nfilt, H, D, tys, 3, tf32);
   if (n <= 0) return fail(BRC_ERR_UNSUPPORTED, "volume shape not supported by the tensor-core filtering");
   *ty = tys[0];
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
@@ -108,7 +108,7 @@ int brc_ctx::tune_tc(int nfilt, int W, int H, int D, const uint16_t* d_taps, boo
     float best = -1.f;
     cudaError_t err = cudaSuccess;
     for (int c = 0; c < n && err == cudaSuccess; c++) {
-      const brc::tc::Geometry g = brc::tc::make_geometry(nfilt, H, D, tys[c]);
+      const brc::tc::Geometry g = brc::tc::make_geometry(nfilt, H, D, tys[c], tf32);
       float ms_best = -1.f;
       for (int rep = 0; rep < 4 && err == cudaSuccess; rep++) {
         err = cudaEventRecord(e0, own_stream);
@@ -276,7 +276,7 @@ int make_filter_path(brc_ctx* ctx, const float* h_filters, int nfilt, int precis
   int ty = 0;
   st = ctx->tune_tc(nfilt, W, H, D, fp->d_taps, tf32, &ty);
   if (st != BRC_OK) return st;
-  fp->g = brc::tc::make_geometry(nfilt, H, D, ty);
+  fp->g = brc::tc::make_geometry(nfilt, H, D, ty, tf32);
   return BRC_OK;
 }
 

@@ -29,11 +29,15 @@
 // A_hi B_hi + A_hi B_lo + A_lo B_hi into the same FP32 TMEM accumulator
 // (relative error of a product ~2^-16; the dropped A_lo B_lo ~2^-18).
 // TF32: data and taps rounded to TF32 (10-bit mantissa, round to nearest,
-// ties away), one product per tap, as two K = 8 MMAs of kind::tf32 per GEMM
-// instead of three K = 16 BF16 ones (relative error of a product ~2^-10).
-// The 16 K samples of a row then sit in four 4-sample 16-byte quarters
-// where the BF16 form keeps a hi and a lo part of two 8-sample halves: the
-// same bytes and the same descriptor strides.
+// ties away), one product per tap (relative error ~2^-10), as ONE
+// structured-sparse MMA of K = 16 per GEMM (tcgen05.mma.sp, kind::tf32,
+// 1:2 sparsity): the banded A holds 7 taps in 16 K columns, and pairing
+// sample P with sample P + 8 (P < 8) puts at most one tap in each pair, so
+// A is stored as one value per pair (half the tap bytes) and a fixed
+// metadata column in TMEM says which of the pair it is.  B's 16 samples of
+// a row sit in four 16-byte quarters in that pair order (quarter q:
+// samples 2q, 2q + 8, 2q + 1, 2q + 9), the bytes and descriptor strides of
+// the BF16 form's hi and lo parts of two 8-sample halves.
 //
 // One persistent CTA per SM walks the tiles of the launch (10 x positions x
 // Ty rows x SP*J planes of one volume each) with its warps specialised:
@@ -41,12 +45,14 @@
 //   warps 12-19    stage a tile's input (FP32 -> BF16 hi/lo or TF32 rows)
 //                  into one of two shared-memory buffers while the GEMMs
 //                  read the other
-//   warp 1, lane 0 issues the tcgen05.mma's: three split products per stage,
-//                  descriptors built once and advanced by adds (every cycle
-//                  of address arithmetic in this thread delays the GEMMs)
-//   warp 2, lane 0 streams the packed taps, two stages (16 KB: hi + lo of
-//                  each) per slot, through a 3-slot ring with cp.async.bulk
-//                  + mbarriers (one wait and one commit per six GEMMs)
+//   warp 1, lane 0 issues the tcgen05.mma's: three split products (BF16X3)
+//                  or one sparse MMA (TF32) per stage, descriptors built
+//                  once and advanced by adds (every cycle of address
+//                  arithmetic in this thread delays the GEMMs)
+//   warp 2, lane 0 streams the packed taps, two stages (BF16X3: 16 KB, hi
+//                  + lo of each; TF32: 8 KB) per slot, through a 3-slot
+//                  ring with cp.async.bulk + mbarriers (one wait and one
+//                  commit per two GEMMs)
 //   warps 4-11     epilogue: tcgen05.ld of the accumulator (TMEM lanes
 //                  32 (warp % 4) .., the two warps of a lane quarter on
 //                  alternate 16-column groups), transposed through shared
@@ -68,7 +74,7 @@
 namespace brc {
 namespace tc {
 
-// Group sizes measured on 199 volumes of 64x64x33 (TF32 / BF16X3 ms):
+// Group sizes measured on 199 volumes of 64x64x33 (dense TF32 / BF16X3 ms):
 // 4 + 4 warps 0.58 / 0.72, 8 + 4 0.57 / 0.74, 4 + 8 0.66 / 0.72, 8 + 8
 // 0.534 / 0.696, 12 + 8 and 8 + 12 0.54-0.55 / 0.70.
 constexpr int kEpiWarps = 8;         // epilogue warps (a multiple of 4: kEpiWarps / 4 per TMEM lane quarter)
@@ -84,6 +90,10 @@ constexpr int kStageHalves = kM * kK;              // BF16 elements of one A (hi
 constexpr int kStageBytes = 2 * kStageHalves * 2;  // hi + lo
 constexpr int kSlotBytes = 2 * kStageBytes;        // a ring slot: two stages
 constexpr int kSlotsPerTile = 28;                  // 7 dy x 4 pairs of input-plane offsets
+// TF32: structured-sparse A, kM rows x 8 stored values (16 K samples)
+constexpr int kStageBytesSp = kM * 8 * 4;
+constexpr int kSlotBytesSp = 2 * kStageBytesSp;
+constexpr uint32_t kMetaCol = 508;  // TMEM column of the sparsity metadata (N <= 240: free)
 constexpr int kEpiBytes = kEpiCols * 6 * 20 * 4;   // SP * nfilt = 6 for both banks
 // barrier block: full_in, empty_in, acc_full, acc_empty (2 each), the ring's
 // full / empty (kRing each), done; then the TMEM address and 7 flags
@@ -228,6 +238,41 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
 }
 
+// One structured-sparse TF32 MMA (K = 16 samples, 8 stored per A row), its
+// metadata in TMEM column tmem_e.
+__device__ __forceinline__ void mma_tf32_sp(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t tmem_e,
+                                            uint32_t idesc, uint32_t accumulate) {
+  const uint32_t z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.sp.cta_group::1.kind::tf32 [%0], %1, %2, [%5], %3, {%6, %7, %8, %9}, p;\n\t"
+      "}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(tmem_e), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+// Sparsity metadata of TMEM lane L for the banded A (the same for every
+// stage): lane L = m0 + 8 k1 + 16 m2 holds rows m0 + 8 m1 + 16 m2 (m1 = 0,
+// 1) in bits 16 m1 .., K half k1; a nibble per sample pair j of that half
+// (pair P = 4 k1 + j: samples P and P + 8), 0b0100 keeping the first and
+// 0b1110 the second; row r's taps are samples xo .. xo + 6.
+__device__ __forceinline__ uint32_t sparse_metadata_word(int L, int SP, int nfilt) {
+  const int m0 = L & 7, k1 = (L >> 3) & 1, m2 = L >> 4;
+  uint32_t word = 0;
+  for (int m1 = 0; m1 < 2; m1++) {
+    const int r = m0 + 8 * m1 + 16 * m2;
+    const int rr = SP == 2 ? (r & 63) : r;
+    const bool valid = rr < 2 * nfilt * kXo;
+    const int xo = rr % kXo;
+    for (int j = 0; j < 4; j++) {
+      const int P = 4 * k1 + j;
+      const bool second = valid && !(P >= xo && P <= xo + 6) && (P + 8 >= xo && P + 8 <= xo + 6);
+      word |= (second ? 0xEu : 0x4u) << (16 * m1 + 4 * j);
+    }
+  }
+  return word;
+}
+
 __device__ __forceinline__ uint32_t tf32_rna(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
@@ -286,6 +331,21 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
+  if (TF32) {
+    // the sparsity metadata, one column for every MMA of the launch
+    if (warp >= 4 && warp < 8) {
+      const int q = warp - 4;
+      const uint32_t word = sparse_metadata_word(32 * q + lane, g.SP, a.nfilt);
+      asm volatile("tcgen05.st.sync.aligned.32x32b.x1.b32 [%0], {%1};" ::"r"(tmem + ((uint32_t)(32 * q) << 16) +
+                                                                             kMetaCol),
+                   "r"(word)
+                   : "memory");
+      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+  }
 
   if (warp >= kStageWarp) {
     // ---- staging: row (parity p, plane slot qq, y row yl) of K half kh
@@ -316,7 +376,42 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
       const bool vec_rows = (a.W & 3) == 0 && (reinterpret_cast<uintptr_t>(src) & 15) == 0;
       uint8_t* hi = inb + (uint32_t)(buf * 4) * rowbytes;
       uint8_t* lo = hi + 2u * rowbytes;
-      for (int item = st; item < 2 * nrows; item += kStageThreads) {
+      if (TF32) {
+        // whole rows of 16 samples x0 - 3 .. x0 + 12, in the K order of the
+        // sparse MMA: quarter q holds samples 2q, 2q + 8, 2q + 1, 2q + 9
+        for (int row = st; row < nrows; row += kStageThreads) {
+          const int par = row / prow, rr = row - par * prow;
+          const int qq = rr / g.Hp, yl = rr - qq * g.Hp;
+          const int zg = z0 - 3 + qq * g.SP + par, yg = y0 - 3 + yl;
+          const bool rowok = zg >= 0 && zg < a.D && yg >= 0 && yg < a.H;
+          const int xs = x0 - 3;
+          float v[16];
+          if (rowok && vec_rows && xs >= 0 && (xs & ~3) + 20 <= a.W) {
+            const int al = xs & 3;
+            const float4* p4 = reinterpret_cast<const float4*>(src + ((long long)zg * a.H + yg) * a.W + (xs - al));
+            const float4 f0 = __ldg(p4), f1 = __ldg(p4 + 1), f2 = __ldg(p4 + 2), f3 = __ldg(p4 + 3),
+                         f4 = __ldg(p4 + 4);
+            const float w[20] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, f1.z, f1.w, f2.x, f2.y,
+                                 f2.z, f2.w, f3.x, f3.y, f3.z, f3.w, f4.x, f4.y, f4.z, f4.w};
+#pragma unroll
+            for (int e = 0; e < 16; e++)
+              v[e] = al == 0 ? w[e] : (al == 1 ? w[e + 1] : (al == 2 ? w[e + 2] : w[e + 3]));
+          } else {
+            const float* rp = src + ((long long)(rowok ? zg : 0) * a.H + (rowok ? yg : 0)) * a.W;
+#pragma unroll
+            for (int e = 0; e < 16; e++) {
+              const int xg = xs + e;
+              v[e] = (rowok && xg >= 0 && xg < a.W) ? __ldg(rp + xg) : 0.f;
+            }
+          }
+          const uint32_t rowoff = (uint32_t)(par * g.RP + qq * g.Hp + yl) * 16u;
+#pragma unroll
+          for (int q = 0; q < 4; q++)
+            *reinterpret_cast<uint4*>(hi + (uint32_t)q * rowbytes + rowoff) =
+                make_uint4(tf32_rna(v[2 * q]), tf32_rna(v[2 * q + 8]), tf32_rna(v[2 * q + 1]), tf32_rna(v[2 * q + 9]));
+        }
+      }
+      for (int item = st; !TF32 && item < 2 * nrows; item += kStageThreads) {
         const int kh = item >= nrows ? 1 : 0, row = item - kh * nrows;
         const int par = row / prow, rr = row - par * prow;
         const int qq = rr / g.Hp, yl = rr - qq * g.Hp;
@@ -340,13 +435,7 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
           }
         }
         const uint32_t rowoff = (uint32_t)(par * g.RP + qq * g.Hp + yl) * 16u;
-        if (TF32) {
-          // quarters 2 kh and 2 kh + 1 (samples 0-3 and 4-7 of this half)
-          uint8_t* q0 = hi + (uint32_t)(2 * kh) * rowbytes + rowoff;
-          *reinterpret_cast<uint4*>(q0) = make_uint4(tf32_rna(v[0]), tf32_rna(v[1]), tf32_rna(v[2]), tf32_rna(v[3]));
-          *reinterpret_cast<uint4*>(q0 + rowbytes) =
-              make_uint4(tf32_rna(v[4]), tf32_rna(v[5]), tf32_rna(v[6]), tf32_rna(v[7]));
-        } else {
+        {
           uint32_t ph4[4], pl4[4];
 #pragma unroll
           for (int e = 0; e < 8; e += 2) {
@@ -373,12 +462,16 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
     // the issuing thread spends its time in tcgen05.mma, not in address
     // arithmetic (which delays every GEMM it precedes).
     // D F32; A, B BF16 (1) or TF32 (2); K-major; N, M
+    // (TF32: structured-sparse MMAs, sparse flag bit 2, metadata in TMEM
+    // column kMetaCol)
     const uint32_t ab = TF32 ? 2u : 1u;
-    const uint32_t idesc = (1u << 4) | (ab << 7) | (ab << 10) | ((uint32_t)(g.N >> 3) << 17) |
-                           ((uint32_t)(kM >> 4) << 24);
+    const uint32_t idesc = (TF32 ? (1u << 2) : 0u) | (1u << 4) | (ab << 7) | (ab << 10) |
+                           ((uint32_t)(g.N >> 3) << 17) | ((uint32_t)(kM >> 4) << 24);
+    const uint32_t tmem_e = tmem + kMetaCol;
     const uint64_t da0 = sdesc(smem_u32(ring), kM * 16, 128);  // slot 0, hi taps
     const uint64_t db0 = sdesc(smem_u32(inb), rowbytes, 128);  // buffer 0, hi part, row 0
-    const uint64_t dslot = kSlotBytes >> 4, dstage = kStageBytes >> 4, dalo = kStageBytes >> 5;
+    const uint64_t dslot = (TF32 ? kSlotBytesSp : kSlotBytes) >> 4;
+    const uint64_t dstage = (TF32 ? kStageBytesSp : kStageBytes) >> 4, dalo = kStageBytes >> 5;
     const uint64_t dbuf = (4u * rowbytes) >> 4, dblo = (2u * rowbytes) >> 4;
     // slot m of dy row dyq holds the taps of input-plane offsets cq = 2m and
     // 2m + 1 (c = cq - 3); their B rows start at parity array cq % SP, plane
@@ -417,9 +510,7 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
           }
           const uint64_t b1 = bh0 + offa[m] + (uint64_t)dyq;
           if (TF32) {
-            // K samples 0-7 (quarters 0, 1), then 8-15 (quarters 2, 3)
-            mma_tf32(dcol, ah, b1, idesc, accf);
-            mma_tf32(dcol, ah + dalo, b1 + dblo, idesc, 1u);
+            mma_tf32_sp(dcol, ah, b1, tmem_e, idesc, accf);
           } else {
             mma_bf16(dcol, ah, b1, idesc, accf);
             mma_bf16(dcol, ah, b1 + dblo, idesc, 1u);
@@ -429,8 +520,7 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
           if (m < 3 || last_pair) {
             const uint64_t b2 = bh0 + offb[m] + (uint64_t)dyq, a2 = ah + dstage;
             if (TF32) {
-              mma_tf32(dcol, a2, b2, idesc, 1u);
-              mma_tf32(dcol, a2 + dalo, b2 + dblo, idesc, 1u);
+              mma_tf32_sp(dcol, a2, b2, tmem_e, idesc, 1u);
             } else {
               mma_bf16(dcol, a2, b2, idesc, 1u);
               mma_bf16(dcol, a2, b2 + dblo, idesc, 1u);
@@ -475,9 +565,10 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
           ok = false;
           break;
         }
-        mbar_expect_tx(&tfull[slot], kSlotBytes);
-        bulk_load(ring + slot * kSlotBytes, src, kSlotBytes, &tfull[slot]);
-        src += kSlotBytes / 2;
+        constexpr int kSl = TF32 ? kSlotBytesSp : kSlotBytes;
+        mbar_expect_tx(&tfull[slot], kSl);
+        bulk_load(ring + slot * kSl, src, kSl, &tfull[slot]);
+        src += kSl / 2;
         if (++slot == kRing) {
           slot = 0;
           ph ^= 1u;
@@ -628,9 +719,9 @@ static float bf16_to_f(uint16_t h) {
 
 int stacked_planes(int nfilt) { return nfilt == 3 ? 2 : 1; }
 int num_stages(int nfilt) { return (7 + stacked_planes(nfilt) - 1) * 7; }
-size_t packed_tap_bytes(int nfilt) {
+size_t packed_tap_bytes(int nfilt, bool tf32) {
   (void)nfilt;
-  return (size_t)kSlotsPerTile * kSlotBytes;
+  return (size_t)kSlotsPerTile * (tf32 ? kSlotBytesSp : kSlotBytes);
 }
 
 static uint32_t tf32_rna_host(float f) {
@@ -641,19 +732,23 @@ static uint32_t tf32_rna_host(float f) {
 }
 
 // Stage (input-plane offset c = cq - 3, dy = dyq - 3) goes to ring slot
-// dyq * 4 + cq / 2, half cq % 2; each half is hi (kM x 16 BF16) then lo, as
-// two K-major 8-row x 16-byte core-matrix blocks, or (tf32) four K quarters
-// of kM x 4 TF32 values, each a K-major block of 8-row x 16-byte core
-// matrices.  Halves without a stage (cq = 7 with one stacked plane) stay
-// zero.
+// dyq * 4 + cq / 2, half cq % 2.  BF16X3: each half is hi (kM x 16 BF16)
+// then lo, as two K-major 8-row x 16-byte core-matrix blocks.  TF32: each
+// half is the structured-sparse A of the stage: the 16 K samples of a row
+// pair up as (P, P + 8), P < 8, and a row's 7 taps (samples xo .. xo + 6)
+// never hold both of a pair, so each row keeps one value per pair -- stored
+// position P, two K-major blocks of kM x 4 TF32 -- and the MMA's metadata
+// says which of the pair it is (sparse_metadata_word).  Halves without a
+// stage (cq = 7 with one stacked plane) stay zero.
 void pack_taps(const float* h_filters, int nfilt, uint16_t* dst, bool tf32) {
   const int SP = stacked_planes(nfilt);
   const int ncq = 6 + SP;
-  memset(dst, 0, packed_tap_bytes(nfilt));
+  memset(dst, 0, packed_tap_bytes(nfilt, tf32));
   for (int cq = 0; cq < ncq; cq++)
     for (int dyq = 0; dyq < 7; dyq++) {
       const int c = cq - 3, dy = dyq - 3;
-      uint16_t* hi = dst + ((size_t)(dyq * 4 + cq / 2) * 2 + (cq & 1)) * 2 * kStageHalves;
+      const size_t stage = (size_t)(dyq * 4 + cq / 2) * 2 + (cq & 1);
+      uint16_t* hi = dst + stage * (tf32 ? kStageBytesSp / 2 : 2 * kStageHalves);
       uint16_t* lo = hi + kStageHalves;
       for (int r = 0; r < kM; r++) {
         int s, f, xo;
@@ -677,7 +772,8 @@ void pack_taps(const float* h_filters, int nfilt, uint16_t* dst, bool tf32) {
           const float w = F[(3 - dz) * 49 + (3 - dy) * 7 + (3 - dx)];
           if (tf32) {
             const uint32_t t = tf32_rna_host(w);
-            const size_t e = (size_t)(kx / 4) * (kM * 4) + (size_t)r * 4 + (kx % 4);
+            const int P = kx & 7;  // pair (P, P + 8): stored position P
+            const size_t e = (size_t)(P / 4) * (kM * 4) + (size_t)r * 4 + (P % 4);
             memcpy(hi + 2 * e, &t, 4);
           } else {
             const uint16_t wh = bf16_rn(w);
@@ -701,12 +797,13 @@ static int smem_bytes(int NR) {
   return need > 116 * 1024 ? need : 116 * 1024;
 }
 
-Geometry make_geometry(int nfilt, int H, int D, int Ty) {
+Geometry make_geometry(int nfilt, int H, int D, int Ty, bool tf32) {
   Geometry g;
+  g.maxN = tf32 ? kMaxNSparse : kMaxN;
   g.SP = stacked_planes(nfilt);
   g.Ty = Ty < H ? Ty : H;
   g.Hp = g.Ty + 6;
-  g.J = kMaxN / g.Hp;
+  g.J = g.maxN / g.Hp;
   if (g.J < 1) g.J = 1;
   // no more plane groups than the volume needs
   const int jmax = (D + g.SP - 1) / g.SP;
@@ -722,7 +819,7 @@ Geometry make_geometry(int nfilt, int H, int D, int Ty) {
 }
 
 bool geometry_ok(const Geometry& g) {
-  return g.Hp <= kMaxN && g.N >= 16 && g.N <= kMaxN && g.smem <= 227 * 1024;
+  return g.Hp <= g.maxN && g.N >= 16 && g.N <= g.maxN && g.smem <= 227 * 1024;
 }
 
 // Cost model of a tile shape: GEMM columns issued over the volume (tiles x
@@ -734,16 +831,17 @@ static long long tile_cost(const Geometry& g, int H, int D) {
   return ny * nz * (g.N + 16);
 }
 
-int candidate_tys(int nfilt, int H, int D, int* tys, int max_n) {
+int candidate_tys(int nfilt, int H, int D, int* tys, int max_n, bool tf32) {
   // the cheapest tile height for each plane-group count J (ties to the
   // taller tile), then the max_n cheapest of those
   long long best_cost[kMaxN + 1];
   int best_ty[kMaxN + 1];
   for (int j = 0; j <= kMaxN; j++) best_ty[j] = -1;
   const int lo = H < 10 ? H : 10;
-  const int hi = H < kMaxN - 6 ? H : kMaxN - 6;
+  const int maxN = tf32 ? kMaxNSparse : kMaxN;
+  const int hi = H < maxN - 6 ? H : maxN - 6;
   for (int ty = hi; ty >= lo; ty--) {
-    const Geometry g = make_geometry(nfilt, H, D, ty);
+    const Geometry g = make_geometry(nfilt, H, D, ty, tf32);
     if (!geometry_ok(g)) continue;
     const long long c = tile_cost(g, H, D);
     if (best_ty[g.J] < 0 || c < best_cost[g.J]) {
@@ -763,9 +861,9 @@ int candidate_tys(int nfilt, int H, int D, int* tys, int max_n) {
   return n;
 }
 
-int pick_ty(int nfilt, int H, int D) {
+int pick_ty(int nfilt, int H, int D, bool tf32) {
   int ty = -1;
-  return candidate_tys(nfilt, H, D, &ty, 1) == 1 ? ty : -1;
+  return candidate_tys(nfilt, H, D, &ty, 1, tf32) == 1 ? ty : -1;
 }
 
 cudaError_t bounded_wait_probe(int wait_ms, int* d_err, cudaStream_t st) {
@@ -788,7 +886,8 @@ cudaError_t init() {
 cudaError_t launch(const float* vol, int W, int H, int D, int batch, long long stride, const uint16_t* d_taps,
                    int nfilt, float* out, ActiveSet act, int* d_err, const Geometry& g, cudaStream_t st, bool tf32) {
   if (g_num_sms <= 0) return cudaErrorInitializationError;
-  if (!geometry_ok(g) || (nfilt != 3 && nfilt != 6) || g.SP != stacked_planes(nfilt) || batch <= 0)
+  if (!geometry_ok(g) || (nfilt != 3 && nfilt != 6) || g.SP != stacked_planes(nfilt) || batch <= 0 ||
+      (tf32 && g.N > kMaxNSparse))
     return cudaErrorInvalidValue;
   TileArgs a;
   a.vstride = stride;

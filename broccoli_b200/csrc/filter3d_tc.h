@@ -14,6 +14,9 @@ constexpr int kM = 128;    // GEMM M: (stacked plane, real filter, x offset) row
 constexpr int kK = 16;     // GEMM K: input samples along x per window
 constexpr int kXo = 10;    // outputs along x per window (kK - 6)
 constexpr int kMaxN = 256; // GEMM N limit (rows of one tile)
+// TF32 runs structured-sparse MMAs whose metadata takes one TMEM column
+// beyond both accumulators: N at most 240
+constexpr int kMaxNSparse = 240;
 
 // Tile geometry of one launch, chosen on the host.  The kernel is
 // persistent (one CTA per SM over all tiles of the launch).
@@ -27,6 +30,7 @@ struct Geometry {
   int NR;      // SP * RP
   int nstage;  // GEMMs per tile: (7 + SP - 1) * 7
   int smem;    // dynamic shared memory bytes of a CTA
+  int maxN;    // N limit of the precision (kMaxN, or kMaxNSparse for TF32)
 };
 
 int stacked_planes(int nfilt);
@@ -34,14 +38,14 @@ int num_stages(int nfilt);
 // Bytes of the packed Toeplitz taps (split BF16, or TF32: the same size) of
 // a bank of nfilt (3 or 6) complex filters, and the packing itself (dst
 // holds packed_tap_bytes/2 16-bit words).
-size_t packed_tap_bytes(int nfilt);
+size_t packed_tap_bytes(int nfilt, bool tf32);
 void pack_taps(const float* h_filters, int nfilt, uint16_t* dst, bool tf32);
-Geometry make_geometry(int nfilt, int H, int D, int Ty);
+Geometry make_geometry(int nfilt, int H, int D, int Ty, bool tf32);
 bool geometry_ok(const Geometry& g);
 // The max_n cheapest tile heights by the cost model, cheapest first; returns
 // how many were found.  pick_ty is the cheapest.
-int candidate_tys(int nfilt, int H, int D, int* tys, int max_n);
-int pick_ty(int nfilt, int H, int D);
+int candidate_tys(int nfilt, int H, int D, int* tys, int max_n, bool tf32);
+int pick_ty(int nfilt, int H, int D, bool tf32);
 cudaError_t init();
 // One CTA waits wait_ms (1..1000) on a barrier nothing completes, then sets *d_err.
 cudaError_t bounded_wait_probe(int wait_ms, int* d_err, cudaStream_t st);
