@@ -55,8 +55,11 @@
 //                  commit per two GEMMs)
 //   warps 4-11     epilogue: tcgen05.ld of the accumulator (TMEM lanes
 //                  32 (warp % 4) .., the two warps of a lane quarter on
-//                  alternate 16-column groups), transposed through shared
-//                  memory into 16-byte stores of the complex outputs
+//                  alternate 16-column groups); TF32 stores each lane's
+//                  values straight to global memory (a warp's store: 80
+//                  contiguous bytes per filter), BF16X3 transposes them
+//                  through shared memory into 16-byte stores (its GEMMs
+//                  bound the launch, and the direct stores slowed them)
 //
 // Two TMEM accumulators (2 x 256 of the SM's 512 columns) let the epilogue
 // of tile i run under the GEMMs of tile i + 1.  Every wait is bounded
@@ -625,50 +628,96 @@ filter3d_tc_kernel(const float* __restrict__ vol, const uint16_t* __restrict__ t
       tc_fence_after();
       const int x0 = xc * kXo, y0 = yt * g.Ty, z0 = zt * g.SP * g.J;
       const uint32_t lanecol = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(acc * 256);
-      for (int cbase = 0; cbase < g.N; cbase += kEpiCols) {
-        const int cend = cbase + kEpiCols < g.N ? cbase + kEpiCols : g.N;
-        for (int c0 = cbase + 16 * half; c0 < cend; c0 += 16 * (kEpiWarps / 4)) {
+      if (TF32) {
+        // each thread stores its row's outputs (filter f >> 1, re/im f & 1,
+        // x0 + xo) column by column straight from the accumulator: a warp's
+        // store covers 20 consecutive lanes = 80 contiguous bytes per filter
+        const int xg = x0 + xo;
+        const bool lane_ok = rvalid && xg < a.W;
+        const int ylim = g.Ty < a.H - y0 ? g.Ty : a.H - y0;
+        const int zrem = a.D - z0 - sp;
+        const int jl0 = zrem > 0 ? (zrem + g.SP - 1) / g.SP : 0;
+        const int jl = jl0 < g.J ? jl0 : g.J;
+        float* obase = out + (((long long)b * a.nfilt + (rvalid ? (f >> 1) : 0)) * V + xg) * 2 + (f & 1);
+        const long long ystep = 2ll * a.W, zwrap = 2ll * a.W * ((long long)g.SP * a.H - g.Hp);
+        constexpr int kStep = 16 * (kEpiWarps / 4);
+        bool arrived = false;
+        for (int c0 = 16 * half; c0 < g.N; c0 += kStep) {
           uint32_t v[16];
           tmem_ld16(lanecol + (uint32_t)c0, v);
-          if (rvalid) {
+          if (c0 + kStep >= g.N) {
+            // this thread's last read of the accumulator: the GEMMs of tile
+            // i + 2 may start once every epilogue thread is here
+            tc_fence_before();
+            mbar_arrive(&acc_empty[acc]);
+            arrived = true;
+          }
+          int j = c0 / g.Hp, yl = c0 - j * g.Hp;
+          float* p = obase + ((long long)(z0 + j * g.SP + sp) * a.H + y0 + yl) * ystep;
 #pragma unroll
-            for (int e = 0; e < 16; e++) E[((c0 + e - cbase) * g.SP + sp) * rowf + ke] = __uint_as_float(v[e]);
+          for (int e = 0; e < 16; e++) {
+            if (lane_ok && j < jl && yl < ylim) *p = __uint_as_float(v[e]);
+            p += ystep;
+            if (++yl == g.Hp) {
+              yl = 0;
+              j++;
+              p += zwrap;
+            }
           }
         }
-        if (cend >= g.N) {
-          // this accumulator is read out: the GEMMs of tile i + 2 may start
+        if (!arrived) {
           tc_fence_before();
           mbar_arrive(&acc_empty[acc]);
         }
-        epi_sync();
-        if (et < 30 * kEpiGroups) {
-          int nl = cgrp;
-          int j = (cbase + nl) / g.Hp, yl = cbase + nl - j * g.Hp;
-          const int xs = x0 + 2 * part;
-          for (; nl < cend - cbase; nl += kEpiGroups) {
-            const int z = z0 + j * g.SP + s2, y = y0 + yl;
-            if (j < g.J && yl < g.Ty && y < a.H && z < a.D && xs < a.W) {
-              const float4 qv = *reinterpret_cast<const float4*>(E + (nl * g.SP + s2) * rowf + k * 20 + part * 4);
-              float* dst = out + (((long long)b * a.nfilt + k) * V + ((long long)z * a.H + y) * a.W + xs) * 2;
-              if (xs + 1 < a.W && vec16) {
-                *reinterpret_cast<float4*>(dst) = qv;
-              } else {
-                *reinterpret_cast<float2*>(dst) = make_float2(qv.x, qv.y);
-                if (xs + 1 < a.W) *reinterpret_cast<float2*>(dst + 2) = make_float2(qv.z, qv.w);
-              }
+      } else {
+        // BF16X3 (tensor-bound: the direct stores above slow its GEMMs):
+        // chunks of kEpiCols columns transposed through shared memory
+        // into 16-byte stores of ten complex samples
+        for (int cbase = 0; cbase < g.N; cbase += kEpiCols) {
+          const int cend = cbase + kEpiCols < g.N ? cbase + kEpiCols : g.N;
+          for (int c0 = cbase + 16 * half; c0 < cend; c0 += 16 * (kEpiWarps / 4)) {
+            uint32_t v[16];
+            tmem_ld16(lanecol + (uint32_t)c0, v);
+            if (rvalid) {
+#pragma unroll
+              for (int e = 0; e < 16; e++) E[((c0 + e - cbase) * g.SP + sp) * rowf + ke] = __uint_as_float(v[e]);
             }
-            yl += kEpiGroups;  // Hp >= 7 and kEpiGroups <= 12: at most two wraps
-            if (yl >= g.Hp) {
-              yl -= g.Hp;
-              j++;
+          }
+          if (cend >= g.N) {
+            // this accumulator is read out: the GEMMs of tile i + 2 may start
+            tc_fence_before();
+            mbar_arrive(&acc_empty[acc]);
+          }
+          epi_sync();
+          if (et < 30 * kEpiGroups) {
+            int nl = cgrp;
+            int j = (cbase + nl) / g.Hp, yl = cbase + nl - j * g.Hp;
+            const int xs = x0 + 2 * part;
+            for (; nl < cend - cbase; nl += kEpiGroups) {
+              const int z = z0 + j * g.SP + s2, y = y0 + yl;
+              if (j < g.J && yl < g.Ty && y < a.H && z < a.D && xs < a.W) {
+                const float4 qv = *reinterpret_cast<const float4*>(E + (nl * g.SP + s2) * rowf + k * 20 + part * 4);
+                float* dst = out + (((long long)b * a.nfilt + k) * V + ((long long)z * a.H + y) * a.W + xs) * 2;
+                if (xs + 1 < a.W && vec16) {
+                  *reinterpret_cast<float4*>(dst) = qv;
+                } else {
+                  *reinterpret_cast<float2*>(dst) = make_float2(qv.x, qv.y);
+                  if (xs + 1 < a.W) *reinterpret_cast<float2*>(dst + 2) = make_float2(qv.z, qv.w);
+                }
+              }
+              yl += kEpiGroups;  // Hp >= 7 and kEpiGroups <= 12: at most two wraps
               if (yl >= g.Hp) {
                 yl -= g.Hp;
                 j++;
+                if (yl >= g.Hp) {
+                  yl -= g.Hp;
+                  j++;
+                }
               }
             }
           }
+          epi_sync();
         }
-        epi_sync();
       }
       i++;
     }
