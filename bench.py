@@ -700,7 +700,7 @@ def run_gpu(args, rank, world, local_rank):
     # is below the algorithmic bytes: the input comes partly from L2 (written
     # by the preceding resampling) and part of the output is still in L2
     # when the kernel ends.
-    tc_bytes_per_vol = ((34571776 + 150313472) if prec == L.PREC_TF32 else (17850368 + 48461056)) / 63
+    tc_bytes_per_vol = ((34503168 + 148295936) if prec == L.PREC_TF32 else (17850368 + 48461056)) / 63
     sym_bytes_per_vol = (34094848 + 147386624) / 63
     traffic = sym_bytes_per_vol * (T - 1) if symmetric_bank(fl) and tuple(SHAPE) == (33, 64, 64) else None
     tc_traffic = tc_bytes_per_vol * (T - 1) if tuple(SHAPE) == (33, 64, 64) else None
@@ -712,10 +712,13 @@ def run_gpu(args, rank, world, local_rank):
                 "GEMMs also issue are not counted")
     if prec == L.PREC_TF32:
         tf32_peak = bf16_peak / 2.0
-        roofline = {"kernel": "filter3d_tc_kernel<TF32> (tcgen05.mma kind::tf32, FP32 accumulate in TMEM)",
+        roofline = {"kernel": "filter3d_tc_kernel<TF32> (tcgen05.mma.sp kind::tf32, 1:2 structured-sparse "
+                              "banded taps, FP32 accumulate in TMEM)",
                     "bound": "tensor", "achieved": achieved, "peak": tf32_peak, "unit": "TFLOP/s",
                     "frac": achieved / tf32_peak,
-                    "peak_source": peak_src + " / 2: the dense kind::tf32 rate is half the kind::f16 rate",
+                    "peak_source": peak_src + " / 2: the dense kind::tf32 rate is half the kind::f16 rate (a "
+                                   "sparse K = 16 MMA multiplies the 8 stored values of each row: the useful "
+                                   "rate stays bounded by the dense one)",
                     "frac_of_bf16_peak": achieved / bf16_peak,
                     "flop_per_launch": f_flop, "flop_note": alg_note, "launch_ms": f_ms,
                     "filter_launch_ms": filter_ms, "traffic": tc_traffic,
