@@ -259,7 +259,7 @@ __device__ __forceinline__ void mma_tf32_sp(uint32_t tmem_d, uint64_t adesc, uin
 // 1) in bits 16 m1 .., K half k1; a nibble per sample pair j of that half
 // (pair P = 4 k1 + j: samples P and P + 8), 0b0100 keeping the first and
 // 0b1110 the second; row r's taps are samples xo .. xo + 6.
-__device__ __forceinline__ uint32_t sparse_metadata_word(int L, int SP, int nfilt) {
+__host__ __device__ __forceinline__ uint32_t sparse_metadata_word(int L, int SP, int nfilt) {
   const int m0 = L & 7, k1 = (L >> 3) & 1, m2 = L >> 4;
   uint32_t word = 0;
   for (int m1 = 0; m1 < 2; m1++) {
@@ -765,6 +765,8 @@ static float bf16_to_f(uint16_t h) {
   memcpy(&f, &u, 4);
   return f;
 }
+
+uint32_t metadata_word(int lane, int SP, int nfilt) { return sparse_metadata_word(lane, SP, nfilt); }
 
 int stacked_planes(int nfilt) { return nfilt == 3 ? 2 : 1; }
 int num_stages(int nfilt) { return (7 + stacked_planes(nfilt) - 1) * 7; }

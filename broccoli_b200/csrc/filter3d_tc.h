@@ -35,11 +35,16 @@ struct Geometry {
 
 int stacked_planes(int nfilt);
 int num_stages(int nfilt);
-// Bytes of the packed Toeplitz taps (split BF16, or TF32: the same size) of
-// a bank of nfilt (3 or 6) complex filters, and the packing itself (dst
-// holds packed_tap_bytes/2 16-bit words).
+// Bytes of the packed Toeplitz taps (split BF16, or TF32: the stored half
+// of the structured-sparse rows, half the bytes) of a bank of nfilt (3 or
+// 6) complex filters, and the packing itself (dst holds
+// packed_tap_bytes/2 16-bit words).
 size_t packed_tap_bytes(int nfilt, bool tf32);
 void pack_taps(const float* h_filters, int nfilt, uint16_t* dst, bool tf32);
+// The 32-bit sparsity-metadata word that the TF32 kernel writes to TMEM
+// lane `lane` (0..127) of its metadata column: which sample of each pair
+// (P, P + 8) a packed row keeps.
+uint32_t metadata_word(int lane, int SP, int nfilt);
 Geometry make_geometry(int nfilt, int H, int D, int Ty, bool tf32);
 bool geometry_ok(const Geometry& g);
 // The max_n cheapest tile heights by the cost model, cheapest first; returns
