@@ -71,9 +71,10 @@ struct brc_ctx {
   // stay the same from one call to the next
   DevBuf r2v_work, r2v_lin, r2v_prm, coh_res, coh_mat, coh_lin, coh_prm, coh_jobs;
   std::map<GraphKey, std::unique_ptr<GraphEntry>> graphs;
-  // packed split-BF16 taps of the tensor-core filtering, per filter bank
-  // (key: hash of the bank and its size); graphs may hold these pointers,
-  // so an entry lives as long as the graphs do
+  // packed taps of the tensor-core filtering (split BF16, or the stored
+  // half of TF32's structured-sparse rows), per filter bank and precision
+  // (key: hash of the bank, its size and the precision); graphs may hold
+  // these pointers, so an entry lives as long as the graphs do
   std::map<uint64_t, std::unique_ptr<DevBuf>> tc_taps;
   DevBuf tc_err;  // device int: a bounded wait of a tensor-core kernel gave up
   // device count of the iterations that registration graphs ran (their

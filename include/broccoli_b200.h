@@ -58,7 +58,8 @@ enum { BRC_TRANSLATION = 0, BRC_RIGID = 1, BRC_AFFINE = 2 };
  * form.  FP32_GENERAL: fp32, always all 343 taps.  BF16X3: split-bf16
  * (hi*hi + hi*lo + lo*hi) products on the tensor cores with fp32
  * accumulation.  TF32: data and taps rounded to tf32 (10-bit mantissa), one
- * product per tap on the tensor cores, fp32 accumulation. */
+ * product per tap on the tensor cores (structured-sparse MMAs: the banded
+ * tap matrix stores one value per sample pair), fp32 accumulation. */
 enum { BRC_PREC_FP32 = 0, BRC_PREC_BF16X3 = 1, BRC_PREC_FP32_GENERAL = 2, BRC_PREC_TF32 = 3 };
 
 typedef struct brc_ctx brc_ctx;
