@@ -467,6 +467,26 @@ def normalisation_rates(ctx, L, prec, sampler, accuracy_on: bool, reps: int = 5)
     return {"t1_to_template": out_t1, "cohort": out_coh}
 
 
+def max_over_ranks(values, world: int, device) -> list:
+    """Each value's maximum over the ranks: the slowest rank's time.  One
+    all_reduce (MAX) of a float64 tensor on `device` (the rank's GPU under
+    NCCL); on one rank the values themselves."""
+    if world <= 1:
+        return [float(v) for v in values]
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v) for v in values], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.cpu()]
+
+
+def whole_job_rate(world: int, steps: int, slowest_ms: float) -> float:
+    """Registrations per second of the whole job: each of the `world`
+    replicas registers T - 1 volumes per step, and the job lasts as long as
+    its slowest rank."""
+    return (T - 1) * world * steps / (slowest_ms / 1000.0)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -678,17 +698,11 @@ def run_gpu(args, rank, world, local_rank):
         sampler.stop()
 
     # ---- reduce over ranks ----
-    t_max = ms
-    e_max = e2e_ms
-    if world > 1:
-        tt = torch.tensor([ms, e2e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max, e_max = float(tt[0]), float(tt[1])
+    t_max, e_max = max_over_ranks([ms, e2e_ms], world, dev)
     if rank != 0:
         return
-    regs = (T - 1) * world * args.steps
-    value = regs / (t_max / 1000.0)
-    e2e_value = regs / (e_max / 1000.0)
+    value = whole_job_rate(world, args.steps, t_max)
+    e2e_value = whole_job_rate(world, args.steps, e_max)
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
     clocks = sampler.section_summary("main") if sampler else None
